@@ -1,0 +1,157 @@
+/*
+ * b200la.h -- C ABI of the B200 (sm_100a) backend for LinearAlgebra's
+ * LU-solve path.
+ *
+ * Every entry point takes plain pointers and sizes.  Matrix, pivot, right-hand
+ * side and workspace pointers are DEVICE pointers (the reference's GPU
+ * contract, docs/gpu_backend_design.md:22-36); `stream` is a cudaStream_t
+ * passed as void* (NULL = the legacy default stream).  Matrices are row-major.
+ * Pivots are int64, 1-based, LAPACK style: pivot[i] is the row swapped with row
+ * i at step i, applied in increasing i (include/matrix_operation/
+ * lu_decomposition.h:25-26).  The library never allocates: callers query
+ * *_workspace_size() and pass that many bytes of device memory.
+ *
+ * Return value: a b200la_status.  Negative values are errors (the C++ shim in
+ * include/linalg_b200/backend_b200.h turns them into exceptions, like the
+ * reference's LINALG_CHECK); b200la_last_error() gives a message for the
+ * calling thread's most recent error.
+ */
+#ifndef B200LA_H
+#define B200LA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#define B200LA_API __attribute__((visibility("default")))
+#else
+#define B200LA_API
+#endif
+
+typedef enum b200la_status
+{
+    B200LA_SUCCESS              = 0,
+    B200LA_SINGULAR             = 1,  /* exact zero pivot: factors complete, U singular */
+    B200LA_NOT_CONVERGED        = 2,  /* refinement did not reach the requested accuracy */
+    B200LA_INVALID_ARGUMENT     = -1, /* null pointer, bad size/stride, aliasing */
+    B200LA_WORKSPACE_TOO_SMALL  = -2,
+    B200LA_CUDA_ERROR           = -3, /* a CUDA runtime call or launch failed */
+    B200LA_DEVICE_TIMEOUT       = -4, /* a bounded device-side wait gave up */
+    B200LA_NOT_SUPPORTED        = -5  /* no sm_100 device, or an unsupported size */
+} b200la_status;
+
+/* linear_solver modes, same values as the reference's linear_solver_type
+ * (include/matrix_operation/linear_solver.h:15-21). */
+#define B200LA_LU_LINEAR_SOLVER 1
+#define B200LA_LU_UPFRONT_LINEAR_SOLVER 2
+
+B200LA_API const char* b200la_last_error(void);
+B200LA_API const char* b200la_status_string(int status);
+B200LA_API int         b200la_version(void);
+
+/* Number of kernel launches the library has issued in this process. */
+B200LA_API int64_t b200la_launch_count(void);
+
+/* Launch recorder for measurement: while started, every launch of a kernel
+ * class in `class_mask` (bit 0 panel, 1 row interchange + U12 solve,
+ * 2 trailing update, 3 triangular solves, 4 general GEMM, 5 mixed-precision
+ * factorization GEMM, 6 FP64 residual, 7 batched solver) is bracketed by a
+ * pair of CUDA events on its stream.  b200la_profile_stop synchronizes those
+ * events and returns the summed device time (ms) and launch count of one
+ * class; it also stops recording. */
+B200LA_API void b200la_profile_start(int class_mask);
+B200LA_API int  b200la_profile_stop(int kernel_class, double* total_ms, int64_t* launches);
+
+/* ---- lu_decomposition ---------------------------------------------------
+ * Replaces lu_decomposition<T, Backend>::apply / ::workspace_size
+ * (include/matrix_operation/lu_decomposition.h:38-53; CUDA_BLAS sibling
+ * src/matrix_operation/gpu/cublas/lu_decomposition_cublas.cpp:172-203).
+ * m: n x n row-major, lda == n (the reference's lda is the order and the
+ * stride).  pivot: n device int64.  info: HOST int, may be NULL; 0 or the
+ * 1-based index of the first exactly-zero U diagonal entry.  Synchronizes
+ * `stream` before returning (the reference's contract for this op).
+ * Returns B200LA_SUCCESS, B200LA_SINGULAR or an error. */
+B200LA_API size_t b200la_dgetrf_workspace_size(int64_t n);
+B200LA_API size_t b200la_sgetrf_workspace_size(int64_t n);
+B200LA_API int    b200la_dgetrf(double* m, int64_t n, int64_t* pivot, void* workspace,
+       size_t workspace_bytes, int* info, void* stream);
+B200LA_API int    b200la_sgetrf(float* m, int64_t n, int64_t* pivot, void* workspace,
+       size_t workspace_bytes, int* info, void* stream);
+
+/* Asynchronous factorization (no host synchronization): the status lands in
+ * the workspace's device status block; read it with b200la_workspace_status.
+ * Extension beyond the reference API (needed for graph capture and
+ * pipelines). */
+B200LA_API int b200la_dgetrf_async(double* m, int64_t n, int64_t* pivot, void* workspace,
+    size_t workspace_bytes, void* stream);
+B200LA_API int b200la_sgetrf_async(float* m, int64_t n, int64_t* pivot, void* workspace,
+    size_t workspace_bytes, void* stream);
+
+/* Copies the device status block at the start of `workspace` to the host
+ * (synchronizing `stream`): *info = LAPACK info of the last factorization,
+ * returns B200LA_SUCCESS / B200LA_SINGULAR / B200LA_DEVICE_TIMEOUT. */
+B200LA_API int b200la_workspace_status(const void* workspace, int* info, void* stream);
+
+/* ---- linear_solver (LU modes) --------------------------------------------
+ * Replaces linear_solver<T, Backend>::apply / ::workspace_size
+ * (include/matrix_operation/linear_solver.h:46-64; NATIVE semantics of
+ * src/matrix_operation/cpu/native/linear_solver_native.cpp:149-191).
+ * mode B200LA_LU_LINEAR_SOLVER factors m in place (pivot written) and then
+ * solves, unless the factorization found an exact zero pivot, in which case x
+ * is left unchanged; B200LA_LU_UPFRONT_LINEAR_SOLVER reuses m and pivot as
+ * given.  x: n device values, overwritten with the solution.  Asynchronous
+ * on `stream`. */
+B200LA_API size_t b200la_dgesv_workspace_size(int64_t n, int mode);
+B200LA_API size_t b200la_sgesv_workspace_size(int64_t n, int mode);
+B200LA_API int    b200la_dgesv(double* m, int64_t* pivot, int64_t n, double* x, int mode,
+       void* workspace, size_t workspace_bytes, void* stream);
+B200LA_API int    b200la_sgesv(float* m, int64_t* pivot, int64_t n, float* x, int mode,
+       void* workspace, size_t workspace_bytes, void* stream);
+
+/* Multi-right-hand-side solve with existing factors and pivots: x is
+ * n x nrhs row-major with row stride ldx >= nrhs.  Extension (the reference
+ * linear_solver is single-RHS). */
+B200LA_API size_t b200la_dgetrs_workspace_size(int64_t n, int64_t nrhs);
+B200LA_API int    b200la_dgetrs(const double* lu, const int64_t* pivot, int64_t n, int64_t nrhs,
+       double* x, int64_t ldx, void* workspace, size_t workspace_bytes, void* stream);
+
+/* ---- triangular_solver ----------------------------------------------------
+ * Replaces triangular_solver<T, Backend>::apply / ::workspace_size
+ * (include/matrix_operation/triangular_solver.h:22-37; argument checks of
+ * src/common/triangular_solver_checks.h:11-35).  Solves op(A) X = B; A n x n
+ * (row stride lda >= n), B and X n x nrhs (ldb, ldx >= nrhs).  Only the
+ * selected triangle is read; the diagonal is not read when unit != 0.  A and
+ * B are preserved; A, B, X must be distinct buffers.  Asynchronous. */
+B200LA_API size_t b200la_dtrsm_workspace_size(int64_t n, int64_t nrhs);
+B200LA_API size_t b200la_strsm_workspace_size(int64_t n, int64_t nrhs);
+B200LA_API int    b200la_dtrsm(int upper, int transpose, int unit, int64_t n, int64_t nrhs,
+       const double* a, int64_t lda, const double* b, int64_t ldb, double* x, int64_t ldx,
+       void* workspace, size_t workspace_bytes, void* stream);
+B200LA_API int    b200la_strsm(int upper, int transpose, int unit, int64_t n, int64_t nrhs,
+       const float* a, int64_t lda, const float* b, int64_t ldb, float* x, int64_t ldx,
+       void* workspace, size_t workspace_bytes, void* stream);
+
+/* ---- multiplication --------------------------------------------------------
+ * Replaces multiplication<T, Backend>::apply (16-argument form) /
+ * ::workspace_size (include/matrix_operation/multiplication.h:47-62,107-114):
+ * c = alpha op(a) op(b) + beta c, row-major, BLAS contract (beta == 0: c is
+ * write-only; alpha == 0: a and b are not read).  Asynchronous. */
+B200LA_API size_t b200la_dgemm_workspace_size(int64_t rows, int64_t cols, int64_t depth);
+B200LA_API size_t b200la_sgemm_workspace_size(int64_t rows, int64_t cols, int64_t depth);
+B200LA_API int    b200la_dgemm(int transpose_a, int transpose_b, int64_t rows, int64_t cols,
+       int64_t depth, double alpha, const double* a, int64_t lda, const double* b, int64_t ldb,
+       double beta, double* c, int64_t ldc, void* workspace, size_t workspace_bytes,
+       void* stream);
+B200LA_API int    b200la_sgemm(int transpose_a, int transpose_b, int64_t rows, int64_t cols,
+       int64_t depth, float alpha, const float* a, int64_t lda, const float* b, int64_t ldb,
+       float beta, float* c, int64_t ldc, void* workspace, size_t workspace_bytes, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* B200LA_H */

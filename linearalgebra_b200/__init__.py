@@ -1,0 +1,21 @@
+"""B200-native (sm_100a) backend for LinearAlgebra's LU-solve path.
+
+Host-side Python mirror of the reference's operator interface over the C ABI
+of libb200la.so (include/b200la.h).  The CUDA library is the only compute
+path; importing works without it, the first call raises if it is missing.
+"""
+from . import workloads  # noqa: F401
+from ._lib import B200Error, B200InvalidArgument  # noqa: F401
+from .api import (  # noqa: F401
+    LU_LINEAR_SOLVER,
+    LU_UPFRONT_LINEAR_SOLVER,
+    gemm,
+    gesv,
+    getrf,
+    getrs,
+    linear_solver,
+    lu_decomposition,
+    multiplication,
+    triangular_solver,
+    trsm,
+)

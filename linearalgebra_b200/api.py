@@ -1,0 +1,179 @@
+"""Python mirror of the reference's operator interface for the LU-solve path,
+over the C ABI.
+
+The reference's API is ``op<T, Backend>::apply(...)`` / ``workspace_size(...)``
+(include/matrix_operation/{lu_decomposition,linear_solver,triangular_solver,
+multiplication}.h).  Here ``T`` is the tensors' dtype (float64 or float32) and
+the backend is always the B200 one.  Arguments keep the reference's names,
+order and meaning; device buffers are torch CUDA tensors (row-major,
+contiguous where the reference expects a packed matrix); ``stream`` is a
+``torch.cuda.Stream`` or ``None`` for the current stream.  Errors raise like
+the reference's LINALG_CHECK (ValueError subclasses for invalid arguments).
+
+Convenience wrappers (``getrf``, ``gesv``, ``getrs``, ``trsm``, ``gemm``)
+allocate the workspace with torch and return results.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import torch
+
+from . import _lib
+
+LU_LINEAR_SOLVER = _lib.LU_LINEAR_SOLVER
+LU_UPFRONT_LINEAR_SOLVER = _lib.LU_UPFRONT_LINEAR_SOLVER
+
+
+def _prefix(dtype: torch.dtype) -> str:
+    if dtype == torch.float64:
+        return "d"
+    if dtype == torch.float32:
+        return "s"
+    raise TypeError(f"unsupported dtype {dtype}: the LU path is float64/float32")
+
+
+def _stream(stream) -> int:
+    if stream is None:
+        return torch.cuda.current_stream().cuda_stream
+    if isinstance(stream, int):
+        return stream
+    return stream.cuda_stream
+
+
+def _ptr(t) -> int:
+    if t is None:
+        return 0
+    if isinstance(t, int):
+        return t
+    return t.data_ptr()
+
+
+def workspace(nbytes: int, device=None) -> torch.Tensor:
+    """A device byte buffer of at least `nbytes` (at least 256 bytes)."""
+    return torch.empty(max(int(nbytes), 256), dtype=torch.uint8,
+                       device=device if device is not None else "cuda")
+
+
+class lu_decomposition:
+    """lu_decomposition<T, B200> (include/matrix_operation/lu_decomposition.h:15-54)."""
+
+    @staticmethod
+    def workspace_size(lda: int, dtype=torch.float64) -> int:
+        return int(getattr(_lib.load(), f"b200la_{_prefix(dtype)}getrf_workspace_size")(lda))
+
+    @staticmethod
+    def apply(m: torch.Tensor, lda: int, pivot: torch.Tensor, workspace: torch.Tensor,
+              workspace_size: int, stream=None):
+        """Factor m in place; returns (ok, info) like the reference's bool and
+        host info.  Synchronizes the stream."""
+        info = ctypes.c_int(-1)
+        f = getattr(_lib.load(), f"b200la_{_prefix(m.dtype)}getrf")
+        st = f(_ptr(m), lda, _ptr(pivot), _ptr(workspace), workspace_size,
+               ctypes.addressof(info), _stream(stream))
+        _lib.check(st, allow=(_lib.SUCCESS, _lib.SINGULAR))
+        return st == _lib.SUCCESS, int(info.value)
+
+
+class linear_solver:
+    """linear_solver<T, B200>, LU modes (include/matrix_operation/linear_solver.h:26-65)."""
+
+    @staticmethod
+    def workspace_size(lda: int, type: int = LU_LINEAR_SOLVER, dtype=torch.float64) -> int:
+        return int(getattr(_lib.load(), f"b200la_{_prefix(dtype)}gesv_workspace_size")(lda, type))
+
+    @staticmethod
+    def apply(m, pivot, lda: int, x, type: int, workspace, workspace_size: int, stream=None):
+        f = getattr(_lib.load(), f"b200la_{_prefix(m.dtype)}gesv")
+        _lib.check(f(_ptr(m), _ptr(pivot), lda, _ptr(x), type, _ptr(workspace), workspace_size,
+                     _stream(stream)))
+
+
+class triangular_solver:
+    """triangular_solver<T, B200> (include/matrix_operation/triangular_solver.h:20-38)."""
+
+    @staticmethod
+    def workspace_size(n: int, nrhs: int, dtype=torch.float64) -> int:
+        return int(getattr(_lib.load(), f"b200la_{_prefix(dtype)}trsm_workspace_size")(n, nrhs))
+
+    @staticmethod
+    def apply(upper: bool, transpose: bool, unit_diagonal: bool, n: int, nrhs: int, a, lda: int,
+              b, ldb: int, x, ldx: int, workspace, workspace_size: int, stream=None):
+        f = getattr(_lib.load(), f"b200la_{_prefix(a.dtype)}trsm")
+        _lib.check(f(int(upper), int(transpose), int(unit_diagonal), n, nrhs, _ptr(a), lda,
+                     _ptr(b), ldb, _ptr(x), ldx, _ptr(workspace), workspace_size, _stream(stream)))
+
+
+class multiplication:
+    """multiplication<T, B200> (include/matrix_operation/multiplication.h:15-114)."""
+
+    @staticmethod
+    def workspace_size(rows: int, columns: int, depth: int, dtype=torch.float64) -> int:
+        return int(getattr(_lib.load(), f"b200la_{_prefix(dtype)}gemm_workspace_size")(rows, columns, depth))
+
+    @staticmethod
+    def apply(transpose_a: bool, transpose_b: bool, rows: int, columns: int, depth: int,
+              alpha, a, lda: int, b, ldb: int, beta, c, ldc: int, workspace=None,
+              workspace_size: int = 0, stream=None):
+        f = getattr(_lib.load(), f"b200la_{_prefix(c.dtype)}gemm")
+        _lib.check(f(int(transpose_a), int(transpose_b), rows, columns, depth, float(alpha),
+                     _ptr(a), lda, _ptr(b), ldb, float(beta), _ptr(c), ldc, _ptr(workspace),
+                     workspace_size, _stream(stream)))
+
+
+# ----------------------------------------------------------------------------
+# convenience wrappers
+# ----------------------------------------------------------------------------
+def getrf(m: torch.Tensor, stream=None):
+    """In-place LU of the square row-major CUDA tensor m.
+    Returns (pivot[int64, 1-based], info)."""
+    n = m.shape[0]
+    assert m.is_contiguous() and m.shape == (n, n)
+    piv = torch.empty(n, dtype=torch.int64, device=m.device)
+    nbytes = lu_decomposition.workspace_size(n, m.dtype)
+    ws = workspace(nbytes, m.device)
+    _, info = lu_decomposition.apply(m, n, piv, ws, ws.numel(), stream)
+    return piv, info
+
+
+def gesv(m: torch.Tensor, x: torch.Tensor, pivot: torch.Tensor | None = None,
+         type: int = LU_LINEAR_SOLVER, stream=None):
+    """linear_solver LU modes in place on (m, x).  Returns the pivot tensor."""
+    n = m.shape[0]
+    if pivot is None:
+        pivot = torch.empty(n, dtype=torch.int64, device=m.device)
+    nbytes = linear_solver.workspace_size(n, type, m.dtype)
+    ws = workspace(nbytes, m.device)
+    linear_solver.apply(m, pivot, n, x, type, ws, ws.numel(), stream)
+    return pivot
+
+
+def getrs(lu: torch.Tensor, pivot: torch.Tensor, x: torch.Tensor, stream=None):
+    """Solve with existing factors, x (n x nrhs, row-major) in place."""
+    n = lu.shape[0]
+    nrhs = 1 if x.dim() == 1 else x.shape[1]
+    ldx = 1 if x.dim() == 1 else x.stride(0)
+    lib = _lib.load()
+    nbytes = lib.b200la_dgetrs_workspace_size(n, nrhs)
+    ws = workspace(nbytes, lu.device)
+    _lib.check(lib.b200la_dgetrs(_ptr(lu), _ptr(pivot), n, nrhs, _ptr(x), ldx, _ptr(ws),
+                                 ws.numel(), _stream(stream)))
+    return x
+
+
+def trsm(upper, transpose, unit, a, b, x=None, stream=None):
+    n = a.shape[0]
+    nrhs = b.shape[1]
+    if x is None:
+        x = torch.empty_like(b)
+    triangular_solver.apply(upper, transpose, unit, n, nrhs, a, a.stride(0), b, b.stride(0),
+                            x, x.stride(0), None, 0, stream)
+    return x
+
+
+def gemm(transpose_a, transpose_b, alpha, a, b, beta, c, stream=None):
+    rows, cols = c.shape
+    depth = a.shape[0] if transpose_a else a.shape[1]
+    multiplication.apply(transpose_a, transpose_b, rows, cols, depth, alpha, a, a.stride(0),
+                         b, b.stride(0), beta, c, c.stride(0), None, 0, stream)
+    return c

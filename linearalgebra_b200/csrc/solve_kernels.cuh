@@ -1,0 +1,449 @@
+// Kernels for the triangular solves, the pivot application of the LU solve
+// and the general GEMM (multiplication op).
+//
+//   k_copy2d / k_scale2d   X = B, C = beta C (row-major, strided)
+//   k_perm_from_pivots     LAPACK pivots -> final row permutation (one CTA)
+//   k_gather_rows          Y[i, :] = X[perm[i], :]
+//   k_trsm_diag            solve one 64-row diagonal block of op(A) X = B
+//   k_trsm_update          X[rows] -= op(A)[rows, block] X[block]
+//   k_gemm                 c = alpha op(a) op(b) + beta c
+//
+// Every kernel that belongs to a solve can be gated on the factorization's
+// device status: with `gate` non-null it returns without touching anything
+// when the factorization found an exact zero pivot (the reference's
+// linear_solver only solves when lu_decomposition succeeded) or a device
+// error was raised.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "common.cuh"
+
+namespace b200la
+{
+
+constexpr int kTrsmBlock = 64;  // rows per diagonal block
+constexpr int kTrsmCols  = 64;  // right-hand-side columns per CTA in k_trsm_diag
+
+__device__ __forceinline__ bool gated(const DeviceStatus* gate)
+{
+    return gate != nullptr && (ld_volatile_i32(&gate->error) != 0 || gate->first_zero >= 0);
+}
+
+template <typename T>
+__global__ void k_copy2d(const T* __restrict__ src, int64_t lds, T* __restrict__ dst, int64_t ldd,
+    int rows, int cols, const DeviceStatus* gate)
+{
+    if (gated(gate))
+    {
+        return;
+    }
+    const int64_t total = (int64_t)rows * cols;
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total;
+         e += (int64_t)gridDim.x * blockDim.x)
+    {
+        const int64_t r = e / cols, c = e - (e / cols) * cols;
+        dst[r * ldd + c] = src[r * lds + c];
+    }
+}
+
+template <typename T>
+__global__ void k_scale2d(T* __restrict__ c, int64_t ldc, int rows, int cols, T beta)
+{
+    const int64_t total = (int64_t)rows * cols;
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total;
+         e += (int64_t)gridDim.x * blockDim.x)
+    {
+        const int64_t r = e / cols, cc = e - (e / cols) * cols;
+        T&            v = c[r * ldc + cc];
+        v               = beta == T(0) ? T(0) : v * beta;
+    }
+}
+
+// Final permutation of the pivot sequence: after applying the swaps
+// (i, pivot[i]-1) for i = 0..n-1 in order to a vector y, y[i] = x[perm[i]].
+// One CTA; the simulation runs in shared memory when n fits (48K entries),
+// else in global memory.  A pivot outside [i+1, n] raises DEV_BAD_PIVOT and
+// is treated as no swap.
+__global__ void k_perm_from_pivots(const int64_t* __restrict__ pivot, int n,
+    int32_t* __restrict__ perm, int use_smem, DeviceStatus* st, const DeviceStatus* gate)
+{
+    extern __shared__ int32_t sperm[];
+    if (gated(gate))
+    {
+        return;
+    }
+    int32_t* p = use_smem ? sperm : perm;
+    for (int i = threadIdx.x; i < n; i += blockDim.x)
+    {
+        p[i] = i;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0)
+    {
+        bool bad = false;
+        for (int i = 0; i < n; ++i)
+        {
+            const int64_t q = pivot[i] - 1;
+            if (q < i || q >= n)
+            {
+                bad = true;
+                continue;
+            }
+            const int32_t t = p[i];
+            p[i]            = p[q];
+            p[q]            = t;
+        }
+        if (bad)
+        {
+            raise_error(st, DEV_BAD_PIVOT, 2);
+        }
+    }
+    __syncthreads();
+    if (use_smem)
+    {
+        for (int i = threadIdx.x; i < n; i += blockDim.x)
+        {
+            perm[i] = p[i];
+        }
+    }
+}
+
+template <typename T>
+__global__ void k_gather_rows(const T* __restrict__ x, int64_t ldx, const int32_t* __restrict__ perm,
+    T* __restrict__ y, int64_t ldy, int n, int nrhs, const DeviceStatus* gate)
+{
+    if (gated(gate))
+    {
+        return;
+    }
+    const int64_t total = (int64_t)n * nrhs;
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total;
+         e += (int64_t)gridDim.x * blockDim.x)
+    {
+        const int64_t r = e / nrhs, c = e - (e / nrhs) * nrhs;
+        y[r * ldy + c] = x[(int64_t)perm[r] * ldx + c];
+    }
+}
+
+// op(A)[i][j] with op = transpose or not.
+template <typename T>
+__device__ __forceinline__ T opa(const T* a, int64_t lda, bool transpose, int64_t i, int64_t j)
+{
+    return transpose ? a[j * lda + i] : a[i * lda + j];
+}
+
+// Solve the diagonal block rows [r0, r0+bw) of op(A) X = X in place, for
+// right-hand-side columns [blockIdx.x*kTrsmCols, ...).  One thread per
+// column; the block's triangle is staged in shared memory.  eff_upper
+// selects back substitution.
+template <typename T>
+__global__ void __launch_bounds__(kTrsmCols) k_trsm_diag(const T* __restrict__ a, int64_t lda,
+    bool transpose, bool eff_upper, bool unit, int r0, int bw, T* __restrict__ x, int64_t ldx,
+    int nrhs, const DeviceStatus* gate)
+{
+    __shared__ T tri[kTrsmBlock][kTrsmBlock + 1];
+    if (gated(gate))
+    {
+        return;
+    }
+    const int tid = threadIdx.x;
+    for (int e = tid; e < bw * bw; e += kTrsmCols)
+    {
+        const int i = e / bw, j = e - (e / bw) * bw;
+        const bool in_tri = eff_upper ? (j >= i) : (j <= i);
+        T          v      = T(0);
+        if (in_tri && !(unit && i == j))
+        {
+            v = opa(a, lda, transpose, (int64_t)r0 + i, (int64_t)r0 + j);
+        }
+        tri[i][j] = v;
+    }
+    __syncthreads();
+    const int col = blockIdx.x * kTrsmCols + tid;
+    if (col >= nrhs)
+    {
+        return;
+    }
+    T v[kTrsmBlock];
+#pragma unroll
+    for (int i = 0; i < kTrsmBlock; ++i)
+    {
+        v[i] = i < bw ? x[(int64_t)(r0 + i) * ldx + col] : T(0);
+    }
+    if (!eff_upper)
+    {
+#pragma unroll
+        for (int p = 0; p < kTrsmBlock; ++p)
+        {
+            if (p < bw)
+            {
+                if (!unit)
+                {
+                    v[p] = v[p] / tri[p][p];
+                }
+#pragma unroll
+                for (int i = p + 1; i < kTrsmBlock; ++i)
+                {
+                    if (i < bw)
+                    {
+                        v[i] = fma(-tri[i][p], v[p], v[i]);
+                    }
+                }
+            }
+        }
+    }
+    else
+    {
+#pragma unroll
+        for (int p = kTrsmBlock - 1; p >= 0; --p)
+        {
+            if (p < bw)
+            {
+                if (!unit)
+                {
+                    v[p] = v[p] / tri[p][p];
+                }
+#pragma unroll
+                for (int i = 0; i < p; ++i)
+                {
+                    v[i] = fma(-tri[i][p], v[p], v[i]);
+                }
+            }
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < kTrsmBlock; ++i)
+    {
+        if (i < bw)
+        {
+            x[(int64_t)(r0 + i) * ldx + col] = v[i];
+        }
+    }
+}
+
+// X[rows r in [u0, u0+um)] -= op(A)[r, r0 .. r0+bw) X[r0 .. r0+bw, :].
+// CTA tile: 64 rows x 16 columns, 256 threads (thread: 1 row x 4 columns).
+constexpr int kUpdCols = 16;
+template <typename T>
+__global__ void __launch_bounds__(256) k_trsm_update(const T* __restrict__ a, int64_t lda,
+    bool transpose, int r0, int bw, int u0, int um, T* __restrict__ x, int64_t ldx, int nrhs,
+    const DeviceStatus* gate)
+{
+    __shared__ T As[64][kTrsmBlock + 1];
+    __shared__ T Xs[kTrsmBlock][kUpdCols];
+    if (gated(gate))
+    {
+        return;
+    }
+    const int tid = threadIdx.x;
+    const int m0  = u0 + blockIdx.y * 64;
+    const int c0  = blockIdx.x * kUpdCols;
+    for (int e = tid; e < 64 * kTrsmBlock; e += 256)
+    {
+        int r, p;
+        if (transpose)
+        {  // op(A)[m][p] = a[p][m]: read along m for coalescing
+            p = e / 64;
+            r = e - p * 64;
+        }
+        else
+        {
+            r = e / kTrsmBlock;
+            p = e - r * kTrsmBlock;
+        }
+        const int m = m0 + r;
+        As[r][p]    = (m < u0 + um && p < bw) ? opa(a, lda, transpose, (int64_t)m, (int64_t)r0 + p) : T(0);
+    }
+    for (int e = tid; e < kTrsmBlock * kUpdCols; e += 256)
+    {
+        const int p = e / kUpdCols, c = e - (e / kUpdCols) * kUpdCols;
+        Xs[p][c]    = (p < bw && c0 + c < nrhs) ? x[(int64_t)(r0 + p) * ldx + c0 + c] : T(0);
+    }
+    __syncthreads();
+    const int r  = tid >> 2;
+    const int cg = (tid & 3) * 4;
+    const int m  = m0 + r;
+    if (m >= u0 + um)
+    {
+        return;
+    }
+    T acc[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+    {
+        acc[j] = T(0);
+    }
+    for (int p = 0; p < bw; ++p)
+    {
+        const T av = As[r][p];
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+        {
+            acc[j] = fma(av, Xs[p][cg + j], acc[j]);
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+    {
+        const int c = c0 + cg + j;
+        if (c < nrhs)
+        {
+            x[(int64_t)m * ldx + c] -= acc[j];
+        }
+    }
+}
+
+// c = alpha op(a) op(b) + beta c.  CTA tile 128 x 64, K in chunks of 32,
+// thread mapping as k_trailing.  For op(b) = b (the two cases whose
+// reference loop nest updates c one depth index at a time) the update is
+// c <- beta c, then c = fma(alpha a_ik, b_kj, c) for k in order; with op(b)
+// = b^T the dot product is accumulated first, then c = fma(alpha, dot, beta c).
+constexpr int kGemmKC = 32;
+template <typename T> constexpr size_t gemm_smem_bytes()
+{
+    return sizeof(T) * (128 * (kGemmKC + 1) + kGemmKC * 64);
+}
+
+template <typename T, bool TA, bool TB>
+__global__ void __launch_bounds__(128, 2) k_gemm(int rows, int cols, int depth, T alpha,
+    const T* __restrict__ a, int64_t lda, const T* __restrict__ b, int64_t ldb, T beta,
+    T* __restrict__ c, int64_t ldc)
+{
+    extern __shared__ __align__(16) unsigned char gemm_smem[];
+    T(*As)[kGemmKC + 1] = reinterpret_cast<T(*)[kGemmKC + 1]>(gemm_smem);  // [128]
+    T(*Bs)[64] = reinterpret_cast<T(*)[64]>(gemm_smem + sizeof(T) * 128 * (kGemmKC + 1));
+
+    const int m0   = blockIdx.y * 128;
+    const int n0   = blockIdx.x * 64;
+    const int tid  = threadIdx.x;
+    const int lane = tid & 31;
+    const int warp = tid >> 5;
+    const int tr   = lane >> 3;
+    const int tc   = lane & 7;
+
+    T acc[8][8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i)
+    {
+        const int r = m0 + warp * 32 + tr + 4 * i;
+#pragma unroll
+        for (int j = 0; j < 8; ++j)
+        {
+            const int cc = n0 + 2 * tc + 16 * (j >> 1) + (j & 1);
+            T         v  = T(0);
+            if (!TB && beta != T(0) && r < rows && cc < cols)
+            {
+                const T cv = c[(int64_t)r * ldc + cc];
+                v          = beta == T(1) ? cv : cv * beta;
+            }
+            acc[i][j] = v;
+        }
+    }
+    for (int k0 = 0; k0 < depth; k0 += kGemmKC)
+    {
+        const int kc = min(kGemmKC, depth - k0);
+        for (int e = tid; e < 128 * kGemmKC; e += 128)
+        {
+            int r, p;
+            if (TA)
+            {
+                p = e / 128;
+                r = e - p * 128;
+            }
+            else
+            {
+                r = e / kGemmKC;
+                p = e - r * kGemmKC;
+            }
+            const int m = m0 + r;
+            T         v = T(0);
+            if (m < rows && p < kc)
+            {
+                v = TA ? a[(int64_t)(k0 + p) * lda + m] : a[(int64_t)m * lda + k0 + p];
+                if (!TB)
+                {
+                    v = alpha * v;
+                }
+            }
+            As[r][p] = v;
+        }
+        for (int e = tid; e < kGemmKC * 64; e += 128)
+        {
+            int p, cc;
+            if (TB)
+            {
+                cc = e / kGemmKC;
+                p  = e - cc * kGemmKC;
+            }
+            else
+            {
+                p  = e / 64;
+                cc = e - p * 64;
+            }
+            const int j = n0 + cc;
+            T         v = T(0);
+            if (j < cols && p < kc)
+            {
+                v = TB ? b[(int64_t)j * ldb + k0 + p] : b[(int64_t)(k0 + p) * ldb + j];
+            }
+            Bs[p][cc] = v;
+        }
+        __syncthreads();
+        for (int p = 0; p < kc; ++p)
+        {
+            T av[8], bv[8];
+#pragma unroll
+            for (int i = 0; i < 8; ++i)
+            {
+                av[i] = As[warp * 32 + tr + 4 * i][p];
+            }
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+            {
+                bv[2 * j]     = Bs[p][2 * tc + 16 * j];
+                bv[2 * j + 1] = Bs[p][2 * tc + 16 * j + 1];
+            }
+#pragma unroll
+            for (int i = 0; i < 8; ++i)
+            {
+#pragma unroll
+                for (int j = 0; j < 8; ++j)
+                {
+                    acc[i][j] = fma(av[i], bv[j], acc[i][j]);
+                }
+            }
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int i = 0; i < 8; ++i)
+    {
+        const int r = m0 + warp * 32 + tr + 4 * i;
+        if (r >= rows)
+        {
+            continue;
+        }
+#pragma unroll
+        for (int j = 0; j < 8; ++j)
+        {
+            const int cc = n0 + 2 * tc + 16 * (j >> 1) + (j & 1);
+            if (cc < cols)
+            {
+                T& out = c[(int64_t)r * ldc + cc];
+                if (TB)
+                {
+                    const T base = beta == T(0) ? T(0) : (beta == T(1) ? out : out * beta);
+                    out          = fma(alpha, acc[i][j], base);
+                }
+                else
+                {
+                    out = acc[i][j];
+                }
+            }
+        }
+    }
+}
+
+}  // namespace b200la

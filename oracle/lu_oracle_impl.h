@@ -1,0 +1,456 @@
+/*
+ * Type-generic body of the CPU oracle (included twice by lu_oracle.c, once
+ * with T=double / SUF=d and once with T=float / SUF=s).
+ *
+ * TEST INFRASTRUCTURE ONLY: a plain-C restatement of the reference's NATIVE
+ * LU-solve path, used by tests/ and by bench.py's CPU-baseline leg as the
+ * checker.  The B200 library never links, loads or calls it.
+ *
+ * Rounding is pinned to the reference build's: the reference's scalar loops
+ * `y -= a * x` and `s += a * b` are contracted by g++ into single fused
+ * multiply-adds, so every such update here is an explicit fma().  With that,
+ * the factors, pivots and solutions below are bit-identical to the
+ * reference's oracle/_ref build (checked by tests/test_oracle.py).
+ */
+
+#define OR_CAT2(a, b) a##b
+#define OR_CAT(a, b) OR_CAT2(a, b)
+#define OR_FN(name) OR_CAT(or_, OR_CAT(SUF, name))
+#define OR_FMA OR_CAT(fma, FMA_SUF)
+#define OR_ABS OR_CAT(fabs, FMA_SUF)
+
+/* Panel width of the blocked LU, lu_decomposition_native.cpp:285
+ * (kLuBlockSize = 64). */
+#define OR_LU_BLOCK 64
+/* Row-block height of the triangular solver, triangular_solver_native.cpp:17
+ * (triangular_block = 32). */
+#define OR_TRSM_BLOCK 32
+
+/* y[c] -= a * x[c], c in [0, len): lu_decomposition_native.cpp:69-122
+ * (lu_axpy_sub, scalar branch), one fused multiply-add per element. */
+static void OR_CAT(axpy_sub_, SUF)(T* y, const T* x, T a, int64_t len)
+{
+    for (int64_t c = 0; c < len; ++c)
+    {
+        y[c] = OR_FMA(-a, x[c], y[c]);
+    }
+}
+
+/* Row dot product, linear_solver_native.cpp:41-88 (lu_dot, scalar branch):
+ * a single accumulator summed in index order.  The reference build (g++ -O3,
+ * AVX2+FMA) computes that loop's products a full vector (4 doubles / 8
+ * floats) at a time, then one half vector, and adds them one by one in
+ * order, so those products are rounded before the add; the few products left
+ * after that are fused into the sum.  The same rounding is reproduced here so
+ * the solutions match the reference build bit for bit. */
+static T OR_CAT(dots_, SUF)(const T* a, int64_t sa, const T* b, int64_t sb, int64_t count)
+{
+    const int64_t vec  = (int64_t)(32 / sizeof(T));
+    const int64_t half = vec / 2;
+    const int64_t main = count >= vec ? (count / vec) * vec : 0;
+    T             s    = 0;
+    int64_t       j    = 0;
+    for (; j < main; ++j)
+    {
+        const T p = a[j * sa] * b[j * sb];
+        s         = s + p;
+    }
+    if (count - j >= half)
+    {
+        for (int64_t q = 0; q < half; ++q, ++j)
+        {
+            const T p = a[j * sa] * b[j * sb];
+            s         = s + p;
+        }
+    }
+    for (; j < count; ++j)
+    {
+        s = OR_FMA(a[j * sa], b[j * sb], s);
+    }
+    return s;
+}
+
+static T OR_CAT(dot_, SUF)(const T* a, const T* b, int64_t count)
+{
+    return OR_CAT(dots_, SUF)(a, 1, b, 1, count);
+}
+
+/* Unblocked panel factorization over columns [start, start+width), all rows
+ * below: lu_decomposition_native.cpp:158-232 (lu_panel_factor).
+ *  - pivot search: initial candidate |a[i][i]|, then rows i+1..n-1 with a
+ *    strict '>' (first maximum wins; a NaN never displaces);
+ *  - row swap over columns [0, start+width) only;
+ *  - exactly-zero pivot: record the first one, skip the column;
+ *  - multiplier: times 1/diag when |diag| >= smallest normal, else divided. */
+static void OR_CAT(panel_, SUF)(T* m, int64_t n, int64_t start, int64_t width, int64_t* pivot,
+    int64_t* first_zero)
+{
+    for (int64_t ii = 0; ii < width; ++ii)
+    {
+        const int64_t i   = start + ii;
+        T*            row = m + i * n;
+        T             mx  = OR_ABS(row[i]);
+        int64_t       imx = i;
+        for (int64_t k = i + 1; k < n; ++k)
+        {
+            const T v = OR_ABS(m[k * n + i]);
+            if (v > mx)
+            {
+                mx  = v;
+                imx = k;
+            }
+        }
+        pivot[i] = imx + 1;
+        if (imx != i)
+        {
+            T* prow = m + imx * n;
+            for (int64_t j = 0; j < start + width; ++j)
+            {
+                const T t = row[j];
+                row[j]    = prow[j];
+                prow[j]   = t;
+            }
+        }
+        const T diag = row[i];
+        if (diag == (T)0)
+        {
+            if (*first_zero < 0)
+            {
+                *first_zero = i;
+            }
+            continue;
+        }
+        const int use_recip = OR_ABS(diag) >= T_MIN_NORMAL;
+        const T   recip     = use_recip ? (T)((T)1 / diag) : (T)1;
+        const T*  li        = row + start;
+        for (int64_t r = i + 1; r < n; ++r)
+        {
+            T* lr = m + r * n + start;
+            if (use_recip)
+            {
+                lr[ii] = lr[ii] * recip;
+            }
+            else
+            {
+                lr[ii] = lr[ii] / diag;
+            }
+            OR_CAT(axpy_sub_, SUF)(lr + ii + 1, li + ii + 1, lr[ii], width - ii - 1);
+        }
+    }
+}
+
+/* Replays pivot[start..start+width) on columns [start+width, n) in increasing
+ * order: lu_decomposition_native.cpp:247-271 (lu_apply_pivots_to_trailing). */
+static void OR_CAT(laswp_trailing_, SUF)(T* m, int64_t n, int64_t start, int64_t width,
+    const int64_t* pivot)
+{
+    for (int64_t i = start; i < start + width; ++i)
+    {
+        const int64_t p = pivot[i] - 1;
+        if (p != i)
+        {
+            T* ri = m + i * n;
+            T* rp = m + p * n;
+            for (int64_t j = start + width; j < n; ++j)
+            {
+                const T t = ri[j];
+                ri[j]     = rp[j];
+                rp[j]     = t;
+            }
+        }
+    }
+}
+
+/* In-place blocked right-looking LU with partial pivoting of the row-major
+ * n x n matrix m: lu_decomposition_native.cpp:329-429
+ * (lu_decomposition_blocked_impl).  `delta` is rest*rest scratch (NULL lets
+ * the oracle allocate it).  Returns 0 if U is nonsingular, else the 1-based
+ * index of the first exactly-zero pivot (also written to *info). */
+int OR_FN(getrf)(T* m, int64_t n, int64_t* pivot, int* info)
+{
+    if (m == NULL || pivot == NULL || n <= 0)
+    {
+        return -1;
+    }
+    for (int64_t i = 0; i < n; ++i)
+    {
+        pivot[i] = i + 1;
+    }
+    const int64_t rest0 = n > OR_LU_BLOCK ? n - OR_LU_BLOCK : 0;
+    T*            delta = NULL;
+    if (rest0 > 0)
+    {
+        delta = (T*)malloc(sizeof(T) * (size_t)rest0 * (size_t)rest0);
+        if (delta == NULL)
+        {
+            return -2;
+        }
+    }
+    int64_t first_zero = -1;
+    for (int64_t k = 0; k < n; k += OR_LU_BLOCK)
+    {
+        const int64_t bs = (n - k) < OR_LU_BLOCK ? (n - k) : OR_LU_BLOCK;
+        OR_CAT(panel_, SUF)(m, n, k, bs, pivot, &first_zero);
+        const int64_t rest = n - k - bs;
+        if (rest == 0)
+        {
+            continue;
+        }
+        OR_CAT(laswp_trailing_, SUF)(m, n, k, bs, pivot);
+        /* U12 = L11^-1 A12 by row axpys, :370-380 */
+        for (int64_t ii = 0; ii < bs; ++ii)
+        {
+            T* rowf = m + (k + ii) * n;
+            T* ri   = rowf + k + bs;
+            for (int64_t p = 0; p < ii; ++p)
+            {
+                OR_CAT(axpy_sub_, SUF)(ri, m + (k + p) * n + k + bs, rowf[k + p], rest);
+            }
+        }
+        /* delta = L21 * U12 (multiplication_native.cpp:1701-1718, the
+         * non-vectorized NN loop: c starts at 0, then c += a_ik * b_kj over k
+         * in order), then A22 -= delta as a separate pass, :400-422. */
+        for (int64_t r = 0; r < rest; ++r)
+        {
+            T*       dr = delta + r * rest;
+            const T* lr = m + (k + bs + r) * n + k;
+            for (int64_t c = 0; c < rest; ++c)
+            {
+                dr[c] = 0;
+            }
+            for (int64_t p = 0; p < bs; ++p)
+            {
+                const T  a  = lr[p];
+                const T* up = m + (k + p) * n + k + bs;
+                for (int64_t c = 0; c < rest; ++c)
+                {
+                    dr[c] = OR_FMA(a, up[c], dr[c]);
+                }
+            }
+        }
+        for (int64_t r = 0; r < rest; ++r)
+        {
+            OR_CAT(axpy_sub_, SUF)(m + (k + bs + r) * n + k + bs, delta + r * rest, (T)1, rest);
+        }
+    }
+    free(delta);
+    if (info)
+    {
+        *info = (int)(first_zero + 1);
+    }
+    return (int)(first_zero + 1);
+}
+
+/* Solve with existing factors, linear_solver_native.cpp:90-113 (lu_solve):
+ * sequential pivot swaps on x, unit-lower forward substitution, then back
+ * substitution dividing by U's diagonal. */
+void OR_FN(getrs)(const T* m, const int64_t* pivot, int64_t n, T* x)
+{
+    for (int64_t i = 0; i < n; ++i)
+    {
+        const int64_t p = pivot[i] - 1;
+        const T       t = x[i];
+        x[i]            = x[p];
+        x[p]            = t;
+    }
+    for (int64_t i = 0; i < n; ++i)
+    {
+        x[i] -= OR_CAT(dot_, SUF)(m + i * n, x, i);
+    }
+    for (int64_t i = n - 1; i >= 0; --i)
+    {
+        const T* ri = m + i * n;
+        x[i]        = (x[i] - OR_CAT(dot_, SUF)(ri + i + 1, x + i + 1, n - i - 1)) / ri[i];
+    }
+}
+
+/* linear_solver LU modes, linear_solver_native.cpp:149-191: mode 1 factors
+ * then solves only if the factorization succeeded; mode 2 reuses the factors
+ * and pivots.  Returns the getrf status for mode 1, 0 for mode 2. */
+int OR_FN(gesv)(T* m, int64_t* pivot, int64_t n, T* x, int mode)
+{
+    if (m == NULL || x == NULL || n <= 0)
+    {
+        return -1;
+    }
+    if (mode == 1)
+    {
+        const int st = OR_FN(getrf)(m, n, pivot, NULL);
+        if (st == 0)
+        {
+            OR_FN(getrs)(m, pivot, n, x);
+        }
+        return st;
+    }
+    if (mode == 2)
+    {
+        OR_FN(getrs)(m, pivot, n, x);
+        return 0;
+    }
+    return -1;
+}
+
+/* c = alpha op(a) op(b) + beta c, row-major, BLAS contract:
+ * multiplication_native.cpp:1542-1567 (beta applied up front; beta == 0
+ * overwrites c), :1807-1814 (alpha == 0 quick return), and the scalar loop
+ * nests :1701-1787 for the four transpose combinations. */
+int OR_FN(gemm)(int ta, int tb, int64_t rows, int64_t cols, int64_t depth, T alpha, const T* a,
+    int64_t lda, const T* b, int64_t ldb, T beta, T* c, int64_t ldc)
+{
+    if (!a || !b || !c || rows <= 0 || cols <= 0 || depth <= 0 || lda <= 0 || ldb <= 0 || ldc <= 0)
+    {
+        return -1;
+    }
+    if (beta != (T)1)
+    {
+        for (int64_t i = 0; i < rows; ++i)
+        {
+            for (int64_t j = 0; j < cols; ++j)
+            {
+                c[i * ldc + j] = beta == (T)0 ? (T)0 : c[i * ldc + j] * beta;
+            }
+        }
+    }
+    if (alpha == (T)0)
+    {
+        return 0;
+    }
+    if (!ta && !tb)
+    {
+        for (int64_t i = 0; i < rows; ++i)
+        {
+            for (int64_t k = 0; k < depth; ++k)
+            {
+                const T s = alpha * a[i * lda + k];
+                for (int64_t j = 0; j < cols; ++j)
+                {
+                    c[i * ldc + j] = OR_FMA(s, b[k * ldb + j], c[i * ldc + j]);
+                }
+            }
+        }
+    }
+    else if (ta && !tb)
+    {
+        for (int64_t k = 0; k < depth; ++k)
+        {
+            for (int64_t i = 0; i < rows; ++i)
+            {
+                const T s = alpha * a[k * lda + i];
+                for (int64_t j = 0; j < cols; ++j)
+                {
+                    c[i * ldc + j] = OR_FMA(s, b[k * ldb + j], c[i * ldc + j]);
+                }
+            }
+        }
+    }
+    else
+    {
+        for (int64_t i = 0; i < rows; ++i)
+        {
+            for (int64_t j = 0; j < cols; ++j)
+            {
+                /* the reference's dot loops (contiguous for NT, strided a
+                 * for TT) round like lu_dot in its build */
+                const T s = ta ? OR_CAT(dots_, SUF)(a + i, lda, b + j * ldb, 1, depth)
+                               : OR_CAT(dot_, SUF)(a + i * lda, b + j * ldb, depth);
+                c[i * ldc + j] = OR_FMA(alpha, s, c[i * ldc + j]);
+            }
+        }
+    }
+    return 0;
+}
+
+/* op(A) X = B, triangular_solver_native.cpp:67-179: X = B, then row blocks of
+ * 32 in substitution order; inside a block, sequential row axpys and a
+ * division by the diagonal (unless unit); below/above it, a GEMM of the
+ * solved block followed by a separate subtraction pass.  A and B are only
+ * read, only the selected triangle is read, the diagonal is not read when
+ * unit != 0.  Argument checks as src/common/triangular_solver_checks.h:11-35. */
+int OR_FN(trsm)(int upper, int transpose, int unit, int64_t n, int64_t nrhs, const T* a,
+    int64_t lda, const T* b, int64_t ldb, T* x, int64_t ldx)
+{
+    if (n <= 0 || nrhs <= 0 || n > 2147483647LL || nrhs > 2147483647LL)
+    {
+        return -1;
+    }
+    if (!a || !b || !x || a == b || a == x || b == x)
+    {
+        return -1;
+    }
+    if (lda < n || ldb < nrhs || ldx < nrhs)
+    {
+        return -1;
+    }
+    const int64_t lim = INT64_MAX / n;
+    if (lda > lim || ldb > lim || ldx > lim)
+    {
+        return -1;
+    }
+    T* update = NULL;
+    if (n > OR_TRSM_BLOCK)
+    {
+        update = (T*)malloc(sizeof(T) * (size_t)n * (size_t)nrhs);
+        if (!update)
+        {
+            return -2;
+        }
+    }
+    for (int64_t i = 0; i < n; ++i)
+    {
+        for (int64_t j = 0; j < nrhs; ++j)
+        {
+            x[i * ldx + j] = b[i * ldb + j];
+        }
+    }
+#define OR_COEF(i, j) (transpose ? a[(j) * lda + (i)] : a[(i) * lda + (j)])
+    const int eff_upper = (upper != 0) != (transpose != 0);
+    for (int64_t done = 0; done < n; done += OR_TRSM_BLOCK)
+    {
+        const int64_t width = (n - done) < OR_TRSM_BLOCK ? (n - done) : OR_TRSM_BLOCK;
+        const int64_t begin = eff_upper ? n - done - width : done;
+        const int64_t end   = begin + width;
+        for (int64_t step = 0; step < width; ++step)
+        {
+            const int64_t i   = eff_upper ? end - step - 1 : begin + step;
+            T*            row = x + i * ldx;
+            const int64_t k0  = eff_upper ? i + 1 : begin;
+            const int64_t k1  = eff_upper ? end : i;
+            for (int64_t k = k0; k < k1; ++k)
+            {
+                OR_CAT(axpy_sub_, SUF)(row, x + k * ldx, OR_COEF(i, k), nrhs);
+            }
+            if (!unit)
+            {
+                const T d = OR_COEF(i, i);
+                for (int64_t j = 0; j < nrhs; ++j)
+                {
+                    row[j] = row[j] / d;
+                }
+            }
+        }
+        const int64_t first = eff_upper ? 0 : end;
+        const int64_t rows  = eff_upper ? begin : n - end;
+        if (rows == 0)
+        {
+            continue;
+        }
+        const T* blk = transpose ? a + begin * lda + first : a + first * lda + begin;
+        OR_FN(gemm)(transpose, 0, rows, nrhs, width, (T)1, blk, lda, x + begin * ldx, ldx, (T)0,
+            update, nrhs);
+        for (int64_t r = 0; r < rows; ++r)
+        {
+            OR_CAT(axpy_sub_, SUF)(x + (first + r) * ldx, update + r * nrhs, (T)1, nrhs);
+        }
+    }
+#undef OR_COEF
+    free(update);
+    return 0;
+}
+
+#undef OR_CAT2
+#undef OR_CAT
+#undef OR_FN
+#undef OR_FMA
+#undef OR_ABS
+#undef OR_LU_BLOCK
+#undef OR_TRSM_BLOCK

@@ -1,0 +1,105 @@
+"""Generate the golden fixtures for the LU-solve path from the reference's own
+NATIVE build (oracle/_ref/libref_native.so, built by oracle/Makefile from the
+reference sources).
+
+Run from the repository root, where the reference build exists:
+
+    make -f oracle/Makefile && python tests/golden/make_golden.py
+
+Writes tests/golden/lu_golden.npz.  Every input is seeded (numpy PCG64) or a
+closed-form known-answer matrix; each array's name says what it is.
+"""
+from __future__ import annotations
+
+import hashlib
+import math
+import os
+import sys
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+sys.path.insert(0, ROOT)
+
+from oracle import Oracle  # noqa: E402
+from linearalgebra_b200.workloads import (  # noqa: E402
+    known_answer_matrices,
+    random_matrix,
+    system,
+    triangular_cases,
+)
+
+LU_SIZES = (1, 2, 3, 17, 63, 64, 65, 130, 200)
+
+OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "lu_golden.npz")
+
+
+def sha(a: np.ndarray) -> str:
+    return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
+
+
+def main() -> None:
+    ref = Oracle("reference")
+    out: dict[str, np.ndarray] = {}
+
+    # 1. seeded LU cases (float64 and float32): inputs regenerated from the
+    #    seed by linearalgebra_b200.workloads; the fixture holds the
+    #    reference's factors.
+    for n in LU_SIZES:
+        for dt in ("f64", "f32"):
+            a = random_matrix(n, seed=1000 + n, dtype=np.float64 if dt == "f64" else np.float32)
+            lu, piv, info = ref.getrf(a)
+            out[f"lu_{dt}_{n}_a_sha"] = np.array(sha(a))
+            out[f"lu_{dt}_{n}_lu"] = lu
+            out[f"lu_{dt}_{n}_piv"] = piv
+            out[f"lu_{dt}_{n}_info"] = np.array(info)
+
+    # 2. known-answer matrices (zero pivots, tiny scale, subnormal pivot)
+    for dt, npdt in (("f64", np.float64), ("f32", np.float32)):
+        for name, aa in known_answer_matrices(npdt).items():
+            lu, piv, info = ref.getrf(aa)
+            out[f"ka_{name}_{dt}_a"] = aa
+            out[f"ka_{name}_{dt}_lu"] = lu
+            out[f"ka_{name}_{dt}_piv"] = piv
+            out[f"ka_{name}_{dt}_info"] = np.array(info)
+
+    # 3. the n=512 plain FP64 LU + solve workload: A ~ N(0,1), x_true ~ U[-1,1]
+    a, x_true, b = system(512, seed=512)
+    m, piv, x = ref.gesv(a, b)
+    out["cfg1_a_sha"] = np.array(sha(a))
+    out["cfg1_b_sha"] = np.array(sha(b))
+    out["cfg1_lu_sha"] = np.array(sha(m))
+    out["cfg1_piv"] = piv
+    out["cfg1_x"] = x
+    out["cfg1_lu_diag"] = np.diag(m).copy()
+
+    # 4. triangular solver known-answer cases (reference outputs)
+    for key, case in triangular_cases(np.float64).items():
+        upper, transpose, unit, n, nrhs, lda, ldb, ldx, a_t, b_t, expected = case
+        x = np.full((n, ldx), -123.0)
+        ref.trsm(upper, transpose, unit, n, nrhs, a_t, lda, b_t, ldb, x, ldx)
+        out[f"trsm_{key}_x"] = x
+
+    # 5. GEMM cases, all four transpose combinations, alpha/beta variants
+    rng = np.random.default_rng(77)
+    for (m_, n_, k_) in ((7, 5, 3), (65, 33, 64), (40, 24, 33)):
+        for ta in (0, 1):
+            for tb in (0, 1):
+                a_ = rng.standard_normal((k_, m_) if ta else (m_, k_))
+                b_ = rng.standard_normal((n_, k_) if tb else (k_, n_))
+                c0 = rng.standard_normal((m_, n_))
+                key = f"gemm_{m_}_{n_}_{k_}_{ta}{tb}"
+                out[key + "_a"] = a_
+                out[key + "_b"] = b_
+                out[key + "_c0"] = c0
+                for alpha, beta in ((1.0, 0.0), (2.5, -0.5), (0.0, 2.0)):
+                    c = c0.copy()
+                    ref.gemm(ta, tb, m_, n_, k_, alpha, a_, a_.shape[1], b_, b_.shape[1], beta, c, n_)
+                    out[f"{key}_{alpha}_{beta}_c"] = c
+
+    np.savez_compressed(OUT, **out)
+    print(f"wrote {OUT}: {len(out)} arrays, {os.path.getsize(OUT)} bytes")
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,70 @@
+"""C-ABI checks that need no GPU: the library loads, exports every symbol
+include/b200la.h declares, sizes its workspaces on the host, and rejects
+invalid arguments before touching a device."""
+import ctypes
+
+import pytest
+
+from linearalgebra_b200 import _lib
+
+
+def test_library_exports_every_declared_symbol():
+    lib = _lib.load()
+    declared = _lib.declared_symbols()
+    assert len(declared) >= 20
+    missing = [s for s in declared if not hasattr(lib, s)]
+    assert not missing, missing
+    # every declared function has a ctypes signature in the binding
+    assert set(declared) <= set(_lib.SIGNATURES), set(declared) - set(_lib.SIGNATURES)
+
+
+def test_workspace_sizes_are_host_side_and_consistent():
+    lib = _lib.load()
+    for n in (1, 64, 512, 16384):
+        d = lib.b200la_dgetrf_workspace_size(n)
+        s = lib.b200la_sgetrf_workspace_size(n)
+        assert d > 0 and s > 0 and s <= d
+        assert lib.b200la_dgesv_workspace_size(n, 1) >= d + 8 * n
+        assert lib.b200la_dgesv_workspace_size(n, 2) == lib.b200la_dgesv_workspace_size(n, 1)
+        assert lib.b200la_dgetrs_workspace_size(n, 64) >= 8 * n * 64
+    assert lib.b200la_dgesv_workspace_size(16, 3) == 0  # Cholesky modes: not provided
+    assert lib.b200la_dgesv_workspace_size(0, 1) == 0
+
+
+def test_status_strings():
+    lib = _lib.load()
+    for st in (0, 1, 2, -1, -2, -3, -4, -5):
+        assert lib.b200la_status_string(st)
+    assert lib.b200la_version() >= 100
+
+
+def test_invalid_arguments_rejected_without_device():
+    lib = _lib.load()
+    info = ctypes.c_int(0)
+    st = lib.b200la_dgetrf(None, 4, None, None, 0, ctypes.addressof(info), None)
+    assert st == _lib.INVALID_ARGUMENT
+    assert "must not be null" in _lib.last_error()
+    st = lib.b200la_dgetrf(1 << 20, 0, 1 << 20, 1 << 20, 1 << 20, None, None)
+    assert st == _lib.INVALID_ARGUMENT and "lda must be positive" in _lib.last_error()
+    st = lib.b200la_dgetrf(1 << 20, 8, 1 << 20, 1 << 20, 16, None, None)
+    assert st == _lib.WORKSPACE_TOO_SMALL
+    # triangular_solver argument checks (src/common/triangular_solver_checks.h)
+    p = 1 << 20
+    assert lib.b200la_dtrsm(0, 0, 0, 0, 1, p, 1, p + 64, 1, p + 128, 1, None, 0, None) == _lib.INVALID_ARGUMENT
+    assert lib.b200la_dtrsm(0, 0, 0, 4, 1, p, 4, p, 1, p + 128, 1, None, 0, None) == _lib.INVALID_ARGUMENT
+    assert "distinct" in _lib.last_error()
+    assert lib.b200la_dtrsm(0, 0, 0, 4, 2, p, 3, p + 64, 2, p + 128, 2, None, 0, None) == _lib.INVALID_ARGUMENT
+    assert "row stride" in _lib.last_error()
+    # multiplication argument checks
+    assert lib.b200la_dgemm(0, 0, 0, 1, 1, 1.0, p, 1, p, 1, 0.0, p, 1, None, 0, None) == _lib.INVALID_ARGUMENT
+    assert lib.b200la_dgemm(0, 0, 1, 1, 1, 1.0, None, 1, p, 1, 0.0, p, 1, None, 0, None) == _lib.INVALID_ARGUMENT
+    # linear_solver: Cholesky modes are not part of this backend
+    assert lib.b200la_dgesv(p, p, 4, p, 3, p, 1 << 20, None) == _lib.NOT_SUPPORTED
+
+
+def test_python_errors_map_to_exceptions():
+    with pytest.raises(ValueError):
+        _lib.check(_lib.INVALID_ARGUMENT)
+    with pytest.raises(_lib.B200Error):
+        _lib.check(_lib.CUDA_ERROR)
+    assert _lib.check(_lib.SINGULAR, allow=(_lib.SUCCESS, _lib.SINGULAR)) == _lib.SINGULAR

@@ -1,0 +1,146 @@
+"""CPU checks of the oracle (no GPU): the plain-C restatement against the
+golden fixtures produced by the reference's own NATIVE build, and against
+that build directly when it is present."""
+import hashlib
+import os
+
+import numpy as np
+import pytest
+
+from linearalgebra_b200.workloads import (
+    KNOWN_ANSWER_INFO,
+    known_answer_matrices,
+    random_matrix,
+    system,
+    triangular_cases,
+)
+from oracle import REF_LIB, Oracle
+
+LU_SIZES = (1, 2, 3, 17, 63, 64, 65, 130, 200)
+EPS64 = np.finfo(np.float64).eps
+
+
+def sha(a):
+    return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
+
+
+@pytest.mark.parametrize("n", LU_SIZES)
+@pytest.mark.parametrize("dt", ["f64", "f32"])
+def test_port_lu_matches_golden_bitwise(port, golden, n, dt):
+    a = random_matrix(n, seed=1000 + n, dtype=np.float64 if dt == "f64" else np.float32)
+    assert sha(a) == str(golden[f"lu_{dt}_{n}_a_sha"]), "seeded generator drifted"
+    lu, piv, info = port.getrf(a)
+    assert np.array_equal(piv, golden[f"lu_{dt}_{n}_piv"])
+    assert np.array_equal(lu, golden[f"lu_{dt}_{n}_lu"])
+    assert info == int(golden[f"lu_{dt}_{n}_info"])
+
+
+@pytest.mark.parametrize("name", sorted(KNOWN_ANSWER_INFO))
+@pytest.mark.parametrize("dt,npdt", [("f64", np.float64), ("f32", np.float32)])
+def test_port_known_answers(port, golden, name, dt, npdt):
+    a = known_answer_matrices(npdt)[name]
+    lu, piv, info = port.getrf(a)
+    assert info == KNOWN_ANSWER_INFO[name]
+    assert info == int(golden[f"ka_{name}_{dt}_info"])
+    assert np.array_equal(piv, golden[f"ka_{name}_{dt}_piv"])
+    np.testing.assert_array_equal(lu, golden[f"ka_{name}_{dt}_lu"])
+    assert np.all(np.isfinite(lu))
+    n = a.shape[0]
+    assert np.all((piv >= np.arange(1, n + 1)) & (piv <= n))
+    # P L U reconstructs A (reference test tolerance: 16 eps)
+    L = np.tril(lu.astype(np.float64), -1) + np.eye(n)
+    U = np.triu(lu.astype(np.float64))
+    r = L @ U
+    for i in range(n - 1, -1, -1):
+        p = piv[i] - 1
+        if p != i:
+            r[[i, p]] = r[[p, i]]
+    tol = 16 * np.finfo(npdt).eps
+    if name == "subnormal":
+        tol = np.finfo(npdt).tiny
+    assert np.max(np.abs(r - a)) <= tol
+
+
+def test_port_config1_solve_matches_golden(port, golden):
+    a, x_true, b = system(512, seed=512)
+    assert sha(a) == str(golden["cfg1_a_sha"])
+    assert sha(b) == str(golden["cfg1_b_sha"])
+    m, piv, x = port.gesv(a, b)
+    assert np.array_equal(piv, golden["cfg1_piv"])
+    assert sha(m) == str(golden["cfg1_lu_sha"])
+    assert np.array_equal(x, golden["cfg1_x"])
+    eta = port.backward_error(a, x, b)
+    assert eta <= 10 * 512 * EPS64
+    assert port.min_pivot_gap(a) > 1e-9
+
+
+def test_port_upfront_mode_reuses_factors(port):
+    a, _, b = system(100, seed=3)
+    m, piv, x1 = port.gesv(a, b)
+    _, _, x2 = port.gesv(m, b, mode=2, pivot=piv)
+    assert np.array_equal(x1, x2)
+
+
+def test_port_singular_leaves_x(port):
+    a = known_answer_matrices(np.float64)["rank_def"]
+    b = np.array([1.0, 2.0, 3.0])
+    _, _, x = port.gesv(a, b)
+    assert np.array_equal(x, b)
+
+
+@pytest.mark.parametrize("key", sorted(triangular_cases(np.float64)))
+def test_port_trsm_known_answers(port, golden, key):
+    upper, transpose, unit, n, nrhs, lda, ldb, ldx, a, b, expected = triangular_cases(np.float64)[key]
+    a0, b0 = a.copy(), b.copy()
+    x = np.full((n, ldx), -123.0)
+    port.trsm(upper, transpose, unit, n, nrhs, a, lda, b, ldb, x, ldx)
+    assert np.array_equal(x, golden[f"trsm_{key}_x"])
+    np.testing.assert_allclose(x[:, :nrhs], expected[:, :nrhs], rtol=0, atol=1e-13)
+    assert np.all(x[:, nrhs:] == -123.0)
+    assert np.array_equal(a0, a, equal_nan=True) and np.array_equal(b0, b)
+
+
+def test_port_trsm_rejects_bad_arguments(port):
+    a = np.eye(4)
+    b = np.ones((4, 2))
+    x = np.zeros((4, 2))
+    with pytest.raises(ValueError):
+        port.trsm(0, 0, 0, 0, 2, a, 4, b, 2, x, 2)
+    with pytest.raises(ValueError):
+        port.trsm(0, 0, 0, 4, 2, a, 3, b, 2, x, 2)
+    with pytest.raises(ValueError):
+        port.trsm(0, 0, 0, 4, 2, a, 4, b, 2, b, 2)
+
+
+def test_port_gemm_matches_golden(port, golden):
+    keys = sorted({k.rsplit("_", 1)[0] for k in golden.files if k.startswith("gemm_") and k.endswith("_a")})
+    assert keys
+    for key in keys:
+        _, m, n, k, tt = key.split("_")
+        m, n, k = int(m), int(n), int(k)
+        ta, tb = int(tt[0]), int(tt[1])
+        a, b, c0 = golden[key + "_a"], golden[key + "_b"], golden[key + "_c0"]
+        for alpha, beta in ((1.0, 0.0), (2.5, -0.5), (0.0, 2.0)):
+            c = c0.copy()
+            port.gemm(ta, tb, m, n, k, alpha, a, a.shape[1], b, b.shape[1], beta, c, n)
+            assert np.array_equal(c, golden[f"{key}_{alpha}_{beta}_c"]), (key, alpha, beta)
+
+
+@pytest.mark.skipif(not os.path.exists(REF_LIB), reason="reference build not present")
+@pytest.mark.parametrize("n", [1, 5, 64, 65, 129, 257, 300])
+def test_port_equals_reference_build(port, n):
+    ref = Oracle("reference")
+    for npdt in (np.float64, np.float32):
+        a = random_matrix(n, seed=77 + n, dtype=npdt)
+        lp, pp, ip = port.getrf(a)
+        lr, pr, ir = ref.getrf(a)
+        assert np.array_equal(pp, pr) and np.array_equal(lp, lr) and ip == ir
+        x = np.random.default_rng(n).uniform(-1, 1, n).astype(npdt)
+        b = (a.astype(np.float64) @ x.astype(np.float64)).astype(npdt)
+        assert np.array_equal(port.gesv(a, b)[2], ref.gesv(a, b)[2])
+
+
+def test_backward_error_metric(port):
+    a, x_true, b = system(64, seed=9)
+    assert port.backward_error(a, x_true, b) < 4 * EPS64
+    assert port.backward_error(a, x_true + 1e-6, b) > 1e-8
