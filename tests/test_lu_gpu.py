@@ -184,8 +184,9 @@ def test_large_factorization_properties():
         q = p[i] - 1
         perm[i], perm[q] = perm[q], perm[i]
     rows = torch.tensor(np.sort(np.random.default_rng(0).choice(n, 64, replace=False)), device="cuda")
-    L = torch.tril(m[rows], -1)
-    L[torch.arange(64), rows] = 1.0
+    cols = torch.arange(n, device="cuda")
+    L = torch.where(cols[None, :] < rows[:, None], m[rows], torch.zeros((), dtype=m.dtype, device="cuda"))
+    L[torch.arange(64, device="cuda"), rows] = 1.0
     U = torch.triu(m)
     pa = a[torch.from_numpy(perm).cuda()[rows]]
     err = (L @ U - pa).abs().max().item()
