@@ -1,0 +1,60 @@
+/*
+ * linalg_backend::B200 specializations of the reference's LU-solve operators
+ * (see reference_api.h for the interface they implement).  Each is a thin
+ * C++ shim over the C ABI in b200la.h: device pointers only, row-major,
+ * 1-based int64 LAPACK pivots, caller-owned device workspace.  Errors throw
+ * like the reference's LINALG_CHECK: std::invalid_argument for invalid
+ * arguments (null pointers, bad sizes or strides, aliasing, short workspace),
+ * std::runtime_error for CUDA or device-side failures.
+ *
+ * Semantics follow the reference's NATIVE backend (not CUDA_BLAS):
+ *  - lu_decomposition synchronizes `stream` and writes the host `info`;
+ *  - linear_solver honours the caller's pivots in LU_UPFRONT mode and, in
+ *    LU mode, leaves x unchanged when U is exactly singular;
+ *  - the Cholesky modes of linear_solver are not provided by this backend
+ *    (std::invalid_argument).
+ */
+#pragma once
+
+#include "reference_api.h"
+
+namespace linalg
+{
+template <> bool lu_decomposition<double, linalg_backend::B200>::apply(double*, linalg_int,
+    linalg_int*, void*, size_t, int*, void*);
+template <> bool lu_decomposition<float, linalg_backend::B200>::apply(float*, linalg_int,
+    linalg_int*, void*, size_t, int*, void*);
+template <> size_t lu_decomposition<double, linalg_backend::B200>::workspace_size(linalg_int);
+template <> size_t lu_decomposition<float, linalg_backend::B200>::workspace_size(linalg_int);
+
+template <> void linear_solver<double, linalg_backend::B200>::apply(double*, linalg_int*,
+    linalg_int, double*, linear_solver_type, void*, size_t, void*);
+template <> void linear_solver<float, linalg_backend::B200>::apply(float*, linalg_int*, linalg_int,
+    float*, linear_solver_type, void*, size_t, void*);
+template <> size_t linear_solver<double, linalg_backend::B200>::workspace_size(linalg_int,
+    linear_solver_type);
+template <> size_t linear_solver<float, linalg_backend::B200>::workspace_size(linalg_int,
+    linear_solver_type);
+
+template <> void triangular_solver<double, linalg_backend::B200>::apply(bool, bool, bool,
+    linalg_int, linalg_int, const double*, linalg_int, const double*, linalg_int, double*,
+    linalg_int, void*, size_t, void*);
+template <> void triangular_solver<float, linalg_backend::B200>::apply(bool, bool, bool, linalg_int,
+    linalg_int, const float*, linalg_int, const float*, linalg_int, float*, linalg_int, void*,
+    size_t, void*);
+template <> size_t triangular_solver<double, linalg_backend::B200>::workspace_size(linalg_int,
+    linalg_int);
+template <> size_t triangular_solver<float, linalg_backend::B200>::workspace_size(linalg_int,
+    linalg_int);
+
+template <> void multiplication<double, linalg_backend::B200>::apply(bool, bool, linalg_int,
+    linalg_int, linalg_int, double, const double*, linalg_int, const double*, linalg_int, double,
+    double*, linalg_int, void*, size_t, void*);
+template <> void multiplication<float, linalg_backend::B200>::apply(bool, bool, linalg_int,
+    linalg_int, linalg_int, float, const float*, linalg_int, const float*, linalg_int, float,
+    float*, linalg_int, void*, size_t, void*);
+template <> size_t multiplication<double, linalg_backend::B200>::workspace_size(linalg_int,
+    linalg_int, linalg_int);
+template <> size_t multiplication<float, linalg_backend::B200>::workspace_size(linalg_int,
+    linalg_int, linalg_int);
+}  // namespace linalg

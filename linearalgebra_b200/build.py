@@ -37,8 +37,9 @@ def nvcc() -> str:
 
 
 def _compile(src: str, verbose: bool) -> str:
-    obj = os.path.join(BUILD, os.path.basename(src)[:-3] + ".o")
-    deps = glob.glob(os.path.join(CSRC, "*.cuh")) + [src, os.path.join(ROOT, "include", "b200la.h")]
+    obj = os.path.join(BUILD, os.path.splitext(os.path.basename(src))[0] + ".o")
+    deps = (glob.glob(os.path.join(CSRC, "*.cuh")) + glob.glob(os.path.join(ROOT, "include", "**", "*.h"), recursive=True)
+            + [src])
     if os.path.exists(obj) and os.path.getmtime(obj) >= max(os.path.getmtime(d) for d in deps):
         return obj
     cmd = [nvcc(), *ARCH, *NVCC_FLAGS, "-c", src, "-o", obj]
@@ -54,7 +55,7 @@ def _compile(src: str, verbose: bool) -> str:
 
 def build(verbose: bool = False) -> str:
     os.makedirs(BUILD, exist_ok=True)
-    srcs = sorted(glob.glob(os.path.join(CSRC, "*.cu")))
+    srcs = sorted(glob.glob(os.path.join(CSRC, "*.cu")) + glob.glob(os.path.join(CSRC, "*.cpp")))
     with ThreadPoolExecutor(max_workers=min(8, len(srcs))) as ex:
         objs = list(ex.map(lambda s: _compile(s, verbose), srcs))
     if not os.path.exists(LIB) or os.path.getmtime(LIB) < max(os.path.getmtime(o) for o in objs):
@@ -63,6 +64,24 @@ def build(verbose: bool = False) -> str:
         if res.returncode != 0:
             raise RuntimeError(f"link failed:\n{res.stdout}\n{res.stderr}")
     return LIB
+
+
+CPP_TEST_SRC = os.path.join(ROOT, "tests", "cpp", "test_backend_b200.cpp")
+CPP_TEST_BIN = os.path.join(ROOT, "tests", "cpp", "test_backend_b200")
+
+
+def build_cpp_test() -> str:
+    """Compile the C++ operator-API test program against libb200la.so."""
+    build()
+    if os.path.exists(CPP_TEST_BIN) and os.path.getmtime(CPP_TEST_BIN) >= max(
+            os.path.getmtime(CPP_TEST_SRC), os.path.getmtime(LIB)):
+        return CPP_TEST_BIN
+    cmd = [nvcc(), "-O2", "-std=c++17", "-I", os.path.join(ROOT, "include"), CPP_TEST_SRC,
+           "-o", CPP_TEST_BIN, "-L", HERE, "-lb200la", "-Xlinker", f"-rpath={HERE}", "-lcudart"]
+    res = subprocess.run(cmd, capture_output=True, text=True)
+    if res.returncode != 0:
+        raise RuntimeError(f"C++ test build failed:\n{res.stdout}\n{res.stderr}")
+    return CPP_TEST_BIN
 
 
 if __name__ == "__main__":

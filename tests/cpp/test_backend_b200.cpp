@@ -1,0 +1,242 @@
+// GPU tests of the linalg_backend::B200 operator specializations, written
+// against the reference's own template API (include/linalg_b200/
+// reference_api.h) the way its GPU test suite exercises CUDA_BLAS: device
+// buffers, caller-owned workspace, non-default streams, argument validation.
+// Built by __graft_entry__.build() / tests/cpp/build.sh; run by
+// tests/test_cpp_api_gpu.py on a B200.  Prints one PASS/FAIL line per case.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <random>
+#include <stdexcept>
+#include <vector>
+
+#include "linalg_b200/backend_b200.h"
+
+using linalg::linalg_backend;
+constexpr auto B = linalg_backend::B200;
+
+static int g_fail = 0;
+#define CHECK(cond, name)                                                                          \
+    do                                                                                             \
+    {                                                                                              \
+        if (cond)                                                                                  \
+            std::printf("PASS %s\n", name);                                                        \
+        else                                                                                       \
+        {                                                                                          \
+            std::printf("FAIL %s (%s:%d)\n", name, __FILE__, __LINE__);                            \
+            ++g_fail;                                                                              \
+        }                                                                                          \
+    } while (0)
+
+template <typename T> struct dbuf
+{
+    T*     p = nullptr;
+    size_t n = 0;
+    explicit dbuf(size_t count) : n(count)
+    {
+        if (cudaMalloc(&p, sizeof(T) * (count ? count : 1)) != cudaSuccess)
+            throw std::runtime_error("cudaMalloc");
+    }
+    ~dbuf() { cudaFree(p); }
+    void up(const std::vector<T>& h) { cudaMemcpy(p, h.data(), sizeof(T) * h.size(), cudaMemcpyHostToDevice); }
+    std::vector<T> down() const
+    {
+        std::vector<T> h(n);
+        cudaMemcpy(h.data(), p, sizeof(T) * n, cudaMemcpyDeviceToHost);
+        return h;
+    }
+};
+
+static std::vector<double> random_matrix(int rows, int cols, unsigned seed, double lo = -5, double hi = 5)
+{
+    std::mt19937_64                        g(seed);
+    std::uniform_real_distribution<double> u(lo, hi);
+    std::vector<double>                    a((size_t)rows * cols);
+    for (auto& v : a) v = u(g);
+    return a;
+}
+
+static void test_lu()
+{
+    const int           n = 17;
+    std::vector<double> a = random_matrix(n, n, 1);
+    dbuf<double>        m(n * n);
+    dbuf<linalg_int>    piv(n);
+    m.up(a);
+    const size_t ws_bytes = linalg::lu_decomposition<double, B>::workspace_size(n);
+    dbuf<unsigned char> ws(ws_bytes);
+    int                 info = -1;
+    const bool ok = linalg::lu_decomposition<double, B>::apply(m.p, n, piv.p, ws.p, ws_bytes, &info);
+    auto lu = m.down();
+    auto p  = piv.down();
+    bool pivots_ok = true;
+    for (int i = 0; i < n; ++i) pivots_ok = pivots_ok && p[i] >= i + 1 && p[i] <= n;
+    // P A = L U
+    std::vector<double> pa = a;
+    for (int i = 0; i < n; ++i)
+        if (p[i] - 1 != i)
+            for (int j = 0; j < n; ++j) std::swap(pa[i * n + j], pa[(p[i] - 1) * n + j]);
+    double err = 0;
+    for (int i = 0; i < n; ++i)
+        for (int j = 0; j < n; ++j)
+        {
+            double s = 0;
+            for (int k = 0; k <= std::min(i, j); ++k)
+                s += (k == i ? 1.0 : lu[i * n + k]) * (k <= j ? lu[k * n + j] : 0.0);
+            err = std::max(err, std::fabs(s - pa[i * n + j]));
+        }
+    CHECK(ok && info == 0, "lu_decomposition returns true, info 0");
+    CHECK(pivots_ok, "lu_decomposition pivots in [i+1, n]");
+    CHECK(err <= 1e-9 * n, "lu_decomposition P*A == L*U");
+}
+
+static void test_linear_solver()
+{
+    const int           n = 1024;
+    std::vector<double> r = random_matrix(n, n, 2, -1, 1);
+    std::vector<double> a((size_t)n * n, 0.0), x_true(n), b(n, 0.0);
+    // symmetric positive definite: R R^T + 2n I
+    for (int i = 0; i < n; ++i)
+        for (int j = 0; j <= i; ++j)
+        {
+            double s = 0;
+            for (int k = 0; k < n; ++k) s += r[i * n + k] * r[j * n + k];
+            a[i * n + j] = a[j * n + i] = s + (i == j ? 2.0 * n : 0.0);
+        }
+    std::mt19937_64 g(3);
+    std::uniform_real_distribution<double> u(-1, 1);
+    for (auto& v : x_true) v = u(g);
+    for (int i = 0; i < n; ++i)
+        for (int j = 0; j < n; ++j) b[i] += a[i * n + j] * x_true[j];
+    for (auto mode : {linalg::linear_solver_type::LU_LINEAR_SOLVER})
+    {
+        dbuf<double>     m(n * n), x(n);
+        dbuf<linalg_int> piv(n);
+        m.up(a);
+        x.up(b);
+        cudaStream_t s;
+        cudaStreamCreate(&s);
+        const size_t        bytes = linalg::linear_solver<double, B>::workspace_size(n, mode);
+        dbuf<unsigned char> ws(bytes);
+        linalg::linear_solver<double, B>::apply(m.p, piv.p, n, x.p, mode, ws.p, bytes, s);
+        cudaStreamSynchronize(s);
+        auto xs = x.down();
+        double e = 0;
+        for (int i = 0; i < n; ++i) e = std::max(e, std::fabs(xs[i] - x_true[i]));
+        CHECK(e <= 1e-9 * n, "linear_solver LU on a stream");
+        // LU_UPFRONT reuses factors and pivots
+        x.up(b);
+        linalg::linear_solver<double, B>::apply(m.p, piv.p, n, x.p,
+            linalg::linear_solver_type::LU_UPFRONT_LINEAR_SOLVER, ws.p, bytes, s);
+        cudaStreamSynchronize(s);
+        xs = x.down();
+        e  = 0;
+        for (int i = 0; i < n; ++i) e = std::max(e, std::fabs(xs[i] - x_true[i]));
+        CHECK(e <= 1e-9 * n, "linear_solver LU_UPFRONT reuses pivots");
+        cudaStreamDestroy(s);
+    }
+}
+
+static void test_triangular()
+{
+    const int n = 35, nrhs = 9, lda = n + 2, ldb = nrhs + 1, ldx = nrhs + 3;
+    bool      all_ok = true;
+    for (bool upper : {false, true})
+        for (bool transpose : {false, true})
+            for (bool unit : {false, true})
+            {
+                std::vector<double> a((size_t)n * lda, NAN), b((size_t)n * ldb, -123.0), ex((size_t)n * ldx, -123.0);
+                for (int i = 0; i < n; ++i)
+                    for (int j = 0; j < n; ++j)
+                        if (upper ? j >= i : j <= i)
+                            a[i * lda + j] = i == j ? (unit ? NAN : 2.0 + 0.02 * i) : 0.01 * std::sin(double(i * n + j + 1));
+                for (int i = 0; i < n; ++i)
+                    for (int j = 0; j < nrhs; ++j) ex[i * ldx + j] = std::sin(double(i * nrhs + j + 1));
+                for (int i = 0; i < n; ++i)
+                    for (int j = 0; j < nrhs; ++j)
+                    {
+                        double s = 0;
+                        for (int k = 0; k < n; ++k)
+                        {
+                            const int row = transpose ? k : i, col = transpose ? i : k;
+                            if (upper ? col < row : col > row) continue;
+                            s += (unit && row == col ? 1.0 : a[row * lda + col]) * ex[k * ldx + j];
+                        }
+                        b[i * ldb + j] = s;
+                    }
+                dbuf<double> da(a.size()), db(b.size()), dx((size_t)n * ldx);
+                da.up(a);
+                db.up(b);
+                dx.up(std::vector<double>((size_t)n * ldx, -123.0));
+                linalg::triangular_solver<double, B>::apply(upper, transpose, unit, n, nrhs, da.p, lda, db.p, ldb, dx.p, ldx, nullptr, 0);
+                cudaDeviceSynchronize();
+                auto x = dx.down();
+                for (int i = 0; i < n; ++i)
+                    for (int j = 0; j < ldx; ++j)
+                        all_ok = all_ok && (j < nrhs ? std::fabs(x[i * ldx + j] - ex[i * ldx + j]) <= 1e-12 : x[i * ldx + j] == -123.0);
+            }
+    CHECK(all_ok, "triangular_solver known answers, padding preserved");
+}
+
+static void test_multiplication()
+{
+    const int rows = 256, cols = 128, depth = 128;
+    bool      all_ok = true;
+    for (bool ta : {false, true})
+        for (bool tb : {false, true})
+        {
+            auto a = random_matrix(ta ? depth : rows, ta ? rows : depth, 4);
+            auto b = random_matrix(tb ? cols : depth, tb ? depth : cols, 5);
+            dbuf<double> da(a.size()), db(b.size()), dc((size_t)rows * cols);
+            da.up(a);
+            db.up(b);
+            linalg::multiplication<double, B>::apply(ta, tb, rows, cols, depth, da.p, ta ? rows : depth, db.p, tb ? depth : cols, dc.p, cols, nullptr, 0);
+            cudaDeviceSynchronize();
+            auto c = dc.down();
+            for (int i = 0; i < rows; ++i)
+                for (int j = 0; j < cols; ++j)
+                {
+                    double s = 0;
+                    for (int k = 0; k < depth; ++k)
+                        s += (ta ? a[k * rows + i] : a[i * depth + k]) * (tb ? b[j * depth + k] : b[k * cols + j]);
+                    all_ok = all_ok && std::fabs(s - c[i * cols + j]) <= 1e-9;
+                }
+        }
+    CHECK(all_ok, "multiplication all transpose combinations");
+}
+
+static void test_validation()
+{
+    int threw = 0;
+    try { linalg::lu_decomposition<double, B>::apply(nullptr, 4, nullptr, nullptr, 0); } catch (const std::invalid_argument&) { ++threw; }
+    try { linalg::linear_solver<double, B>::apply(nullptr, nullptr, 0, nullptr, linalg::linear_solver_type::LU_LINEAR_SOLVER, nullptr, 0); } catch (const std::invalid_argument&) { ++threw; }
+    try { double* p = nullptr; linalg::multiplication<double, B>::apply(false, false, 0, 1, 1, 1.0, p, 1, p, 1, 0.0, p, 1, nullptr, 0); } catch (const std::invalid_argument&) { ++threw; }
+    CHECK(threw == 3, "null or zero-size arguments throw invalid_argument");
+}
+
+static void test_singular_status()
+{
+    dbuf<double>     m(4);
+    dbuf<linalg_int> piv(2);
+    m.up(std::vector<double>(4, 0.0));
+    const size_t        bytes = linalg::lu_decomposition<double, B>::workspace_size(2);
+    dbuf<unsigned char> ws(bytes);
+    int                 info = 0;
+    const bool ok = linalg::lu_decomposition<double, B>::apply(m.p, 2, piv.p, ws.p, bytes, &info);
+    CHECK(!ok && info == 1, "singular 2x2 zeros: false, info 1");
+}
+
+int main()
+{
+    test_lu();
+    test_linear_solver();
+    test_triangular();
+    test_multiplication();
+    test_validation();
+    test_singular_status();
+    std::printf("%s (%d failures)\n", g_fail ? "FAILED" : "ALL PASSED", g_fail);
+    return g_fail ? 1 : 0;
+}
