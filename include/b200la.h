@@ -119,6 +119,21 @@ B200LA_API size_t b200la_dgetrs_workspace_size(int64_t n, int64_t nrhs);
 B200LA_API int    b200la_dgetrs(const double* lu, const int64_t* pivot, int64_t n, int64_t nrhs,
        double* x, int64_t ldx, void* workspace, size_t workspace_bytes, void* stream);
 
+/* Allocation-free variant of b200la_dgesv, for callers that cannot allocate
+ * device memory (for example a host-language binding or a plugin host that is
+ * handed only the matrix, pivot and right-hand-side pointers, or a service
+ * that forbids allocation after start-up).  No counterpart in the reference.
+ * Same arguments and semantics as b200la_dgesv minus the workspace: the
+ * scratch is one fixed 512 KiB device array inside this library, which every
+ * GPU that loads the library holds until the process exits.  Limit: n <= 16384
+ * (larger orders return B200LA_INVALID_ARGUMENT).  The first call on a device
+ * looks up that array's device address (cudaGetSymbolAddress) with the device
+ * current; make that first call before any stream capture.  Every call shares
+ * the one array, so calls whose GPU work overlaps (other streams, other host
+ * threads) race and must be serialized by the caller.  Allocates nothing. */
+B200LA_API int b200la_dgesv_noalloc(double* m, int64_t* pivot, int64_t n, double* x, int mode,
+    void* stream);
+
 /* ---- triangular_solver ----------------------------------------------------
  * Replaces triangular_solver<T, Backend>::apply / ::workspace_size
  * (include/matrix_operation/triangular_solver.h:22-37; argument checks of

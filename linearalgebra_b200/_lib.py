@@ -51,6 +51,7 @@ SIGNATURES: dict[str, tuple] = {
     "b200la_sgesv_workspace_size": (_sz, [_i64, _i32]),
     "b200la_dgesv": (_i32, [_p, _p, _i64, _p, _i32, _p, _sz, _p]),
     "b200la_sgesv": (_i32, [_p, _p, _i64, _p, _i32, _p, _sz, _p]),
+    "b200la_dgesv_noalloc": (_i32, [_p, _p, _i64, _p, _i32, _p]),
     "b200la_dgetrs_workspace_size": (_sz, [_i64, _i64]),
     "b200la_dgetrs": (_i32, [_p, _p, _i64, _i64, _p, _i64, _p, _sz, _p]),
     "b200la_dtrsm_workspace_size": (_sz, [_i64, _i64]),

@@ -676,3 +676,99 @@ B200LA_API int b200la_sgemm(int ta, int tb, int64_t rows, int64_t cols, int64_t 
     return gemm<float>(ta, tb, rows, cols, depth, alpha, a, lda, b, ldb, beta, c, ldc, stream);
 }
 }
+
+// ---------------------------------------------------------------------------
+// Allocation-free linear solve (b200la_dgesv_noalloc).
+//
+// For callers that cannot allocate device memory themselves -- a host-language
+// binding or plugin host that only hands over the device pointers of the
+// matrix, pivots and right-hand side, or a service that forbids allocation
+// once it is running -- the scratch of the LU solve lives in one fixed
+// file-scope device array instead of a caller workspace.  Every GPU that
+// loads this library holds that array (512 KiB) until the process exits.
+// ---------------------------------------------------------------------------
+namespace b200la
+{
+namespace
+{
+constexpr int64_t kNoAllocMaxOrder     = 16384;
+constexpr size_t  kNoAllocScratchBytes = 512 * 1024;
+}  // namespace
+}  // namespace b200la
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[b200la::kNoAllocScratchBytes];
+
+namespace b200la
+{
+namespace
+{
+std::mutex g_noalloc_mutex;
+void*      g_noalloc_address[64] = {};
+
+// Device address of g_noalloc_scratch on the current device.  The host-side
+// name of the array is only a stand-in, so the address is looked up once per
+// device (with that device current) and cached.
+int noalloc_scratch(void** out)
+{
+    int dev = 0;
+    B200LA_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64)
+    {
+        return set_error(B200LA_NOT_SUPPORTED, "dgesv_noalloc: device index %d out of range", dev);
+    }
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (g_noalloc_address[dev] == nullptr)
+    {
+        void*             p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess)
+        {
+            return cuda_check(e, "cudaGetSymbolAddress(g_noalloc_scratch)");
+        }
+        g_noalloc_address[dev] = p;
+    }
+    *out = g_noalloc_address[dev];
+    return B200LA_SUCCESS;
+}
+}  // namespace
+}  // namespace b200la
+
+extern "C" B200LA_API int b200la_dgesv_noalloc(double* m, int64_t* pivot, int64_t n, double* x,
+    int mode, void* stream)
+{
+    using namespace b200la;
+    if (n > kNoAllocMaxOrder)
+    {
+        return set_error(B200LA_INVALID_ARGUMENT,
+            "dgesv_noalloc: order %lld exceeds the fixed scratch limit of %lld; use b200la_dgesv "
+            "with a caller-provided workspace",
+            (long long)n, (long long)kNoAllocMaxOrder);
+    }
+    const size_t need = gesv_ws_size<double>(n, mode);
+    if (need > kNoAllocScratchBytes)
+    {
+        return set_error(B200LA_NOT_SUPPORTED, "dgesv_noalloc: needs %zu bytes of scratch, has %zu",
+            need, kNoAllocScratchBytes);
+    }
+    if (m == nullptr || x == nullptr || pivot == nullptr || n <= 0 ||
+        (mode != B200LA_LU_LINEAR_SOLVER && mode != B200LA_LU_UPFRONT_LINEAR_SOLVER))
+    {
+        // argument errors are reported by the shared checks, before any
+        // device work
+        return gesv<double>(m, pivot, n, x, mode, nullptr, 0, stream);
+    }
+    {
+        const int st = prepare_device();
+        if (st != B200LA_SUCCESS)
+        {
+            return st;
+        }
+    }
+    void* scratch = nullptr;
+    const int st  = noalloc_scratch(&scratch);
+    if (st != B200LA_SUCCESS)
+    {
+        return st;
+    }
+    return gesv<double>(m, pivot, n, x, mode, scratch, kNoAllocScratchBytes, stream);
+}
