@@ -263,6 +263,17 @@ def run_b200(args, world, rank, local):
 
     ms_per_step = max_over_ranks(world, elapsed_ms / args.steps)
 
+    # per-kernel-class breakdown of one extra (untimed) step
+    classes = {0: "panel", 1: "laswp_u12", 2: "trailing", 3: "solve"}
+    lib.b200la_profile_start(sum(1 << c for c in classes))
+    step()
+    torch.cuda.synchronize()
+    breakdown = {}
+    for c, name in classes.items():
+        t_ms, cnt = ctypes.c_double(0), ctypes.c_int64(0)
+        lib.b200la_profile_stop(c, ctypes.addressof(t_ms), ctypes.addressof(cnt))
+        breakdown[name] = {"ms": round(t_ms.value, 3), "launches": int(cnt.value)}
+
     # accuracy of the last solve (FP64 residual, checked on the device)
     r = b - A @ x
     eta = (r.abs().max() / (A.abs().sum(1).max() * x.abs().max() + b.abs().max())).item()
@@ -354,6 +365,7 @@ def run_b200(args, world, rank, local):
             "cpu_baseline": cpu,
             "e2e": e2e,
             "gpu_launches": int(launches),
+            "breakdown_one_step": breakdown,
             "clocks": clk,
             "peaks": measured_peaks(),
         }

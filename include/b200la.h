@@ -124,7 +124,7 @@ B200LA_API int    b200la_dgetrs(const double* lu, const int64_t* pivot, int64_t 
  * handed only the matrix, pivot and right-hand-side pointers, or a service
  * that forbids allocation after start-up).  No counterpart in the reference.
  * Same arguments and semantics as b200la_dgesv minus the workspace: the
- * scratch is one fixed 512 KiB device array inside this library, which every
+ * scratch is one fixed 1 MiB device array inside this library, which every
  * GPU that loads the library holds until the process exits.  Limit: n <= 16384
  * (larger orders return B200LA_INVALID_ARGUMENT).  The first call on a device
  * looks up that array's device address (cudaGetSymbolAddress) with the device

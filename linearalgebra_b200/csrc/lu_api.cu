@@ -5,6 +5,7 @@
 
 #include <climits>
 #include <cstdint>
+#include <cstdlib>
 #include <mutex>
 
 #include "lu_kernels.cuh"
@@ -18,13 +19,39 @@ namespace
 {
 constexpr size_t kPanelSmemMax = 200 * 1024;
 
-template <typename T> constexpr size_t laswp_smem_bytes()
+
+// Cluster size usable by k_panel_cluster on each device (0: none).
+template <typename T> int& cluster_size_slot(int dev)
 {
-    return sizeof(T) * (2 * kNB * kSwapCols + kNB * (kNB + 1));
+    static int sizes[64] = {};
+    return sizes[dev];
 }
-template <typename T> constexpr size_t trailing_smem_bytes()
+
+template <typename T> int probe_cluster_size()
 {
-    return sizeof(T) * (kTileM * (kNB + 1) + kNB * kTileN);
+    for (int cl : {16, 8})
+    {
+        cudaLaunchConfig_t  cfg = {};
+        cudaLaunchAttribute attr[1];
+        cfg.gridDim                    = dim3(cl);
+        cfg.blockDim                   = dim3(kPanelThreads);
+        cfg.dynamicSmemBytes           = kPanelSmemMax;
+        attr[0].id                     = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x       = cl;
+        attr[0].val.clusterDim.y       = 1;
+        attr[0].val.clusterDim.z       = 1;
+        cfg.attrs                      = attr;
+        cfg.numAttrs                   = 1;
+        int clusters                   = 0;
+        if (cudaOccupancyMaxActiveClusters(&clusters, (const void*)k_panel_cluster<T>, &cfg) ==
+                cudaSuccess &&
+            clusters > 0)
+        {
+            return cl;
+        }
+        cudaGetLastError();
+    }
+    return 0;
 }
 
 // Raise the dynamic shared-memory limits once per device and type.
@@ -41,6 +68,14 @@ template <typename T> int ensure_kernel_attributes()
     }
     B200LA_CUDA(cudaFuncSetAttribute(
         k_panel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPanelSmemMax));
+    B200LA_CUDA(cudaFuncSetAttribute(
+        k_panel_cluster<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPanelSmemMax));
+    B200LA_CUDA(cudaFuncSetAttribute(
+        k_panel_cluster<T>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+    if (dev >= 0 && dev < 64)
+    {
+        cluster_size_slot<T>(dev) = probe_cluster_size<T>();
+    }
     B200LA_CUDA(cudaFuncSetAttribute(
         k_laswp_trsm<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)laswp_smem_bytes<T>()));
     B200LA_CUDA(cudaFuncSetAttribute(
@@ -82,9 +117,9 @@ template <typename T> int prepare()
 template <typename T> struct GetrfPlan
 {
     DeviceStatus* st;
-    SlotHeader*   hdr;
-    T*            payload;
-    T*            diag;
+    uint64_t*     hdr;
+    uint64_t*     payload;
+    uint64_t*     diag;
     PermList*     perm;
 };
 
@@ -92,9 +127,9 @@ template <typename T> GetrfPlan<T> plan_getrf(Arena& a)
 {
     GetrfPlan<T> p;
     p.st      = a.next<DeviceStatus>(1);
-    p.hdr     = a.next<SlotHeader>(2 * kMaxPanelCtas);
-    p.payload = a.next<T>((size_t)2 * kMaxPanelCtas * kNB);
-    p.diag    = a.next<T>(2 * kNB);
+    p.hdr     = a.next<uint64_t>(panel_hdr_words<T>());
+    p.payload = a.next<uint64_t>(panel_payload_words<T>());
+    p.diag    = a.next<uint64_t>(panel_diag_words<T>());
     p.perm    = a.next<PermList>(1);
     return p;
 }
@@ -127,19 +162,57 @@ inline int grid_1d(int64_t total, int threads)
 template <typename T>
 int enqueue_getrf(T* m, int n, int64_t* pivot, const GetrfPlan<T>& p, cudaStream_t s)
 {
-    B200LA_CUDA(cudaMemsetAsync(p.hdr, 0, sizeof(SlotHeader) * 2 * kMaxPanelCtas, s));
+    // the exchange words carry column flags: clear them so no word of an
+    // earlier factorization can validate
+    B200LA_CUDA(cudaMemsetAsync(p.hdr, 0, sizeof(uint64_t) * panel_hdr_words<T>(), s));
+    B200LA_CUDA(cudaMemsetAsync(p.payload, 0, sizeof(uint64_t) * panel_payload_words<T>(), s));
+    B200LA_CUDA(cudaMemsetAsync(p.diag, 0, sizeof(uint64_t) * panel_diag_words<T>(), s));
     prof_begin(KC_SOLVE, s);
     k_status_init<<<1, 32, 0, s>>>(p.st, p.perm);
     prof_end(KC_SOLVE, s);
     B200LA_LAUNCH_CHECK();
     const int sms  = device_sm_count();
     const int gmax = sms < kMaxPanelCtas ? sms : kMaxPanelCtas;
+    int       dev  = 0;
+    B200LA_CUDA(cudaGetDevice(&dev));
+    // B200LA_FORCE_GRID_PANEL=1 keeps every panel on the grid-wide kernel
+    // (used by the tests to check both panel paths)
+    const char* force_grid = getenv("B200LA_FORCE_GRID_PANEL");
+    const int   cl = (force_grid != nullptr && force_grid[0] == '1')
+                       ? 0
+                       : ((dev >= 0 && dev < 64) ? cluster_size_slot<T>(dev) : 0);
     PanelWs<T> ws{p.hdr, p.payload, p.diag, p.perm};
     DeviceStatus* st = p.st;
     for (int k = 0; k < n; k += kNB)
     {
         int       w   = n - k < kNB ? n - k : kNB;
         const int R   = n - k;
+        // the panel inside one thread-block cluster when its rows fit there
+        if (cl > 0)
+        {
+            const int    rpc_c  = (R + cl - 1) / cl;
+            const size_t smem_c = (size_t)rpc_c * (kNB + 1) * sizeof(T);
+            if (smem_c <= kPanelSmemMax)
+            {
+                cudaLaunchConfig_t  cfg = {};
+                cudaLaunchAttribute attr[1];
+                cfg.gridDim              = dim3(cl);
+                cfg.blockDim             = dim3(kPanelThreads);
+                cfg.dynamicSmemBytes     = smem_c;
+                cfg.stream               = s;
+                attr[0].id               = cudaLaunchAttributeClusterDimension;
+                attr[0].val.clusterDim.x = cl;
+                attr[0].val.clusterDim.y = 1;
+                attr[0].val.clusterDim.z = 1;
+                cfg.attrs                = attr;
+                cfg.numAttrs             = 1;
+                prof_begin(KC_PANEL, s);
+                B200LA_CUDA(cudaLaunchKernelEx(&cfg, k_panel_cluster<T>, m, n, k, w, rpc_c, pivot, p.perm, p.st));
+                prof_end(KC_PANEL, s);
+                goto panel_done;
+            }
+        }
+        {
         int       G   = (R + 15) / 16;
         G             = G < 1 ? 1 : (G > gmax ? gmax : G);
         int rpc       = (R + G - 1) / G;
@@ -157,19 +230,21 @@ int enqueue_getrf(T* m, int n, int64_t* pivot, const GetrfPlan<T>& p, cudaStream
         B200LA_CUDA(cudaLaunchCooperativeKernel(
             (const void*)k_panel<T>, dim3(G), dim3(kPanelThreads), args, smem, s));
         prof_end(KC_PANEL, s);
+        }
+    panel_done:
         const int rest = n - k - w;
         const int nl   = (k + kSwapCols - 1) / kSwapCols;
         const int nr   = (rest + kSwapCols - 1) / kSwapCols;
         if (nl + nr > 0)
         {
             prof_begin(KC_SWAP, s);
-            k_laswp_trsm<T><<<nl + nr, kSwapCols, laswp_smem_bytes<T>(), s>>>(m, n, k, w, p.perm, nl);
+            k_laswp_trsm<T><<<nl + nr, kSwapThreads, laswp_smem_bytes<T>(), s>>>(m, n, k, w, p.perm, nl);
             prof_end(KC_SWAP, s);
             B200LA_LAUNCH_CHECK();
         }
         if (rest > 0)
         {
-            dim3 grid((rest + kTileN - 1) / kTileN, (rest + kTileM - 1) / kTileM);
+            dim3 grid((rest + kChunkN - 1) / kChunkN, (rest + kBandM - 1) / kBandM);
             prof_begin(KC_TRAILING, s);
             k_trailing<T><<<grid, 128, trailing_smem_bytes<T>(), s>>>(m, n, k, w);
             prof_end(KC_TRAILING, s);
@@ -685,14 +760,14 @@ B200LA_API int b200la_sgemm(int ta, int tb, int64_t rows, int64_t cols, int64_t 
 // matrix, pivots and right-hand side, or a service that forbids allocation
 // once it is running -- the scratch of the LU solve lives in one fixed
 // file-scope device array instead of a caller workspace.  Every GPU that
-// loads this library holds that array (512 KiB) until the process exits.
+// loads this library holds that array (1 MiB) until the process exits.
 // ---------------------------------------------------------------------------
 namespace b200la
 {
 namespace
 {
 constexpr int64_t kNoAllocMaxOrder     = 16384;
-constexpr size_t  kNoAllocScratchBytes = 512 * 1024;
+constexpr size_t  kNoAllocScratchBytes = 1024 * 1024;
 }  // namespace
 }  // namespace b200la
 

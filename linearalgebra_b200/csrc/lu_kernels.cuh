@@ -26,6 +26,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <cooperative_groups.h>
+
 #include <cfloat>
 #include <climits>
 
@@ -36,7 +38,7 @@ namespace b200la
 
 constexpr int kNB           = 64;   // panel width (reference kLuBlockSize)
 constexpr int kPanelThreads = 256;
-constexpr int kMaxPanelCtas = 256;
+constexpr int kMaxPanelCtas = 160;  // >= the SM count of a B200 (148)
 constexpr int kSwapCols     = 64;   // columns per CTA in k_laswp_trsm
 
 template <typename T> struct Vec2;
@@ -59,15 +61,78 @@ template <> struct Limits<float>
     __device__ static constexpr float min_normal() { return FLT_MIN; }
 };
 
-// One per-CTA candidate of the pivot exchange.  `seq` = global column + 1
-// marks the slot as filled for that column (the workspace is cleared at the
-// start of every factorization).
-struct alignas(16) SlotHeader
+// The pivot exchange of k_panel uses self-validating 8-byte words: the low
+// half carries 4 data bytes, the high half the flag of the column being
+// exchanged (global column + 1).  An aligned 8-byte access is single-copy
+// atomic, so a reader that sees the expected flag in every word it needs has
+// the data of that column without any release/acquire fence.  The exchange
+// buffers are cleared at the start of every factorization.
+__device__ __forceinline__ uint64_t ll_word(uint32_t data, uint32_t flag)
 {
-    double   key;
-    int32_t  row;
-    uint32_t seq;
+    return ((uint64_t)flag << 32) | data;
+}
+__device__ __forceinline__ void st_u64x2(uint64_t* p, uint64_t a, uint64_t b)
+{
+    asm volatile("st.relaxed.gpu.global.v2.u64 [%0], {%1, %2};" ::"l"(p), "l"(a), "l"(b) : "memory");
+}
+__device__ __forceinline__ void st_u64(uint64_t* p, uint64_t a)
+{
+    asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(a) : "memory");
+}
+__device__ __forceinline__ void ld_u64x2(const uint64_t* p, uint64_t& a, uint64_t& b)
+{
+    asm volatile("ld.relaxed.gpu.global.v2.u64 {%0, %1}, [%2];" : "=l"(a), "=l"(b) : "l"(p) : "memory");
+}
+__device__ __forceinline__ uint64_t ld_u64(const uint64_t* p)
+{
+    uint64_t v;
+    asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+
+template <typename T> struct LLWords;
+template <> struct LLWords<double>
+{
+    static constexpr int kWords = 2;
 };
+template <> struct LLWords<float>
+{
+    static constexpr int kWords = 1;
+};
+
+__device__ __forceinline__ void ll_store(uint64_t* base, int idx, double v, uint32_t flag)
+{
+    const uint64_t bits = (uint64_t)__double_as_longlong(v);
+    st_u64x2(base + 2 * idx, ll_word((uint32_t)bits, flag), ll_word((uint32_t)(bits >> 32), flag));
+}
+__device__ __forceinline__ void ll_store(uint64_t* base, int idx, float v, uint32_t flag)
+{
+    st_u64(base + idx, ll_word(__float_as_uint(v), flag));
+}
+__device__ __forceinline__ bool ll_load(const uint64_t* base, int idx, uint32_t flag, double& v)
+{
+    uint64_t a, b;
+    ld_u64x2(base + 2 * idx, a, b);
+    if ((uint32_t)(a >> 32) != flag || (uint32_t)(b >> 32) != flag)
+    {
+        return false;
+    }
+    v = __longlong_as_double((long long)(((b & 0xffffffffull) << 32) | (a & 0xffffffffull)));
+    return true;
+}
+__device__ __forceinline__ bool ll_load(const uint64_t* base, int idx, uint32_t flag, float& v)
+{
+    const uint64_t a = ld_u64(base + idx);
+    if ((uint32_t)(a >> 32) != flag)
+    {
+        return false;
+    }
+    v = __uint_as_float((uint32_t)a);
+    return true;
+}
+
+// Header of one CTA's candidate: 4 words = key (2), row, unused.
+constexpr int kHdrWords = 4;
 
 // Row interchanges of one panel, as a permutation of the rows they touch:
 // row dst[q] receives the pre-panel contents of row src[q], q < count.
@@ -82,11 +147,18 @@ struct PermList
 
 template <typename T> struct PanelWs
 {
-    SlotHeader* hdr;      // [2][kMaxPanelCtas]
-    T*          payload;  // [2][kMaxPanelCtas][kNB]
-    T*          diag;     // [2][kNB]
-    PermList*   perm;
+    uint64_t* hdr;      // [2][kMaxPanelCtas][kHdrWords]
+    uint64_t* payload;  // [2][kMaxPanelCtas][kNB * LLWords<T>::kWords]
+    uint64_t* diag;     // [2][kNB * LLWords<T>::kWords]
+    PermList* perm;
 };
+
+template <typename T> constexpr size_t panel_hdr_words() { return (size_t)2 * kMaxPanelCtas * kHdrWords; }
+template <typename T> constexpr size_t panel_payload_words()
+{
+    return (size_t)2 * kMaxPanelCtas * kNB * LLWords<T>::kWords;
+}
+template <typename T> constexpr size_t panel_diag_words() { return (size_t)2 * kNB * LLWords<T>::kWords; }
 
 // (key, row) ordering of the pivot search: larger key wins, equal keys go to
 // the lower row, i.e. the first maximum in row order like the reference's
@@ -110,6 +182,168 @@ template <typename T> __device__ __forceinline__ double pivot_key(T v, int gr, i
     return nan ? -1.0 : (double)fabs(v);
 }
 
+// The interchanges of one panel (pivot rows piv_loc[0..w), 0-based) as one
+// permutation of the rows they touch (PermList).  Run by one warp.
+__device__ __noinline__ void build_perm_list(const int* piv_loc, int k, int w, PermList* perm, int lane)
+{
+    __shared__ int pos_s[2 * kNB];
+    __shared__ int cont_s[2 * kNB];
+    __shared__ int cnt_s;
+    for (int q = lane; q < w; q += 32)
+    {
+        pos_s[q]  = k + q;
+        cont_s[q] = k + q;
+    }
+    if (lane == 0)
+    {
+        cnt_s = w;
+    }
+    __syncwarp();
+    for (int jj = 0; jj < w; ++jj)
+    {
+        const int i = k + jj;
+        const int p = piv_loc[jj];
+        if (p == i)
+        {
+            continue;
+        }
+        int slot_p;
+        if (p < k + w)
+        {
+            slot_p = p - k;
+        }
+        else
+        {
+            const int cnt = cnt_s;
+            slot_p        = -1;
+            for (int q0 = w; q0 < cnt; q0 += 32)
+            {
+                const int      q   = q0 + lane;
+                const unsigned hit = __ballot_sync(0xffffffffu, q < cnt && pos_s[q] == p);
+                if (hit)
+                {
+                    slot_p = q0 + __ffs(hit) - 1;
+                    break;
+                }
+            }
+            if (slot_p < 0)
+            {
+                slot_p = cnt;
+                __syncwarp();
+                if (lane == 0)
+                {
+                    pos_s[slot_p]  = p;
+                    cont_s[slot_p] = p;
+                    cnt_s          = cnt + 1;
+                }
+            }
+        }
+        __syncwarp();
+        if (lane == 0)
+        {
+            const int t    = cont_s[jj];
+            cont_s[jj]     = cont_s[slot_p];
+            cont_s[slot_p] = t;
+        }
+        __syncwarp();
+    }
+    const int cnt = cnt_s;
+    for (int q = lane; q < cnt; q += 32)
+    {
+        perm->dst[q] = pos_s[q];
+        perm->src[q] = cont_s[q];
+    }
+    if (lane == 0)
+    {
+        perm->count = cnt;
+    }
+}
+
+__device__ __forceinline__ void warp_best(double& key, int& row)
+{
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1)
+    {
+        const double ok   = __shfl_down_sync(0xffffffffu, key, off);
+        const int    orow = __shfl_down_sync(0xffffffffu, row, off);
+        if (better(ok, orow, key, row))
+        {
+            key = ok;
+            row = orow;
+        }
+    }
+}
+
+// Block-wide best (key, row): every thread passes its own candidate; all
+// threads get the result.  Two barriers.
+__device__ __forceinline__ void block_best(double& key, int& row, double* red_key, int* red_row)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    warp_best(key, row);
+    if (lane == 0)
+    {
+        red_key[warp] = key;
+        red_row[warp] = row;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0)
+    {
+        for (int q = 1; q < kPanelThreads / 32; ++q)
+        {
+            if (better(red_key[q], red_row[q], key, row))
+            {
+                key = red_key[q];
+                row = red_row[q];
+            }
+        }
+        red_key[kPanelThreads / 32] = key;
+        red_row[kPanelThreads / 32] = row;
+    }
+    __syncthreads();
+    key = red_key[kPanelThreads / 32];
+    row = red_row[kPanelThreads / 32];
+}
+
+// Multipliers and rank-1 update of the panel rows below the diagonal row c
+// for column jj, one thread per row, plus that thread's best candidate for
+// the next column.  Per element the operations are the reference's:
+// l = a_rj * (1/d) (or a_rj / d), then a_rc = fma(-l, u_c, a_rc) for c > j.
+template <typename T>
+__device__ __forceinline__ void panel_update_rows(T* loc, size_t ldl, int rbeg, int nloc, int r0,
+    int jj, int w, int c, const T* urow, T d, double& nk, int& nr)
+{
+    const bool zero      = d == T(0);
+    const bool use_recip = fabs(d) >= Limits<T>::min_normal();
+    const T    recip     = use_recip ? (T)(T(1) / d) : T(1);
+    const bool has_next  = jj + 1 < w;
+    for (int r = rbeg + (int)threadIdx.x; r < nloc; r += kPanelThreads)
+    {
+        T* row = loc + (size_t)r * ldl;
+        if (!zero)
+        {
+            const T x = row[jj];
+            const T l = use_recip ? x * recip : x / d;
+            row[jj]   = l;
+#pragma unroll 4
+            for (int cc = jj + 1; cc < w; ++cc)
+            {
+                row[cc] = fma(-l, urow[cc], row[cc]);
+            }
+        }
+        if (has_next)
+        {
+            const double key = pivot_key(row[jj + 1], r0 + r, c + 1);
+            if (better(key, r0 + r, nk, nr))
+            {
+                nk = key;
+                nr = r0 + r;
+            }
+        }
+    }
+}
+
+constexpr int kMaxSlotsPerLane = (kMaxPanelCtas + 31) / 32;
+
 template <typename T>
 __global__ void __launch_bounds__(kPanelThreads) k_panel(T* __restrict__ A, int n, int k, int w,
     int rows_per_cta, int in_smem, int64_t* __restrict__ pivot, PanelWs<T> ws,
@@ -117,9 +351,10 @@ __global__ void __launch_bounds__(kPanelThreads) k_panel(T* __restrict__ A, int 
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ T      urow[kNB];
+    __shared__ T      drow[kNB];
     __shared__ int    piv_loc[kNB];
-    __shared__ double red_key[kPanelThreads / 32];
-    __shared__ int    red_row[kPanelThreads / 32];
+    __shared__ double red_key[kPanelThreads / 32 + 1];
+    __shared__ int    red_row[kPanelThreads / 32 + 1];
     __shared__ int    s_p, s_g, s_abort;
 
     const int tid  = threadIdx.x;
@@ -151,114 +386,104 @@ __global__ void __launch_bounds__(kPanelThreads) k_panel(T* __restrict__ A, int 
     }
     __syncthreads();
 
+    // candidate for the first column
+    double cand_key = -2.0;
+    int    cand_row = INT_MAX;
+    for (int r = max(0, k - r0) + tid; r < nloc; r += kPanelThreads)
+    {
+        const double key = pivot_key(loc[r * ldl], r0 + r, k);
+        if (better(key, r0 + r, cand_key, cand_row))
+        {
+            cand_key = key;
+            cand_row = r0 + r;
+        }
+    }
+    block_best(cand_key, cand_row, red_key, red_row);
+
     int64_t first_zero = -1;
     for (int jj = 0; jj < w; ++jj)
     {
         const int c   = k + jj;
         const int par = jj & 1;
 
-        // ---- local candidate: best (key, row) over owned rows >= c
-        double best    = -2.0;
-        int    bestrow = INT_MAX;
-        for (int r = max(0, c - r0) + tid; r < nloc; r += kPanelThreads)
+        // ---- publish this CTA's candidate row, its header and (owner of row
+        // c) the diagonal row as flagged words; no fence is needed
+        const uint32_t flag = (uint32_t)(c + 1);
+        uint64_t*      H    = ws.hdr + (size_t)par * kMaxPanelCtas * kHdrWords;
+        constexpr int  PW   = kNB * LLWords<T>::kWords;
+        if (cand_row != INT_MAX && tid < w)
         {
-            const double key = pivot_key(loc[r * ldl + jj], r0 + r, c);
-            if (better(key, r0 + r, best, bestrow))
-            {
-                best    = key;
-                bestrow = r0 + r;
-            }
+            ll_store(ws.payload + ((size_t)par * kMaxPanelCtas + b) * PW, tid,
+                loc[(size_t)(cand_row - r0) * ldl + tid], flag);
         }
-#pragma unroll
-        for (int off = 16; off > 0; off >>= 1)
+        if (c >= r0 && c < r0 + nloc && tid >= 64 && tid < 64 + w)
         {
-            const double ok = __shfl_down_sync(0xffffffffu, best, off);
-            const int    orow = __shfl_down_sync(0xffffffffu, bestrow, off);
-            if (better(ok, orow, best, bestrow))
-            {
-                best    = ok;
-                bestrow = orow;
-            }
+            ll_store(ws.diag + (size_t)par * PW, tid - 64, loc[(size_t)(c - r0) * ldl + (tid - 64)], flag);
         }
-        if (lane == 0)
+        if (tid == kPanelThreads - 1)
         {
-            red_key[warp] = best;
-            red_row[warp] = bestrow;
-        }
-        __syncthreads();
-        if (tid == 0)
-        {
-            for (int q = 1; q < kPanelThreads / 32; ++q)
-            {
-                if (better(red_key[q], red_row[q], best, bestrow))
-                {
-                    best    = red_key[q];
-                    bestrow = red_row[q];
-                }
-            }
-            red_key[0] = best;
-            red_row[0] = bestrow;
-        }
-        __syncthreads();
-        best    = red_key[0];
-        bestrow = red_row[0];
-
-        // ---- publish: candidate row, then (owner of row c) the diagonal row
-        SlotHeader* H = ws.hdr + par * kMaxPanelCtas;
-        if (bestrow != INT_MAX)
-        {
-            T* P = ws.payload + ((size_t)par * kMaxPanelCtas + b) * kNB;
-            for (int cc = tid; cc < w; cc += kPanelThreads)
-            {
-                P[cc] = loc[(size_t)(bestrow - r0) * ldl + cc];
-            }
-        }
-        if (c >= r0 && c < r0 + nloc)
-        {
-            T* D = ws.diag + par * kNB;
-            for (int cc = tid; cc < w; cc += kPanelThreads)
-            {
-                D[cc] = loc[(size_t)(c - r0) * ldl + cc];
-            }
-        }
-        __syncthreads();
-        if (tid == 0)
-        {
-            H[b].key = best;
-            H[b].row = bestrow;
-            __threadfence();
-            st_release_u32(&H[b].seq, (uint32_t)(c + 1));
+            ll_store(H + (size_t)b * kHdrWords, 0, cand_key, flag);
+            st_u64x2(H + (size_t)b * kHdrWords + 2, ll_word((uint32_t)cand_row, flag), ll_word(0u, flag));
         }
 
-        // ---- gather every CTA's candidate (bounded wait), pick the pivot
+        // ---- wait for every CTA's header (all of a lane's slots polled
+        // together, bounded) and pick the pivot
         if (warp == 0)
         {
-            double wk = -2.0;
-            int    wr = INT_MAX, wg = -1;
-            bool   timed_out = false;
-            for (int g = lane; g < G; g += 32)
+            double         hk[kMaxSlotsPerLane];
+            int            hr[kMaxSlotsPerLane];
+            bool           done[kMaxSlotsPerLane];
+            const uint64_t t0        = global_ns();
+            bool           timed_out = false;
+#pragma unroll
+            for (int t = 0; t < kMaxSlotsPerLane; ++t)
             {
-                const uint64_t t0    = global_ns();
-                uint32_t       polls = 0;
-                while (ld_acquire_u32(&H[g].seq) != (uint32_t)(c + 1))
+                done[t] = lane + 32 * t >= G;
+                hk[t]   = -2.0;
+                hr[t]   = INT_MAX;
+            }
+            for (uint32_t polls = 0;; ++polls)
+            {
+                bool all = true;
+#pragma unroll
+                for (int t = 0; t < kMaxSlotsPerLane; ++t)
                 {
-                    if ((++polls & 255u) == 0 && global_ns() - t0 > kWaitLimitNs)
+                    if (!done[t])
                     {
-                        timed_out = true;
-                        break;
+                        const uint64_t* h = H + (size_t)(lane + 32 * t) * kHdrWords;
+                        double          kv;
+                        uint64_t        w0, w1;
+                        const bool      kok = ll_load(h, 0, flag, kv);
+                        ld_u64x2(h + 2, w0, w1);
+                        if (kok && (uint32_t)(w0 >> 32) == flag)
+                        {
+                            hk[t]   = kv;
+                            hr[t]   = (int)(uint32_t)w0;
+                            done[t] = true;
+                        }
+                        all = all && done[t];
                     }
                 }
-                if (timed_out)
+                if (all)
                 {
                     break;
                 }
-                const double kg = __ldcg(&H[g].key);
-                const int    rg = __ldcg(&H[g].row);
-                if (better(kg, rg, wk, wr))
+                if ((polls & 63u) == 63u && global_ns() - t0 > kWaitLimitNs)
                 {
-                    wk = kg;
-                    wr = rg;
-                    wg = g;
+                    timed_out = true;
+                    break;
+                }
+            }
+            double wk = -2.0;
+            int    wr = INT_MAX, wg = -1;
+#pragma unroll
+            for (int t = 0; t < kMaxSlotsPerLane; ++t)
+            {
+                if (lane + 32 * t < G && better(hk[t], hr[t], wk, wr))
+                {
+                    wk = hk[t];
+                    wr = hr[t];
+                    wg = lane + 32 * t;
                 }
             }
             if (__any_sync(0xffffffffu, timed_out))
@@ -272,9 +497,9 @@ __global__ void __launch_bounds__(kPanelThreads) k_panel(T* __restrict__ A, int 
 #pragma unroll
             for (int off = 16; off > 0; off >>= 1)
             {
-                const double ok = __shfl_down_sync(0xffffffffu, wk, off);
+                const double ok   = __shfl_down_sync(0xffffffffu, wk, off);
                 const int    orow = __shfl_down_sync(0xffffffffu, wr, off);
-                const int    og = __shfl_down_sync(0xffffffffu, wg, off);
+                const int    og   = __shfl_down_sync(0xffffffffu, wg, off);
                 if (better(ok, orow, wk, wr))
                 {
                     wk = ok;
@@ -303,73 +528,81 @@ __global__ void __launch_bounds__(kPanelThreads) k_panel(T* __restrict__ A, int 
                 pivot[c] = (int64_t)p + 1;
             }
         }
+        // ---- the pivot row (and, for the owner of row p, the old row c) in
+        // one round trip
+        const bool own_c = c >= r0 && c < r0 + nloc;
+        const bool own_p = p != c && p >= r0 && p < r0 + nloc;
         {
-            const T* P = ws.payload + ((size_t)par * kMaxPanelCtas + g) * kNB;
-            for (int cc = tid; cc < w; cc += kPanelThreads)
+            const uint64_t* src = nullptr;
+            int             cc  = -1;
+            T*              dst = nullptr;
+            if (tid < w)
             {
-                urow[cc] = __ldcg(P + cc);
+                src = ws.payload + ((size_t)par * kMaxPanelCtas + g) * PW;
+                cc  = tid;
+                dst = urow;
+            }
+            else if (own_p && tid >= 64 && tid < 64 + w)
+            {
+                src = ws.diag + (size_t)par * PW;
+                cc  = tid - 64;
+                dst = drow;
+            }
+            if (src != nullptr)
+            {
+                const uint64_t t0 = global_ns();
+                T              v;
+                uint32_t       polls = 0;
+                while (!ll_load(src, cc, flag, v))
+                {
+                    if ((++polls & 63u) == 0 && global_ns() - t0 > kWaitLimitNs)
+                    {
+                        raise_error(st, DEV_WAIT_TIMEOUT, 2);
+                        s_abort = 1;
+                        break;
+                    }
+                }
+                dst[cc] = v;
             }
         }
         __syncthreads();
+        if (s_abort)
+        {
+            return;
+        }
 
         // ---- swap rows c and p inside the panel
         if (p != c)
         {
-            if (c >= r0 && c < r0 + nloc)
+            if (own_c)
             {
                 for (int cc = tid; cc < w; cc += kPanelThreads)
                 {
                     loc[(size_t)(c - r0) * ldl + cc] = urow[cc];
                 }
             }
-            if (p >= r0 && p < r0 + nloc)
+            if (own_p)
             {
-                const T* D = ws.diag + par * kNB;
                 for (int cc = tid; cc < w; cc += kPanelThreads)
                 {
-                    loc[(size_t)(p - r0) * ldl + cc] = __ldcg(D + cc);
+                    loc[(size_t)(p - r0) * ldl + cc] = drow[cc];
                 }
             }
+            __syncthreads();
         }
-        __syncthreads();
 
-        // ---- multipliers and rank-1 update of rows > c
+        // ---- multipliers, rank-1 update and the next column's candidate
         const T d = urow[jj];
-        if (d == T(0))
+        if (d == T(0) && first_zero < 0)
         {
-            if (first_zero < 0)
-            {
-                first_zero = c;
-            }
-            continue;
+            first_zero = c;
         }
-        const bool use_recip = fabs(d) >= Limits<T>::min_normal();
-        const T    recip     = use_recip ? (T)(T(1) / d) : T(1);
-        const int  rbeg      = max(0, c + 1 - r0);
-        for (int r = rbeg + tid; r < nloc; r += kPanelThreads)
-        {
-            T& l = loc[(size_t)r * ldl + jj];
-            l    = use_recip ? l * recip : l / d;
-        }
-        __syncthreads();
-        const int wrem = w - jj - 1;
-        if (wrem > 0)
-        {
-            // 4 row lanes x 64 column lanes
-            const int cl = tid & 63;
-            const int rl = tid >> 6;
-            if (cl < wrem)
-            {
-                const int cc = jj + 1 + cl;
-                const T   u  = urow[cc];
-                for (int r = rbeg + rl; r < nloc; r += kPanelThreads / 64)
-                {
-                    T* row = loc + (size_t)r * ldl;
-                    row[cc] = fma(-row[jj], u, row[cc]);
-                }
-            }
-        }
-        __syncthreads();
+        double nk = -2.0;
+        int    nr = INT_MAX;
+        panel_update_rows(loc, ldl, max(0, c + 1 - r0), nloc, r0, jj, w, c, urow, d, nk, nr);
+        cand_key = nk;
+        cand_row = nr;
+        block_best(cand_key, cand_row, red_key, red_row);
     }
 
     // ---- write the factored slice back
@@ -391,272 +624,517 @@ __global__ void __launch_bounds__(kPanelThreads) k_panel(T* __restrict__ A, int 
                 st->first_zero = first_zero;
             }
         }
-        // The panel's interchanges as one permutation of the rows they touch.
         if (warp == 0)
         {
-            __shared__ int pos_s[2 * kNB];
-            __shared__ int cont_s[2 * kNB];
-            __shared__ int cnt_s;
-            for (int q = lane; q < w; q += 32)
+            build_perm_list(piv_loc, k, w, ws.perm, lane);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Panel factorization inside one thread-block cluster.
+//
+// Used when the panel's rows fit in the shared memory of one cluster of
+// `cl` CTAs (16 where the device allows that cluster size, else 8).  Same
+// arithmetic as k_panel; the per-column agreement on the pivot goes through
+// distributed shared memory: each CTA posts its candidate (key, row) in its
+// own shared memory, and after a cluster barrier every CTA reads all of
+// them, then reads the pivot row (and, for the owner of row p, the old row c)
+// straight from the owning CTA's shared memory.  A second cluster barrier
+// keeps the swap from overwriting rows that are still being read.  The
+// cluster barriers are hardware barriers over co-scheduled CTAs, so there is
+// no spin-wait in this kernel.
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void __launch_bounds__(kPanelThreads, 1) k_panel_cluster(T* __restrict__ A, int n, int k,
+    int w, int rows_per_cta, int64_t* __restrict__ pivot, PermList* __restrict__ perm,
+    DeviceStatus* __restrict__ st)
+{
+    namespace cg = cooperative_groups;
+    cg::cluster_group cluster = cg::this_cluster();
+
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ T      urow[kNB];
+    __shared__ T      drow[kNB];
+    __shared__ int    piv_loc[kNB];
+    __shared__ double red_key[kPanelThreads / 32 + 1];
+    __shared__ int    red_row[kPanelThreads / 32 + 1];
+    __shared__ double post_key;  // this CTA's candidate, read by the cluster
+    __shared__ int    post_row;
+    __shared__ int    s_p, s_rank_p;
+
+    const int tid  = threadIdx.x;
+    const int lane = tid & 31;
+    const int warp = tid >> 5;
+    const int CL   = (int)cluster.num_blocks();
+    const int b    = (int)cluster.block_rank();
+    const int r0   = k + b * rows_per_cta;
+    const int nloc = max(0, min(n, r0 + rows_per_cta) - r0);
+    constexpr int ldl = kNB + 1;
+
+    T* loc = reinterpret_cast<T*>(smem_raw);
+    for (int e = tid; e < nloc * w; e += kPanelThreads)
+    {
+        const int r = e / w, c = e - (e / w) * w;
+        loc[r * ldl + c] = A[(size_t)(r0 + r) * n + k + c];
+    }
+    __syncthreads();
+
+    double cand_key = -2.0;
+    int    cand_row = INT_MAX;
+    for (int r = max(0, k - r0) + tid; r < nloc; r += kPanelThreads)
+    {
+        const double key = pivot_key(loc[r * ldl], r0 + r, k);
+        if (better(key, r0 + r, cand_key, cand_row))
+        {
+            cand_key = key;
+            cand_row = r0 + r;
+        }
+    }
+    block_best(cand_key, cand_row, red_key, red_row);
+
+    int64_t first_zero = -1;
+    for (int jj = 0; jj < w; ++jj)
+    {
+        const int c = k + jj;
+        if (tid == 0)
+        {
+            post_key = cand_key;
+            post_row = cand_row;
+        }
+        cluster.sync();  // every CTA's candidate (and its rows) is readable
+        if (warp == 0)
+        {
+            double wk = -2.0;
+            int    wr = INT_MAX, wrank = -1;
+            if (lane < CL)
             {
-                pos_s[q]  = k + q;
-                cont_s[q] = k + q;
+                wk    = *cluster.map_shared_rank(&post_key, lane);
+                wr    = *cluster.map_shared_rank(&post_row, lane);
+                wrank = lane;
+            }
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1)
+            {
+                const double ok    = __shfl_down_sync(0xffffffffu, wk, off);
+                const int    orow  = __shfl_down_sync(0xffffffffu, wr, off);
+                const int    orank = __shfl_down_sync(0xffffffffu, wrank, off);
+                if (better(ok, orow, wk, wr))
+                {
+                    wk    = ok;
+                    wr    = orow;
+                    wrank = orank;
+                }
             }
             if (lane == 0)
             {
-                cnt_s = w;
+                s_p      = wr;
+                s_rank_p = wrank;
             }
-            __syncwarp();
-            for (int jj = 0; jj < w; ++jj)
+        }
+        __syncthreads();
+        const int  p      = s_p;
+        const int  rank_p = s_rank_p;
+        const int  rank_c = (c - k) / rows_per_cta;
+        const bool own_c  = b == rank_c;
+        const bool own_p  = p != c && b == rank_p;
+        if (tid == 0)
+        {
+            piv_loc[jj] = p;
+            if (b == 0)
             {
-                const int i = k + jj;
-                const int p = piv_loc[jj];
-                if (p == i)
-                {
-                    continue;
-                }
-                int slot_p;
-                if (p < k + w)
-                {
-                    slot_p = p - k;
-                }
-                else
-                {
-                    const int cnt = cnt_s;
-                    slot_p        = -1;
-                    for (int q0 = w; q0 < cnt; q0 += 32)
-                    {
-                        const int      q   = q0 + lane;
-                        const unsigned hit = __ballot_sync(0xffffffffu, q < cnt && pos_s[q] == p);
-                        if (hit)
-                        {
-                            slot_p = q0 + __ffs(hit) - 1;
-                            break;
-                        }
-                    }
-                    if (slot_p < 0)
-                    {
-                        slot_p = cnt;
-                        __syncwarp();
-                        if (lane == 0)
-                        {
-                            pos_s[slot_p]  = p;
-                            cont_s[slot_p] = p;
-                            cnt_s          = cnt + 1;
-                        }
-                    }
-                }
-                __syncwarp();
-                if (lane == 0)
-                {
-                    const int t     = cont_s[jj];
-                    cont_s[jj]      = cont_s[slot_p];
-                    cont_s[slot_p]  = t;
-                }
-                __syncwarp();
+                pivot[c] = (int64_t)p + 1;
             }
-            const int cnt = cnt_s;
-            for (int q = lane; q < cnt; q += 32)
+        }
+        if (tid < w)
+        {
+            const T* prow = cluster.map_shared_rank(loc, rank_p) + (size_t)(p - (k + rank_p * rows_per_cta)) * ldl;
+            urow[tid]     = prow[tid];
+        }
+        else if (own_p && tid >= 64 && tid < 64 + w)
+        {
+            const T* crow = cluster.map_shared_rank(loc, rank_c) + (size_t)(c - (k + rank_c * rows_per_cta)) * ldl;
+            drow[tid - 64] = crow[tid - 64];
+        }
+        cluster.sync();  // remote reads of rows p and c are complete
+        if (p != c)
+        {
+            if (own_c)
             {
-                ws.perm->dst[q] = pos_s[q];
-                ws.perm->src[q] = cont_s[q];
+                for (int cc = tid; cc < w; cc += kPanelThreads)
+                {
+                    loc[(size_t)(c - r0) * ldl + cc] = urow[cc];
+                }
             }
-            if (lane == 0)
+            if (own_p)
             {
-                ws.perm->count = cnt;
+                for (int cc = tid; cc < w; cc += kPanelThreads)
+                {
+                    loc[(size_t)(p - r0) * ldl + cc] = drow[cc];
+                }
             }
+            __syncthreads();
+        }
+
+        const T d = urow[jj];
+        if (d == T(0) && first_zero < 0)
+        {
+            first_zero = c;
+        }
+        double nk = -2.0;
+        int    nr = INT_MAX;
+        panel_update_rows(loc, ldl, max(0, c + 1 - r0), nloc, r0, jj, w, c, urow, d, nk, nr);
+        cand_key = nk;
+        cand_row = nr;
+        block_best(cand_key, cand_row, red_key, red_row);
+    }
+    cluster.sync();  // no CTA exits while its shared memory may still be read
+
+    for (int e = tid; e < nloc * w; e += kPanelThreads)
+    {
+        const int r = e / w, c = e - (e / w) * w;
+        A[(size_t)(r0 + r) * n + k + c] = loc[r * ldl + c];
+    }
+    if (b == 0)
+    {
+        if (tid == 0 && first_zero >= 0 && st->first_zero < 0)
+        {
+            st->first_zero = first_zero;
+        }
+        if (warp == 0)
+        {
+            build_perm_list(piv_loc, k, w, perm, lane);
         }
     }
 }
 
 // Row interchanges outside the panel and, right of it, U12 = L11^-1 A12.
 // CTA b < n_left: columns [b*kSwapCols, ...) of [0, k); otherwise columns of
-// [k+w, n).  One thread per column.
+// [k+w, n).  256 threads: 4 row groups x 64 columns for the gather/scatter
+// (each thread loads its up to 32 rows before storing, so the loads overlap),
+// then one thread per column for the substitution.
+constexpr int kSwapThreads = 256;
+constexpr int kSwapGroups  = kSwapThreads / kSwapCols;
+constexpr int kSwapPerThr  = (2 * kNB + kSwapGroups - 1) / kSwapGroups;
+
+template <typename T> constexpr size_t laswp_smem_bytes()
+{
+    return sizeof(T) * (2 * kNB * kSwapCols + kNB * (kNB + 1));
+}
+
 template <typename T>
-__global__ void __launch_bounds__(kSwapCols) k_laswp_trsm(T* __restrict__ A, int n, int k, int w,
+__global__ void __launch_bounds__(kSwapThreads) k_laswp_trsm(T* __restrict__ A, int n, int k, int w,
     const PermList* __restrict__ perm, int n_left)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    T(*staged)[kSwapCols] = reinterpret_cast<T(*)[kSwapCols]>(smem_raw);           // [2*kNB]
-    T(*L11)[kNB + 1]      = reinterpret_cast<T(*)[kNB + 1]>(smem_raw + sizeof(T) * 2 * kNB * kSwapCols);
+    T(*staged)[kSwapCols] = reinterpret_cast<T(*)[kSwapCols]>(smem_raw);  // [2*kNB]
+    T(*L11)[kNB + 1] = reinterpret_cast<T(*)[kNB + 1]>(smem_raw + sizeof(T) * 2 * kNB * kSwapCols);
 
     const int  tid   = threadIdx.x;
+    const int  cl    = tid % kSwapCols;
+    const int  rg    = tid / kSwapCols;
     const bool left  = (int)blockIdx.x < n_left;
     const int  c0    = left ? blockIdx.x * kSwapCols : k + w + (blockIdx.x - n_left) * kSwapCols;
     const int  cend  = left ? k : n;
-    const int  col   = c0 + tid;
+    const int  col   = c0 + cl;
     const bool valid = col < cend;
     const int  cnt   = perm->count;
 
-    for (int q = 0; q < cnt; ++q)
     {
-        staged[q][tid] = valid ? A[(size_t)perm->src[q] * n + col] : T(0);
+        T v[kSwapPerThr];
+#pragma unroll
+        for (int t = 0; t < kSwapPerThr; ++t)
+        {
+            const int q = rg + kSwapGroups * t;
+            v[t]        = (valid && q < cnt) ? A[(size_t)perm->src[q] * n + col] : T(0);
+        }
+#pragma unroll
+        for (int t = 0; t < kSwapPerThr; ++t)
+        {
+            const int q = rg + kSwapGroups * t;
+            if (q < cnt)
+            {
+                staged[q][cl] = v[t];
+            }
+        }
+    }
+    if (!left)
+    {
+        for (int e = tid; e < w * w; e += kSwapThreads)
+        {
+            const int i = e / w, p = e - (e / w) * w;
+            L11[i][p]   = p < i ? A[(size_t)(k + i) * n + k + p] : T(0);
+        }
+    }
+    __syncthreads();
+    // scatter: every touched row (left), or the rows displaced below the
+    // panel (right; the panel rows receive U12 below)
+    if (valid)
+    {
+        for (int q = (left ? 0 : w) + rg; q < cnt; q += kSwapGroups)
+        {
+            const int dst = perm->dst[q];
+            if (!left || dst != perm->src[q])
+            {
+                A[(size_t)dst * n + col] = staged[q][cl];
+            }
+        }
     }
     if (left)
     {
-        if (valid)
-        {
-            for (int q = 0; q < cnt; ++q)
-            {
-                if (perm->dst[q] != perm->src[q])
-                {
-                    A[(size_t)perm->dst[q] * n + col] = staged[q][tid];
-                }
-            }
-        }
         return;
     }
-    // rows displaced below the panel
-    if (valid)
+    // U12 = L11^-1 A12 on the staged panel rows, column-oriented: step p
+    // applies row p (final) to rows p+1..w-1, so row i receives the updates
+    // of rows 0..i-1 in that order, as in the reference's row-axpy loop.
+    for (int p = 0; p + 1 < w; ++p)
     {
-        for (int q = w; q < cnt; ++q)
+        __syncthreads();
+        const T xp = staged[p][cl];
+        for (int i = p + 1 + rg; i < w; i += kSwapGroups)
         {
-            A[(size_t)perm->dst[q] * n + col] = staged[q][tid];
+            staged[i][cl] = fma(-L11[i][p], xp, staged[i][cl]);
         }
-    }
-    // L11 (unit lower, strictly below the diagonal)
-    for (int e = tid; e < w * w; e += kSwapCols)
-    {
-        const int i = e / w, p = e - (e / w) * w;
-        L11[i][p]   = p < i ? A[(size_t)(k + i) * n + k + p] : T(0);
     }
     __syncthreads();
-    if (!valid)
+    if (valid)
     {
-        return;
-    }
-    T x[kNB];
-#pragma unroll
-    for (int i = 0; i < kNB; ++i)
-    {
-        x[i] = i < w ? staged[i][tid] : T(0);
-    }
-    // column-oriented forward substitution: row i receives the updates of
-    // rows 0..i-1 in that order, as in the reference's row-axpy loop
-#pragma unroll
-    for (int p = 0; p < kNB; ++p)
-    {
-        if (p < w)
+        for (int i = rg; i < w; i += kSwapGroups)
         {
-#pragma unroll
-            for (int i = p + 1; i < kNB; ++i)
-            {
-                if (i < w)
-                {
-                    x[i] = fma(-L11[i][p], x[p], x[i]);
-                }
-            }
-        }
-    }
-#pragma unroll
-    for (int i = 0; i < kNB; ++i)
-    {
-        if (i < w)
-        {
-            A[(size_t)(k + i) * n + col] = x[i];
+            A[(size_t)(k + i) * n + col] = staged[i][cl];
         }
     }
 }
 
-// Trailing update A22 -= L21 U12 for one 128 x 64 tile of A22 per CTA.
-// delta is accumulated per element from zero over the panel's w columns in
-// order with fused multiply-adds, then subtracted from A22 once.
-// Thread (warp, tr = lane/8, tc = lane%8) owns rows warp*32 + tr + 4i
-// (i < 8) and columns 2*tc + 16*j + e (j < 4, e < 2) of the tile.
-constexpr int kTileM = 128;
-constexpr int kTileN = 64;
+// ---------------------------------------------------------------------------
+// cp.async helpers (Ampere-style asynchronous global->shared copies).
+// `bytes` is 16 or the element size; src_bytes = 0 zero-fills.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem, bool valid)
+{
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(s), "l"(gmem),
+        "r"(valid ? 16 : 0)
+        : "memory");
+}
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem, bool valid)
+{
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(s), "l"(gmem),
+        "r"(valid ? 8 : 0)
+        : "memory");
+}
+__device__ __forceinline__ void cp_async4(void* smem, const void* gmem, bool valid)
+{
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;" ::"r"(s), "l"(gmem),
+        "r"(valid ? 4 : 0)
+        : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N> __device__ __forceinline__ void cp_async_wait()
+{
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+// Copy `count` contiguous elements (count * sizeof(T) a multiple of 16 when
+// vec16) from gmem to smem, zero-filling when !valid; chunks are distributed
+// by the caller.
+template <typename T>
+__device__ __forceinline__ void cp_async_chunk(T* smem, const T* gmem, bool valid, bool vec16)
+{
+    if (vec16)
+    {
+        cp_async16(smem, gmem, valid);
+    }
+    else
+    {
+#pragma unroll
+        for (int e = 0; e < (int)(16 / sizeof(T)); ++e)
+        {
+            if (sizeof(T) == 8)
+                cp_async8(smem + e, gmem + e, valid);
+            else
+                cp_async4(smem + e, gmem + e, valid);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Trailing update A22 -= L21 U12.
+//
+// A CTA owns a band of kBandM = 128 rows of A22 and a chunk of kChunkN = 256
+// of its columns.  The band's L21 rows (128 x w) are staged once in shared
+// memory; the chunk is streamed as 8 tiles of 128 x 32 with a two-stage
+// cp.async pipeline carrying the tile's U12 slice (w x 32) and its A22 tile.
+// For every element, delta is accumulated from zero over the panel's w
+// columns in order with fused multiply-adds and then subtracted from A22 once
+// (the reference computes delta with its GEMM and subtracts it in a second
+// pass).  Thread (warp, tr = lane/8, tc = lane%8) owns tile rows
+// warp*32 + tr + 4i (i < 8) and columns 2*tc + 16*j + e (j, e < 2).
+// L21 is stored with the 16-byte chunk index XORed by (row % 4) so the four
+// rows a warp reads at one depth index hit different banks.
+// ---------------------------------------------------------------------------
+constexpr int kBandM  = 128;
+constexpr int kTileNc = 32;
+constexpr int kChunkN = 256;
+
+template <typename T> constexpr int chunk_elems() { return 16 / (int)sizeof(T); }
+
+template <typename T> constexpr size_t trailing_smem_bytes()
+{
+    return sizeof(T) * ((size_t)kBandM * kNB + 2 * ((size_t)kNB * kTileNc + (size_t)kBandM * kTileNc));
+}
 
 template <typename T>
-__global__ void __launch_bounds__(128, 2) k_trailing(T* __restrict__ A, int n, int k, int w)
+__device__ __forceinline__ void trailing_issue_tile(T* Bs, T* Cs, const T* U12, const T* C, int n,
+    int w, int rest, int m0, int nt0, bool vec16)
+{
+    constexpr int CE = chunk_elems<T>();
+    constexpr int BC = kTileNc / CE;  // chunks per tile row
+    // U12 slice: w x 32
+    for (int e = threadIdx.x; e < kNB * BC; e += 128)
+    {
+        const int  p = e / BC, q = e - (e / BC) * BC;
+        const int  col = nt0 + q * CE;
+        const bool v   = p < w && col < rest;
+        cp_async_chunk(Bs + p * kTileNc + q * CE, v ? U12 + (size_t)p * n + col : U12, v, vec16);
+    }
+    // A22 tile: 128 x 32
+    for (int e = threadIdx.x; e < kBandM * BC; e += 128)
+    {
+        const int  r = e / BC, q = e - (e / BC) * BC;
+        const int  col = nt0 + q * CE;
+        const bool v   = m0 + r < rest && col < rest;
+        cp_async_chunk(Cs + r * kTileNc + q * CE, v ? C + (size_t)(m0 + r) * n + col : C, v, vec16);
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(128, 1) k_trailing(T* __restrict__ A, int n, int k, int w)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    T* As = reinterpret_cast<T*>(smem_raw);   // [kTileM][kNB + 1]
-    T* Bs = As + kTileM * (kNB + 1);           // [kNB][kTileN]
+    constexpr int CE = chunk_elems<T>();
+    T*            As = reinterpret_cast<T*>(smem_raw);           // [kBandM][kNB], swizzled
+    T*            Bs = As + kBandM * kNB;                          // [2][kNB][kTileNc]
+    T*            Cs = Bs + 2 * kNB * kTileNc;                     // [2][kBandM][kTileNc]
 
     const int rest = n - k - w;
-    const int m0   = blockIdx.y * kTileM;
-    const int n0   = blockIdx.x * kTileN;
+    const int m0   = blockIdx.y * kBandM;
+    const int n0   = blockIdx.x * kChunkN;
     const int tid  = threadIdx.x;
     const int lane = tid & 31;
     const int warp = tid >> 5;
     const int tr   = lane >> 3;
     const int tc   = lane & 7;
+    const bool vec16 = (((size_t)n * sizeof(T)) % 16 == 0) && ((reinterpret_cast<uintptr_t>(A) & 15) == 0);
 
     const T* L21 = A + (size_t)(k + w) * n + k;
     const T* U12 = A + (size_t)k * n + k + w;
     T*       C   = A + (size_t)(k + w) * n + k + w;
 
-    for (int e = tid; e < kTileM * kNB; e += 128)
+    // stage the band's L21 rows (chunk index XOR (row % 4))
     {
-        const int r = e / kNB, p = e % kNB;
-        As[r * (kNB + 1) + p] = (m0 + r < rest && p < w) ? L21[(size_t)(m0 + r) * n + p] : T(0);
+        constexpr int AC = kNB / CE;  // chunks per row
+        for (int e = tid; e < kBandM * AC; e += 128)
+        {
+            const int  r = e / AC, q = e - (e / AC) * AC;
+            const bool v = m0 + r < rest && q * CE < w;
+            cp_async_chunk(As + r * kNB + (q ^ (r & 3)) * CE,
+                v ? L21 + (size_t)(m0 + r) * n + q * CE : L21, v, vec16);
+        }
     }
-    for (int e = tid; e < kNB * kTileN; e += 128)
+    const int ntiles = min(kChunkN, rest - n0) > 0 ? (min(kChunkN, rest - n0) + kTileNc - 1) / kTileNc : 0;
+    trailing_issue_tile(Bs, Cs, U12, C, n, w, rest, m0, n0, vec16);
+    cp_async_commit();
+    if (ntiles > 1)
     {
-        const int p = e / kTileN, cc = e % kTileN;
-        Bs[p * kTileN + cc] = (p < w && n0 + cc < rest) ? U12[(size_t)p * n + n0 + cc] : T(0);
+        trailing_issue_tile(Bs + kNB * kTileNc, Cs + kBandM * kTileNc, U12, C, n, w, rest, m0,
+            n0 + kTileNc, vec16);
     }
-    __syncthreads();
+    cp_async_commit();
 
-    T acc[8][8];
-#pragma unroll
-    for (int i = 0; i < 8; ++i)
+    // element p of row r lives at As[r][((p / CE) ^ (r % 4)) * CE + p % CE]
+    const T* arow = As + (warp * 32 + tr) * kNB;
+    const int sw  = tr & 3;  // rows warp*32 + tr + 4i all have row % 4 == tr % 4
+
+    for (int t = 0; t < ntiles; ++t)
     {
-#pragma unroll
-        for (int j = 0; j < 8; ++j)
-        {
-            acc[i][j] = T(0);
-        }
-    }
-    const T* arow = As + (warp * 32 + tr) * (kNB + 1);
-    for (int p = 0; p < w; ++p)
-    {
-        T a[8], bv[8];
+        cp_async_wait<1>();
+        __syncthreads();
+        const T* B  = Bs + (t & 1) * kNB * kTileNc;
+        T*       Ct = Cs + (t & 1) * kBandM * kTileNc;
+
+        T acc[8][4];
 #pragma unroll
         for (int i = 0; i < 8; ++i)
         {
-            a[i] = arow[4 * i * (kNB + 1) + p];
-        }
-#pragma unroll
-        for (int j = 0; j < 4; ++j)
-        {
-            const auto v2 = *reinterpret_cast<const typename Vec2<T>::type*>(
-                Bs + p * kTileN + 2 * tc + 16 * j);
-            bv[2 * j]     = v2.x;
-            bv[2 * j + 1] = v2.y;
-        }
-#pragma unroll
-        for (int i = 0; i < 8; ++i)
-        {
-#pragma unroll
-            for (int j = 0; j < 8; ++j)
-            {
-                acc[i][j] = fma(a[i], bv[j], acc[i][j]);
-            }
-        }
-    }
-#pragma unroll
-    for (int i = 0; i < 8; ++i)
-    {
-        const int r = m0 + warp * 32 + tr + 4 * i;
-        if (r < rest)
-        {
-            T* crow = C + (size_t)r * n;
 #pragma unroll
             for (int j = 0; j < 4; ++j)
             {
+                acc[i][j] = T(0);
+            }
+        }
+        for (int p = 0; p < w; ++p)
+        {
+            const int pa = ((p / CE) ^ sw) * CE + (p % CE);
+            T         a[8], bv[4];
 #pragma unroll
-                for (int e = 0; e < 2; ++e)
+            for (int i = 0; i < 8; ++i)
+            {
+                a[i] = arow[4 * i * kNB + pa];
+            }
+#pragma unroll
+            for (int j = 0; j < 2; ++j)
+            {
+                const auto v2 = *reinterpret_cast<const typename Vec2<T>::type*>(B + p * kTileNc + 2 * tc + 16 * j);
+                bv[2 * j]     = v2.x;
+                bv[2 * j + 1] = v2.y;
+            }
+#pragma unroll
+            for (int i = 0; i < 8; ++i)
+            {
+#pragma unroll
+                for (int j = 0; j < 4; ++j)
                 {
-                    const int cc = n0 + 2 * tc + 16 * j + e;
-                    if (cc < rest)
+                    acc[i][j] = fma(a[i], bv[j], acc[i][j]);
+                }
+            }
+        }
+        const int nt0 = n0 + t * kTileNc;
+#pragma unroll
+        for (int i = 0; i < 8; ++i)
+        {
+            const int rl = warp * 32 + tr + 4 * i;
+            const int r  = m0 + rl;
+            if (r < rest)
+            {
+                T* crow = C + (size_t)r * n;
+#pragma unroll
+                for (int j = 0; j < 2; ++j)
+                {
+                    const int cl = 2 * tc + 16 * j;
+                    const auto v2 = *reinterpret_cast<const typename Vec2<T>::type*>(Ct + rl * kTileNc + cl);
+                    if (nt0 + cl < rest)
                     {
-                        crow[cc] = crow[cc] - acc[i][2 * j + e];
+                        crow[nt0 + cl] = v2.x - acc[i][2 * j];
+                    }
+                    if (nt0 + cl + 1 < rest)
+                    {
+                        crow[nt0 + cl + 1] = v2.y - acc[i][2 * j + 1];
                     }
                 }
             }
         }
+        __syncthreads();  // buffer (t & 1) is free again
+        if (t + 2 < ntiles)
+        {
+            trailing_issue_tile(Bs + (t & 1) * kNB * kTileNc, Cs + (t & 1) * kBandM * kTileNc, U12, C,
+                n, w, rest, m0, n0 + (t + 2) * kTileNc, vec16);
+        }
+        cp_async_commit();
     }
+    cp_async_wait<0>();
 }
 
 __global__ void k_status_init(DeviceStatus* st, PermList* perm)

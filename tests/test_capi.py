@@ -68,3 +68,11 @@ def test_python_errors_map_to_exceptions():
     with pytest.raises(_lib.B200Error):
         _lib.check(_lib.CUDA_ERROR)
     assert _lib.check(_lib.SINGULAR, allow=(_lib.SUCCESS, _lib.SINGULAR)) == _lib.SINGULAR
+
+
+def test_no_alloc_scratch_covers_its_largest_order():
+    lib = _lib.load()
+    # the allocation-free solve carves the same plan as b200la_dgesv from a
+    # fixed 1 MiB device array, for orders up to 16384
+    assert lib.b200la_dgesv_workspace_size(16384, 1) <= 1 << 20
+    assert lib.b200la_dgesv_workspace_size(16384, 2) <= 1 << 20

@@ -78,6 +78,18 @@ def test_lu_bitwise_vs_oracle(port, n):
     assert np.array_equal(lu, lu_o)
 
 
+@pytest.mark.parametrize("n", [300, 1500])
+def test_lu_grid_panel_path_bitwise(port, monkeypatch, n):
+    """The grid-wide panel kernel (used when a panel does not fit in one
+    thread-block cluster) gives the same bits as the cluster one."""
+    monkeypatch.setenv("B200LA_FORCE_GRID_PANEL", "1")
+    a = random_matrix(n, seed=31 + n)
+    lu_o, piv_o, _ = port.getrf(a)
+    lu, piv, _ = gpu_getrf(a)
+    assert np.array_equal(piv, piv_o)
+    assert np.array_equal(lu, lu_o)
+
+
 def test_lu_float32_bitwise_vs_oracle(port):
     a = random_matrix(700, seed=11, dtype=np.float32)
     lu_o, piv_o, _ = port.getrf(a)
