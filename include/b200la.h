@@ -165,6 +165,21 @@ B200LA_API int    b200la_sgemm(int transpose_a, int transpose_b, int64_t rows, i
        int64_t depth, float alpha, const float* a, int64_t lda, const float* b, int64_t ldb,
        float beta, float* c, int64_t ldc, void* workspace, size_t workspace_bytes, void* stream);
 
+/* ---- tensor-core update (mixed-precision LU building block) ---------------
+ * c[m x n] (fp32, row stride ldc) -= a[m x k] * b[n x k]^T on the tcgen05
+ * tensor cores with FP32 accumulation.  a and b are K-major (row stride k
+ * elements), 16-byte aligned, k a multiple of 32 (TF32) or 64 (BF16/FP16).
+ * kind: 0 = TF32 (fp32 containers), 1 = BF16, 2 = FP16.  split3 (TF32 only):
+ * a = a + a_small, b = b + b_small split operands, product
+ * a*b + a*b_small + a_small*b.  workspace: b200la_tc_update_workspace_size()
+ * bytes of device memory (status block).  The trailing update of
+ * lu_decomposition_native.cpp:400-422 done in low precision; no direct
+ * reference counterpart. */
+B200LA_API size_t b200la_tc_update_workspace_size(void);
+B200LA_API int    b200la_sgemm_tc_update(int kind, int split3, float* c, int64_t ldc, int64_t m, int64_t n,
+       int64_t k, const void* a, const void* b, const void* a_small, const void* b_small,
+       void* workspace, size_t workspace_bytes, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -62,6 +62,8 @@ SIGNATURES: dict[str, tuple] = {
     "b200la_sgemm_workspace_size": (_sz, [_i64, _i64, _i64]),
     "b200la_dgemm": (_i32, [_i32, _i32, _i64, _i64, _i64, _d, _p, _i64, _p, _i64, _d, _p, _i64, _p, _sz, _p]),
     "b200la_sgemm": (_i32, [_i32, _i32, _i64, _i64, _i64, _f, _p, _i64, _p, _i64, _f, _p, _i64, _p, _sz, _p]),
+    "b200la_tc_update_workspace_size": (_sz, []),
+    "b200la_sgemm_tc_update": (_i32, [_i32, _i32, _p, _i64, _i64, _i64, _i64, _p, _p, _p, _p, _p, _sz, _p]),
 }
 
 

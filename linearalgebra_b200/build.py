@@ -22,6 +22,22 @@ BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libb200la.so")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+def cutlass_include() -> str:
+    """CuTe/CUTLASS header tree (used for the tcgen05 descriptor layouts)."""
+    cands = []
+    try:
+        import flashinfer  # noqa: F401
+        cands.append(os.path.join(os.path.dirname(flashinfer.__file__), "data", "cutlass", "include"))
+    except Exception:
+        pass
+    cands.append(os.path.join(sys.prefix, "lib", f"python{sys.version_info.major}.{sys.version_info.minor}",
+                              "site-packages", "flashinfer", "data", "cutlass", "include"))
+    for c in cands:
+        if os.path.exists(os.path.join(c, "cute", "arch", "mma_sm100_desc.hpp")):
+            return c
+    raise RuntimeError("CuTe headers (cute/arch/mma_sm100_desc.hpp) not found")
+
+
 NVCC_FLAGS = [
     "-O3", "-std=c++17", "-lineinfo", "--expt-relaxed-constexpr",
     "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",
@@ -42,7 +58,7 @@ def _compile(src: str, verbose: bool) -> str:
             + [src])
     if os.path.exists(obj) and os.path.getmtime(obj) >= max(os.path.getmtime(d) for d in deps):
         return obj
-    cmd = [nvcc(), *ARCH, *NVCC_FLAGS, "-c", src, "-o", obj]
+    cmd = [nvcc(), *ARCH, *NVCC_FLAGS, "-I", cutlass_include(), "-c", src, "-o", obj]
     if verbose:
         cmd.insert(1, "-Xptxas=-v")
     res = subprocess.run(cmd, capture_output=True, text=True)

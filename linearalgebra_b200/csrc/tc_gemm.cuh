@@ -1,0 +1,398 @@
+// Tensor-core (tcgen05) trailing update for the mixed-precision LU:
+//
+//     C[M x N] (fp32, row-major, ldc)  -=  A[M x K] * B[N x K]^T
+//
+// A and B are K-major operand copies (row stride K elements) in TF32 (fp32
+// containers), BF16 or FP16.  One CTA computes one 128 x 128 tile of C:
+//   * warp 0 / lane 0 issues TMA loads of 128-byte-wide K slices of A and B
+//     (128B swizzle) into a ring of shared-memory stages, completing on
+//     mbarriers;
+//   * warp 1 / lane 0 issues tcgen05.mma (M=128, N=128, 32 bytes of K per
+//     instruction) accumulating in FP32 in tensor memory, and frees each
+//     stage with tcgen05.commit;
+//   * all four warps then read the accumulator from tensor memory
+//     (tcgen05.ld, one row per thread) and write C - acc.
+// With SPLIT3 the operands come in two parts each (x = big + small, big the
+// TF32-truncated value) and the product is big*big + big*small + small*big,
+// which recovers nearly FP32 accuracy from TF32 tensor cores (Ootomo &
+// Yokota, IJHPCA 2022).
+//
+// Every mbarrier wait is bounded (2 s); on a timeout the kernel records an
+// error in the device status block, waits (bounded) for its own copies in
+// flight, releases its tensor memory and returns.
+#pragma once
+
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <cute/arch/mma_sm100_desc.hpp>
+
+#include "common.cuh"
+
+namespace b200la
+{
+
+enum TcKind : int
+{
+    TC_TF32 = 0,
+    TC_BF16 = 1,
+    TC_FP16 = 2
+};
+
+constexpr int kTcBM        = 128;
+constexpr int kTcBN        = 128;
+constexpr int kTcAtomBytes = 128;  // one 128B-swizzle atom of K per stage
+constexpr int kTcTileBytes = kTcBM * kTcAtomBytes;  // 16 KB per operand tile per stage
+
+template <int KIND> struct TcTraits;
+template <> struct TcTraits<TC_TF32>
+{
+    static constexpr int      elem = 4;
+    static constexpr uint32_t fmt  = 2;  // TF32
+};
+template <> struct TcTraits<TC_BF16>
+{
+    static constexpr int      elem = 2;
+    static constexpr uint32_t fmt  = 1;  // BF16
+};
+template <> struct TcTraits<TC_FP16>
+{
+    static constexpr int      elem = 2;
+    static constexpr uint32_t fmt  = 0;  // F16
+};
+
+template <bool SPLIT3> constexpr int tc_stages() { return SPLIT3 ? 3 : 4; }
+template <bool SPLIT3> constexpr int tc_operands() { return SPLIT3 ? 4 : 2; }
+template <bool SPLIT3> constexpr size_t tc_smem_bytes()
+{
+    // stages + 1 KB alignment slack + barriers/TMEM address
+    return (size_t)tc_stages<SPLIT3>() * tc_operands<SPLIT3>() * kTcTileBytes + 1024 + 256;
+}
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p)
+{
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+        "r"(bytes)
+        : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity)
+{
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// Bounded wait on an mbarrier phase; false when the 2 s limit ran out.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity)
+{
+    if (mbar_try_wait(bar, parity))
+    {
+        return true;
+    }
+    const uint64_t t0    = global_ns();
+    uint32_t       polls = 0;
+    while (!mbar_try_wait(bar, parity))
+    {
+        if ((++polls & 255u) == 0 && global_ns() - t0 > kWaitLimitNs)
+        {
+            return false;
+        }
+    }
+    return true;
+}
+
+__device__ __forceinline__ void tma_load_2d(void* smem, const CUtensorMap* map, int x, int y, uint64_t* bar)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, "
+        "%3}], [%4];" ::"r"(smem_u32(smem)),
+        "l"(map), "r"(x), "r"(y), "r"(smem_u32(bar))
+        : "memory");
+}
+
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+template <int KIND>
+__device__ __forceinline__ void tc_mma(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+    uint32_t accumulate)
+{
+    if constexpr (KIND == TC_TF32)
+    {
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem_d),
+            "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
+            : "memory");
+    }
+    else
+    {
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem_d),
+            "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
+            : "memory");
+    }
+}
+
+__device__ __forceinline__ void tc_commit(uint64_t* bar)
+{
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                     smem_u32(bar))
+                 : "memory");
+}
+
+// Shared-memory matrix descriptor of a K-major tile stored as TMA writes it
+// with 128B swizzle: rows of 128 bytes, 8-row groups 1024 bytes apart.
+__device__ __forceinline__ uint64_t tc_desc(uint32_t smem_addr)
+{
+    cute::UMMA::SmemDescriptor d;
+    d.desc_                = 0;
+    d.start_address_       = (uint16_t)((smem_addr & 0x3FFFF) >> 4);
+    d.leading_byte_offset_ = 1;
+    d.stride_byte_offset_  = 1024 >> 4;
+    d.version_             = 1;
+    d.base_offset_         = 0;
+    d.lbo_mode_            = 0;
+    d.layout_type_         = (uint8_t)cute::UMMA::LayoutType::SWIZZLE_128B;
+    return d.desc_;
+}
+
+// Instruction descriptor (the bit layout of cute::UMMA::InstrDescriptor):
+// F32 accumulate (bit 4), A/B formats (bits 7-9, 10-12), K-major A and B
+// (bits 15, 16 = 0), N >> 3 (bits 17-22), M >> 4 (bits 24-28).
+template <int KIND> __host__ __device__ constexpr uint32_t tc_idesc()
+{
+    return (1u << 4) | (TcTraits<KIND>::fmt << 7) | (TcTraits<KIND>::fmt << 10) |
+           ((uint32_t)(kTcBN >> 3) << 17) | ((uint32_t)(kTcBM >> 4) << 24);
+}
+static_assert(tc_idesc<TC_TF32>() == 0x8200910u, "TF32 instruction descriptor layout");
+
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32])
+{
+    uint32_t r[32];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+        "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+        "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]),
+        "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]),
+        "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 32; ++i)
+    {
+        v[i] = __uint_as_float(r[i]);
+    }
+}
+
+template <int KIND, bool SPLIT3>
+__global__ void __launch_bounds__(128, 1) k_tc_update(const __grid_constant__ CUtensorMap tmA,
+    const __grid_constant__ CUtensorMap tmB, const __grid_constant__ CUtensorMap tmAs,
+    const __grid_constant__ CUtensorMap tmBs, float* __restrict__ C, int64_t ldc, int M, int N, int K,
+    DeviceStatus* __restrict__ st)
+{
+    constexpr int S   = tc_stages<SPLIT3>();
+    constexpr int OPS = tc_operands<SPLIT3>();
+    constexpr int EA  = kTcAtomBytes / TcTraits<KIND>::elem;  // K elements per stage
+    constexpr uint32_t IDESC = tc_idesc<KIND>();
+
+    extern __shared__ __align__(1024) unsigned char tc_smem_raw[];
+    unsigned char* base = reinterpret_cast<unsigned char*>(
+        (reinterpret_cast<uintptr_t>(tc_smem_raw) + 1023) & ~uintptr_t(1023));
+    unsigned char* tiles    = base;  // [S][OPS][16 KB]
+    uint64_t*      full     = reinterpret_cast<uint64_t*>(base + (size_t)S * OPS * kTcTileBytes);
+    uint64_t*      empty    = full + S;
+    uint64_t*      done     = empty + S;
+    uint32_t*      tmem_ptr = reinterpret_cast<uint32_t*>(done + 1);
+    int*           s_fail   = reinterpret_cast<int*>(tmem_ptr + 1);
+    int*           s_issued = s_fail + 1;  // K slices whose loads were issued
+
+    const int warp = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31;
+    const int m0   = blockIdx.y * kTcBM;
+    const int n0   = blockIdx.x * kTcBN;
+    const int natoms = K / EA;
+
+    if (threadIdx.x == 0)
+    {
+        for (int s = 0; s < S; ++s)
+        {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], 1);
+        }
+        mbar_init(done, 1);
+        *s_fail   = 0;
+        *s_issued = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0)
+    {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                         smem_u32(tmem_ptr)),
+            "r"(kTcBN)
+            : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tmem_ptr;
+
+    if (warp == 0 && lane == 0)
+    {
+        // producer: TMA loads of K slices into the stage ring
+        for (int a = 0; a < natoms; ++a)
+        {
+            const int s = a % S;
+            if (a >= S && !mbar_wait(&empty[s], ((a / S) - 1) & 1))
+            {
+                raise_error(st, DEV_WAIT_TIMEOUT, 10);
+                atomicExch(s_fail, 1);
+                break;
+            }
+            if (*reinterpret_cast<volatile int*>(s_fail))
+            {
+                break;
+            }
+            unsigned char* stage = tiles + (size_t)s * OPS * kTcTileBytes;
+            mbar_expect_tx(&full[s], OPS * kTcTileBytes);
+            tma_load_2d(stage, &tmA, a * EA, m0, &full[s]);
+            tma_load_2d(stage + kTcTileBytes, &tmB, a * EA, n0, &full[s]);
+            if constexpr (SPLIT3)
+            {
+                tma_load_2d(stage + 2 * kTcTileBytes, &tmAs, a * EA, m0, &full[s]);
+                tma_load_2d(stage + 3 * kTcTileBytes, &tmBs, a * EA, n0, &full[s]);
+            }
+            *reinterpret_cast<volatile int*>(s_issued) = a + 1;
+        }
+    }
+    else if (warp == 1 && lane == 0)
+    {
+        // MMA issuer
+        for (int a = 0; a < natoms; ++a)
+        {
+            const int s = a % S;
+            if (!mbar_wait(&full[s], (a / S) & 1))
+            {
+                raise_error(st, DEV_WAIT_TIMEOUT, 11);
+                atomicExch(s_fail, 1);
+                break;
+            }
+            tc_fence_after();
+            const uint32_t sa = smem_u32(tiles + (size_t)s * OPS * kTcTileBytes);
+            const uint32_t sb = sa + kTcTileBytes;
+#pragma unroll
+            for (int kk = 0; kk < kTcAtomBytes / 32; ++kk)
+            {
+                const uint64_t da = tc_desc(sa + kk * 32);
+                const uint64_t db = tc_desc(sb + kk * 32);
+                tc_mma<KIND>(tmem, da, db, IDESC, (a > 0 || kk > 0) ? 1u : 0u);
+                if constexpr (SPLIT3)
+                {
+                    const uint64_t das = tc_desc(sa + 2 * kTcTileBytes + kk * 32);
+                    const uint64_t dbs = tc_desc(sa + 3 * kTcTileBytes + kk * 32);
+                    tc_mma<KIND>(tmem, da, dbs, IDESC, 1u);
+                    tc_mma<KIND>(tmem, das, db, IDESC, 1u);
+                }
+            }
+            tc_commit(&empty[s]);
+        }
+        tc_commit(done);
+    }
+    __syncwarp();
+
+    // epilogue: thread = one row of the tile, 32 columns per tensor-memory load
+    const bool ok = mbar_wait(done, 0);
+    if (!ok)
+    {
+        raise_error(st, DEV_WAIT_TIMEOUT, 12);
+    }
+    tc_fence_after();
+    if (ok && !*reinterpret_cast<volatile int*>(s_fail))
+    {
+        const int  r     = m0 + warp * 32 + lane;
+        const bool row_ok = r < M;
+        float*     crow  = C + (size_t)(row_ok ? r : 0) * ldc;
+        const bool vec   = ((ldc & 3) == 0) && ((reinterpret_cast<uintptr_t>(C) & 15) == 0);
+#pragma unroll 1
+        for (int j = 0; j < kTcBN / 32; ++j)
+        {
+            float v[32];
+            tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(j * 32), v);
+            const int c0 = n0 + j * 32;
+            if (!row_ok)
+            {
+                continue;
+            }
+            if (vec && c0 + 32 <= N)
+            {
+                float4* p = reinterpret_cast<float4*>(crow + c0);
+#pragma unroll
+                for (int q = 0; q < 8; ++q)
+                {
+                    float4 x = p[q];
+                    x.x -= v[4 * q];
+                    x.y -= v[4 * q + 1];
+                    x.z -= v[4 * q + 2];
+                    x.w -= v[4 * q + 3];
+                    p[q] = x;
+                }
+            }
+            else
+            {
+#pragma unroll
+                for (int q = 0; q < 32; ++q)
+                {
+                    if (c0 + q < N)
+                    {
+                        crow[c0 + q] -= v[q];
+                    }
+                }
+            }
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0 && lane == 0 && *reinterpret_cast<volatile int*>(s_fail))
+    {
+        // drain: wait (bounded) for the loads this CTA issued so no copy is
+        // still writing shared memory when the CTA exits
+        const int issued = *reinterpret_cast<volatile int*>(s_issued);
+        for (int s = 0; s < S; ++s)
+        {
+            if (s < issued)
+            {
+                const int last_a = ((issued - 1 - s) / S) * S + s;
+                mbar_wait(&full[s], (last_a / S) & 1);
+            }
+        }
+    }
+    __syncthreads();
+    if (warp == 0)
+    {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTcBN)
+                     : "memory");
+    }
+}
+
+}  // namespace b200la

@@ -1,0 +1,69 @@
+"""tcgen05 tensor-core update c -= a b^T (the mixed-precision LU's trailing
+update) against a float64 reference of the same (quantized) operands (GPU)."""
+import pytest
+import torch
+
+from linearalgebra_b200 import _lib
+
+pytestmark = pytest.mark.gpu
+
+TF32, BF16, FP16 = 0, 1, 2
+
+
+def tf32_trunc(x: torch.Tensor) -> torch.Tensor:
+    """fp32 with the 13 low mantissa bits cleared (the TF32 value the tensor
+    core reads from an fp32 container)."""
+    return (x.view(torch.int32) & ~0x1FFF).view(torch.float32)
+
+
+def run(kind, split3, m, n, k, seed=0):
+    lib = _lib.load()
+    g = torch.Generator(device="cuda").manual_seed(seed)
+    a32 = torch.randn(m, k, device="cuda", generator=g)
+    b32 = torch.randn(n, k, device="cuda", generator=g)
+    c = torch.randn(m, n, device="cuda", generator=g)
+    c0 = c.clone()
+    if kind == TF32:
+        a, b = a32, b32
+        if split3:
+            a_s, b_s = a32 - tf32_trunc(a32), b32 - tf32_trunc(b32)
+        else:
+            a_s = b_s = None
+    else:
+        dt = torch.bfloat16 if kind == BF16 else torch.float16
+        a, b = a32.to(dt), b32.to(dt)
+        a_s = b_s = None
+    ws = torch.empty(lib.b200la_tc_update_workspace_size(), dtype=torch.uint8, device="cuda")
+    st = lib.b200la_sgemm_tc_update(kind, int(split3), c.data_ptr(), n, m, n, k, a.data_ptr(), b.data_ptr(),
+                                    a_s.data_ptr() if a_s is not None else None,
+                                    b_s.data_ptr() if b_s is not None else None,
+                                    ws.data_ptr(), ws.numel(), torch.cuda.current_stream().cuda_stream)
+    _lib.check(st)
+    torch.cuda.synchronize()
+    if kind == TF32 and not split3:
+        ref = c0.double() - tf32_trunc(a32).double() @ tf32_trunc(b32).double().T
+        tol = 4 * k * 2.0 ** -10
+    elif kind == TF32:
+        ref = c0.double() - a32.double() @ b32.double().T
+        tol = 4 * k * 2.0 ** -20
+    else:
+        ref = c0.double() - a.double() @ b.double().T
+        tol = 4 * k * 2.0 ** -22
+    err = (c.double() - ref).abs().max().item()
+    return err, tol
+
+
+@pytest.mark.parametrize("kind,split3", [(TF32, False), (TF32, True), (BF16, False), (FP16, False)])
+@pytest.mark.parametrize("m,n,k", [(128, 128, 128), (300, 200, 256), (1000, 520, 128)])
+def test_tc_update_matches_reference(kind, split3, m, n, k):
+    err, tol = run(kind, split3, m, n, k)
+    assert err <= tol, (err, tol)
+
+
+def test_tc_update_rejects_bad_depth():
+    lib = _lib.load()
+    p = torch.empty(1024, device="cuda")
+    ws = torch.empty(256, dtype=torch.uint8, device="cuda")
+    st = lib.b200la_sgemm_tc_update(BF16, 0, p.data_ptr(), 8, 8, 8, 40, p.data_ptr(), p.data_ptr(), None, None,
+                                    ws.data_ptr(), 256, None)
+    assert st == _lib.INVALID_ARGUMENT
