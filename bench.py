@@ -49,6 +49,9 @@ def parse():
     p.add_argument("--n", type=int, default=N_DEFAULT)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-compare", action="store_true", help="skip timing the other method")
+    p.add_argument("--method", choices=["mixed", "fp64"], default="mixed")
+    p.add_argument("--precision", choices=["fp32", "tf32", "bf16", "fp16"], default="fp32")
     return p.parse_args()
 
 
@@ -208,6 +211,29 @@ def cpu_model():
 # ---------------------------------------------------------------------------
 # B200 arm
 # ---------------------------------------------------------------------------
+CLASS_NAMES = {0: "panel", 1: "laswp_u12", 2: "trailing_simt", 3: "solve", 4: "gemm", 5: "tc_update",
+               6: "residual", 7: "batched", 8: "operand_prep"}
+
+
+def algorithmic_work(n: int, method: str, nb_out: int = 256):
+    """Per-step algorithmic flops / bytes of the kernel classes that have a
+    roofline, for one solve of order n (nrhs = 1)."""
+    work = {}
+    if method == "fp64":
+        fl = sum(2 * (n - k - min(64, n - k)) ** 2 * min(64, n - k) for k in range(0, n, 64))
+        work[2] = {"bound": "fp64", "flops": fl, "bytes": 16 * sum((n - k - 64) ** 2 for k in range(0, n, 64) if n - k > 64)}
+    else:
+        fl, by = 0, 0
+        for K in range(0, n, nb_out):
+            rest = n - min(K + nb_out, n)
+            if rest > 0:
+                fl += 2 * rest * rest * nb_out
+                by += 8 * rest * rest
+        work[5] = {"bound": "hbm", "flops": fl, "bytes": by}
+        work[6] = {"bound": "hbm", "flops": 2 * n * n, "bytes": 8 * n * n}
+    return work
+
+
 def run_b200(args, world, rank, local):
     import numpy as np
     import torch
@@ -223,28 +249,55 @@ def run_b200(args, world, rank, local):
     A = torch.randn(n, n, dtype=torch.float64, device=dev, generator=gen)
     x_true = torch.rand(n, dtype=torch.float64, device=dev, generator=gen) * 2 - 1
     b = A @ x_true
-    m = torch.empty_like(A)
     x = torch.empty_like(b)
+    stream = torch.cuda.current_stream(dev)
+    sp = stream.cuda_stream
+    peaks = measured_peaks()
+
+    # ---- the FP64 comparison arm: plain FP64 LU + solve (the reference's algorithm)
+    m = torch.empty_like(A)
+    xf = torch.empty_like(b)
     piv = torch.empty(n, dtype=torch.int64, device=dev)
     ws_bytes = lib.b200la_dgesv_workspace_size(n, la.LU_LINEAR_SOLVER)
     ws = torch.empty(ws_bytes, dtype=torch.uint8, device=dev)
-    stream = torch.cuda.current_stream(dev)
-    sp = stream.cuda_stream
 
-    def step():
+    def step_fp64():
         m.copy_(A)
-        x.copy_(b)
-        _lib.check(lib.b200la_dgesv(m.data_ptr(), piv.data_ptr(), n, x.data_ptr(),
+        xf.copy_(b)
+        _lib.check(lib.b200la_dgesv(m.data_ptr(), piv.data_ptr(), n, xf.data_ptr(),
                                     la.LU_LINEAR_SOLVER, ws.data_ptr(), ws_bytes, sp))
 
+    # ---- the headline arm: mixed-precision LU-IR to eta <= 1e-14
+    solver = la.MixedSolver(n, 1, dev, precision=args.precision, tolerance=1e-14)
+    last = {}
+
+    def step_mixed():
+        _, res, st = solver(A, b, x, stream)
+        last.update(res)
+        last["status"] = st
+
+    step = step_mixed if args.method == "mixed" else step_fp64
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize()
 
+    # ---- per-class breakdown of one untimed step (picks the roofline kernel)
+    lib.b200la_profile_start(sum(1 << c for c in CLASS_NAMES))
+    step()
+    torch.cuda.synchronize()
+    breakdown = {}
+    for c, name in CLASS_NAMES.items():
+        t_ms, cnt = ctypes.c_double(0), ctypes.c_int64(0)
+        lib.b200la_profile_stop(c, ctypes.addressof(t_ms), ctypes.addressof(cnt))
+        if cnt.value:
+            breakdown[name] = {"ms": round(t_ms.value, 3), "launches": int(cnt.value)}
+    work = algorithmic_work(n, args.method)
+    roof_cls = max(work, key=lambda c: breakdown.get(CLASS_NAMES[c], {"ms": 0})["ms"])
+
     # ---- timed region
     clocks = ClockSampler(local)
     launches0 = lib.b200la_launch_count()
-    lib.b200la_profile_start(1 << 2)  # trailing update kernel class
+    lib.b200la_profile_start(1 << roof_cls)
     barrier(world)
     torch.cuda.synchronize()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -255,56 +308,59 @@ def run_b200(args, world, rank, local):
     torch.cuda.synchronize()
     barrier(world)
     elapsed_ms = ev0.elapsed_time(ev1)
-    trail_ms = ctypes.c_double(0)
-    trail_n = ctypes.c_int64(0)
-    lib.b200la_profile_stop(2, ctypes.addressof(trail_ms), ctypes.addressof(trail_n))
+    k_ms, k_n = ctypes.c_double(0), ctypes.c_int64(0)
+    lib.b200la_profile_stop(roof_cls, ctypes.addressof(k_ms), ctypes.addressof(k_n))
     launches = lib.b200la_launch_count() - launches0
     clk = clocks.stop()
-
     ms_per_step = max_over_ranks(world, elapsed_ms / args.steps)
 
-    # per-kernel-class breakdown of one extra (untimed) step
-    classes = {0: "panel", 1: "laswp_u12", 2: "trailing", 3: "solve"}
-    lib.b200la_profile_start(sum(1 << c for c in classes))
-    step()
-    torch.cuda.synchronize()
-    breakdown = {}
-    for c, name in classes.items():
-        t_ms, cnt = ctypes.c_double(0), ctypes.c_int64(0)
-        lib.b200la_profile_stop(c, ctypes.addressof(t_ms), ctypes.addressof(cnt))
-        breakdown[name] = {"ms": round(t_ms.value, 3), "launches": int(cnt.value)}
+    # accuracy of the last solve, checked on the device in FP64
+    xs = x if args.method == "mixed" else xf
+    r = b - A @ xs
+    eta = (r.abs().max() / (A.abs().sum(1).max() * xs.abs().max() + b.abs().max())).item()
+    fwd = ((xs - x_true).abs().max() / x_true.abs().max()).item()
 
-    # accuracy of the last solve (FP64 residual, checked on the device)
-    r = b - A @ x
-    eta = (r.abs().max() / (A.abs().sum(1).max() * x.abs().max() + b.abs().max())).item()
-    fwd = ((x - x_true).abs().max() / x_true.abs().max()).item()
-
-    # ---- roofline of the trailing update (dominant kernel): algorithmic
-    # flops 2 * rest^2 * w per panel step
-    flops_per_solve = 0
-    for k in range(0, n, 64):
-        w = min(64, n - k)
-        rest = n - k - w
-        flops_per_solve += 2 * rest * rest * w
-    trail_launches_per_solve = sum(1 for k in range(0, n, 64) if n - k - min(64, n - k) > 0)
-    achieved_tflops = (flops_per_solve * args.steps) / (trail_ms.value * 1e-3) / 1e12 if trail_ms.value else None
-    fp64_peak = measured_fp64_peak_tflops()
+    # ---- roofline of the dominant kernel class, timed live over the region
+    w = work[roof_cls]
+    secs = k_ms.value * 1e-3
+    if w["bound"] == "fp64":
+        achieved = w["flops"] * args.steps / secs / 1e12 if secs else None
+        peak, unit = measured_fp64_peak_tflops(), "TFLOP/s"
+        peak_src = ("cuBLAS DGEMM 8192^3 via torch.matmul, best of 5, measured in this run "
+                    "(MEASURED_PEAKS.json holds no FP64 figure)")
+    else:
+        achieved = w["bytes"] * args.steps / secs / 1e9 if secs else None
+        peak, unit = peaks["hbm_gbs"], "GB/s"
+        peak_src = peaks["source"]
     roofline = {
-        "kernel": "k_trailing<double> (A22 -= L21*U12, FP64 DFMA)",
-        "bound": "fp64",
-        "achieved": achieved_tflops,
-        "peak": fp64_peak,
-        "peak_source": "cuBLAS DGEMM 8192^3 via torch.matmul, best of 5, measured in this run "
-                       "(MEASURED_PEAKS.json holds no FP64 figure)",
-        "unit": "TFLOP/s",
-        "frac": (achieved_tflops / fp64_peak) if achieved_tflops else None,
-        "traffic": None,
-        "launches": int(trail_n.value),
-        "launches_per_step": trail_launches_per_solve,
-        "avg_launch_ms": trail_ms.value / max(1, trail_n.value),
-        "share_of_step": (trail_ms.value / args.steps) / ms_per_step if ms_per_step else None,
-        "algorithmic_flops_per_step": flops_per_solve,
+        "kernel": CLASS_NAMES[roof_cls], "bound": w["bound"], "achieved": achieved, "peak": peak,
+        "unit": unit, "frac": achieved / peak if achieved else None, "traffic": None,
+        "peak_source": peak_src, "launches": int(k_n.value),
+        "avg_launch_ms": k_ms.value / max(1, k_n.value),
+        "share_of_step": (k_ms.value / args.steps) / ms_per_step if ms_per_step else None,
+        "algorithmic_per_step": {"flops": w["flops"], "bytes": w["bytes"]},
+        "tensor_tflops": (w["flops"] * args.steps / secs / 1e12) if (secs and w["bound"] == "hbm") else None,
     }
+
+    # ---- the other arm, timed the same way (fewer steps)
+    other = {}
+    if not args.no_compare:
+        ostep = step_fp64 if args.method == "mixed" else step_mixed
+        ostep()
+        torch.cuda.synchronize()
+        o0, o1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ksteps = max(1, min(args.steps, 2))
+        o0.record(stream)
+        for _ in range(ksteps):
+            ostep()
+        o1.record(stream)
+        torch.cuda.synchronize()
+        o_ms = max_over_ranks(world, o0.elapsed_time(o1) / ksteps)
+        ox = xf if args.method == "mixed" else x
+        rr = b - A @ ox
+        oeta = (rr.abs().max() / (A.abs().sum(1).max() * ox.abs().max() + b.abs().max())).item()
+        other = {"method": "fp64_lu" if args.method == "mixed" else "mixed_ir", "s": o_ms / 1e3,
+                 "backward_error": oeta, "steps": ksteps}
 
     # ---- end to end through the C ABI from pinned host buffers
     e2e = None
@@ -312,24 +368,32 @@ def run_b200(args, world, rank, local):
         hA = A.cpu().pin_memory()
         hb = b.cpu().pin_memory()
         hx = torch.empty(n, dtype=torch.float64).pin_memory()
+        dA = torch.empty_like(A)
+        db = torch.empty_like(b)
         e_steps = max(1, min(args.steps, 3))
         torch.cuda.synchronize()
         barrier(world)
         s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         s0.record(stream)
         for _ in range(e_steps):
-            m.copy_(hA, non_blocking=True)
-            x.copy_(hb, non_blocking=True)
-            _lib.check(lib.b200la_dgesv(m.data_ptr(), piv.data_ptr(), n, x.data_ptr(),
-                                        la.LU_LINEAR_SOLVER, ws.data_ptr(), ws_bytes, sp))
-            hx.copy_(x, non_blocking=True)
+            dA.copy_(hA, non_blocking=True)
+            db.copy_(hb, non_blocking=True)
+            if args.method == "mixed":
+                solver(dA, db, x, stream)
+                hx.copy_(x, non_blocking=True)
+            else:
+                m.copy_(dA)
+                xf.copy_(db)
+                _lib.check(lib.b200la_dgesv(m.data_ptr(), piv.data_ptr(), n, xf.data_ptr(),
+                                            la.LU_LINEAR_SOLVER, ws.data_ptr(), ws_bytes, sp))
+                hx.copy_(xf, non_blocking=True)
         s1.record(stream)
         torch.cuda.synchronize()
         barrier(world)
         e2e_s = max_over_ranks(world, s0.elapsed_time(s1) / e_steps) / 1e3
         e2e = {"value": e2e_s, "unit": "s", "h2d_bytes_per_step": 8 * n * n + 8 * n,
                "d2h_bytes_per_step": 8 * n, "steps": e_steps}
-        del hA, hb, hx
+        del hA, hb, hx, dA, db
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -342,6 +406,9 @@ def run_b200(args, world, rank, local):
                          "has no threading"}
 
     if rank == 0:
+        method_desc = (f"mixed-precision LU-IR ({args.precision} factorization on tcgen05, FP64 "
+                       "refinement to backward error <= 1e-14)" if args.method == "mixed"
+                       else "plain FP64 blocked LU + solve")
         line = {
             "metric": METRIC,
             "value": ms_per_step / 1e3,
@@ -353,21 +420,28 @@ def run_b200(args, world, rank, local):
             "higher_is_better": False,
             "scaling": "weak",
             "vs_baseline": None,
-            "dtype": "f64",
+            "dtype": "f64" if args.method == "fp64" else f"{args.precision}+f64",
             "data": f"synthetic: A iid N(0,1) (torch generator seed {SEED}+rank), x_true iid U[-1,1], b = A x_true",
-            "config": {"workload": f"dense LU solve n={n} nrhs=1 (plain FP64 blocked LU + solve)",
-                       "n": n, "nrhs": 1, "method": "fp64_lu", "panel": 64,
-                       "step": "restore A and b (device copies, 2 GiB), factor, solve",
+            "config": {"workload": f"dense LU solve n={n} nrhs=1, {method_desc}",
+                       "n": n, "nrhs": 1, "method": args.method,
+                       "precision": args.precision if args.method == "mixed" else "fp64",
+                       "step": ("solve from A, b resident in HBM (A left unchanged)" if args.method == "mixed"
+                                else "restore A and b (device copies, 2 GiB), factor, solve"),
                        "l2": "inputs (2 GiB) larger than L2; no flush",
                        "parallelism": "replicas" if world > 1 else "single GPU"},
-            "accuracy": {"backward_error": eta, "forward_error": fwd, "bound_10n_eps": 10 * n * EPS64},
+            "accuracy": {"backward_error": eta, "forward_error": fwd, "target": 1e-14,
+                         "refinement": {k: last[k] for k in ("precision_used", "iterations", "gmres_iterations",
+                                                             "escalations", "converged", "factor_ms", "refine_ms")}
+                         if last else None},
+            "compare": other,
+            "speedup_vs_fp64_lu": (other["s"] / (ms_per_step / 1e3)) if other and args.method == "mixed" else None,
             "roofline": roofline,
             "cpu_baseline": cpu,
             "e2e": e2e,
             "gpu_launches": int(launches),
             "breakdown_one_step": breakdown,
             "clocks": clk,
-            "peaks": measured_peaks(),
+            "peaks": peaks,
         }
         print(json.dumps(line), flush=True)
 

@@ -59,7 +59,8 @@ B200LA_API int64_t b200la_launch_count(void);
 /* Launch recorder for measurement: while started, every launch of a kernel
  * class in `class_mask` (bit 0 panel, 1 row interchange + U12 solve,
  * 2 trailing update, 3 triangular solves, 4 general GEMM, 5 mixed-precision
- * factorization GEMM, 6 FP64 residual, 7 batched solver) is bracketed by a
+ * factorization GEMM, 6 FP64 residual, 7 batched solver, 8 mixed-precision
+ * operand preparation and outer U12 solve) is bracketed by a
  * pair of CUDA events on its stream.  b200la_profile_stop synchronizes those
  * events and returns the summed device time (ms) and launch count of one
  * class; it also stops recording. */
@@ -164,6 +165,52 @@ B200LA_API int    b200la_dgemm(int transpose_a, int transpose_b, int64_t rows, i
 B200LA_API int    b200la_sgemm(int transpose_a, int transpose_b, int64_t rows, int64_t cols,
        int64_t depth, float alpha, const float* a, int64_t lda, const float* b, int64_t ldb,
        float beta, float* c, int64_t ldc, void* workspace, size_t workspace_bytes, void* stream);
+
+/* ---- mixed-precision LU solve with FP64 iterative refinement --------------
+ * Solves A X = B (A n x n FP64, row stride n, left unchanged; B, X n x nrhs,
+ * row strides ldb, ldx >= nrhs, nrhs <= 64) to a normwise backward error
+ * max_j ||b_j - A x_j|| / (||A|| ||x_j|| + ||b_j||) (inf norms) <= tolerance:
+ * LU with partial pivoting of an FP32 copy of A whose trailing updates run on
+ * the tcgen05 tensor cores in the chosen precision with FP32 accumulation,
+ * then FP64 refinement (residual, update and test in FP64), switching to
+ * GMRES-IR preconditioned by the low-precision factors when plain
+ * refinement stalls, and escalating to the next precision (FP32, then plain
+ * FP64 LU) when that fails too.  Synchronous (reads the residual norms).
+ * Extension: the reference has no mixed-precision solver. */
+#define B200LA_PREC_FP64 0 /* plain FP64 LU (the reference's algorithm) + refinement */
+#define B200LA_PREC_FP32 1 /* FP32 factors, three-term TF32 tensor-core updates */
+#define B200LA_PREC_TF32 2 /* FP32 factors, TF32 tensor-core updates */
+#define B200LA_PREC_BF16 3 /* FP32 factors, BF16 tensor-core updates */
+#define B200LA_PREC_FP16 4 /* FP32 factors, FP16 tensor-core updates */
+
+typedef struct b200la_refine_options
+{
+    int    precision;      /* B200LA_PREC_* of the factorization */
+    int    max_iterations; /* refinement iterations (default 50) */
+    double tolerance;      /* target normwise backward error (default 1e-14) */
+    int    gmres_restart;  /* GMRES-IR restart length, 0 disables (nrhs == 1 only) */
+    int    escalate;       /* on failure, retry at the next precision up to FP64 */
+} b200la_refine_options;
+
+typedef struct b200la_refine_result
+{
+    int    precision_used;   /* B200LA_PREC_* of the factorization that finished */
+    int    info;             /* LAPACK info of that factorization */
+    int    converged;        /* backward error <= tolerance */
+    int    iterations;       /* refinement corrections applied */
+    int    gmres_iterations; /* inner GMRES iterations */
+    int    escalations;      /* precision escalations */
+    double backward_error;   /* final max_j eta_j */
+    double factor_ms;        /* device time of the factorization(s) */
+    double refine_ms;        /* device time of the solves and refinement */
+} b200la_refine_result;
+
+B200LA_API void   b200la_refine_default_options(b200la_refine_options* options);
+B200LA_API size_t b200la_dsolve_mixed_workspace_size(int64_t n, int64_t nrhs,
+       const b200la_refine_options* options);
+B200LA_API int    b200la_dsolve_mixed(const double* a, int64_t n, int64_t nrhs, const double* b,
+       int64_t ldb, double* x, int64_t ldx, const b200la_refine_options* options,
+       b200la_refine_result* result, void* workspace, size_t workspace_bytes, void* stream);
 
 /* ---- tensor-core update (mixed-precision LU building block) ---------------
  * c[m x n] (fp32, row stride ldc) -= a[m x k] * b[n x k]^T on the tcgen05

@@ -9,6 +9,7 @@ from ._lib import B200Error, B200InvalidArgument  # noqa: F401
 from .api import (  # noqa: F401
     LU_LINEAR_SOLVER,
     LU_UPFRONT_LINEAR_SOLVER,
+    MixedSolver,
     gemm,
     gesv,
     getrf,
@@ -16,6 +17,7 @@ from .api import (  # noqa: F401
     linear_solver,
     lu_decomposition,
     multiplication,
+    solve_mixed,
     triangular_solver,
     trsm,
 )

@@ -62,9 +62,32 @@ SIGNATURES: dict[str, tuple] = {
     "b200la_sgemm_workspace_size": (_sz, [_i64, _i64, _i64]),
     "b200la_dgemm": (_i32, [_i32, _i32, _i64, _i64, _i64, _d, _p, _i64, _p, _i64, _d, _p, _i64, _p, _sz, _p]),
     "b200la_sgemm": (_i32, [_i32, _i32, _i64, _i64, _i64, _f, _p, _i64, _p, _i64, _f, _p, _i64, _p, _sz, _p]),
+    "b200la_refine_default_options": (None, [_p]),
+    "b200la_dsolve_mixed_workspace_size": (_sz, [_i64, _i64, _p]),
+    "b200la_dsolve_mixed": (_i32, [_p, _i64, _i64, _p, _i64, _p, _i64, _p, _p, _p, _sz, _p]),
     "b200la_tc_update_workspace_size": (_sz, []),
     "b200la_sgemm_tc_update": (_i32, [_i32, _i32, _p, _i64, _i64, _i64, _i64, _p, _p, _p, _p, _p, _sz, _p]),
 }
+
+
+PREC_FP64, PREC_FP32, PREC_TF32, PREC_BF16, PREC_FP16 = 0, 1, 2, 3, 4
+PREC_NAMES = {PREC_FP64: "fp64", PREC_FP32: "fp32", PREC_TF32: "tf32", PREC_BF16: "bf16", PREC_FP16: "fp16"}
+
+
+class RefineOptions(ctypes.Structure):
+    _fields_ = [("precision", ctypes.c_int), ("max_iterations", ctypes.c_int),
+                ("tolerance", ctypes.c_double), ("gmres_restart", ctypes.c_int),
+                ("escalate", ctypes.c_int)]
+
+
+class RefineResult(ctypes.Structure):
+    _fields_ = [("precision_used", ctypes.c_int), ("info", ctypes.c_int), ("converged", ctypes.c_int),
+                ("iterations", ctypes.c_int), ("gmres_iterations", ctypes.c_int),
+                ("escalations", ctypes.c_int), ("backward_error", ctypes.c_double),
+                ("factor_ms", ctypes.c_double), ("refine_ms", ctypes.c_double)]
+
+    def as_dict(self):
+        return {f: getattr(self, f) for f, _ in self._fields_}
 
 
 class B200Error(RuntimeError):

@@ -177,3 +177,53 @@ def gemm(transpose_a, transpose_b, alpha, a, b, beta, c, stream=None):
     multiplication.apply(transpose_a, transpose_b, rows, cols, depth, alpha, a, a.stride(0),
                          b, b.stride(0), beta, c, c.stride(0), None, 0, stream)
     return c
+
+
+# ----------------------------------------------------------------------------
+# mixed-precision LU-IR (extension; no reference counterpart)
+# ----------------------------------------------------------------------------
+PRECISIONS = {"fp64": _lib.PREC_FP64, "fp32": _lib.PREC_FP32, "tf32": _lib.PREC_TF32,
+              "bf16": _lib.PREC_BF16, "fp16": _lib.PREC_FP16}
+
+
+def refine_options(precision="fp32", tolerance=1e-14, max_iterations=50, gmres_restart=30, escalate=True):
+    o = _lib.RefineOptions()
+    _lib.load().b200la_refine_default_options(ctypes.byref(o))
+    o.precision = PRECISIONS[precision] if isinstance(precision, str) else int(precision)
+    o.tolerance = tolerance
+    o.max_iterations = max_iterations
+    o.gmres_restart = gmres_restart
+    o.escalate = int(bool(escalate))
+    return o
+
+
+class MixedSolver:
+    """Reusable workspace + call of b200la_dsolve_mixed for one (n, nrhs, options)."""
+
+    def __init__(self, n, nrhs=1, device=None, **opts):
+        self.n, self.nrhs = n, nrhs
+        self.opts = refine_options(**opts)
+        lib = _lib.load()
+        self.nbytes = int(lib.b200la_dsolve_mixed_workspace_size(n, nrhs, ctypes.byref(self.opts)))
+        self.ws = workspace(self.nbytes, device)
+
+    def __call__(self, a, b, x=None, stream=None):
+        n, nrhs = self.n, self.nrhs
+        if x is None:
+            x = torch.empty_like(b)
+        ldb = 1 if b.dim() == 1 else b.stride(0)
+        ldx = 1 if x.dim() == 1 else x.stride(0)
+        res = _lib.RefineResult()
+        st = _lib.load().b200la_dsolve_mixed(_ptr(a), n, nrhs, _ptr(b), ldb, _ptr(x), ldx,
+                                             ctypes.byref(self.opts), ctypes.byref(res), _ptr(self.ws),
+                                             self.nbytes, _stream(stream))
+        _lib.check(st, allow=(_lib.SUCCESS, _lib.NOT_CONVERGED, _lib.SINGULAR))
+        return x, res.as_dict(), st
+
+
+def solve_mixed(a, b, precision="fp32", **opts):
+    """Mixed-precision LU-IR solve of a x = b (FP64 CUDA tensors, a row-major
+    n x n, b n or n x nrhs).  Returns (x, result dict, status)."""
+    nrhs = 1 if b.dim() == 1 else b.shape[1]
+    solver = MixedSolver(a.shape[0], nrhs, a.device, precision=precision, **opts)
+    return solver(a, b)

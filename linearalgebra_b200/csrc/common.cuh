@@ -128,7 +128,8 @@ enum KernelClass : int
     KC_MIXED    = 5,
     KC_RESIDUAL = 6,
     KC_BATCHED  = 7,
-    KC_COUNT    = 8
+    KC_PREP     = 8,
+    KC_COUNT    = 9
 };
 
 // Host helpers shared by the entry points (defined in runtime.cu).

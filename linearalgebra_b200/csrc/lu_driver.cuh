@@ -1,0 +1,713 @@
+// Host-side helpers shared by the LU drivers (plain FP64/FP32 LU-solve path
+// and the mixed-precision solver): workspace plans, kernel attributes, panel
+// launch, triangular-solve sequencing.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <climits>
+#include <cstdint>
+#include <cstdlib>
+#include <mutex>
+
+#include "lu_kernels.cuh"
+#include "solve_kernels.cuh"
+
+namespace b200la
+{
+int require_sm100();
+
+constexpr size_t kPanelSmemMax = 200 * 1024;
+
+
+// Cluster size usable by k_panel_cluster on each device (0: none).
+template <typename T> int& cluster_size_slot(int dev)
+{
+    static int sizes[64] = {};
+    return sizes[dev];
+}
+
+template <typename T> int probe_cluster_size()
+{
+    for (int cl : {16, 8})
+    {
+        cudaLaunchConfig_t  cfg = {};
+        cudaLaunchAttribute attr[1];
+        cfg.gridDim                    = dim3(cl);
+        cfg.blockDim                   = dim3(kPanelThreads);
+        cfg.dynamicSmemBytes           = kPanelSmemMax;
+        attr[0].id                     = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x       = cl;
+        attr[0].val.clusterDim.y       = 1;
+        attr[0].val.clusterDim.z       = 1;
+        cfg.attrs                      = attr;
+        cfg.numAttrs                   = 1;
+        int clusters                   = 0;
+        if (cudaOccupancyMaxActiveClusters(&clusters, (const void*)k_panel_cluster<T>, &cfg) ==
+                cudaSuccess &&
+            clusters > 0)
+        {
+            return cl;
+        }
+        cudaGetLastError();
+    }
+    return 0;
+}
+
+// Raise the dynamic shared-memory limits once per device and type.
+template <typename T> int ensure_kernel_attributes()
+{
+    static std::mutex m;
+    static bool       done[64] = {};
+    int               dev      = 0;
+    B200LA_CUDA(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lock(m);
+    if (dev >= 0 && dev < 64 && done[dev])
+    {
+        return B200LA_SUCCESS;
+    }
+    B200LA_CUDA(cudaFuncSetAttribute(
+        k_panel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPanelSmemMax));
+    B200LA_CUDA(cudaFuncSetAttribute(
+        k_perm_from_pivots<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    B200LA_CUDA(cudaFuncSetAttribute(
+        k_panel_cluster<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPanelSmemMax));
+    B200LA_CUDA(cudaFuncSetAttribute(
+        k_panel_cluster<T>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+    if (dev >= 0 && dev < 64)
+    {
+        cluster_size_slot<T>(dev) = probe_cluster_size<T>();
+    }
+    B200LA_CUDA(cudaFuncSetAttribute(
+        k_laswp_trsm<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)laswp_smem_bytes<T>()));
+    B200LA_CUDA(cudaFuncSetAttribute(
+        k_trailing<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)trailing_smem_bytes<T>()));
+    B200LA_CUDA(cudaFuncSetAttribute(k_gemm<T, false, false>,
+        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gemm_smem_bytes<T>()));
+    B200LA_CUDA(cudaFuncSetAttribute(k_gemm<T, true, false>,
+        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gemm_smem_bytes<T>()));
+    B200LA_CUDA(cudaFuncSetAttribute(k_gemm<T, false, true>,
+        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gemm_smem_bytes<T>()));
+    B200LA_CUDA(cudaFuncSetAttribute(k_gemm<T, true, true>,
+        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gemm_smem_bytes<T>()));
+    if (dev >= 0 && dev < 64)
+    {
+        done[dev] = true;
+    }
+    return B200LA_SUCCESS;
+}
+
+// Shared memory for k_perm_from_pivots: the whole permutation when it fits
+// in 200 KB (n <= 51200), else 0 (the kernel then works in global memory).
+inline size_t perm_smem_bytes(int n)
+{
+    const size_t b = (size_t)n * sizeof(int32_t);
+    return b <= 200 * 1024 ? b : 0;
+}
+
+inline int prepare_device()
+{
+    return require_sm100();
+}
+
+template <typename T> int prepare()
+{
+    int st = prepare_device();
+    if (st != B200LA_SUCCESS)
+    {
+        return st;
+    }
+    return ensure_kernel_attributes<T>();
+}
+
+// ---------------------------------------------------------------------------
+// Workspace plans.  The same function sizes (Arena()) and carves
+// (Arena(base, bytes)).
+// ---------------------------------------------------------------------------
+template <typename T> struct GetrfPlan
+{
+    DeviceStatus* st;
+    uint64_t*     hdr;
+    uint64_t*     payload;
+    uint64_t*     diag;
+    PermList*     perm;
+};
+
+template <typename T> GetrfPlan<T> plan_getrf(Arena& a)
+{
+    GetrfPlan<T> p;
+    p.st      = a.next<DeviceStatus>(1);
+    p.hdr     = a.next<uint64_t>(panel_hdr_words<T>());
+    p.payload = a.next<uint64_t>(panel_payload_words<T>());
+    p.diag    = a.next<uint64_t>(panel_diag_words<T>());
+    p.perm    = a.next<PermList>(1);
+    return p;
+}
+
+template <typename T> struct SolvePlan
+{
+    int32_t* perm;
+    T*       y;
+};
+
+template <typename T> SolvePlan<T> plan_solve(Arena& a, int64_t n, int64_t nrhs)
+{
+    SolvePlan<T> p;
+    p.perm = a.next<int32_t>((size_t)n);
+    p.y    = a.next<T>((size_t)n * (size_t)nrhs);
+    return p;
+}
+
+inline cudaStream_t as_stream(void* s) { return static_cast<cudaStream_t>(s); }
+
+inline int grid_1d(int64_t total, int threads)
+{
+    const int64_t g = (total + threads - 1) / threads;
+    return (int)(g < 1 ? 1 : (g > 148 * 16 ? 148 * 16 : g));
+}
+
+// ---------------------------------------------------------------------------
+// LU factorization (asynchronous).
+// ---------------------------------------------------------------------------
+// Factor panel [k, k+w) of rows [k, n): inside one thread-block cluster when
+// its rows fit there (cl > 0), else with the grid-wide kernel.
+template <typename T>
+int launch_panel(T* m, int n, int k, int w, int64_t* pivot, const GetrfPlan<T>& p, int cl, int gmax,
+    cudaStream_t s)
+{
+    const int R = n - k;
+    PanelWs<T> ws{p.hdr, p.payload, p.diag, p.perm};
+    DeviceStatus* st = p.st;
+        // the panel inside one thread-block cluster when its rows fit there
+        if (cl > 0)
+        {
+            const int    rpc_c  = (R + cl - 1) / cl;
+            const size_t smem_c = (size_t)rpc_c * (kNB + 1) * sizeof(T);
+            if (smem_c <= kPanelSmemMax)
+            {
+                cudaLaunchConfig_t  cfg = {};
+                cudaLaunchAttribute attr[1];
+                cfg.gridDim              = dim3(cl);
+                cfg.blockDim             = dim3(kPanelThreads);
+                cfg.dynamicSmemBytes     = smem_c;
+                cfg.stream               = s;
+                attr[0].id               = cudaLaunchAttributeClusterDimension;
+                attr[0].val.clusterDim.x = cl;
+                attr[0].val.clusterDim.y = 1;
+                attr[0].val.clusterDim.z = 1;
+                cfg.attrs                = attr;
+                cfg.numAttrs             = 1;
+                prof_begin(KC_PANEL, s);
+                B200LA_CUDA(cudaLaunchKernelEx(&cfg, k_panel_cluster<T>, m, n, k, w, rpc_c, pivot, p.perm, p.st));
+                prof_end(KC_PANEL, s);
+                return B200LA_SUCCESS;
+            }
+        }
+        {
+        int       G   = (R + 15) / 16;
+        G             = G < 1 ? 1 : (G > gmax ? gmax : G);
+        int rpc       = (R + G - 1) / G;
+        G             = (R + rpc - 1) / rpc;
+        size_t smem   = (size_t)rpc * (kNB + 1) * sizeof(T);
+        int    in_smem = smem <= kPanelSmemMax ? 1 : 0;
+        if (!in_smem)
+        {
+            smem = 0;
+        }
+        int   kk     = k;
+        int   nn     = n;
+        void* args[] = {&m, &nn, &kk, &w, &rpc, &in_smem, &pivot, &ws, &st};
+        prof_begin(KC_PANEL, s);
+        B200LA_CUDA(cudaLaunchCooperativeKernel(
+            (const void*)k_panel<T>, dim3(G), dim3(kPanelThreads), args, smem, s));
+        prof_end(KC_PANEL, s);
+        }
+
+    return B200LA_SUCCESS;
+}
+
+// Cluster size for the cluster panel kernel on the current device (0: the
+// grid-wide kernel only) and the grid kernel's CTA limit.
+// B200LA_FORCE_GRID_PANEL=1 keeps every panel on the grid-wide kernel (used
+// by the tests to check both panel paths).
+template <typename T> int panel_config(int& cl, int& gmax)
+{
+    const int sms = device_sm_count();
+    gmax          = sms < kMaxPanelCtas ? sms : kMaxPanelCtas;
+    int dev       = 0;
+    B200LA_CUDA(cudaGetDevice(&dev));
+    const char* force_grid = getenv("B200LA_FORCE_GRID_PANEL");
+    cl = (force_grid != nullptr && force_grid[0] == '1')
+             ? 0
+             : ((dev >= 0 && dev < 64) ? cluster_size_slot<T>(dev) : 0);
+    return B200LA_SUCCESS;
+}
+
+template <typename T> int clear_panel_exchange(const GetrfPlan<T>& p, cudaStream_t s)
+{
+    // the exchange words carry column flags: clear them so no word of an
+    // earlier factorization can validate
+    B200LA_CUDA(cudaMemsetAsync(p.hdr, 0, sizeof(uint64_t) * panel_hdr_words<T>(), s));
+    B200LA_CUDA(cudaMemsetAsync(p.payload, 0, sizeof(uint64_t) * panel_payload_words<T>(), s));
+    B200LA_CUDA(cudaMemsetAsync(p.diag, 0, sizeof(uint64_t) * panel_diag_words<T>(), s));
+    return B200LA_SUCCESS;
+}
+
+template <typename T>
+int enqueue_getrf(T* m, int n, int64_t* pivot, const GetrfPlan<T>& p, cudaStream_t s)
+{
+    {
+        const int rc = clear_panel_exchange<T>(p, s);
+        if (rc != B200LA_SUCCESS)
+        {
+            return rc;
+        }
+    }
+    prof_begin(KC_SOLVE, s);
+    k_status_init<<<1, 32, 0, s>>>(p.st, p.perm);
+    prof_end(KC_SOLVE, s);
+    B200LA_LAUNCH_CHECK();
+    int cl = 0, gmax = 0;
+    {
+        const int rc = panel_config<T>(cl, gmax);
+        if (rc != B200LA_SUCCESS)
+        {
+            return rc;
+        }
+    }
+    for (int k = 0; k < n; k += kNB)
+    {
+        int w = n - k < kNB ? n - k : kNB;
+        {
+            const int prc = launch_panel<T>(m, n, k, w, pivot, p, cl, gmax, s);
+            if (prc != B200LA_SUCCESS)
+            {
+                return prc;
+            }
+        }
+        const int rest = n - k - w;
+        const int nl   = (k + kSwapCols - 1) / kSwapCols;
+        const int nr   = (rest + kSwapCols - 1) / kSwapCols;
+        if (nl + nr > 0)
+        {
+            prof_begin(KC_SWAP, s);
+            k_laswp_trsm<T><<<nl + nr, kSwapThreads, laswp_smem_bytes<T>(), s>>>(m, n, k, w, p.perm, nl, n);
+            prof_end(KC_SWAP, s);
+            B200LA_LAUNCH_CHECK();
+        }
+        if (rest > 0)
+        {
+            dim3 grid((rest + kChunkN - 1) / kChunkN, (rest + kBandM - 1) / kBandM);
+            prof_begin(KC_TRAILING, s);
+            k_trailing<T><<<grid, 128, trailing_smem_bytes<T>(), s>>>(m, n, k, w, rest);
+            prof_end(KC_TRAILING, s);
+            B200LA_LAUNCH_CHECK();
+        }
+    }
+    prof_begin(KC_SOLVE, s);
+    k_status_finish<<<1, 32, 0, s>>>(p.st);
+    prof_end(KC_SOLVE, s);
+    B200LA_LAUNCH_CHECK();
+    return B200LA_SUCCESS;
+}
+
+template <typename T> size_t getrf_ws_size(int64_t)
+{
+    Arena a;
+    plan_getrf<T>(a);
+    return a.size();
+}
+
+template <typename T>
+int check_getrf_args(const T* m, int64_t n, const int64_t* pivot, void* ws, size_t bytes)
+{
+    if (m == nullptr || pivot == nullptr)
+    {
+        return set_error(B200LA_INVALID_ARGUMENT, "lu_decomposition: m and pivot must not be null");
+    }
+    if (n <= 0)
+    {
+        return set_error(B200LA_INVALID_ARGUMENT, "lu_decomposition: lda must be positive (got %lld)",
+            (long long)n);
+    }
+    if (n > INT_MAX / 2)
+    {
+        return set_error(B200LA_NOT_SUPPORTED, "lu_decomposition: order %lld is too large",
+            (long long)n);
+    }
+    const size_t need = getrf_ws_size<T>(n);
+    if (ws == nullptr || bytes < need)
+    {
+        return set_error(B200LA_WORKSPACE_TOO_SMALL,
+            "lu_decomposition: workspace is null or too small (%zu < %zu bytes)", bytes, need);
+    }
+    return B200LA_SUCCESS;
+}
+
+template <typename T>
+int getrf_async(T* m, int64_t n, int64_t* pivot, void* ws, size_t bytes, void* stream)
+{
+    int st = check_getrf_args(m, n, pivot, ws, bytes);
+    if (st != B200LA_SUCCESS)
+    {
+        return st;
+    }
+    st = prepare<T>();
+    if (st != B200LA_SUCCESS)
+    {
+        return st;
+    }
+    Arena        a(ws, bytes);
+    GetrfPlan<T> p = plan_getrf<T>(a);
+    return enqueue_getrf<T>(m, (int)n, pivot, p, as_stream(stream));
+}
+
+inline int read_status(const DeviceStatus* dst, int* info, cudaStream_t s)
+{
+    DeviceStatus h;
+    B200LA_CUDA(cudaMemcpyAsync(&h, dst, sizeof(h), cudaMemcpyDeviceToHost, s));
+    B200LA_CUDA(cudaStreamSynchronize(s));
+    if (h.error == DEV_WAIT_TIMEOUT)
+    {
+        return set_error(B200LA_DEVICE_TIMEOUT,
+            "a bounded device-side wait gave up (site %d); results are incomplete", h.error_site);
+    }
+    if (h.error == DEV_BAD_PIVOT)
+    {
+        return set_error(B200LA_INVALID_ARGUMENT,
+            "pivot vector holds an entry outside [i+1, n]; those entries were ignored");
+    }
+    if (h.error != 0)
+    {
+        return set_error(B200LA_CUDA_ERROR, "device status %d", h.error);
+    }
+    if (info)
+    {
+        *info = (int)h.info;
+    }
+    return h.info == 0 ? B200LA_SUCCESS : B200LA_SINGULAR;
+}
+
+template <typename T>
+int getrf_sync(T* m, int64_t n, int64_t* pivot, void* ws, size_t bytes, int* info, void* stream)
+{
+    int st = getrf_async<T>(m, n, pivot, ws, bytes, stream);
+    if (st != B200LA_SUCCESS)
+    {
+        return st;
+    }
+    Arena        a(ws, bytes);
+    GetrfPlan<T> p = plan_getrf<T>(a);
+    return read_status(p.st, info, as_stream(stream));
+}
+
+// ---------------------------------------------------------------------------
+// Triangular solves, in place on X (X already holds the right-hand sides).
+// ---------------------------------------------------------------------------
+template <typename TA, typename T = TA>
+int enqueue_trsm_inplace(bool upper, bool transpose, bool unit, int n, int nrhs, const TA* a,
+    int64_t lda, T* x, int64_t ldx, const DeviceStatus* gate, cudaStream_t s)
+{
+    const bool eff_upper = upper != transpose;
+    const int  nblocks   = (n + kTrsmBlock - 1) / kTrsmBlock;
+    for (int step = 0; step < nblocks; ++step)
+    {
+        int r0, bw, u0, um;
+        if (!eff_upper)
+        {
+            r0 = step * kTrsmBlock;
+            bw = n - r0 < kTrsmBlock ? n - r0 : kTrsmBlock;
+            u0 = r0 + bw;
+            um = n - u0;
+        }
+        else
+        {
+            const int hi = n - step * kTrsmBlock;
+            r0           = hi - kTrsmBlock > 0 ? hi - kTrsmBlock : 0;
+            bw           = hi - r0;
+            u0           = 0;
+            um           = r0;
+        }
+        prof_begin(KC_SOLVE, s);
+        k_trsm_diag<TA, T><<<(nrhs + kTrsmCols - 1) / kTrsmCols, kTrsmCols, 0, s>>>(
+            a, lda, transpose, eff_upper, unit, r0, bw, x, ldx, nrhs, gate);
+        prof_end(KC_SOLVE, s);
+        B200LA_LAUNCH_CHECK();
+        if (um > 0)
+        {
+            dim3 grid((nrhs + kUpdCols - 1) / kUpdCols, (um + 63) / 64);
+            prof_begin(KC_SOLVE, s);
+            k_trsm_update<TA, T><<<grid, 256, 0, s>>>(a, lda, transpose, r0, bw, u0, um, x, ldx, nrhs, gate);
+            prof_end(KC_SOLVE, s);
+            B200LA_LAUNCH_CHECK();
+        }
+    }
+    return B200LA_SUCCESS;
+}
+
+// Solve with LU factors: Y = P X, L Y' = Y, U X = Y'.  x is n x nrhs (ldx).
+template <typename T>
+int enqueue_getrs(const T* lu, const int64_t* pivot, int n, int nrhs, T* x, int64_t ldx,
+    const SolvePlan<T>& sp, DeviceStatus* st, const DeviceStatus* gate, cudaStream_t s)
+{
+    const size_t perm_smem = perm_smem_bytes(n);
+    const int    use_smem  = perm_smem > 0 ? 1 : 0;
+    prof_begin(KC_SOLVE, s);
+    k_perm_from_pivots<0><<<1, 256, perm_smem, s>>>(pivot, n, sp.perm, use_smem, st, gate);
+    prof_end(KC_SOLVE, s);
+    B200LA_LAUNCH_CHECK();
+    const int64_t total = (int64_t)n * nrhs;
+    prof_begin(KC_SOLVE, s);
+    k_gather_rows<T><<<grid_1d(total, 256), 256, 0, s>>>(x, ldx, sp.perm, sp.y, nrhs, n, nrhs, gate);
+    prof_end(KC_SOLVE, s);
+    B200LA_LAUNCH_CHECK();
+    int rc = enqueue_trsm_inplace<T>(false, false, true, n, nrhs, lu, n, sp.y, nrhs, gate, s);
+    if (rc != B200LA_SUCCESS)
+    {
+        return rc;
+    }
+    rc = enqueue_trsm_inplace<T>(true, false, false, n, nrhs, lu, n, sp.y, nrhs, gate, s);
+    if (rc != B200LA_SUCCESS)
+    {
+        return rc;
+    }
+    prof_begin(KC_SOLVE, s);
+    k_copy2d<T><<<grid_1d(total, 256), 256, 0, s>>>(sp.y, nrhs, x, ldx, n, nrhs, gate);
+    prof_end(KC_SOLVE, s);
+    B200LA_LAUNCH_CHECK();
+    return B200LA_SUCCESS;
+}
+
+template <typename T> size_t gesv_ws_size(int64_t n, int mode)
+{
+    if (n <= 0 || (mode != B200LA_LU_LINEAR_SOLVER && mode != B200LA_LU_UPFRONT_LINEAR_SOLVER))
+    {
+        return 0;
+    }
+    Arena a;
+    plan_getrf<T>(a);
+    plan_solve<T>(a, n, 1);
+    return a.size();
+}
+
+template <typename T>
+int gesv(T* m, int64_t* pivot, int64_t n, T* x, int mode, void* ws, size_t bytes, void* stream)
+{
+    if (m == nullptr || x == nullptr)
+    {
+        return set_error(B200LA_INVALID_ARGUMENT, "linear_solver::apply: m and x must not be null");
+    }
+    if (n <= 0)
+    {
+        return set_error(B200LA_INVALID_ARGUMENT, "linear_solver::apply: lda must be positive");
+    }
+    if (mode != B200LA_LU_LINEAR_SOLVER && mode != B200LA_LU_UPFRONT_LINEAR_SOLVER)
+    {
+        return set_error(B200LA_NOT_SUPPORTED,
+            "linear_solver: only the LU modes are provided by this backend (mode %d)", mode);
+    }
+    if (pivot == nullptr)
+    {
+        return set_error(B200LA_INVALID_ARGUMENT, "linear_solver: LU modes need a pivot array");
+    }
+    if (n > INT_MAX / 2)
+    {
+        return set_error(B200LA_NOT_SUPPORTED, "linear_solver: order too large");
+    }
+    const size_t need = gesv_ws_size<T>(n, mode);
+    if (ws == nullptr || bytes < need)
+    {
+        return set_error(B200LA_WORKSPACE_TOO_SMALL,
+            "linear_solver: workspace is null or too small (%zu < %zu bytes)", bytes, need);
+    }
+    int st = prepare<T>();
+    if (st != B200LA_SUCCESS)
+    {
+        return st;
+    }
+    Arena         a(ws, bytes);
+    GetrfPlan<T>  gp = plan_getrf<T>(a);
+    SolvePlan<T>  sp = plan_solve<T>(a, n, 1);
+    cudaStream_t  s  = as_stream(stream);
+    if (mode == B200LA_LU_LINEAR_SOLVER)
+    {
+        st = enqueue_getrf<T>(m, (int)n, pivot, gp, s);
+    }
+    else
+    {
+        prof_begin(KC_SOLVE, s);
+        k_status_init<<<1, 32, 0, s>>>(gp.st, gp.perm);
+        prof_end(KC_SOLVE, s);
+        B200LA_LAUNCH_CHECK();
+        st = B200LA_SUCCESS;
+    }
+    if (st != B200LA_SUCCESS)
+    {
+        return st;
+    }
+    return enqueue_getrs<T>(m, pivot, (int)n, 1, x, 1, sp, gp.st, gp.st, s);
+}
+
+template <typename T> size_t getrs_ws_size(int64_t n, int64_t nrhs)
+{
+    if (n <= 0 || nrhs <= 0)
+    {
+        return 0;
+    }
+    Arena a;
+    plan_getrf<T>(a);
+    plan_solve<T>(a, n, nrhs);
+    return a.size();
+}
+
+template <typename T>
+int getrs(const T* lu, const int64_t* pivot, int64_t n, int64_t nrhs, T* x, int64_t ldx, void* ws,
+    size_t bytes, void* stream)
+{
+    if (lu == nullptr || pivot == nullptr || x == nullptr)
+    {
+        return set_error(B200LA_INVALID_ARGUMENT, "getrs: null pointer");
+    }
+    if (n <= 0 || nrhs <= 0 || ldx < nrhs || n > INT_MAX / 2 || nrhs > INT_MAX / 2)
+    {
+        return set_error(B200LA_INVALID_ARGUMENT, "getrs: invalid sizes");
+    }
+    const size_t need = getrs_ws_size<T>(n, nrhs);
+    if (ws == nullptr || bytes < need)
+    {
+        return set_error(B200LA_WORKSPACE_TOO_SMALL, "getrs: workspace too small (%zu < %zu)", bytes, need);
+    }
+    int st = prepare<T>();
+    if (st != B200LA_SUCCESS)
+    {
+        return st;
+    }
+    Arena        a(ws, bytes);
+    GetrfPlan<T> gp = plan_getrf<T>(a);
+    SolvePlan<T> sp = plan_solve<T>(a, n, nrhs);
+    cudaStream_t s  = as_stream(stream);
+    prof_begin(KC_SOLVE, s);
+    k_status_init<<<1, 32, 0, s>>>(gp.st, gp.perm);
+    prof_end(KC_SOLVE, s);
+    B200LA_LAUNCH_CHECK();
+    return enqueue_getrs<T>(lu, pivot, (int)n, (int)nrhs, x, ldx, sp, gp.st, gp.st, s);
+}
+
+// ---------------------------------------------------------------------------
+// triangular_solver
+// ---------------------------------------------------------------------------
+template <typename T>
+int check_trsm(int64_t n, int64_t nrhs, const T* a, int64_t lda, const T* b, int64_t ldb, const T* x,
+    int64_t ldx)
+{
+    if (n <= 0 || nrhs <= 0)
+    {
+        return set_error(B200LA_INVALID_ARGUMENT, "triangular_solver: dimensions must be positive");
+    }
+    if (n > INT_MAX || nrhs > INT_MAX)
+    {
+        return set_error(B200LA_INVALID_ARGUMENT, "checked_narrow: value does not fit in target type");
+    }
+    if (!a || !b || !x)
+    {
+        return set_error(B200LA_INVALID_ARGUMENT, "triangular_solver: matrices must not be null");
+    }
+    if ((const void*)a == (const void*)b || (const void*)a == (const void*)x ||
+        (const void*)b == (const void*)x)
+    {
+        return set_error(B200LA_INVALID_ARGUMENT, "triangular_solver: matrices must use distinct buffers");
+    }
+    if (lda < n || ldb < nrhs || ldx < nrhs)
+    {
+        return set_error(B200LA_INVALID_ARGUMENT, "triangular_solver: invalid row stride");
+    }
+    const int64_t limit = INT64_MAX / n;
+    if (lda > limit || ldb > limit || ldx > limit)
+    {
+        return set_error(B200LA_INVALID_ARGUMENT,
+            "triangular_solver: row stride span exceeds supported range");
+    }
+    return B200LA_SUCCESS;
+}
+
+template <typename T>
+int trsm(int upper, int transpose, int unit, int64_t n, int64_t nrhs, const T* a, int64_t lda,
+    const T* b, int64_t ldb, T* x, int64_t ldx, void* ws, size_t bytes, void* stream)
+{
+    int st = check_trsm<T>(n, nrhs, a, lda, b, ldb, x, ldx);
+    if (st != B200LA_SUCCESS)
+    {
+        return st;
+    }
+    (void)ws;
+    (void)bytes;
+    st = prepare<T>();
+    if (st != B200LA_SUCCESS)
+    {
+        return st;
+    }
+    cudaStream_t  s     = as_stream(stream);
+    const int64_t total = n * nrhs;
+    prof_begin(KC_SOLVE, s);
+    k_copy2d<T><<<grid_1d(total, 256), 256, 0, s>>>(b, ldb, x, ldx, (int)n, (int)nrhs, nullptr);
+    prof_end(KC_SOLVE, s);
+    B200LA_LAUNCH_CHECK();
+    return enqueue_trsm_inplace<T>(upper != 0, transpose != 0, unit != 0, (int)n, (int)nrhs, a, lda, x,
+        ldx, nullptr, s);
+}
+
+// ---------------------------------------------------------------------------
+// multiplication
+// ---------------------------------------------------------------------------
+template <typename T>
+int gemm(int ta, int tb, int64_t rows, int64_t cols, int64_t depth, T alpha, const T* a, int64_t lda,
+    const T* b, int64_t ldb, T beta, T* c, int64_t ldc, void* stream)
+{
+    if (!a || !b || !c)
+    {
+        return set_error(B200LA_INVALID_ARGUMENT, "multiplication::apply: a, b, and c must not be null");
+    }
+    if (rows <= 0 || cols <= 0 || depth <= 0 || lda <= 0 || ldb <= 0 || ldc <= 0)
+    {
+        return set_error(B200LA_INVALID_ARGUMENT,
+            "multiplication::apply: rows/columns/depth/lda/ldb/ldc must be positive");
+    }
+    if (rows > INT_MAX / 2 || cols > INT_MAX / 2 || depth > INT_MAX / 2)
+    {
+        return set_error(B200LA_NOT_SUPPORTED, "multiplication: dimension too large");
+    }
+    int st = prepare<T>();
+    if (st != B200LA_SUCCESS)
+    {
+        return st;
+    }
+    cudaStream_t s = as_stream(stream);
+    if (alpha == T(0))
+    {
+        if (beta != T(1))
+        {
+            prof_begin(KC_GEMM, s);
+            k_scale2d<T><<<grid_1d(rows * cols, 256), 256, 0, s>>>(c, ldc, (int)rows, (int)cols, beta);
+            prof_end(KC_GEMM, s);
+            B200LA_LAUNCH_CHECK();
+        }
+        return B200LA_SUCCESS;
+    }
+    dim3         grid((unsigned)((cols + 63) / 64), (unsigned)((rows + 127) / 128));
+    const size_t smem = gemm_smem_bytes<T>();
+    const int    r = (int)rows, co = (int)cols, d = (int)depth;
+    prof_begin(KC_GEMM, s);
+    if (!ta && !tb)
+        k_gemm<T, false, false><<<grid, 128, smem, s>>>(r, co, d, alpha, a, lda, b, ldb, beta, c, ldc);
+    else if (ta && !tb)
+        k_gemm<T, true, false><<<grid, 128, smem, s>>>(r, co, d, alpha, a, lda, b, ldb, beta, c, ldc);
+    else if (!ta && tb)
+        k_gemm<T, false, true><<<grid, 128, smem, s>>>(r, co, d, alpha, a, lda, b, ldb, beta, c, ldc);
+    else
+        k_gemm<T, true, true><<<grid, 128, smem, s>>>(r, co, d, alpha, a, lda, b, ldb, beta, c, ldc);
+    prof_end(KC_GEMM, s);
+    B200LA_LAUNCH_CHECK();
+    return B200LA_SUCCESS;
+}
+
+}  // namespace b200la

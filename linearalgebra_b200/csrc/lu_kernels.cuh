@@ -184,7 +184,7 @@ template <typename T> __device__ __forceinline__ double pivot_key(T v, int gr, i
 
 // The interchanges of one panel (pivot rows piv_loc[0..w), 0-based) as one
 // permutation of the rows they touch (PermList).  Run by one warp.
-__device__ __noinline__ void build_perm_list(const int* piv_loc, int k, int w, PermList* perm, int lane)
+static __device__ __noinline__ void build_perm_list(const int* piv_loc, int k, int w, PermList* perm, int lane)
 {
     __shared__ int pos_s[2 * kNB];
     __shared__ int cont_s[2 * kNB];
@@ -824,7 +824,7 @@ template <typename T> constexpr size_t laswp_smem_bytes()
 
 template <typename T>
 __global__ void __launch_bounds__(kSwapThreads) k_laswp_trsm(T* __restrict__ A, int n, int k, int w,
-    const PermList* __restrict__ perm, int n_left)
+    const PermList* __restrict__ perm, int n_left, int u12_end)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T(*staged)[kSwapCols] = reinterpret_cast<T(*)[kSwapCols]>(smem_raw);  // [2*kNB]
@@ -833,9 +833,12 @@ __global__ void __launch_bounds__(kSwapThreads) k_laswp_trsm(T* __restrict__ A, 
     const int  tid   = threadIdx.x;
     const int  cl    = tid % kSwapCols;
     const int  rg    = tid / kSwapCols;
-    const bool left  = (int)blockIdx.x < n_left;
-    const int  c0    = left ? blockIdx.x * kSwapCols : k + w + (blockIdx.x - n_left) * kSwapCols;
-    const int  cend  = left ? k : n;
+    const int  c0    = (int)blockIdx.x < n_left ? blockIdx.x * kSwapCols
+                                                : k + w + (blockIdx.x - n_left) * kSwapCols;
+    // `left`: only the interchanges (columns left of the panel, or right of
+    // it at or beyond u12_end, whose U12 rows are solved later)
+    const bool left  = (int)blockIdx.x < n_left || c0 >= u12_end;
+    const int  cend  = (int)blockIdx.x < n_left ? k : n;
     const int  col   = c0 + cl;
     const bool valid = col < cend;
     const int  cnt   = perm->count;
@@ -988,7 +991,7 @@ template <typename T> constexpr size_t trailing_smem_bytes()
 
 template <typename T>
 __device__ __forceinline__ void trailing_issue_tile(T* Bs, T* Cs, const T* U12, const T* C, int n,
-    int w, int rest, int m0, int nt0, bool vec16)
+    int w, int rest, int ncols, int m0, int nt0, bool vec16)
 {
     constexpr int CE = chunk_elems<T>();
     constexpr int BC = kTileNc / CE;  // chunks per tile row
@@ -997,7 +1000,7 @@ __device__ __forceinline__ void trailing_issue_tile(T* Bs, T* Cs, const T* U12, 
     {
         const int  p = e / BC, q = e - (e / BC) * BC;
         const int  col = nt0 + q * CE;
-        const bool v   = p < w && col < rest;
+        const bool v   = p < w && col < ncols;
         cp_async_chunk(Bs + p * kTileNc + q * CE, v ? U12 + (size_t)p * n + col : U12, v, vec16);
     }
     // A22 tile: 128 x 32
@@ -1005,13 +1008,13 @@ __device__ __forceinline__ void trailing_issue_tile(T* Bs, T* Cs, const T* U12, 
     {
         const int  r = e / BC, q = e - (e / BC) * BC;
         const int  col = nt0 + q * CE;
-        const bool v   = m0 + r < rest && col < rest;
+        const bool v   = m0 + r < rest && col < ncols;
         cp_async_chunk(Cs + r * kTileNc + q * CE, v ? C + (size_t)(m0 + r) * n + col : C, v, vec16);
     }
 }
 
 template <typename T>
-__global__ void __launch_bounds__(128, 1) k_trailing(T* __restrict__ A, int n, int k, int w)
+__global__ void __launch_bounds__(128, 1) k_trailing(T* __restrict__ A, int n, int k, int w, int ncols)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     constexpr int CE = chunk_elems<T>();
@@ -1019,7 +1022,7 @@ __global__ void __launch_bounds__(128, 1) k_trailing(T* __restrict__ A, int n, i
     T*            Bs = As + kBandM * kNB;                          // [2][kNB][kTileNc]
     T*            Cs = Bs + 2 * kNB * kTileNc;                     // [2][kBandM][kTileNc]
 
-    const int rest = n - k - w;
+    const int rest = n - k - w;  // rows of A22; its columns are [0, ncols)
     const int m0   = blockIdx.y * kBandM;
     const int n0   = blockIdx.x * kChunkN;
     const int tid  = threadIdx.x;
@@ -1044,12 +1047,12 @@ __global__ void __launch_bounds__(128, 1) k_trailing(T* __restrict__ A, int n, i
                 v ? L21 + (size_t)(m0 + r) * n + q * CE : L21, v, vec16);
         }
     }
-    const int ntiles = min(kChunkN, rest - n0) > 0 ? (min(kChunkN, rest - n0) + kTileNc - 1) / kTileNc : 0;
-    trailing_issue_tile(Bs, Cs, U12, C, n, w, rest, m0, n0, vec16);
+    const int ntiles = min(kChunkN, ncols - n0) > 0 ? (min(kChunkN, ncols - n0) + kTileNc - 1) / kTileNc : 0;
+    trailing_issue_tile(Bs, Cs, U12, C, n, w, rest, ncols, m0, n0, vec16);
     cp_async_commit();
     if (ntiles > 1)
     {
-        trailing_issue_tile(Bs + kNB * kTileNc, Cs + kBandM * kTileNc, U12, C, n, w, rest, m0,
+        trailing_issue_tile(Bs + kNB * kTileNc, Cs + kBandM * kTileNc, U12, C, n, w, rest, ncols, m0,
             n0 + kTileNc, vec16);
     }
     cp_async_commit();
@@ -1115,11 +1118,11 @@ __global__ void __launch_bounds__(128, 1) k_trailing(T* __restrict__ A, int n, i
                 {
                     const int cl = 2 * tc + 16 * j;
                     const auto v2 = *reinterpret_cast<const typename Vec2<T>::type*>(Ct + rl * kTileNc + cl);
-                    if (nt0 + cl < rest)
+                    if (nt0 + cl < ncols)
                     {
                         crow[nt0 + cl] = v2.x - acc[i][2 * j];
                     }
-                    if (nt0 + cl + 1 < rest)
+                    if (nt0 + cl + 1 < ncols)
                     {
                         crow[nt0 + cl + 1] = v2.y - acc[i][2 * j + 1];
                     }
@@ -1130,14 +1133,14 @@ __global__ void __launch_bounds__(128, 1) k_trailing(T* __restrict__ A, int n, i
         if (t + 2 < ntiles)
         {
             trailing_issue_tile(Bs + (t & 1) * kNB * kTileNc, Cs + (t & 1) * kBandM * kTileNc, U12, C,
-                n, w, rest, m0, n0 + (t + 2) * kTileNc, vec16);
+                n, w, rest, ncols, m0, n0 + (t + 2) * kTileNc, vec16);
         }
         cp_async_commit();
     }
     cp_async_wait<0>();
 }
 
-__global__ void k_status_init(DeviceStatus* st, PermList* perm)
+static __global__ void k_status_init(DeviceStatus* st, PermList* perm)
 {
     if (threadIdx.x == 0)
     {
@@ -1149,7 +1152,7 @@ __global__ void k_status_init(DeviceStatus* st, PermList* perm)
     }
 }
 
-__global__ void k_status_finish(DeviceStatus* st)
+static __global__ void k_status_finish(DeviceStatus* st)
 {
     if (threadIdx.x == 0)
     {

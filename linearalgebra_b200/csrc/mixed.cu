@@ -1,0 +1,912 @@
+// Mixed-precision LU solve with FP64 iterative refinement (LU-IR) and
+// GMRES-IR, on the B200 tensor cores.
+//
+//   1. A (FP64) -> A32 (FP32 copy), ||A||_inf on the way.
+//   2. Blocked LU with partial pivoting of A32 in 256-column outer blocks:
+//      inside a block, 64-column panels (the FP32 panel kernels), their row
+//      interchanges, and in-block updates (SIMT FP32); then the block's
+//      U12 = L11^-1 A12 (FP32, k_outer_u12), the operand copies of L21 and
+//      U12^T in the factorization precision, and the trailing update
+//      A22 -= L21 U12 on tcgen05 with FP32 accumulation (k_tc_update).
+//      Precisions: FP32 (three-term TF32 split), TF32, BF16, FP16.
+//   3. x0 = U^-1 L^-1 P b with the FP32 factors applied in FP64; then
+//      r = b - A x in FP64, eta = ||r|| / (||A|| ||x|| + ||b||) (inf norms),
+//      stop at eta <= tolerance; else d = U^-1 L^-1 P r, x += d.  When plain
+//      refinement stalls, GMRES-IR: restarted GMRES in FP64 on A d = r, left
+//      preconditioned by the low-precision factors (Carson & Higham, SISC
+//      40(2), 2018).  If that fails too, the next precision up is tried, down
+//      to plain FP64 LU.
+// FP64 stays on the GPU for the residual, the update and the test.
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "lu_driver.cuh"
+#include "tc_api.cuh"
+#include "trsv.cuh"
+
+namespace b200la
+{
+namespace
+{
+constexpr int kOuterNB = 256;
+
+// ---------------------------------------------------------------------------
+// kernels
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void atomic_max_nonneg(unsigned long long* p, double v)
+{
+    atomicMax(p, (unsigned long long)__double_as_longlong(v));
+}
+
+// A32 = (float)A, and ||A||_inf = max row sum of |A|.  A warp per row.
+__global__ void k_convert_a(const double* __restrict__ a, int64_t lda, float* __restrict__ a32, int n,
+    unsigned long long* anorm)
+{
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (warp >= n)
+    {
+        return;
+    }
+    const double* row = a + (int64_t)warp * lda;
+    float*        out = a32 + (int64_t)warp * n;
+    double        s   = 0.0;
+    for (int j = lane; j < n; j += 32)
+    {
+        const double v = row[j];
+        out[j]         = (float)v;
+        s += fabs(v);
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1)
+    {
+        s += __shfl_down_sync(0xffffffffu, s, off);
+    }
+    if (lane == 0)
+    {
+        atomic_max_nonneg(anorm, s);
+    }
+}
+
+__device__ __forceinline__ float tf32_trunc(float x) { return __uint_as_float(__float_as_uint(x) & ~0x1FFFu); }
+
+template <int KIND> struct OpStore;
+template <> struct OpStore<TC_TF32>
+{
+    using type = float;
+    __device__ static float conv(float x) { return x; }
+};
+template <> struct OpStore<TC_BF16>
+{
+    using type = __nv_bfloat16;
+    __device__ static __nv_bfloat16 conv(float x) { return __float2bfloat16_rn(x); }
+};
+template <> struct OpStore<TC_FP16>
+{
+    using type = __half;
+    __device__ static __half conv(float x) { return __float2half_rn(x); }
+};
+
+// L21 operand: rows [r_begin, n) x columns [K, K+256) of A32 -> K-major copy.
+template <int KIND, bool SPLIT>
+__global__ void k_make_l21(const float* __restrict__ a32, int n, int K, int r_begin,
+    typename OpStore<KIND>::type* __restrict__ op, float* __restrict__ op_small)
+{
+    const int64_t total = (int64_t)(n - r_begin) * kOuterNB;
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x)
+    {
+        const int64_t r  = e / kOuterNB;
+        const int     kk = (int)(e - r * kOuterNB);
+        const float   v  = a32[(r_begin + r) * (int64_t)n + K + kk];
+        op[e]            = OpStore<KIND>::conv(v);
+        if constexpr (SPLIT)
+        {
+            op_small[e] = v - tf32_trunc(v);
+        }
+    }
+}
+
+// U12 = L11^-1 A12 for the outer block rows [K, K+256), columns [K+256, n)
+// (strips of 64 columns), written back in FP32 and as the transposed operand
+// copy U12^T (rows = columns of A22, K-major).
+constexpr int kOuStrip = 64;
+template <int KIND, bool SPLIT>
+__global__ void __launch_bounds__(256) k_outer_u12(float* __restrict__ a32, int n, int K,
+    typename OpStore<KIND>::type* __restrict__ opT, float* __restrict__ opT_small)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    float(*S)[kOuStrip + 1]  = reinterpret_cast<float(*)[kOuStrip + 1]>(smem_raw);  // [256]
+    float(*Lb)[kNB + 1]      = reinterpret_cast<float(*)[kNB + 1]>(smem_raw + sizeof(float) * kOuterNB * (kOuStrip + 1));
+    const int tid = threadIdx.x;
+    const int cl  = tid % kOuStrip;
+    const int rg  = tid / kOuStrip;  // 4 row groups
+    const int Kend = K + kOuterNB;
+    const int c0  = Kend + blockIdx.x * kOuStrip;
+    const int col = c0 + cl;
+    const bool valid = col < n;
+
+    for (int i = rg; i < kOuterNB; i += 4)
+    {
+        S[i][cl] = valid ? a32[(int64_t)(K + i) * n + col] : 0.f;
+    }
+    for (int jb = 0; jb < kOuterNB / kNB; ++jb)
+    {
+        __syncthreads();
+        for (int e = tid; e < kNB * kNB; e += 256)
+        {
+            const int i = e / kNB, p = e % kNB;
+            Lb[i][p]    = p < i ? a32[(int64_t)(K + jb * kNB + i) * n + K + jb * kNB + p] : 0.f;
+        }
+        // unit-lower diagonal block, column-oriented substitution
+        for (int p = 0; p + 1 < kNB; ++p)
+        {
+            __syncthreads();
+            const float xp = S[jb * kNB + p][cl];
+            for (int i = p + 1 + rg; i < kNB; i += 4)
+            {
+                S[jb * kNB + i][cl] = fmaf(-Lb[i][p], xp, S[jb * kNB + i][cl]);
+            }
+        }
+        for (int jb2 = jb + 1; jb2 < kOuterNB / kNB; ++jb2)
+        {
+            __syncthreads();
+            for (int e = tid; e < kNB * kNB; e += 256)
+            {
+                const int i = e / kNB, p = e % kNB;
+                Lb[i][p]    = a32[(int64_t)(K + jb2 * kNB + i) * n + K + jb * kNB + p];
+            }
+            __syncthreads();
+            for (int i = rg; i < kNB; i += 4)
+            {
+                float acc = 0.f;
+#pragma unroll 8
+                for (int p = 0; p < kNB; ++p)
+                {
+                    acc = fmaf(Lb[i][p], S[jb * kNB + p][cl], acc);
+                }
+                S[jb2 * kNB + i][cl] -= acc;
+            }
+        }
+    }
+    __syncthreads();
+    for (int i = rg; i < kOuterNB; i += 4)
+    {
+        if (valid)
+        {
+            a32[(int64_t)(K + i) * n + col] = S[i][cl];
+        }
+    }
+    // transposed operand copy: row (col - Kend), K index kk
+    for (int e = tid; e < kOuStrip * kOuterNB; e += 256)
+    {
+        const int c  = e / kOuterNB;
+        const int kk = e % kOuterNB;
+        if (c0 + c < n)
+        {
+            const float   v   = S[kk][c];
+            const int64_t idx = (int64_t)(c0 + c - Kend) * kOuterNB + kk;
+            opT[idx]          = OpStore<KIND>::conv(v);
+            if constexpr (SPLIT)
+            {
+                opT_small[idx] = v - tf32_trunc(v);
+            }
+        }
+    }
+}
+
+constexpr size_t outer_u12_smem() { return sizeof(float) * ((size_t)kOuterNB * (kOuStrip + 1) + kNB * (kNB + 1)); }
+
+// r = b - A x (one right-hand side), FP64; b == nullptr means b = 0.  A CTA
+// handles 32 rows; x is staged through shared memory in chunks.  Also max|r|
+// (atomic).
+constexpr int kResRows  = 32;
+constexpr int kResChunk = 2048;
+__global__ void __launch_bounds__(256) k_residual(const double* __restrict__ a, int64_t lda,
+    const double* __restrict__ x, const double* __restrict__ b, double* __restrict__ r, int n,
+    unsigned long long* rmax)
+{
+    __shared__ double xs[kResChunk];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int row0 = blockIdx.x * kResRows + warp * 4;
+    double    acc[4] = {0, 0, 0, 0};
+    for (int c0 = 0; c0 < n; c0 += kResChunk)
+    {
+        const int cw = min(kResChunk, n - c0);
+        __syncthreads();
+        for (int j = threadIdx.x; j < cw; j += 256)
+        {
+            xs[j] = x[c0 + j];
+        }
+        __syncthreads();
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+        {
+            const int row = row0 + q;
+            if (row < n)
+            {
+                const double* ar = a + (int64_t)row * lda + c0;
+                double        s  = 0.0;
+                for (int j = lane; j < cw; j += 32)
+                {
+                    s = fma(ar[j], xs[j], s);
+                }
+                acc[q] += s;
+            }
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+    {
+        double s = acc[q];
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1)
+        {
+            s += __shfl_down_sync(0xffffffffu, s, off);
+        }
+        const int row = row0 + q;
+        if (lane == 0 && row < n)
+        {
+            const double v = (b != nullptr ? b[row] : 0.0) - s;
+            r[row]         = v;
+            atomic_max_nonneg(rmax, fabs(v));
+        }
+    }
+}
+
+// Per-column max |v| of an n x m row-major block (ld), into out[m].
+__global__ void k_colmax(const double* __restrict__ v, int64_t ld, int n, int m, unsigned long long* out)
+{
+    const int64_t total = (int64_t)n * m;
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x)
+    {
+        const int64_t r = e / m;
+        const int     c = (int)(e - r * m);
+        atomic_max_nonneg(out + c, fabs(v[r * ld + c]));
+    }
+}
+
+// x += d (n x m, row strides ldx / ldd)
+__global__ void k_axpy2d(double* __restrict__ x, int64_t ldx, const double* __restrict__ d, int64_t ldd, int n, int m)
+{
+    const int64_t total = (int64_t)n * m;
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x)
+    {
+        const int64_t r = e / m;
+        const int     c = (int)(e - r * m);
+        x[r * ldx + c] += d[r * ldd + c];
+    }
+}
+
+// ---- GMRES helpers (one right-hand side) ----------------------------------
+// h[i] += sum_r V[i][r] w[r] for i < m (V: m vectors of n, contiguous)
+__global__ void k_dots(const double* __restrict__ V, const double* __restrict__ w, int n, int m, double* h)
+{
+    const int i = blockIdx.y;
+    double    s = 0.0;
+    for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < n; r += (int64_t)gridDim.x * blockDim.x)
+    {
+        s = fma(V[(int64_t)i * n + r], w[r], s);
+    }
+    __shared__ double red[8];
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1)
+    {
+        s += __shfl_down_sync(0xffffffffu, s, off);
+    }
+    if ((threadIdx.x & 31) == 0)
+    {
+        red[threadIdx.x >> 5] = s;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0)
+    {
+        double t = 0;
+        for (int q = 0; q < (int)(blockDim.x >> 5); ++q)
+        {
+            t += red[q];
+        }
+        atomicAdd(h + i, t);
+    }
+}
+
+// w[r] -= sum_{i<m} h[i] V[i][r]   (or, with sign +1 and w = 0, w = V h)
+__global__ void k_comb(const double* __restrict__ V, const double* __restrict__ h, int n, int m, double sign,
+    double* __restrict__ w)
+{
+    for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < n; r += (int64_t)gridDim.x * blockDim.x)
+    {
+        double s = 0.0;
+        for (int i = 0; i < m; ++i)
+        {
+            s = fma(h[i], V[(int64_t)i * n + r], s);
+        }
+        w[r] += sign * s;
+    }
+}
+
+__global__ void k_scale_copy(const double* __restrict__ src, double alpha, double* __restrict__ dst, int n)
+{
+    for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < n; r += (int64_t)gridDim.x * blockDim.x)
+    {
+        dst[r] = alpha * src[r];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// host
+// ---------------------------------------------------------------------------
+inline int grid_for(int64_t total, int threads = 256)
+{
+    int64_t g = (total + threads - 1) / threads;
+    if (g < 1)
+        g = 1;
+    if (g > 148 * 8)
+        g = 148 * 8;
+    return (int)g;
+}
+
+struct MixedPlan
+{
+    GetrfPlan<float>   gp;
+    float*             a32;
+    int64_t*           piv;
+    void*              l21op;
+    float*             l21small;
+    void*              u12op;
+    float*             u12small;
+    int32_t*           perm;
+    double*            r;       // n x nrhs residual / correction
+    double*            y;       // n x nrhs scratch for the solves
+    unsigned long long* norms;  // [0] ||A||, [1..] per-column maxima (3 x 64)
+    TrsvSync*          tsync;
+    double*            V;       // GMRES basis (m+1) x n
+    double*            h;       // GMRES dot products (m+1)
+    double*            a64;     // FP64 copy of A for the FP64 fallback
+    GetrfPlan<double>  gp64;
+    int64_t*           piv64;
+};
+
+constexpr int kMaxNrhsMixed = 64;
+constexpr int kGmresMaxRestart = 50;
+
+MixedPlan plan_mixed(Arena& a, int64_t n, int64_t nrhs, int restart, bool fp64_fallback)
+{
+    MixedPlan p{};
+    p.gp       = plan_getrf<float>(a);
+    p.a32      = a.next<float>((size_t)n * n);
+    p.piv      = a.next<int64_t>((size_t)n);
+    p.l21op    = a.next<float>((size_t)n * kOuterNB);
+    p.l21small = a.next<float>((size_t)n * kOuterNB);
+    p.u12op    = a.next<float>((size_t)n * kOuterNB);
+    p.u12small = a.next<float>((size_t)n * kOuterNB);
+    p.perm     = a.next<int32_t>((size_t)n);
+    p.r        = a.next<double>((size_t)n * nrhs);
+    p.y        = a.next<double>((size_t)n * nrhs);
+    p.norms    = a.next<unsigned long long>(4 + 3 * kMaxNrhsMixed);
+    p.tsync    = reinterpret_cast<TrsvSync*>(a.next<int32_t>(32 + (size_t)(n + kTvRows - 1) / kTvRows + 32));
+    const int m = restart > 0 ? restart : 0;
+    p.V        = a.next<double>((size_t)(m + 1) * n);
+    p.h        = a.next<double>((size_t)m + 2);
+    if (fp64_fallback)
+    {
+        p.a64   = a.next<double>((size_t)n * n);
+        p.gp64  = plan_getrf<double>(a);
+        p.piv64 = a.next<int64_t>((size_t)n);
+    }
+    return p;
+}
+
+// Mixed-precision factorization of p.a32 in place; pivots in p.piv.
+int enqueue_getrf_mixed(MixedPlan& p, int n, int kind, bool split, cudaStream_t s)
+{
+    int rc = clear_panel_exchange<float>(p.gp, s);
+    if (rc != B200LA_SUCCESS)
+        return rc;
+    k_status_init<<<1, 32, 0, s>>>(p.gp.st, p.gp.perm);
+    B200LA_LAUNCH_CHECK();
+    int cl = 0, gmax = 0;
+    if ((rc = panel_config<float>(cl, gmax)) != B200LA_SUCCESS)
+        return rc;
+    CUtensorMap ma, mb, mas, mbs;
+    if ((rc = make_kmajor_map(&ma, p.l21op, kind, n, kOuterNB, kOuterNB)) != B200LA_SUCCESS ||
+        (rc = make_kmajor_map(&mb, p.u12op, kind, n, kOuterNB, kOuterNB)) != B200LA_SUCCESS)
+        return rc;
+    mas = ma;
+    mbs = mb;
+    if (split && ((rc = make_kmajor_map(&mas, p.l21small, TC_TF32, n, kOuterNB, kOuterNB)) != B200LA_SUCCESS ||
+                     (rc = make_kmajor_map(&mbs, p.u12small, TC_TF32, n, kOuterNB, kOuterNB)) != B200LA_SUCCESS))
+        return rc;
+    float* a32 = p.a32;
+    for (int K = 0; K < n; K += kOuterNB)
+    {
+        const int Kend = K + kOuterNB < n ? K + kOuterNB : n;
+        for (int k = K; k < Kend; k += kNB)
+        {
+            const int w = n - k < kNB ? n - k : kNB;
+            if ((rc = launch_panel<float>(a32, n, k, w, p.piv, p.gp, cl, gmax, s)) != B200LA_SUCCESS)
+                return rc;
+            const int rest = n - k - w;
+            const int nl   = (k + kSwapCols - 1) / kSwapCols;
+            const int nr   = (rest + kSwapCols - 1) / kSwapCols;
+            if (nl + nr > 0)
+            {
+                prof_begin(KC_SWAP, s);
+                k_laswp_trsm<float><<<nl + nr, kSwapThreads, laswp_smem_bytes<float>(), s>>>(a32, n, k, w, p.gp.perm, nl, Kend);
+                prof_end(KC_SWAP, s);
+                B200LA_LAUNCH_CHECK();
+            }
+            const int ncols = Kend - (k + w);
+            if (rest > 0 && ncols > 0)
+            {
+                dim3 grid((ncols + kChunkN - 1) / kChunkN, (rest + kBandM - 1) / kBandM);
+                prof_begin(KC_TRAILING, s);
+                k_trailing<float><<<grid, 128, trailing_smem_bytes<float>(), s>>>(a32, n, k, w, ncols);
+                prof_end(KC_TRAILING, s);
+                B200LA_LAUNCH_CHECK();
+            }
+        }
+        const int rest = n - Kend;
+        if (rest <= 0)
+        {
+            continue;
+        }
+        const int64_t elems = (int64_t)rest * kOuterNB;
+        prof_begin(KC_PREP, s);
+        if (kind == TC_TF32 && split)
+        {
+            k_make_l21<TC_TF32, true><<<grid_for(elems), 256, 0, s>>>(a32, n, K, Kend, (float*)p.l21op, p.l21small);
+            k_outer_u12<TC_TF32, true><<<(rest + kOuStrip - 1) / kOuStrip, 256, outer_u12_smem(), s>>>(a32, n, K, (float*)p.u12op, p.u12small);
+        }
+        else if (kind == TC_TF32)
+        {
+            k_make_l21<TC_TF32, false><<<grid_for(elems), 256, 0, s>>>(a32, n, K, Kend, (float*)p.l21op, nullptr);
+            k_outer_u12<TC_TF32, false><<<(rest + kOuStrip - 1) / kOuStrip, 256, outer_u12_smem(), s>>>(a32, n, K, (float*)p.u12op, nullptr);
+        }
+        else if (kind == TC_BF16)
+        {
+            k_make_l21<TC_BF16, false><<<grid_for(elems), 256, 0, s>>>(a32, n, K, Kend, (__nv_bfloat16*)p.l21op, nullptr);
+            k_outer_u12<TC_BF16, false><<<(rest + kOuStrip - 1) / kOuStrip, 256, outer_u12_smem(), s>>>(a32, n, K, (__nv_bfloat16*)p.u12op, nullptr);
+        }
+        else
+        {
+            k_make_l21<TC_FP16, false><<<grid_for(elems), 256, 0, s>>>(a32, n, K, Kend, (__half*)p.l21op, nullptr);
+            k_outer_u12<TC_FP16, false><<<(rest + kOuStrip - 1) / kOuStrip, 256, outer_u12_smem(), s>>>(a32, n, K, (__half*)p.u12op, nullptr);
+        }
+        prof_end(KC_PREP, s);
+        B200LA_LAUNCH_CHECK();
+        if ((rc = enqueue_tc_update(kind, split, ma, mb, mas, mbs, a32 + (int64_t)Kend * n + Kend, n, rest, rest,
+                 kOuterNB, p.gp.st, s)) != B200LA_SUCCESS)
+            return rc;
+    }
+    k_status_finish<<<1, 32, 0, s>>>(p.gp.st);
+    B200LA_LAUNCH_CHECK();
+    return B200LA_SUCCESS;
+}
+
+int set_mixed_attributes()
+{
+    static std::mutex m;
+    static bool       done[64] = {};
+    int               dev      = 0;
+    B200LA_CUDA(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lock(m);
+    if (dev >= 0 && dev < 64 && done[dev])
+        return B200LA_SUCCESS;
+    B200LA_CUDA(cudaFuncSetAttribute(k_outer_u12<TC_TF32, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)outer_u12_smem()));
+    B200LA_CUDA(cudaFuncSetAttribute(k_outer_u12<TC_TF32, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)outer_u12_smem()));
+    B200LA_CUDA(cudaFuncSetAttribute(k_outer_u12<TC_BF16, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)outer_u12_smem()));
+    B200LA_CUDA(cudaFuncSetAttribute(k_outer_u12<TC_FP16, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)outer_u12_smem()));
+    if (dev >= 0 && dev < 64)
+        done[dev] = true;
+    return B200LA_SUCCESS;
+}
+
+// v (n x nrhs, row stride ldv) <- U^-1 L^-1 P v with the factors `lu`
+// (float or double) applied in FP64.  Uses p.y as scratch.
+template <typename TA>
+int enqueue_lu_apply(const TA* lu, const int32_t* perm, int n, int nrhs, double* v, int64_t ldv, MixedPlan& p,
+    DeviceStatus* st, cudaStream_t s)
+{
+    const int64_t total = (int64_t)n * nrhs;
+    prof_begin(KC_SOLVE, s);
+    k_gather_rows<double><<<grid_for(total), 256, 0, s>>>(v, ldv, perm, p.y, nrhs, n, nrhs, nullptr);
+    prof_end(KC_SOLVE, s);
+    B200LA_LAUNCH_CHECK();
+    if (nrhs == 1)
+    {
+        const int nb = (n + kTvRows - 1) / kTvRows;
+        for (int pass = 0; pass < 2; ++pass)
+        {
+            B200LA_CUDA(cudaMemsetAsync(p.tsync, 0, sizeof(int32_t) * (32 + nb), s));
+            prof_begin(KC_SOLVE, s);
+            k_trsv_syncfree<TA, double><<<nb, kTvThreads, 0, s>>>(lu, n, p.y, n, pass, pass == 0 ? 1 : 0, p.tsync, st, nullptr);
+            prof_end(KC_SOLVE, s);
+            B200LA_LAUNCH_CHECK();
+        }
+    }
+    else
+    {
+        int rc = enqueue_trsm_inplace<TA, double>(false, false, true, n, nrhs, lu, n, p.y, nrhs, nullptr, s);
+        if (rc != B200LA_SUCCESS)
+            return rc;
+        rc = enqueue_trsm_inplace<TA, double>(true, false, false, n, nrhs, lu, n, p.y, nrhs, nullptr, s);
+        if (rc != B200LA_SUCCESS)
+            return rc;
+    }
+    prof_begin(KC_SOLVE, s);
+    k_copy2d<double><<<grid_for(total), 256, 0, s>>>(p.y, nrhs, v, ldv, n, nrhs, nullptr);
+    prof_end(KC_SOLVE, s);
+    B200LA_LAUNCH_CHECK();
+    return B200LA_SUCCESS;
+}
+
+// r = b - A x and eta_j = ||r_j|| / (||A|| ||x_j|| + ||b_j||); returns max_j eta_j.
+int residual_eta(const double* a, int64_t lda, int n, int nrhs, const double* b, int64_t ldb, const double* x,
+    int64_t ldx, MixedPlan& p, double anorm, const std::vector<double>& bnorm, double* eta, cudaStream_t s)
+{
+    B200LA_CUDA(cudaMemsetAsync(p.norms + 4, 0, sizeof(unsigned long long) * 3 * kMaxNrhsMixed, s));
+    if (nrhs == 1)
+    {
+        prof_begin(KC_RESIDUAL, s);
+        k_residual<<<(n + kResRows - 1) / kResRows, 256, 0, s>>>(a, lda, x, b, p.r, n, p.norms + 4);
+        prof_end(KC_RESIDUAL, s);
+        B200LA_LAUNCH_CHECK();
+        prof_begin(KC_RESIDUAL, s);
+        k_colmax<<<grid_for(n), 256, 0, s>>>(x, ldx, n, 1, p.norms + 4 + kMaxNrhsMixed);
+        prof_end(KC_RESIDUAL, s);
+    }
+    else
+    {
+        // R = B - A X on the FP64 GEMM
+        prof_begin(KC_RESIDUAL, s);
+        k_copy2d<double><<<grid_for((int64_t)n * nrhs), 256, 0, s>>>(b, ldb, p.r, nrhs, n, nrhs, nullptr);
+        prof_end(KC_RESIDUAL, s);
+        dim3 grid((unsigned)((nrhs + 63) / 64), (unsigned)((n + 127) / 128));
+        prof_begin(KC_RESIDUAL, s);
+        k_gemm<double, false, false><<<grid, 128, gemm_smem_bytes<double>(), s>>>(n, nrhs, n, -1.0, a, lda, x, ldx, 1.0, p.r, nrhs);
+        prof_end(KC_RESIDUAL, s);
+        B200LA_LAUNCH_CHECK();
+        prof_begin(KC_RESIDUAL, s);
+        k_colmax<<<grid_for((int64_t)n * nrhs), 256, 0, s>>>(p.r, nrhs, n, nrhs, p.norms + 4);
+        k_colmax<<<grid_for((int64_t)n * nrhs), 256, 0, s>>>(x, ldx, n, nrhs, p.norms + 4 + kMaxNrhsMixed);
+        prof_end(KC_RESIDUAL, s);
+    }
+    B200LA_LAUNCH_CHECK();
+    std::vector<unsigned long long> h(2 * kMaxNrhsMixed);
+    B200LA_CUDA(cudaMemcpyAsync(h.data(), p.norms + 4, sizeof(unsigned long long) * 2 * kMaxNrhsMixed,
+        cudaMemcpyDeviceToHost, s));
+    B200LA_CUDA(cudaStreamSynchronize(s));
+    double worst = 0.0;
+    for (int j = 0; j < nrhs; ++j)
+    {
+        double rn, xn;
+        memcpy(&rn, &h[j], 8);
+        memcpy(&xn, &h[kMaxNrhsMixed + j], 8);
+        const double den = anorm * xn + bnorm[j];
+        const double e   = den > 0 ? rn / den : (rn > 0 ? INFINITY : 0.0);
+        if (!(e <= worst))
+            worst = e;  // NaN propagates
+    }
+    *eta = worst;
+    return B200LA_SUCCESS;
+}
+
+double dot_host(const double* a, const double* b, int n, double* h, cudaStream_t s)
+{
+    cudaMemsetAsync(h, 0, sizeof(double), s);
+    dim3 grid(grid_for(n), 1);
+    k_dots<<<grid, 256, 0, s>>>(a, b, n, 1, h);
+    double v = 0;
+    cudaMemcpyAsync(&v, h, sizeof(double), cudaMemcpyDeviceToHost, s);
+    cudaStreamSynchronize(s);
+    return v;
+}
+
+// One restarted-GMRES solve of A d = r (r in p.r), left preconditioned by the
+// factors; d accumulated into x.  Returns the iterations used.
+template <typename TA>
+int gmres_correction(const double* a, int64_t lda, const TA* lu, int n, int restart, double rtol, double* x,
+    MixedPlan& p, DeviceStatus* st, cudaStream_t s, int* iters)
+{
+    const int m = restart;
+    double*   V = p.V;
+    // z0 = M^-1 r  -> V[0]
+    B200LA_CUDA(cudaMemcpyAsync(V, p.r, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+    int rc = enqueue_lu_apply<TA>(lu, p.perm, n, 1, V, 1, p, st, s);
+    if (rc != B200LA_SUCCESS)
+        return rc;
+    const double beta = std::sqrt(dot_host(V, V, n, p.h, s));
+    if (!(beta > 0) || !std::isfinite(beta))
+    {
+        *iters = 0;
+        return B200LA_SUCCESS;
+    }
+    k_scale_copy<<<grid_for(n), 256, 0, s>>>(V, 1.0 / beta, V, n);
+    std::vector<double> H((size_t)(m + 1) * m, 0.0), cs(m), sn(m), g(m + 1, 0.0);
+    g[0] = beta;
+    int j = 0;
+    for (; j < m; ++j)
+    {
+        double* w = V + (size_t)(j + 1) * n;
+        // w = M^-1 A v_j
+        k_residual<<<(n + kResRows - 1) / kResRows, 256, 0, s>>>(a, lda, V + (size_t)j * n, nullptr, w, n, p.norms + 2);
+        B200LA_LAUNCH_CHECK();
+        rc = enqueue_lu_apply<TA>(lu, p.perm, n, 1, w, 1, p, st, s);
+        if (rc != B200LA_SUCCESS)
+            return rc;
+        // w currently holds -M^-1 A v_j (b = 0); flip sign while orthogonalizing
+        k_scale_copy<<<grid_for(n), 256, 0, s>>>(w, -1.0, w, n);
+        // classical Gram-Schmidt, twice
+        std::vector<double> hcol(j + 1, 0.0);
+        for (int pass = 0; pass < 2; ++pass)
+        {
+            B200LA_CUDA(cudaMemsetAsync(p.h, 0, sizeof(double) * (j + 1), s));
+            k_dots<<<dim3(grid_for(n) / 4 + 1, j + 1), 256, 0, s>>>(V, w, n, j + 1, p.h);
+            k_comb<<<grid_for(n), 256, 0, s>>>(V, p.h, n, j + 1, -1.0, w);
+            std::vector<double> hh(j + 1);
+            B200LA_CUDA(cudaMemcpyAsync(hh.data(), p.h, sizeof(double) * (j + 1), cudaMemcpyDeviceToHost, s));
+            B200LA_CUDA(cudaStreamSynchronize(s));
+            for (int i = 0; i <= j; ++i)
+                hcol[i] += hh[i];
+        }
+        const double hn = std::sqrt(dot_host(w, w, n, p.h, s));
+        for (int i = 0; i <= j; ++i)
+            H[(size_t)i * m + j] = hcol[i];
+        H[(size_t)(j + 1) * m + j] = hn;
+        if (hn > 0)
+            k_scale_copy<<<grid_for(n), 256, 0, s>>>(w, 1.0 / hn, w, n);
+        // Givens rotations on column j
+        for (int i = 0; i < j; ++i)
+        {
+            const double t0 = H[(size_t)i * m + j], t1 = H[(size_t)(i + 1) * m + j];
+            H[(size_t)i * m + j]       = cs[i] * t0 + sn[i] * t1;
+            H[(size_t)(i + 1) * m + j] = -sn[i] * t0 + cs[i] * t1;
+        }
+        const double a0 = H[(size_t)j * m + j], a1 = H[(size_t)(j + 1) * m + j];
+        const double rr = std::hypot(a0, a1);
+        cs[j]           = rr > 0 ? a0 / rr : 1.0;
+        sn[j]           = rr > 0 ? a1 / rr : 0.0;
+        H[(size_t)j * m + j]       = rr;
+        H[(size_t)(j + 1) * m + j] = 0.0;
+        g[j + 1]        = -sn[j] * g[j];
+        g[j]            = cs[j] * g[j];
+        if (std::fabs(g[j + 1]) <= rtol * beta || hn == 0)
+        {
+            ++j;
+            break;
+        }
+    }
+    // y = H^-1 g (upper triangular j x j), d = V y, x += d
+    std::vector<double> yv(j, 0.0);
+    for (int i = j - 1; i >= 0; --i)
+    {
+        double t = g[i];
+        for (int q = i + 1; q < j; ++q)
+            t -= H[(size_t)i * m + q] * yv[q];
+        yv[i] = H[(size_t)i * m + i] != 0 ? t / H[(size_t)i * m + i] : 0.0;
+    }
+    B200LA_CUDA(cudaMemcpyAsync(p.h, yv.data(), sizeof(double) * j, cudaMemcpyHostToDevice, s));
+    k_comb<<<grid_for(n), 256, 0, s>>>(V, p.h, n, j, 1.0, x);
+    B200LA_LAUNCH_CHECK();
+    *iters = j;
+    return B200LA_SUCCESS;
+}
+
+}  // namespace
+}  // namespace b200la
+
+// ---------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------
+using namespace b200la;
+
+extern "C" {
+
+B200LA_API void b200la_refine_default_options(b200la_refine_options* o)
+{
+    if (o == nullptr)
+        return;
+    o->precision      = B200LA_PREC_FP32;
+    o->max_iterations = 50;
+    o->tolerance      = 1e-14;
+    o->gmres_restart  = 30;
+    o->escalate       = 1;
+}
+
+B200LA_API size_t b200la_dsolve_mixed_workspace_size(int64_t n, int64_t nrhs, const b200la_refine_options* o)
+{
+    if (n <= 0 || nrhs <= 0 || nrhs > kMaxNrhsMixed)
+        return 0;
+    b200la_refine_options d;
+    b200la_refine_default_options(&d);
+    if (o == nullptr)
+        o = &d;
+    const int restart = nrhs == 1 ? (o->gmres_restart > kGmresMaxRestart ? kGmresMaxRestart : (o->gmres_restart < 0 ? 0 : o->gmres_restart)) : 0;
+    Arena a;
+    plan_mixed(a, n, nrhs, restart, o->escalate != 0 || o->precision == B200LA_PREC_FP64);
+    return a.size();
+}
+
+B200LA_API int b200la_dsolve_mixed(const double* a, int64_t n, int64_t nrhs, const double* b, int64_t ldb,
+    double* x, int64_t ldx, const b200la_refine_options* opts, b200la_refine_result* res, void* ws,
+    size_t ws_bytes, void* stream)
+{
+    b200la_refine_options d;
+    b200la_refine_default_options(&d);
+    const b200la_refine_options* o = opts ? opts : &d;
+    if (a == nullptr || b == nullptr || x == nullptr)
+        return set_error(B200LA_INVALID_ARGUMENT, "dsolve_mixed: a, b and x must not be null");
+    if (n <= 0 || nrhs <= 0 || nrhs > kMaxNrhsMixed || ldb < nrhs || ldx < nrhs || n > 65536)
+        return set_error(B200LA_INVALID_ARGUMENT, "dsolve_mixed: invalid sizes (n %lld, nrhs %lld; nrhs <= %d)",
+            (long long)n, (long long)nrhs, kMaxNrhsMixed);
+    if (o->precision < B200LA_PREC_FP64 || o->precision > B200LA_PREC_FP16 || o->max_iterations < 1 ||
+        !(o->tolerance > 0))
+        return set_error(B200LA_INVALID_ARGUMENT, "dsolve_mixed: invalid options");
+    const size_t need = b200la_dsolve_mixed_workspace_size(n, nrhs, o);
+    if (ws == nullptr || ws_bytes < need)
+        return set_error(B200LA_WORKSPACE_TOO_SMALL, "dsolve_mixed: workspace too small (%zu < %zu)", ws_bytes, need);
+    int rc = prepare<float>();
+    if (rc != B200LA_SUCCESS)
+        return rc;
+    if ((rc = prepare<double>()) != B200LA_SUCCESS)
+        return rc;
+    if ((rc = set_mixed_attributes()) != B200LA_SUCCESS)
+        return rc;
+    cudaStream_t s       = static_cast<cudaStream_t>(stream);
+    const int    restart = nrhs == 1 ? (o->gmres_restart > kGmresMaxRestart ? kGmresMaxRestart : (o->gmres_restart < 0 ? 0 : o->gmres_restart)) : 0;
+    const bool   fallback = o->escalate != 0 || o->precision == B200LA_PREC_FP64;
+    Arena        ar(ws, ws_bytes);
+    MixedPlan    p  = plan_mixed(ar, n, nrhs, restart, fallback);
+    const int    nn = (int)n, nr = (int)nrhs;
+
+    b200la_refine_result out{};
+    out.backward_error = INFINITY;
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+
+    // ||A||_inf, ||b_j||_inf
+    B200LA_CUDA(cudaMemsetAsync(p.norms, 0, sizeof(unsigned long long) * (4 + 3 * kMaxNrhsMixed), s));
+    std::vector<double> bnorm(nr, 0.0);
+    {
+        k_colmax<<<grid_for((int64_t)n * nrhs), 256, 0, s>>>(b, ldb, nn, nr, p.norms + 4 + 2 * kMaxNrhsMixed);
+        B200LA_LAUNCH_CHECK();
+    }
+
+    int precision = o->precision;
+    int escalations = 0;
+    double anorm = 0.0;
+    bool   have_anorm = false;
+    for (;;)
+    {
+        const bool use64 = precision == B200LA_PREC_FP64;
+        const int  kind  = precision == B200LA_PREC_BF16 ? TC_BF16 : (precision == B200LA_PREC_FP16 ? TC_FP16 : TC_TF32);
+        const bool split = precision == B200LA_PREC_FP32;
+        cudaEventRecord(e0, s);
+        DeviceStatus* st = use64 ? p.gp64.st : p.gp.st;
+        if (!use64)
+        {
+            // A32 and ||A||
+            k_convert_a<<<(nn * 32 + 255) / 256, 256, 0, s>>>(a, n, p.a32, nn, p.norms);
+            B200LA_LAUNCH_CHECK();
+            if ((rc = enqueue_getrf_mixed(p, nn, kind, split, s)) != B200LA_SUCCESS)
+                return rc;
+            k_perm_from_pivots<0><<<1, 256, perm_smem_bytes(nn), s>>>(p.piv, nn, p.perm, perm_smem_bytes(nn) > 0 ? 1 : 0, st, nullptr);
+        }
+        else
+        {
+            B200LA_CUDA(cudaMemcpy2DAsync(p.a64, sizeof(double) * n, a, sizeof(double) * n, sizeof(double) * n, n,
+                cudaMemcpyDeviceToDevice, s));
+            if (!have_anorm)
+            {
+                k_convert_a<<<(nn * 32 + 255) / 256, 256, 0, s>>>(a, n, p.a32, nn, p.norms);
+                B200LA_LAUNCH_CHECK();
+            }
+            if ((rc = enqueue_getrf<double>(p.a64, nn, p.piv64, p.gp64, s)) != B200LA_SUCCESS)
+                return rc;
+            k_perm_from_pivots<0><<<1, 256, perm_smem_bytes(nn), s>>>(p.piv64, nn, p.perm, perm_smem_bytes(nn) > 0 ? 1 : 0, st, nullptr);
+        }
+        B200LA_LAUNCH_CHECK();
+        int info = 0;
+        if ((rc = read_status(st, &info, s)) < 0)
+            return rc;
+        cudaEventRecord(e1, s);
+        cudaEventSynchronize(e1);
+        float fms = 0;
+        cudaEventElapsedTime(&fms, e0, e1);
+        out.factor_ms += fms;
+        out.info = info;
+        if (!have_anorm)
+        {
+            unsigned long long hb[1 + kMaxNrhsMixed];
+            B200LA_CUDA(cudaMemcpy(hb, p.norms, sizeof(unsigned long long), cudaMemcpyDeviceToHost));
+            memcpy(&anorm, &hb[0], 8);
+            B200LA_CUDA(cudaMemcpy(hb + 1, p.norms + 4 + 2 * kMaxNrhsMixed, sizeof(unsigned long long) * nr,
+                cudaMemcpyDeviceToHost));
+            for (int j = 0; j < nr; ++j)
+                memcpy(&bnorm[j], &hb[1 + j], 8);
+            have_anorm = true;
+        }
+        bool converged = false;
+        if (info == 0)
+        {
+            cudaEventRecord(e0, s);
+            // x0 = M^-1 b
+            k_copy2d<double><<<grid_for((int64_t)n * nrhs), 256, 0, s>>>(b, ldb, x, ldx, nn, nr, nullptr);
+            B200LA_LAUNCH_CHECK();
+            rc = use64 ? enqueue_lu_apply<double>(p.a64, p.perm, nn, nr, x, ldx, p, st, s)
+                       : enqueue_lu_apply<float>(p.a32, p.perm, nn, nr, x, ldx, p, st, s);
+            if (rc != B200LA_SUCCESS)
+                return rc;
+            double eta_prev = INFINITY;
+            bool   gmres_on = false;
+            for (int it = 0; it < o->max_iterations; ++it)
+            {
+                double eta = INFINITY;
+                if ((rc = residual_eta(a, n, nn, nr, b, ldb, x, ldx, p, anorm, bnorm, &eta, s)) != B200LA_SUCCESS)
+                    return rc;
+                out.backward_error = eta;
+                if (eta <= o->tolerance)
+                {
+                    converged = true;
+                    break;
+                }
+                const bool stalled = !std::isfinite(eta) || (it > 0 && eta > 0.5 * eta_prev);
+                if (stalled && (!gmres_on && restart > 0))
+                {
+                    gmres_on = true;  // switch to GMRES-IR for the remaining iterations
+                }
+                else if (stalled && it > 1)
+                {
+                    break;  // give up on this precision
+                }
+                eta_prev = eta;
+                out.iterations++;
+                if (gmres_on)
+                {
+                    int gi = 0;
+                    rc = use64 ? gmres_correction<double>(a, n, p.a64, nn, restart, 1e-6, x, p, st, s, &gi)
+                               : gmres_correction<float>(a, n, p.a32, nn, restart, 1e-6, x, p, st, s, &gi);
+                    if (rc != B200LA_SUCCESS)
+                        return rc;
+                    out.gmres_iterations += gi;
+                }
+                else
+                {
+                    rc = use64 ? enqueue_lu_apply<double>(p.a64, p.perm, nn, nr, p.r, nr, p, st, s)
+                               : enqueue_lu_apply<float>(p.a32, p.perm, nn, nr, p.r, nr, p, st, s);
+                    if (rc != B200LA_SUCCESS)
+                        return rc;
+                    k_axpy2d<<<grid_for((int64_t)n * nrhs), 256, 0, s>>>(x, ldx, p.r, nr, nn, nr);
+                    B200LA_LAUNCH_CHECK();
+                }
+            }
+            cudaEventRecord(e1, s);
+            cudaEventSynchronize(e1);
+            float rms = 0;
+            cudaEventElapsedTime(&rms, e0, e1);
+            out.refine_ms += rms;
+        }
+        out.precision_used = precision;
+        out.converged      = converged ? 1 : 0;
+        if (converged || !o->escalate || precision == B200LA_PREC_FP64)
+            break;
+        // escalate: low precisions -> FP32 (three-term TF32) -> FP64
+        precision = (precision == B200LA_PREC_FP32) ? B200LA_PREC_FP64 : B200LA_PREC_FP32;
+        ++escalations;
+    }
+    out.escalations = escalations;
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (res)
+        *res = out;
+    if (out.info != 0)
+        return B200LA_SINGULAR;
+    return out.converged ? B200LA_SUCCESS : B200LA_NOT_CONVERGED;
+}
+}

@@ -66,6 +66,7 @@ __global__ void k_scale2d(T* __restrict__ c, int64_t ldc, int rows, int cols, T 
 // One CTA; the simulation runs in shared memory when n fits (48K entries),
 // else in global memory.  A pivot outside [i+1, n] raises DEV_BAD_PIVOT and
 // is treated as no swap.
+template <int Unused = 0>
 __global__ void k_perm_from_pivots(const int64_t* __restrict__ pivot, int n,
     int32_t* __restrict__ perm, int use_smem, DeviceStatus* st, const DeviceStatus* gate)
 {
@@ -138,8 +139,8 @@ __device__ __forceinline__ T opa(const T* a, int64_t lda, bool transpose, int64_
 // right-hand-side columns [blockIdx.x*kTrsmCols, ...).  One thread per
 // column; the block's triangle is staged in shared memory.  eff_upper
 // selects back substitution.
-template <typename T>
-__global__ void __launch_bounds__(kTrsmCols) k_trsm_diag(const T* __restrict__ a, int64_t lda,
+template <typename TA, typename T = TA>
+__global__ void __launch_bounds__(kTrsmCols) k_trsm_diag(const TA* __restrict__ a, int64_t lda,
     bool transpose, bool eff_upper, bool unit, int r0, int bw, T* __restrict__ x, int64_t ldx,
     int nrhs, const DeviceStatus* gate)
 {
@@ -156,7 +157,7 @@ __global__ void __launch_bounds__(kTrsmCols) k_trsm_diag(const T* __restrict__ a
         T          v      = T(0);
         if (in_tri && !(unit && i == j))
         {
-            v = opa(a, lda, transpose, (int64_t)r0 + i, (int64_t)r0 + j);
+            v = (T)opa(a, lda, transpose, (int64_t)r0 + i, (int64_t)r0 + j);
         }
         tri[i][j] = v;
     }
@@ -226,8 +227,8 @@ __global__ void __launch_bounds__(kTrsmCols) k_trsm_diag(const T* __restrict__ a
 // X[rows r in [u0, u0+um)] -= op(A)[r, r0 .. r0+bw) X[r0 .. r0+bw, :].
 // CTA tile: 64 rows x 16 columns, 256 threads (thread: 1 row x 4 columns).
 constexpr int kUpdCols = 16;
-template <typename T>
-__global__ void __launch_bounds__(256) k_trsm_update(const T* __restrict__ a, int64_t lda,
+template <typename TA, typename T = TA>
+__global__ void __launch_bounds__(256) k_trsm_update(const TA* __restrict__ a, int64_t lda,
     bool transpose, int r0, int bw, int u0, int um, T* __restrict__ x, int64_t ldx, int nrhs,
     const DeviceStatus* gate)
 {
@@ -254,7 +255,7 @@ __global__ void __launch_bounds__(256) k_trsm_update(const T* __restrict__ a, in
             p = e - r * kTrsmBlock;
         }
         const int m = m0 + r;
-        As[r][p]    = (m < u0 + um && p < bw) ? opa(a, lda, transpose, (int64_t)m, (int64_t)r0 + p) : T(0);
+        As[r][p]    = (m < u0 + um && p < bw) ? (T)opa(a, lda, transpose, (int64_t)m, (int64_t)r0 + p) : T(0);
     }
     for (int e = tid; e < kTrsmBlock * kUpdCols; e += 256)
     {

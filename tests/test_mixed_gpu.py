@@ -1,0 +1,82 @@
+"""Mixed-precision LU with FP64 iterative refinement (GPU): every
+factorization precision reaches the requested normwise backward error on the
+benchmark's matrix classes, and the answer agrees with the FP64 oracle."""
+import numpy as np
+import pytest
+import torch
+
+import linearalgebra_b200 as la
+from linearalgebra_b200.workloads import conditioned, system
+
+pytestmark = pytest.mark.gpu
+
+EPS64 = np.finfo(np.float64).eps
+
+
+def dev(a):
+    return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+
+def eta_of(a, x, b):
+    r = b - a @ x
+    return np.abs(r).max() / (np.abs(a).sum(1).max() * np.abs(x).max() + np.abs(b).max())
+
+
+@pytest.mark.parametrize("precision", ["fp32", "tf32", "bf16", "fp16"])
+@pytest.mark.parametrize("n", [300, 1100])
+def test_mixed_reaches_fp64_accuracy(port, precision, n):
+    a, x_true, b = system(n, seed=70 + n)
+    x, res, st = la.solve_mixed(dev(a), dev(b), precision=precision, tolerance=1e-14)
+    torch.cuda.synchronize()
+    assert st == 0 and res["converged"] == 1, res
+    xs = x.cpu().numpy()
+    assert port.backward_error(a, xs, b) <= 1e-14
+    # against the FP64 oracle's solution (forward error, conditioning-scaled)
+    _, _, x_ref = port.gesv(a, b)
+    assert np.abs(xs - x_ref).max() / np.abs(x_ref).max() < 1e-9
+
+
+def test_mixed_fp32_takes_few_iterations():
+    a, _, b = system(2048, seed=5)
+    _, res, st = la.solve_mixed(dev(a), dev(b), precision="fp32")
+    assert st == 0 and res["precision_used"] == la._lib.PREC_FP32
+    assert res["iterations"] <= 6 and res["escalations"] == 0, res
+
+
+def test_mixed_multi_rhs():
+    n, nrhs = 700, 64
+    a, x_true, b = system(n, seed=8, nrhs=nrhs)
+    x, res, st = la.solve_mixed(dev(a), dev(b), precision="fp32")
+    torch.cuda.synchronize()
+    assert st == 0, res
+    xs = x.cpu().numpy()
+    for j in range(0, nrhs, 9):
+        assert eta_of(a, xs[:, j], b[:, j]) <= 1e-14
+
+
+@pytest.mark.parametrize("kappa", [1e4, 1e8])
+def test_mixed_conditioned_gmres_or_escalation(kappa):
+    n = 1024
+    a = conditioned(n, kappa, seed=3)
+    x_true = np.random.default_rng(1).uniform(-1, 1, n)
+    b = a @ x_true
+    x, res, st = la.solve_mixed(dev(a), dev(b), precision="bf16", tolerance=1e-14)
+    torch.cuda.synchronize()
+    assert st == 0 and res["converged"] == 1, res
+    assert eta_of(a, x.cpu().numpy(), b) <= 1e-14
+
+
+def test_mixed_fp64_precision_is_plain_lu():
+    a, _, b = system(600, seed=2)
+    x, res, st = la.solve_mixed(dev(a), dev(b), precision="fp64")
+    assert st == 0 and res["precision_used"] == la._lib.PREC_FP64
+    assert eta_of(a, x.cpu().numpy(), b) <= 1e-14
+
+
+def test_mixed_singular_reports_info():
+    a = np.zeros((130, 130))
+    a[np.arange(130), np.arange(130)] = 1.0
+    a[:, 77] = 0.0
+    b = np.ones(130)
+    x, res, st = la.solve_mixed(dev(a), dev(b), precision="fp32", escalate=False)
+    assert st == la._lib.SINGULAR and res["info"] == 78
