@@ -182,7 +182,7 @@ int launch_panel(T* m, int n, int k, int w, int64_t* pivot, const GetrfPlan<T>& 
         if (cl > 0)
         {
             const int    rpc_c  = (R + cl - 1) / cl;
-            const size_t smem_c = (size_t)rpc_c * (kNB + 1) * sizeof(T);
+            const size_t smem_c = (size_t)rpc_c * panel_ldl<T>() * sizeof(T);
             if (smem_c <= kPanelSmemMax)
             {
                 cudaLaunchConfig_t  cfg = {};
@@ -208,7 +208,7 @@ int launch_panel(T* m, int n, int k, int w, int64_t* pivot, const GetrfPlan<T>& 
         G             = G < 1 ? 1 : (G > gmax ? gmax : G);
         int rpc       = (R + G - 1) / G;
         G             = (R + rpc - 1) / rpc;
-        size_t smem   = (size_t)rpc * (kNB + 1) * sizeof(T);
+        size_t smem   = (size_t)rpc * panel_ldl<T>() * sizeof(T);
         int    in_smem = smem <= kPanelSmemMax ? 1 : 0;
         if (!in_smem)
         {

@@ -51,6 +51,21 @@ template <> struct Vec2<float>
     using type = float2;
 };
 
+template <typename T> struct Vec16;
+template <> struct Vec16<double>
+{
+    using type = double2;
+};
+template <> struct Vec16<float>
+{
+    using type = float4;
+};
+
+// Row stride of a panel slice held in shared memory: 64 values plus 16 bytes
+// of padding, so rows stay 16-byte aligned for vector access while
+// consecutive rows start in different banks.
+template <typename T> constexpr int panel_ldl() { return kNB + 16 / (int)sizeof(T); }
+
 template <typename T> struct Limits;
 template <> struct Limits<double>
 {
@@ -312,10 +327,13 @@ template <typename T>
 __device__ __forceinline__ void panel_update_rows(T* loc, size_t ldl, int rbeg, int nloc, int r0,
     int jj, int w, int c, const T* urow, T d, double& nk, int& nr)
 {
+    using VT             = typename Vec16<T>::type;
+    constexpr int V      = 16 / (int)sizeof(T);
     const bool zero      = d == T(0);
     const bool use_recip = fabs(d) >= Limits<T>::min_normal();
     const T    recip     = use_recip ? (T)(T(1) / d) : T(1);
     const bool has_next  = jj + 1 < w;
+    const bool vec_ok    = ((ldl * sizeof(T)) % 16 == 0) && ((reinterpret_cast<uintptr_t>(loc) & 15) == 0);
     for (int r = rbeg + (int)threadIdx.x; r < nloc; r += kPanelThreads)
     {
         T* row = loc + (size_t)r * ldl;
@@ -324,8 +342,33 @@ __device__ __forceinline__ void panel_update_rows(T* loc, size_t ldl, int rbeg, 
             const T x = row[jj];
             const T l = use_recip ? x * recip : x / d;
             row[jj]   = l;
-#pragma unroll 4
-            for (int cc = jj + 1; cc < w; ++cc)
+            int cc    = jj + 1;
+            if (vec_ok)
+            {
+                for (; cc < w && (cc % V) != 0; ++cc)
+                {
+                    row[cc] = fma(-l, urow[cc], row[cc]);
+                }
+                for (; cc + V <= w; cc += V)
+                {
+                    VT       rv = *reinterpret_cast<VT*>(row + cc);
+                    const VT uv = *reinterpret_cast<const VT*>(urow + cc);
+                    if constexpr (V == 2)
+                    {
+                        rv.x = fma(-l, uv.x, rv.x);
+                        rv.y = fma(-l, uv.y, rv.y);
+                    }
+                    else
+                    {
+                        rv.x = fma(-l, uv.x, rv.x);
+                        rv.y = fma(-l, uv.y, rv.y);
+                        rv.z = fma(-l, uv.z, rv.z);
+                        rv.w = fma(-l, uv.w, rv.w);
+                    }
+                    *reinterpret_cast<VT*>(row + cc) = rv;
+                }
+            }
+            for (; cc < w; ++cc)
             {
                 row[cc] = fma(-l, urow[cc], row[cc]);
             }
@@ -350,8 +393,8 @@ __global__ void __launch_bounds__(kPanelThreads) k_panel(T* __restrict__ A, int 
     DeviceStatus* __restrict__ st)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    __shared__ T      urow[kNB];
-    __shared__ T      drow[kNB];
+    __shared__ __align__(16) T urow[kNB];
+    __shared__ __align__(16) T drow[kNB];
     __shared__ int    piv_loc[kNB];
     __shared__ double red_key[kPanelThreads / 32 + 1];
     __shared__ int    red_row[kPanelThreads / 32 + 1];
@@ -366,7 +409,7 @@ __global__ void __launch_bounds__(kPanelThreads) k_panel(T* __restrict__ A, int 
     const int nloc = max(0, min(n, r0 + rows_per_cta) - r0);
 
     T*           loc;
-    const size_t ldl = in_smem ? (size_t)(kNB + 1) : (size_t)n;
+    const size_t ldl = in_smem ? (size_t)panel_ldl<T>() : (size_t)n;
     if (in_smem)
     {
         loc = reinterpret_cast<T*>(smem_raw);
@@ -654,8 +697,8 @@ __global__ void __launch_bounds__(kPanelThreads, 1) k_panel_cluster(T* __restric
     cg::cluster_group cluster = cg::this_cluster();
 
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    __shared__ T      urow[kNB];
-    __shared__ T      drow[kNB];
+    __shared__ __align__(16) T urow[kNB];
+    __shared__ __align__(16) T drow[kNB];
     __shared__ int    piv_loc[kNB];
     __shared__ double red_key[kPanelThreads / 32 + 1];
     __shared__ int    red_row[kPanelThreads / 32 + 1];
@@ -670,7 +713,7 @@ __global__ void __launch_bounds__(kPanelThreads, 1) k_panel_cluster(T* __restric
     const int b    = (int)cluster.block_rank();
     const int r0   = k + b * rows_per_cta;
     const int nloc = max(0, min(n, r0 + rows_per_cta) - r0);
-    constexpr int ldl = kNB + 1;
+    constexpr int ldl = panel_ldl<T>();
 
     T* loc = reinterpret_cast<T*>(smem_raw);
     for (int e = tid; e < nloc * w; e += kPanelThreads)

@@ -21,6 +21,7 @@
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -364,6 +365,8 @@ struct MixedPlan
     double*            y;       // n x nrhs scratch for the solves
     unsigned long long* norms;  // [0] ||A||, [1..] per-column maxima (3 x 64)
     TrsvSync*          tsync;
+    double*            dinv;    // inverses of the 64 x 64 diagonal blocks of L and U
+    uint64_t*          xll;     // flagged copies of solved blocks (k_trsv_blocks)
     double*            V;       // GMRES basis (m+1) x n
     double*            h;       // GMRES dot products (m+1)
     double*            a64;     // FP64 copy of A for the FP64 fallback
@@ -372,6 +375,19 @@ struct MixedPlan
 };
 
 constexpr int kMaxNrhsMixed = 64;
+
+// Epochs of the flagged words of k_trsv_blocks: distinct for every launch in
+// this process (never 0, the value of cleared memory).
+uint32_t next_epoch()
+{
+    static std::atomic<uint32_t> e{0};
+    uint32_t v = e.fetch_add(1) + 1;
+    if (v == 0)
+    {
+        v = e.fetch_add(1) + 1;
+    }
+    return v;
+}
 constexpr int kGmresMaxRestart = 50;
 
 MixedPlan plan_mixed(Arena& a, int64_t n, int64_t nrhs, int restart, bool fp64_fallback)
@@ -389,6 +405,8 @@ MixedPlan plan_mixed(Arena& a, int64_t n, int64_t nrhs, int restart, bool fp64_f
     p.y        = a.next<double>((size_t)n * nrhs);
     p.norms    = a.next<unsigned long long>(4 + 3 * kMaxNrhsMixed);
     p.tsync    = reinterpret_cast<TrsvSync*>(a.next<int32_t>(32 + (size_t)(n + kTvRows - 1) / kTvRows + 32));
+    p.dinv     = a.next<double>((size_t)((n + kTvRows - 1) / kTvRows) * 2 * kTvRows * kTvRows);
+    p.xll      = a.next<uint64_t>((size_t)((n + kTvRows - 1) / kTvRows) * kTvRows * 2);
     const int m = restart > 0 ? restart : 0;
     p.V        = a.next<double>((size_t)(m + 1) * n);
     p.h        = a.next<double>((size_t)m + 2);
@@ -413,13 +431,13 @@ int enqueue_getrf_mixed(MixedPlan& p, int n, int kind, bool split, cudaStream_t 
     if ((rc = panel_config<float>(cl, gmax)) != B200LA_SUCCESS)
         return rc;
     CUtensorMap ma, mb, mas, mbs;
-    if ((rc = make_kmajor_map(&ma, p.l21op, kind, n, kOuterNB, kOuterNB)) != B200LA_SUCCESS ||
-        (rc = make_kmajor_map(&mb, p.u12op, kind, n, kOuterNB, kOuterNB)) != B200LA_SUCCESS)
+    if ((rc = make_kmajor_map(&ma, p.l21op, kind, n, kOuterNB, kOuterNB, kTcBM)) != B200LA_SUCCESS ||
+        (rc = make_kmajor_map(&mb, p.u12op, kind, n, kOuterNB, kOuterNB, kTcBN)) != B200LA_SUCCESS)
         return rc;
     mas = ma;
     mbs = mb;
-    if (split && ((rc = make_kmajor_map(&mas, p.l21small, TC_TF32, n, kOuterNB, kOuterNB)) != B200LA_SUCCESS ||
-                     (rc = make_kmajor_map(&mbs, p.u12small, TC_TF32, n, kOuterNB, kOuterNB)) != B200LA_SUCCESS))
+    if (split && ((rc = make_kmajor_map(&mas, p.l21small, TC_TF32, n, kOuterNB, kOuterNB, kTcBM)) != B200LA_SUCCESS ||
+                     (rc = make_kmajor_map(&mbs, p.u12small, TC_TF32, n, kOuterNB, kOuterNB, kTcBN)) != B200LA_SUCCESS))
         return rc;
     float* a32 = p.a32;
     for (int K = 0; K < n; K += kOuterNB)
@@ -522,9 +540,11 @@ int enqueue_lu_apply(const TA* lu, const int32_t* perm, int n, int nrhs, double*
         const int nb = (n + kTvRows - 1) / kTvRows;
         for (int pass = 0; pass < 2; ++pass)
         {
-            B200LA_CUDA(cudaMemsetAsync(p.tsync, 0, sizeof(int32_t) * (32 + nb), s));
+            B200LA_CUDA(cudaMemsetAsync(p.tsync, 0, sizeof(int32_t), s));
+            const uint32_t epoch = next_epoch();
             prof_begin(KC_SOLVE, s);
-            k_trsv_syncfree<TA, double><<<nb, kTvThreads, 0, s>>>(lu, n, p.y, n, pass, pass == 0 ? 1 : 0, p.tsync, st, nullptr);
+            k_trsv_blocks<TA><<<nb, kTvThreads, 0, s>>>(lu, n, p.y, n, pass, p.dinv, p.xll, epoch,
+                reinterpret_cast<int32_t*>(p.tsync), st);
             prof_end(KC_SOLVE, s);
             B200LA_LAUNCH_CHECK();
         }
@@ -812,6 +832,16 @@ B200LA_API int b200la_dsolve_mixed(const double* a, int64_t n, int64_t nrhs, con
             k_perm_from_pivots<0><<<1, 256, perm_smem_bytes(nn), s>>>(p.piv64, nn, p.perm, perm_smem_bytes(nn) > 0 ? 1 : 0, st, nullptr);
         }
         B200LA_LAUNCH_CHECK();
+        {
+            const int nbk = (nn + kTvRows - 1) / kTvRows;
+            prof_begin(KC_SOLVE, s);
+            if (use64)
+                k_invert_diag_blocks<double><<<dim3(nbk, 2), kTvRows, 0, s>>>(p.a64, n, nn, p.dinv);
+            else
+                k_invert_diag_blocks<float><<<dim3(nbk, 2), kTvRows, 0, s>>>(p.a32, n, nn, p.dinv);
+            prof_end(KC_SOLVE, s);
+            B200LA_LAUNCH_CHECK();
+        }
         int info = 0;
         if ((rc = read_status(st, &info, s)) < 0)
             return rc;

@@ -58,7 +58,8 @@ template <int KIND, bool SPLIT3> int set_attr_once()
 }
 }  // namespace
 
-int make_kmajor_map(CUtensorMap* map, const void* base, int kind, int64_t rows, int64_t k, int64_t ld)
+int make_kmajor_map(CUtensorMap* map, const void* base, int kind, int64_t rows, int64_t k, int64_t ld,
+    int box_rows)
 {
     EncodeTiledFn fn = encode_fn();
     if (fn == nullptr)
@@ -75,7 +76,7 @@ int make_kmajor_map(CUtensorMap* map, const void* base, int kind, int64_t rows, 
     }
     cuuint64_t dims[2]    = {(cuuint64_t)k, (cuuint64_t)rows};
     cuuint64_t strides[1] = {(cuuint64_t)(ld * elem)};
-    cuuint32_t box[2]     = {(cuuint32_t)(kTcAtomBytes / elem), (cuuint32_t)kTcBM};
+    cuuint32_t box[2]     = {(cuuint32_t)(kTcAtomBytes / elem), (cuuint32_t)box_rows};
     cuuint32_t estr[2]    = {1, 1};
     const CUresult r = fn(map, dt, 2, const_cast<void*>(base), dims, strides, box, estr,
         CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
@@ -160,15 +161,15 @@ extern "C" B200LA_API int b200la_sgemm_tc_update(int kind, int split3, float* c,
         return rc;
     }
     CUtensorMap ma, mb, mas, mbs;
-    if ((rc = make_kmajor_map(&ma, a, kind, m, k, k)) != B200LA_SUCCESS ||
-        (rc = make_kmajor_map(&mb, b, kind, n, k, k)) != B200LA_SUCCESS)
+    if ((rc = make_kmajor_map(&ma, a, kind, m, k, k, kTcBM)) != B200LA_SUCCESS ||
+        (rc = make_kmajor_map(&mb, b, kind, n, k, k, kTcBN)) != B200LA_SUCCESS)
     {
         return rc;
     }
     mas = ma;
     mbs = mb;
-    if (split3 && ((rc = make_kmajor_map(&mas, a_small, kind, m, k, k)) != B200LA_SUCCESS ||
-                      (rc = make_kmajor_map(&mbs, b_small, kind, n, k, k)) != B200LA_SUCCESS))
+    if (split3 && ((rc = make_kmajor_map(&mas, a_small, kind, m, k, k, kTcBM)) != B200LA_SUCCESS ||
+                      (rc = make_kmajor_map(&mbs, b_small, kind, n, k, k, kTcBN)) != B200LA_SUCCESS))
     {
         return rc;
     }

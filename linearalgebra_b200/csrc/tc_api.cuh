@@ -9,8 +9,9 @@
 namespace b200la
 {
 // TMA map of a K-major operand: `rows` rows of `k` elements, row stride `ld`
-// elements, boxes of one 128-byte K slice x 128 rows, 128B swizzle.
-int make_kmajor_map(CUtensorMap* map, const void* base, int kind, int64_t rows, int64_t k, int64_t ld);
+// elements, boxes of one 128-byte K slice x box_rows rows, 128B swizzle.
+int make_kmajor_map(CUtensorMap* map, const void* base, int kind, int64_t rows, int64_t k, int64_t ld,
+    int box_rows);
 
 // C[m x n] -= A B^T on the tensor cores (see k_tc_update).
 int enqueue_tc_update(int kind, bool split3, const CUtensorMap& a, const CUtensorMap& b, const CUtensorMap& as,

@@ -3,11 +3,11 @@
 //     C[M x N] (fp32, row-major, ldc)  -=  A[M x K] * B[N x K]^T
 //
 // A and B are K-major operand copies (row stride K elements) in TF32 (fp32
-// containers), BF16 or FP16.  One CTA computes one 128 x 128 tile of C:
+// containers), BF16 or FP16.  One CTA computes one 128 x 256 tile of C:
 //   * warp 0 / lane 0 issues TMA loads of 128-byte-wide K slices of A and B
 //     (128B swizzle) into a ring of shared-memory stages, completing on
 //     mbarriers;
-//   * warp 1 / lane 0 issues tcgen05.mma (M=128, N=128, 32 bytes of K per
+//   * warp 1 / lane 0 issues tcgen05.mma (M=128, N=256, 32 bytes of K per
 //     instruction) accumulating in FP32 in tensor memory, and frees each
 //     stage with tcgen05.commit;
 //   * all four warps then read the accumulator from tensor memory
@@ -41,9 +41,11 @@ enum TcKind : int
 };
 
 constexpr int kTcBM        = 128;
-constexpr int kTcBN        = 128;
-constexpr int kTcAtomBytes = 128;  // one 128B-swizzle atom of K per stage
-constexpr int kTcTileBytes = kTcBM * kTcAtomBytes;  // 16 KB per operand tile per stage
+constexpr int kTcBN        = 256;
+constexpr int kTcAtomBytes = 128;                    // one 128B-swizzle atom of K per stage
+constexpr int kTcTileA     = kTcBM * kTcAtomBytes;   // 16 KB: A slice of a stage
+constexpr int kTcTileB     = kTcBN * kTcAtomBytes;   // 32 KB: B slice of a stage
+constexpr int kTcPair      = kTcTileA + kTcTileB;    // one product's operands
 
 template <int KIND> struct TcTraits;
 template <> struct TcTraits<TC_TF32>
@@ -62,12 +64,12 @@ template <> struct TcTraits<TC_FP16>
     static constexpr uint32_t fmt  = 0;  // F16
 };
 
-template <bool SPLIT3> constexpr int tc_stages() { return SPLIT3 ? 3 : 4; }
-template <bool SPLIT3> constexpr int tc_operands() { return SPLIT3 ? 4 : 2; }
+template <bool SPLIT3> constexpr int tc_stages() { return SPLIT3 ? 2 : 4; }
+template <bool SPLIT3> constexpr int tc_stage_bytes() { return SPLIT3 ? 2 * kTcPair : kTcPair; }
 template <bool SPLIT3> constexpr size_t tc_smem_bytes()
 {
     // stages + 1 KB alignment slack + barriers/TMEM address
-    return (size_t)tc_stages<SPLIT3>() * tc_operands<SPLIT3>() * kTcTileBytes + 1024 + 256;
+    return (size_t)tc_stages<SPLIT3>() * tc_stage_bytes<SPLIT3>() + 1024 + 256;
 }
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p)
@@ -181,7 +183,8 @@ template <int KIND> __host__ __device__ constexpr uint32_t tc_idesc()
     return (1u << 4) | (TcTraits<KIND>::fmt << 7) | (TcTraits<KIND>::fmt << 10) |
            ((uint32_t)(kTcBN >> 3) << 17) | ((uint32_t)(kTcBM >> 4) << 24);
 }
-static_assert(tc_idesc<TC_TF32>() == 0x8200910u, "TF32 instruction descriptor layout");
+static_assert((tc_idesc<TC_TF32>() & ~(0x3Fu << 17)) == (0x8200910u & ~(0x3Fu << 17)),
+    "TF32 instruction descriptor layout");
 
 __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32])
 {
@@ -211,15 +214,15 @@ __global__ void __launch_bounds__(128, 1) k_tc_update(const __grid_constant__ CU
     DeviceStatus* __restrict__ st)
 {
     constexpr int S   = tc_stages<SPLIT3>();
-    constexpr int OPS = tc_operands<SPLIT3>();
+    constexpr int SB  = tc_stage_bytes<SPLIT3>();
     constexpr int EA  = kTcAtomBytes / TcTraits<KIND>::elem;  // K elements per stage
     constexpr uint32_t IDESC = tc_idesc<KIND>();
 
     extern __shared__ __align__(1024) unsigned char tc_smem_raw[];
     unsigned char* base = reinterpret_cast<unsigned char*>(
         (reinterpret_cast<uintptr_t>(tc_smem_raw) + 1023) & ~uintptr_t(1023));
-    unsigned char* tiles    = base;  // [S][OPS][16 KB]
-    uint64_t*      full     = reinterpret_cast<uint64_t*>(base + (size_t)S * OPS * kTcTileBytes);
+    unsigned char* tiles    = base;  // [S] x {A 16 KB, B 32 KB [, A_small, B_small]}
+    uint64_t*      full     = reinterpret_cast<uint64_t*>(base + (size_t)S * SB);
     uint64_t*      empty    = full + S;
     uint64_t*      done     = empty + S;
     uint32_t*      tmem_ptr = reinterpret_cast<uint32_t*>(done + 1);
@@ -273,14 +276,14 @@ __global__ void __launch_bounds__(128, 1) k_tc_update(const __grid_constant__ CU
             {
                 break;
             }
-            unsigned char* stage = tiles + (size_t)s * OPS * kTcTileBytes;
-            mbar_expect_tx(&full[s], OPS * kTcTileBytes);
+            unsigned char* stage = tiles + (size_t)s * SB;
+            mbar_expect_tx(&full[s], SB);
             tma_load_2d(stage, &tmA, a * EA, m0, &full[s]);
-            tma_load_2d(stage + kTcTileBytes, &tmB, a * EA, n0, &full[s]);
+            tma_load_2d(stage + kTcTileA, &tmB, a * EA, n0, &full[s]);
             if constexpr (SPLIT3)
             {
-                tma_load_2d(stage + 2 * kTcTileBytes, &tmAs, a * EA, m0, &full[s]);
-                tma_load_2d(stage + 3 * kTcTileBytes, &tmBs, a * EA, n0, &full[s]);
+                tma_load_2d(stage + kTcPair, &tmAs, a * EA, m0, &full[s]);
+                tma_load_2d(stage + kTcPair + kTcTileA, &tmBs, a * EA, n0, &full[s]);
             }
             *reinterpret_cast<volatile int*>(s_issued) = a + 1;
         }
@@ -298,8 +301,8 @@ __global__ void __launch_bounds__(128, 1) k_tc_update(const __grid_constant__ CU
                 break;
             }
             tc_fence_after();
-            const uint32_t sa = smem_u32(tiles + (size_t)s * OPS * kTcTileBytes);
-            const uint32_t sb = sa + kTcTileBytes;
+            const uint32_t sa = smem_u32(tiles + (size_t)s * SB);
+            const uint32_t sb = sa + kTcTileA;
 #pragma unroll
             for (int kk = 0; kk < kTcAtomBytes / 32; ++kk)
             {
@@ -308,8 +311,8 @@ __global__ void __launch_bounds__(128, 1) k_tc_update(const __grid_constant__ CU
                 tc_mma<KIND>(tmem, da, db, IDESC, (a > 0 || kk > 0) ? 1u : 0u);
                 if constexpr (SPLIT3)
                 {
-                    const uint64_t das = tc_desc(sa + 2 * kTcTileBytes + kk * 32);
-                    const uint64_t dbs = tc_desc(sa + 3 * kTcTileBytes + kk * 32);
+                    const uint64_t das = tc_desc(sa + kTcPair + kk * 32);
+                    const uint64_t dbs = tc_desc(sa + kTcPair + kTcTileA + kk * 32);
                     tc_mma<KIND>(tmem, da, dbs, IDESC, 1u);
                     tc_mma<KIND>(tmem, das, db, IDESC, 1u);
                 }
@@ -319,6 +322,16 @@ __global__ void __launch_bounds__(128, 1) k_tc_update(const __grid_constant__ CU
         tc_commit(done);
     }
     __syncwarp();
+
+    // while the MMAs run: pull this thread's row of the C tile into L2
+    {
+        const int r = m0 + warp * 32 + lane;
+        if (r < M && n0 + kTcBN <= N && ((ldc & 3) == 0) && ((reinterpret_cast<uintptr_t>(C) & 15) == 0))
+        {
+            const float* src = C + (size_t)r * ldc + n0;
+            asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(src), "r"(kTcBN * 4) : "memory");
+        }
+    }
 
     // epilogue: thread = one row of the tile, 32 columns per tensor-memory load
     const bool ok = mbar_wait(done, 0);
@@ -336,20 +349,32 @@ __global__ void __launch_bounds__(128, 1) k_tc_update(const __grid_constant__ CU
 #pragma unroll 1
         for (int j = 0; j < kTcBN / 32; ++j)
         {
+            const int  c0   = n0 + j * 32;
+            const bool fast = row_ok && vec && c0 + 32 <= N;
+            float4     cv[8];
+            if (fast)
+            {
+                // C loads first: they do not depend on the accumulator
+                const float4* p = reinterpret_cast<const float4*>(crow + c0);
+#pragma unroll
+                for (int q = 0; q < 8; ++q)
+                {
+                    cv[q] = p[q];
+                }
+            }
             float v[32];
             tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(j * 32), v);
-            const int c0 = n0 + j * 32;
             if (!row_ok)
             {
                 continue;
             }
-            if (vec && c0 + 32 <= N)
+            if (fast)
             {
                 float4* p = reinterpret_cast<float4*>(crow + c0);
 #pragma unroll
                 for (int q = 0; q < 8; ++q)
                 {
-                    float4 x = p[q];
+                    float4 x = cv[q];
                     x.x -= v[4 * q];
                     x.y -= v[4 * q + 1];
                     x.z -= v[4 * q + 2];

@@ -31,28 +31,111 @@ struct TrsvSync
     uint32_t flags[1];  // [nblocks], cleared per call
 };
 
-template <typename TA, typename TX>
-__global__ void __launch_bounds__(kTvThreads) k_trsv_syncfree(const TA* __restrict__ a, int64_t lda,
-    TX* __restrict__ x, int n, int upper, int unit, TrsvSync* sync, DeviceStatus* st,
-    const DeviceStatus* gate)
+// Inverses of the kTvRows x kTvRows diagonal blocks of the unit-lower (L)
+// and upper (U) triangles of an LU factor, FP64, row-major per block:
+// dinv[(2*b + 0)] = L_bb^-1, dinv[(2*b + 1)] = U_bb^-1.  grid (nblocks, 2),
+// one thread per column of the inverse (forward/back substitution on e_j).
+// A partial last block is padded with the identity.
+template <typename TA>
+__global__ void __launch_bounds__(kTvRows) k_invert_diag_blocks(const TA* __restrict__ a, int64_t lda, int n,
+    double* __restrict__ dinv)
 {
-    __shared__ TX  part[kTvRows][kTvThreads / kTvRows + 1];
-    __shared__ TX  tri[kTvRows][kTvRows + 1];
-    __shared__ TX  xst[2][kTvRows];
-    __shared__ int s_blk, s_abort, s_ready;
-    if (gate != nullptr && (ld_volatile_i32(&gate->error) != 0 || gate->first_zero >= 0))
+    __shared__ double tri[kTvRows][kTvRows + 1];
+    const int  blk   = blockIdx.x;
+    const bool upper = blockIdx.y == 1;
+    const int  r0    = blk * kTvRows;
+    const int  br    = min(kTvRows, n - r0);
+    const int  j     = threadIdx.x;
+    for (int e = j; e < kTvRows * kTvRows; e += kTvRows)
     {
-        return;
+        const int i = e / kTvRows, c = e % kTvRows;
+        double    v = (i == c) ? 1.0 : 0.0;
+        if (i < br && c < br && (upper ? c >= i : c < i))
+        {
+            v = (double)a[(int64_t)(r0 + i) * lda + r0 + c];
+        }
+        tri[i][c] = v;
     }
+    __syncthreads();
+    // column j of the inverse, built in place in the output block (each
+    // thread reads back only its own column)
+    double* out = dinv + ((size_t)blk * 2 + (upper ? 1 : 0)) * kTvRows * kTvRows;
+    if (!upper)
+    {
+        for (int i = 0; i < kTvRows; ++i)
+        {
+            double s = (i == j) ? 1.0 : 0.0;
+            for (int p = j; p < i; ++p)
+            {
+                s = fma(-tri[i][p], out[p * kTvRows + j], s);
+            }
+            out[i * kTvRows + j] = i < j ? 0.0 : s;
+        }
+    }
+    else
+    {
+        for (int i = kTvRows - 1; i >= 0; --i)
+        {
+            double s = (i == j) ? 1.0 : 0.0;
+            for (int p = i + 1; p <= j; ++p)
+            {
+                s = fma(-tri[i][p], out[p * kTvRows + j], s);
+            }
+            out[i * kTvRows + j] = i > j ? 0.0 : s / tri[i][i];
+        }
+    }
+}
+
+// Flagged publication of a solved block: value i of block b is two 8-byte
+// words (low/high halves of the double, each with the call's epoch in the
+// high 32 bits), so a reader that sees the epoch in both words has the value.
+__device__ __forceinline__ void tv_publish(uint64_t* xll, int blk, int i, double v, uint32_t epoch)
+{
+    const uint64_t bits = (uint64_t)__double_as_longlong(v);
+    const uint64_t w0   = ((uint64_t)epoch << 32) | (bits & 0xffffffffull);
+    const uint64_t w1   = ((uint64_t)epoch << 32) | (bits >> 32);
+    asm volatile("st.relaxed.gpu.global.v2.u64 [%0], {%1, %2};" ::"l"(xll + ((size_t)blk * kTvRows + i) * 2),
+        "l"(w0), "l"(w1)
+        : "memory");
+}
+__device__ __forceinline__ bool tv_read(const uint64_t* xll, int blk, int i, uint32_t epoch, double& v)
+{
+    uint64_t w0, w1;
+    asm volatile("ld.relaxed.gpu.global.v2.u64 {%0, %1}, [%2];" : "=l"(w0), "=l"(w1)
+                 : "l"(xll + ((size_t)blk * kTvRows + i) * 2)
+                 : "memory");
+    if ((uint32_t)(w0 >> 32) != epoch || (uint32_t)(w1 >> 32) != epoch)
+    {
+        return false;
+    }
+    v = __longlong_as_double((long long)(((w1 & 0xffffffffull) << 32) | (w0 & 0xffffffffull)));
+    return true;
+}
+
+// x <- T^-1 x for T the unit-lower (upper = 0) or upper (upper = 1) triangle
+// of the factor `a`, using dinv (k_invert_diag_blocks).  CTA = one 64-row
+// block, claimed by ticket in solve order; xll receives the flagged copies of
+// the solved blocks (epoch: a value this call's flags carry, never reused).
+template <typename TA>
+__global__ void __launch_bounds__(kTvThreads) k_trsv_blocks(const TA* __restrict__ a, int64_t lda,
+    double* __restrict__ x, int n, int upper, const double* __restrict__ dinv, uint64_t* __restrict__ xll,
+    uint32_t epoch, int32_t* __restrict__ ticket, DeviceStatus* st)
+{
+    constexpr int Q = kTvRows / (kTvThreads / kTvRows);  // columns per thread per tile (16)
+    __shared__ double inv[kTvRows][kTvRows + 1];
+    __shared__ double part[kTvRows][kTvThreads / kTvRows + 1];
+    __shared__ double xs[2][kTvRows];
+    __shared__ double vb[kTvRows];
+    __shared__ int    s_t, s_abort;
     const int nb  = (n + kTvRows - 1) / kTvRows;
     const int tid = threadIdx.x;
     if (tid == 0)
     {
-        s_blk   = atomicAdd(&sync->ticket, 1);
+        s_t     = atomicAdd(ticket, 1);
         s_abort = 0;
     }
     __syncthreads();
-    const int t = s_blk;  // position in solve order
+    const int t = s_t;
     if (t >= nb)
     {
         return;
@@ -60,197 +143,108 @@ __global__ void __launch_bounds__(kTvThreads) k_trsv_syncfree(const TA* __restri
     const int blk = upper ? nb - 1 - t : t;
     const int r0  = blk * kTvRows;
     const int br  = min(kTvRows, n - r0);
-
-    // ---- stage the diagonal block (only the selected triangle)
-    for (int e = tid; e < kTvRows * kTvRows; e += kTvThreads)
     {
-        const int i = e / kTvRows, j = e % kTvRows;
-        TX        v = TX(0);
-        if (i < br && j < br && (upper ? j >= i : j <= i) && !(unit && i == j))
+        const double* src = dinv + ((size_t)blk * 2 + (upper ? 1 : 0)) * kTvRows * kTvRows;
+        for (int e = tid; e < kTvRows * kTvRows; e += kTvThreads)
         {
-            v = (TX)a[(int64_t)(r0 + i) * lda + r0 + j];
+            inv[e / kTvRows][e % kTvRows] = src[e];
         }
-        tri[i][j] = v;
     }
-
-    // ---- accumulate the solved blocks: thread = (row r, quarter q).  Warp 0
-    // checks 32 flags at a time and publishes how many consecutive blocks
-    // (in solve order) are ready; each ready block's x is staged in shared
-    // memory once.
-    const int r     = tid % kTvRows;
-    const int q     = tid / kTvRows;
-    TX        acc   = TX(0);
-    int       ready = 0;
+    const int r = tid % kTvRows;
+    const int q = tid / kTvRows;
+    double    acc = 0.0;
+    // software pipeline: A tile of the next block in registers, and (threads
+    // < 64) the flagged x value of the next block
+    TA     an[Q];
+    double xn     = 0.0;
+    bool   xn_ok  = false;
+    auto   load_a = [&](int s, TA (&dst)[Q]) {
+        const int jb = upper ? nb - 1 - s : s;
+        const int c0 = jb * kTvRows + q * Q;
+#pragma unroll
+        for (int j = 0; j < Q; ++j)
+        {
+            dst[j] = (r < br && c0 + j < n) ? a[(int64_t)(r0 + r) * lda + c0 + j] : TA(0);
+        }
+    };
+    if (t > 0)
+    {
+        load_a(0, an);
+        if (tid < kTvRows)
+        {
+            xn_ok = tv_read(xll, upper ? nb - 1 : 0, tid, epoch, xn);
+        }
+    }
     for (int s = 0; s < t; ++s)
     {
-        if (s >= ready)
+        const int jb = upper ? nb - 1 - s : s;
+        TA        ac[Q];
+#pragma unroll
+        for (int j = 0; j < Q; ++j)
         {
-            if (tid < 32)
+            ac[j] = an[j];
+        }
+        if (tid < kTvRows)
+        {
+            const int cw = min(kTvRows, n - jb * kTvRows);
+            if (tid < cw && !xn_ok)
             {
                 const uint64_t t0    = global_ns();
                 uint32_t       polls = 0;
-                int            got   = 0;
-                for (;;)
+                while (!tv_read(xll, jb, tid, epoch, xn))
                 {
-                    const int  ss   = s + tid;
-                    const int  jb   = upper ? nb - 1 - ss : ss;
-                    const bool set  = ss < t && ld_acquire_u32(&sync->flags[jb]) != 0;
-                    const unsigned m = __ballot_sync(0xffffffffu, set);
-                    got              = __ffs(~m) - 1;  // leading run of set flags
-                    if (m == 0xffffffffu)
-                    {
-                        got = 32;
-                    }
-                    if (got > 0)
-                    {
-                        break;
-                    }
                     if ((++polls & 255u) == 0 && global_ns() - t0 > kWaitLimitNs)
                     {
-                        if (tid == 0)
-                        {
-                            raise_error(st, DEV_WAIT_TIMEOUT, 20);
-                            s_abort = 1;
-                        }
+                        raise_error(st, DEV_WAIT_TIMEOUT, 20);
+                        s_abort = 1;
                         break;
                     }
                 }
-                if (tid == 0)
-                {
-                    s_ready = s + got;
-                }
             }
-            __syncthreads();
-            if (s_abort)
-            {
-                return;
-            }
-            ready = s_ready;
-        }
-        const int jb = upper ? nb - 1 - s : s;
-        const int c0 = jb * kTvRows;
-        const int cw = min(kTvRows, n - c0);
-        TX*       xs = xst[s & 1];
-        if (tid < kTvRows)
-        {
-            xs[tid] = tid < cw ? __ldcg(x + c0 + tid) : TX(0);
+            xs[s & 1][tid] = tid < cw ? xn : 0.0;
         }
         __syncthreads();
-        if (r < br)
+        if (s_abort)
         {
-            const TA* arow = a + (int64_t)(r0 + r) * lda + c0;
-            const int j0   = q * (kTvRows / 4);
-#pragma unroll 4
-            for (int j = j0; j < j0 + kTvRows / 4; ++j)
+            return;
+        }
+        if (s + 1 < t)
+        {
+            load_a(s + 1, an);
+            if (tid < kTvRows)
             {
-                if (j < cw)
-                {
-                    acc = fma((TX)arow[j], xs[j], acc);
-                }
+                xn_ok = tv_read(xll, upper ? nb - 2 - s : s + 1, tid, epoch, xn);
             }
+        }
+#pragma unroll
+        for (int j = 0; j < Q; ++j)
+        {
+            acc = fma((double)ac[j], xs[s & 1][q * Q + j], acc);
         }
     }
     part[r][q] = acc;
     __syncthreads();
-
-    // ---- diagonal block: one warp, lane owns rows lane and lane + 32
-    if (tid < 32)
+    if (tid < kTvRows)
     {
-        const int lane = tid;
-        TX        v0 = TX(0), v1 = TX(0);
-        if (lane < br)
+        double sum = 0.0;
+#pragma unroll
+        for (int g = 0; g < kTvThreads / kTvRows; ++g)
         {
-            v0 = x[r0 + lane] - (part[lane][0] + part[lane][1] + part[lane][2] + part[lane][3]);
+            sum += part[tid][g];
         }
-        if (lane + 32 < br)
+        vb[tid] = tid < br ? x[r0 + tid] - sum : 0.0;
+    }
+    __syncthreads();
+    if (tid < br)
+    {
+        double v = 0.0;
+#pragma unroll 8
+        for (int c = 0; c < kTvRows; ++c)
         {
-            const int i = lane + 32;
-            v1          = x[r0 + i] - (part[i][0] + part[i][1] + part[i][2] + part[i][3]);
+            v = fma(inv[tid][c], vb[c], v);
         }
-        if (!upper)
-        {
-            for (int p = 0; p < br; ++p)
-            {
-                TX xp;
-                if (p < 32)
-                {
-                    TX mine = v0;
-                    if (!unit && lane == p)
-                    {
-                        mine = v0 / tri[p][p];
-                        v0   = mine;
-                    }
-                    xp = __shfl_sync(0xffffffffu, mine, p);
-                }
-                else
-                {
-                    TX mine = v1;
-                    if (!unit && lane == p - 32)
-                    {
-                        mine = v1 / tri[p][p];
-                        v1   = mine;
-                    }
-                    xp = __shfl_sync(0xffffffffu, mine, p - 32);
-                }
-                if (lane > p && lane < br)
-                {
-                    v0 = fma(-tri[lane][p], xp, v0);
-                }
-                if (lane + 32 > p && lane + 32 < br)
-                {
-                    v1 = fma(-tri[lane + 32][p], xp, v1);
-                }
-            }
-        }
-        else
-        {
-            for (int p = br - 1; p >= 0; --p)
-            {
-                TX xp;
-                if (p < 32)
-                {
-                    TX mine = v0;
-                    if (!unit && lane == p)
-                    {
-                        mine = v0 / tri[p][p];
-                        v0   = mine;
-                    }
-                    xp = __shfl_sync(0xffffffffu, mine, p);
-                }
-                else
-                {
-                    TX mine = v1;
-                    if (!unit && lane == p - 32)
-                    {
-                        mine = v1 / tri[p][p];
-                        v1   = mine;
-                    }
-                    xp = __shfl_sync(0xffffffffu, mine, p - 32);
-                }
-                if (lane < p)
-                {
-                    v0 = fma(-tri[lane][p], xp, v0);
-                }
-                if (lane + 32 < p)
-                {
-                    v1 = fma(-tri[lane + 32][p], xp, v1);
-                }
-            }
-        }
-        if (lane < br)
-        {
-            x[r0 + lane] = v0;
-        }
-        if (lane + 32 < br)
-        {
-            x[r0 + lane + 32] = v1;
-        }
-        __syncwarp();
-        if (lane == 0)
-        {
-            __threadfence();
-            st_release_u32(&sync->flags[blk], 1u);
-        }
+        x[r0 + tid] = v;
+        tv_publish(xll, blk, tid, v, epoch);
     }
 }
 
