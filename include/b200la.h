@@ -212,6 +212,28 @@ B200LA_API int    b200la_dsolve_mixed(const double* a, int64_t n, int64_t nrhs, 
        int64_t ldb, double* x, int64_t ldx, const b200la_refine_options* options,
        b200la_refine_result* result, void* workspace, size_t workspace_bytes, void* stream);
 
+/* ---- batched solver for many small systems of uneven order ----------------
+ * Solves `count` independent systems A_i x_i = b_i, 1 <= n_i <= 512, in ONE
+ * persistent kernel launch (one CTA per system at a time, taken from an
+ * atomic queue in the order given by `order`, NULL = index order; pass the
+ * largest systems first).  Device arrays: sizes[count] (n_i), offsets_a
+ * [count] (element offset of the row-major n_i x n_i matrix in a),
+ * offsets_v[count] (element offset of b_i / x_i), status[count] (refinement
+ * corrections used; 1000 + corrections for a system finished with FP64
+ * factors after its FP32 refinement stalled; -(info) for an exactly singular
+ * U; -1000000 if not converged), backward_error[count].  total_a / total_v: element sizes of a and b.  precision
+ * B200LA_PREC_FP32 (FP32 factors, FP64 refinement to `tolerance`; systems
+ * whose refinement stalls are refactored in FP64 by a second persistent
+ * launch that skips all others) or B200LA_PREC_FP64 (FP64 LU + refinement).  nb_table[8]: panel width per order
+ * bucket of 64 (the autotuner's choice; 16 or 32 for FP32, 16 for FP64).
+ * Asynchronous.  Extension: the reference has no batched solver. */
+B200LA_API size_t b200la_dgesv_batched_workspace_size(int64_t total_a, int64_t total_v, int precision);
+B200LA_API int    b200la_dgesv_batched(int64_t count, const int32_t* sizes, const int64_t* offsets_a,
+       const int64_t* offsets_v, const int32_t* order, const double* a, const double* b, double* x,
+       int64_t total_a, int64_t total_v, int precision, const int32_t* nb_table, int max_iterations,
+       double tolerance, int32_t* status, double* backward_error, void* workspace,
+       size_t workspace_bytes, void* stream);
+
 /* ---- tensor-core update (mixed-precision LU building block) ---------------
  * c[m x n] (fp32, row stride ldc) -= a[m x k] * b[n x k]^T on the tcgen05
  * tensor cores with FP32 accumulation.  a and b are K-major (row stride k
