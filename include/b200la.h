@@ -174,14 +174,17 @@ B200LA_API int    b200la_sgemm(int transpose_a, int transpose_b, int64_t rows, i
  * the tcgen05 tensor cores in the chosen precision with FP32 accumulation,
  * then FP64 refinement (residual, update and test in FP64), switching to
  * GMRES-IR preconditioned by the low-precision factors when plain
- * refinement stalls, and escalating to the next precision (FP32, then plain
- * FP64 LU) when that fails too.  Synchronous (reads the residual norms).
+ * refinement stalls, and escalating to the next precision (FP8 -> BF16;
+ * BF16, FP16, TF32 -> FP32; FP32 -> plain FP64 LU) when that fails too.  Synchronous (reads the residual norms).
  * Extension: the reference has no mixed-precision solver. */
 #define B200LA_PREC_FP64 0 /* plain FP64 LU (the reference's algorithm) + refinement */
 #define B200LA_PREC_FP32 1 /* FP32 factors, three-term TF32 tensor-core updates */
 #define B200LA_PREC_TF32 2 /* FP32 factors, TF32 tensor-core updates */
 #define B200LA_PREC_BF16 3 /* FP32 factors, BF16 tensor-core updates */
 #define B200LA_PREC_FP16 4 /* FP32 factors, FP16 tensor-core updates */
+#define B200LA_PREC_FP8  5 /* FP32 factors, FP8-E4M3 tensor-core updates with
+                              power-of-two scales per row of L21 / column of U12;
+                              escalates to BF16 */
 
 typedef struct b200la_refine_options
 {
@@ -247,6 +250,12 @@ B200LA_API int    b200la_dgesv_batched(int64_t count, const int32_t* sizes, cons
 B200LA_API size_t b200la_tc_update_workspace_size(void);
 B200LA_API int    b200la_sgemm_tc_update(int kind, int split3, float* c, int64_t ldc, int64_t m, int64_t n,
        int64_t k, const void* a, const void* b, const void* a_small, const void* b_small,
+       void* workspace, size_t workspace_bytes, void* stream);
+/* FP8-E4M3 form: c[i][j] -= a_inv_scale[i] * b_inv_scale[j] * sum_k a[i][k] b[j][k]
+ * (tcgen05 kind::f8f6f4, FP32 accumulation); a, b are E4M3 bytes, K-major,
+ * k a multiple of 128. */
+B200LA_API int    b200la_sgemm_tc_update_fp8(float* c, int64_t ldc, int64_t m, int64_t n, int64_t k,
+       const void* a, const void* b, const float* a_inv_scale, const float* b_inv_scale,
        void* workspace, size_t workspace_bytes, void* stream);
 
 #ifdef __cplusplus

@@ -70,11 +70,18 @@ SIGNATURES: dict[str, tuple] = {
                                     _p, _sz, _p]),
     "b200la_tc_update_workspace_size": (_sz, []),
     "b200la_sgemm_tc_update": (_i32, [_i32, _i32, _p, _i64, _i64, _i64, _i64, _p, _p, _p, _p, _p, _sz, _p]),
+    "b200la_sgemm_tc_update_fp8": (_i32, [_p, _i64, _i64, _i64, _i64, _p, _p, _p, _p, _p, _sz, _p]),
+    "b200la_mlp_param_count": (_i32, []),
+    "b200la_mlp_forward": (_i32, [_p, _p, _i64, _p, _p]),
+    "b200la_mlp_gradient": (_i32, [_p, _p, _p, _i64, _p, _p, _p]),
+    "b200la_mlp_adam": (_i32, [_p, _p, _p, _p, _i64, _f, _f, _f, _f, _i32, _f, _p]),
+    "b200la_matrix_features": (_i32, [_p, _i64, _p, _p, _p]),
 }
 
 
-PREC_FP64, PREC_FP32, PREC_TF32, PREC_BF16, PREC_FP16 = 0, 1, 2, 3, 4
-PREC_NAMES = {PREC_FP64: "fp64", PREC_FP32: "fp32", PREC_TF32: "tf32", PREC_BF16: "bf16", PREC_FP16: "fp16"}
+PREC_FP64, PREC_FP32, PREC_TF32, PREC_BF16, PREC_FP16, PREC_FP8 = 0, 1, 2, 3, 4, 5
+PREC_NAMES = {PREC_FP64: "fp64", PREC_FP32: "fp32", PREC_TF32: "tf32", PREC_BF16: "bf16", PREC_FP16: "fp16",
+              PREC_FP8: "fp8"}
 
 
 class RefineOptions(ctypes.Structure):

@@ -183,7 +183,7 @@ def gemm(transpose_a, transpose_b, alpha, a, b, beta, c, stream=None):
 # mixed-precision LU-IR (extension; no reference counterpart)
 # ----------------------------------------------------------------------------
 PRECISIONS = {"fp64": _lib.PREC_FP64, "fp32": _lib.PREC_FP32, "tf32": _lib.PREC_TF32,
-              "bf16": _lib.PREC_BF16, "fp16": _lib.PREC_FP16}
+              "bf16": _lib.PREC_BF16, "fp16": _lib.PREC_FP16, "fp8": _lib.PREC_FP8}
 
 
 def refine_options(precision="fp32", tolerance=1e-14, max_iterations=50, gmres_restart=30, escalate=True):

@@ -8,7 +8,9 @@
 //      U12 = L11^-1 A12 (FP32, k_outer_u12), the operand copies of L21 and
 //      U12^T in the factorization precision, and the trailing update
 //      A22 -= L21 U12 on tcgen05 with FP32 accumulation (k_tc_update).
-//      Precisions: FP32 (three-term TF32 split), TF32, BF16, FP16.
+//      Precisions: FP32 (three-term TF32 split), TF32, BF16, FP16, and
+//      FP8-E4M3 with power-of-two scales per row of L21 and per column of
+//      U12 (each spanning the block's 256-deep reduction).
 //   3. x0 = U^-1 L^-1 P b with the FP32 factors applied in FP64; then
 //      r = b - A x in FP64, eta = ||r|| / (||A|| ||x|| + ||b||) (inf norms),
 //      stop at eta <= tolerance; else d = U^-1 L^-1 P r, x += d.  When plain
@@ -19,6 +21,7 @@
 // FP64 stays on the GPU for the residual, the update and the test.
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
+#include <cuda_fp8.h>
 #include <cuda_runtime.h>
 
 #include <atomic>
@@ -92,6 +95,67 @@ template <> struct OpStore<TC_FP16>
     using type = __half;
     __device__ static __half conv(float x) { return __float2half_rn(x); }
 };
+template <> struct OpStore<TC_FP8>
+{
+    using type = __nv_fp8_storage_t;
+    __device__ static __nv_fp8_storage_t conv(float x) { return __nv_cvt_float_to_fp8(x, __NV_SATFINITE, __NV_E4M3); }
+};
+
+// Power-of-two scale s with amax * s in [128, 256) (E4M3's largest finite
+// value is 448), exponent clamped to the normal float range; 1 for amax 0.
+// Returns s and stores 1/s (exact) in *inv.
+__device__ __forceinline__ float fp8_scale(float amax, float* inv)
+{
+    if (!(amax > 0.f) || !isfinite(amax))
+    {
+        *inv = 1.f;
+        return 1.f;
+    }
+    int e = 0;
+    frexpf(amax, &e);  // amax = f 2^e, f in [0.5, 1)
+    int se = 8 - e;
+    se     = se > 126 ? 126 : (se < -126 ? -126 : se);
+    *inv   = ldexpf(1.f, -se);
+    return ldexpf(1.f, se);
+}
+
+// FP8 L21 operand: a warp per row of rows [r_begin, n) x columns [K, K+256)
+// of A32; the row's scale brings its largest entry into [128, 256).
+__global__ void k_make_l21_fp8(const float* __restrict__ a32, int n, int K, int r_begin,
+    __nv_fp8_storage_t* __restrict__ op, float* __restrict__ inv_scale)
+{
+    const int     lane = threadIdx.x & 31;
+    const int64_t rows = n - r_begin;
+    for (int64_t r = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; r < rows;
+         r += ((int64_t)gridDim.x * blockDim.x) >> 5)
+    {
+        const float* src = a32 + (r_begin + r) * (int64_t)n + K;
+        float        v[kOuterNB / 32];
+        float        amax = 0.f;
+#pragma unroll
+        for (int q = 0; q < kOuterNB / 32; ++q)
+        {
+            v[q] = src[q * 32 + lane];
+            amax = fmaxf(amax, fabsf(v[q]));
+        }
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1)
+        {
+            amax = fmaxf(amax, __shfl_xor_sync(0xffffffffu, amax, off));
+        }
+        float       inv;
+        const float sc = fp8_scale(amax, &inv);
+#pragma unroll
+        for (int q = 0; q < kOuterNB / 32; ++q)
+        {
+            op[r * kOuterNB + q * 32 + lane] = OpStore<TC_FP8>::conv(v[q] * sc);
+        }
+        if (lane == 0)
+        {
+            inv_scale[r] = inv;
+        }
+    }
+}
 
 // L21 operand: rows [r_begin, n) x columns [K, K+256) of A32 -> K-major copy.
 template <int KIND, bool SPLIT>
@@ -118,7 +182,7 @@ __global__ void k_make_l21(const float* __restrict__ a32, int n, int K, int r_be
 constexpr int kOuStrip = 64;
 template <int KIND, bool SPLIT>
 __global__ void __launch_bounds__(256) k_outer_u12(float* __restrict__ a32, int n, int K,
-    typename OpStore<KIND>::type* __restrict__ opT, float* __restrict__ opT_small)
+    typename OpStore<KIND>::type* __restrict__ opT, float* __restrict__ opT_small, float* __restrict__ inv_scale)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     float(*S)[kOuStrip + 1]  = reinterpret_cast<float(*)[kOuStrip + 1]>(smem_raw);  // [256]
@@ -182,6 +246,30 @@ __global__ void __launch_bounds__(256) k_outer_u12(float* __restrict__ a32, int 
             a32[(int64_t)(K + i) * n + col] = S[i][cl];
         }
     }
+    // FP8: power-of-two scale per column (per row of the transposed copy)
+    __shared__ float colsc[kOuStrip];
+    if constexpr (KIND == TC_FP8)
+    {
+        __shared__ float part[4][kOuStrip];
+        float            amax = 0.f;
+        for (int i = rg; i < kOuterNB; i += 4)
+        {
+            amax = fmaxf(amax, fabsf(S[i][cl]));
+        }
+        part[rg][cl] = amax;
+        __syncthreads();
+        if (rg == 0)
+        {
+            amax = fmaxf(fmaxf(part[0][cl], part[1][cl]), fmaxf(part[2][cl], part[3][cl]));
+            float inv;
+            colsc[cl] = fp8_scale(amax, &inv);
+            if (valid)
+            {
+                inv_scale[col - Kend] = inv;
+            }
+        }
+        __syncthreads();
+    }
     // transposed operand copy: row (col - Kend), K index kk
     for (int e = tid; e < kOuStrip * kOuterNB; e += 256)
     {
@@ -189,7 +277,11 @@ __global__ void __launch_bounds__(256) k_outer_u12(float* __restrict__ a32, int 
         const int kk = e % kOuterNB;
         if (c0 + c < n)
         {
-            const float   v   = S[kk][c];
+            float v = S[kk][c];
+            if constexpr (KIND == TC_FP8)
+            {
+                v *= colsc[c];
+            }
             const int64_t idx = (int64_t)(c0 + c - Kend) * kOuterNB + kk;
             opT[idx]          = OpStore<KIND>::conv(v);
             if constexpr (SPLIT)
@@ -369,6 +461,8 @@ struct MixedPlan
     uint64_t*          xll;     // flagged copies of solved blocks (k_trsv_blocks)
     double*            V;       // GMRES basis (m+1) x n
     double*            h;       // GMRES dot products (m+1)
+    float*             l21inv;  // FP8: inverse row scales of L21
+    float*             u12inv;  // FP8: inverse row scales of U12^T
     double*            a64;     // FP64 copy of A for the FP64 fallback
     GetrfPlan<double>  gp64;
     int64_t*           piv64;
@@ -401,6 +495,8 @@ MixedPlan plan_mixed(Arena& a, int64_t n, int64_t nrhs, int restart, bool fp64_f
     p.u12op    = a.next<float>((size_t)n * kOuterNB);
     p.u12small = a.next<float>((size_t)n * kOuterNB);
     p.perm     = a.next<int32_t>((size_t)n);
+    p.l21inv   = a.next<float>((size_t)n);
+    p.u12inv   = a.next<float>((size_t)n);
     p.r        = a.next<double>((size_t)n * nrhs);
     p.y        = a.next<double>((size_t)n * nrhs);
     p.norms    = a.next<unsigned long long>(4 + 3 * kMaxNrhsMixed);
@@ -478,27 +574,32 @@ int enqueue_getrf_mixed(MixedPlan& p, int n, int kind, bool split, cudaStream_t 
         if (kind == TC_TF32 && split)
         {
             k_make_l21<TC_TF32, true><<<grid_for(elems), 256, 0, s>>>(a32, n, K, Kend, (float*)p.l21op, p.l21small);
-            k_outer_u12<TC_TF32, true><<<(rest + kOuStrip - 1) / kOuStrip, 256, outer_u12_smem(), s>>>(a32, n, K, (float*)p.u12op, p.u12small);
+            k_outer_u12<TC_TF32, true><<<(rest + kOuStrip - 1) / kOuStrip, 256, outer_u12_smem(), s>>>(a32, n, K, (float*)p.u12op, p.u12small, nullptr);
         }
         else if (kind == TC_TF32)
         {
             k_make_l21<TC_TF32, false><<<grid_for(elems), 256, 0, s>>>(a32, n, K, Kend, (float*)p.l21op, nullptr);
-            k_outer_u12<TC_TF32, false><<<(rest + kOuStrip - 1) / kOuStrip, 256, outer_u12_smem(), s>>>(a32, n, K, (float*)p.u12op, nullptr);
+            k_outer_u12<TC_TF32, false><<<(rest + kOuStrip - 1) / kOuStrip, 256, outer_u12_smem(), s>>>(a32, n, K, (float*)p.u12op, nullptr, nullptr);
         }
         else if (kind == TC_BF16)
         {
             k_make_l21<TC_BF16, false><<<grid_for(elems), 256, 0, s>>>(a32, n, K, Kend, (__nv_bfloat16*)p.l21op, nullptr);
-            k_outer_u12<TC_BF16, false><<<(rest + kOuStrip - 1) / kOuStrip, 256, outer_u12_smem(), s>>>(a32, n, K, (__nv_bfloat16*)p.u12op, nullptr);
+            k_outer_u12<TC_BF16, false><<<(rest + kOuStrip - 1) / kOuStrip, 256, outer_u12_smem(), s>>>(a32, n, K, (__nv_bfloat16*)p.u12op, nullptr, nullptr);
+        }
+        else if (kind == TC_FP16)
+        {
+            k_make_l21<TC_FP16, false><<<grid_for(elems), 256, 0, s>>>(a32, n, K, Kend, (__half*)p.l21op, nullptr);
+            k_outer_u12<TC_FP16, false><<<(rest + kOuStrip - 1) / kOuStrip, 256, outer_u12_smem(), s>>>(a32, n, K, (__half*)p.u12op, nullptr, nullptr);
         }
         else
         {
-            k_make_l21<TC_FP16, false><<<grid_for(elems), 256, 0, s>>>(a32, n, K, Kend, (__half*)p.l21op, nullptr);
-            k_outer_u12<TC_FP16, false><<<(rest + kOuStrip - 1) / kOuStrip, 256, outer_u12_smem(), s>>>(a32, n, K, (__half*)p.u12op, nullptr);
+            k_make_l21_fp8<<<grid_for((int64_t)rest * 32), 256, 0, s>>>(a32, n, K, Kend, (__nv_fp8_storage_t*)p.l21op, p.l21inv);
+            k_outer_u12<TC_FP8, false><<<(rest + kOuStrip - 1) / kOuStrip, 256, outer_u12_smem(), s>>>(a32, n, K, (__nv_fp8_storage_t*)p.u12op, nullptr, p.u12inv);
         }
         prof_end(KC_PREP, s);
         B200LA_LAUNCH_CHECK();
         if ((rc = enqueue_tc_update(kind, split, ma, mb, mas, mbs, a32 + (int64_t)Kend * n + Kend, n, rest, rest,
-                 kOuterNB, p.gp.st, s)) != B200LA_SUCCESS)
+                 kOuterNB, p.gp.st, s, p.l21inv, p.u12inv)) != B200LA_SUCCESS)
             return rc;
     }
     k_status_finish<<<1, 32, 0, s>>>(p.gp.st);
@@ -519,6 +620,7 @@ int set_mixed_attributes()
     B200LA_CUDA(cudaFuncSetAttribute(k_outer_u12<TC_TF32, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)outer_u12_smem()));
     B200LA_CUDA(cudaFuncSetAttribute(k_outer_u12<TC_BF16, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)outer_u12_smem()));
     B200LA_CUDA(cudaFuncSetAttribute(k_outer_u12<TC_FP16, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)outer_u12_smem()));
+    B200LA_CUDA(cudaFuncSetAttribute(k_outer_u12<TC_FP8, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)outer_u12_smem()));
     if (dev >= 0 && dev < 64)
         done[dev] = true;
     return B200LA_SUCCESS;
@@ -764,7 +866,7 @@ B200LA_API int b200la_dsolve_mixed(const double* a, int64_t n, int64_t nrhs, con
     if (n <= 0 || nrhs <= 0 || nrhs > kMaxNrhsMixed || ldb < nrhs || ldx < nrhs || n > 65536)
         return set_error(B200LA_INVALID_ARGUMENT, "dsolve_mixed: invalid sizes (n %lld, nrhs %lld; nrhs <= %d)",
             (long long)n, (long long)nrhs, kMaxNrhsMixed);
-    if (o->precision < B200LA_PREC_FP64 || o->precision > B200LA_PREC_FP16 || o->max_iterations < 1 ||
+    if (o->precision < B200LA_PREC_FP64 || o->precision > B200LA_PREC_FP8 || o->max_iterations < 1 ||
         !(o->tolerance > 0))
         return set_error(B200LA_INVALID_ARGUMENT, "dsolve_mixed: invalid options");
     const size_t need = b200la_dsolve_mixed_workspace_size(n, nrhs, o);
@@ -805,7 +907,10 @@ B200LA_API int b200la_dsolve_mixed(const double* a, int64_t n, int64_t nrhs, con
     for (;;)
     {
         const bool use64 = precision == B200LA_PREC_FP64;
-        const int  kind  = precision == B200LA_PREC_BF16 ? TC_BF16 : (precision == B200LA_PREC_FP16 ? TC_FP16 : TC_TF32);
+        const int  kind  = precision == B200LA_PREC_BF16   ? TC_BF16
+                           : precision == B200LA_PREC_FP16 ? TC_FP16
+                           : precision == B200LA_PREC_FP8  ? TC_FP8
+                                                           : TC_TF32;
         const bool split = precision == B200LA_PREC_FP32;
         cudaEventRecord(e0, s);
         DeviceStatus* st = use64 ? p.gp64.st : p.gp.st;
@@ -926,8 +1031,11 @@ B200LA_API int b200la_dsolve_mixed(const double* a, int64_t n, int64_t nrhs, con
         out.converged      = converged ? 1 : 0;
         if (converged || !o->escalate || precision == B200LA_PREC_FP64)
             break;
-        // escalate: low precisions -> FP32 (three-term TF32) -> FP64
-        precision = (precision == B200LA_PREC_FP32) ? B200LA_PREC_FP64 : B200LA_PREC_FP32;
+        // escalate: FP8 -> BF16; other low precisions -> FP32 (three-term
+        // TF32) -> FP64
+        precision = precision == B200LA_PREC_FP8    ? B200LA_PREC_BF16
+                    : precision == B200LA_PREC_FP32 ? B200LA_PREC_FP64
+                                                    : B200LA_PREC_FP32;
         ++escalations;
     }
     out.escalations = escalations;

@@ -66,10 +66,11 @@ int make_kmajor_map(CUtensorMap* map, const void* base, int kind, int64_t rows, 
     {
         return set_error(B200LA_CUDA_ERROR, "cuTensorMapEncodeTiled is not available");
     }
-    const int                elem  = kind == TC_TF32 ? 4 : 2;
-    const CUtensorMapDataType dt   = kind == TC_TF32 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32
+    const int                elem  = tc_elem_bytes(kind);
+    const CUtensorMapDataType dt   = kind == TC_TF32   ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32
                                     : kind == TC_BF16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16
-                                                      : CU_TENSOR_MAP_DATA_TYPE_FLOAT16;
+                                    : kind == TC_FP16 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT16
+                                                      : CU_TENSOR_MAP_DATA_TYPE_UINT8;
     if ((reinterpret_cast<uintptr_t>(base) & 15) != 0 || (ld * elem) % 16 != 0)
     {
         return set_error(B200LA_INVALID_ARGUMENT, "tensor-core operand not 16-byte aligned");
@@ -90,7 +91,8 @@ int make_kmajor_map(CUtensorMap* map, const void* base, int kind, int64_t rows, 
 
 template <int KIND, bool SPLIT3>
 static int launch_tc(const CUtensorMap& a, const CUtensorMap& b, const CUtensorMap& as, const CUtensorMap& bs,
-    float* c, int64_t ldc, int m, int n, int k, DeviceStatus* st, cudaStream_t s)
+    float* c, int64_t ldc, int m, int n, int k, DeviceStatus* st, const float* inv_sa, const float* inv_sb,
+    cudaStream_t s)
 {
     int rc = set_attr_once<KIND, SPLIT3>();
     if (rc != B200LA_SUCCESS)
@@ -99,28 +101,30 @@ static int launch_tc(const CUtensorMap& a, const CUtensorMap& b, const CUtensorM
     }
     dim3 grid((n + kTcBN - 1) / kTcBN, (m + kTcBM - 1) / kTcBM);
     prof_begin(KC_MIXED, s);
-    k_tc_update<KIND, SPLIT3><<<grid, 128, tc_smem_bytes<SPLIT3>(), s>>>(a, b, as, bs, c, ldc, m, n, k, st);
+    k_tc_update<KIND, SPLIT3><<<grid, 128, tc_smem_bytes<SPLIT3>(), s>>>(a, b, as, bs, c, ldc, m, n, k, st, inv_sa,
+        inv_sb);
     prof_end(KC_MIXED, s);
     B200LA_LAUNCH_CHECK();
     return B200LA_SUCCESS;
 }
 
 int enqueue_tc_update(int kind, bool split3, const CUtensorMap& a, const CUtensorMap& b, const CUtensorMap& as,
-    const CUtensorMap& bs, float* c, int64_t ldc, int m, int n, int k, DeviceStatus* st, cudaStream_t s)
+    const CUtensorMap& bs, float* c, int64_t ldc, int m, int n, int k, DeviceStatus* st, cudaStream_t s,
+    const float* inv_sa, const float* inv_sb)
 {
     if (m <= 0 || n <= 0)
     {
         return B200LA_SUCCESS;
     }
-    const int ea = kTcAtomBytes / (kind == TC_TF32 ? 4 : 2);
+    const int ea = kTcAtomBytes / tc_elem_bytes(kind);
     if (k <= 0 || k % ea != 0)
     {
         return set_error(B200LA_INVALID_ARGUMENT, "tensor-core update: depth %d is not a multiple of %d", k, ea);
     }
     if (kind == TC_TF32)
     {
-        return split3 ? launch_tc<TC_TF32, true>(a, b, as, bs, c, ldc, m, n, k, st, s)
-                      : launch_tc<TC_TF32, false>(a, b, as, bs, c, ldc, m, n, k, st, s);
+        return split3 ? launch_tc<TC_TF32, true>(a, b, as, bs, c, ldc, m, n, k, st, nullptr, nullptr, s)
+                      : launch_tc<TC_TF32, false>(a, b, as, bs, c, ldc, m, n, k, st, nullptr, nullptr, s);
     }
     if (split3)
     {
@@ -128,9 +132,17 @@ int enqueue_tc_update(int kind, bool split3, const CUtensorMap& a, const CUtenso
     }
     if (kind == TC_BF16)
     {
-        return launch_tc<TC_BF16, false>(a, b, as, bs, c, ldc, m, n, k, st, s);
+        return launch_tc<TC_BF16, false>(a, b, as, bs, c, ldc, m, n, k, st, nullptr, nullptr, s);
     }
-    return launch_tc<TC_FP16, false>(a, b, as, bs, c, ldc, m, n, k, st, s);
+    if (kind == TC_FP8)
+    {
+        if (inv_sa == nullptr || inv_sb == nullptr)
+        {
+            return set_error(B200LA_INVALID_ARGUMENT, "tensor-core update: FP8 operands need their scales");
+        }
+        return launch_tc<TC_FP8, false>(a, b, as, bs, c, ldc, m, n, k, st, inv_sa, inv_sb, s);
+    }
+    return launch_tc<TC_FP16, false>(a, b, as, bs, c, ldc, m, n, k, st, nullptr, nullptr, s);
 }
 
 }  // namespace b200la
@@ -180,3 +192,38 @@ extern "C" B200LA_API int b200la_sgemm_tc_update(int kind, int split3, float* c,
 }
 
 extern "C" B200LA_API size_t b200la_tc_update_workspace_size(void) { return sizeof(DeviceStatus); }
+
+extern "C" B200LA_API int b200la_sgemm_tc_update_fp8(float* c, int64_t ldc, int64_t m, int64_t n, int64_t k,
+    const void* a, const void* b, const float* a_inv_scale, const float* b_inv_scale, void* workspace,
+    size_t workspace_bytes, void* stream)
+{
+    if (c == nullptr || a == nullptr || b == nullptr || a_inv_scale == nullptr || b_inv_scale == nullptr)
+    {
+        return set_error(B200LA_INVALID_ARGUMENT, "tc_update_fp8: null operand");
+    }
+    if (m <= 0 || n <= 0 || k <= 0 || ldc < n || m > INT_MAX / 2 || n > INT_MAX / 2 || k > INT_MAX / 2)
+    {
+        return set_error(B200LA_INVALID_ARGUMENT, "tc_update_fp8: invalid sizes");
+    }
+    if (workspace == nullptr || workspace_bytes < sizeof(DeviceStatus))
+    {
+        return set_error(B200LA_WORKSPACE_TOO_SMALL, "tc_update_fp8: needs %zu bytes of workspace",
+            sizeof(DeviceStatus));
+    }
+    int rc = require_sm100();
+    if (rc != B200LA_SUCCESS)
+    {
+        return rc;
+    }
+    CUtensorMap ma, mb;
+    if ((rc = make_kmajor_map(&ma, a, TC_FP8, m, k, k, kTcBM)) != B200LA_SUCCESS ||
+        (rc = make_kmajor_map(&mb, b, TC_FP8, n, k, k, kTcBN)) != B200LA_SUCCESS)
+    {
+        return rc;
+    }
+    cudaStream_t s  = static_cast<cudaStream_t>(stream);
+    auto*        st = static_cast<DeviceStatus*>(workspace);
+    B200LA_CUDA(cudaMemsetAsync(st, 0, sizeof(DeviceStatus), s));
+    return enqueue_tc_update(TC_FP8, false, ma, mb, ma, mb, c, ldc, (int)m, (int)n, (int)k, st, s, a_inv_scale,
+        b_inv_scale);
+}

@@ -13,7 +13,9 @@ namespace b200la
 int make_kmajor_map(CUtensorMap* map, const void* base, int kind, int64_t rows, int64_t k, int64_t ld,
     int box_rows);
 
-// C[m x n] -= A B^T on the tensor cores (see k_tc_update).
+// C[m x n] -= A B^T on the tensor cores (see k_tc_update).  FP8 operands
+// need the inverse power-of-two scales of their rows (inv_sa[m], inv_sb[n]).
 int enqueue_tc_update(int kind, bool split3, const CUtensorMap& a, const CUtensorMap& b, const CUtensorMap& as,
-    const CUtensorMap& bs, float* c, int64_t ldc, int m, int n, int k, DeviceStatus* st, cudaStream_t s);
+    const CUtensorMap& bs, float* c, int64_t ldc, int m, int n, int k, DeviceStatus* st, cudaStream_t s,
+    const float* inv_sa = nullptr, const float* inv_sb = nullptr);
 }  // namespace b200la

@@ -3,7 +3,11 @@
 //     C[M x N] (fp32, row-major, ldc)  -=  A[M x K] * B[N x K]^T
 //
 // A and B are K-major operand copies (row stride K elements) in TF32 (fp32
-// containers), BF16 or FP16.  One CTA computes one 128 x 256 tile of C:
+// containers), BF16, FP16 or FP8-E4M3.  FP8 operands carry power-of-two
+// scales, one per row of A and one per row of B (a row spans the whole K
+// depth, so the scale is constant along the reduction); the epilogue applies
+// C -= inv_sa[row] * inv_sb[col] * acc.  One CTA computes one 128 x 256 tile
+// of C:
 //   * warp 0 / lane 0 issues TMA loads of 128-byte-wide K slices of A and B
 //     (128B swizzle) into a ring of shared-memory stages, completing on
 //     mbarriers;
@@ -37,7 +41,8 @@ enum TcKind : int
 {
     TC_TF32 = 0,
     TC_BF16 = 1,
-    TC_FP16 = 2
+    TC_FP16 = 2,
+    TC_FP8  = 3   // E4M3, kind::f8f6f4
 };
 
 constexpr int kTcBM        = 128;
@@ -63,6 +68,17 @@ template <> struct TcTraits<TC_FP16>
     static constexpr int      elem = 2;
     static constexpr uint32_t fmt  = 0;  // F16
 };
+
+template <> struct TcTraits<TC_FP8>
+{
+    static constexpr int      elem = 1;
+    static constexpr uint32_t fmt  = 0;  // E4M3 (kind::f8f6f4 encoding)
+};
+
+__host__ __device__ constexpr int tc_elem_bytes(int kind)
+{
+    return kind == TC_TF32 ? 4 : (kind == TC_FP8 ? 1 : 2);
+}
 
 template <bool SPLIT3> constexpr int tc_stages() { return SPLIT3 ? 2 : 4; }
 template <bool SPLIT3> constexpr int tc_stage_bytes() { return SPLIT3 ? 2 * kTcPair : kTcPair; }
@@ -142,6 +158,14 @@ __device__ __forceinline__ void tc_mma(uint32_t tmem_d, uint64_t adesc, uint64_t
             "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
             : "memory");
     }
+    else if constexpr (KIND == TC_FP8)
+    {
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::1.kind::f8f6f4 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem_d),
+            "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
+            : "memory");
+    }
     else
     {
         asm volatile(
@@ -211,7 +235,7 @@ template <int KIND, bool SPLIT3>
 __global__ void __launch_bounds__(128, 1) k_tc_update(const __grid_constant__ CUtensorMap tmA,
     const __grid_constant__ CUtensorMap tmB, const __grid_constant__ CUtensorMap tmAs,
     const __grid_constant__ CUtensorMap tmBs, float* __restrict__ C, int64_t ldc, int M, int N, int K,
-    DeviceStatus* __restrict__ st)
+    DeviceStatus* __restrict__ st, const float* __restrict__ inv_sa, const float* __restrict__ inv_sb)
 {
     constexpr int S   = tc_stages<SPLIT3>();
     constexpr int SB  = tc_stage_bytes<SPLIT3>();
@@ -367,6 +391,15 @@ __global__ void __launch_bounds__(128, 1) k_tc_update(const __grid_constant__ CU
             if (!row_ok)
             {
                 continue;
+            }
+            if constexpr (KIND == TC_FP8)
+            {
+                const float ra = inv_sa[r];
+#pragma unroll
+                for (int q = 0; q < 32; ++q)
+                {
+                    v[q] *= ra * (c0 + q < N ? inv_sb[c0 + q] : 0.f);
+                }
             }
             if (fast)
             {

@@ -22,7 +22,7 @@ def eta_of(a, x, b):
     return np.abs(r).max() / (np.abs(a).sum(1).max() * np.abs(x).max() + np.abs(b).max())
 
 
-@pytest.mark.parametrize("precision", ["fp32", "tf32", "bf16", "fp16"])
+@pytest.mark.parametrize("precision", ["fp32", "tf32", "bf16", "fp16", "fp8"])
 @pytest.mark.parametrize("n", [300, 1100])
 def test_mixed_reaches_fp64_accuracy(port, precision, n):
     a, x_true, b = system(n, seed=70 + n)
@@ -80,3 +80,28 @@ def test_mixed_singular_reports_info():
     b = np.ones(130)
     x, res, st = la.solve_mixed(dev(a), dev(b), precision="fp32", escalate=False)
     assert st == la._lib.SINGULAR and res["info"] == 78
+
+
+def test_mixed_fp8_well_conditioned_without_escalation():
+    """FP8-E4M3 updates (per-row / per-column power-of-two scales) on a
+    well-conditioned system: GMRES-IR on the FP8-updated factors converges
+    to FP64 accuracy without leaving FP8."""
+    n = 1024
+    a = conditioned(n, 1e1, seed=11)
+    b = a @ np.random.default_rng(2).uniform(-1, 1, n)
+    x, res, st = la.solve_mixed(dev(a), dev(b), precision="fp8", escalate=False)
+    torch.cuda.synchronize()
+    assert st == 0 and res["converged"] == 1 and res["precision_used"] == la._lib.PREC_FP8, res
+    assert eta_of(a, x.cpu().numpy(), b) <= 1e-14
+
+
+def test_mixed_fp8_escalation_chain_reaches_fp64():
+    """kappa = 1e12 defeats every low precision: FP8 -> BF16 -> FP32 -> FP64."""
+    n = 512
+    a = conditioned(n, 1e12, seed=11)
+    b = a @ np.random.default_rng(3).uniform(-1, 1, n)
+    x, res, st = la.solve_mixed(dev(a), dev(b), precision="fp8", max_iterations=10)
+    torch.cuda.synchronize()
+    assert st == 0 and res["converged"] == 1, res
+    assert res["precision_used"] == la._lib.PREC_FP64 and res["escalations"] == 3, res
+    assert eta_of(a, x.cpu().numpy(), b) <= 1e-14

@@ -67,3 +67,49 @@ def test_tc_update_rejects_bad_depth():
     st = lib.b200la_sgemm_tc_update(BF16, 0, p.data_ptr(), 8, 8, 8, 40, p.data_ptr(), p.data_ptr(), None, None,
                                     ws.data_ptr(), 256, None)
     assert st == _lib.INVALID_ARGUMENT
+
+
+def pow2_row_scales(x: torch.Tensor):
+    """Per-row power-of-two scale s with max|row| * s in [128, 256)."""
+    amax = x.abs().amax(dim=1).clamp_min(1e-30)
+    e = torch.frexp(amax).exponent
+    s = torch.ldexp(torch.ones_like(amax), (8 - e).clamp(-126, 126))
+    return s, 1.0 / s
+
+
+@pytest.mark.parametrize("m,n,k", [(128, 128, 128), (300, 200, 256), (1000, 520, 384)])
+def test_tc_update_fp8_matches_reference(m, n, k):
+    """E4M3 operands with per-row power-of-two scales: the kernel's result
+    equals c - (inv_sa a)(inv_sb b)^T of the same E4M3 values up to FP32
+    accumulation rounding."""
+    lib = _lib.load()
+    g = torch.Generator(device="cuda").manual_seed(7)
+    a32 = torch.randn(m, k, device="cuda", generator=g) * torch.logspace(-3, 3, m, device="cuda")[:, None]
+    b32 = torch.randn(n, k, device="cuda", generator=g)
+    c = torch.randn(m, n, device="cuda", generator=g)
+    c0 = c.clone()
+    sa, ia = pow2_row_scales(a32)
+    sb, ib = pow2_row_scales(b32)
+    a8 = (a32 * sa[:, None]).to(torch.float8_e4m3fn)
+    b8 = (b32 * sb[:, None]).to(torch.float8_e4m3fn)
+    ws = torch.empty(lib.b200la_tc_update_workspace_size(), dtype=torch.uint8, device="cuda")
+    st = lib.b200la_sgemm_tc_update_fp8(c.data_ptr(), n, m, n, k, a8.data_ptr(), b8.data_ptr(),
+                                        ia.contiguous().data_ptr(), ib.contiguous().data_ptr(),
+                                        ws.data_ptr(), ws.numel(), torch.cuda.current_stream().cuda_stream)
+    _lib.check(st)
+    torch.cuda.synchronize()
+    ad = a8.double() * ia.double()[:, None]
+    bd = b8.double() * ib.double()[:, None]
+    ref = c0.double() - ad @ bd.T
+    scale = (ad.abs() @ bd.abs().T) + c0.double().abs()
+    rel = ((c.double() - ref).abs() / scale.clamp_min(1e-300)).max().item()
+    assert rel <= 4 * k * 2.0 ** -24, rel
+
+
+def test_tc_update_fp8_rejects_missing_scales():
+    lib = _lib.load()
+    p = torch.empty(4096, device="cuda")
+    ws = torch.empty(256, dtype=torch.uint8, device="cuda")
+    st = lib.b200la_sgemm_tc_update_fp8(p.data_ptr(), 8, 8, 8, 128, p.data_ptr(), p.data_ptr(), None,
+                                        p.data_ptr(), ws.data_ptr(), 256, None)
+    assert st == _lib.INVALID_ARGUMENT
