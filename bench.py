@@ -214,7 +214,7 @@ def cpu_model():
 # B200 arm
 # ---------------------------------------------------------------------------
 CLASS_NAMES = {0: "panel", 1: "laswp_u12", 2: "trailing_simt", 3: "solve", 4: "gemm", 5: "tc_update",
-               6: "residual", 7: "batched", 8: "operand_prep"}
+               6: "residual", 7: "batched", 8: "operand_prep", 9: "selector"}
 
 
 def algorithmic_work(n: int, method: str, nb_out: int = 256):

@@ -60,7 +60,8 @@ B200LA_API int64_t b200la_launch_count(void);
  * class in `class_mask` (bit 0 panel, 1 row interchange + U12 solve,
  * 2 trailing update, 3 triangular solves, 4 general GEMM, 5 mixed-precision
  * factorization GEMM, 6 FP64 residual, 7 batched solver, 8 mixed-precision
- * operand preparation and outer U12 solve) is bracketed by a
+ * operand preparation and outer U12 solve, 9 precision selector: network
+ * and matrix statistics) is bracketed by a
  * pair of CUDA events on its stream.  b200la_profile_stop synchronizes those
  * events and returns the summed device time (ms) and launch count of one
  * class; it also stops recording. */
@@ -214,6 +215,65 @@ B200LA_API size_t b200la_dsolve_mixed_workspace_size(int64_t n, int64_t nrhs,
 B200LA_API int    b200la_dsolve_mixed(const double* a, int64_t n, int64_t nrhs, const double* b,
        int64_t ldb, double* x, int64_t ldx, const b200la_refine_options* options,
        b200la_refine_result* result, void* workspace, size_t workspace_bytes, void* stream);
+
+/* ---- learned precision selector --------------------------------------------
+ * Extension: the reference has no precision selection.
+ *
+ * Network: 12 -> 64 -> 64 -> 4 MLP, ReLU, softmax over the classes
+ * {FP8, BF16, FP32, FP64}, FP32.  params: b200la_mlp_param_count() = 5252
+ * floats, W1[12][64] b1[64] W2[64][64] b2[64] W3[64][4] b3[4] (row-major,
+ * y = x W + b), device memory.  x: batch x 12 standardized features.
+ *   mlp_forward:  probs[batch][4] = softmax(net(x)).
+ *   mlp_gradient: grads[5252] += d/dparams of the summed cross-entropy
+ *                 against labels[batch] (0..3); *loss_sum += summed loss
+ *                 (device float).  Forward and backward in one kernel.
+ *   mlp_adam:     one Adam step on grads / batch (+ weight_decay * params),
+ *                 step counted from 1; clears grads.
+ * All asynchronous on `stream`. */
+B200LA_API int b200la_mlp_param_count(void);
+B200LA_API int b200la_mlp_forward(const float* params, const float* x, int64_t batch, float* probs,
+       void* stream);
+B200LA_API int b200la_mlp_gradient(const float* params, const float* x, const int32_t* labels,
+       int64_t batch, float* grads, float* loss_sum, void* stream);
+B200LA_API int b200la_mlp_adam(float* params, float* grads, float* m1, float* m2, int64_t batch,
+       float lr, float beta1, float beta2, float eps, int step, float weight_decay, void* stream);
+
+/* Matrix statistics behind the features: sixteen 64-bit words at `out`
+ * (device).  With `a` (n x n FP64, row-major, lda = n) the words are reset
+ * and A's statistics gathered: [0] ||A||_inf, [1] max|a_ij|, [2] sum a_ij^2,
+ * [3] max_i 1/(1+r_i) with r_i = |a_ii| / sum_{j!=i}|a_ij|, [4] number of
+ * rows with r_i >= 1 (integer), [5] ||A||_1, [7] min|a_ii|, [8] max|a_ii|,
+ * [9] sum|a_ij| (doubles as bit patterns).  With `lu32` (FP32 LU factors,
+ * row-major n x n) words [6] max|u_ij|, [10] min|u_ii|, [11] max|u_ii| are
+ * added.  Asynchronous. */
+B200LA_API int b200la_matrix_stats(const double* a, int64_t n, const float* lu32, unsigned long long* out,
+       void* stream);
+
+/* The 12 selector features of A (host floats): log2(n)/12; log10 of
+ * ||A||_inf/max|a|, ||A||_1/max|a|, ||A||_F/(n max|a|), mean|a|/max|a|;
+ * log10(min_i r_i)/4; fraction of diagonally dominant rows;
+ * log10(min|a_ii|/max|a|)/4; log10(max|a_ii|/max|a|); log10 of the growth
+ * max|u_ij|/max|a|; log10 of the 1-norm condition estimate
+ * ||A||_1 est(||A^-1||_1)/4 (Hager's estimator with Higham's refinements on
+ * one FP32 LU of A, three-term TF32 updates); log10(min|u_ii|/max|u_ii|)/4.
+ * Workspace: b200la_dsolve_mixed_workspace_size(n, 1, NULL).  *info: the
+ * FP32 LU's info.  Synchronous. */
+B200LA_API int b200la_selector_features(const double* a, int64_t n, float* features, int* info,
+       void* workspace, size_t workspace_bytes, void* stream);
+
+/* Solve A x = b (one right-hand side) with the precision the network picks
+ * from the features above: `params` (device) holds the 5252 weights followed
+ * by 24 floats, the features' mean[12] and inverse standard deviation[12].
+ * Predicted FP8, BF16 or FP32: refinement with the FP32 factors computed for
+ * the features; predicted FP64: plain FP64 LU and refinement.  Refinement
+ * failure escalates up to FP64 as in b200la_dsolve_mixed, so the accuracy
+ * never depends on the prediction.  options->precision and ->escalate are
+ * ignored.  *predicted: B200LA_PREC_* of the network's class; features: the
+ * 12 features (host, may be NULL).  Workspace as b200la_dsolve_mixed with
+ * nrhs = 1.  Synchronous. */
+B200LA_API int b200la_dsolve_selected(const double* a, int64_t n, const double* b, double* x,
+       const float* params, const b200la_refine_options* options, b200la_refine_result* result,
+       int* predicted, float* features, void* workspace, size_t workspace_bytes, void* stream);
 
 /* ---- batched solver for many small systems of uneven order ----------------
  * Solves `count` independent systems A_i x_i = b_i, 1 <= n_i <= 512, in ONE

@@ -129,7 +129,8 @@ enum KernelClass : int
     KC_RESIDUAL = 6,
     KC_BATCHED  = 7,
     KC_PREP     = 8,
-    KC_COUNT    = 9
+    KC_SELECT   = 9,
+    KC_COUNT    = 10
 };
 
 // Host helpers shared by the entry points (defined in runtime.cu).

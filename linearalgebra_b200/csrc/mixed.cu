@@ -461,6 +461,7 @@ struct MixedPlan
     uint64_t*          xll;     // flagged copies of solved blocks (k_trsv_blocks)
     double*            V;       // GMRES basis (m+1) x n
     double*            h;       // GMRES dot products (m+1)
+    float*             sel;     // selector network input (12) and output (4)
     float*             l21inv;  // FP8: inverse row scales of L21
     float*             u12inv;  // FP8: inverse row scales of U12^T
     double*            a64;     // FP64 copy of A for the FP64 fallback
@@ -495,11 +496,12 @@ MixedPlan plan_mixed(Arena& a, int64_t n, int64_t nrhs, int restart, bool fp64_f
     p.u12op    = a.next<float>((size_t)n * kOuterNB);
     p.u12small = a.next<float>((size_t)n * kOuterNB);
     p.perm     = a.next<int32_t>((size_t)n);
+    p.sel      = a.next<float>(64);
     p.l21inv   = a.next<float>((size_t)n);
     p.u12inv   = a.next<float>((size_t)n);
     p.r        = a.next<double>((size_t)n * nrhs);
     p.y        = a.next<double>((size_t)n * nrhs);
-    p.norms    = a.next<unsigned long long>(4 + 3 * kMaxNrhsMixed);
+    p.norms    = a.next<unsigned long long>(4 + 3 * kMaxNrhsMixed + 16);
     p.tsync    = reinterpret_cast<TrsvSync*>(a.next<int32_t>(32 + (size_t)(n + kTvRows - 1) / kTvRows + 32));
     p.dinv     = a.next<double>((size_t)((n + kTvRows - 1) / kTvRows) * 2 * kTvRows * kTvRows);
     p.xll      = a.next<uint64_t>((size_t)((n + kTvRows - 1) / kTvRows) * kTvRows * 2);
@@ -819,6 +821,371 @@ int gmres_correction(const double* a, int64_t lda, const TA* lu, int n, int rest
     return B200LA_SUCCESS;
 }
 
+
+// ---------------------------------------------------------------------------
+// factor / refine steps shared by the mixed and the selected solves
+// ---------------------------------------------------------------------------
+struct SolveState
+{
+    double              anorm      = 0.0;
+    bool                have_anorm = false;
+    std::vector<double> bnorm;
+};
+
+// Factor A in `precision` into p.a32 (or p.a64 for FP64), with p.perm and the
+// inverted diagonal blocks; *info = LAPACK info.  Adds the device time to
+// out.factor_ms.  Reads ||A|| and ||b_j|| the first time.
+int mixed_factor(const double* a, int nn, int nr, int precision, MixedPlan& p, SolveState& ss, int* info,
+    b200la_refine_result& out, cudaEvent_t e0, cudaEvent_t e1, cudaStream_t s)
+{
+    const int64_t n     = nn;
+    const bool    use64 = precision == B200LA_PREC_FP64;
+    const int     kind  = precision == B200LA_PREC_BF16   ? TC_BF16
+                          : precision == B200LA_PREC_FP16 ? TC_FP16
+                          : precision == B200LA_PREC_FP8  ? TC_FP8
+                                                          : TC_TF32;
+    const bool    split = precision == B200LA_PREC_FP32;
+    int           rc    = B200LA_SUCCESS;
+    cudaEventRecord(e0, s);
+    DeviceStatus* st = use64 ? p.gp64.st : p.gp.st;
+    if (!use64)
+    {
+        k_convert_a<<<(nn * 32 + 255) / 256, 256, 0, s>>>(a, n, p.a32, nn, p.norms);
+        B200LA_LAUNCH_CHECK();
+        if ((rc = enqueue_getrf_mixed(p, nn, kind, split, s)) != B200LA_SUCCESS)
+            return rc;
+        k_perm_from_pivots<0><<<1, 256, perm_smem_bytes(nn), s>>>(p.piv, nn, p.perm, perm_smem_bytes(nn) > 0 ? 1 : 0, st, nullptr);
+    }
+    else
+    {
+        B200LA_CUDA(cudaMemcpy2DAsync(p.a64, sizeof(double) * n, a, sizeof(double) * n, sizeof(double) * n, n,
+            cudaMemcpyDeviceToDevice, s));
+        if (!ss.have_anorm)
+        {
+            k_convert_a<<<(nn * 32 + 255) / 256, 256, 0, s>>>(a, n, p.a32, nn, p.norms);
+            B200LA_LAUNCH_CHECK();
+        }
+        if ((rc = enqueue_getrf<double>(p.a64, nn, p.piv64, p.gp64, s)) != B200LA_SUCCESS)
+            return rc;
+        k_perm_from_pivots<0><<<1, 256, perm_smem_bytes(nn), s>>>(p.piv64, nn, p.perm, perm_smem_bytes(nn) > 0 ? 1 : 0, st, nullptr);
+    }
+    B200LA_LAUNCH_CHECK();
+    {
+        const int nbk = (nn + kTvRows - 1) / kTvRows;
+        prof_begin(KC_SOLVE, s);
+        if (use64)
+            k_invert_diag_blocks<double><<<dim3(nbk, 2), kTvRows, 0, s>>>(p.a64, n, nn, p.dinv);
+        else
+            k_invert_diag_blocks<float><<<dim3(nbk, 2), kTvRows, 0, s>>>(p.a32, n, nn, p.dinv);
+        prof_end(KC_SOLVE, s);
+        B200LA_LAUNCH_CHECK();
+    }
+    *info = 0;
+    if ((rc = read_status(st, info, s)) < 0)
+        return rc;
+    cudaEventRecord(e1, s);
+    cudaEventSynchronize(e1);
+    float fms = 0;
+    cudaEventElapsedTime(&fms, e0, e1);
+    out.factor_ms += fms;
+    out.info = *info;
+    if (!ss.have_anorm)
+    {
+        unsigned long long hb[1 + kMaxNrhsMixed];
+        B200LA_CUDA(cudaMemcpy(hb, p.norms, sizeof(unsigned long long), cudaMemcpyDeviceToHost));
+        memcpy(&ss.anorm, &hb[0], 8);
+        B200LA_CUDA(cudaMemcpy(hb + 1, p.norms + 4 + 2 * kMaxNrhsMixed, sizeof(unsigned long long) * nr,
+            cudaMemcpyDeviceToHost));
+        ss.bnorm.assign(nr, 0.0);
+        for (int j = 0; j < nr; ++j)
+            memcpy(&ss.bnorm[j], &hb[1 + j], 8);
+        ss.have_anorm = true;
+    }
+    return B200LA_SUCCESS;
+}
+
+// x0 = M^-1 b with the factors of `precision`, then refinement (LU-IR,
+// switching to GMRES-IR when it stalls) until eta <= tolerance or
+// max_iterations corrections.  *converged on exit.
+int mixed_refine(const double* a, int nn, int nr, const double* b, int64_t ldb, double* x, int64_t ldx,
+    int precision, const b200la_refine_options* o, int restart, MixedPlan& p, SolveState& ss, bool* converged,
+    b200la_refine_result& out, cudaEvent_t e0, cudaEvent_t e1, cudaStream_t s)
+{
+    const int64_t n     = nn;
+    const int64_t nrhs  = nr;
+    const bool    use64 = precision == B200LA_PREC_FP64;
+    DeviceStatus* st    = use64 ? p.gp64.st : p.gp.st;
+    int           rc    = B200LA_SUCCESS;
+    *converged          = false;
+    cudaEventRecord(e0, s);
+    k_copy2d<double><<<grid_for((int64_t)n * nrhs), 256, 0, s>>>(b, ldb, x, ldx, nn, nr, nullptr);
+    B200LA_LAUNCH_CHECK();
+    rc = use64 ? enqueue_lu_apply<double>(p.a64, p.perm, nn, nr, x, ldx, p, st, s)
+               : enqueue_lu_apply<float>(p.a32, p.perm, nn, nr, x, ldx, p, st, s);
+    if (rc != B200LA_SUCCESS)
+        return rc;
+    double eta_prev = INFINITY;
+    bool   gmres_on = false;
+    for (int it = 0; it < o->max_iterations; ++it)
+    {
+        double eta = INFINITY;
+        if ((rc = residual_eta(a, n, nn, nr, b, ldb, x, ldx, p, ss.anorm, ss.bnorm, &eta, s)) != B200LA_SUCCESS)
+            return rc;
+        out.backward_error = eta;
+        if (eta <= o->tolerance)
+        {
+            *converged = true;
+            break;
+        }
+        const bool stalled = !std::isfinite(eta) || (it > 0 && eta > 0.5 * eta_prev);
+        if (stalled && (!gmres_on && restart > 0))
+        {
+            gmres_on = true;  // switch to GMRES-IR for the remaining iterations
+        }
+        else if (stalled && it > 1)
+        {
+            break;  // give up on this precision
+        }
+        eta_prev = eta;
+        out.iterations++;
+        if (gmres_on)
+        {
+            int gi = 0;
+            rc = use64 ? gmres_correction<double>(a, n, p.a64, nn, restart, 1e-6, x, p, st, s, &gi)
+                       : gmres_correction<float>(a, n, p.a32, nn, restart, 1e-6, x, p, st, s, &gi);
+            if (rc != B200LA_SUCCESS)
+                return rc;
+            out.gmres_iterations += gi;
+        }
+        else
+        {
+            rc = use64 ? enqueue_lu_apply<double>(p.a64, p.perm, nn, nr, p.r, nr, p, st, s)
+                       : enqueue_lu_apply<float>(p.a32, p.perm, nn, nr, p.r, nr, p, st, s);
+            if (rc != B200LA_SUCCESS)
+                return rc;
+            k_axpy2d<<<grid_for((int64_t)n * nrhs), 256, 0, s>>>(x, ldx, p.r, nr, nn, nr);
+            B200LA_LAUNCH_CHECK();
+        }
+    }
+    cudaEventRecord(e1, s);
+    cudaEventSynchronize(e1);
+    float rms = 0;
+    cudaEventElapsedTime(&rms, e0, e1);
+    out.refine_ms += rms;
+    return B200LA_SUCCESS;
+}
+
+// Next precision up after a failed attempt: FP8 -> BF16; BF16, FP16, TF32 ->
+// FP32 (three-term TF32); FP32 -> FP64.
+int next_precision(int precision)
+{
+    return precision == B200LA_PREC_FP8    ? B200LA_PREC_BF16
+           : precision == B200LA_PREC_FP32 ? B200LA_PREC_FP64
+                                           : B200LA_PREC_FP32;
+}
+
+// Factor-refine-escalate loop from `precision`.  With `prefactored` the FP32
+// factors (three-term TF32) are already in p (info `pre_info`) and the first
+// attempt reuses them.
+int mixed_loop(const double* a, int nn, int nr, const double* b, int64_t ldb, double* x, int64_t ldx,
+    int precision, bool prefactored, int pre_info, const b200la_refine_options* o, int restart, MixedPlan& p,
+    SolveState& ss, b200la_refine_result& out, cudaEvent_t e0, cudaEvent_t e1, cudaStream_t s)
+{
+    int escalations = 0;
+    for (;;)
+    {
+        int info = 0, rc;
+        if (prefactored)
+        {
+            info     = pre_info;
+            out.info = info;
+            prefactored = false;
+        }
+        else if ((rc = mixed_factor(a, nn, nr, precision, p, ss, &info, out, e0, e1, s)) != B200LA_SUCCESS &&
+                 rc != B200LA_SINGULAR)
+        {
+            return rc;
+        }
+        bool converged = false;
+        if (info == 0)
+        {
+            if ((rc = mixed_refine(a, nn, nr, b, ldb, x, ldx, precision, o, restart, p, ss, &converged, out, e0,
+                     e1, s)) != B200LA_SUCCESS)
+                return rc;
+        }
+        out.precision_used = precision;
+        out.converged      = converged ? 1 : 0;
+        if (converged || !o->escalate || precision == B200LA_PREC_FP64)
+            break;
+        precision = next_precision(precision);
+        ++escalations;
+    }
+    out.escalations += escalations;
+    return B200LA_SUCCESS;
+}
+
+// ---------------------------------------------------------------------------
+// selector features
+// ---------------------------------------------------------------------------
+// out[] words: see k_row_features / k_col_features / k_lu_features
+// (selector.cu); the FP32 factors are in p.a32 / p.perm.
+
+// z = A^-T v with the FP32 factors (P A = L U => A^T = U^T L^T P):
+// U^T w = v, L^T u = w, z = P^T u.  v is overwritten; z must not alias v.
+__global__ void k_scatter_perm(const double* __restrict__ u, const int32_t* __restrict__ perm, int n,
+    double* __restrict__ z)
+{
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    {
+        z[perm[i]] = u[i];
+    }
+}
+
+int apply_inverse_transpose(MixedPlan& p, int n, double* v, double* z, cudaStream_t s)
+{
+    int rc = enqueue_trsm_inplace<float, double>(true, true, false, n, 1, p.a32, n, v, 1, nullptr, s);
+    if (rc != B200LA_SUCCESS)
+        return rc;
+    rc = enqueue_trsm_inplace<float, double>(false, true, true, n, 1, p.a32, n, v, 1, nullptr, s);
+    if (rc != B200LA_SUCCESS)
+        return rc;
+    k_scatter_perm<<<grid_for(n), 256, 0, s>>>(v, p.perm, n, z);
+    B200LA_LAUNCH_CHECK();
+    return B200LA_SUCCESS;
+}
+
+// Hager's estimate of ||A^-1||_1 (Hager, SIAM J. Sci. Stat. Comput. 5, 1984)
+// with Higham's extra test vector and stopping rules (Higham, ACM TOMS 14,
+// 1988), using the FP32 LU factors in p applied in FP64.  Vectors are reduced
+// on the host (n doubles per step, at most five steps).
+int hager_inverse_norm1(MixedPlan& p, int n, double* est, cudaStream_t s)
+{
+    std::vector<double> hx(n, 1.0 / n), hy(n), hz(n);
+    double*             dv = p.r;   // n doubles
+    double*             dz = p.V != nullptr ? p.V : p.y;
+    double              e  = 0.0;
+    int                 rc;
+    int                 jlast = -1;
+    for (int iter = 0; iter < 5; ++iter)
+    {
+        B200LA_CUDA(cudaMemcpyAsync(dv, hx.data(), sizeof(double) * n, cudaMemcpyHostToDevice, s));
+        if ((rc = enqueue_lu_apply<float>(p.a32, p.perm, n, 1, dv, 1, p, p.gp.st, s)) != B200LA_SUCCESS)
+            return rc;
+        B200LA_CUDA(cudaMemcpyAsync(hy.data(), dv, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
+        B200LA_CUDA(cudaStreamSynchronize(s));
+        double e_new = 0.0;
+        for (int i = 0; i < n; ++i)
+            e_new += std::fabs(hy[i]);
+        if (!std::isfinite(e_new))
+        {
+            *est = INFINITY;
+            return B200LA_SUCCESS;
+        }
+        if (iter > 0 && e_new <= e)
+            break;
+        e = e_new;
+        for (int i = 0; i < n; ++i)
+            hy[i] = hy[i] >= 0 ? 1.0 : -1.0;
+        B200LA_CUDA(cudaMemcpyAsync(dv, hy.data(), sizeof(double) * n, cudaMemcpyHostToDevice, s));
+        if ((rc = apply_inverse_transpose(p, n, dv, dz, s)) != B200LA_SUCCESS)
+            return rc;
+        B200LA_CUDA(cudaMemcpyAsync(hz.data(), dz, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
+        B200LA_CUDA(cudaStreamSynchronize(s));
+        int    j  = 0;
+        double zx = 0.0;
+        for (int i = 0; i < n; ++i)
+        {
+            if (std::fabs(hz[i]) > std::fabs(hz[j]))
+                j = i;
+            zx += hz[i] * hx[i];
+        }
+        if (iter > 0 && (std::fabs(hz[j]) <= zx || j == jlast))
+            break;
+        jlast = j;
+        std::fill(hx.begin(), hx.end(), 0.0);
+        hx[j] = 1.0;
+    }
+    // Higham's alternating test vector
+    for (int i = 0; i < n; ++i)
+        hx[i] = (i % 2 == 0 ? 1.0 : -1.0) * (1.0 + (n > 1 ? (double)i / (n - 1) : 0.0));
+    B200LA_CUDA(cudaMemcpyAsync(dv, hx.data(), sizeof(double) * n, cudaMemcpyHostToDevice, s));
+    if ((rc = enqueue_lu_apply<float>(p.a32, p.perm, n, 1, dv, 1, p, p.gp.st, s)) != B200LA_SUCCESS)
+        return rc;
+    B200LA_CUDA(cudaMemcpyAsync(hy.data(), dv, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
+    B200LA_CUDA(cudaStreamSynchronize(s));
+    double alt = 0.0;
+    for (int i = 0; i < n; ++i)
+        alt += std::fabs(hy[i]);
+    alt = 2.0 * alt / (3.0 * n);
+    *est = alt > e ? alt : e;
+    return B200LA_SUCCESS;
+}
+
+}  // namespace
+
+// The selector's statistics kernels and network (selector.cu).
+int enqueue_matrix_stats(const double* a, int n, const float* lu32, unsigned long long* out, cudaStream_t s);
+int enqueue_mlp_forward(const float* params, const float* x, int batch, float* probs, cudaStream_t s);
+constexpr int kSelFeatures = 12, kSelClasses = 4, kSelParams = 5252;
+
+namespace
+{
+inline double word_to_double(unsigned long long w)
+{
+    double d;
+    memcpy(&d, &w, 8);
+    return d;
+}
+inline float safe_log10(double v) { return (float)std::log10(v > 1e-300 ? v : 1e-300); }
+
+// The 12 selector features of A (host floats); factors A in FP32 (three-term
+// TF32) into p as a side effect (*info = its LAPACK info).
+int selector_features(const double* a, int nn, MixedPlan& p, SolveState& ss, float* f, int* info,
+    b200la_refine_result& out, cudaEvent_t e0, cudaEvent_t e1, cudaStream_t s)
+{
+    unsigned long long* stats = p.norms + 4 + 3 * kMaxNrhsMixed;  // 16 words after the norms
+    int                 rc    = enqueue_matrix_stats(a, nn, nullptr, stats, s);
+    if (rc != B200LA_SUCCESS)
+        return rc;
+    if ((rc = mixed_factor(a, nn, 1, B200LA_PREC_FP32, p, ss, info, out, e0, e1, s)) != B200LA_SUCCESS &&
+        rc != B200LA_SINGULAR)
+        return rc;
+    if ((rc = enqueue_matrix_stats(nullptr, nn, p.a32, stats, s)) != B200LA_SUCCESS)
+        return rc;
+    unsigned long long h[16];
+    B200LA_CUDA(cudaMemcpyAsync(h, stats, sizeof(h), cudaMemcpyDeviceToHost, s));
+    B200LA_CUDA(cudaStreamSynchronize(s));
+    double ainv1 = INFINITY;
+    if (*info == 0 && (rc = hager_inverse_norm1(p, nn, &ainv1, s)) != B200LA_SUCCESS)
+        return rc;
+    const double n         = nn;
+    const double norm_inf  = word_to_double(h[0]);
+    const double amax      = word_to_double(h[1]);
+    const double fro       = std::sqrt(word_to_double(h[2]));
+    const double dd_inv    = word_to_double(h[3]);  // max over rows of 1 / (1 + ratio)
+    const double dd_rows   = (double)h[4];
+    const double norm_1    = word_to_double(h[5]);
+    const double umax      = word_to_double(h[6]);
+    const double dmin      = word_to_double(h[7]);
+    const double dmax      = word_to_double(h[8]);
+    const double abs_sum   = word_to_double(h[9]);
+    const double udmin     = word_to_double(h[10]);
+    const double udmax     = word_to_double(h[11]);
+    const double min_ratio = dd_inv > 0 ? 1.0 / dd_inv - 1.0 : 1e30;
+    f[0]  = (float)(std::log2(n) / 12.0);
+    f[1]  = safe_log10(norm_inf / amax);
+    f[2]  = safe_log10(norm_1 / amax);
+    f[3]  = safe_log10(fro / (amax * n));
+    f[4]  = safe_log10(abs_sum / (amax * n * n));
+    f[5]  = safe_log10(min_ratio) / 4.0f;
+    f[6]  = (float)(dd_rows / n);
+    f[7]  = safe_log10(dmin / amax) / 4.0f;
+    f[8]  = safe_log10(dmax / amax);
+    f[9]  = safe_log10(umax / amax);
+    f[10] = std::isfinite(ainv1) ? safe_log10(ainv1 * norm_1) / 4.0f : 5.0f;
+    f[11] = safe_log10(udmin / udmax) / 4.0f;
+    return B200LA_SUCCESS;
+}
 }  // namespace
 }  // namespace b200la
 
@@ -854,6 +1221,57 @@ B200LA_API size_t b200la_dsolve_mixed_workspace_size(int64_t n, int64_t nrhs, co
     return a.size();
 }
 
+static int check_mixed_call(const double* a, int64_t n, int64_t nrhs, const double* b, int64_t ldb,
+    const double* x, int64_t ldx, const b200la_refine_options* o, void* ws, size_t ws_bytes)
+{
+    if (a == nullptr || b == nullptr || x == nullptr)
+        return set_error(B200LA_INVALID_ARGUMENT, "a, b and x must not be null");
+    if (n <= 0 || nrhs <= 0 || nrhs > kMaxNrhsMixed || ldb < nrhs || ldx < nrhs || n > 65536)
+        return set_error(B200LA_INVALID_ARGUMENT, "invalid sizes (n %lld, nrhs %lld; nrhs <= %d)",
+            (long long)n, (long long)nrhs, kMaxNrhsMixed);
+    if (o->precision < B200LA_PREC_FP64 || o->precision > B200LA_PREC_FP8 || o->max_iterations < 1 ||
+        !(o->tolerance > 0))
+        return set_error(B200LA_INVALID_ARGUMENT, "invalid refinement options");
+    const size_t need = b200la_dsolve_mixed_workspace_size(n, nrhs, o);
+    if (ws == nullptr || ws_bytes < need)
+        return set_error(B200LA_WORKSPACE_TOO_SMALL, "workspace too small (%zu < %zu)", ws_bytes, need);
+    int rc = prepare<float>();
+    if (rc != B200LA_SUCCESS)
+        return rc;
+    if ((rc = prepare<double>()) != B200LA_SUCCESS)
+        return rc;
+    return set_mixed_attributes();
+}
+
+static int restart_of(const b200la_refine_options* o, int64_t nrhs)
+{
+    return nrhs == 1 ? (o->gmres_restart > kGmresMaxRestart ? kGmresMaxRestart : (o->gmres_restart < 0 ? 0 : o->gmres_restart)) : 0;
+}
+
+struct MixedEvents
+{
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    MixedEvents()
+    {
+        cudaEventCreate(&e0);
+        cudaEventCreate(&e1);
+    }
+    ~MixedEvents()
+    {
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+    }
+};
+
+static int finish_result(b200la_refine_result& out, b200la_refine_result* res)
+{
+    if (res)
+        *res = out;
+    if (out.info != 0)
+        return B200LA_SINGULAR;
+    return out.converged ? B200LA_SUCCESS : B200LA_NOT_CONVERGED;
+}
+
 B200LA_API int b200la_dsolve_mixed(const double* a, int64_t n, int64_t nrhs, const double* b, int64_t ldb,
     double* x, int64_t ldx, const b200la_refine_options* opts, b200la_refine_result* res, void* ws,
     size_t ws_bytes, void* stream)
@@ -861,26 +1279,11 @@ B200LA_API int b200la_dsolve_mixed(const double* a, int64_t n, int64_t nrhs, con
     b200la_refine_options d;
     b200la_refine_default_options(&d);
     const b200la_refine_options* o = opts ? opts : &d;
-    if (a == nullptr || b == nullptr || x == nullptr)
-        return set_error(B200LA_INVALID_ARGUMENT, "dsolve_mixed: a, b and x must not be null");
-    if (n <= 0 || nrhs <= 0 || nrhs > kMaxNrhsMixed || ldb < nrhs || ldx < nrhs || n > 65536)
-        return set_error(B200LA_INVALID_ARGUMENT, "dsolve_mixed: invalid sizes (n %lld, nrhs %lld; nrhs <= %d)",
-            (long long)n, (long long)nrhs, kMaxNrhsMixed);
-    if (o->precision < B200LA_PREC_FP64 || o->precision > B200LA_PREC_FP8 || o->max_iterations < 1 ||
-        !(o->tolerance > 0))
-        return set_error(B200LA_INVALID_ARGUMENT, "dsolve_mixed: invalid options");
-    const size_t need = b200la_dsolve_mixed_workspace_size(n, nrhs, o);
-    if (ws == nullptr || ws_bytes < need)
-        return set_error(B200LA_WORKSPACE_TOO_SMALL, "dsolve_mixed: workspace too small (%zu < %zu)", ws_bytes, need);
-    int rc = prepare<float>();
+    int rc = check_mixed_call(a, n, nrhs, b, ldb, x, ldx, o, ws, ws_bytes);
     if (rc != B200LA_SUCCESS)
         return rc;
-    if ((rc = prepare<double>()) != B200LA_SUCCESS)
-        return rc;
-    if ((rc = set_mixed_attributes()) != B200LA_SUCCESS)
-        return rc;
-    cudaStream_t s       = static_cast<cudaStream_t>(stream);
-    const int    restart = nrhs == 1 ? (o->gmres_restart > kGmresMaxRestart ? kGmresMaxRestart : (o->gmres_restart < 0 ? 0 : o->gmres_restart)) : 0;
+    cudaStream_t s        = static_cast<cudaStream_t>(stream);
+    const int    restart  = restart_of(o, nrhs);
     const bool   fallback = o->escalate != 0 || o->precision == B200LA_PREC_FP64;
     Arena        ar(ws, ws_bytes);
     MixedPlan    p  = plan_mixed(ar, n, nrhs, restart, fallback);
@@ -888,163 +1291,106 @@ B200LA_API int b200la_dsolve_mixed(const double* a, int64_t n, int64_t nrhs, con
 
     b200la_refine_result out{};
     out.backward_error = INFINITY;
-    cudaEvent_t e0, e1;
-    cudaEventCreate(&e0);
-    cudaEventCreate(&e1);
-
-    // ||A||_inf, ||b_j||_inf
+    MixedEvents ev;
+    // ||b_j||_inf (read with ||A|| after the first factorization)
     B200LA_CUDA(cudaMemsetAsync(p.norms, 0, sizeof(unsigned long long) * (4 + 3 * kMaxNrhsMixed), s));
-    std::vector<double> bnorm(nr, 0.0);
-    {
-        k_colmax<<<grid_for((int64_t)n * nrhs), 256, 0, s>>>(b, ldb, nn, nr, p.norms + 4 + 2 * kMaxNrhsMixed);
-        B200LA_LAUNCH_CHECK();
-    }
+    k_colmax<<<grid_for((int64_t)n * nrhs), 256, 0, s>>>(b, ldb, nn, nr, p.norms + 4 + 2 * kMaxNrhsMixed);
+    B200LA_LAUNCH_CHECK();
+    SolveState ss;
+    if ((rc = mixed_loop(a, nn, nr, b, ldb, x, ldx, o->precision, false, 0, o, restart, p, ss, out, ev.e0, ev.e1,
+             s)) != B200LA_SUCCESS)
+        return rc;
+    return finish_result(out, res);
+}
 
-    int precision = o->precision;
-    int escalations = 0;
-    double anorm = 0.0;
-    bool   have_anorm = false;
-    for (;;)
-    {
-        const bool use64 = precision == B200LA_PREC_FP64;
-        const int  kind  = precision == B200LA_PREC_BF16   ? TC_BF16
-                           : precision == B200LA_PREC_FP16 ? TC_FP16
-                           : precision == B200LA_PREC_FP8  ? TC_FP8
-                                                           : TC_TF32;
-        const bool split = precision == B200LA_PREC_FP32;
-        cudaEventRecord(e0, s);
-        DeviceStatus* st = use64 ? p.gp64.st : p.gp.st;
-        if (!use64)
-        {
-            // A32 and ||A||
-            k_convert_a<<<(nn * 32 + 255) / 256, 256, 0, s>>>(a, n, p.a32, nn, p.norms);
-            B200LA_LAUNCH_CHECK();
-            if ((rc = enqueue_getrf_mixed(p, nn, kind, split, s)) != B200LA_SUCCESS)
-                return rc;
-            k_perm_from_pivots<0><<<1, 256, perm_smem_bytes(nn), s>>>(p.piv, nn, p.perm, perm_smem_bytes(nn) > 0 ? 1 : 0, st, nullptr);
-        }
-        else
-        {
-            B200LA_CUDA(cudaMemcpy2DAsync(p.a64, sizeof(double) * n, a, sizeof(double) * n, sizeof(double) * n, n,
-                cudaMemcpyDeviceToDevice, s));
-            if (!have_anorm)
-            {
-                k_convert_a<<<(nn * 32 + 255) / 256, 256, 0, s>>>(a, n, p.a32, nn, p.norms);
-                B200LA_LAUNCH_CHECK();
-            }
-            if ((rc = enqueue_getrf<double>(p.a64, nn, p.piv64, p.gp64, s)) != B200LA_SUCCESS)
-                return rc;
-            k_perm_from_pivots<0><<<1, 256, perm_smem_bytes(nn), s>>>(p.piv64, nn, p.perm, perm_smem_bytes(nn) > 0 ? 1 : 0, st, nullptr);
-        }
-        B200LA_LAUNCH_CHECK();
-        {
-            const int nbk = (nn + kTvRows - 1) / kTvRows;
-            prof_begin(KC_SOLVE, s);
-            if (use64)
-                k_invert_diag_blocks<double><<<dim3(nbk, 2), kTvRows, 0, s>>>(p.a64, n, nn, p.dinv);
-            else
-                k_invert_diag_blocks<float><<<dim3(nbk, 2), kTvRows, 0, s>>>(p.a32, n, nn, p.dinv);
-            prof_end(KC_SOLVE, s);
-            B200LA_LAUNCH_CHECK();
-        }
-        int info = 0;
-        if ((rc = read_status(st, &info, s)) < 0)
-            return rc;
-        cudaEventRecord(e1, s);
-        cudaEventSynchronize(e1);
-        float fms = 0;
-        cudaEventElapsedTime(&fms, e0, e1);
-        out.factor_ms += fms;
-        out.info = info;
-        if (!have_anorm)
-        {
-            unsigned long long hb[1 + kMaxNrhsMixed];
-            B200LA_CUDA(cudaMemcpy(hb, p.norms, sizeof(unsigned long long), cudaMemcpyDeviceToHost));
-            memcpy(&anorm, &hb[0], 8);
-            B200LA_CUDA(cudaMemcpy(hb + 1, p.norms + 4 + 2 * kMaxNrhsMixed, sizeof(unsigned long long) * nr,
-                cudaMemcpyDeviceToHost));
-            for (int j = 0; j < nr; ++j)
-                memcpy(&bnorm[j], &hb[1 + j], 8);
-            have_anorm = true;
-        }
-        bool converged = false;
-        if (info == 0)
-        {
-            cudaEventRecord(e0, s);
-            // x0 = M^-1 b
-            k_copy2d<double><<<grid_for((int64_t)n * nrhs), 256, 0, s>>>(b, ldb, x, ldx, nn, nr, nullptr);
-            B200LA_LAUNCH_CHECK();
-            rc = use64 ? enqueue_lu_apply<double>(p.a64, p.perm, nn, nr, x, ldx, p, st, s)
-                       : enqueue_lu_apply<float>(p.a32, p.perm, nn, nr, x, ldx, p, st, s);
-            if (rc != B200LA_SUCCESS)
-                return rc;
-            double eta_prev = INFINITY;
-            bool   gmres_on = false;
-            for (int it = 0; it < o->max_iterations; ++it)
-            {
-                double eta = INFINITY;
-                if ((rc = residual_eta(a, n, nn, nr, b, ldb, x, ldx, p, anorm, bnorm, &eta, s)) != B200LA_SUCCESS)
-                    return rc;
-                out.backward_error = eta;
-                if (eta <= o->tolerance)
-                {
-                    converged = true;
-                    break;
-                }
-                const bool stalled = !std::isfinite(eta) || (it > 0 && eta > 0.5 * eta_prev);
-                if (stalled && (!gmres_on && restart > 0))
-                {
-                    gmres_on = true;  // switch to GMRES-IR for the remaining iterations
-                }
-                else if (stalled && it > 1)
-                {
-                    break;  // give up on this precision
-                }
-                eta_prev = eta;
-                out.iterations++;
-                if (gmres_on)
-                {
-                    int gi = 0;
-                    rc = use64 ? gmres_correction<double>(a, n, p.a64, nn, restart, 1e-6, x, p, st, s, &gi)
-                               : gmres_correction<float>(a, n, p.a32, nn, restart, 1e-6, x, p, st, s, &gi);
-                    if (rc != B200LA_SUCCESS)
-                        return rc;
-                    out.gmres_iterations += gi;
-                }
-                else
-                {
-                    rc = use64 ? enqueue_lu_apply<double>(p.a64, p.perm, nn, nr, p.r, nr, p, st, s)
-                               : enqueue_lu_apply<float>(p.a32, p.perm, nn, nr, p.r, nr, p, st, s);
-                    if (rc != B200LA_SUCCESS)
-                        return rc;
-                    k_axpy2d<<<grid_for((int64_t)n * nrhs), 256, 0, s>>>(x, ldx, p.r, nr, nn, nr);
-                    B200LA_LAUNCH_CHECK();
-                }
-            }
-            cudaEventRecord(e1, s);
-            cudaEventSynchronize(e1);
-            float rms = 0;
-            cudaEventElapsedTime(&rms, e0, e1);
-            out.refine_ms += rms;
-        }
-        out.precision_used = precision;
-        out.converged      = converged ? 1 : 0;
-        if (converged || !o->escalate || precision == B200LA_PREC_FP64)
-            break;
-        // escalate: FP8 -> BF16; other low precisions -> FP32 (three-term
-        // TF32) -> FP64
-        precision = precision == B200LA_PREC_FP8    ? B200LA_PREC_BF16
-                    : precision == B200LA_PREC_FP32 ? B200LA_PREC_FP64
-                                                    : B200LA_PREC_FP32;
-        ++escalations;
-    }
-    out.escalations = escalations;
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
-    if (res)
-        *res = out;
-    if (out.info != 0)
-        return B200LA_SINGULAR;
-    return out.converged ? B200LA_SUCCESS : B200LA_NOT_CONVERGED;
+B200LA_API int b200la_selector_features(const double* a, int64_t n, float* features, int* info, void* ws,
+    size_t ws_bytes, void* stream)
+{
+    b200la_refine_options o;
+    b200la_refine_default_options(&o);
+    if (features == nullptr)
+        return set_error(B200LA_INVALID_ARGUMENT, "selector_features: features must not be null");
+    int rc = check_mixed_call(a, n, 1, a, 1, a, 1, &o, ws, ws_bytes);
+    if (rc != B200LA_SUCCESS)
+        return rc;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    Arena        ar(ws, ws_bytes);
+    MixedPlan    p = plan_mixed(ar, n, 1, restart_of(&o, 1), true);
+    B200LA_CUDA(cudaMemsetAsync(p.norms, 0, sizeof(unsigned long long) * (4 + 3 * kMaxNrhsMixed), s));
+    b200la_refine_result out{};
+    MixedEvents          ev;
+    SolveState           ss;
+    int                  inf = 0;
+    if ((rc = selector_features(a, (int)n, p, ss, features, &inf, out, ev.e0, ev.e1, s)) != B200LA_SUCCESS)
+        return rc;
+    if (info)
+        *info = inf;
+    return B200LA_SUCCESS;
+}
+
+B200LA_API int b200la_dsolve_selected(const double* a, int64_t n, const double* b, double* x,
+    const float* params, const b200la_refine_options* opts, b200la_refine_result* res, int* predicted,
+    float* features, void* ws, size_t ws_bytes, void* stream)
+{
+    b200la_refine_options d;
+    b200la_refine_default_options(&d);
+    b200la_refine_options o = opts ? *opts : d;
+    o.precision             = B200LA_PREC_FP32;
+    o.escalate              = 1;
+    if (params == nullptr)
+        return set_error(B200LA_INVALID_ARGUMENT, "dsolve_selected: params must not be null");
+    int rc = check_mixed_call(a, n, 1, b, 1, x, 1, &o, ws, ws_bytes);
+    if (rc != B200LA_SUCCESS)
+        return rc;
+    cudaStream_t s       = static_cast<cudaStream_t>(stream);
+    const int    restart = restart_of(&o, 1);
+    Arena        ar(ws, ws_bytes);
+    MixedPlan    p  = plan_mixed(ar, n, 1, restart, true);
+    const int    nn = (int)n;
+
+    b200la_refine_result out{};
+    out.backward_error = INFINITY;
+    MixedEvents ev;
+    B200LA_CUDA(cudaMemsetAsync(p.norms, 0, sizeof(unsigned long long) * (4 + 3 * kMaxNrhsMixed), s));
+    k_colmax<<<grid_for(n), 256, 0, s>>>(b, 1, nn, 1, p.norms + 4 + 2 * kMaxNrhsMixed);
+    B200LA_LAUNCH_CHECK();
+    SolveState ss;
+    float      f[kSelFeatures];
+    int        info = 0;
+    if ((rc = selector_features(a, nn, p, ss, f, &info, out, ev.e0, ev.e1, s)) != B200LA_SUCCESS)
+        return rc;
+    if (features)
+        memcpy(features, f, sizeof(f));
+    // standardize with the network's stored mean / inverse std, then infer
+    float norm[2 * kSelFeatures];
+    B200LA_CUDA(cudaMemcpyAsync(norm, params + kSelParams, sizeof(norm), cudaMemcpyDeviceToHost, s));
+    B200LA_CUDA(cudaStreamSynchronize(s));
+    float xin[kSelFeatures];
+    for (int i = 0; i < kSelFeatures; ++i)
+        xin[i] = (f[i] - norm[i]) * norm[kSelFeatures + i];
+    B200LA_CUDA(cudaMemcpyAsync(p.sel, xin, sizeof(xin), cudaMemcpyHostToDevice, s));
+    if ((rc = enqueue_mlp_forward(params, p.sel, 1, p.sel + kSelFeatures, s)) != B200LA_SUCCESS)
+        return rc;
+    float probs[kSelClasses];
+    B200LA_CUDA(cudaMemcpyAsync(probs, p.sel + kSelFeatures, sizeof(probs), cudaMemcpyDeviceToHost, s));
+    B200LA_CUDA(cudaStreamSynchronize(s));
+    int cls = 0;
+    for (int c = 1; c < kSelClasses; ++c)
+        if (probs[c] > probs[cls])
+            cls = c;
+    static const int kClassPrec[kSelClasses] = {B200LA_PREC_FP8, B200LA_PREC_BF16, B200LA_PREC_FP32,
+        B200LA_PREC_FP64};
+    if (predicted)
+        *predicted = kClassPrec[cls];
+    // FP8 / BF16 / FP32: refine with the FP32 factors already made for the
+    // features (at least as accurate as the predicted precision's); FP64:
+    // plain FP64 LU.  Escalation on failure either way.
+    if (kClassPrec[cls] == B200LA_PREC_FP64)
+        rc = mixed_loop(a, nn, 1, b, 1, x, 1, B200LA_PREC_FP64, false, 0, &o, restart, p, ss, out, ev.e0, ev.e1, s);
+    else
+        rc = mixed_loop(a, nn, 1, b, 1, x, 1, B200LA_PREC_FP32, true, info, &o, restart, p, ss, out, ev.e0, ev.e1, s);
+    if (rc != B200LA_SUCCESS)
+        return rc;
+    return finish_result(out, res);
 }
 }

@@ -1,0 +1,423 @@
+// Learned precision selector: a 12 -> 64 -> 64 -> 4 MLP (ReLU, softmax
+// cross-entropy), FP32, with hand-written inference, training (forward +
+// backward) and Adam kernels, and the kernels that gather the matrix
+// statistics its features are made of.
+//
+// Parameter vector (5252 floats): W1[12][64] | b1[64] | W2[64][64] | b2[64] |
+// W3[64][4] | b3[4]; y = relu(x W1 + b1), z = relu(y W2 + b2),
+// logits = z W3 + b3.
+#include <cuda_runtime.h>
+
+#include <climits>
+#include <cmath>
+#include <cstdint>
+
+#include "common.cuh"
+
+namespace b200la
+{
+namespace
+{
+constexpr int kIn = 12, kH = 64, kOut = 4;
+constexpr int kOffW1 = 0, kOffB1 = kIn * kH, kOffW2 = kOffB1 + kH, kOffB2 = kOffW2 + kH * kH;
+constexpr int kOffW3 = kOffB2 + kH, kOffB3 = kOffW3 + kH * kOut, kParams = kOffB3 + kOut;
+static_assert(kParams == 5252, "parameter count");
+constexpr int kMlpThreads = 128;
+
+__device__ __forceinline__ void mlp_forward(const float* p, const float* x, float* h1, float* h2, float* logits)
+{
+    for (int j = 0; j < kH; ++j)
+    {
+        float s = p[kOffB1 + j];
+        for (int i = 0; i < kIn; ++i)
+        {
+            s = fmaf(x[i], p[kOffW1 + i * kH + j], s);
+        }
+        h1[j] = fmaxf(s, 0.f);
+    }
+    for (int j = 0; j < kH; ++j)
+    {
+        float s = p[kOffB2 + j];
+        for (int i = 0; i < kH; ++i)
+        {
+            s = fmaf(h1[i], p[kOffW2 + i * kH + j], s);
+        }
+        h2[j] = fmaxf(s, 0.f);
+    }
+    for (int k = 0; k < kOut; ++k)
+    {
+        float s = p[kOffB3 + k];
+        for (int i = 0; i < kH; ++i)
+        {
+            s = fmaf(h2[i], p[kOffW3 + i * kOut + k], s);
+        }
+        logits[k] = s;
+    }
+}
+
+// probs[b][4] = softmax(MLP(x_b)), one thread per sample, parameters in
+// shared memory.
+__global__ void __launch_bounds__(kMlpThreads) k_mlp_forward(const float* __restrict__ params,
+    const float* __restrict__ X, int batch, float* __restrict__ probs)
+{
+    __shared__ float p[kParams];
+    for (int i = threadIdx.x; i < kParams; i += kMlpThreads)
+    {
+        p[i] = params[i];
+    }
+    __syncthreads();
+    const int b = blockIdx.x * kMlpThreads + threadIdx.x;
+    if (b >= batch)
+    {
+        return;
+    }
+    float x[kIn], h1[kH], h2[kH], lg[kOut];
+    for (int i = 0; i < kIn; ++i)
+    {
+        x[i] = X[(size_t)b * kIn + i];
+    }
+    mlp_forward(p, x, h1, h2, lg);
+    float m = lg[0];
+    for (int k = 1; k < kOut; ++k)
+    {
+        m = fmaxf(m, lg[k]);
+    }
+    float z = 0.f;
+    for (int k = 0; k < kOut; ++k)
+    {
+        lg[k] = expf(lg[k] - m);
+        z += lg[k];
+    }
+    for (int k = 0; k < kOut; ++k)
+    {
+        probs[(size_t)b * kOut + k] = lg[k] / z;
+    }
+}
+
+// Forward + backward of the mean softmax cross-entropy over the batch:
+// grads += d(loss_sum)/d(params) (not yet divided by the batch), loss_sum +=
+// sum of per-sample losses.  One thread per sample; per-CTA gradient sums in
+// shared memory, then one global atomic add per parameter per CTA.
+__global__ void __launch_bounds__(kMlpThreads) k_mlp_grad(const float* __restrict__ params,
+    const float* __restrict__ X, const int32_t* __restrict__ labels, int batch, float* __restrict__ grads,
+    float* __restrict__ loss_sum)
+{
+    __shared__ float p[kParams];
+    __shared__ float g[kParams];
+    for (int i = threadIdx.x; i < kParams; i += kMlpThreads)
+    {
+        p[i] = params[i];
+        g[i] = 0.f;
+    }
+    __syncthreads();
+    const int b = blockIdx.x * kMlpThreads + threadIdx.x;
+    if (b < batch)
+    {
+        float x[kIn], h1[kH], h2[kH], lg[kOut];
+        for (int i = 0; i < kIn; ++i)
+        {
+            x[i] = X[(size_t)b * kIn + i];
+        }
+        mlp_forward(p, x, h1, h2, lg);
+        float m = lg[0];
+        for (int k = 1; k < kOut; ++k)
+        {
+            m = fmaxf(m, lg[k]);
+        }
+        float z = 0.f;
+        for (int k = 0; k < kOut; ++k)
+        {
+            lg[k] = expf(lg[k] - m);
+            z += lg[k];
+        }
+        const int y = labels[b];
+        float     dl[kOut];
+        for (int k = 0; k < kOut; ++k)
+        {
+            const float pk = lg[k] / z;
+            dl[k]          = pk - (k == y ? 1.f : 0.f);
+        }
+        atomicAdd(loss_sum, -logf(fmaxf(lg[y] / z, 1e-30f)));
+        // layer 3
+        float dh2[kH];
+        for (int i = 0; i < kH; ++i)
+        {
+            float s = 0.f;
+            for (int k = 0; k < kOut; ++k)
+            {
+                atomicAdd(&g[kOffW3 + i * kOut + k], h2[i] * dl[k]);
+                s = fmaf(p[kOffW3 + i * kOut + k], dl[k], s);
+            }
+            dh2[i] = h2[i] > 0.f ? s : 0.f;
+        }
+        for (int k = 0; k < kOut; ++k)
+        {
+            atomicAdd(&g[kOffB3 + k], dl[k]);
+        }
+        // layer 2
+        float dh1[kH];
+        for (int i = 0; i < kH; ++i)
+        {
+            dh1[i] = 0.f;
+        }
+        for (int j = 0; j < kH; ++j)
+        {
+            if (dh2[j] == 0.f)
+            {
+                continue;
+            }
+            atomicAdd(&g[kOffB2 + j], dh2[j]);
+            for (int i = 0; i < kH; ++i)
+            {
+                atomicAdd(&g[kOffW2 + i * kH + j], h1[i] * dh2[j]);
+                dh1[i] = fmaf(p[kOffW2 + i * kH + j], dh2[j], dh1[i]);
+            }
+        }
+        // layer 1
+        for (int j = 0; j < kH; ++j)
+        {
+            const float d = h1[j] > 0.f ? dh1[j] : 0.f;
+            if (d == 0.f)
+            {
+                continue;
+            }
+            atomicAdd(&g[kOffB1 + j], d);
+            for (int i = 0; i < kIn; ++i)
+            {
+                atomicAdd(&g[kOffW1 + i * kH + j], x[i] * d);
+            }
+        }
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < kParams; i += kMlpThreads)
+    {
+        if (g[i] != 0.f)
+        {
+            atomicAdd(&grads[i], g[i]);
+        }
+    }
+}
+
+// Adam on the mean gradient (grads / batch); clears grads.
+__global__ void k_adam(float* __restrict__ params, float* __restrict__ grads, float* __restrict__ m1,
+    float* __restrict__ m2, float inv_batch, float lr, float beta1, float beta2, float eps, int step,
+    float weight_decay)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= kParams)
+    {
+        return;
+    }
+    const float gr = grads[i] * inv_batch + weight_decay * params[i];
+    grads[i]       = 0.f;
+    m1[i]          = beta1 * m1[i] + (1.f - beta1) * gr;
+    m2[i]          = beta2 * m2[i] + (1.f - beta2) * gr * gr;
+    const float mh = m1[i] / (1.f - powf(beta1, (float)step));
+    const float vh = m2[i] / (1.f - powf(beta2, (float)step));
+    params[i] -= lr * mh / (sqrtf(vh) + eps);
+}
+
+// ---- matrix statistics for the selector's features ------------------------
+// Sixteen 64-bit words; non-negative doubles are kept as their bit patterns,
+// whose unsigned order is the numeric order (atomicMax / atomicMin):
+//   [0] ||A||_inf   [1] max |a_ij|   [2] sum a_ij^2   [3] max_i 1/(1+r_i),
+//   r_i = |a_ii| / sum_{j!=i} |a_ij|   [4] rows with r_i >= 1 (count)
+//   [5] ||A||_1     [6] max |u_ij| of the LU factors   [7] min |a_ii|
+//   [8] max |a_ii|  [9] sum |a_ij|   [10] min |u_ii|   [11] max |u_ii|
+__device__ __forceinline__ void amax_d(unsigned long long* p, double v)
+{
+    atomicMax(p, (unsigned long long)__double_as_longlong(v));
+}
+__device__ __forceinline__ void amin_d(unsigned long long* p, double v)
+{
+    atomicMin(p, (unsigned long long)__double_as_longlong(v));
+}
+
+__global__ void k_stats_init(unsigned long long* out)
+{
+    const int i = threadIdx.x;
+    if (i < 16)
+    {
+        out[i] = (i == 7 || i == 10) ? (unsigned long long)__double_as_longlong(INFINITY) : 0ull;
+    }
+}
+
+// A warp per row: [0] [1] [2] [3] [4] [7] [8] [9].
+__global__ void k_row_stats(const double* __restrict__ a, int n, unsigned long long* out)
+{
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (warp >= n)
+    {
+        return;
+    }
+    const double* row = a + (int64_t)warp * n;
+    double        s = 0.0, mx = 0.0, sq = 0.0;
+    for (int j = lane; j < n; j += 32)
+    {
+        const double v = fabs(row[j]);
+        s += v;
+        mx = fmax(mx, v);
+        sq = fma(v, v, sq);
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1)
+    {
+        s += __shfl_down_sync(0xffffffffu, s, off);
+        mx = fmax(mx, __shfl_down_sync(0xffffffffu, mx, off));
+        sq += __shfl_down_sync(0xffffffffu, sq, off);
+    }
+    if (lane == 0)
+    {
+        amax_d(out + 0, s);
+        amax_d(out + 1, mx);
+        atomicAdd(reinterpret_cast<double*>(out + 2), sq);
+        atomicAdd(reinterpret_cast<double*>(out + 9), s);
+        const double d     = fabs(row[warp]);
+        const double off   = s - d;
+        const double ratio = off > 0 ? d / off : 1e30;
+        amax_d(out + 3, 1.0 / (1.0 + ratio));
+        if (ratio >= 1.0)
+        {
+            atomicAdd(out + 4, 1ull);
+        }
+        amin_d(out + 7, d);
+        amax_d(out + 8, d);
+    }
+}
+
+// [5]: one thread per column, coalesced across the warp.
+__global__ void k_col_stats(const double* __restrict__ a, int n, unsigned long long* out)
+{
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n)
+    {
+        return;
+    }
+    double s = 0.0;
+    for (int i = 0; i < n; ++i)
+    {
+        s += fabs(a[(int64_t)i * n + j]);
+    }
+    amax_d(out + 5, s);
+}
+
+// FP32 LU factors (row-major n x n): [6] [10] [11].  A warp per row.
+__global__ void k_lu_stats(const float* __restrict__ f, int n, unsigned long long* out)
+{
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (warp >= n)
+    {
+        return;
+    }
+    const float* row = f + (int64_t)warp * n;
+    double       mx  = 0.0;
+    for (int j = warp + lane; j < n; j += 32)
+    {
+        mx = fmax(mx, (double)fabsf(row[j]));
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1)
+    {
+        mx = fmax(mx, __shfl_down_sync(0xffffffffu, mx, off));
+    }
+    if (lane == 0)
+    {
+        amax_d(out + 6, mx);
+        const double d = fabs((double)row[warp]);
+        amin_d(out + 10, d);
+        amax_d(out + 11, d);
+    }
+}
+}  // namespace
+int require_sm100();
+
+int enqueue_mlp_forward(const float* params, const float* x, int batch, float* probs, cudaStream_t s)
+{
+    prof_begin(KC_SELECT, s);
+    k_mlp_forward<<<(batch + kMlpThreads - 1) / kMlpThreads, kMlpThreads, 0, s>>>(params, x, batch, probs);
+    prof_end(KC_SELECT, s);
+    B200LA_LAUNCH_CHECK();
+    return B200LA_SUCCESS;
+}
+
+// With `a`: resets the sixteen words and accumulates A's statistics; with
+// `lu32`: adds the statistics of the FP32 factors (words 6, 10, 11).
+int enqueue_matrix_stats(const double* a, int n, const float* lu32, unsigned long long* out, cudaStream_t s)
+{
+    prof_begin(KC_SELECT, s);
+    if (a != nullptr)
+    {
+        k_stats_init<<<1, 32, 0, s>>>(out);
+        k_row_stats<<<(int)(((int64_t)n * 32 + 255) / 256), 256, 0, s>>>(a, n, out);
+        k_col_stats<<<(n + 255) / 256, 256, 0, s>>>(a, n, out);
+    }
+    if (lu32 != nullptr)
+    {
+        k_lu_stats<<<(int)(((int64_t)n * 32 + 255) / 256), 256, 0, s>>>(lu32, n, out);
+    }
+    prof_end(KC_SELECT, s);
+    B200LA_LAUNCH_CHECK();
+    return B200LA_SUCCESS;
+}
+}  // namespace b200la
+
+using namespace b200la;
+
+extern "C" {
+
+B200LA_API int b200la_mlp_param_count(void) { return kParams; }
+
+B200LA_API int b200la_mlp_forward(const float* params, const float* x, int64_t batch, float* probs, void* stream)
+{
+    if (!params || !x || !probs || batch <= 0 || batch > INT_MAX / 2)
+        return set_error(B200LA_INVALID_ARGUMENT, "mlp_forward: invalid arguments");
+    int rc = require_sm100();
+    if (rc != B200LA_SUCCESS)
+        return rc;
+    return enqueue_mlp_forward(params, x, (int)batch, probs, static_cast<cudaStream_t>(stream));
+}
+
+B200LA_API int b200la_mlp_gradient(const float* params, const float* x, const int32_t* labels, int64_t batch,
+    float* grads, float* loss_sum, void* stream)
+{
+    if (!params || !x || !labels || !grads || !loss_sum || batch <= 0 || batch > INT_MAX / 2)
+        return set_error(B200LA_INVALID_ARGUMENT, "mlp_gradient: invalid arguments");
+    int rc = require_sm100();
+    if (rc != B200LA_SUCCESS)
+        return rc;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    prof_begin(KC_SELECT, s);
+    k_mlp_grad<<<(int)((batch + kMlpThreads - 1) / kMlpThreads), kMlpThreads, 0, s>>>(params, x, labels, (int)batch,
+        grads, loss_sum);
+    prof_end(KC_SELECT, s);
+    B200LA_LAUNCH_CHECK();
+    return B200LA_SUCCESS;
+}
+
+B200LA_API int b200la_mlp_adam(float* params, float* grads, float* m1, float* m2, int64_t batch, float lr,
+    float beta1, float beta2, float eps, int step, float weight_decay, void* stream)
+{
+    if (!params || !grads || !m1 || !m2 || batch <= 0 || step < 1)
+        return set_error(B200LA_INVALID_ARGUMENT, "mlp_adam: invalid arguments");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    prof_begin(KC_SELECT, s);
+    k_adam<<<(kParams + 255) / 256, 256, 0, s>>>(params, grads, m1, m2, 1.f / (float)batch, lr, beta1, beta2, eps, step,
+        weight_decay);
+    prof_end(KC_SELECT, s);
+    B200LA_LAUNCH_CHECK();
+    return B200LA_SUCCESS;
+}
+
+B200LA_API int b200la_matrix_stats(const double* a, int64_t n, const float* lu32, unsigned long long* out,
+    void* stream)
+{
+    if ((!a && !lu32) || !out || n <= 0 || n > 65536)
+        return set_error(B200LA_INVALID_ARGUMENT, "matrix_stats: invalid arguments");
+    int rc = require_sm100();
+    if (rc != B200LA_SUCCESS)
+        return rc;
+    return enqueue_matrix_stats(a, (int)n, lu32, out, static_cast<cudaStream_t>(stream));
+}
+}
