@@ -25,7 +25,9 @@ Weights are stored as JSON with a schema tag, the feature standardization and
 a SHA-256 of the float32 parameter bytes (checked on load).
 
 CLI (GPU):
-    python -m linearalgebra_b200.selector train --systems 50000 --out W.json
+    python -m linearalgebra_b200.selector label --start 0 --count 25000 --out shard0.npz
+    python -m linearalgebra_b200.selector train --dataset shard0.npz,shard1.npz --out W.json
+    python -m linearalgebra_b200.selector train --systems 50000 --out W.json  # label + train
     python -m linearalgebra_b200.selector evaluate --weights W.json --systems 5000
 """
 from __future__ import annotations
@@ -386,32 +388,49 @@ def evaluate(net: Network, count: int, seed: int, strategies=STRATEGIES, warmup:
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
     sub = ap.add_subparsers(dest="cmd", required=True)
+    lab = sub.add_parser("label", help="label a slice of the seeded training stream into an npz shard")
+    lab.add_argument("--systems", type=int, default=50000, help="length of the seeded stream")
+    lab.add_argument("--seed", type=int, default=1)
+    lab.add_argument("--start", type=int, default=0)
+    lab.add_argument("--count", type=int, default=None)
+    lab.add_argument("--out", required=True)
     t = sub.add_parser("train")
     t.add_argument("--systems", type=int, default=50000)
     t.add_argument("--seed", type=int, default=1)
     t.add_argument("--epochs", type=int, default=300)
     t.add_argument("--out", default=DEFAULT_WEIGHTS)
-    t.add_argument("--dataset", default=None, help="npz to save the labelled dataset to / load it from")
+    t.add_argument("--dataset", default=None,
+                   help="comma-separated npz shards to train on (else label --systems here)")
     e = sub.add_parser("evaluate")
     e.add_argument("--weights", default=DEFAULT_WEIGHTS)
     e.add_argument("--systems", type=int, default=5000)
     e.add_argument("--seed", type=int, default=2)
     e.add_argument("--out", default=None)
     args = ap.parse_args(argv)
+    if args.cmd == "label":
+        systems = sample_stream(args.systems, args.seed)
+        end = len(systems) if args.count is None else min(len(systems), args.start + args.count)
+        t0 = time.time()
+        parts = []
+        for c0 in range(args.start, end, 2500):
+            parts.append(generate_systems(systems[c0:min(c0 + 2500, end)], log_every=500))
+            d = {k: np.concatenate([p[k] for p in parts]) for k in parts[0]}
+            d["label_seconds"] = np.array(time.time() - t0)
+            d["stream"] = np.array([args.systems, args.seed, args.start, c0 + len(parts[-1]["labels"])])
+            np.savez_compressed(args.out, **d)
+        print(json.dumps({"systems": int(len(d["labels"])), "seconds": float(d["label_seconds"]),
+                          "class_counts": np.bincount(d["labels"], minlength=4).tolist()}))
+        return
     if args.cmd == "train":
-        if args.dataset and os.path.exists(args.dataset):
-            d = dict(np.load(args.dataset))
+        if args.dataset:
+            shards = [dict(np.load(f)) for f in args.dataset.split(",")]
+            d = {k: np.concatenate([sh[k] for sh in shards]) for k in ("features", "labels", "n", "kappa",
+                                                                          "converged", "ms")}
+            d["label_seconds"] = np.array(sum(float(sh["label_seconds"]) for sh in shards))
         else:
-            # label in chunks of the same seeded stream, saving after each
             t0 = time.time()
-            systems = sample_stream(args.systems, args.seed)
-            parts = []
-            for c0 in range(0, args.systems, 2500):
-                parts.append(generate_systems(systems[c0:c0 + 2500], log_every=500))
-                d = {k: np.concatenate([p[k] for p in parts]) for k in parts[0]}
-                d["label_seconds"] = np.array(time.time() - t0)
-                if args.dataset:
-                    np.savez_compressed(args.dataset, **d)
+            d = generate(args.systems, args.seed, log_every=1000)
+            d["label_seconds"] = np.array(time.time() - t0)
         nval = max(1, len(d["labels"]) // 10)
         t1 = time.time()
         net, hist = train(d["features"][nval:], d["labels"][nval:], epochs=args.epochs, log_every=50)
