@@ -1,0 +1,64 @@
+/*
+ * extern "C" wrapper over the reference's own CUDA_BLAS (cuSOLVER) LU solve,
+ * linear_solver<double, linalg_backend::CUDA_BLAS> in LU mode, so bench.py
+ * can time the reference's GPU backend beside this library.  Compiled
+ * together with the reference's sources
+ * (src/matrix_operation/gpu/cublas/{linear_solver,lu_decomposition,
+ * transpose,cholesky_decomposition}_cublas.cpp) by baseline/Makefile into
+ * baseline/_ref/libref_cublas.so.
+ *
+ * BASELINE INFRASTRUCTURE ONLY.  Nothing in the B200 library links or calls
+ * this; it runs NVIDIA's cuSOLVER and cuBLAS exactly as the reference does.
+ *
+ * All pointers are device pointers (the reference's GPU contract); the
+ * caller passes a workspace of ref_cublas_dgesv_workspace_size(n) bytes.
+ * Returns 0, or -1 if the reference threw (message in ref_cublas_last_error).
+ */
+#include <cstdint>
+#include <cstring>
+#include <exception>
+#include <string>
+
+#include "include/matrix_operation/linear_solver.h"
+
+using linalg::linalg_backend;
+using linalg::linear_solver_type;
+
+namespace
+{
+thread_local std::string g_err;
+}
+
+extern "C" {
+
+const char* ref_cublas_last_error(void) { return g_err.c_str(); }
+
+size_t ref_cublas_dgesv_workspace_size(int64_t n)
+{
+    try
+    {
+        return linalg::linear_solver<double, linalg_backend::CUDA_BLAS>::workspace_size(
+            n, linear_solver_type::LU_LINEAR_SOLVER);
+    }
+    catch (const std::exception& e)
+    {
+        g_err = e.what();
+        return 0;
+    }
+}
+
+int ref_cublas_dgesv(double* m, int64_t* pivot, int64_t n, double* x, void* ws, size_t ws_bytes, void* stream)
+{
+    try
+    {
+        linalg::linear_solver<double, linalg_backend::CUDA_BLAS>::apply(m, reinterpret_cast<linalg_int*>(pivot), n,
+            x, linear_solver_type::LU_LINEAR_SOLVER, ws, ws_bytes, stream);
+        return 0;
+    }
+    catch (const std::exception& e)
+    {
+        g_err = e.what();
+        return -1;
+    }
+}
+}

@@ -12,9 +12,11 @@ than the 126 MB L2, so no L2 flush is needed between steps.
 --impl b200 (default) prints one JSON line with the device-timed value, the
 end-to-end value through the C ABI with host buffers, the roofline of the
 dominant kernel (timed live with the library's launch recorder), the CPU
-baseline (the reference's own NATIVE LU solve, bounded sample) and the clocks
-seen during the timed region.  --impl reference times the reference's NATIVE
-CPU implementation alone on a bounded sample of the same workload.  With
+baseline (the reference's own NATIVE LU solve, bounded sample), the clocks
+seen during the timed region, and the reference's own cuSOLVER (CUDA_BLAS)
+LU solve of the same system as a GPU baseline.  --impl reference times the
+reference's NATIVE CPU implementation alone on a bounded sample of the same
+workload.  With
 N > 1 (torchrun), each rank solves its own system (replicas: a single dense
 LU has no data-parallel split); the value is the max over ranks.
 """
@@ -208,6 +210,57 @@ def cpu_model():
     except OSError:
         pass
     return "unknown"
+
+
+# ---------------------------------------------------------------------------
+# GPU baseline: the reference's own CUDA_BLAS LU solve (cuSOLVER), when built
+# ---------------------------------------------------------------------------
+def cusolver_reference_seconds(A, b, stream, steps: int = 2):
+    """linear_solver<double, CUDA_BLAS> LU mode from baseline/_ref on the same
+    system, timed with CUDA events on `stream` (each step restores A and b
+    by device copies, as the FP64 arm does)."""
+    import torch
+
+    path = os.path.join(ROOT, "baseline", "_ref", "libref_cublas.so")
+    if not os.path.exists(path):
+        return {"unavailable": "baseline/_ref/libref_cublas.so is not built (needs the reference sources)"}
+    lib = ctypes.CDLL(path)
+    lib.ref_cublas_dgesv_workspace_size.restype = ctypes.c_size_t
+    lib.ref_cublas_dgesv_workspace_size.argtypes = [ctypes.c_int64]
+    lib.ref_cublas_dgesv.restype = ctypes.c_int
+    lib.ref_cublas_dgesv.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p,
+                                     ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p]
+    lib.ref_cublas_last_error.restype = ctypes.c_char_p
+    n = A.shape[0]
+    nbytes = int(lib.ref_cublas_dgesv_workspace_size(n))
+    ws = torch.empty(max(nbytes, 256), dtype=torch.uint8, device=A.device)
+    m = torch.empty_like(A)
+    xx = torch.empty_like(b)
+    piv = torch.empty(n, dtype=torch.int64, device=A.device)
+
+    def step():
+        m.copy_(A)
+        xx.copy_(b)
+        if lib.ref_cublas_dgesv(m.data_ptr(), piv.data_ptr(), n, xx.data_ptr(), ws.data_ptr(), nbytes,
+                                stream.cuda_stream) != 0:
+            raise RuntimeError(lib.ref_cublas_last_error().decode())
+
+    step()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    r = b - A @ xx
+    eta = (r.abs().max() / (A.abs().sum(1).max() * xx.abs().max() + b.abs().max())).item()
+    out = {"value": e0.elapsed_time(e1) / steps / 1e3, "unit": "s", "backward_error": eta, "steps": steps,
+           "what": "the reference's linear_solver<double,CUDA_BLAS> LU mode (cuSOLVER getrf/getrs with the "
+                   "reference's row/column-major transposes and host pivot round trip), same system"}
+    del m, xx, piv, ws
+    torch.cuda.empty_cache()
+    return out
 
 
 # ---------------------------------------------------------------------------
@@ -483,6 +536,10 @@ def run_b200(args, world, rank, local):
                "d2h_bytes_per_step": 8 * n, "steps": e_steps}
         del hA, hb, hx, dA, db
 
+    cusolver = None
+    if rank == 0 and world == 1 and not args.no_compare:
+        cusolver = cusolver_reference_seconds(A, b, stream)
+
     batched = None
     if not args.no_batched:
         del m, xf, ws
@@ -531,6 +588,7 @@ def run_b200(args, world, rank, local):
             "speedup_vs_fp64_lu": (other["s"] / (ms_per_step / 1e3)) if other and args.method == "mixed" else None,
             "roofline": roofline,
             "cpu_baseline": cpu,
+            "cusolver_baseline": cusolver,
             "e2e": e2e,
             "gpu_launches": int(launches),
             "breakdown_one_step": breakdown,
