@@ -677,17 +677,23 @@ __global__ void __launch_bounds__(kPanelThreads) k_panel(T* __restrict__ A, int 
 // ---------------------------------------------------------------------------
 // Panel factorization inside one thread-block cluster.
 //
-// Used when the panel's rows fit in the shared memory of one cluster of
-// `cl` CTAs (16 where the device allows that cluster size, else 8).  Same
-// arithmetic as k_panel; the per-column agreement on the pivot goes through
-// distributed shared memory: each CTA posts its candidate (key, row) in its
-// own shared memory, and after a cluster barrier every CTA reads all of
-// them, then reads the pivot row (and, for the owner of row p, the old row c)
-// straight from the owning CTA's shared memory.  A second cluster barrier
-// keeps the swap from overwriting rows that are still being read.  The
-// cluster barriers are hardware barriers over co-scheduled CTAs, so there is
-// no spin-wait in this kernel.
+// Used when the panel's rows fit in the shared memory of one cluster of `CL`
+// CTAs (a power of two up to 16, chosen per panel from its height).  Same
+// arithmetic as k_panel.  Per column, one cluster barrier:
+//   * before it, every CTA posts in its own shared memory (double-buffered
+//     by column parity) its candidate's key, row index and the candidate
+//     row's w values, and the owner of the diagonal row c posts row c;
+//   * after it, warp 0 reads the CL keys while the other warps copy every
+//     CTA's posted candidate row and the posted row c into local shared
+//     memory (all reads independent, so the distributed-shared-memory
+//     latency is paid once); the winner's copy is the pivot row.
+// A slot of parity q is rewritten two columns later, after the next barrier,
+// which no CTA passes before every CTA has finished reading it, so no second
+// barrier is needed.  Cluster barriers are hardware barriers over
+// co-scheduled CTAs: there is no spin-wait in this kernel.
 // ---------------------------------------------------------------------------
+constexpr int kMaxCluster = 16;
+
 template <typename T>
 __global__ void __launch_bounds__(kPanelThreads, 1) k_panel_cluster(T* __restrict__ A, int n, int k,
     int w, int rows_per_cta, int64_t* __restrict__ pivot, PermList* __restrict__ perm,
@@ -697,13 +703,15 @@ __global__ void __launch_bounds__(kPanelThreads, 1) k_panel_cluster(T* __restric
     cg::cluster_group cluster = cg::this_cluster();
 
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    __shared__ __align__(16) T urow[kNB];
-    __shared__ __align__(16) T drow[kNB];
+    __shared__ __align__(16) T cand[kMaxCluster][kNB];  // every CTA's posted candidate row
+    __shared__ __align__(16) T drow[kNB];               // row c
+    __shared__ __align__(16) T post_data[2][kNB];       // read by the cluster
+    __shared__ __align__(16) T post_crow[2][kNB];
+    __shared__ double post_key[2];
+    __shared__ int    post_row[2];
     __shared__ int    piv_loc[kNB];
     __shared__ double red_key[kPanelThreads / 32 + 1];
     __shared__ int    red_row[kPanelThreads / 32 + 1];
-    __shared__ double post_key;  // this CTA's candidate, read by the cluster
-    __shared__ int    post_row;
     __shared__ int    s_p, s_rank_p;
 
     const int tid  = threadIdx.x;
@@ -739,21 +747,34 @@ __global__ void __launch_bounds__(kPanelThreads, 1) k_panel_cluster(T* __restric
     int64_t first_zero = -1;
     for (int jj = 0; jj < w; ++jj)
     {
-        const int c = k + jj;
+        const int  c      = k + jj;
+        const int  par    = jj & 1;
+        const int  rank_c = (c - k) / rows_per_cta;
+        const bool own_c  = b == rank_c;
+        // ---- post
         if (tid == 0)
         {
-            post_key = cand_key;
-            post_row = cand_row;
+            post_key[par] = cand_key;
+            post_row[par] = cand_row;
         }
-        cluster.sync();  // every CTA's candidate (and its rows) is readable
+        if (tid < w && cand_row != INT_MAX)
+        {
+            post_data[par][tid] = loc[(size_t)(cand_row - r0) * ldl + tid];
+        }
+        else if (own_c && tid >= 64 && tid < 64 + w)
+        {
+            post_crow[par][tid - 64] = loc[(size_t)(c - r0) * ldl + (tid - 64)];
+        }
+        cluster.sync();  // every CTA's posts are readable
+        // ---- gather: keys (warp 0), candidate rows and row c (warps 1..)
         if (warp == 0)
         {
             double wk = -2.0;
             int    wr = INT_MAX, wrank = -1;
             if (lane < CL)
             {
-                wk    = *cluster.map_shared_rank(&post_key, lane);
-                wr    = *cluster.map_shared_rank(&post_row, lane);
+                wk    = cluster.map_shared_rank(post_key, lane)[par];
+                wr    = cluster.map_shared_rank(post_row, lane)[par];
                 wrank = lane;
             }
 #pragma unroll
@@ -775,12 +796,31 @@ __global__ void __launch_bounds__(kPanelThreads, 1) k_panel_cluster(T* __restric
                 s_rank_p = wrank;
             }
         }
+        else
+        {
+            // CL candidate rows and row c, w values each, over warps 1..7
+            for (int e = tid - 32; e < (CL + 1) * kNB; e += kPanelThreads - 32)
+            {
+                const int q  = e / kNB;
+                const int cc = e - q * kNB;
+                if (cc < w)
+                {
+                    if (q < CL)
+                    {
+                        cand[q][cc] = cluster.map_shared_rank(&post_data[0][0], q)[par * kNB + cc];
+                    }
+                    else
+                    {
+                        drow[cc] = cluster.map_shared_rank(&post_crow[0][0], rank_c)[par * kNB + cc];
+                    }
+                }
+            }
+        }
         __syncthreads();
         const int  p      = s_p;
         const int  rank_p = s_rank_p;
-        const int  rank_c = (c - k) / rows_per_cta;
-        const bool own_c  = b == rank_c;
         const bool own_p  = p != c && b == rank_p;
+        const T*   urow   = cand[rank_p];
         if (tid == 0)
         {
             piv_loc[jj] = p;
@@ -789,17 +829,6 @@ __global__ void __launch_bounds__(kPanelThreads, 1) k_panel_cluster(T* __restric
                 pivot[c] = (int64_t)p + 1;
             }
         }
-        if (tid < w)
-        {
-            const T* prow = cluster.map_shared_rank(loc, rank_p) + (size_t)(p - (k + rank_p * rows_per_cta)) * ldl;
-            urow[tid]     = prow[tid];
-        }
-        else if (own_p && tid >= 64 && tid < 64 + w)
-        {
-            const T* crow = cluster.map_shared_rank(loc, rank_c) + (size_t)(c - (k + rank_c * rows_per_cta)) * ldl;
-            drow[tid - 64] = crow[tid - 64];
-        }
-        cluster.sync();  // remote reads of rows p and c are complete
         if (p != c)
         {
             if (own_c)
@@ -852,8 +881,12 @@ __global__ void __launch_bounds__(kPanelThreads, 1) k_panel_cluster(T* __restric
 }
 
 // Row interchanges outside the panel and, right of it, U12 = L11^-1 A12.
-// CTA b < n_left: columns [b*kSwapCols, ...) of [0, k); otherwise columns of
-// [k+w, n).  256 threads: 4 row groups x 64 columns for the gather/scatter
+// CTA b < n_left: columns [left_begin + b*kSwapCols, ...) of
+// [left_begin, left_end), interchanges only; otherwise columns of
+// [k+w, right_end), with U12 solved for those below u12_end.  (The plain LU
+// passes left [0, k) and right [k+w, n); the mixed LU's look-ahead applies an
+// outer block's interchanges right of the block in a later launch with only
+// a left range.)  256 threads: 4 row groups x 64 columns for the gather/scatter
 // (each thread loads its up to 32 rows before storing, so the loads overlap),
 // then one thread per column for the substitution.
 constexpr int kSwapThreads = 256;
@@ -867,7 +900,7 @@ template <typename T> constexpr size_t laswp_smem_bytes()
 
 template <typename T>
 __global__ void __launch_bounds__(kSwapThreads) k_laswp_trsm(T* __restrict__ A, int n, int k, int w,
-    const PermList* __restrict__ perm, int n_left, int u12_end)
+    const PermList* __restrict__ perm, int n_left, int u12_end, int left_begin, int left_end, int right_end)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T(*staged)[kSwapCols] = reinterpret_cast<T(*)[kSwapCols]>(smem_raw);  // [2*kNB]
@@ -876,12 +909,12 @@ __global__ void __launch_bounds__(kSwapThreads) k_laswp_trsm(T* __restrict__ A, 
     const int  tid   = threadIdx.x;
     const int  cl    = tid % kSwapCols;
     const int  rg    = tid / kSwapCols;
-    const int  c0    = (int)blockIdx.x < n_left ? blockIdx.x * kSwapCols
-                                                : k + w + (blockIdx.x - n_left) * kSwapCols;
-    // `left`: only the interchanges (columns left of the panel, or right of
-    // it at or beyond u12_end, whose U12 rows are solved later)
+    const int  c0    = (int)blockIdx.x < n_left ? left_begin + (int)blockIdx.x * kSwapCols
+                                                : k + w + ((int)blockIdx.x - n_left) * kSwapCols;
+    // `left`: only the interchanges (the left range, or right of the panel
+    // at or beyond u12_end, whose U12 rows are solved later)
     const bool left  = (int)blockIdx.x < n_left || c0 >= u12_end;
-    const int  cend  = (int)blockIdx.x < n_left ? k : n;
+    const int  cend  = (int)blockIdx.x < n_left ? left_end : right_end;
     const int  col   = c0 + cl;
     const bool valid = col < cend;
     const int  cnt   = perm->count;

@@ -27,6 +27,7 @@
 #include <atomic>
 #include <cmath>
 #include <cstring>
+#include <mutex>
 #include <vector>
 
 #include "lu_driver.cuh"
@@ -461,6 +462,7 @@ struct MixedPlan
     uint64_t*          xll;     // flagged copies of solved blocks (k_trsv_blocks)
     double*            V;       // GMRES basis (m+1) x n
     double*            h;       // GMRES dot products (m+1)
+    PermList*          perms;   // interchange lists of an outer block's four panels
     float*             sel;     // selector network input (12) and output (4)
     float*             l21inv;  // FP8: inverse row scales of L21
     float*             u12inv;  // FP8: inverse row scales of U12^T
@@ -496,6 +498,7 @@ MixedPlan plan_mixed(Arena& a, int64_t n, int64_t nrhs, int restart, bool fp64_f
     p.u12op    = a.next<float>((size_t)n * kOuterNB);
     p.u12small = a.next<float>((size_t)n * kOuterNB);
     p.perm     = a.next<int32_t>((size_t)n);
+    p.perms    = a.next<PermList>(kOuterNB / kNB);
     p.sel      = a.next<float>(64);
     p.l21inv   = a.next<float>((size_t)n);
     p.u12inv   = a.next<float>((size_t)n);
@@ -517,7 +520,123 @@ MixedPlan plan_mixed(Arena& a, int64_t n, int64_t nrhs, int restart, bool fp64_f
     return p;
 }
 
+// Inner panels of the outer block [K, Kend): 64-column panels, their row
+// interchanges on columns [0, Kend) (right of the block they are applied
+// later by enqueue_block_swaps), U12 inside the block and the SIMT updates
+// inside the block.  Panel j's interchange list goes to p.perms[j].
+int enqueue_block_panels(MixedPlan& p, int n, int K, int Kend, int cl, int gmax, cudaStream_t s)
+{
+    float* a32 = p.a32;
+    int    rc  = B200LA_SUCCESS;
+    for (int k = K, j = 0; k < Kend; k += kNB, ++j)
+    {
+        const int        w  = n - k < kNB ? n - k : kNB;
+        GetrfPlan<float> gp = p.gp;
+        gp.perm             = p.perms + j;
+        if ((rc = launch_panel<float>(a32, n, k, w, p.piv, gp, cl, gmax, s)) != B200LA_SUCCESS)
+            return rc;
+        const int nl = (k + kSwapCols - 1) / kSwapCols;
+        const int nr = (Kend - (k + w) + kSwapCols - 1) / kSwapCols;
+        if (nl + nr > 0)
+        {
+            prof_begin(KC_SWAP, s);
+            k_laswp_trsm<float><<<nl + nr, kSwapThreads, laswp_smem_bytes<float>(), s>>>(a32, n, k, w, gp.perm, nl,
+                Kend, 0, k, Kend);
+            prof_end(KC_SWAP, s);
+            B200LA_LAUNCH_CHECK();
+        }
+        const int rest  = n - k - w;
+        const int ncols = Kend - (k + w);
+        if (rest > 0 && ncols > 0)
+        {
+            dim3 grid((ncols + kChunkN - 1) / kChunkN, (rest + kBandM - 1) / kBandM);
+            prof_begin(KC_TRAILING, s);
+            k_trailing<float><<<grid, 128, trailing_smem_bytes<float>(), s>>>(a32, n, k, w, ncols);
+            prof_end(KC_TRAILING, s);
+            B200LA_LAUNCH_CHECK();
+        }
+    }
+    return B200LA_SUCCESS;
+}
+
+// The outer block's row interchanges on columns [Kend, n), panel by panel in
+// the order they were chosen.
+int enqueue_block_swaps(MixedPlan& p, int n, int K, int Kend, cudaStream_t s)
+{
+    const int cols = n - Kend;
+    if (cols <= 0)
+        return B200LA_SUCCESS;
+    const int nl = (cols + kSwapCols - 1) / kSwapCols;
+    for (int k = K, j = 0; k < Kend; k += kNB, ++j)
+    {
+        const int w = n - k < kNB ? n - k : kNB;
+        prof_begin(KC_SWAP, s);
+        k_laswp_trsm<float><<<nl, kSwapThreads, laswp_smem_bytes<float>(), s>>>(p.a32, n, k, w, p.perms + j, nl, n,
+            Kend, n, n);
+        prof_end(KC_SWAP, s);
+        B200LA_LAUNCH_CHECK();
+    }
+    return B200LA_SUCCESS;
+}
+
+// A high-priority stream per device for the look-ahead panels.
+cudaStream_t lookahead_stream(int* rc)
+{
+    static std::mutex   m;
+    static cudaStream_t streams[64] = {};
+    int                 dev         = 0;
+    *rc                             = B200LA_SUCCESS;
+    cudaError_t e                   = cudaGetDevice(&dev);
+    if (e != cudaSuccess)
+    {
+        *rc = cuda_check(e, "cudaGetDevice");
+        return nullptr;
+    }
+    if (dev < 0 || dev >= 64)
+    {
+        *rc = set_error(B200LA_NOT_SUPPORTED, "device index %d out of range", dev);
+        return nullptr;
+    }
+    std::lock_guard<std::mutex> lock(m);
+    if (streams[dev] == nullptr)
+    {
+        int least = 0, greatest = 0;
+        cudaDeviceGetStreamPriorityRange(&least, &greatest);
+        e = cudaStreamCreateWithPriority(&streams[dev], cudaStreamNonBlocking, greatest);
+        if (e != cudaSuccess)
+        {
+            streams[dev] = nullptr;
+            *rc          = cuda_check(e, "cudaStreamCreateWithPriority");
+            return nullptr;
+        }
+    }
+    return streams[dev];
+}
+
+bool lookahead_enabled()
+{
+    const char* e = getenv("B200LA_MIXED_LOOKAHEAD");
+    return !(e != nullptr && e[0] == '0');
+}
+
+// The tensor-core trailing update of the outer block (columns [c0, n) of
+// A22 = rows and columns from Kend), operands from the block's copies.
+int enqueue_block_update(MixedPlan& p, int n, int Kend, int c0, int kind, bool split, const CUtensorMap& ma,
+    const CUtensorMap& mb, const CUtensorMap& mas, const CUtensorMap& mbs, int ncols, cudaStream_t s)
+{
+    const int rest = n - Kend;
+    return enqueue_tc_update(kind, split, ma, mb, mas, mbs, p.a32 + (int64_t)Kend * n + c0, n, rest, ncols, kOuterNB,
+        p.gp.st, s, p.l21inv, p.u12inv + (c0 - Kend));
+}
+
 // Mixed-precision factorization of p.a32 in place; pivots in p.piv.
+//
+// Look-ahead: after outer block K's operand copies, the tensor-core update
+// first covers the next block's 256 columns only; the next block's panels
+// then run on a high-priority stream while the rest of the update runs on
+// `s`.  The next block's interchanges right of it wait until that update is
+// done (enqueue_block_swaps), so both streams touch disjoint columns; every
+// per-element operation is the same as without look-ahead.
 int enqueue_getrf_mixed(MixedPlan& p, int n, int kind, bool split, cudaStream_t s)
 {
     int rc = clear_panel_exchange<float>(p.gp, s);
@@ -528,7 +647,9 @@ int enqueue_getrf_mixed(MixedPlan& p, int n, int kind, bool split, cudaStream_t 
     int cl = 0, gmax = 0;
     if ((rc = panel_config<float>(cl, gmax)) != B200LA_SUCCESS)
         return rc;
-    CUtensorMap ma, mb, mas, mbs;
+    const int  elem = tc_elem_bytes(kind);
+    const bool la   = lookahead_enabled() && n > 2 * kOuterNB;
+    CUtensorMap ma, mb, mas, mbs, mb2, mbs2;
     if ((rc = make_kmajor_map(&ma, p.l21op, kind, n, kOuterNB, kOuterNB, kTcBM)) != B200LA_SUCCESS ||
         (rc = make_kmajor_map(&mb, p.u12op, kind, n, kOuterNB, kOuterNB, kTcBN)) != B200LA_SUCCESS)
         return rc;
@@ -537,35 +658,55 @@ int enqueue_getrf_mixed(MixedPlan& p, int n, int kind, bool split, cudaStream_t 
     if (split && ((rc = make_kmajor_map(&mas, p.l21small, TC_TF32, n, kOuterNB, kOuterNB, kTcBM)) != B200LA_SUCCESS ||
                      (rc = make_kmajor_map(&mbs, p.u12small, TC_TF32, n, kOuterNB, kOuterNB, kTcBN)) != B200LA_SUCCESS))
         return rc;
+    mb2  = mb;
+    mbs2 = mbs;
+    if (la)
+    {
+        // B operand rows from the second 256 on (the columns right of the next block)
+        const size_t off = (size_t)kOuterNB * kOuterNB;
+        if ((rc = make_kmajor_map(&mb2, static_cast<unsigned char*>(p.u12op) + off * elem, kind, n - kOuterNB,
+                 kOuterNB, kOuterNB, kTcBN)) != B200LA_SUCCESS)
+            return rc;
+        if (split && (rc = make_kmajor_map(&mbs2, p.u12small + off, TC_TF32, n - kOuterNB, kOuterNB, kOuterNB,
+                          kTcBN)) != B200LA_SUCCESS)
+            return rc;
+    }
+    cudaStream_t side = s;
+    cudaEvent_t  ev_update = nullptr, ev_panels = nullptr;
+    if (la)
+    {
+        side = lookahead_stream(&rc);
+        if (rc != B200LA_SUCCESS)
+            return rc;
+        B200LA_CUDA(cudaEventCreateWithFlags(&ev_update, cudaEventDisableTiming));
+        B200LA_CUDA(cudaEventCreateWithFlags(&ev_panels, cudaEventDisableTiming));
+    }
+    struct EventGuard
+    {
+        cudaEvent_t a, b;
+        ~EventGuard()
+        {
+            if (a)
+                cudaEventDestroy(a);
+            if (b)
+                cudaEventDestroy(b);
+        }
+    } guard{ev_update, ev_panels};
+
     float* a32 = p.a32;
+    if ((rc = enqueue_block_panels(p, n, 0, n < kOuterNB ? n : kOuterNB, cl, gmax, s)) != B200LA_SUCCESS)
+        return rc;
+    bool panels_on_side = false;
     for (int K = 0; K < n; K += kOuterNB)
     {
         const int Kend = K + kOuterNB < n ? K + kOuterNB : n;
-        for (int k = K; k < Kend; k += kNB)
+        if (panels_on_side)
         {
-            const int w = n - k < kNB ? n - k : kNB;
-            if ((rc = launch_panel<float>(a32, n, k, w, p.piv, p.gp, cl, gmax, s)) != B200LA_SUCCESS)
-                return rc;
-            const int rest = n - k - w;
-            const int nl   = (k + kSwapCols - 1) / kSwapCols;
-            const int nr   = (rest + kSwapCols - 1) / kSwapCols;
-            if (nl + nr > 0)
-            {
-                prof_begin(KC_SWAP, s);
-                k_laswp_trsm<float><<<nl + nr, kSwapThreads, laswp_smem_bytes<float>(), s>>>(a32, n, k, w, p.gp.perm, nl, Kend);
-                prof_end(KC_SWAP, s);
-                B200LA_LAUNCH_CHECK();
-            }
-            const int ncols = Kend - (k + w);
-            if (rest > 0 && ncols > 0)
-            {
-                dim3 grid((ncols + kChunkN - 1) / kChunkN, (rest + kBandM - 1) / kBandM);
-                prof_begin(KC_TRAILING, s);
-                k_trailing<float><<<grid, 128, trailing_smem_bytes<float>(), s>>>(a32, n, k, w, ncols);
-                prof_end(KC_TRAILING, s);
-                B200LA_LAUNCH_CHECK();
-            }
+            B200LA_CUDA(cudaStreamWaitEvent(s, ev_panels, 0));
+            panels_on_side = false;
         }
+        if ((rc = enqueue_block_swaps(p, n, K, Kend, s)) != B200LA_SUCCESS)
+            return rc;
         const int rest = n - Kend;
         if (rest <= 0)
         {
@@ -600,9 +741,30 @@ int enqueue_getrf_mixed(MixedPlan& p, int n, int kind, bool split, cudaStream_t 
         }
         prof_end(KC_PREP, s);
         B200LA_LAUNCH_CHECK();
-        if ((rc = enqueue_tc_update(kind, split, ma, mb, mas, mbs, a32 + (int64_t)Kend * n + Kend, n, rest, rest,
-                 kOuterNB, p.gp.st, s, p.l21inv, p.u12inv)) != B200LA_SUCCESS)
-            return rc;
+        const int Kend2 = Kend + kOuterNB < n ? Kend + kOuterNB : n;
+        if (la && Kend2 < n)
+        {
+            // the next block's columns, then its panels beside the rest of the update
+            if ((rc = enqueue_block_update(p, n, Kend, Kend, kind, split, ma, mb, mas, mbs, Kend2 - Kend, s)) !=
+                B200LA_SUCCESS)
+                return rc;
+            B200LA_CUDA(cudaEventRecord(ev_update, s));
+            B200LA_CUDA(cudaStreamWaitEvent(side, ev_update, 0));
+            if ((rc = enqueue_block_panels(p, n, Kend, Kend2, cl, gmax, side)) != B200LA_SUCCESS)
+                return rc;
+            B200LA_CUDA(cudaEventRecord(ev_panels, side));
+            panels_on_side = true;
+            if ((rc = enqueue_block_update(p, n, Kend, Kend2, kind, split, ma, mb2, mas, mbs2, n - Kend2, s)) !=
+                B200LA_SUCCESS)
+                return rc;
+        }
+        else
+        {
+            if ((rc = enqueue_block_update(p, n, Kend, Kend, kind, split, ma, mb, mas, mbs, rest, s)) != B200LA_SUCCESS)
+                return rc;
+            if ((rc = enqueue_block_panels(p, n, Kend, Kend2, cl, gmax, s)) != B200LA_SUCCESS)
+                return rc;
+        }
     }
     k_status_finish<<<1, 32, 0, s>>>(p.gp.st);
     B200LA_LAUNCH_CHECK();

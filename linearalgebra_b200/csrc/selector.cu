@@ -11,6 +11,7 @@
 #include <climits>
 #include <cmath>
 #include <cstdint>
+#include <mutex>
 
 #include "common.cuh"
 
@@ -94,106 +95,178 @@ __global__ void __launch_bounds__(kMlpThreads) k_mlp_forward(const float* __rest
     }
 }
 
-// Forward + backward of the mean softmax cross-entropy over the batch:
-// grads += d(loss_sum)/d(params) (not yet divided by the batch), loss_sum +=
-// sum of per-sample losses.  One thread per sample; per-CTA gradient sums in
-// shared memory, then one global atomic add per parameter per CTA.
-__global__ void __launch_bounds__(kMlpThreads) k_mlp_grad(const float* __restrict__ params,
+// Forward + backward of the summed softmax cross-entropy: grads +=
+// d(loss_sum)/d(params), loss_sum += sum of the per-sample losses.  A CTA
+// takes kGradSamples samples in two phases:
+//   1. thread = sample: forward, softmax, and the backward deltas
+//      dl = p - onehot(y), dh2 = (W3 dl) * [h2 > 0], dh1 = (W2 dh2) * [h1 > 0],
+//      written with the activations to shared memory as [unit][sample]
+//      (row stride kGradSamples + 1, so a warp reading one sample column of
+//      consecutive units hits distinct banks);
+//   2. thread = parameter (strided): dW1 = x^T dh1, dW2 = h1^T dh2,
+//      dW3 = h2^T dl and the bias sums over the CTA's samples, in a fixed
+//      order, then one global atomic add per parameter per CTA.
+// Samples past `batch` contribute zeros.
+constexpr int kGradSamples = 128;
+constexpr int kGradLd      = kGradSamples + 1;
+constexpr int kGradUnits   = kIn + kH + kH + kOut + kH + kH;  // x h1 h2 dl dh2 dh1
+constexpr size_t grad_smem_bytes() { return sizeof(float) * ((size_t)kParams + (size_t)kGradUnits * kGradLd); }
+
+__global__ void __launch_bounds__(kGradSamples) k_mlp_grad(const float* __restrict__ params,
     const float* __restrict__ X, const int32_t* __restrict__ labels, int batch, float* __restrict__ grads,
     float* __restrict__ loss_sum)
 {
-    __shared__ float p[kParams];
-    __shared__ float g[kParams];
-    for (int i = threadIdx.x; i < kParams; i += kMlpThreads)
+    extern __shared__ float gsm[];
+    float* p   = gsm;
+    float* xs  = p + kParams;           // [kIn][kGradLd]
+    float* h1s = xs + kIn * kGradLd;    // [kH]
+    float* h2s = h1s + kH * kGradLd;    // [kH]
+    float* dls = h2s + kH * kGradLd;    // [kOut]
+    float* d2s = dls + kOut * kGradLd;  // [kH] dh2
+    float* d1s = d2s + kH * kGradLd;    // [kH] dh1
+    const int t = threadIdx.x;
+    for (int i = t; i < kParams; i += kGradSamples)
     {
         p[i] = params[i];
-        g[i] = 0.f;
     }
     __syncthreads();
-    const int b = blockIdx.x * kMlpThreads + threadIdx.x;
-    if (b < batch)
+
+    // phase 1: thread = sample
+    const int  b     = blockIdx.x * kGradSamples + t;
+    const bool valid = b < batch;
+    for (int i = 0; i < kIn; ++i)
     {
-        float x[kIn], h1[kH], h2[kH], lg[kOut];
+        xs[i * kGradLd + t] = valid ? X[(size_t)b * kIn + i] : 0.f;
+    }
+    for (int j = 0; j < kH; ++j)
+    {
+        float acc = p[kOffB1 + j];
         for (int i = 0; i < kIn; ++i)
         {
-            x[i] = X[(size_t)b * kIn + i];
+            acc = fmaf(xs[i * kGradLd + t], p[kOffW1 + i * kH + j], acc);
         }
-        mlp_forward(p, x, h1, h2, lg);
-        float m = lg[0];
-        for (int k = 1; k < kOut; ++k)
-        {
-            m = fmaxf(m, lg[k]);
-        }
-        float z = 0.f;
-        for (int k = 0; k < kOut; ++k)
-        {
-            lg[k] = expf(lg[k] - m);
-            z += lg[k];
-        }
-        const int y = labels[b];
-        float     dl[kOut];
-        for (int k = 0; k < kOut; ++k)
-        {
-            const float pk = lg[k] / z;
-            dl[k]          = pk - (k == y ? 1.f : 0.f);
-        }
-        atomicAdd(loss_sum, -logf(fmaxf(lg[y] / z, 1e-30f)));
-        // layer 3
-        float dh2[kH];
+        h1s[j * kGradLd + t] = valid ? fmaxf(acc, 0.f) : 0.f;
+    }
+    for (int j = 0; j < kH; ++j)
+    {
+        float acc = p[kOffB2 + j];
         for (int i = 0; i < kH; ++i)
         {
-            float s = 0.f;
-            for (int k = 0; k < kOut; ++k)
-            {
-                atomicAdd(&g[kOffW3 + i * kOut + k], h2[i] * dl[k]);
-                s = fmaf(p[kOffW3 + i * kOut + k], dl[k], s);
-            }
-            dh2[i] = h2[i] > 0.f ? s : 0.f;
+            acc = fmaf(h1s[i * kGradLd + t], p[kOffW2 + i * kH + j], acc);
         }
-        for (int k = 0; k < kOut; ++k)
-        {
-            atomicAdd(&g[kOffB3 + k], dl[k]);
-        }
-        // layer 2
-        float dh1[kH];
+        h2s[j * kGradLd + t] = valid ? fmaxf(acc, 0.f) : 0.f;
+    }
+    float lg[kOut];
+    for (int k = 0; k < kOut; ++k)
+    {
+        float acc = p[kOffB3 + k];
         for (int i = 0; i < kH; ++i)
         {
-            dh1[i] = 0.f;
+            acc = fmaf(h2s[i * kGradLd + t], p[kOffW3 + i * kOut + k], acc);
         }
+        lg[k] = acc;
+    }
+    float m = lg[0];
+    for (int k = 1; k < kOut; ++k)
+    {
+        m = fmaxf(m, lg[k]);
+    }
+    float z = 0.f;
+    for (int k = 0; k < kOut; ++k)
+    {
+        lg[k] = expf(lg[k] - m);
+        z += lg[k];
+    }
+    const int y    = valid ? labels[b] : 0;
+    float     loss = valid ? -logf(fmaxf(lg[y] / z, 1e-30f)) : 0.f;
+    for (int k = 0; k < kOut; ++k)
+    {
+        dls[k * kGradLd + t] = valid ? lg[k] / z - (k == y ? 1.f : 0.f) : 0.f;
+    }
+    for (int i = 0; i < kH; ++i)
+    {
+        float acc = 0.f;
+        for (int k = 0; k < kOut; ++k)
+        {
+            acc = fmaf(p[kOffW3 + i * kOut + k], dls[k * kGradLd + t], acc);
+        }
+        d2s[i * kGradLd + t] = h2s[i * kGradLd + t] > 0.f ? acc : 0.f;
+    }
+    for (int i = 0; i < kH; ++i)
+    {
+        float acc = 0.f;
         for (int j = 0; j < kH; ++j)
         {
-            if (dh2[j] == 0.f)
-            {
-                continue;
-            }
-            atomicAdd(&g[kOffB2 + j], dh2[j]);
-            for (int i = 0; i < kH; ++i)
-            {
-                atomicAdd(&g[kOffW2 + i * kH + j], h1[i] * dh2[j]);
-                dh1[i] = fmaf(p[kOffW2 + i * kH + j], dh2[j], dh1[i]);
-            }
+            acc = fmaf(p[kOffW2 + i * kH + j], d2s[j * kGradLd + t], acc);
         }
-        // layer 1
-        for (int j = 0; j < kH; ++j)
-        {
-            const float d = h1[j] > 0.f ? dh1[j] : 0.f;
-            if (d == 0.f)
-            {
-                continue;
-            }
-            atomicAdd(&g[kOffB1 + j], d);
-            for (int i = 0; i < kIn; ++i)
-            {
-                atomicAdd(&g[kOffW1 + i * kH + j], x[i] * d);
-            }
-        }
+        d1s[i * kGradLd + t] = h1s[i * kGradLd + t] > 0.f ? acc : 0.f;
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1)
+    {
+        loss += __shfl_down_sync(0xffffffffu, loss, off);
+    }
+    if ((t & 31) == 0 && loss != 0.f)
+    {
+        atomicAdd(loss_sum, loss);
     }
     __syncthreads();
-    for (int i = threadIdx.x; i < kParams; i += kMlpThreads)
+
+    // phase 2: thread = parameter
+    for (int q = t; q < kParams; q += kGradSamples)
     {
-        if (g[i] != 0.f)
+        const float* u;  // left factor row (nullptr: bias, sum of v)
+        const float* v;
+        if (q < kOffB1)
         {
-            atomicAdd(&grads[i], g[i]);
+            u = xs + (q / kH) * kGradLd;
+            v = d1s + (q % kH) * kGradLd;
+        }
+        else if (q < kOffW2)
+        {
+            u = nullptr;
+            v = d1s + (q - kOffB1) * kGradLd;
+        }
+        else if (q < kOffB2)
+        {
+            u = h1s + ((q - kOffW2) / kH) * kGradLd;
+            v = d2s + ((q - kOffW2) % kH) * kGradLd;
+        }
+        else if (q < kOffW3)
+        {
+            u = nullptr;
+            v = d2s + (q - kOffB2) * kGradLd;
+        }
+        else if (q < kOffB3)
+        {
+            u = h2s + ((q - kOffW3) / kOut) * kGradLd;
+            v = dls + ((q - kOffW3) % kOut) * kGradLd;
+        }
+        else
+        {
+            u = nullptr;
+            v = dls + (q - kOffB3) * kGradLd;
+        }
+        float acc = 0.f;
+        if (u != nullptr)
+        {
+#pragma unroll 8
+            for (int s2 = 0; s2 < kGradSamples; ++s2)
+            {
+                acc = fmaf(u[s2], v[s2], acc);
+            }
+        }
+        else
+        {
+#pragma unroll 8
+            for (int s2 = 0; s2 < kGradSamples; ++s2)
+            {
+                acc += v[s2];
+            }
+        }
+        if (acc != 0.f)
+        {
+            atomicAdd(&grads[q], acc);
         }
     }
 }
@@ -388,9 +461,23 @@ B200LA_API int b200la_mlp_gradient(const float* params, const float* x, const in
     if (rc != B200LA_SUCCESS)
         return rc;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
+    static std::mutex attr_m;
+    static bool       attr_done[64] = {};
+    int               dev           = 0;
+    B200LA_CUDA(cudaGetDevice(&dev));
+    {
+        std::lock_guard<std::mutex> lock(attr_m);
+        if (dev < 0 || dev >= 64 || !attr_done[dev])
+        {
+            B200LA_CUDA(cudaFuncSetAttribute(k_mlp_grad, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                (int)grad_smem_bytes()));
+            if (dev >= 0 && dev < 64)
+                attr_done[dev] = true;
+        }
+    }
     prof_begin(KC_SELECT, s);
-    k_mlp_grad<<<(int)((batch + kMlpThreads - 1) / kMlpThreads), kMlpThreads, 0, s>>>(params, x, labels, (int)batch,
-        grads, loss_sum);
+    k_mlp_grad<<<(int)((batch + kGradSamples - 1) / kGradSamples), kGradSamples, grad_smem_bytes(), s>>>(params, x,
+        labels, (int)batch, grads, loss_sum);
     prof_end(KC_SELECT, s);
     B200LA_LAUNCH_CHECK();
     return B200LA_SUCCESS;

@@ -105,3 +105,31 @@ def test_mixed_fp8_escalation_chain_reaches_fp64():
     assert st == 0 and res["converged"] == 1, res
     assert res["precision_used"] == la._lib.PREC_FP64 and res["escalations"] == 3, res
     assert eta_of(a, x.cpu().numpy(), b) <= 1e-14
+
+
+@pytest.mark.parametrize("precision", ["fp32", "tf32", "fp8"])
+@pytest.mark.parametrize("n", [777, 1300, 2048])
+def test_mixed_lookahead_is_neutral(monkeypatch, precision, n):
+    """The look-ahead (next block's panels on a second stream beside the
+    rest of the tensor-core update, interchanges right of the block deferred)
+    performs the same operations.  Plain refinement is deterministic, so the
+    solution is bit-identical with the look-ahead switched off; GMRES-IR sums
+    its dot products with atomics, so there both runs must converge and agree
+    to the conditioning."""
+    a, _, b = system(n, seed=90 + n)
+    da, db = dev(a), dev(b)
+    out = {}
+    for flag in ("1", "0"):
+        monkeypatch.setenv("B200LA_MIXED_LOOKAHEAD", flag)
+        x, res, st = la.solve_mixed(da, db, precision=precision)
+        torch.cuda.synchronize()
+        assert st == 0 and res["converged"] == 1, res
+        out[flag] = (x.cpu().numpy(), res)
+    x1, r1 = out["1"]
+    x0, r0 = out["0"]
+    if r1["gmres_iterations"] == 0 and r0["gmres_iterations"] == 0 and r1["escalations"] == 0:
+        assert r1["iterations"] == r0["iterations"]
+        assert np.array_equal(x1, x0)
+    else:
+        assert eta_of(a, x1, b) <= 1e-14 and eta_of(a, x0, b) <= 1e-14
+        assert np.abs(x1 - x0).max() / np.abs(x0).max() < 1e-8
