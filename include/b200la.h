@@ -239,38 +239,44 @@ B200LA_API int b200la_mlp_adam(float* params, float* grads, float* m1, float* m2
        float lr, float beta1, float beta2, float eps, int step, float weight_decay, void* stream);
 
 /* Matrix statistics behind the features: sixteen 64-bit words at `out`
- * (device).  With `a` (n x n FP64, row-major, lda = n) the words are reset
- * and A's statistics gathered: [0] ||A||_inf, [1] max|a_ij|, [2] sum a_ij^2,
- * [3] max_i 1/(1+r_i) with r_i = |a_ii| / sum_{j!=i}|a_ij|, [4] number of
- * rows with r_i >= 1 (integer), [5] ||A||_1, [7] min|a_ii|, [8] max|a_ii|,
- * [9] sum|a_ij| (doubles as bit patterns).  With `lu32` (FP32 LU factors,
- * row-major n x n) words [6] max|u_ij|, [10] min|u_ii|, [11] max|u_ii| are
- * added.  Asynchronous. */
-B200LA_API int b200la_matrix_stats(const double* a, int64_t n, const float* lu32, unsigned long long* out,
-       void* stream);
+ * (device), reset and gathered from A (n x n FP64, row-major, lda = n):
+ * [0] ||A||_inf, [1] max|a_ij|, [2] sum a_ij^2, [3] max_i 1/(1+r_i) with
+ * r_i = |a_ii| / sum_{j!=i}|a_ij|, [4] number of rows with r_i >= 1
+ * (integer), [5] ||A||_1, [6] min row sum of |a|, [7] min|a_ii|,
+ * [8] max|a_ii|, [9] sum|a_ij|, [10] min column sum, [11] sum|a_ii| (doubles
+ * as bit patterns).  Asynchronous. */
+B200LA_API int b200la_matrix_stats(const double* a, int64_t n, unsigned long long* out, void* stream);
 
-/* The 12 selector features of A (host floats): log2(n)/12; log10 of
- * ||A||_inf/max|a|, ||A||_1/max|a|, ||A||_F/(n max|a|), mean|a|/max|a|;
- * log10(min_i r_i)/4; fraction of diagonally dominant rows;
- * log10(min|a_ii|/max|a|)/4; log10(max|a_ii|/max|a|); log10 of the growth
- * max|u_ij|/max|a|; log10 of the 1-norm condition estimate
- * ||A||_1 est(||A^-1||_1)/4 (Hager's estimator with Higham's refinements on
- * one FP32 LU of A, three-term TF32 updates); log10(min|u_ii|/max|u_ii|)/4.
- * Workspace: b200la_dsolve_mixed_workspace_size(n, 1, NULL).  *info: the
- * FP32 LU's info.  Synchronous. */
-B200LA_API int b200la_selector_features(const double* a, int64_t n, float* features, int* info,
+/* The 12 selector features of A (host floats), all from the O(n^2)
+ * statistics above: log2(n)/12; log10 of ||A||_inf/max|a|, ||A||_1/max|a|,
+ * ||A||_F/(n max|a|), mean|a|/max|a|; log10(min_i r_i)/4; the fraction of
+ * diagonally dominant rows; log10(min|a_ii|/max|a|)/4;
+ * log10(max|a_ii|/max|a|); log10(min row sum/||A||_inf)/4;
+ * log10(min column sum/||A||_1)/4; log10(mean|a_ii|/max|a|).  Workspace:
+ * 128 bytes of device memory, 8-byte aligned.  Synchronous. */
+B200LA_API int b200la_selector_features(const double* a, int64_t n, float* features, void* workspace,
+       size_t workspace_bytes, void* stream);
+
+/* 1-norm condition estimate kappa1 = ||A||_1 est(||A^-1||_1) from one FP32
+ * LU of A (three-term TF32 updates): Hager's estimator (SIAM J. Sci. Stat.
+ * Comput. 5, 1984) with Higham's stopping rules and alternating test vector
+ * (ACM TOMS 14, 1988), the solves with A and A^T applied in FP64 with the
+ * FP32 factors.  A lower bound of kappa1, usually within a small factor
+ * while kappa1 * 2^-24 < 1.  Workspace: b200la_dsolve_mixed_workspace_size(n,
+ * 1, NULL).  Returns B200LA_SINGULAR (kappa1 = inf) for an exactly singular
+ * FP32 factor.  Synchronous.  Extension: no reference counterpart. */
+B200LA_API int b200la_dcondition_estimate(const double* a, int64_t n, double* kappa1, int* info,
        void* workspace, size_t workspace_bytes, void* stream);
 
 /* Solve A x = b (one right-hand side) with the precision the network picks
  * from the features above: `params` (device) holds the 5252 weights followed
  * by 24 floats, the features' mean[12] and inverse standard deviation[12].
- * Predicted FP8, BF16 or FP32: refinement with the FP32 factors computed for
- * the features; predicted FP64: plain FP64 LU and refinement.  Refinement
- * failure escalates up to FP64 as in b200la_dsolve_mixed, so the accuracy
- * never depends on the prediction.  options->precision and ->escalate are
- * ignored.  *predicted: B200LA_PREC_* of the network's class; features: the
- * 12 features (host, may be NULL).  Workspace as b200la_dsolve_mixed with
- * nrhs = 1.  Synchronous. */
+ * The predicted precision is tried first (FP64: plain FP64 LU and
+ * refinement); refinement failure escalates up to FP64 as in
+ * b200la_dsolve_mixed, so the accuracy never depends on the prediction.
+ * options->precision and ->escalate are ignored.  *predicted: B200LA_PREC_*
+ * of the network's class; features: the 12 features (host, may be NULL).
+ * Workspace as b200la_dsolve_mixed with nrhs = 1.  Synchronous. */
 B200LA_API int b200la_dsolve_selected(const double* a, int64_t n, const double* b, double* x,
        const float* params, const b200la_refine_options* options, b200la_refine_result* result,
        int* predicted, float* features, void* workspace, size_t workspace_bytes, void* stream);

@@ -75,8 +75,9 @@ SIGNATURES: dict[str, tuple] = {
     "b200la_mlp_forward": (_i32, [_p, _p, _i64, _p, _p]),
     "b200la_mlp_gradient": (_i32, [_p, _p, _p, _i64, _p, _p, _p]),
     "b200la_mlp_adam": (_i32, [_p, _p, _p, _p, _i64, _f, _f, _f, _f, _i32, _f, _p]),
-    "b200la_matrix_stats": (_i32, [_p, _i64, _p, _p, _p]),
-    "b200la_selector_features": (_i32, [_p, _i64, _p, _p, _p, _sz, _p]),
+    "b200la_matrix_stats": (_i32, [_p, _i64, _p, _p]),
+    "b200la_selector_features": (_i32, [_p, _i64, _p, _p, _sz, _p]),
+    "b200la_dcondition_estimate": (_i32, [_p, _i64, _p, _p, _p, _sz, _p]),
     "b200la_dsolve_selected": (_i32, [_p, _i64, _p, _p, _p, _p, _p, _p, _p, _p, _sz, _p]),
 }
 

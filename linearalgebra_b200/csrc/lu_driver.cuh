@@ -18,9 +18,6 @@ namespace b200la
 int require_sm100();
 
 constexpr size_t kPanelSmemMax = 200 * 1024;
-// Rows per CTA the cluster panel aims for (two per thread): fewer CTAs per
-// cluster mean cheaper per-column barriers.
-constexpr int kClusterRows = 512;
 
 
 // Cluster size usable by k_panel_cluster on each device (0: none).
@@ -184,22 +181,7 @@ int launch_panel(T* m, int n, int k, int w, int64_t* pivot, const GetrfPlan<T>& 
         // the panel inside one thread-block cluster when its rows fit there
         if (cl > 0)
         {
-            // the smallest power-of-two cluster (up to cl) with at most
-            // kClusterRows rows per CTA, else the widest whose rows fit
-            int csel = 0;
-            for (int c2 = 1; c2 <= cl; c2 *= 2)
-            {
-                const int rows = (R + c2 - 1) / c2;
-                if ((size_t)rows * panel_ldl<T>() * sizeof(T) <= kPanelSmemMax)
-                {
-                    csel = c2;
-                    if (rows <= kClusterRows)
-                        break;
-                }
-            }
-            if (csel == 0 || (size_t)((R + csel - 1) / csel) * panel_ldl<T>() * sizeof(T) > kPanelSmemMax)
-                csel = cl;  // the widest cluster; checked below
-            const int    cl_use = csel;
+            const int    cl_use = cl;  // the widest cluster: the most update bandwidth per column
             const int    rpc_c  = (R + cl_use - 1) / cl_use;
             const size_t smem_c = (size_t)rpc_c * panel_ldl<T>() * sizeof(T);
             if (smem_c <= kPanelSmemMax)

@@ -678,21 +678,19 @@ __global__ void __launch_bounds__(kPanelThreads) k_panel(T* __restrict__ A, int 
 // Panel factorization inside one thread-block cluster.
 //
 // Used when the panel's rows fit in the shared memory of one cluster of `CL`
-// CTAs (a power of two up to 16, chosen per panel from its height).  Same
+// CTAs (16 where the device allows that cluster size, else 8).  Same
 // arithmetic as k_panel.  Per column, one cluster barrier:
 //   * before it, every CTA posts in its own shared memory (double-buffered
 //     by column parity) its candidate's key, row index and the candidate
 //     row's w values, and the owner of the diagonal row c posts row c;
-//   * after it, warp 0 reads the CL keys while the other warps copy every
-//     CTA's posted candidate row and the posted row c into local shared
-//     memory (all reads independent, so the distributed-shared-memory
-//     latency is paid once); the winner's copy is the pivot row.
+//   * after it, warp 0 reads the CL keys and picks the pivot, then the pivot
+//     row is read from its owner's posted copy (and, by the owner of row p,
+//     row c from its posted copy) through distributed shared memory.
 // A slot of parity q is rewritten two columns later, after the next barrier,
 // which no CTA passes before every CTA has finished reading it, so no second
 // barrier is needed.  Cluster barriers are hardware barriers over
 // co-scheduled CTAs: there is no spin-wait in this kernel.
 // ---------------------------------------------------------------------------
-constexpr int kMaxCluster = 16;
 
 template <typename T>
 __global__ void __launch_bounds__(kPanelThreads, 1) k_panel_cluster(T* __restrict__ A, int n, int k,
@@ -703,7 +701,7 @@ __global__ void __launch_bounds__(kPanelThreads, 1) k_panel_cluster(T* __restric
     cg::cluster_group cluster = cg::this_cluster();
 
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    __shared__ __align__(16) T cand[kMaxCluster][kNB];  // every CTA's posted candidate row
+    __shared__ __align__(16) T urow[kNB];               // the pivot row
     __shared__ __align__(16) T drow[kNB];               // row c
     __shared__ __align__(16) T post_data[2][kNB];       // read by the cluster
     __shared__ __align__(16) T post_crow[2][kNB];
@@ -766,7 +764,7 @@ __global__ void __launch_bounds__(kPanelThreads, 1) k_panel_cluster(T* __restric
             post_crow[par][tid - 64] = loc[(size_t)(c - r0) * ldl + (tid - 64)];
         }
         cluster.sync();  // every CTA's posts are readable
-        // ---- gather: keys (warp 0), candidate rows and row c (warps 1..)
+        // ---- the pivot: keys (warp 0), then the pivot row and row c
         if (warp == 0)
         {
             double wk = -2.0;
@@ -796,31 +794,19 @@ __global__ void __launch_bounds__(kPanelThreads, 1) k_panel_cluster(T* __restric
                 s_rank_p = wrank;
             }
         }
-        else
-        {
-            // CL candidate rows and row c, w values each, over warps 1..7
-            for (int e = tid - 32; e < (CL + 1) * kNB; e += kPanelThreads - 32)
-            {
-                const int q  = e / kNB;
-                const int cc = e - q * kNB;
-                if (cc < w)
-                {
-                    if (q < CL)
-                    {
-                        cand[q][cc] = cluster.map_shared_rank(&post_data[0][0], q)[par * kNB + cc];
-                    }
-                    else
-                    {
-                        drow[cc] = cluster.map_shared_rank(&post_crow[0][0], rank_c)[par * kNB + cc];
-                    }
-                }
-            }
-        }
         __syncthreads();
         const int  p      = s_p;
         const int  rank_p = s_rank_p;
         const bool own_p  = p != c && b == rank_p;
-        const T*   urow   = cand[rank_p];
+        if (tid < w)
+        {
+            urow[tid] = cluster.map_shared_rank(&post_data[0][0], rank_p)[par * kNB + tid];
+        }
+        else if (own_p && tid >= 64 && tid < 64 + w)
+        {
+            drow[tid - 64] = cluster.map_shared_rank(&post_crow[0][0], rank_c)[par * kNB + tid - 64];
+        }
+        __syncthreads();
         if (tid == 0)
         {
             piv_loc[jj] = p;

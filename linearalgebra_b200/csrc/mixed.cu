@@ -1286,7 +1286,7 @@ int hager_inverse_norm1(MixedPlan& p, int n, double* est, cudaStream_t s)
 }  // namespace
 
 // The selector's statistics kernels and network (selector.cu).
-int enqueue_matrix_stats(const double* a, int n, const float* lu32, unsigned long long* out, cudaStream_t s);
+int enqueue_matrix_stats(const double* a, int n, unsigned long long* out, cudaStream_t s);
 int enqueue_mlp_forward(const float* params, const float* x, int batch, float* probs, cudaStream_t s);
 constexpr int kSelFeatures = 12, kSelClasses = 4, kSelParams = 5252;
 
@@ -1300,39 +1300,29 @@ inline double word_to_double(unsigned long long w)
 }
 inline float safe_log10(double v) { return (float)std::log10(v > 1e-300 ? v : 1e-300); }
 
-// The 12 selector features of A (host floats); factors A in FP32 (three-term
-// TF32) into p as a side effect (*info = its LAPACK info).
-int selector_features(const double* a, int nn, MixedPlan& p, SolveState& ss, float* f, int* info,
-    b200la_refine_result& out, cudaEvent_t e0, cudaEvent_t e1, cudaStream_t s)
+// The 12 selector features of A (host floats) from its O(n^2) statistics
+// (enqueue_matrix_stats into `stats`, 16 device words).  Synchronizes `s`.
+int selector_features(const double* a, int nn, unsigned long long* stats, float* f, cudaStream_t s)
 {
-    unsigned long long* stats = p.norms + 4 + 3 * kMaxNrhsMixed;  // 16 words after the norms
-    int                 rc    = enqueue_matrix_stats(a, nn, nullptr, stats, s);
+    int rc = enqueue_matrix_stats(a, nn, stats, s);
     if (rc != B200LA_SUCCESS)
-        return rc;
-    if ((rc = mixed_factor(a, nn, 1, B200LA_PREC_FP32, p, ss, info, out, e0, e1, s)) != B200LA_SUCCESS &&
-        rc != B200LA_SINGULAR)
-        return rc;
-    if ((rc = enqueue_matrix_stats(nullptr, nn, p.a32, stats, s)) != B200LA_SUCCESS)
         return rc;
     unsigned long long h[16];
     B200LA_CUDA(cudaMemcpyAsync(h, stats, sizeof(h), cudaMemcpyDeviceToHost, s));
     B200LA_CUDA(cudaStreamSynchronize(s));
-    double ainv1 = INFINITY;
-    if (*info == 0 && (rc = hager_inverse_norm1(p, nn, &ainv1, s)) != B200LA_SUCCESS)
-        return rc;
     const double n         = nn;
     const double norm_inf  = word_to_double(h[0]);
     const double amax      = word_to_double(h[1]);
     const double fro       = std::sqrt(word_to_double(h[2]));
-    const double dd_inv    = word_to_double(h[3]);  // max over rows of 1 / (1 + ratio)
+    const double dd_inv    = word_to_double(h[3]);  // max over rows of 1 / (1 + r_i)
     const double dd_rows   = (double)h[4];
     const double norm_1    = word_to_double(h[5]);
-    const double umax      = word_to_double(h[6]);
+    const double row_min   = word_to_double(h[6]);
     const double dmin      = word_to_double(h[7]);
     const double dmax      = word_to_double(h[8]);
     const double abs_sum   = word_to_double(h[9]);
-    const double udmin     = word_to_double(h[10]);
-    const double udmax     = word_to_double(h[11]);
+    const double col_min   = word_to_double(h[10]);
+    const double diag_sum  = word_to_double(h[11]);
     const double min_ratio = dd_inv > 0 ? 1.0 / dd_inv - 1.0 : 1e30;
     f[0]  = (float)(std::log2(n) / 12.0);
     f[1]  = safe_log10(norm_inf / amax);
@@ -1343,9 +1333,9 @@ int selector_features(const double* a, int nn, MixedPlan& p, SolveState& ss, flo
     f[6]  = (float)(dd_rows / n);
     f[7]  = safe_log10(dmin / amax) / 4.0f;
     f[8]  = safe_log10(dmax / amax);
-    f[9]  = safe_log10(umax / amax);
-    f[10] = std::isfinite(ainv1) ? safe_log10(ainv1 * norm_1) / 4.0f : 5.0f;
-    f[11] = safe_log10(udmin / udmax) / 4.0f;
+    f[9]  = safe_log10(row_min / norm_inf) / 4.0f;
+    f[10] = safe_log10(col_min / norm_1) / 4.0f;
+    f[11] = safe_log10(diag_sum / (amax * n));
     return B200LA_SUCCESS;
 }
 }  // namespace
@@ -1465,17 +1455,32 @@ B200LA_API int b200la_dsolve_mixed(const double* a, int64_t n, int64_t nrhs, con
     return finish_result(out, res);
 }
 
-B200LA_API int b200la_selector_features(const double* a, int64_t n, float* features, int* info, void* ws,
+B200LA_API int b200la_selector_features(const double* a, int64_t n, float* features, void* ws, size_t ws_bytes,
+    void* stream)
+{
+    if (a == nullptr || features == nullptr || n <= 0 || n > 65536)
+        return set_error(B200LA_INVALID_ARGUMENT, "selector_features: invalid arguments");
+    if (ws == nullptr || ws_bytes < 16 * sizeof(unsigned long long) || (reinterpret_cast<uintptr_t>(ws) & 7) != 0)
+        return set_error(B200LA_WORKSPACE_TOO_SMALL, "selector_features: needs 128 bytes of 8-byte aligned workspace");
+    int rc = require_sm100();
+    if (rc != B200LA_SUCCESS)
+        return rc;
+    return selector_features(a, (int)n, static_cast<unsigned long long*>(ws), features,
+        static_cast<cudaStream_t>(stream));
+}
+
+B200LA_API int b200la_dcondition_estimate(const double* a, int64_t n, double* kappa1, int* info, void* ws,
     size_t ws_bytes, void* stream)
 {
     b200la_refine_options o;
     b200la_refine_default_options(&o);
-    if (features == nullptr)
-        return set_error(B200LA_INVALID_ARGUMENT, "selector_features: features must not be null");
+    if (kappa1 == nullptr)
+        return set_error(B200LA_INVALID_ARGUMENT, "condition_estimate: kappa1 must not be null");
     int rc = check_mixed_call(a, n, 1, a, 1, a, 1, &o, ws, ws_bytes);
     if (rc != B200LA_SUCCESS)
         return rc;
-    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    cudaStream_t s  = static_cast<cudaStream_t>(stream);
+    const int    nn = (int)n;
     Arena        ar(ws, ws_bytes);
     MixedPlan    p = plan_mixed(ar, n, 1, restart_of(&o, 1), true);
     B200LA_CUDA(cudaMemsetAsync(p.norms, 0, sizeof(unsigned long long) * (4 + 3 * kMaxNrhsMixed), s));
@@ -1483,10 +1488,26 @@ B200LA_API int b200la_selector_features(const double* a, int64_t n, float* featu
     MixedEvents          ev;
     SolveState           ss;
     int                  inf = 0;
-    if ((rc = selector_features(a, (int)n, p, ss, features, &inf, out, ev.e0, ev.e1, s)) != B200LA_SUCCESS)
+    // ||A||_1 from the statistics, then one FP32 LU (three-term TF32 updates)
+    unsigned long long* stats = p.norms + 4 + 3 * kMaxNrhsMixed;
+    if ((rc = enqueue_matrix_stats(a, nn, stats, s)) != B200LA_SUCCESS)
+        return rc;
+    unsigned long long h[16];
+    B200LA_CUDA(cudaMemcpyAsync(h, stats, sizeof(h), cudaMemcpyDeviceToHost, s));
+    if ((rc = mixed_factor(a, nn, 1, B200LA_PREC_FP32, p, ss, &inf, out, ev.e0, ev.e1, s)) != B200LA_SUCCESS &&
+        rc != B200LA_SINGULAR)
         return rc;
     if (info)
         *info = inf;
+    if (inf != 0)
+    {
+        *kappa1 = INFINITY;
+        return B200LA_SINGULAR;
+    }
+    double ainv1 = INFINITY;
+    if ((rc = hager_inverse_norm1(p, nn, &ainv1, s)) != B200LA_SUCCESS)
+        return rc;
+    *kappa1 = word_to_double(h[5]) * ainv1;
     return B200LA_SUCCESS;
 }
 
@@ -1516,10 +1537,8 @@ B200LA_API int b200la_dsolve_selected(const double* a, int64_t n, const double* 
     B200LA_CUDA(cudaMemsetAsync(p.norms, 0, sizeof(unsigned long long) * (4 + 3 * kMaxNrhsMixed), s));
     k_colmax<<<grid_for(n), 256, 0, s>>>(b, 1, nn, 1, p.norms + 4 + 2 * kMaxNrhsMixed);
     B200LA_LAUNCH_CHECK();
-    SolveState ss;
-    float      f[kSelFeatures];
-    int        info = 0;
-    if ((rc = selector_features(a, nn, p, ss, f, &info, out, ev.e0, ev.e1, s)) != B200LA_SUCCESS)
+    float f[kSelFeatures];
+    if ((rc = selector_features(a, nn, p.norms + 4 + 3 * kMaxNrhsMixed, f, s)) != B200LA_SUCCESS)
         return rc;
     if (features)
         memcpy(features, f, sizeof(f));
@@ -1544,14 +1563,10 @@ B200LA_API int b200la_dsolve_selected(const double* a, int64_t n, const double* 
         B200LA_PREC_FP64};
     if (predicted)
         *predicted = kClassPrec[cls];
-    // FP8 / BF16 / FP32: refine with the FP32 factors already made for the
-    // features (at least as accurate as the predicted precision's); FP64:
-    // plain FP64 LU.  Escalation on failure either way.
-    if (kClassPrec[cls] == B200LA_PREC_FP64)
-        rc = mixed_loop(a, nn, 1, b, 1, x, 1, B200LA_PREC_FP64, false, 0, &o, restart, p, ss, out, ev.e0, ev.e1, s);
-    else
-        rc = mixed_loop(a, nn, 1, b, 1, x, 1, B200LA_PREC_FP32, true, info, &o, restart, p, ss, out, ev.e0, ev.e1, s);
-    if (rc != B200LA_SUCCESS)
+    // the predicted precision first; refinement failure escalates
+    SolveState ss;
+    if ((rc = mixed_loop(a, nn, 1, b, 1, x, 1, kClassPrec[cls], false, 0, &o, restart, p, ss, out, ev.e0, ev.e1,
+             s)) != B200LA_SUCCESS)
         return rc;
     return finish_result(out, res);
 }

@@ -293,10 +293,11 @@ __global__ void k_adam(float* __restrict__ params, float* __restrict__ grads, fl
 // ---- matrix statistics for the selector's features ------------------------
 // Sixteen 64-bit words; non-negative doubles are kept as their bit patterns,
 // whose unsigned order is the numeric order (atomicMax / atomicMin):
-//   [0] ||A||_inf   [1] max |a_ij|   [2] sum a_ij^2   [3] max_i 1/(1+r_i),
-//   r_i = |a_ii| / sum_{j!=i} |a_ij|   [4] rows with r_i >= 1 (count)
-//   [5] ||A||_1     [6] max |u_ij| of the LU factors   [7] min |a_ii|
-//   [8] max |a_ii|  [9] sum |a_ij|   [10] min |u_ii|   [11] max |u_ii|
+//   [0] ||A||_inf (max row sum of |a|)   [1] max |a_ij|   [2] sum a_ij^2
+//   [3] max_i 1/(1+r_i), r_i = |a_ii| / sum_{j!=i} |a_ij|
+//   [4] rows with r_i >= 1 (count)   [5] ||A||_1 (max column sum)
+//   [6] min row sum   [7] min |a_ii|   [8] max |a_ii|   [9] sum |a_ij|
+//   [10] min column sum   [11] sum |a_ii|
 __device__ __forceinline__ void amax_d(unsigned long long* p, double v)
 {
     atomicMax(p, (unsigned long long)__double_as_longlong(v));
@@ -311,11 +312,11 @@ __global__ void k_stats_init(unsigned long long* out)
     const int i = threadIdx.x;
     if (i < 16)
     {
-        out[i] = (i == 7 || i == 10) ? (unsigned long long)__double_as_longlong(INFINITY) : 0ull;
+        out[i] = (i == 6 || i == 7 || i == 10) ? (unsigned long long)__double_as_longlong(INFINITY) : 0ull;
     }
 }
 
-// A warp per row: [0] [1] [2] [3] [4] [7] [8] [9].
+// A warp per row: [0] [1] [2] [3] [4] [6] [7] [8] [9] [11].
 __global__ void k_row_stats(const double* __restrict__ a, int n, unsigned long long* out)
 {
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -354,12 +355,14 @@ __global__ void k_row_stats(const double* __restrict__ a, int n, unsigned long l
         {
             atomicAdd(out + 4, 1ull);
         }
+        amin_d(out + 6, s);
         amin_d(out + 7, d);
         amax_d(out + 8, d);
+        atomicAdd(reinterpret_cast<double*>(out + 11), d);
     }
 }
 
-// [5]: one thread per column, coalesced across the warp.
+// [5] [10]: one thread per column, coalesced across the warp.
 __global__ void k_col_stats(const double* __restrict__ a, int n, unsigned long long* out)
 {
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
@@ -373,36 +376,9 @@ __global__ void k_col_stats(const double* __restrict__ a, int n, unsigned long l
         s += fabs(a[(int64_t)i * n + j]);
     }
     amax_d(out + 5, s);
+    amin_d(out + 10, s);
 }
 
-// FP32 LU factors (row-major n x n): [6] [10] [11].  A warp per row.
-__global__ void k_lu_stats(const float* __restrict__ f, int n, unsigned long long* out)
-{
-    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int lane = threadIdx.x & 31;
-    if (warp >= n)
-    {
-        return;
-    }
-    const float* row = f + (int64_t)warp * n;
-    double       mx  = 0.0;
-    for (int j = warp + lane; j < n; j += 32)
-    {
-        mx = fmax(mx, (double)fabsf(row[j]));
-    }
-#pragma unroll
-    for (int off = 16; off > 0; off >>= 1)
-    {
-        mx = fmax(mx, __shfl_down_sync(0xffffffffu, mx, off));
-    }
-    if (lane == 0)
-    {
-        amax_d(out + 6, mx);
-        const double d = fabs((double)row[warp]);
-        amin_d(out + 10, d);
-        amax_d(out + 11, d);
-    }
-}
 }  // namespace
 int require_sm100();
 
@@ -415,21 +391,13 @@ int enqueue_mlp_forward(const float* params, const float* x, int batch, float* p
     return B200LA_SUCCESS;
 }
 
-// With `a`: resets the sixteen words and accumulates A's statistics; with
-// `lu32`: adds the statistics of the FP32 factors (words 6, 10, 11).
-int enqueue_matrix_stats(const double* a, int n, const float* lu32, unsigned long long* out, cudaStream_t s)
+// Resets the sixteen words and gathers A's statistics (row-major, lda = n).
+int enqueue_matrix_stats(const double* a, int n, unsigned long long* out, cudaStream_t s)
 {
     prof_begin(KC_SELECT, s);
-    if (a != nullptr)
-    {
-        k_stats_init<<<1, 32, 0, s>>>(out);
-        k_row_stats<<<(int)(((int64_t)n * 32 + 255) / 256), 256, 0, s>>>(a, n, out);
-        k_col_stats<<<(n + 255) / 256, 256, 0, s>>>(a, n, out);
-    }
-    if (lu32 != nullptr)
-    {
-        k_lu_stats<<<(int)(((int64_t)n * 32 + 255) / 256), 256, 0, s>>>(lu32, n, out);
-    }
+    k_stats_init<<<1, 32, 0, s>>>(out);
+    k_row_stats<<<(int)(((int64_t)n * 32 + 255) / 256), 256, 0, s>>>(a, n, out);
+    k_col_stats<<<(n + 255) / 256, 256, 0, s>>>(a, n, out);
     prof_end(KC_SELECT, s);
     B200LA_LAUNCH_CHECK();
     return B200LA_SUCCESS;
@@ -497,14 +465,13 @@ B200LA_API int b200la_mlp_adam(float* params, float* grads, float* m1, float* m2
     return B200LA_SUCCESS;
 }
 
-B200LA_API int b200la_matrix_stats(const double* a, int64_t n, const float* lu32, unsigned long long* out,
-    void* stream)
+B200LA_API int b200la_matrix_stats(const double* a, int64_t n, unsigned long long* out, void* stream)
 {
-    if ((!a && !lu32) || !out || n <= 0 || n > 65536)
+    if (!a || !out || n <= 0 || n > 65536)
         return set_error(B200LA_INVALID_ARGUMENT, "matrix_stats: invalid arguments");
     int rc = require_sm100();
     if (rc != B200LA_SUCCESS)
         return rc;
-    return enqueue_matrix_stats(a, (int)n, lu32, out, static_cast<cudaStream_t>(stream));
+    return enqueue_matrix_stats(a, (int)n, out, static_cast<cudaStream_t>(stream));
 }
 }

@@ -3,18 +3,18 @@
 A 12 -> 64 -> 64 -> 4 MLP maps cheap matrix features to the factorization
 precision class {FP8, BF16, FP32, FP64}.  Everything that computes runs in
 libb200la.so: the features (b200la_selector_features: O(n^2) statistics of
-A plus a Hager-Higham condition estimate and growth factor from one FP32 LU),
-the network's forward pass, its training (b200la_mlp_gradient: forward and
-backward in one kernel; b200la_mlp_adam), and the selected solve
-(b200la_dsolve_selected), which refines with the FP32 factors it already has
-when the class is FP8/BF16/FP32 and goes straight to FP64 LU otherwise;
-refinement failure escalates, so accuracy never depends on the network.
+A, no factorization), the network's forward pass, its training
+(b200la_mlp_gradient: forward and backward in one kernel; b200la_mlp_adam),
+and the selected solve (b200la_dsolve_selected), which tries the predicted
+precision first; refinement failure escalates, so accuracy never depends on
+the network.
 
-Labels come from the method itself: for each training system, the cheapest
-precision in the order FP8 < BF16 < FP32 < FP64 whose factors make
-refinement reach the tolerance within 10 iterations (a GMRES-IR correction
-counts as one), without escalation.  Attempts run from FP32 down: if FP32
-fails the label is FP64 and the lower precisions are not tried.
+Labels come from the method itself: each training system is solved at FP32,
+then BF16 and FP8 while the previous one converged, and at FP64, each attempt
+without escalation and timed; the label is the precision with the shortest
+time among those whose refinement reached the tolerance within 10 iterations
+(a GMRES-IR correction counts as one).  FP64 always converges, so every
+system has a label.
 
 Systems: A = U diag(sigma) V^T with U, V products of 8 seeded Householder
 reflectors and sigma geometric from 1 to 1/kappa (the construction of
@@ -27,7 +27,6 @@ a SHA-256 of the float32 parameter bytes (checked on load).
 CLI (GPU):
     python -m linearalgebra_b200.selector label --start 0 --count 25000 --out shard0.npz
     python -m linearalgebra_b200.selector train --dataset shard0.npz,shard1.npz --out W.json
-    python -m linearalgebra_b200.selector train --systems 50000 --out W.json  # label + train
     python -m linearalgebra_b200.selector evaluate --weights W.json --systems 5000
 """
 from __future__ import annotations
@@ -52,7 +51,7 @@ CLASS_PREC = (_lib.PREC_FP8, _lib.PREC_BF16, _lib.PREC_FP32, _lib.PREC_FP64)
 PREC_CLASS = {p: i for i, p in enumerate(CLASS_PREC)}
 N_FEATURES = 12
 N_PARAMS = 5252
-SCHEMA = "b200la-selector/1"
+SCHEMA = "b200la-selector/2"
 DEFAULT_WEIGHTS = os.path.join(os.path.dirname(os.path.abspath(__file__)), "selector_weights.json")
 LABEL_ITERATIONS = 10
 TOLERANCE = 1e-14
@@ -115,18 +114,30 @@ class _Workspace:
 
 
 _WS = _Workspace()
+_STATS = {}
 
 
-def features(a: torch.Tensor, stream=None):
-    """(12 features as float32 numpy, FP32 LU info) of the square FP64 CUDA
-    tensor a."""
+def features(a: torch.Tensor, stream=None) -> np.ndarray:
+    """The 12 features (float32 numpy) of the square FP64 CUDA tensor a."""
     n = a.shape[0]
     f = (ctypes.c_float * N_FEATURES)()
+    ws = _STATS.get(a.device)
+    if ws is None:
+        ws = _STATS[a.device] = torch.empty(16, dtype=torch.int64, device=a.device)
+    _lib.check(_lib.load().b200la_selector_features(_ptr(a), n, f, _ptr(ws), 128, _stream(stream)))
+    return np.frombuffer(f, dtype=np.float32).copy()
+
+
+def condition_estimate(a: torch.Tensor, stream=None) -> float:
+    """kappa_1 estimate of a from one FP32 LU (Hager / Higham)."""
+    n = a.shape[0]
+    k = ctypes.c_double(0)
     info = ctypes.c_int(0)
     ws = _WS.get(n)
-    _lib.check(_lib.load().b200la_selector_features(_ptr(a), n, f, ctypes.byref(info), _ptr(ws), ws.numel(),
-                                                     _stream(stream)))
-    return np.frombuffer(f, dtype=np.float32).copy(), int(info.value)
+    _lib.check(_lib.load().b200la_dcondition_estimate(_ptr(a), n, ctypes.byref(k), ctypes.byref(info), _ptr(ws),
+                                                       ws.numel(), _stream(stream)),
+               allow=(_lib.SUCCESS, _lib.SINGULAR))
+    return float(k.value)
 
 
 def attempt(a, b, precision: str, max_iterations: int = LABEL_ITERATIONS, escalate=False):
@@ -144,19 +155,17 @@ def attempt(a, b, precision: str, max_iterations: int = LABEL_ITERATIONS, escala
 
 
 def label_system(a, b):
-    """(label class, {precision: outcome}) by the method itself: FP32 first,
-    then BF16 and FP8 while the higher one converged."""
-    out = {}
-    order = ["fp32", "bf16", "fp8"]
-    label = PREC_CLASS[_lib.PREC_FP64]
-    for p in order:
+    """(label class, {precision: outcome}) by the method itself: FP64, then
+    FP32, BF16, FP8 while the previous low precision converged; the label is
+    the fastest attempt that converged within LABEL_ITERATIONS."""
+    out = {"fp64": attempt(a, b, "fp64")[1]}
+    for p in ("fp32", "bf16", "fp8"):
         _, r = attempt(a, b, p)
         out[p] = r
-        if r["converged"] and r["iterations"] <= LABEL_ITERATIONS:
-            label = CLASSES.index(p)
-        else:
+        if not (r["converged"] and r["iterations"] <= LABEL_ITERATIONS):
             break
-    return label, out
+    ok = {p: r["ms"] for p, r in out.items() if r["converged"] and r["iterations"] <= LABEL_ITERATIONS}
+    return CLASSES.index(min(ok, key=ok.get)), out
 
 
 def generate(count: int, seed: int, log_every: int = 0, **stream_kw):
@@ -166,22 +175,22 @@ def generate(count: int, seed: int, log_every: int = 0, **stream_kw):
 
 def generate_systems(systems, log_every: int = 0):
     """Label the given (n, kappa, seed) systems.  Returns a dict of numpy
-    arrays: features [count, 12], labels, n, kappa, and per attempted
-    precision (fp8, bf16, fp32) its convergence and wall time (-1 / NaN where
-    not attempted)."""
+    arrays: features [count, 12], labels, n, kappa, and per precision
+    (columns fp8, bf16, fp32, fp64) convergence within the label's
+    iterations and wall time (-1 / NaN where not attempted)."""
     count = len(systems)
     feats = np.zeros((count, N_FEATURES), np.float32)
     labels = np.zeros(count, np.int32)
-    conv = np.full((count, 3), -1, np.int8)
-    ms = np.full((count, 3), np.nan)
+    conv = np.full((count, 4), -1, np.int8)
+    ms = np.full((count, 4), np.nan)
     t_start = time.time()
     for i, (n, kappa, s) in enumerate(systems):
         a, b, _ = make_system(n, kappa, s)
-        feats[i], _ = features(a)
+        feats[i] = features(a)
         labels[i], outs = label_system(a, b)
-        for j, p in enumerate(("fp8", "bf16", "fp32")):
+        for j, p in enumerate(CLASSES):
             if p in outs:
-                conv[i, j] = outs[p]["converged"]
+                conv[i, j] = int(outs[p]["converged"] and outs[p]["iterations"] <= LABEL_ITERATIONS)
                 ms[i, j] = outs[p]["ms"]
         if log_every and (i + 1) % log_every == 0:
             print(f"[selector] labelled {i + 1}/{count} in {time.time() - t_start:.0f} s; "
@@ -426,6 +435,8 @@ def main(argv=None):
             shards = [dict(np.load(f)) for f in args.dataset.split(",")]
             d = {k: np.concatenate([sh[k] for sh in shards]) for k in ("features", "labels", "n", "kappa",
                                                                           "converged", "ms")}
+            if d["ms"].shape[1] != len(CLASSES):
+                raise ValueError("dataset shards predate the time-aware labels; label them again")
             d["label_seconds"] = np.array(sum(float(sh["label_seconds"]) for sh in shards))
         else:
             t0 = time.time()

@@ -162,13 +162,38 @@ def test_training_on_gpu_learns_a_separable_rule():
 
 
 @gpu
+def test_matrix_stats_match_numpy():
+    from linearalgebra_b200 import _lib
+    rng = np.random.default_rng(8)
+    n = 333
+    a = rng.normal(size=(n, n))
+    a[np.arange(0, n, 3), np.arange(0, n, 3)] += 3 * n  # some dominant rows
+    da = _dev(a, torch.float64)
+    out = torch.zeros(16, dtype=torch.int64, device="cuda")
+    _lib.check(_lib.load().b200la_matrix_stats(da.data_ptr(), n, out.data_ptr(), None))
+    w = out.cpu().numpy()
+    d = w.view(np.float64)
+    ab = np.abs(a)
+    rs, cs, dg = ab.sum(1), ab.sum(0), np.abs(np.diag(a))
+    off = rs - dg
+    assert np.isclose(d[0], rs.max(), rtol=1e-13) and d[1] == ab.max()
+    assert np.isclose(d[2], (a * a).sum(), rtol=1e-12)
+    assert np.isclose(d[3], (1 / (1 + dg / off)).max(), rtol=1e-12)
+    assert w[4] == int((dg / off >= 1).sum())
+    assert np.isclose(d[5], cs.max(), rtol=1e-13) and np.isclose(d[6], rs.min(), rtol=1e-13)
+    assert d[7] == dg.min() and d[8] == dg.max() and np.isclose(d[9], ab.sum(), rtol=1e-12)
+    assert np.isclose(d[10], cs.min(), rtol=1e-13) and np.isclose(d[11], dg.sum(), rtol=1e-12)
+    f = sel.features(da)
+    assert np.isfinite(f).all() and abs(f[0] - np.log2(n) / 12) < 1e-6
+    assert abs(f[6] - (dg / off >= 1).mean()) < 1e-6
+
+
+@gpu
 @pytest.mark.parametrize("kappa", [1e2, 1e6, 1e10])
-def test_features_condition_estimate(kappa):
+def test_condition_estimate(kappa):
     n = 300
     a = conditioned(n, kappa, seed=21)
-    f, info = sel.features(_dev(a, torch.float64))
-    assert info == 0 and np.isfinite(f).all()
-    est = 10 ** (4 * f[10])
+    est = sel.condition_estimate(_dev(a, torch.float64))
     exact = orc.condition_1(a)
     if kappa * 2.0 ** -24 < 1:
         # accurate FP32 factors: Hager's estimate is a lower bound of
@@ -178,7 +203,15 @@ def test_features_condition_estimate(kappa):
         # kappa u32 >> 1: the FP32 factors' inverse is far from A^-1, the
         # estimate only has to flag the ill-conditioning
         assert est >= 1e8, (est, exact)
-    assert abs(f[0] - np.log2(n) / 12) < 1e-6
+
+
+@gpu
+def test_labels_are_the_fastest_converged_attempt():
+    for (n, kappa, s) in [(300, 1e2, 3), (900, 1e11, 4)]:
+        a, b, _ = sel.make_system(n, kappa, s)
+        label, outs = sel.label_system(a, b)
+        ok = {p: r["ms"] for p, r in outs.items() if r["converged"] and r["iterations"] <= sel.LABEL_ITERATIONS}
+        assert "fp64" in ok and sel.CLASSES[label] == min(ok, key=ok.get)
 
 
 @gpu
