@@ -385,6 +385,84 @@ __device__ __forceinline__ void panel_update_rows(T* loc, size_t ldl, int rbeg, 
     }
 }
 
+
+// Copy a panel slice (nloc rows of w values at A[r0.., k..], row stride n)
+// into shared memory (row stride ldl) or back.  16-byte vectors when the
+// rows allow it, and every thread issues 8 loads before it stores any, so a
+// thread's loads overlap instead of each waiting for the previous one.
+template <typename T, bool TO_SMEM>
+__device__ __forceinline__ void panel_slice_copy(T* loc, int ldl, T* A, int n, int r0, int k, int nloc, int w)
+{
+    using VT         = typename Vec16<T>::type;
+    constexpr int V  = 16 / (int)sizeof(T);
+    constexpr int B  = 8;
+    const bool    vec = w == kNB && (n % V) == 0 && (k % V) == 0 &&
+                     (reinterpret_cast<uintptr_t>(A) & 15) == 0 && ((ldl * sizeof(T)) % 16) == 0 &&
+                     (reinterpret_cast<uintptr_t>(loc) & 15) == 0;
+    if (vec)
+    {
+        constexpr int CPR   = kNB / V;  // chunks per row
+        const int     total = nloc * CPR;
+        for (int e0 = threadIdx.x; e0 < total; e0 += kPanelThreads * B)
+        {
+            VT v[B];
+#pragma unroll
+            for (int t = 0; t < B; ++t)
+            {
+                const int e = e0 + t * kPanelThreads;
+                if (e < total)
+                {
+                    const int r = e / CPR, c = (e - (e / CPR) * CPR) * V;
+                    v[t]        = TO_SMEM ? *reinterpret_cast<const VT*>(A + (size_t)(r0 + r) * n + k + c)
+                                          : *reinterpret_cast<const VT*>(loc + (size_t)r * ldl + c);
+                }
+            }
+#pragma unroll
+            for (int t = 0; t < B; ++t)
+            {
+                const int e = e0 + t * kPanelThreads;
+                if (e < total)
+                {
+                    const int r = e / CPR, c = (e - (e / CPR) * CPR) * V;
+                    if (TO_SMEM)
+                        *reinterpret_cast<VT*>(loc + (size_t)r * ldl + c) = v[t];
+                    else
+                        *reinterpret_cast<VT*>(A + (size_t)(r0 + r) * n + k + c) = v[t];
+                }
+            }
+        }
+        return;
+    }
+    const int total = nloc * w;
+    for (int e0 = threadIdx.x; e0 < total; e0 += kPanelThreads * B)
+    {
+        T v[B];
+#pragma unroll
+        for (int t = 0; t < B; ++t)
+        {
+            const int e = e0 + t * kPanelThreads;
+            if (e < total)
+            {
+                const int r = e / w, c = e - (e / w) * w;
+                v[t]        = TO_SMEM ? A[(size_t)(r0 + r) * n + k + c] : loc[(size_t)r * ldl + c];
+            }
+        }
+#pragma unroll
+        for (int t = 0; t < B; ++t)
+        {
+            const int e = e0 + t * kPanelThreads;
+            if (e < total)
+            {
+                const int r = e / w, c = e - (e / w) * w;
+                if (TO_SMEM)
+                    loc[(size_t)r * ldl + c] = v[t];
+                else
+                    A[(size_t)(r0 + r) * n + k + c] = v[t];
+            }
+        }
+    }
+}
+
 constexpr int kMaxSlotsPerLane = (kMaxPanelCtas + 31) / 32;
 
 template <typename T>
@@ -413,11 +491,7 @@ __global__ void __launch_bounds__(kPanelThreads) k_panel(T* __restrict__ A, int 
     if (in_smem)
     {
         loc = reinterpret_cast<T*>(smem_raw);
-        for (int e = tid; e < nloc * w; e += kPanelThreads)
-        {
-            const int r = e / w, c = e - (e / w) * w;
-            loc[r * ldl + c] = A[(size_t)(r0 + r) * n + k + c];
-        }
+        panel_slice_copy<T, true>(loc, (int)ldl, A, n, r0, k, nloc, w);
     }
     else
     {
@@ -651,11 +725,7 @@ __global__ void __launch_bounds__(kPanelThreads) k_panel(T* __restrict__ A, int 
     // ---- write the factored slice back
     if (in_smem)
     {
-        for (int e = tid; e < nloc * w; e += kPanelThreads)
-        {
-            const int r = e / w, c = e - (e / w) * w;
-            A[(size_t)(r0 + r) * n + k + c] = loc[r * ldl + c];
-        }
+        panel_slice_copy<T, false>(loc, (int)ldl, A, n, r0, k, nloc, w);
     }
 
     if (b == 0)
@@ -722,11 +792,7 @@ __global__ void __launch_bounds__(kPanelThreads, 1) k_panel_cluster(T* __restric
     constexpr int ldl = panel_ldl<T>();
 
     T* loc = reinterpret_cast<T*>(smem_raw);
-    for (int e = tid; e < nloc * w; e += kPanelThreads)
-    {
-        const int r = e / w, c = e - (e / w) * w;
-        loc[r * ldl + c] = A[(size_t)(r0 + r) * n + k + c];
-    }
+    panel_slice_copy<T, true>(loc, ldl, A, n, r0, k, nloc, w);
     __syncthreads();
 
     double cand_key = -2.0;
@@ -848,11 +914,7 @@ __global__ void __launch_bounds__(kPanelThreads, 1) k_panel_cluster(T* __restric
     }
     cluster.sync();  // no CTA exits while its shared memory may still be read
 
-    for (int e = tid; e < nloc * w; e += kPanelThreads)
-    {
-        const int r = e / w, c = e - (e / w) * w;
-        A[(size_t)(r0 + r) * n + k + c] = loc[r * ldl + c];
-    }
+    panel_slice_copy<T, false>(loc, ldl, A, n, r0, k, nloc, w);
     if (b == 0)
     {
         if (tid == 0 && first_zero >= 0 && st->first_zero < 0)
@@ -925,10 +987,21 @@ __global__ void __launch_bounds__(kSwapThreads) k_laswp_trsm(T* __restrict__ A, 
     }
     if (!left)
     {
-        for (int e = tid; e < w * w; e += kSwapThreads)
+        // L11, 16 loads per thread in flight before the stores
+        constexpr int PT = kNB * kNB / kSwapThreads;
+        T             lv[PT];
+#pragma unroll
+        for (int t = 0; t < PT; ++t)
         {
-            const int i = e / w, p = e - (e / w) * w;
-            L11[i][p]   = p < i ? A[(size_t)(k + i) * n + k + p] : T(0);
+            const int e = tid + t * kSwapThreads;
+            const int i = e / kNB, p = e - (e / kNB) * kNB;
+            lv[t]       = (i < w && p < i) ? A[(size_t)(k + i) * n + k + p] : T(0);
+        }
+#pragma unroll
+        for (int t = 0; t < PT; ++t)
+        {
+            const int e = tid + t * kSwapThreads;
+            L11[e / kNB][e - (e / kNB) * kNB] = lv[t];
         }
     }
     __syncthreads();

@@ -181,13 +181,38 @@ __global__ void k_make_l21(const float* __restrict__ a32, int n, int K, int r_be
 // (strips of 64 columns), written back in FP32 and as the transposed operand
 // copy U12^T (rows = columns of A22, K-major).
 constexpr int kOuStrip = 64;
+
+// Lb = the 64 x 64 block of A32 at (r0, c0) (strictly lower part only when
+// `unit_lower`), by 256 threads with all 16 loads of a thread in flight
+// before any store.
+constexpr int kLbLd = kNB + 4;  // 16-byte aligned rows for float4 reads
+
+__device__ __forceinline__ void load_lblock(float (*Lb)[kLbLd], const float* __restrict__ a32, int n, int r0,
+    int c0, bool unit_lower)
+{
+    float v[kNB * kNB / 256];
+#pragma unroll
+    for (int t = 0; t < kNB * kNB / 256; ++t)
+    {
+        const int e = threadIdx.x + 256 * t;
+        const int i = e / kNB, p = e % kNB;
+        v[t]        = (!unit_lower || p < i) ? a32[(int64_t)(r0 + i) * n + c0 + p] : 0.f;
+    }
+#pragma unroll
+    for (int t = 0; t < kNB * kNB / 256; ++t)
+    {
+        const int e = threadIdx.x + 256 * t;
+        Lb[e / kNB][e % kNB] = v[t];
+    }
+}
+
 template <int KIND, bool SPLIT>
 __global__ void __launch_bounds__(256) k_outer_u12(float* __restrict__ a32, int n, int K,
     typename OpStore<KIND>::type* __restrict__ opT, float* __restrict__ opT_small, float* __restrict__ inv_scale)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     float(*S)[kOuStrip + 1]  = reinterpret_cast<float(*)[kOuStrip + 1]>(smem_raw);  // [256]
-    float(*Lb)[kNB + 1]      = reinterpret_cast<float(*)[kNB + 1]>(smem_raw + sizeof(float) * kOuterNB * (kOuStrip + 1));
+    float(*Lb)[kLbLd]        = reinterpret_cast<float(*)[kLbLd]>(smem_raw + sizeof(float) * kOuterNB * (kOuStrip + 1));
     const int tid = threadIdx.x;
     const int cl  = tid % kOuStrip;
     const int rg  = tid / kOuStrip;  // 4 row groups
@@ -196,18 +221,30 @@ __global__ void __launch_bounds__(256) k_outer_u12(float* __restrict__ a32, int 
     const int col = c0 + cl;
     const bool valid = col < n;
 
-    for (int i = rg; i < kOuterNB; i += 4)
+    // the strip, 16 independent loads per thread in flight
+    for (int i0 = rg; i0 < kOuterNB; i0 += 4 * 16)
     {
-        S[i][cl] = valid ? a32[(int64_t)(K + i) * n + col] : 0.f;
+        float v[16];
+#pragma unroll
+        for (int t = 0; t < 16; ++t)
+        {
+            const int i = i0 + 4 * t;
+            v[t]        = (valid && i < kOuterNB) ? a32[(int64_t)(K + i) * n + col] : 0.f;
+        }
+#pragma unroll
+        for (int t = 0; t < 16; ++t)
+        {
+            const int i = i0 + 4 * t;
+            if (i < kOuterNB)
+            {
+                S[i][cl] = v[t];
+            }
+        }
     }
     for (int jb = 0; jb < kOuterNB / kNB; ++jb)
     {
         __syncthreads();
-        for (int e = tid; e < kNB * kNB; e += 256)
-        {
-            const int i = e / kNB, p = e % kNB;
-            Lb[i][p]    = p < i ? a32[(int64_t)(K + jb * kNB + i) * n + K + jb * kNB + p] : 0.f;
-        }
+        load_lblock(Lb, a32, n, K + jb * kNB, K + jb * kNB, true);
         // unit-lower diagonal block, column-oriented substitution
         for (int p = 0; p + 1 < kNB; ++p)
         {
@@ -221,21 +258,34 @@ __global__ void __launch_bounds__(256) k_outer_u12(float* __restrict__ a32, int 
         for (int jb2 = jb + 1; jb2 < kOuterNB / kNB; ++jb2)
         {
             __syncthreads();
-            for (int e = tid; e < kNB * kNB; e += 256)
-            {
-                const int i = e / kNB, p = e % kNB;
-                Lb[i][p]    = a32[(int64_t)(K + jb2 * kNB + i) * n + K + jb * kNB + p];
-            }
+            load_lblock(Lb, a32, n, K + jb2 * kNB, K + jb * kNB, false);
             __syncthreads();
-            for (int i = rg; i < kNB; i += 4)
+            // rows rg, rg+4, ... : each S value read once, L read as float4
+            // broadcasts; per element the sum runs over p in order
+            float acc[kNB / 4];
+#pragma unroll
+            for (int t = 0; t < kNB / 4; ++t)
             {
-                float acc = 0.f;
-#pragma unroll 8
-                for (int p = 0; p < kNB; ++p)
+                acc[t] = 0.f;
+            }
+            for (int p = 0; p < kNB; p += 4)
+            {
+                const float s0 = S[jb * kNB + p][cl], s1 = S[jb * kNB + p + 1][cl];
+                const float s2 = S[jb * kNB + p + 2][cl], s3 = S[jb * kNB + p + 3][cl];
+#pragma unroll
+                for (int t = 0; t < kNB / 4; ++t)
                 {
-                    acc = fmaf(Lb[i][p], S[jb * kNB + p][cl], acc);
+                    const float4 l = *reinterpret_cast<const float4*>(&Lb[rg + 4 * t][p]);
+                    acc[t]         = fmaf(l.x, s0, acc[t]);
+                    acc[t]         = fmaf(l.y, s1, acc[t]);
+                    acc[t]         = fmaf(l.z, s2, acc[t]);
+                    acc[t]         = fmaf(l.w, s3, acc[t]);
                 }
-                S[jb2 * kNB + i][cl] -= acc;
+            }
+#pragma unroll
+            for (int t = 0; t < kNB / 4; ++t)
+            {
+                S[jb2 * kNB + rg + 4 * t][cl] -= acc[t];
             }
         }
     }
@@ -293,7 +343,7 @@ __global__ void __launch_bounds__(256) k_outer_u12(float* __restrict__ a32, int 
     }
 }
 
-constexpr size_t outer_u12_smem() { return sizeof(float) * ((size_t)kOuterNB * (kOuStrip + 1) + kNB * (kNB + 1)); }
+constexpr size_t outer_u12_smem() { return sizeof(float) * ((size_t)kOuterNB * (kOuStrip + 1) + kNB * kLbLd); }
 
 // r = b - A x (one right-hand side), FP64; b == nullptr means b = 0.  A CTA
 // handles 32 rows; x is staged through shared memory in chunks.  Also max|r|
@@ -520,6 +570,38 @@ MixedPlan plan_mixed(Arena& a, int64_t n, int64_t nrhs, int restart, bool fp64_f
     return p;
 }
 
+// rowid[i] = i: the row permutation of the factorization, tracked as it
+// happens (row i of P A is row rowid[i] of A).
+__global__ void k_iota(int32_t* __restrict__ rowid, int n)
+{
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    {
+        rowid[i] = (int32_t)i;
+    }
+}
+
+// Applies the interchange lists of an outer block's panels, in order, to
+// rowid (the same gather/scatter the interchanges do to a column).  One CTA.
+__global__ void k_rowid_apply(int32_t* __restrict__ rowid, const PermList* __restrict__ perms, int npanels)
+{
+    for (int j = 0; j < npanels; ++j)
+    {
+        const PermList* pl  = perms + j;
+        const int       cnt = pl->count;
+        int32_t         v   = 0;
+        if ((int)threadIdx.x < cnt)
+        {
+            v = rowid[pl->src[threadIdx.x]];
+        }
+        __syncthreads();
+        if ((int)threadIdx.x < cnt)
+        {
+            rowid[pl->dst[threadIdx.x]] = v;
+        }
+        __syncthreads();
+    }
+}
+
 // Inner panels of the outer block [K, Kend): 64-column panels, their row
 // interchanges on columns [0, Kend) (right of the block they are applied
 // later by enqueue_block_swaps), U12 inside the block and the SIMT updates
@@ -563,6 +645,8 @@ int enqueue_block_panels(MixedPlan& p, int n, int K, int Kend, int cl, int gmax,
 // the order they were chosen.
 int enqueue_block_swaps(MixedPlan& p, int n, int K, int Kend, cudaStream_t s)
 {
+    k_rowid_apply<<<1, 2 * kNB, 0, s>>>(p.perm, p.perms, (Kend - K + kNB - 1) / kNB);
+    B200LA_LAUNCH_CHECK();
     const int cols = n - Kend;
     if (cols <= 0)
         return B200LA_SUCCESS;
@@ -643,6 +727,7 @@ int enqueue_getrf_mixed(MixedPlan& p, int n, int kind, bool split, cudaStream_t 
     if (rc != B200LA_SUCCESS)
         return rc;
     k_status_init<<<1, 32, 0, s>>>(p.gp.st, p.gp.perm);
+    k_iota<<<grid_for(n), 256, 0, s>>>(p.perm, n);
     B200LA_LAUNCH_CHECK();
     int cl = 0, gmax = 0;
     if ((rc = panel_config<float>(cl, gmax)) != B200LA_SUCCESS)
@@ -1014,9 +1099,9 @@ int mixed_factor(const double* a, int nn, int nr, int precision, MixedPlan& p, S
     {
         k_convert_a<<<(nn * 32 + 255) / 256, 256, 0, s>>>(a, n, p.a32, nn, p.norms);
         B200LA_LAUNCH_CHECK();
+        // the factorization leaves its row permutation in p.perm
         if ((rc = enqueue_getrf_mixed(p, nn, kind, split, s)) != B200LA_SUCCESS)
             return rc;
-        k_perm_from_pivots<0><<<1, 256, perm_smem_bytes(nn), s>>>(p.piv, nn, p.perm, perm_smem_bytes(nn) > 0 ? 1 : 0, st, nullptr);
     }
     else
     {

@@ -366,65 +366,78 @@ __global__ void __launch_bounds__(128, 1) k_tc_update(const __grid_constant__ CU
     tc_fence_after();
     if (ok && !*reinterpret_cast<volatile int*>(s_fail))
     {
-        const int  r     = m0 + warp * 32 + lane;
+        const int  r      = m0 + warp * 32 + lane;
         const bool row_ok = r < M;
-        float*     crow  = C + (size_t)(row_ok ? r : 0) * ldc;
-        const bool vec   = ((ldc & 3) == 0) && ((reinterpret_cast<uintptr_t>(C) & 15) == 0);
+        float*     crow   = C + (size_t)(row_ok ? r : 0) * ldc;
+        const bool vec    = ((ldc & 3) == 0) && ((reinterpret_cast<uintptr_t>(C) & 15) == 0);
+        // C of chunk j + 1 is loaded while chunk j is finished, so each
+        // chunk's load latency overlaps the previous chunk's work
+        float4 cv[8], cn[8];
+        auto   fast_at = [&](int j) { return row_ok && vec && n0 + j * 32 + 32 <= N; };
+        auto   load_c  = [&](int j, float4(&dst)[8]) {
+            const float4* p = reinterpret_cast<const float4*>(crow + n0 + j * 32);
+#pragma unroll
+            for (int q = 0; q < 8; ++q)
+            {
+                dst[q] = p[q];
+            }
+        };
+        if (fast_at(0))
+        {
+            load_c(0, cv);
+        }
 #pragma unroll 1
         for (int j = 0; j < kTcBN / 32; ++j)
         {
             const int  c0   = n0 + j * 32;
-            const bool fast = row_ok && vec && c0 + 32 <= N;
-            float4     cv[8];
-            if (fast)
+            const bool fast = fast_at(j);
+            if (j + 1 < kTcBN / 32 && fast_at(j + 1))
             {
-                // C loads first: they do not depend on the accumulator
-                const float4* p = reinterpret_cast<const float4*>(crow + c0);
-#pragma unroll
-                for (int q = 0; q < 8; ++q)
-                {
-                    cv[q] = p[q];
-                }
+                load_c(j + 1, cn);
             }
             float v[32];
             tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(j * 32), v);
-            if (!row_ok)
+            if (row_ok)
             {
-                continue;
-            }
-            if constexpr (KIND == TC_FP8)
-            {
-                const float ra = inv_sa[r];
-#pragma unroll
-                for (int q = 0; q < 32; ++q)
+                if constexpr (KIND == TC_FP8)
                 {
-                    v[q] *= ra * (c0 + q < N ? inv_sb[c0 + q] : 0.f);
-                }
-            }
-            if (fast)
-            {
-                float4* p = reinterpret_cast<float4*>(crow + c0);
+                    const float ra = inv_sa[r];
 #pragma unroll
-                for (int q = 0; q < 8; ++q)
-                {
-                    float4 x = cv[q];
-                    x.x -= v[4 * q];
-                    x.y -= v[4 * q + 1];
-                    x.z -= v[4 * q + 2];
-                    x.w -= v[4 * q + 3];
-                    p[q] = x;
-                }
-            }
-            else
-            {
-#pragma unroll
-                for (int q = 0; q < 32; ++q)
-                {
-                    if (c0 + q < N)
+                    for (int q = 0; q < 32; ++q)
                     {
-                        crow[c0 + q] -= v[q];
+                        v[q] *= ra * (c0 + q < N ? inv_sb[c0 + q] : 0.f);
                     }
                 }
+                if (fast)
+                {
+                    float4* p = reinterpret_cast<float4*>(crow + c0);
+#pragma unroll
+                    for (int q = 0; q < 8; ++q)
+                    {
+                        float4 x = cv[q];
+                        x.x -= v[4 * q];
+                        x.y -= v[4 * q + 1];
+                        x.z -= v[4 * q + 2];
+                        x.w -= v[4 * q + 3];
+                        p[q] = x;
+                    }
+                }
+                else
+                {
+#pragma unroll
+                    for (int q = 0; q < 32; ++q)
+                    {
+                        if (c0 + q < N)
+                        {
+                            crow[c0 + q] -= v[q];
+                        }
+                    }
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < 8; ++q)
+            {
+                cv[q] = cn[q];
             }
         }
     }
