@@ -208,7 +208,8 @@ __device__ __forceinline__ void load_lblock(float (*Lb)[kLbLd], const float* __r
 
 template <int KIND, bool SPLIT>
 __global__ void __launch_bounds__(256) k_outer_u12(float* __restrict__ a32, int n, int K,
-    typename OpStore<KIND>::type* __restrict__ opT, float* __restrict__ opT_small, float* __restrict__ inv_scale)
+    typename OpStore<KIND>::type* __restrict__ opT, float* __restrict__ opT_small, float* __restrict__ inv_scale,
+    int strip0)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     float(*S)[kOuStrip + 1]  = reinterpret_cast<float(*)[kOuStrip + 1]>(smem_raw);  // [256]
@@ -217,7 +218,7 @@ __global__ void __launch_bounds__(256) k_outer_u12(float* __restrict__ a32, int 
     const int cl  = tid % kOuStrip;
     const int rg  = tid / kOuStrip;  // 4 row groups
     const int Kend = K + kOuterNB;
-    const int c0  = Kend + blockIdx.x * kOuStrip;
+    const int c0  = Kend + (strip0 + (int)blockIdx.x) * kOuStrip;
     const int col = c0 + cl;
     const bool valid = col < n;
 
@@ -512,7 +513,7 @@ struct MixedPlan
     uint64_t*          xll;     // flagged copies of solved blocks (k_trsv_blocks)
     double*            V;       // GMRES basis (m+1) x n
     double*            h;       // GMRES dot products (m+1)
-    PermList*          perms;   // interchange lists of an outer block's four panels
+    PermList*          perms;   // interchange lists of the panels of two outer blocks (by block parity)
     float*             sel;     // selector network input (12) and output (4)
     float*             l21inv;  // FP8: inverse row scales of L21
     float*             u12inv;  // FP8: inverse row scales of U12^T
@@ -548,7 +549,7 @@ MixedPlan plan_mixed(Arena& a, int64_t n, int64_t nrhs, int restart, bool fp64_f
     p.u12op    = a.next<float>((size_t)n * kOuterNB);
     p.u12small = a.next<float>((size_t)n * kOuterNB);
     p.perm     = a.next<int32_t>((size_t)n);
-    p.perms    = a.next<PermList>(kOuterNB / kNB);
+    p.perms    = a.next<PermList>(2 * (kOuterNB / kNB));
     p.sel      = a.next<float>(64);
     p.l21inv   = a.next<float>((size_t)n);
     p.u12inv   = a.next<float>((size_t)n);
@@ -602,10 +603,60 @@ __global__ void k_rowid_apply(int32_t* __restrict__ rowid, const PermList* __res
     }
 }
 
+// An outer block's row interchanges on columns [c_begin, c_end): CTA = 64
+// columns; the panels' interchange lists are applied in order, each as one
+// gather of the rows it touches and one scatter.
+constexpr int kBlockSwapThreads = 256;
+constexpr int kBlockSwapGroups  = kBlockSwapThreads / kSwapCols;
+__global__ void __launch_bounds__(kBlockSwapThreads) k_laswp_block(float* __restrict__ a32, int n,
+    const PermList* __restrict__ perms, int npanels, int c_begin, int c_end)
+{
+    __shared__ float staged[2 * kNB][kSwapCols];
+    const int  tid   = threadIdx.x;
+    const int  cl    = tid % kSwapCols;
+    const int  rg    = tid / kSwapCols;
+    const int  col   = c_begin + (int)blockIdx.x * kSwapCols + cl;
+    const bool valid = col < c_end;
+    constexpr int PT = 2 * kNB / kBlockSwapGroups;
+    for (int j = 0; j < npanels; ++j)
+    {
+        const PermList* pl  = perms + j;
+        const int       cnt = pl->count;
+        float           v[PT];
+#pragma unroll
+        for (int t = 0; t < PT; ++t)
+        {
+            const int q = rg + kBlockSwapGroups * t;
+            v[t]        = (valid && q < cnt) ? a32[(size_t)pl->src[q] * n + col] : 0.f;
+        }
+#pragma unroll
+        for (int t = 0; t < PT; ++t)
+        {
+            staged[rg + kBlockSwapGroups * t][cl] = v[t];
+        }
+        __syncthreads();
+        if (valid)
+        {
+            for (int q = rg; q < cnt; q += kBlockSwapGroups)
+            {
+                if (pl->dst[q] != pl->src[q])
+                {
+                    a32[(size_t)pl->dst[q] * n + col] = staged[q][cl];
+                }
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// The interchange lists of outer block K's panels (two sets, by the block's
+// parity, so a block's lists stay valid while the next block's panels run).
+inline PermList* block_perms(MixedPlan& p, int K) { return p.perms + ((K / kOuterNB) & 1) * (kOuterNB / kNB); }
+
 // Inner panels of the outer block [K, Kend): 64-column panels, their row
 // interchanges on columns [0, Kend) (right of the block they are applied
 // later by enqueue_block_swaps), U12 inside the block and the SIMT updates
-// inside the block.  Panel j's interchange list goes to p.perms[j].
+// inside the block.  Panel j's interchange list goes to block_perms(p, K)[j].
 int enqueue_block_panels(MixedPlan& p, int n, int K, int Kend, int cl, int gmax, cudaStream_t s)
 {
     float* a32 = p.a32;
@@ -614,16 +665,19 @@ int enqueue_block_panels(MixedPlan& p, int n, int K, int Kend, int cl, int gmax,
     {
         const int        w  = n - k < kNB ? n - k : kNB;
         GetrfPlan<float> gp = p.gp;
-        gp.perm             = p.perms + j;
+        gp.perm             = block_perms(p, K) + j;
         if ((rc = launch_panel<float>(a32, n, k, w, p.piv, gp, cl, gmax, s)) != B200LA_SUCCESS)
             return rc;
-        const int nl = (k + kSwapCols - 1) / kSwapCols;
+        // interchanges inside the block here; left of the block they are
+        // applied later (enqueue_block_left_swaps), right of it after the
+        // block (enqueue_block_swaps)
+        const int nl = (k - K + kSwapCols - 1) / kSwapCols;
         const int nr = (Kend - (k + w) + kSwapCols - 1) / kSwapCols;
         if (nl + nr > 0)
         {
             prof_begin(KC_SWAP, s);
             k_laswp_trsm<float><<<nl + nr, kSwapThreads, laswp_smem_bytes<float>(), s>>>(a32, n, k, w, gp.perm, nl,
-                Kend, 0, k, Kend);
+                Kend, K, k, Kend);
             prof_end(KC_SWAP, s);
             B200LA_LAUNCH_CHECK();
         }
@@ -641,33 +695,42 @@ int enqueue_block_panels(MixedPlan& p, int n, int K, int Kend, int cl, int gmax,
     return B200LA_SUCCESS;
 }
 
-// The outer block's row interchanges on columns [Kend, n), panel by panel in
-// the order they were chosen.
-int enqueue_block_swaps(MixedPlan& p, int n, int K, int Kend, cudaStream_t s)
+// The outer block's row interchanges on columns [c_begin, c_end) (right of
+// the block), all its panels in one launch.
+int enqueue_block_swaps(MixedPlan& p, int n, int K, int Kend, int c_begin, int c_end, cudaStream_t s)
 {
-    k_rowid_apply<<<1, 2 * kNB, 0, s>>>(p.perm, p.perms, (Kend - K + kNB - 1) / kNB);
-    B200LA_LAUNCH_CHECK();
-    const int cols = n - Kend;
+    const int cols = c_end - c_begin;
     if (cols <= 0)
         return B200LA_SUCCESS;
-    const int nl = (cols + kSwapCols - 1) / kSwapCols;
-    for (int k = K, j = 0; k < Kend; k += kNB, ++j)
-    {
-        const int w = n - k < kNB ? n - k : kNB;
-        prof_begin(KC_SWAP, s);
-        k_laswp_trsm<float><<<nl, kSwapThreads, laswp_smem_bytes<float>(), s>>>(p.a32, n, k, w, p.perms + j, nl, n,
-            Kend, n, n);
-        prof_end(KC_SWAP, s);
-        B200LA_LAUNCH_CHECK();
-    }
+    prof_begin(KC_SWAP, s);
+    k_laswp_block<<<(cols + kSwapCols - 1) / kSwapCols, kBlockSwapThreads, 0, s>>>(p.a32, n, block_perms(p, K),
+        (Kend - K + kNB - 1) / kNB, c_begin, c_end);
+    prof_end(KC_SWAP, s);
+    B200LA_LAUNCH_CHECK();
     return B200LA_SUCCESS;
 }
 
-// A high-priority stream per device for the look-ahead panels.
-cudaStream_t lookahead_stream(int* rc)
+// The outer block's interchanges on the columns left of it, [0, K).
+int enqueue_block_left_swaps(MixedPlan& p, int n, int K, int Kend, cudaStream_t s)
+{
+    return enqueue_block_swaps(p, n, K, Kend, 0, K, s);
+}
+
+// The outer block's interchanges applied to the row permutation.
+int enqueue_block_rowid(MixedPlan& p, int K, int Kend, cudaStream_t s)
+{
+    k_rowid_apply<<<1, 2 * kNB, 0, s>>>(p.perm, block_perms(p, K), (Kend - K + kNB - 1) / kNB);
+    B200LA_LAUNCH_CHECK();
+    return B200LA_SUCCESS;
+}
+
+// A stream per device (high priority for the look-ahead panels, low for the
+// interchanges left of a block, which nothing reads before the solve).
+cudaStream_t lookahead_stream(int* rc, bool high = true)
 {
     static std::mutex   m;
-    static cudaStream_t streams[64] = {};
+    static cudaStream_t all_streams[2][64] = {};
+    cudaStream_t*       streams            = all_streams[high ? 0 : 1];
     int                 dev         = 0;
     *rc                             = B200LA_SUCCESS;
     cudaError_t e                   = cudaGetDevice(&dev);
@@ -686,7 +749,7 @@ cudaStream_t lookahead_stream(int* rc)
     {
         int least = 0, greatest = 0;
         cudaDeviceGetStreamPriorityRange(&least, &greatest);
-        e = cudaStreamCreateWithPriority(&streams[dev], cudaStreamNonBlocking, greatest);
+        e = cudaStreamCreateWithPriority(&streams[dev], cudaStreamNonBlocking, high ? greatest : least);
         if (e != cudaSuccess)
         {
             streams[dev] = nullptr;
@@ -703,6 +766,50 @@ bool lookahead_enabled()
     return !(e != nullptr && e[0] == '0');
 }
 
+// The outer block's operand copies for strips [strip0, strip0 + count) of
+// U12 (64 columns each) and, with `l21`, the L21 copy (all rows).
+void enqueue_block_operands(MixedPlan& p, int n, int K, int Kend, int rest, int kind, bool split, int strip0,
+    int count, bool l21, cudaStream_t s)
+{
+    float*        a32   = p.a32;
+    const int64_t elems = (int64_t)rest * kOuterNB;
+    if (kind == TC_TF32 && split)
+    {
+        if (l21)
+            k_make_l21<TC_TF32, true><<<grid_for(elems), 256, 0, s>>>(a32, n, K, Kend, (float*)p.l21op, p.l21small);
+        if (count > 0)
+            k_outer_u12<TC_TF32, true><<<count, 256, outer_u12_smem(), s>>>(a32, n, K, (float*)p.u12op, p.u12small, nullptr, strip0);
+    }
+    else if (kind == TC_TF32)
+    {
+        if (l21)
+            k_make_l21<TC_TF32, false><<<grid_for(elems), 256, 0, s>>>(a32, n, K, Kend, (float*)p.l21op, nullptr);
+        if (count > 0)
+            k_outer_u12<TC_TF32, false><<<count, 256, outer_u12_smem(), s>>>(a32, n, K, (float*)p.u12op, nullptr, nullptr, strip0);
+    }
+    else if (kind == TC_BF16)
+    {
+        if (l21)
+            k_make_l21<TC_BF16, false><<<grid_for(elems), 256, 0, s>>>(a32, n, K, Kend, (__nv_bfloat16*)p.l21op, nullptr);
+        if (count > 0)
+            k_outer_u12<TC_BF16, false><<<count, 256, outer_u12_smem(), s>>>(a32, n, K, (__nv_bfloat16*)p.u12op, nullptr, nullptr, strip0);
+    }
+    else if (kind == TC_FP16)
+    {
+        if (l21)
+            k_make_l21<TC_FP16, false><<<grid_for(elems), 256, 0, s>>>(a32, n, K, Kend, (__half*)p.l21op, nullptr);
+        if (count > 0)
+            k_outer_u12<TC_FP16, false><<<count, 256, outer_u12_smem(), s>>>(a32, n, K, (__half*)p.u12op, nullptr, nullptr, strip0);
+    }
+    else
+    {
+        if (l21)
+            k_make_l21_fp8<<<grid_for((int64_t)rest * 32), 256, 0, s>>>(a32, n, K, Kend, (__nv_fp8_storage_t*)p.l21op, p.l21inv);
+        if (count > 0)
+            k_outer_u12<TC_FP8, false><<<count, 256, outer_u12_smem(), s>>>(a32, n, K, (__nv_fp8_storage_t*)p.u12op, nullptr, p.u12inv, strip0);
+    }
+}
+
 // The tensor-core trailing update of the outer block (columns [c0, n) of
 // A22 = rows and columns from Kend), operands from the block's copies.
 int enqueue_block_update(MixedPlan& p, int n, int Kend, int c0, int kind, bool split, const CUtensorMap& ma,
@@ -715,12 +822,14 @@ int enqueue_block_update(MixedPlan& p, int n, int Kend, int c0, int kind, bool s
 
 // Mixed-precision factorization of p.a32 in place; pivots in p.piv.
 //
-// Look-ahead: after outer block K's operand copies, the tensor-core update
-// first covers the next block's 256 columns only; the next block's panels
-// then run on a high-priority stream while the rest of the update runs on
-// `s`.  The next block's interchanges right of it wait until that update is
-// done (enqueue_block_swaps), so both streams touch disjoint columns; every
-// per-element operation is the same as without look-ahead.
+// Look-ahead: outer block K first gets only what the next block's panels
+// need (its interchanges, U12 strips and operand copies for the next block's
+// 256 columns, and those columns' tensor-core update); the next block's
+// panels then run on a high-priority stream while the rest of block K's
+// interchanges, U12 strips and update run on `s`.  The next block's
+// interchanges right of it wait until that update is done, so both streams
+// touch disjoint columns; every per-element operation is the same as
+// without look-ahead.
 int enqueue_getrf_mixed(MixedPlan& p, int n, int kind, bool split, cudaStream_t s)
 {
     int rc = clear_panel_exchange<float>(p.gp, s);
@@ -756,27 +865,47 @@ int enqueue_getrf_mixed(MixedPlan& p, int n, int kind, bool split, cudaStream_t 
                           kTcBN)) != B200LA_SUCCESS)
             return rc;
     }
-    cudaStream_t side = s;
-    cudaEvent_t  ev_update = nullptr, ev_panels = nullptr;
+    cudaStream_t side = s, left = s;
+    cudaEvent_t  ev_update = nullptr, ev_panels = nullptr, ev_left[2] = {nullptr, nullptr};
     if (la)
     {
         side = lookahead_stream(&rc);
         if (rc != B200LA_SUCCESS)
             return rc;
+        left = lookahead_stream(&rc, false);
+        if (rc != B200LA_SUCCESS)
+            return rc;
         B200LA_CUDA(cudaEventCreateWithFlags(&ev_update, cudaEventDisableTiming));
         B200LA_CUDA(cudaEventCreateWithFlags(&ev_panels, cudaEventDisableTiming));
+        B200LA_CUDA(cudaEventCreateWithFlags(&ev_left[0], cudaEventDisableTiming));
+        B200LA_CUDA(cudaEventCreateWithFlags(&ev_left[1], cudaEventDisableTiming));
     }
     struct EventGuard
     {
-        cudaEvent_t a, b;
+        cudaEvent_t e[4];
         ~EventGuard()
         {
-            if (a)
-                cudaEventDestroy(a);
-            if (b)
-                cudaEventDestroy(b);
+            for (cudaEvent_t x : e)
+                if (x)
+                    cudaEventDestroy(x);
         }
-    } guard{ev_update, ev_panels};
+    } guard{{ev_update, ev_panels, ev_left[0], ev_left[1]}};
+    // interchanges left of block K once its panels are done (`done_on`:
+    // where they ran); the event guards the interchange lists' slot
+    auto left_swaps = [&](int K, int Kend, cudaStream_t done_on) -> int {
+        if (K <= 0)
+            return B200LA_SUCCESS;
+        if (la)
+        {
+            B200LA_CUDA(cudaStreamWaitEvent(left, done_on == s ? ev_update : ev_panels, 0));
+        }
+        int r = enqueue_block_left_swaps(p, n, K, Kend, left);
+        if (r == B200LA_SUCCESS && la)
+        {
+            B200LA_CUDA(cudaEventRecord(ev_left[(K / kOuterNB) & 1], left));
+        }
+        return r;
+    };
 
     float* a32 = p.a32;
     if ((rc = enqueue_block_panels(p, n, 0, n < kOuterNB ? n : kOuterNB, cl, gmax, s)) != B200LA_SUCCESS)
@@ -790,55 +919,52 @@ int enqueue_getrf_mixed(MixedPlan& p, int n, int kind, bool split, cudaStream_t 
             B200LA_CUDA(cudaStreamWaitEvent(s, ev_panels, 0));
             panels_on_side = false;
         }
-        if ((rc = enqueue_block_swaps(p, n, K, Kend, s)) != B200LA_SUCCESS)
+        if ((rc = enqueue_block_rowid(p, K, Kend, s)) != B200LA_SUCCESS)
             return rc;
         const int rest = n - Kend;
         if (rest <= 0)
         {
             continue;
         }
-        const int64_t elems = (int64_t)rest * kOuterNB;
+        const int  Kend2 = Kend + kOuterNB < n ? Kend + kOuterNB : n;
+        const bool ahead = la && Kend2 < n;
+        // with look-ahead, first only what the next block's panels need: its
+        // columns' interchanges and U12 strips, then its columns' update
+        const int  c_first = ahead ? Kend2 : n;
+        if ((rc = enqueue_block_swaps(p, n, K, Kend, Kend, c_first, s)) != B200LA_SUCCESS)
+            return rc;
+        const int nstrips = (rest + kOuStrip - 1) / kOuStrip;
+        const int first   = ahead ? (Kend2 - Kend) / kOuStrip : nstrips;
         prof_begin(KC_PREP, s);
-        if (kind == TC_TF32 && split)
-        {
-            k_make_l21<TC_TF32, true><<<grid_for(elems), 256, 0, s>>>(a32, n, K, Kend, (float*)p.l21op, p.l21small);
-            k_outer_u12<TC_TF32, true><<<(rest + kOuStrip - 1) / kOuStrip, 256, outer_u12_smem(), s>>>(a32, n, K, (float*)p.u12op, p.u12small, nullptr);
-        }
-        else if (kind == TC_TF32)
-        {
-            k_make_l21<TC_TF32, false><<<grid_for(elems), 256, 0, s>>>(a32, n, K, Kend, (float*)p.l21op, nullptr);
-            k_outer_u12<TC_TF32, false><<<(rest + kOuStrip - 1) / kOuStrip, 256, outer_u12_smem(), s>>>(a32, n, K, (float*)p.u12op, nullptr, nullptr);
-        }
-        else if (kind == TC_BF16)
-        {
-            k_make_l21<TC_BF16, false><<<grid_for(elems), 256, 0, s>>>(a32, n, K, Kend, (__nv_bfloat16*)p.l21op, nullptr);
-            k_outer_u12<TC_BF16, false><<<(rest + kOuStrip - 1) / kOuStrip, 256, outer_u12_smem(), s>>>(a32, n, K, (__nv_bfloat16*)p.u12op, nullptr, nullptr);
-        }
-        else if (kind == TC_FP16)
-        {
-            k_make_l21<TC_FP16, false><<<grid_for(elems), 256, 0, s>>>(a32, n, K, Kend, (__half*)p.l21op, nullptr);
-            k_outer_u12<TC_FP16, false><<<(rest + kOuStrip - 1) / kOuStrip, 256, outer_u12_smem(), s>>>(a32, n, K, (__half*)p.u12op, nullptr, nullptr);
-        }
-        else
-        {
-            k_make_l21_fp8<<<grid_for((int64_t)rest * 32), 256, 0, s>>>(a32, n, K, Kend, (__nv_fp8_storage_t*)p.l21op, p.l21inv);
-            k_outer_u12<TC_FP8, false><<<(rest + kOuStrip - 1) / kOuStrip, 256, outer_u12_smem(), s>>>(a32, n, K, (__nv_fp8_storage_t*)p.u12op, nullptr, p.u12inv);
-        }
+        enqueue_block_operands(p, n, K, Kend, rest, kind, split, 0, first, true, s);
         prof_end(KC_PREP, s);
         B200LA_LAUNCH_CHECK();
-        const int Kend2 = Kend + kOuterNB < n ? Kend + kOuterNB : n;
-        if (la && Kend2 < n)
+        if (ahead)
         {
-            // the next block's columns, then its panels beside the rest of the update
             if ((rc = enqueue_block_update(p, n, Kend, Kend, kind, split, ma, mb, mas, mbs, Kend2 - Kend, s)) !=
                 B200LA_SUCCESS)
                 return rc;
             B200LA_CUDA(cudaEventRecord(ev_update, s));
             B200LA_CUDA(cudaStreamWaitEvent(side, ev_update, 0));
+            // the lists' slot of block K+1 was last used by block K-1's
+            // left-of-block interchanges
+            if (K > 0)
+            {
+                B200LA_CUDA(cudaStreamWaitEvent(side, ev_left[((K / kOuterNB) + 1) & 1], 0));
+            }
             if ((rc = enqueue_block_panels(p, n, Kend, Kend2, cl, gmax, side)) != B200LA_SUCCESS)
                 return rc;
             B200LA_CUDA(cudaEventRecord(ev_panels, side));
             panels_on_side = true;
+            if ((rc = left_swaps(Kend, Kend2, side)) != B200LA_SUCCESS)
+                return rc;
+            // the rest, beside the next block's panels
+            if ((rc = enqueue_block_swaps(p, n, K, Kend, Kend2, n, s)) != B200LA_SUCCESS)
+                return rc;
+            prof_begin(KC_PREP, s);
+            enqueue_block_operands(p, n, K, Kend, rest, kind, split, first, nstrips - first, false, s);
+            prof_end(KC_PREP, s);
+            B200LA_LAUNCH_CHECK();
             if ((rc = enqueue_block_update(p, n, Kend, Kend2, kind, split, ma, mb2, mas, mbs2, n - Kend2, s)) !=
                 B200LA_SUCCESS)
                 return rc;
@@ -847,9 +973,25 @@ int enqueue_getrf_mixed(MixedPlan& p, int n, int kind, bool split, cudaStream_t 
         {
             if ((rc = enqueue_block_update(p, n, Kend, Kend, kind, split, ma, mb, mas, mbs, rest, s)) != B200LA_SUCCESS)
                 return rc;
+            if (la && K > 0)
+            {
+                B200LA_CUDA(cudaStreamWaitEvent(s, ev_left[((K / kOuterNB) + 1) & 1], 0));
+            }
             if ((rc = enqueue_block_panels(p, n, Kend, Kend2, cl, gmax, s)) != B200LA_SUCCESS)
                 return rc;
+            if (la)
+            {
+                B200LA_CUDA(cudaEventRecord(ev_update, s));
+            }
+            if ((rc = left_swaps(Kend, Kend2, s)) != B200LA_SUCCESS)
+                return rc;
         }
+    }
+    if (la)
+    {
+        // the solve needs every interchange applied
+        B200LA_CUDA(cudaEventRecord(ev_left[0], left));
+        B200LA_CUDA(cudaStreamWaitEvent(s, ev_left[0], 0));
     }
     k_status_finish<<<1, 32, 0, s>>>(p.gp.st);
     B200LA_LAUNCH_CHECK();
