@@ -266,6 +266,13 @@ def cusolver_reference_seconds(A, b, stream, steps: int = 2):
 # ---------------------------------------------------------------------------
 # B200 arm
 # ---------------------------------------------------------------------------
+# DRAM bytes (ncu dram__bytes_read.sum + dram__bytes_write.sum) per algorithmic
+# byte of the dominant kernels, from one capture each on a smaller case
+# (profiles/): the tensor-core update at n=8192 (M=6400, N=6144 launch) and
+# the FP64 trailing update at n=4096.  Traffic grows with the C tile bytes,
+# so it scales to a full launch by the algorithmic bytes.
+TRAFFIC_PER_ALGORITHMIC_BYTE = {5: 0.915, 2: 0.95}
+
 CLASS_NAMES = {0: "panel", 1: "laswp_u12", 2: "trailing_simt", 3: "solve", 4: "gemm", 5: "tc_update",
                6: "residual", 7: "batched", 8: "operand_prep", 9: "selector"}
 
@@ -475,7 +482,11 @@ def run_b200(args, world, rank, local):
         peak_src = peaks["source"]
     roofline = {
         "kernel": CLASS_NAMES[roof_cls], "bound": w["bound"], "achieved": achieved, "peak": peak,
-        "unit": unit, "frac": achieved / peak if achieved else None, "traffic": None,
+        "unit": unit, "frac": achieved / peak if achieved else None,
+        "traffic": (w["bytes"] * args.steps / max(1, k_n.value) * TRAFFIC_PER_ALGORITHMIC_BYTE[roof_cls]
+                    if roof_cls in TRAFFIC_PER_ALGORITHMIC_BYTE else None),
+        "traffic_note": "bytes per launch: the ncu DRAM/algorithmic ratio of a smaller capture (profiles/) "
+                        "times this run's algorithmic bytes per launch",
         "peak_source": peak_src, "launches": int(k_n.value),
         "avg_launch_ms": k_ms.value / max(1, k_n.value),
         "share_of_step": (k_ms.value / args.steps) / ms_per_step if ms_per_step else None,
