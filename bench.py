@@ -268,10 +268,11 @@ def cusolver_reference_seconds(A, b, stream, steps: int = 2):
 # ---------------------------------------------------------------------------
 # DRAM bytes (ncu dram__bytes_read.sum + dram__bytes_write.sum) per algorithmic
 # byte of the dominant kernels, from one capture each on a smaller case
-# (profiles/): the tensor-core update at n=8192 (M=6400, N=6144 launch) and
-# the FP64 trailing update at n=4096.  Traffic grows with the C tile bytes,
-# so it scales to a full launch by the algorithmic bytes.
-TRAFFIC_PER_ALGORITHMIC_BYTE = {5: 0.915, 2: 0.95}
+# (profiles/): the tensor-core update at n=8192 (M=6400, N=6144 launch:
+# 287.2 of 314.6 MB) and the FP64 trailing update at n=8192 (rest=7488:
+# 846.6 of 897.1 MB).  Traffic grows with the C tile bytes, so it scales to
+# a full launch by the algorithmic bytes.
+TRAFFIC_PER_ALGORITHMIC_BYTE = {5: 0.913, 2: 0.944}
 
 CLASS_NAMES = {0: "panel", 1: "laswp_u12", 2: "trailing_simt", 3: "solve", 4: "gemm", 5: "tc_update",
                6: "residual", 7: "batched", 8: "operand_prep", 9: "selector"}
