@@ -7,7 +7,7 @@
  * transpose,cholesky_decomposition}_cublas.cpp) by baseline/Makefile into
  * baseline/_ref/libref_cublas.so.
  *
- * BASELINE INFRASTRUCTURE ONLY.  Nothing in the B200 library links or calls
+ * Timing-comparison code only.  Nothing in the B200 library links or calls
  * this; it runs NVIDIA's cuSOLVER and cuBLAS exactly as the reference does.
  *
  * All pointers are device pointers (the reference's GPU contract); the

@@ -37,7 +37,7 @@
 /* Normwise backward error of x for A x = b (infinity norms):
  *   eta = ||b - A x|| / (||A|| ||x|| + ||b||),
  * with the residual accumulated in long double.  Used by the tests as the
- * accuracy metric the path is judged by. */
+ * accuracy metric the path is held to. */
 double or_backward_error(const double* a, int64_t n, int64_t lda, const double* x,
     const double* b)
 {
