@@ -1,4 +1,4 @@
-"""CPU checkers for the LU-solve path.
+"""CPU oracles for the LU-solve path.
 
 TEST INFRASTRUCTURE ONLY.  Only tests/, ``__graft_entry__.smoke()`` and the
 CPU-baseline leg of ``bench.py`` import this package, and only as the thing

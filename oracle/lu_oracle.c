@@ -3,7 +3,7 @@
  * NATIVE algorithm (see lu_oracle_impl.h for the per-function citations).
  *
  * TEST INFRASTRUCTURE ONLY.  Imported by tests/, by __graft_entry__.smoke()
- * and by bench.py's CPU-baseline leg as the checker; the B200 library never
+ * and by bench.py's CPU-baseline leg as the oracle; the B200 library never
  * links or calls it.  Parity is pinned two ways: bit-for-bit against the
  * reference's own sources compiled into oracle/_ref (oracle/Makefile), and
  * against the committed fixtures in tests/golden/ that were produced by that

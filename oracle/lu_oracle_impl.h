@@ -4,7 +4,7 @@
  *
  * TEST INFRASTRUCTURE ONLY: a plain-C restatement of the reference's NATIVE
  * LU-solve path, used by tests/ and by bench.py's CPU-baseline leg as the
- * checker.  The B200 library never links, loads or calls it.
+ * oracle.  The B200 library never links, loads or calls it.
  *
  * Rounding is pinned to the reference build's: the reference's scalar loops
  * `y -= a * x` and `s += a * b` are contracted by g++ into single fused
