@@ -1,10 +1,11 @@
 /*
- * extern "C" wrapper over the reference's own CUDA_BLAS (cuSOLVER) LU solve,
- * linear_solver<double, linalg_backend::CUDA_BLAS> in LU mode, so bench.py
- * can time the reference's GPU backend beside this library.  Compiled
- * together with the reference's sources
- * (src/matrix_operation/gpu/cublas/{linear_solver,lu_decomposition,
- * transpose,cholesky_decomposition}_cublas.cpp) by baseline/Makefile into
+ * extern "C" wrappers over the reference's own CUDA_BLAS (cuSOLVER) LU solve,
+ * linear_solver<double, linalg_backend::CUDA_BLAS> in LU mode, and its
+ * CUDA_BLAS inversion and determinant in LU mode, so bench.py can time the
+ * reference's GPU backend beside this library.  Compiled together with the
+ * reference's sources (src/matrix_operation/gpu/cublas/{linear_solver,
+ * lu_decomposition,transpose,cholesky_decomposition}_cublas.cpp and
+ * inversion_cublas.cu) by baseline/Makefile into
  * baseline/_ref/libref_cublas.so.
  *
  * Timing-comparison code only.  Nothing in the B200 library links or calls
@@ -19,6 +20,8 @@
 #include <exception>
 #include <string>
 
+#include "include/matrix_operation/determinant.h"
+#include "include/matrix_operation/inversion.h"
 #include "include/matrix_operation/linear_solver.h"
 
 using linalg::linalg_backend;
@@ -53,6 +56,64 @@ int ref_cublas_dgesv(double* m, int64_t* pivot, int64_t n, double* x, void* ws, 
     {
         linalg::linear_solver<double, linalg_backend::CUDA_BLAS>::apply(m, reinterpret_cast<linalg_int*>(pivot), n,
             x, linear_solver_type::LU_LINEAR_SOLVER, ws, ws_bytes, stream);
+        return 0;
+    }
+    catch (const std::exception& e)
+    {
+        g_err = e.what();
+        return -1;
+    }
+}
+
+size_t ref_cublas_dinverse_workspace_size(int64_t n)
+{
+    try
+    {
+        return linalg::inversion<double, linalg_backend::CUDA_BLAS>::workspace_size(
+            n, linear_solver_type::LU_LINEAR_SOLVER);
+    }
+    catch (const std::exception& e)
+    {
+        g_err = e.what();
+        return 0;
+    }
+}
+
+int ref_cublas_dinverse(double* m, int64_t n, void* ws, size_t ws_bytes, void* stream)
+{
+    try
+    {
+        linalg::inversion<double, linalg_backend::CUDA_BLAS>::apply(
+            m, nullptr, n, linear_solver_type::LU_LINEAR_SOLVER, ws, ws_bytes, stream);
+        return 0;
+    }
+    catch (const std::exception& e)
+    {
+        g_err = e.what();
+        return -1;
+    }
+}
+
+size_t ref_cublas_ddeterminant_workspace_size(int64_t n)
+{
+    try
+    {
+        return linalg::determinant<double, linalg_backend::CUDA_BLAS>::workspace_size(
+            n, linear_solver_type::LU_LINEAR_SOLVER);
+    }
+    catch (const std::exception& e)
+    {
+        g_err = e.what();
+        return 0;
+    }
+}
+
+int ref_cublas_ddeterminant(double* m, int64_t n, double* out, void* ws, size_t ws_bytes, void* stream)
+{
+    try
+    {
+        *out = linalg::determinant<double, linalg_backend::CUDA_BLAS>::apply(
+            m, nullptr, n, linear_solver_type::LU_LINEAR_SOLVER, ws, ws_bytes, stream);
         return 0;
     }
     catch (const std::exception& e)

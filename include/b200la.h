@@ -61,7 +61,9 @@ B200LA_API int64_t b200la_launch_count(void);
  * 2 trailing update, 3 triangular solves, 4 general GEMM, 5 mixed-precision
  * factorization GEMM, 6 FP64 residual, 7 batched solver, 8 mixed-precision
  * operand preparation and outer U12 solve, 9 precision selector: network
- * and matrix statistics) is bracketed by a
+ * and matrix statistics, 10 inversion GEMM updates, 11 inversion and
+ * determinant helpers: identity, column gather, diagonal product) is
+ * bracketed by a
  * pair of CUDA events on its stream.  b200la_profile_stop synchronizes those
  * events and returns the summed device time (ms) and launch count of one
  * class; it also stops recording. */
@@ -151,6 +153,47 @@ B200LA_API int    b200la_dtrsm(int upper, int transpose, int unit, int64_t n, in
 B200LA_API int    b200la_strsm(int upper, int transpose, int unit, int64_t n, int64_t nrhs,
        const float* a, int64_t lda, const float* b, int64_t ldb, float* x, int64_t ldx,
        void* workspace, size_t workspace_bytes, void* stream);
+
+/* ---- inversion (LU modes) ---------------------------------------------------
+ * Replaces inversion<T, Backend>::apply / ::workspace_size
+ * (include/matrix_operation/inversion.h:15-53; NATIVE semantics of
+ * src/matrix_operation/cpu/native/inversion_native.cpp:412-440).  m: n x n
+ * row-major (lda == n), overwritten with the inverse.  Mode
+ * B200LA_LU_LINEAR_SOLVER factors m first (pivots written to `pivot`, or kept
+ * in the workspace when pivot is NULL, as the CUDA_BLAS backend allows) and
+ * leaves the factors in m when the factorization met an exact zero pivot;
+ * B200LA_LU_UPFRONT_LINEAR_SOLVER inverts the factors and pivots given in m
+ * and pivot.  The Cholesky modes are not provided (B200LA_NOT_SUPPORTED).
+ * Asynchronous on `stream`; the factorization's status lands in the
+ * workspace (b200la_workspace_status).  Workspace: one n x n scratch plus
+ * O(n); the inverse agrees with the reference's to rounding, not bit for
+ * bit (its entries come from GEMM-blocked substitutions). */
+B200LA_API size_t b200la_dinverse_workspace_size(int64_t n, int mode);
+B200LA_API size_t b200la_sinverse_workspace_size(int64_t n, int mode);
+B200LA_API int    b200la_dinverse(double* m, int64_t* pivot, int64_t n, int mode, void* workspace,
+       size_t workspace_bytes, void* stream);
+B200LA_API int    b200la_sinverse(float* m, int64_t* pivot, int64_t n, int mode, void* workspace,
+       size_t workspace_bytes, void* stream);
+
+/* ---- determinant (LU modes) -------------------------------------------------
+ * Replaces determinant<T, Backend>::apply / ::workspace_size
+ * (include/matrix_operation/determinant.h; src/matrix_operation/cpu/
+ * determinant.cpp:18-27,56-80).  Mode B200LA_LU_LINEAR_SOLVER factors m in
+ * place (pivot as for inversion, NULL allowed); LU_UPFRONT reads the given
+ * factors and pivots.  Outputs (host): *product = the product of U's
+ * diagonal in index order, one multiply at a time in the input type (the
+ * reference's NATIVE value, bit for bit; 0 when LU mode met an exact zero
+ * pivot, then the return is B200LA_SINGULAR); *sign = (-1)^(number of i with
+ * pivot[i] != i+1), may be NULL, so that det(A) = sign * product (the
+ * reference's NATIVE reduction omits this sign, its CUDA_BLAS one applies
+ * it); *log_abs = sum of log|u_ii|, may be NULL, finite where the product
+ * over- or underflows.  Synchronous (the reference returns the value). */
+B200LA_API size_t b200la_ddeterminant_workspace_size(int64_t n, int mode);
+B200LA_API size_t b200la_sdeterminant_workspace_size(int64_t n, int mode);
+B200LA_API int    b200la_ddeterminant(double* m, int64_t* pivot, int64_t n, int mode, double* product,
+       int* sign, double* log_abs, void* workspace, size_t workspace_bytes, void* stream);
+B200LA_API int    b200la_sdeterminant(float* m, int64_t* pivot, int64_t n, int mode, float* product,
+       int* sign, double* log_abs, void* workspace, size_t workspace_bytes, void* stream);
 
 /* ---- multiplication --------------------------------------------------------
  * Replaces multiplication<T, Backend>::apply (16-argument form) /

@@ -11,8 +11,16 @@
  *  - lu_decomposition synchronizes `stream` and writes the host `info`;
  *  - linear_solver honours the caller's pivots in LU_UPFRONT mode and, in
  *    LU mode, leaves x unchanged when U is exactly singular;
- *  - the Cholesky modes of linear_solver are not provided by this backend
- *    (std::invalid_argument).
+ *  - the Cholesky modes of linear_solver, inversion and determinant are not
+ *    provided by this backend (std::invalid_argument);
+ *  - inversion and determinant honour LU_UPFRONT (m and pivot are the
+ *    caller's factors) and, in LU mode, accept a null pivot (CUDA_BLAS's
+ *    contract) by keeping the pivots in the workspace; inversion is
+ *    asynchronous like CUDA_BLAS's, determinant synchronizes and returns;
+ *  - determinant returns det(A) with the pivot sign applied, as CUDA_BLAS
+ *    does; the NATIVE reduction omits that sign (include/matrix_operation/
+ *    determinant.h), its magnitude is the same bits (b200la_ddeterminant
+ *    returns both parts).
  */
 #pragma once
 
@@ -57,4 +65,22 @@ template <> size_t multiplication<double, linalg_backend::B200>::workspace_size(
     linalg_int, linalg_int);
 template <> size_t multiplication<float, linalg_backend::B200>::workspace_size(linalg_int,
     linalg_int, linalg_int);
+
+template <> void inversion<double, linalg_backend::B200>::apply(double*, linalg_int*, linalg_int,
+    linear_solver_type, void*, size_t, void*);
+template <> void inversion<float, linalg_backend::B200>::apply(float*, linalg_int*, linalg_int,
+    linear_solver_type, void*, size_t, void*);
+template <> size_t inversion<double, linalg_backend::B200>::workspace_size(linalg_int,
+    linear_solver_type);
+template <> size_t inversion<float, linalg_backend::B200>::workspace_size(linalg_int,
+    linear_solver_type);
+
+template <> double determinant<double, linalg_backend::B200>::apply(double*, linalg_int*,
+    linalg_int, linear_solver_type, void*, size_t, void*);
+template <> float determinant<float, linalg_backend::B200>::apply(float*, linalg_int*, linalg_int,
+    linear_solver_type, void*, size_t, void*);
+template <> size_t determinant<double, linalg_backend::B200>::workspace_size(linalg_int,
+    linear_solver_type);
+template <> size_t determinant<float, linalg_backend::B200>::workspace_size(linalg_int,
+    linear_solver_type);
 }  // namespace linalg

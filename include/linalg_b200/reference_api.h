@@ -7,6 +7,8 @@
  *   include/matrix_operation/linear_solver.h:15-65
  *   include/matrix_operation/triangular_solver.h:20-38
  *   include/matrix_operation/multiplication.h:15-114
+ *   include/matrix_operation/inversion.h:15-53
+ *   include/matrix_operation/determinant.h
  * Names, argument order, default arguments and meaning are the reference's;
  * that is what makes the backend a drop-in.  Inside the reference tree define
  * LINALG_B200_USE_REFERENCE_HEADERS and add B200 as the last enumerator of
@@ -20,6 +22,8 @@
 #if defined(LINALG_B200_USE_REFERENCE_HEADERS)
 #include "include/common/backend.h"
 #include "include/common/types.h"
+#include "include/matrix_operation/determinant.h"
+#include "include/matrix_operation/inversion.h"
 #include "include/matrix_operation/linear_solver.h"
 #include "include/matrix_operation/lu_decomposition.h"
 #include "include/matrix_operation/multiplication.h"
@@ -98,6 +102,20 @@ template <typename T, linalg_backend Backend> struct multiplication
     }
 
     LINALG_API static size_t workspace_size(linalg_int rows, linalg_int columns, linalg_int depth);
+};
+
+template <typename T, linalg_backend Backend> struct inversion
+{
+    LINALG_API static void apply(T* m, linalg_int* pivot, linalg_int lda, linear_solver_type type,
+        void* workspace, size_t workspace_size, void* stream = nullptr);
+    LINALG_API static size_t workspace_size(linalg_int lda, linear_solver_type type);
+};
+
+template <typename T, linalg_backend Backend> struct determinant
+{
+    LINALG_API static T apply(T* m, linalg_int* pivot, linalg_int lda, linear_solver_type type,
+        void* workspace, size_t workspace_size, void* stream = nullptr);
+    LINALG_API static size_t workspace_size(linalg_int lda, linear_solver_type type);
 };
 }  // namespace linalg
 #endif

@@ -10,10 +10,14 @@ from .api import (  # noqa: F401
     LU_LINEAR_SOLVER,
     LU_UPFRONT_LINEAR_SOLVER,
     MixedSolver,
+    det,
+    determinant,
     gemm,
     gesv,
     getrf,
     getrs,
+    inverse,
+    inversion,
     linear_solver,
     lu_decomposition,
     multiplication,

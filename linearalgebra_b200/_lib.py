@@ -54,6 +54,14 @@ SIGNATURES: dict[str, tuple] = {
     "b200la_dgesv_noalloc": (_i32, [_p, _p, _i64, _p, _i32, _p]),
     "b200la_dgetrs_workspace_size": (_sz, [_i64, _i64]),
     "b200la_dgetrs": (_i32, [_p, _p, _i64, _i64, _p, _i64, _p, _sz, _p]),
+    "b200la_dinverse_workspace_size": (_sz, [_i64, _i32]),
+    "b200la_sinverse_workspace_size": (_sz, [_i64, _i32]),
+    "b200la_dinverse": (_i32, [_p, _p, _i64, _i32, _p, _sz, _p]),
+    "b200la_sinverse": (_i32, [_p, _p, _i64, _i32, _p, _sz, _p]),
+    "b200la_ddeterminant_workspace_size": (_sz, [_i64, _i32]),
+    "b200la_sdeterminant_workspace_size": (_sz, [_i64, _i32]),
+    "b200la_ddeterminant": (_i32, [_p, _p, _i64, _i32, _p, _p, _p, _p, _sz, _p]),
+    "b200la_sdeterminant": (_i32, [_p, _p, _i64, _i32, _p, _p, _p, _p, _sz, _p]),
     "b200la_dtrsm_workspace_size": (_sz, [_i64, _i64]),
     "b200la_strsm_workspace_size": (_sz, [_i64, _i64]),
     "b200la_dtrsm": (_i32, [_i32, _i32, _i32, _i64, _i64, _p, _i64, _p, _i64, _p, _i64, _p, _sz, _p]),

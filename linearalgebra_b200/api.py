@@ -10,8 +10,11 @@ contiguous where the reference expects a packed matrix); ``stream`` is a
 ``torch.cuda.Stream`` or ``None`` for the current stream.  Errors raise like
 the reference's LINALG_CHECK (ValueError subclasses for invalid arguments).
 
-Convenience wrappers (``getrf``, ``gesv``, ``getrs``, ``trsm``, ``gemm``)
-allocate the workspace with torch and return results.
+``inversion`` and ``determinant`` (include/matrix_operation/{inversion,
+determinant}.h) follow the same pattern for their LU modes.
+
+Convenience wrappers (``getrf``, ``gesv``, ``getrs``, ``trsm``, ``gemm``,
+``inverse``, ``det``) allocate the workspace with torch and return results.
 """
 from __future__ import annotations
 
@@ -121,6 +124,47 @@ class multiplication:
                      workspace_size, _stream(stream)))
 
 
+class inversion:
+    """inversion<T, B200>, LU modes (include/matrix_operation/inversion.h:15-53)."""
+
+    @staticmethod
+    def workspace_size(lda: int, type: int = LU_LINEAR_SOLVER, dtype=torch.float64) -> int:
+        return int(getattr(_lib.load(), f"b200la_{_prefix(dtype)}inverse_workspace_size")(lda, type))
+
+    @staticmethod
+    def apply(m, pivot, lda: int, type: int, workspace, workspace_size: int, stream=None):
+        """Invert m in place (asynchronous).  pivot may be None in LU mode."""
+        f = getattr(_lib.load(), f"b200la_{_prefix(m.dtype)}inverse")
+        _lib.check(f(_ptr(m), _ptr(pivot), lda, type, _ptr(workspace), workspace_size, _stream(stream)))
+
+
+class determinant:
+    """determinant<T, B200>, LU modes (include/matrix_operation/determinant.h)."""
+
+    @staticmethod
+    def workspace_size(lda: int, type: int = LU_LINEAR_SOLVER, dtype=torch.float64) -> int:
+        return int(getattr(_lib.load(), f"b200la_{_prefix(dtype)}determinant_workspace_size")(lda, type))
+
+    @staticmethod
+    def parts(m, pivot, lda: int, type: int, workspace, workspace_size: int, stream=None):
+        """(product, sign, log_abs, singular): U's diagonal product in index
+        order (the reference's NATIVE value), the pivot sign, sum log|u_ii|,
+        and whether LU mode met an exact zero pivot (product 0)."""
+        ct = ctypes.c_double if m.dtype == torch.float64 else ctypes.c_float
+        product, sign, log_abs = ct(0), ctypes.c_int(1), ctypes.c_double(0)
+        f = getattr(_lib.load(), f"b200la_{_prefix(m.dtype)}determinant")
+        st = f(_ptr(m), _ptr(pivot), lda, type, ctypes.addressof(product), ctypes.addressof(sign),
+               ctypes.addressof(log_abs), _ptr(workspace), workspace_size, _stream(stream))
+        _lib.check(st, allow=(_lib.SUCCESS, _lib.SINGULAR))
+        return product.value, sign.value, log_abs.value, st == _lib.SINGULAR
+
+    @staticmethod
+    def apply(m, pivot, lda: int, type: int, workspace, workspace_size: int, stream=None) -> float:
+        """det(A) = sign * product (0 when LU mode met an exact zero pivot)."""
+        product, sign, _, _ = determinant.parts(m, pivot, lda, type, workspace, workspace_size, stream)
+        return 0.0 if product == 0 else (-product if sign < 0 else product)
+
+
 # ----------------------------------------------------------------------------
 # convenience wrappers
 # ----------------------------------------------------------------------------
@@ -159,6 +203,37 @@ def getrs(lu: torch.Tensor, pivot: torch.Tensor, x: torch.Tensor, stream=None):
     _lib.check(lib.b200la_dgetrs(_ptr(lu), _ptr(pivot), n, nrhs, _ptr(x), ldx, _ptr(ws),
                                  ws.numel(), _stream(stream)))
     return x
+
+
+def inverse(m: torch.Tensor, pivot: torch.Tensor | None = None, type: int = LU_LINEAR_SOLVER,
+            stream=None):
+    """inversion LU modes in place on m.  Returns (pivot, info): info is the
+    factorization's LAPACK info (nonzero: m holds the factors, not the
+    inverse).  Synchronizes the stream to read it."""
+    n = m.shape[0]
+    if pivot is None:
+        pivot = torch.empty(n, dtype=torch.int64, device=m.device)
+    nbytes = inversion.workspace_size(n, type, m.dtype)
+    ws = workspace(nbytes, m.device)
+    inversion.apply(m, pivot, n, type, ws, ws.numel(), stream)
+    info = ctypes.c_int(0)
+    _lib.check(_lib.load().b200la_workspace_status(_ptr(ws), ctypes.addressof(info), _stream(stream)),
+               allow=(_lib.SUCCESS, _lib.SINGULAR))
+    return pivot, int(info.value)
+
+
+def det(m: torch.Tensor, pivot: torch.Tensor | None = None, type: int = LU_LINEAR_SOLVER, stream=None):
+    """determinant LU modes (m factored in place in LU mode).  Returns a dict
+    with det (signed), product, sign, log_abs, singular and the pivot tensor."""
+    n = m.shape[0]
+    if pivot is None:
+        pivot = torch.empty(n, dtype=torch.int64, device=m.device)
+    nbytes = determinant.workspace_size(n, type, m.dtype)
+    ws = workspace(nbytes, m.device)
+    product, sign, log_abs, singular = determinant.parts(m, pivot, n, type, ws, ws.numel(), stream)
+    value = 0.0 if product == 0 else (-product if sign < 0 else product)
+    return {"det": value, "product": product, "sign": sign, "log_abs": log_abs, "singular": singular,
+            "pivot": pivot}
 
 
 def trsm(upper, transpose, unit, a, b, x=None, stream=None):

@@ -145,4 +145,63 @@ size_t multiplication<float, linalg_backend::B200>::workspace_size(
 {
     return b200la_sgemm_workspace_size(rows, columns, depth);
 }
+
+// ---- inversion --------------------------------------------------------------
+template <>
+void inversion<double, linalg_backend::B200>::apply(double* m, linalg_int* pivot, linalg_int lda,
+    linear_solver_type type, void* workspace, size_t workspace_size, void* stream)
+{
+    check_status(b200la_dinverse(m, pv(pivot), lda, static_cast<int>(type), workspace,
+        workspace_size, stream));
+}
+template <>
+void inversion<float, linalg_backend::B200>::apply(float* m, linalg_int* pivot, linalg_int lda,
+    linear_solver_type type, void* workspace, size_t workspace_size, void* stream)
+{
+    check_status(b200la_sinverse(m, pv(pivot), lda, static_cast<int>(type), workspace,
+        workspace_size, stream));
+}
+template <>
+size_t inversion<double, linalg_backend::B200>::workspace_size(linalg_int lda, linear_solver_type type)
+{
+    return b200la_dinverse_workspace_size(lda, static_cast<int>(type));
+}
+template <>
+size_t inversion<float, linalg_backend::B200>::workspace_size(linalg_int lda, linear_solver_type type)
+{
+    return b200la_sinverse_workspace_size(lda, static_cast<int>(type));
+}
+
+// ---- determinant ------------------------------------------------------------
+// det(A) = sign * product; an exactly singular factorization gives +0.
+template <>
+double determinant<double, linalg_backend::B200>::apply(double* m, linalg_int* pivot,
+    linalg_int lda, linear_solver_type type, void* workspace, size_t workspace_size, void* stream)
+{
+    double product = 0.0;
+    int    sign    = 1;
+    check_status(b200la_ddeterminant(m, pv(pivot), lda, static_cast<int>(type), &product, &sign,
+        nullptr, workspace, workspace_size, stream));
+    return product == 0.0 ? 0.0 : (sign < 0 ? -product : product);
+}
+template <>
+float determinant<float, linalg_backend::B200>::apply(float* m, linalg_int* pivot, linalg_int lda,
+    linear_solver_type type, void* workspace, size_t workspace_size, void* stream)
+{
+    float product = 0.0f;
+    int   sign    = 1;
+    check_status(b200la_sdeterminant(m, pv(pivot), lda, static_cast<int>(type), &product, &sign,
+        nullptr, workspace, workspace_size, stream));
+    return product == 0.0f ? 0.0f : (sign < 0 ? -product : product);
+}
+template <>
+size_t determinant<double, linalg_backend::B200>::workspace_size(linalg_int lda, linear_solver_type type)
+{
+    return b200la_ddeterminant_workspace_size(lda, static_cast<int>(type));
+}
+template <>
+size_t determinant<float, linalg_backend::B200>::workspace_size(linalg_int lda, linear_solver_type type)
+{
+    return b200la_sdeterminant_workspace_size(lda, static_cast<int>(type));
+}
 }  // namespace linalg

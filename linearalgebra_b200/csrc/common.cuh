@@ -130,7 +130,9 @@ enum KernelClass : int
     KC_BATCHED  = 7,
     KC_PREP     = 8,
     KC_SELECT   = 9,
-    KC_COUNT    = 10
+    KC_INV_GEMM = 10,  // inversion: the blocked substitutions' GEMM updates
+    KC_INV_AUX  = 11,  // inversion / determinant: identity, column gather, diagonal product
+    KC_COUNT    = 12
 };
 
 // Host helpers shared by the entry points (defined in runtime.cu).

@@ -1,0 +1,314 @@
+// FP64 matrix update on the tensor cores: C[M x N] -= A[M x K] B[K x N]
+// (row-major, row strides lda, ldb, ldc) with mma.sync m8n8k4 f64 (DMMA).
+//
+// One m8n8k4 DMMA computes, for every element of its 8 x 8 tile,
+// d = c + a0 b0 + a1 b1 + a2 b2 + a3 b3 as four fused multiply-adds in k
+// order, each rounded: on the B200 a chain of them along k gives the same
+// bits as the scalar loop d = fma(a_k, b_k, d) for k = 0, 1, ... (measured
+// on normal, subnormal, underflowing, overflowing, NaN/Inf and signed-zero
+// operands).  That is what lets the blocked LU's trailing update run here
+// and still reproduce the reference's factors bit for bit.
+//
+// Two modes:
+//   FROM_ZERO = true   delta = sum_k a_ik b_kj accumulated from zero in k
+//                      order, then C = C - delta: the LU trailing update of
+//                      lu_decomposition_native.cpp:400-422 (delta from the
+//                      GEMM, then subtracted), bit-identical to it;
+//   FROM_ZERO = false  the accumulators start at -C and end at -(C - A B),
+//                      stored negated (inversion: no bit-parity requirement,
+//                      and C is loaded while the first stages are in flight).
+//
+// CTA tile kDmTile x kDmTile, 16 warps of 32 x 32 (4 x 4 DMMA tiles, 32
+// accumulators per thread, 4 warps per scheduler), K streamed in kDmKC-deep
+// stages through a kDmStages cp.async ring.  Fragments (g = lane/4,
+// t = lane%4): A[8 rows][4 k] -> a = A[g][t]; B[4 k][8 cols] -> b = B[t][g];
+// C[8][8] -> c0, c1 = C[g][2t], C[g][2t+1].  The padded smem rows (A: kDmKC
+// + 4 doubles, B: kDmTile + 4) place the rows one fragment load touches 8
+// banks apart, so every fragment load is the minimal two wavefronts.
+// Zero-filled padding (k >= K, rows >= M, columns >= N) adds +0 products,
+// which leave a from-zero sum unchanged (it is never -0).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "lu_kernels.cuh"
+#include "solve_kernels.cuh"
+
+namespace b200la
+{
+
+constexpr int    kDmTile    = 128;
+constexpr int    kDmThreads = 512;
+constexpr int    kDmKC      = 32;
+constexpr int    kDmLDA     = kDmKC + 4;
+constexpr int    kDmLDB     = kDmTile + 4;
+constexpr int    kDmStages  = 3;
+constexpr int    kDmAElems  = kDmTile * kDmLDA;
+constexpr int    kDmStage   = kDmAElems + kDmKC * kDmLDB;
+constexpr size_t kDmSmem    = sizeof(double) * (size_t)kDmStages * kDmStage;
+
+__device__ __forceinline__ void dmma_884(double& c0, double& c1, double a, double b)
+{
+    asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+        : "+d"(c0), "+d"(c1)
+        : "d"(a), "d"(b));
+}
+
+// One 16-byte piece (two doubles) global -> shared; `valid` leading elements
+// copied, the rest zero-filled.  Whole pieces as one 16-byte cp.async when
+// the rows are 16-byte aligned, else element by element.
+__device__ __forceinline__ void dm_piece(double* s, const double* g, const double* safe, int valid, bool vec16)
+{
+    if (vec16 && (valid >= 2 || valid <= 0))
+    {
+        cp_async16(s, valid > 0 ? g : safe, valid > 0);
+        return;
+    }
+    cp_async8(s, valid > 0 ? g : safe, valid > 0);
+    cp_async8(s + 1, valid > 1 ? g + 1 : safe, valid > 1);
+}
+
+__device__ __forceinline__ void dm_load_stage(double* sa, double* sb, const double* A, int64_t lda,
+    const double* B, int64_t ldb, int M, int N, int K, int m0, int n0, int k0, bool vec16)
+{
+    constexpr int APR = kDmKC / 2;    // pieces per A row
+    constexpr int BPR = kDmTile / 2;  // pieces per B row
+#pragma unroll
+    for (int e = threadIdx.x; e < kDmTile * APR; e += kDmThreads)
+    {
+        const int r = e / APR, q = e - (e / APR) * APR;
+        const int row = m0 + r, col = k0 + 2 * q;
+        const int valid = row < M ? min(2, K - col) : 0;
+        dm_piece(sa + r * kDmLDA + 2 * q, valid > 0 ? A + (int64_t)row * lda + col : A, A, valid, vec16);
+    }
+#pragma unroll
+    for (int e = threadIdx.x; e < kDmKC * BPR; e += kDmThreads)
+    {
+        const int p = e / BPR, q = e - (e / BPR) * BPR;
+        const int row = k0 + p, col = n0 + 2 * q;
+        const int valid = row < K ? min(2, N - col) : 0;
+        dm_piece(sb + p * kDmLDB + 2 * q, valid > 0 ? B + (int64_t)row * ldb + col : B, B, valid, vec16);
+    }
+}
+
+template <bool FROM_ZERO>
+__global__ void __launch_bounds__(kDmThreads, 1) k_dmma_update(int M, int N, int K, const double* __restrict__ A,
+    int64_t lda, const double* __restrict__ B, int64_t ldb, double* __restrict__ C, int64_t ldc, int vec16,
+    const DeviceStatus* gate)
+{
+    extern __shared__ __align__(16) unsigned char dm_smem[];
+    if (gated(gate))
+    {
+        return;
+    }
+    double*    smem    = reinterpret_cast<double*>(dm_smem);
+    const int  m0      = blockIdx.y * kDmTile;
+    const int  n0      = blockIdx.x * kDmTile;
+    const int  warp    = threadIdx.x >> 5;
+    const int  lane    = threadIdx.x & 31;
+    const int  g       = lane >> 2;
+    const int  t       = lane & 3;
+    const int  wm      = (warp >> 2) * 32;
+    const int  wn      = (warp & 3) * 32;
+    const int  nchunks = (K + kDmKC - 1) / kDmKC;
+    const bool v16     = vec16 != 0;
+
+    double acc[4][4][2];
+    if (FROM_ZERO)
+    {
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+        {
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+            {
+                acc[i][j][0] = 0.0;
+                acc[i][j][1] = 0.0;
+            }
+        }
+        // pull the C tile into L2 while the products accumulate
+        const int r = threadIdx.x >> 2, q = threadIdx.x & 3;
+        if (m0 + r < M)
+        {
+            const double* crow = C + (int64_t)(m0 + r) * ldc + n0;
+#pragma unroll
+            for (int h = 0; h < 2; ++h)
+            {
+                const int c = (q + 4 * h) * 16;
+                if (n0 + c < N)
+                {
+                    asm volatile("prefetch.global.L2 [%0];" ::"l"(crow + c));
+                }
+            }
+        }
+    }
+    else
+    {
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+        {
+            const int     row  = m0 + wm + 8 * i + g;
+            const double* crow = C + (int64_t)row * ldc;
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+            {
+                const int col = n0 + wn + 8 * j + 2 * t;
+                double2   v   = make_double2(0.0, 0.0);
+                if (row < M)
+                {
+                    if (v16 && col + 1 < N)
+                    {
+                        v = *reinterpret_cast<const double2*>(crow + col);
+                    }
+                    else
+                    {
+                        v.x = col < N ? crow[col] : 0.0;
+                        v.y = col + 1 < N ? crow[col + 1] : 0.0;
+                    }
+                }
+                acc[i][j][0] = -v.x;
+                acc[i][j][1] = -v.y;
+            }
+        }
+    }
+
+#pragma unroll
+    for (int s = 0; s < kDmStages - 1; ++s)
+    {
+        if (s < nchunks)
+        {
+            double* sa = smem + s * kDmStage;
+            dm_load_stage(sa, sa + kDmAElems, A, lda, B, ldb, M, N, K, m0, n0, s * kDmKC, v16);
+        }
+        cp_async_commit();
+    }
+    for (int c = 0; c < nchunks; ++c)
+    {
+        cp_async_wait<kDmStages - 2>();
+        __syncthreads();  // stage c landed for every thread; stage c-1 is free
+        const int pf = c + kDmStages - 1;
+        if (pf < nchunks)
+        {
+            double* sa = smem + (pf % kDmStages) * kDmStage;
+            dm_load_stage(sa, sa + kDmAElems, A, lda, B, ldb, M, N, K, m0, n0, pf * kDmKC, v16);
+        }
+        cp_async_commit();
+        const double* sa = smem + (c % kDmStages) * kDmStage + (wm + g) * kDmLDA + t;
+        const double* sb = smem + (c % kDmStages) * kDmStage + kDmAElems + t * kDmLDB + wn + g;
+#pragma unroll
+        for (int ks = 0; ks < kDmKC / 4; ++ks)
+        {
+            double af[4], bf[4];
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+            {
+                af[i] = sa[8 * i * kDmLDA + 4 * ks];
+            }
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+            {
+                bf[j] = sb[4 * ks * kDmLDB + 8 * j];
+            }
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+            {
+#pragma unroll
+                for (int j = 0; j < 4; ++j)
+                {
+                    dmma_884(acc[i][j][0], acc[i][j][1], af[i], bf[j]);
+                }
+            }
+        }
+    }
+    cp_async_wait<0>();
+
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+    {
+        const int row = m0 + wm + 8 * i + g;
+        if (row >= M)
+        {
+            continue;
+        }
+        double* crow = C + (int64_t)row * ldc;
+        if (FROM_ZERO)
+        {
+            double2 cv[4];
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+            {
+                const int col = n0 + wn + 8 * j + 2 * t;
+                if (v16 && col + 1 < N)
+                {
+                    cv[j] = *reinterpret_cast<const double2*>(crow + col);
+                }
+                else
+                {
+                    cv[j].x = col < N ? crow[col] : 0.0;
+                    cv[j].y = col + 1 < N ? crow[col + 1] : 0.0;
+                }
+            }
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+            {
+                cv[j].x = cv[j].x - acc[i][j][0];
+                cv[j].y = cv[j].y - acc[i][j][1];
+            }
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+            {
+                const int col = n0 + wn + 8 * j + 2 * t;
+                if (v16 && col + 1 < N)
+                {
+                    *reinterpret_cast<double2*>(crow + col) = cv[j];
+                }
+                else
+                {
+                    if (col < N)
+                    {
+                        crow[col] = cv[j].x;
+                    }
+                    if (col + 1 < N)
+                    {
+                        crow[col + 1] = cv[j].y;
+                    }
+                }
+            }
+        }
+        else
+        {
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+            {
+                const int col = n0 + wn + 8 * j + 2 * t;
+                if (v16 && col + 1 < N)
+                {
+                    *reinterpret_cast<double2*>(crow + col) = make_double2(-acc[i][j][0], -acc[i][j][1]);
+                }
+                else
+                {
+                    if (col < N)
+                    {
+                        crow[col] = -acc[i][j][0];
+                    }
+                    if (col + 1 < N)
+                    {
+                        crow[col + 1] = -acc[i][j][1];
+                    }
+                }
+            }
+        }
+    }
+}
+
+inline bool dm_aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; }
+
+// 1 when every operand's rows start 16-byte aligned (the 16-byte copy path).
+inline int dm_vec16(const double* a, int64_t lda, const double* b, int64_t ldb, const double* c, int64_t ldc)
+{
+    return dm_aligned16(a) && dm_aligned16(b) && dm_aligned16(c) && (lda * 8) % 16 == 0 && (ldb * 8) % 16 == 0 &&
+           (ldc * 8) % 16 == 0;
+}
+
+}  // namespace b200la

@@ -10,6 +10,7 @@
 #include <cstdlib>
 #include <mutex>
 
+#include "dmma.cuh"
 #include "lu_kernels.cuh"
 #include "solve_kernels.cuh"
 
@@ -82,6 +83,10 @@ template <typename T> int ensure_kernel_attributes()
         k_laswp_trsm<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)laswp_smem_bytes<T>()));
     B200LA_CUDA(cudaFuncSetAttribute(
         k_trailing<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)trailing_smem_bytes<T>()));
+    B200LA_CUDA(cudaFuncSetAttribute(
+        k_dmma_update<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDmSmem));
+    B200LA_CUDA(cudaFuncSetAttribute(
+        k_dmma_update<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDmSmem));
     B200LA_CUDA(cudaFuncSetAttribute(k_gemm<T, false, false>,
         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gemm_smem_bytes<T>()));
     B200LA_CUDA(cudaFuncSetAttribute(k_gemm<T, true, false>,
@@ -298,9 +303,23 @@ int enqueue_getrf(T* m, int n, int64_t* pivot, const GetrfPlan<T>& p, cudaStream
         }
         if (rest > 0)
         {
-            dim3 grid((rest + kChunkN - 1) / kChunkN, (rest + kBandM - 1) / kBandM);
             prof_begin(KC_TRAILING, s);
-            k_trailing<T><<<grid, 128, trailing_smem_bytes<T>(), s>>>(m, n, k, w, rest);
+            if constexpr (sizeof(T) == 8)
+            {
+                // A22 -= L21 U12 on the tensor cores, delta from zero then
+                // subtracted: the same bits as k_trailing's fma loop.
+                const double* l21 = m + (int64_t)(k + w) * n + k;
+                const double* u12 = m + (int64_t)k * n + k + w;
+                double*       a22 = m + (int64_t)(k + w) * n + k + w;
+                const dim3    grid((rest + kDmTile - 1) / kDmTile, (rest + kDmTile - 1) / kDmTile);
+                k_dmma_update<true><<<grid, kDmThreads, kDmSmem, s>>>(
+                    rest, rest, w, l21, n, u12, n, a22, n, dm_vec16(l21, n, u12, n, a22, n), nullptr);
+            }
+            else
+            {
+                dim3 grid((rest + kChunkN - 1) / kChunkN, (rest + kBandM - 1) / kBandM);
+                k_trailing<T><<<grid, 128, trailing_smem_bytes<T>(), s>>>(m, n, k, w, rest);
+            }
             prof_end(KC_TRAILING, s);
             B200LA_LAUNCH_CHECK();
         }

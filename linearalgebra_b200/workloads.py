@@ -107,6 +107,30 @@ def known_answer_matrices(dtype=np.float64) -> dict[str, np.ndarray]:
 
 KNOWN_ANSWER_INFO = {"zero_col": 1, "rank_def": 2, "zeros2": 1, "tiny_eye": 0, "subnormal": 0}
 
+
+def spd_product(n: int, seed: int, dtype=np.float64) -> np.ndarray:
+    """A = R R^T with R unit lower triangular, R[i][j] = 0.4 U[0,1) below the
+    diagonal: the construction of the reference's inversion test
+    (Testing/Cxx/TestInversion.cxx:46-68), seeded here."""
+    rng = np.random.default_rng(seed)
+    r = np.tril(0.4 * rng.random((n, n)), -1) + np.eye(n)
+    r = r.astype(dtype)
+    return (r.astype(np.float64) @ r.T.astype(np.float64)).astype(dtype)
+
+
+def determinant_known_answers() -> dict[str, tuple[list[float], float]]:
+    """Diagonal matrices and their determinants, the LU-mode cases of the
+    reference's determinant test (Testing/Cxx/TestDeterminant.cxx:84-127):
+    name -> (diagonal, determinant)."""
+    return {
+        "diag2": ([2.0, 3.0], 6.0),
+        "diag3": ([2.0, 3.0, 4.0], 24.0),
+        "diag4": ([1.0, 2.0, 3.0, 5.0], 30.0),
+        "eye1": ([1.0], 1.0),
+        "eye4": ([1.0] * 4, 1.0),
+        "singular": ([1.0, 0.0, 1.0], 0.0),
+    }
+
 TRIANGULAR_SHAPES = ((1, 1), (5, 3), (17, 7), (35, 1), (35, 9), (65, 2))
 
 

@@ -78,6 +78,16 @@ class Oracle:
             ct = ctypes.c_double if t == "d" else ctypes.c_float
             f.argtypes = [_int, _int, _i64, _i64, _i64, ct, _p, _i64, _p, _i64, ct, _p, _i64]
             f.restype = _int
+            f = getattr(self.lib, f"{pre}{t}getri")
+            f.argtypes = [_p, _p, _i64, _int]
+            f.restype = _int
+            f = getattr(self.lib, f"{pre}{t}det")
+            if kind == "port":
+                f.argtypes = [_p, _p, _i64, _int, _p]
+                f.restype = ct
+            else:
+                f.argtypes = [_p, _p, _i64, _int, _p]
+                f.restype = _int
         if kind == "port":
             self.lib.or_backward_error.argtypes = [_p, _i64, _i64, _p, _p]
             self.lib.or_backward_error.restype = ctypes.c_double
@@ -129,6 +139,37 @@ class Oracle:
         if st < 0:
             raise ValueError(f"gemm rejected its arguments (status {st})")
         return c
+
+    def getri(self, a: np.ndarray, mode: int = LU_LINEAR_SOLVER, pivot=None):
+        """inversion LU modes on copies; returns (m, pivot, status): m holds
+        the inverse, or the factors when mode 1 met an exact zero pivot."""
+        m = np.ascontiguousarray(a).copy()
+        n = m.shape[0]
+        piv = np.full(n, -1, dtype=np.int64) if pivot is None else np.ascontiguousarray(pivot, dtype=np.int64).copy()
+        st = getattr(self.lib, f"{self._pre}{self._t(m)}getri")(_ptr(m), _ptr(piv), n, mode)
+        if st < 0:
+            raise ValueError(f"inversion rejected its arguments (status {st})")
+        return m, piv, int(st)
+
+    def det(self, a: np.ndarray, mode: int = LU_LINEAR_SOLVER, pivot=None):
+        """determinant LU modes on a copy; returns (value, m, pivot): the
+        reference's value (U's diagonal product, no pivot sign; 0 when mode 1
+        met an exact zero pivot) and the factored matrix."""
+        m = np.ascontiguousarray(a).copy()
+        n = m.shape[0]
+        piv = np.full(n, -1, dtype=np.int64) if pivot is None else np.ascontiguousarray(pivot, dtype=np.int64).copy()
+        f = getattr(self.lib, f"{self._pre}{self._t(m)}det")
+        if self.kind == "port":
+            st = ctypes.c_int(-1)
+            val = f(_ptr(m), _ptr(piv), n, mode, ctypes.addressof(st))
+            status = st.value
+        else:
+            out = np.zeros(1, dtype=m.dtype)
+            status = f(_ptr(m), _ptr(piv), n, mode, _ptr(out))
+            val = out[0]
+        if status < 0:
+            raise ValueError(f"determinant rejected its arguments (status {status})")
+        return m.dtype.type(val), m, piv
 
     # --- metrics (port build only) ---
     def backward_error(self, a: np.ndarray, x: np.ndarray, b: np.ndarray) -> float:

@@ -290,6 +290,110 @@ int OR_FN(gesv)(T* m, int64_t* pivot, int64_t n, T* x, int mode)
     return -1;
 }
 
+/* Inverse from LU factors, inversion_native.cpp:228-304 (lu_invert):
+ *  - inv = I, then rows (i, pivot[i]-1) swapped for i = 0..n-1 in order;
+ *  - forward, rows i = 0..n-1: row_i -= m[i][k] row_k for k = 0..i-1 in
+ *    order, one fused multiply-add per element (inv_axpy_sub, :82-126);
+ *  - backward, rows i = n-1..0: row_i -= m[i][k] row_k for k = i+1..n-1 in
+ *    order, then row_i *= 1 / m[i][i] (a reciprocal, then products);
+ *  - m = inv.
+ * Mode dispatch, inversion_native.cpp:412-440: mode 1 factors m first and
+ * inverts only if the factorization found no exact zero pivot (m then keeps
+ * the factors); mode 2 inverts the factors and pivots as given.  Returns the
+ * getrf status for mode 1, 0 for mode 2, -1 for invalid arguments. */
+int OR_FN(getri)(T* m, int64_t* pivot, int64_t n, int mode)
+{
+    if (m == NULL || pivot == NULL || n <= 0 || (mode != 1 && mode != 2))
+    {
+        return -1;
+    }
+    int st = 0;
+    if (mode == 1)
+    {
+        st = OR_FN(getrf)(m, n, pivot, NULL);
+        if (st != 0)
+        {
+            return st;
+        }
+    }
+    T* inv = (T*)calloc((size_t)(n * n), sizeof(T));
+    if (inv == NULL)
+    {
+        return -2;
+    }
+    for (int64_t i = 0; i < n; ++i)
+    {
+        inv[i * n + i] = (T)1;
+    }
+    for (int64_t i = 0; i < n; ++i)
+    {
+        const int64_t p = pivot[i] - 1;
+        if (p != i)
+        {
+            for (int64_t c = 0; c < n; ++c)
+            {
+                const T t        = inv[i * n + c];
+                inv[i * n + c] = inv[p * n + c];
+                inv[p * n + c] = t;
+            }
+        }
+    }
+    for (int64_t i = 0; i < n; ++i)
+    {
+        for (int64_t k = 0; k < i; ++k)
+        {
+            OR_CAT(axpy_sub_, SUF)(inv + i * n, inv + k * n, m[i * n + k], n);
+        }
+    }
+    for (int64_t i = n - 1; i >= 0; --i)
+    {
+        for (int64_t k = i + 1; k < n; ++k)
+        {
+            OR_CAT(axpy_sub_, SUF)(inv + i * n, inv + k * n, m[i * n + k], n);
+        }
+        const T inv_diag = (T)1 / m[i * n + i];
+        for (int64_t c = 0; c < n; ++c)
+        {
+            inv[i * n + c] *= inv_diag;
+        }
+    }
+    for (int64_t e = 0; e < n * n; ++e)
+    {
+        m[e] = inv[e];
+    }
+    free(inv);
+    return st;
+}
+
+/* Determinant, determinant.cpp:18-27 (lu_determinant: the product of U's
+ * diagonal in index order, no pivot sign) and :56-80 (LU modes): mode 1
+ * factors m in place and returns the product if the factorization found no
+ * exact zero pivot, else 0; mode 2 multiplies the diagonal of m as given.
+ * *status: the getrf status (mode 1), 0 (mode 2) or -1 (invalid). */
+T OR_FN(det)(T* m, int64_t* pivot, int64_t n, int mode, int* status)
+{
+    *status = -1;
+    if (m == NULL || n <= 0 || (mode != 1 && mode != 2) || (mode == 1 && pivot == NULL))
+    {
+        return (T)0;
+    }
+    *status = 0;
+    if (mode == 1)
+    {
+        *status = OR_FN(getrf)(m, n, pivot, NULL);
+        if (*status != 0)
+        {
+            return (T)0;
+        }
+    }
+    T det = m[0];
+    for (int64_t i = 1; i < n; ++i)
+    {
+        det *= m[i * n + i];
+    }
+    return det;
+}
+
 /* c = alpha op(a) op(b) + beta c, row-major, BLAS contract:
  * multiplication_native.cpp:1542-1567 (beta applied up front; beta == 0
  * overwrites c), :1807-1814 (alpha == 0 quick return), and the scalar loop

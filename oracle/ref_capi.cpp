@@ -3,8 +3,9 @@
  * Python tests and the CPU baseline arm of bench.py can call the reference
  * implementation through ctypes.  Compiled together with the reference's
  * sources (src/matrix_operation/cpu/native/{lu_decomposition,linear_solver,
- * triangular_solver,multiplication,cholesky_decomposition}_native.cpp) by
- * oracle/Makefile into oracle/_ref/libref_native.so.
+ * triangular_solver,multiplication,cholesky_decomposition,inversion}_native.cpp
+ * and src/matrix_operation/cpu/determinant.cpp) by oracle/Makefile into
+ * oracle/_ref/libref_native.so.
  *
  * TEST INFRASTRUCTURE ONLY.  Nothing in the B200 library links or calls this.
  *
@@ -20,6 +21,8 @@
 #include <new>
 #include <vector>
 
+#include "include/matrix_operation/determinant.h"
+#include "include/matrix_operation/inversion.h"
 #include "include/matrix_operation/linear_solver.h"
 #include "include/matrix_operation/lu_decomposition.h"
 #include "include/matrix_operation/multiplication.h"
@@ -128,6 +131,47 @@ int ref_gemm(int ta, int tb, int64_t rows, int64_t cols, int64_t depth, T alpha,
         return -1;
     }
 }
+template <typename T> int ref_getri(T* m, int64_t* pivot, int64_t n, int type)
+{
+    try
+    {
+        const auto   t     = static_cast<linalg::linear_solver_type>(type);
+        const size_t bytes = linalg::inversion<T, linalg_backend::NATIVE>::workspace_size(n, t);
+        std::vector<unsigned char> ws(bytes ? bytes : 1);
+        linalg::inversion<T, linalg_backend::NATIVE>::apply(
+            m, reinterpret_cast<linalg_int*>(pivot), n, t, ws.data(), bytes);
+        return 0;
+    }
+    catch (const std::bad_alloc&)
+    {
+        return -2;
+    }
+    catch (...)
+    {
+        return -1;
+    }
+}
+
+template <typename T> int ref_det(T* m, int64_t* pivot, int64_t n, int type, T* out)
+{
+    try
+    {
+        const auto   t     = static_cast<linalg::linear_solver_type>(type);
+        const size_t bytes = linalg::determinant<T, linalg_backend::NATIVE>::workspace_size(n, t);
+        std::vector<unsigned char> ws(bytes ? bytes : 1);
+        *out = linalg::determinant<T, linalg_backend::NATIVE>::apply(
+            m, reinterpret_cast<linalg_int*>(pivot), n, t, ws.data(), bytes);
+        return 0;
+    }
+    catch (const std::bad_alloc&)
+    {
+        return -2;
+    }
+    catch (...)
+    {
+        return -1;
+    }
+}
 }  // namespace
 
 extern "C" {
@@ -167,6 +211,22 @@ int ref_sgemm(int ta, int tb, int64_t rows, int64_t cols, int64_t depth, float a
     const float* a, int64_t lda, const float* b, int64_t ldb, float beta, float* c, int64_t ldc)
 {
     return ref_gemm(ta, tb, rows, cols, depth, alpha, a, lda, b, ldb, beta, c, ldc);
+}
+int ref_dgetri(double* m, int64_t* pivot, int64_t n, int type)
+{
+    return ref_getri(m, pivot, n, type);
+}
+int ref_sgetri(float* m, int64_t* pivot, int64_t n, int type)
+{
+    return ref_getri(m, pivot, n, type);
+}
+int ref_ddet(double* m, int64_t* pivot, int64_t n, int type, double* out)
+{
+    return ref_det(m, pivot, n, type, out);
+}
+int ref_sdet(float* m, int64_t* pivot, int64_t n, int type, float* out)
+{
+    return ref_det(m, pivot, n, type, out);
 }
 size_t ref_dgetrf_workspace_size(int64_t n)
 {

@@ -33,6 +33,12 @@ def golden():
 
 
 @pytest.fixture(scope="session")
+def inverse_golden():
+    import numpy as np
+    return np.load(os.path.join(ROOT, "tests", "golden", "inverse_golden.npz"))
+
+
+@pytest.fixture(scope="session")
 def port():
     from oracle import Oracle
     return Oracle("port")

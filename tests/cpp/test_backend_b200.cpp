@@ -229,6 +229,67 @@ static void test_singular_status()
     CHECK(!ok && info == 1, "singular 2x2 zeros: false, info 1");
 }
 
+// Mirrors the reference's GPU inversion test (A * A^-1 == I on an SPD matrix
+// of order 23, null pivot allowed in LU mode) and its 2x2 determinant case.
+static void test_inversion_determinant()
+{
+    const int n = 23;
+    auto      r = random_matrix(n, n, 11, -1, 1);
+    std::vector<double> a((size_t)n * n, 0.0);
+    for (int i = 0; i < n; ++i)
+        for (int j = 0; j < n; ++j)
+        {
+            double s = 0;
+            for (int k = 0; k < n; ++k) s += r[i * n + k] * r[j * n + k];
+            a[i * n + j] = s + (i == j ? n : 0.0);
+        }
+    const auto          type  = linalg::linear_solver_type::LU_LINEAR_SOLVER;
+    const size_t        bytes = linalg::inversion<double, B>::workspace_size(n, type);
+    dbuf<unsigned char> ws(bytes);
+    dbuf<double>        dm(a.size());
+    dm.up(a);
+    linalg::inversion<double, B>::apply(dm.p, nullptr, n, type, ws.p, bytes);
+    cudaDeviceSynchronize();
+    auto   inv = dm.down();
+    double err = 0;
+    for (int i = 0; i < n; ++i)
+        for (int j = 0; j < n; ++j)
+        {
+            double s = 0;
+            for (int k = 0; k < n; ++k) s += inv[i * n + k] * a[k * n + j];
+            err = std::fmax(err, std::fabs(s - (i == j ? 1.0 : 0.0)));
+        }
+    CHECK(err <= 1e-12 * n, "inversion LU mode, null pivot: A^-1 A == I");
+
+    dm.up(a);
+    const size_t        dbytes = linalg::determinant<double, B>::workspace_size(n, type);
+    dbuf<unsigned char> dws(dbytes);
+    const double        det = linalg::determinant<double, B>::apply(dm.p, nullptr, n, type, dws.p, dbytes);
+    CHECK(det > 0.0, "determinant of an SPD matrix is positive");
+
+    dbuf<double> d2(4);
+    d2.up({4.0, 0.0, 0.0, 2.0});
+    cudaStream_t s = nullptr;
+    cudaStreamCreate(&s);
+    const double det2 = linalg::determinant<double, B>::apply(d2.p, nullptr, 2, type, dws.p, dbytes, s);
+    cudaStreamDestroy(s);
+    CHECK(det2 == 8.0, "determinant [[4,0],[0,2]] == 8");
+
+    dbuf<float> f2(4);
+    f2.up(std::vector<float>{0.0f, 1.0f, 1.0f, 0.0f});
+    const size_t        fbytes = linalg::determinant<float, B>::workspace_size(2, type);
+    dbuf<unsigned char> fws(fbytes);
+    const float fdet = linalg::determinant<float, B>::apply(f2.p, nullptr, 2, type, fws.p, fbytes);
+    CHECK(fdet == -1.0f, "determinant of a row swap is -1 (pivot sign applied)");
+
+    int threw = 0;
+    try { linalg::inversion<double, B>::apply(nullptr, nullptr, n, type, ws.p, bytes); } catch (const std::invalid_argument&) { ++threw; }
+    try { linalg::inversion<double, B>::apply(dm.p, nullptr, 0, type, ws.p, bytes); } catch (const std::invalid_argument&) { ++threw; }
+    try { linalg::inversion<double, B>::apply(dm.p, nullptr, n, (linalg::linear_solver_type)5, ws.p, bytes); } catch (const std::invalid_argument&) { ++threw; }
+    try { linalg::determinant<double, B>::apply(nullptr, nullptr, n, type, dws.p, dbytes); } catch (const std::invalid_argument&) { ++threw; }
+    CHECK(threw == 4, "inversion / determinant argument checks throw");
+}
+
 int main()
 {
     test_lu();
@@ -237,6 +298,7 @@ int main()
     test_multiplication();
     test_validation();
     test_singular_status();
+    test_inversion_determinant();
     std::printf("%s (%d failures)\n", g_fail ? "FAILED" : "ALL PASSED", g_fail);
     return g_fail ? 1 : 0;
 }

@@ -6,8 +6,10 @@ Run from the repository root, where the reference build exists:
 
     make -f oracle/Makefile && python tests/golden/make_golden.py
 
-Writes tests/golden/lu_golden.npz.  Every input is seeded (numpy PCG64) or a
-closed-form known-answer matrix; each array's name says what it is.
+Writes tests/golden/lu_golden.npz (LU, solve, triangular solver, GEMM) and
+tests/golden/inverse_golden.npz (inversion and determinant; `--inverse` writes
+only that one).  Every input is seeded (numpy PCG64) or a closed-form
+known-answer matrix; each array's name says what it is.
 """
 from __future__ import annotations
 
@@ -23,8 +25,10 @@ sys.path.insert(0, ROOT)
 
 from oracle import Oracle  # noqa: E402
 from linearalgebra_b200.workloads import (  # noqa: E402
+    determinant_known_answers,
     known_answer_matrices,
     random_matrix,
+    spd_product,
     system,
     triangular_cases,
 )
@@ -32,6 +36,8 @@ from linearalgebra_b200.workloads import (  # noqa: E402
 LU_SIZES = (1, 2, 3, 17, 63, 64, 65, 130, 200)
 
 OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "lu_golden.npz")
+OUT_INV = os.path.join(os.path.dirname(os.path.abspath(__file__)), "inverse_golden.npz")
+INV_SIZES = (1, 2, 3, 17, 64, 65, 130, 257)
 
 
 def sha(a: np.ndarray) -> str:
@@ -101,5 +107,52 @@ def main() -> None:
     print(f"wrote {OUT}: {len(out)} arrays, {os.path.getsize(OUT)} bytes")
 
 
+def inverse_main() -> None:
+    """Inversion and determinant fixtures.  The large inverses are stored as
+    SHA-256 digests of their bytes (the oracle must reproduce them bit for
+    bit); the small ones, the pivots and the determinants in full."""
+    ref = Oracle("reference")
+    out: dict[str, np.ndarray] = {}
+    for dt, npdt in (("f64", np.float64), ("f32", np.float32)):
+        # 1. seeded N(0,1) matrices, LU mode
+        for n in INV_SIZES:
+            a = random_matrix(n, seed=5000 + n, dtype=npdt)
+            inv, piv, _ = ref.getri(a, mode=1)
+            d, lu, dpiv = ref.det(a, mode=1)
+            assert np.array_equal(piv, dpiv)
+            key = f"inv_{dt}_{n}"
+            out[key + "_a_sha"] = np.array(sha(a))
+            out[key + "_inv_sha"] = np.array(sha(inv))
+            out[key + "_piv"] = piv
+            out[key + "_det"] = np.array(d)
+            out[key + "_absmax"] = np.array(np.abs(inv).max())
+            if n <= 17:
+                out[key + "_inv"] = inv
+            # LU_UPFRONT on the reference's own factors gives the same inverse
+            inv2, _, _ = ref.getri(lu, mode=2, pivot=piv)
+            assert sha(inv2) == sha(inv)
+        # 2. the reference inversion test's construction (A = R R^T), n = 3, 198
+        for n in (3, 198):
+            a = spd_product(n, seed=6000 + n, dtype=npdt)
+            inv, piv, _ = ref.getri(a, mode=1)
+            out[f"spd_{dt}_{n}_a_sha"] = np.array(sha(a))
+            out[f"spd_{dt}_{n}_inv_sha"] = np.array(sha(inv))
+            out[f"spd_{dt}_{n}_piv"] = piv
+        # 3. determinant known answers (diagonal matrices, a singular one)
+        for name, (diag, _) in determinant_known_answers().items():
+            a = np.diag(np.array(diag, dtype=npdt))
+            d, _, _ = ref.det(a, mode=1)
+            out[f"det_{name}_{dt}"] = np.array(d)
+        # 4. singular LU mode: the inverse call leaves the factors
+        a = np.array([[1, 2, 3], [2, 4, 5], [4, 8, 1]], dtype=npdt)
+        m, piv, _ = ref.getri(a, mode=1)
+        out[f"sing_{dt}_m"] = m
+        out[f"sing_{dt}_piv"] = piv
+    np.savez_compressed(OUT_INV, **out)
+    print(f"wrote {OUT_INV}: {len(out)} arrays, {os.path.getsize(OUT_INV)} bytes")
+
+
 if __name__ == "__main__":
-    main()
+    if "--inverse" not in sys.argv[1:]:
+        main()
+    inverse_main()

@@ -144,3 +144,83 @@ def test_backward_error_metric(port):
     a, x_true, b = system(64, seed=9)
     assert port.backward_error(a, x_true, b) < 4 * EPS64
     assert port.backward_error(a, x_true + 1e-6, b) > 1e-8
+
+
+# ---- inversion / determinant ------------------------------------------------
+INV_SIZES = (1, 2, 3, 17, 64, 65, 130, 257)
+INV_TYPES = [("f64", np.float64), ("f32", np.float32)]
+
+
+@pytest.mark.parametrize("n", INV_SIZES)
+@pytest.mark.parametrize("dt,npdt", INV_TYPES)
+def test_port_inverse_matches_golden_bitwise(port, inverse_golden, n, dt, npdt):
+    g = inverse_golden
+    key = f"inv_{dt}_{n}"
+    a = random_matrix(n, seed=5000 + n, dtype=npdt)
+    assert sha(a) == str(g[key + "_a_sha"])
+    inv, piv, st = port.getri(a, mode=1)
+    assert st == 0
+    assert np.array_equal(piv, g[key + "_piv"])
+    assert sha(inv) == str(g[key + "_inv_sha"])
+    if key + "_inv" in g:
+        assert np.array_equal(inv, g[key + "_inv"])
+    d, lu, dpiv = port.det(a, mode=1)
+    assert np.array_equal(dpiv, piv)
+    assert np.array_equal(np.array(d), g[key + "_det"])
+    # LU_UPFRONT on the factors: same inverse, same determinant
+    inv2, _, _ = port.getri(lu, mode=2, pivot=piv)
+    assert sha(inv2) == sha(inv)
+    d2, _, _ = port.det(lu, mode=2, pivot=piv)
+    assert np.array_equal(np.array(d2), np.array(d))
+
+
+@pytest.mark.parametrize("n", (3, 198))
+@pytest.mark.parametrize("dt,npdt", INV_TYPES)
+def test_port_inverse_spd_case(port, inverse_golden, n, dt, npdt):
+    """The reference inversion test's construction: golden bits and its
+    acceptance bound ||A^-1 A - I||_max <= 5e-12 (double) / 2e-4 (float)."""
+    from linearalgebra_b200.workloads import spd_product
+    a = spd_product(n, seed=6000 + n, dtype=npdt)
+    assert sha(a) == str(inverse_golden[f"spd_{dt}_{n}_a_sha"])
+    inv, piv, _ = port.getri(a, mode=1)
+    assert sha(inv) == str(inverse_golden[f"spd_{dt}_{n}_inv_sha"])
+    assert np.array_equal(piv, inverse_golden[f"spd_{dt}_{n}_piv"])
+    err = np.abs(inv.astype(np.float64) @ a.astype(np.float64) - np.eye(n)).max()
+    assert err <= (5e-12 if npdt == np.float64 else 2e-4)
+
+
+@pytest.mark.parametrize("dt,npdt", INV_TYPES)
+def test_port_determinant_known_answers(port, inverse_golden, dt, npdt):
+    from linearalgebra_b200.workloads import determinant_known_answers
+    for name, (diag, expected) in determinant_known_answers().items():
+        d, _, _ = port.det(np.diag(np.array(diag, dtype=npdt)), mode=1)
+        assert d == expected, name
+        assert np.array_equal(np.array(d), inverse_golden[f"det_{name}_{dt}"]), name
+
+
+@pytest.mark.parametrize("dt,npdt", INV_TYPES)
+def test_port_singular_inverse_leaves_factors(port, inverse_golden, dt, npdt):
+    a = np.array([[1, 2, 3], [2, 4, 5], [4, 8, 1]], dtype=npdt)
+    m, piv, st = port.getri(a, mode=1)
+    assert st == 2
+    assert np.array_equal(m, inverse_golden[f"sing_{dt}_m"])
+    assert np.array_equal(piv, inverse_golden[f"sing_{dt}_piv"])
+    lu, lpiv, _ = port.getrf(a)
+    assert np.array_equal(m, lu) and np.array_equal(piv, lpiv)
+
+
+def test_port_inverse_rejects_bad_mode(port):
+    with pytest.raises(ValueError):
+        port.getri(np.eye(3), mode=5)
+    with pytest.raises(ValueError):
+        port.det(np.eye(3), mode=3)
+
+
+@pytest.mark.skipif(not os.path.exists(REF_LIB), reason="reference build not present")
+@pytest.mark.parametrize("n", [5, 66, 129])
+def test_port_inverse_equals_reference_build(port, n):
+    ref = Oracle("reference")
+    for npdt in (np.float64, np.float32):
+        a = random_matrix(n, seed=88 + n, dtype=npdt)
+        assert sha(port.getri(a)[0]) == sha(ref.getri(a)[0])
+        assert np.array_equal(np.array(port.det(a)[0]), np.array(ref.det(a)[0]))
