@@ -56,6 +56,8 @@ def parse():
     p.add_argument("--precision", choices=["fp32", "tf32", "bf16", "fp16"], default="fp32")
     p.add_argument("--batch-count", type=int, default=20000)
     p.add_argument("--no-batched", action="store_true")
+    p.add_argument("--inv-n", type=int, default=16384, help="order of the inversion / determinant measurement")
+    p.add_argument("--no-inversion", action="store_true")
     return p.parse_args()
 
 
@@ -180,6 +182,176 @@ def measured_peaks() -> dict:
                 "source": "measured (MEASURED_PEAKS.json)"}
     return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "source": "fallback"}
 
+# ---------------------------------------------------------------------------
+# inversion / determinant (LU modes): this library vs the reference's
+# CUDA_BLAS path (baseline/_ref) at the same order
+# ---------------------------------------------------------------------------
+def inversion_gemm_flops(n: int, nb: int = 256, sub: int = 64) -> int:
+    """Flops of the inversion's GEMM updates (k_dmma_update launches) for
+    order n: the block-row sub-updates and the big forward / backward ones."""
+    fl = 0
+    for b0 in range(0, n, nb):
+        bw = min(nb, n - b0)
+        k1 = b0 + bw
+        for phase_cols in (k1, n):  # forward block row: k1 columns; backward: n
+            for r0 in range(0, bw, sub):
+                sw = min(sub, bw - r0)
+                rows_left = bw - r0 - sw  # rows of the block still to update
+                fl += 2 * rows_left * phase_cols * sw
+        if k1 < n:
+            fl += 2 * (n - k1) * k1 * bw  # forward: rows below, columns [0, k1)
+        if b0 > 0:
+            fl += 2 * b0 * n * bw  # backward: rows above, all columns
+    return fl
+
+
+def cuda_blas_inverse(lib_path, A, stream, steps):
+    import torch
+    lib = ctypes.CDLL(lib_path)
+    lib.ref_cublas_dinverse_workspace_size.restype = ctypes.c_size_t
+    lib.ref_cublas_dinverse_workspace_size.argtypes = [ctypes.c_int64]
+    lib.ref_cublas_dinverse.argtypes = [ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_size_t,
+                                        ctypes.c_void_p]
+    lib.ref_cublas_ddeterminant_workspace_size.restype = ctypes.c_size_t
+    lib.ref_cublas_ddeterminant_workspace_size.argtypes = [ctypes.c_int64]
+    lib.ref_cublas_ddeterminant.argtypes = [ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p,
+                                            ctypes.c_size_t, ctypes.c_void_p]
+    lib.ref_cublas_last_error.restype = ctypes.c_char_p
+    n = A.shape[0]
+    nb = int(lib.ref_cublas_dinverse_workspace_size(n))
+    ws = torch.empty(max(nb, 256), dtype=torch.uint8, device=A.device)
+    m = torch.empty_like(A)
+
+    def inv_step():
+        m.copy_(A)
+        if lib.ref_cublas_dinverse(m.data_ptr(), n, ws.data_ptr(), nb, stream.cuda_stream) != 0:
+            raise RuntimeError(lib.ref_cublas_last_error().decode())
+
+    inv_step()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        inv_step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    t_inv = e0.elapsed_time(e1) / steps / 1e3
+    res = (torch.mm(A, m) - torch.eye(n, dtype=A.dtype, device=A.device)).abs().max().item()
+    del ws
+    db = int(lib.ref_cublas_ddeterminant_workspace_size(n))
+    dws = torch.empty(max(db, 256), dtype=torch.uint8, device=A.device)
+    out = ctypes.c_double(0)
+    m.copy_(A)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    if lib.ref_cublas_ddeterminant(m.data_ptr(), n, ctypes.addressof(out), dws.data_ptr(), db,
+                                   stream.cuda_stream) != 0:
+        raise RuntimeError(lib.ref_cublas_last_error().decode())
+    t_det = time.perf_counter() - t0
+    del m, dws
+    torch.cuda.empty_cache()
+    return {"inverse_s": t_inv, "inverse_residual": res, "determinant_s": t_det, "steps": steps,
+            "what": "the reference's inversion / determinant<double,CUDA_BLAS> LU mode (cuSOLVER getrf, getrs "
+                    "against the identity, the reference's transposes; determinant host-synchronous)"}
+
+
+def run_inversion(args, world, rank, local):
+    """inversion / determinant<double, B200> LU mode at order args.inv_n:
+    each step restores m from A (device copy), factors and inverts in place."""
+    import torch
+
+    import linearalgebra_b200 as la
+    from linearalgebra_b200 import _lib
+
+    lib = _lib.load()
+    n = args.inv_n
+    dev = torch.device("cuda", local)
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(SEED + 1 + rank)
+    A = torch.randn(n, n, dtype=torch.float64, device=dev, generator=gen)
+    m = torch.empty_like(A)
+    piv = torch.empty(n, dtype=torch.int64, device=dev)
+    nbytes = la.inversion.workspace_size(n, la.LU_LINEAR_SOLVER)
+    ws = torch.empty(nbytes, dtype=torch.uint8, device=dev)
+    stream = torch.cuda.current_stream(dev)
+
+    def step():
+        m.copy_(A)
+        la.inversion.apply(m, piv, n, la.LU_LINEAR_SOLVER, ws, nbytes, stream)
+
+    steps = 2
+    step()
+    torch.cuda.synchronize()
+    lib.b200la_profile_start(sum(1 << c for c in CLASS_NAMES))
+    step()
+    torch.cuda.synchronize()
+    breakdown = {}
+    for c, name in CLASS_NAMES.items():
+        t_ms, cnt = ctypes.c_double(0), ctypes.c_int64(0)
+        lib.b200la_profile_stop(c, ctypes.addressof(t_ms), ctypes.addressof(cnt))
+        if cnt.value:
+            breakdown[name] = {"ms": round(t_ms.value, 3), "launches": int(cnt.value)}
+    lib.b200la_profile_start(1 << 10)
+    barrier(world)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier(world)
+    k_ms, k_n = ctypes.c_double(0), ctypes.c_int64(0)
+    lib.b200la_profile_stop(10, ctypes.addressof(k_ms), ctypes.addressof(k_n))
+    t_inv = max_over_ranks(world, e0.elapsed_time(e1) / steps) / 1e3
+    res = (torch.mm(A, m) - torch.eye(n, dtype=A.dtype, device=dev)).abs().max().item()
+    xnorm = torch.linalg.matrix_norm(m, ord=float("inf")).item()
+    anorm = torch.linalg.matrix_norm(A, ord=float("inf")).item()
+    gflops = inversion_gemm_flops(n)
+    peak = measured_fp64_peak_tflops()
+    achieved = gflops * steps / (k_ms.value * 1e-3) / 1e12 if k_ms.value else None
+
+    # determinant, LU mode (factor + diagonal product), host-synchronous
+    m.copy_(A)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    d = la.det(m, piv)
+    t_det = time.perf_counter() - t0
+
+    out = {"n": n, "inverse_s": t_inv, "steps": steps,
+           "residual_max_abs_AX_minus_I": res,
+           "residual_bound_2n_eps_normA_normX": 2 * n * EPS64 * anorm * xnorm,
+           "determinant_s": t_det, "log_abs_det": d["log_abs"], "det_sign": d["sign"],
+           "roofline": {"kernel": "inversion_gemm (k_dmma_update, DMMA m8n8k4)", "bound": "fp64",
+                        "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                        "frac": achieved / peak if achieved else None,
+                        "peak_source": "cuBLAS DGEMM 8192^3 via torch.matmul, best of 5, measured in this run",
+                        "flops_per_step": gflops, "launches": int(k_n.value),
+                        "share_of_step": (k_ms.value / steps / 1e3) / t_inv if t_inv else None},
+           "breakdown_one_step": breakdown}
+    del m, ws
+    torch.cuda.empty_cache()
+    path = os.path.join(ROOT, "baseline", "_ref", "libref_cublas.so")
+    if rank == 0 and world == 1 and os.path.exists(path):
+        out["cuda_blas"] = cuda_blas_inverse(path, A, stream, steps)
+        out["speedup_vs_cuda_blas"] = out["cuda_blas"]["inverse_s"] / t_inv
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        import numpy as np
+        from oracle import Oracle, available
+        kind = "reference" if available("reference") else "port"
+        o = Oracle(kind)
+        ns = 768
+        a = np.random.default_rng(ns).standard_normal((ns, ns))
+        t0 = time.perf_counter()
+        o.getri(a)
+        t = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": t * (n / ns) ** 3, "unit": "s", "cores": 1, "kind": kind,
+                               "sample": f"inversion<double,NATIVE> LU mode at n={ns} ({t:.2f} s) scaled by "
+                                         f"(n/{ns})^3 to n={n}; 1 thread"}
+    del A
+    torch.cuda.empty_cache()
+    return out
+
 
 # ---------------------------------------------------------------------------
 # CPU: the reference's own NATIVE linear_solver (oracle/_ref), single thread
@@ -269,13 +441,15 @@ def cusolver_reference_seconds(A, b, stream, steps: int = 2):
 # DRAM bytes (ncu dram__bytes_read.sum + dram__bytes_write.sum) per algorithmic
 # byte of the dominant kernels, from one capture each on a smaller case
 # (profiles/): the tensor-core update at n=8192 (M=6400, N=6144 launch:
-# 287.2 of 314.6 MB) and the FP64 trailing update at n=8192 (rest=7488:
-# 846.6 of 897.1 MB).  Traffic grows with the C tile bytes, so it scales to
-# a full launch by the algorithmic bytes.
-TRAFFIC_PER_ALGORITHMIC_BYTE = {5: 0.913, 2: 0.944}
+# 287.2 of 314.6 MB) and the FP64 trailing update (DMMA band kernel) at
+# n=4096 (rest=3712: 168.8 of 220.5 MB; the rest of the writes were still
+# in L2 when the launch ended).  Traffic grows with the C tile bytes, so it
+# scales to a full launch by the algorithmic bytes.
+TRAFFIC_PER_ALGORITHMIC_BYTE = {5: 0.913, 2: 0.766}
 
-CLASS_NAMES = {0: "panel", 1: "laswp_u12", 2: "trailing_simt", 3: "solve", 4: "gemm", 5: "tc_update",
-               6: "residual", 7: "batched", 8: "operand_prep", 9: "selector"}
+CLASS_NAMES = {0: "panel", 1: "laswp_u12", 2: "trailing", 3: "solve", 4: "gemm", 5: "tc_update",
+               6: "residual", 7: "batched", 8: "operand_prep", 9: "selector", 10: "inversion_gemm",
+               11: "inversion_aux"}
 
 
 def algorithmic_work(n: int, method: str, nb_out: int = 256):
@@ -558,6 +732,13 @@ def run_b200(args, world, rank, local):
         torch.cuda.empty_cache()
         batched = run_batched(args, world, rank, local)
 
+    inversion = None
+    if not args.no_inversion:
+        if batched is None:
+            del m, xf, ws
+            torch.cuda.empty_cache()
+        inversion = run_inversion(args, world, rank, local)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         kind, t, ceta = cpu_reference_solve_seconds(CPU_SAMPLE_N)
@@ -605,6 +786,7 @@ def run_b200(args, world, rank, local):
             "gpu_launches": int(launches),
             "breakdown_one_step": breakdown,
             "batched": batched,
+            "inversion": inversion,
             "clocks": clk,
             "peaks": peaks,
         }

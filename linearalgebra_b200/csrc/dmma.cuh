@@ -69,26 +69,57 @@ __device__ __forceinline__ void dm_piece(double* s, const double* g, const doubl
     cp_async8(s + 1, valid > 1 ? g + 1 : safe, valid > 1);
 }
 
-__device__ __forceinline__ void dm_load_stage(double* sa, double* sb, const double* A, int64_t lda,
-    const double* B, int64_t ldb, int M, int N, int K, int m0, int n0, int k0, bool vec16)
+// A thread's share of one stage: pieces i < 4 of the A tile (row tid/16 +
+// 32 i, columns 2 (tid%16) .. +1 of the stage) and of the B tile (row
+// tid/64 + 8 i, columns 2 (tid%64) .. +1).  Addresses are formed once per
+// tile; a stage only advances them by its depth.
+struct DmLoader
 {
-    constexpr int APR = kDmKC / 2;    // pieces per A row
-    constexpr int BPR = kDmTile / 2;  // pieces per B row
+    const double* a;     // A row tid/16 of the tile, column 2 (tid%16)
+    const double* b;     // B row tid/64, column n0 + 2 (tid%64)
+    int           acol;  // 2 (tid%16)
+    int           arows; // bit i: A row tid/16 + 32 i is inside M
+    int           bcols; // valid columns of the B piece (0..2)
+    int           brow;  // tid/64
+};
+
+__device__ __forceinline__ DmLoader dm_loader(const double* A, int64_t lda, const double* B, int64_t ldb, int M,
+    int N, int m0, int n0)
+{
+    DmLoader  L;
+    const int ra = threadIdx.x >> 4, qa = threadIdx.x & 15;
+    const int rb = threadIdx.x >> 6, qb = threadIdx.x & 63;
+    L.acol  = 2 * qa;
+    L.a     = A + (int64_t)(m0 + ra) * lda + L.acol;
+    L.arows = 0;
 #pragma unroll
-    for (int e = threadIdx.x; e < kDmTile * APR; e += kDmThreads)
+    for (int i = 0; i < 4; ++i)
     {
-        const int r = e / APR, q = e - (e / APR) * APR;
-        const int row = m0 + r, col = k0 + 2 * q;
-        const int valid = row < M ? min(2, K - col) : 0;
-        dm_piece(sa + r * kDmLDA + 2 * q, valid > 0 ? A + (int64_t)row * lda + col : A, A, valid, vec16);
+        L.arows |= (m0 + ra + 32 * i < M) ? (1 << i) : 0;
     }
-#pragma unroll
-    for (int e = threadIdx.x; e < kDmKC * BPR; e += kDmThreads)
+    L.brow  = rb;
+    L.bcols = max(0, min(2, N - (n0 + 2 * qb)));
+    L.b     = B + (int64_t)rb * ldb + n0 + 2 * qb;
+    return L;
+}
+
+// Issue piece `i` (0..3: A, 4..7: B) of the stage at depth k0 into slot `st`.
+__device__ __forceinline__ void dm_issue(const DmLoader& L, double* st, int i, const double* A, int64_t lda,
+    const double* B, int64_t ldb, int K, int k0, bool vec16)
+{
+    if (i < 4)
     {
-        const int p = e / BPR, q = e - (e / BPR) * BPR;
-        const int row = k0 + p, col = n0 + 2 * q;
-        const int valid = row < K ? min(2, N - col) : 0;
-        dm_piece(sb + p * kDmLDB + 2 * q, valid > 0 ? B + (int64_t)row * ldb + col : B, B, valid, vec16);
+        const int  valid = (L.arows >> i) & 1 ? min(2, K - (k0 + L.acol)) : 0;
+        const int  r     = (threadIdx.x >> 4) + 32 * i;
+        dm_piece(st + r * kDmLDA + L.acol, L.a + (int64_t)(32 * i) * lda + k0, A, valid, vec16);
+    }
+    else
+    {
+        const int i4    = i - 4;
+        const int p     = L.brow + 8 * i4;
+        const int valid = k0 + p < K ? L.bcols : 0;
+        dm_piece(st + kDmAElems + p * kDmLDB + 2 * (threadIdx.x & 63), L.b + (int64_t)(k0 + 8 * i4) * ldb, B,
+            valid, vec16);
     }
 }
 
@@ -173,13 +204,17 @@ __global__ void __launch_bounds__(kDmThreads, 1) k_dmma_update(int M, int N, int
         }
     }
 
+    const DmLoader L = dm_loader(A, lda, B, ldb, M, N, m0, n0);
 #pragma unroll
     for (int s = 0; s < kDmStages - 1; ++s)
     {
         if (s < nchunks)
         {
-            double* sa = smem + s * kDmStage;
-            dm_load_stage(sa, sa + kDmAElems, A, lda, B, ldb, M, N, K, m0, n0, s * kDmKC, v16);
+#pragma unroll
+            for (int i = 0; i < 8; ++i)
+            {
+                dm_issue(L, smem + s * kDmStage, i, A, lda, B, ldb, K, s * kDmKC, v16);
+            }
         }
         cp_async_commit();
     }
@@ -187,18 +222,18 @@ __global__ void __launch_bounds__(kDmThreads, 1) k_dmma_update(int M, int N, int
     {
         cp_async_wait<kDmStages - 2>();
         __syncthreads();  // stage c landed for every thread; stage c-1 is free
-        const int pf = c + kDmStages - 1;
-        if (pf < nchunks)
-        {
-            double* sa = smem + (pf % kDmStages) * kDmStage;
-            dm_load_stage(sa, sa + kDmAElems, A, lda, B, ldb, M, N, K, m0, n0, pf * kDmKC, v16);
-        }
-        cp_async_commit();
-        const double* sa = smem + (c % kDmStages) * kDmStage + (wm + g) * kDmLDA + t;
-        const double* sb = smem + (c % kDmStages) * kDmStage + kDmAElems + t * kDmLDB + wn + g;
+        const int     pf   = c + kDmStages - 1;
+        double*       dst  = smem + (pf % kDmStages) * kDmStage;
+        const double* sa   = smem + (c % kDmStages) * kDmStage + (wm + g) * kDmLDA + t;
+        const double* sb   = smem + (c % kDmStages) * kDmStage + kDmAElems + t * kDmLDB + wn + g;
 #pragma unroll
         for (int ks = 0; ks < kDmKC / 4; ++ks)
         {
+            // one piece of stage pf per depth step, spread over the chunk
+            if (pf < nchunks)
+            {
+                dm_issue(L, dst, ks, A, lda, B, ldb, K, pf * kDmKC, v16);
+            }
             double af[4], bf[4];
 #pragma unroll
             for (int i = 0; i < 4; ++i)
@@ -220,6 +255,7 @@ __global__ void __launch_bounds__(kDmThreads, 1) k_dmma_update(int M, int N, int
                 }
             }
         }
+        cp_async_commit();
     }
     cp_async_wait<0>();
 
@@ -300,6 +336,200 @@ __global__ void __launch_bounds__(kDmThreads, 1) k_dmma_update(int M, int N, int
             }
         }
     }
+}
+
+// The LU trailing update A22 -= L21 U12 (panel depth K <= kBandK) as a
+// band kernel, bit-identical to k_dmma_update<true>: the CTA keeps its
+// kDmTile x K slice of L21 resident in shared memory and walks `tiles`
+// consecutive kDmTile-column tiles of U12 / A22, computing tile j while
+// tile j+1's U12 slice lands in the other buffer and its A22 rows are pulled
+// into L2.  Per tile: delta from zero over k in order, then A22 - delta.
+constexpr int    kBandK      = 64;
+constexpr int    kBandLDA    = kBandK + 4;
+constexpr int    kBandAElems = kDmTile * kBandLDA;
+constexpr int    kBandBElems = kBandK * kDmLDB;
+constexpr size_t kBandSmem   = sizeof(double) * ((size_t)kBandAElems + 2 * (size_t)kBandBElems);
+
+__device__ __forceinline__ void band_load_b(double* sb, const double* B, int64_t ldb, int N, int K, int n0, bool vec16)
+{
+    constexpr int BPR = kDmTile / 2;
+#pragma unroll
+    for (int e = threadIdx.x; e < kBandK * BPR; e += kDmThreads)
+    {
+        const int p = e / BPR, q = e - (e / BPR) * BPR;
+        const int col = n0 + 2 * q;
+        const int valid = p < K ? min(2, N - col) : 0;
+        dm_piece(sb + p * kDmLDB + 2 * q, valid > 0 ? B + (int64_t)p * ldb + col : B, B, valid, vec16);
+    }
+}
+
+__device__ __forceinline__ void band_prefetch_c(const double* C, int64_t ldc, int M, int N, int m0, int n0)
+{
+    const int r = threadIdx.x >> 2, q = threadIdx.x & 3;
+    if (m0 + r < M)
+    {
+        const double* crow = C + (int64_t)(m0 + r) * ldc + n0;
+#pragma unroll
+        for (int h = 0; h < 2; ++h)
+        {
+            const int c = (q + 4 * h) * 16;
+            if (n0 + c < N)
+            {
+                asm volatile("prefetch.global.L2 [%0];" ::"l"(crow + c));
+            }
+        }
+    }
+}
+
+template <int Unused = 0>
+__global__ void __launch_bounds__(kDmThreads, 1) k_dmma_band(int M, int N, int K, const double* __restrict__ A,
+    int64_t lda, const double* __restrict__ B, int64_t ldb, double* __restrict__ C, int64_t ldc, int tiles,
+    int vec16)
+{
+    extern __shared__ __align__(16) unsigned char dm_smem[];
+    double*    sa    = reinterpret_cast<double*>(dm_smem);
+    double*    sbuf  = sa + kBandAElems;
+    const int  m0    = blockIdx.y * kDmTile;
+    const int  nt0   = blockIdx.x * tiles;  // first column tile
+    const int  ntile = (N + kDmTile - 1) / kDmTile;
+    const int  nend  = min(ntile, nt0 + tiles);
+    const int  warp  = threadIdx.x >> 5;
+    const int  lane  = threadIdx.x & 31;
+    const int  g     = lane >> 2;
+    const int  t     = lane & 3;
+    const int  wm    = (warp >> 2) * 32;
+    const int  wn    = (warp & 3) * 32;
+    const bool v16   = vec16 != 0;
+    if (nt0 >= nend)
+    {
+        return;
+    }
+
+    // L21 slice (kDmTile x K, zero-filled past M and K) and the first U12 tile
+    {
+        constexpr int APR = kBandK / 2;
+#pragma unroll
+        for (int e = threadIdx.x; e < kDmTile * APR; e += kDmThreads)
+        {
+            const int r = e / APR, q = e - (e / APR) * APR;
+            const int row = m0 + r, col = 2 * q;
+            const int valid = row < M ? min(2, K - col) : 0;
+            dm_piece(sa + r * kBandLDA + col, valid > 0 ? A + (int64_t)row * lda + col : A, A, valid, v16);
+        }
+    }
+    band_load_b(sbuf, B, ldb, N, K, nt0 * kDmTile, v16);
+    cp_async_commit();
+    band_prefetch_c(C, ldc, M, N, m0, nt0 * kDmTile);
+
+    for (int nt = nt0; nt < nend; ++nt)
+    {
+        const int n0  = nt * kDmTile;
+        const int cur = (nt - nt0) & 1;
+        cp_async_wait<0>();
+        __syncthreads();  // this tile's U12 landed; the other buffer is free
+        if (nt + 1 < nend)
+        {
+            band_load_b(sbuf + (cur ^ 1) * kBandBElems, B, ldb, N, K, n0 + kDmTile, v16);
+            band_prefetch_c(C, ldc, M, N, m0, n0 + kDmTile);
+        }
+        cp_async_commit();
+
+        double acc[4][4][2];
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+        {
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+            {
+                acc[i][j][0] = 0.0;
+                acc[i][j][1] = 0.0;
+            }
+        }
+        const double* fa = sa + (wm + g) * kBandLDA + t;
+        const double* fb = sbuf + cur * kBandBElems + t * kDmLDB + wn + g;
+#pragma unroll 4
+        for (int ks = 0; ks < kBandK / 4; ++ks)
+        {
+            double af[4], bf[4];
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+            {
+                af[i] = fa[8 * i * kBandLDA + 4 * ks];
+            }
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+            {
+                bf[j] = fb[4 * ks * kDmLDB + 8 * j];
+            }
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+            {
+#pragma unroll
+                for (int j = 0; j < 4; ++j)
+                {
+                    dmma_884(acc[i][j][0], acc[i][j][1], af[i], bf[j]);
+                }
+            }
+        }
+
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+        {
+            const int row = m0 + wm + 8 * i + g;
+            if (row >= M)
+            {
+                continue;
+            }
+            double* crow = C + (int64_t)row * ldc;
+            double2 cv[4];
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+            {
+                const int col = n0 + wn + 8 * j + 2 * t;
+                if (v16 && col + 1 < N)
+                {
+                    cv[j] = *reinterpret_cast<const double2*>(crow + col);
+                }
+                else
+                {
+                    cv[j].x = col < N ? crow[col] : 0.0;
+                    cv[j].y = col + 1 < N ? crow[col + 1] : 0.0;
+                }
+            }
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+            {
+                const int col = n0 + wn + 8 * j + 2 * t;
+                cv[j].x       = cv[j].x - acc[i][j][0];
+                cv[j].y       = cv[j].y - acc[i][j][1];
+                if (v16 && col + 1 < N)
+                {
+                    *reinterpret_cast<double2*>(crow + col) = cv[j];
+                }
+                else
+                {
+                    if (col < N)
+                    {
+                        crow[col] = cv[j].x;
+                    }
+                    if (col + 1 < N)
+                    {
+                        crow[col + 1] = cv[j].y;
+                    }
+                }
+            }
+        }
+    }
+    cp_async_wait<0>();
+}
+
+// Column tiles per CTA for k_dmma_band: as many as keep at least two waves
+// of CTAs over the SMs, at most 8.
+inline int band_tiles_per_cta(int rows, int cols, int sms)
+{
+    const int rt = (rows + kDmTile - 1) / kDmTile, ct = (cols + kDmTile - 1) / kDmTile;
+    const int per = (rt * ct) / (2 * (sms > 0 ? sms : 148));
+    return per < 1 ? 1 : (per > 8 ? 8 : per);
 }
 
 inline bool dm_aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; }

@@ -87,6 +87,7 @@ template <typename T> int ensure_kernel_attributes()
         k_dmma_update<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDmSmem));
     B200LA_CUDA(cudaFuncSetAttribute(
         k_dmma_update<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDmSmem));
+    B200LA_CUDA(cudaFuncSetAttribute(k_dmma_band<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBandSmem));
     B200LA_CUDA(cudaFuncSetAttribute(k_gemm<T, false, false>,
         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gemm_smem_bytes<T>()));
     B200LA_CUDA(cudaFuncSetAttribute(k_gemm<T, true, false>,
@@ -311,9 +312,12 @@ int enqueue_getrf(T* m, int n, int64_t* pivot, const GetrfPlan<T>& p, cudaStream
                 const double* l21 = m + (int64_t)(k + w) * n + k;
                 const double* u12 = m + (int64_t)k * n + k + w;
                 double*       a22 = m + (int64_t)(k + w) * n + k + w;
-                const dim3    grid((rest + kDmTile - 1) / kDmTile, (rest + kDmTile - 1) / kDmTile);
-                k_dmma_update<true><<<grid, kDmThreads, kDmSmem, s>>>(
-                    rest, rest, w, l21, n, u12, n, a22, n, dm_vec16(l21, n, u12, n, a22, n), nullptr);
+                static_assert(kNB <= kBandK, "the band kernel holds one panel's L21 slice");
+                const int     tpc = band_tiles_per_cta(rest, rest, device_sm_count());
+                const int     ct  = (rest + kDmTile - 1) / kDmTile;
+                const dim3    grid((ct + tpc - 1) / tpc, (rest + kDmTile - 1) / kDmTile);
+                k_dmma_band<0><<<grid, kDmThreads, kBandSmem, s>>>(
+                    rest, rest, w, l21, n, u12, n, a22, n, tpc, dm_vec16(l21, n, u12, n, a22, n));
             }
             else
             {

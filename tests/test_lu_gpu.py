@@ -90,6 +90,41 @@ def test_lu_grid_panel_path_bitwise(port, monkeypatch, n):
     assert np.array_equal(lu, lu_o)
 
 
+def wide_exponent_matrix(n, seed, kind):
+    """N(0,1) entries scaled by 2^e with e spread over most of the FP64
+    range: 'wide' (|e| <= 900, products over- and underflow), 'subnormal'
+    (a tenth of the entries scaled into the subnormal range), 'zeros' (a
+    third exact zeros, some -0)."""
+    rng = np.random.default_rng(seed)
+    a = rng.standard_normal((n, n))
+    if kind == "wide":
+        a *= np.exp2(rng.integers(-900, 900, size=(n, n)).astype(np.float64))
+    elif kind == "subnormal":
+        mask = rng.random((n, n)) < 0.1
+        a[mask] *= 2.0 ** -1060
+    else:
+        mask = rng.random((n, n))
+        a[mask < 0.33] = 0.0
+        a[(mask >= 0.33) & (mask < 0.4)] = -0.0
+        a += np.eye(n)
+    return a
+
+
+@pytest.mark.parametrize("kind", ["wide", "subnormal", "zeros"])
+def test_lu_bitwise_special_values(port, kind):
+    """The FP64 trailing update runs on the FP64 tensor cores (DMMA chains,
+    delta from zero in k order): its bits must equal the reference's fma loop
+    also where products overflow, underflow into subnormals, or vanish."""
+    n = 450
+    a = wide_exponent_matrix(n, seed=99, kind=kind)
+    lu_o, piv_o, info_o = port.getrf(a)
+    lu, piv, info = gpu_getrf(a)
+    assert info == info_o
+    assert np.array_equal(piv, piv_o)
+    same = (lu.view(np.uint64) == lu_o.view(np.uint64)) | (np.isnan(lu) & np.isnan(lu_o))
+    assert same.all(), int((~same).sum())
+
+
 def test_lu_float32_bitwise_vs_oracle(port):
     a = random_matrix(700, seed=11, dtype=np.float32)
     lu_o, piv_o, _ = port.getrf(a)
