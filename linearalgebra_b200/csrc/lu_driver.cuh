@@ -19,6 +19,7 @@ namespace b200la
 int require_sm100();
 
 constexpr size_t kPanelSmemMax = 200 * 1024;
+constexpr int    kLeanPanelCtas = 48;  // grid panel CTAs beside a concurrent trailing update
 
 
 // Cluster size usable by k_panel_cluster on each device (0: none).
@@ -179,7 +180,7 @@ inline int grid_1d(int64_t total, int threads)
 // its rows fit there (cl > 0), else with the grid-wide kernel.
 template <typename T>
 int launch_panel(T* m, int n, int k, int w, int64_t* pivot, const GetrfPlan<T>& p, int cl, int gmax,
-    cudaStream_t s)
+    cudaStream_t s, bool lean = false)
 {
     const int R = n - k;
     PanelWs<T> ws{p.hdr, p.payload, p.diag, p.perm};
@@ -212,6 +213,15 @@ int launch_panel(T* m, int n, int k, int w, int64_t* pivot, const GetrfPlan<T>& 
         }
         {
         int       G   = (R + 15) / 16;
+        if (lean)
+        {
+            // beside a concurrent trailing update: the fewest CTAs that hold
+            // the panel in shared memory (at least kLeanPanelCtas), so the
+            // update keeps the other SMs
+            const int rows_fit = (int)(kPanelSmemMax / (panel_ldl<T>() * sizeof(T)));
+            const int g_fit    = (R + rows_fit - 1) / rows_fit;
+            G                  = G < kLeanPanelCtas ? G : (g_fit > kLeanPanelCtas ? g_fit : kLeanPanelCtas);
+        }
         G             = G < 1 ? 1 : (G > gmax ? gmax : G);
         int rpc       = (R + G - 1) / G;
         G             = (R + rpc - 1) / rpc;
@@ -260,6 +270,82 @@ template <typename T> int clear_panel_exchange(const GetrfPlan<T>& p, cudaStream
     return B200LA_SUCCESS;
 }
 
+// The high-priority stream the next panel runs on while the current
+// trailing update finishes (one per device, created on first use).
+inline cudaStream_t panel_side_stream(int* rc)
+{
+    static std::mutex   mu;
+    static cudaStream_t streams[64] = {};
+    int                 dev         = 0;
+    *rc                             = B200LA_SUCCESS;
+    cudaError_t e                   = cudaGetDevice(&dev);
+    if (e != cudaSuccess)
+    {
+        *rc = cuda_check(e, "cudaGetDevice");
+        return nullptr;
+    }
+    if (dev < 0 || dev >= 64)
+    {
+        *rc = set_error(B200LA_NOT_SUPPORTED, "device index %d out of range", dev);
+        return nullptr;
+    }
+    std::lock_guard<std::mutex> lock(mu);
+    if (streams[dev] == nullptr)
+    {
+        int least = 0, greatest = 0;
+        cudaDeviceGetStreamPriorityRange(&least, &greatest);
+        e = cudaStreamCreateWithPriority(&streams[dev], cudaStreamNonBlocking, greatest);
+        if (e != cudaSuccess)
+        {
+            streams[dev] = nullptr;
+            *rc          = cuda_check(e, "cudaStreamCreateWithPriority");
+            return nullptr;
+        }
+    }
+    return streams[dev];
+}
+
+// B200LA_LU_LOOKAHEAD=0 turns the look-ahead off (used to check that it
+// leaves every bit unchanged).
+inline bool lu_lookahead_enabled()
+{
+    const char* e = getenv("B200LA_LU_LOOKAHEAD");
+    return !(e != nullptr && e[0] == '0');
+}
+
+// Trailing update A22[:, c0:c1] -= L21 U12[:, c0:c1] of panel (k, w); the
+// columns c0, c1 are relative to the first trailing column k + w.
+template <typename T>
+int launch_trailing(T* m, int n, int k, int w, int c0, int c1, cudaStream_t s)
+{
+    const int rest = n - k - w;
+    prof_begin(KC_TRAILING, s);
+    if constexpr (sizeof(T) == 8)
+    {
+        // A22 -= L21 U12 on the tensor cores, delta from zero then
+        // subtracted: the same bits as k_trailing's fma loop.
+        static_assert(kNB <= kBandK, "the band kernel holds one panel's L21 slice");
+        const double* l21 = m + (int64_t)(k + w) * n + k;
+        const double* u12 = m + (int64_t)k * n + k + w + c0;
+        double*       a22 = m + (int64_t)(k + w) * n + k + w + c0;
+        const int     nc  = c1 - c0;
+        const int     tpc = band_tiles_per_cta(rest, nc, device_sm_count());
+        const int     ct  = (nc + kDmTile - 1) / kDmTile;
+        const dim3    grid((ct + tpc - 1) / tpc, (rest + kDmTile - 1) / kDmTile);
+        k_dmma_band<0><<<grid, kDmThreads, kBandSmem, s>>>(
+            rest, nc, w, l21, n, u12, n, a22, n, tpc, dm_vec16(l21, n, u12, n, a22, n));
+    }
+    else
+    {
+        // k_trailing covers columns [0, ncols) of A22; only whole updates here
+        dim3 grid((c1 + kChunkN - 1) / kChunkN, (rest + kBandM - 1) / kBandM);
+        k_trailing<T><<<grid, 128, trailing_smem_bytes<T>(), s>>>(m, n, k, w, c1);
+    }
+    prof_end(KC_TRAILING, s);
+    B200LA_LAUNCH_CHECK();
+    return B200LA_SUCCESS;
+}
+
 template <typename T>
 int enqueue_getrf(T* m, int n, int64_t* pivot, const GetrfPlan<T>& p, cudaStream_t s)
 {
@@ -282,16 +368,47 @@ int enqueue_getrf(T* m, int n, int64_t* pivot, const GetrfPlan<T>& p, cudaStream
             return rc;
         }
     }
+    // Look-ahead (FP64): after panel k's interchanges and U12, the trailing
+    // update of the next panel's columns runs first; panel k+1 then factors
+    // on the side stream while the rest of the update runs here.  Every
+    // element sees the same operations in the same order as without it.
+    const bool   ahead = sizeof(T) == 8 && lu_lookahead_enabled() && n > 2 * kNB;
+    cudaStream_t side  = nullptr;
+    cudaEvent_t  ev_cols = nullptr, ev_panel = nullptr;
+    if (ahead)
+    {
+        int rc = B200LA_SUCCESS;
+        side   = panel_side_stream(&rc);
+        if (rc != B200LA_SUCCESS)
+        {
+            return rc;
+        }
+        B200LA_CUDA(cudaEventCreateWithFlags(&ev_cols, cudaEventDisableTiming));
+        B200LA_CUDA(cudaEventCreateWithFlags(&ev_panel, cudaEventDisableTiming));
+    }
+    struct EventGuard
+    {
+        cudaEvent_t a, b;
+        ~EventGuard()
+        {
+            if (a)
+                cudaEventDestroy(a);
+            if (b)
+                cudaEventDestroy(b);
+        }
+    } guard{ev_cols, ev_panel};
+
+    {
+        const int w0  = n < kNB ? n : kNB;
+        const int prc = launch_panel<T>(m, n, 0, w0, pivot, p, cl, gmax, s);
+        if (prc != B200LA_SUCCESS)
+        {
+            return prc;
+        }
+    }
     for (int k = 0; k < n; k += kNB)
     {
-        int w = n - k < kNB ? n - k : kNB;
-        {
-            const int prc = launch_panel<T>(m, n, k, w, pivot, p, cl, gmax, s);
-            if (prc != B200LA_SUCCESS)
-            {
-                return prc;
-            }
-        }
+        const int w    = n - k < kNB ? n - k : kNB;
         const int rest = n - k - w;
         const int nl   = (k + kSwapCols - 1) / kSwapCols;
         const int nr   = (rest + kSwapCols - 1) / kSwapCols;
@@ -302,30 +419,47 @@ int enqueue_getrf(T* m, int n, int64_t* pivot, const GetrfPlan<T>& p, cudaStream
             prof_end(KC_SWAP, s);
             B200LA_LAUNCH_CHECK();
         }
-        if (rest > 0)
+        if (rest <= 0)
         {
-            prof_begin(KC_TRAILING, s);
-            if constexpr (sizeof(T) == 8)
+            break;
+        }
+        const int kn = k + w;  // the next panel
+        const int wn = rest < kNB ? rest : kNB;
+        int       rc = B200LA_SUCCESS;
+        if (ahead && rest > wn)
+        {
+            rc = launch_trailing<T>(m, n, k, w, 0, wn, s);
+            if (rc != B200LA_SUCCESS)
             {
-                // A22 -= L21 U12 on the tensor cores, delta from zero then
-                // subtracted: the same bits as k_trailing's fma loop.
-                const double* l21 = m + (int64_t)(k + w) * n + k;
-                const double* u12 = m + (int64_t)k * n + k + w;
-                double*       a22 = m + (int64_t)(k + w) * n + k + w;
-                static_assert(kNB <= kBandK, "the band kernel holds one panel's L21 slice");
-                const int     tpc = band_tiles_per_cta(rest, rest, device_sm_count());
-                const int     ct  = (rest + kDmTile - 1) / kDmTile;
-                const dim3    grid((ct + tpc - 1) / tpc, (rest + kDmTile - 1) / kDmTile);
-                k_dmma_band<0><<<grid, kDmThreads, kBandSmem, s>>>(
-                    rest, rest, w, l21, n, u12, n, a22, n, tpc, dm_vec16(l21, n, u12, n, a22, n));
+                return rc;
             }
-            else
+            B200LA_CUDA(cudaEventRecord(ev_cols, s));
+            B200LA_CUDA(cudaStreamWaitEvent(side, ev_cols, 0));
+            rc = launch_panel<T>(m, n, kn, wn, pivot, p, cl, gmax, side, true);
+            if (rc != B200LA_SUCCESS)
             {
-                dim3 grid((rest + kChunkN - 1) / kChunkN, (rest + kBandM - 1) / kBandM);
-                k_trailing<T><<<grid, 128, trailing_smem_bytes<T>(), s>>>(m, n, k, w, rest);
+                return rc;
             }
-            prof_end(KC_TRAILING, s);
-            B200LA_LAUNCH_CHECK();
+            B200LA_CUDA(cudaEventRecord(ev_panel, side));
+            rc = launch_trailing<T>(m, n, k, w, wn, rest, s);
+            if (rc != B200LA_SUCCESS)
+            {
+                return rc;
+            }
+            B200LA_CUDA(cudaStreamWaitEvent(s, ev_panel, 0));
+        }
+        else
+        {
+            rc = launch_trailing<T>(m, n, k, w, 0, rest, s);
+            if (rc != B200LA_SUCCESS)
+            {
+                return rc;
+            }
+            rc = launch_panel<T>(m, n, kn, wn, pivot, p, cl, gmax, s);
+            if (rc != B200LA_SUCCESS)
+            {
+                return rc;
+            }
         }
     }
     prof_begin(KC_SOLVE, s);

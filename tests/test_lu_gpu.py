@@ -90,6 +90,37 @@ def test_lu_grid_panel_path_bitwise(port, monkeypatch, n):
     assert np.array_equal(lu, lu_o)
 
 
+@pytest.mark.parametrize("force_grid", ["0", "1"])
+def test_lu_lookahead_bitwise(port, monkeypatch, force_grid):
+    """The FP64 look-ahead (next panel on a side stream beside the rest of
+    the trailing update; grid panels on fewer CTAs there) changes only the
+    schedule: the factors equal the oracle's and the run without it."""
+    monkeypatch.setenv("B200LA_FORCE_GRID_PANEL", force_grid)
+    n = 1500
+    a = random_matrix(n, seed=77 + n)
+    lu_o, piv_o, _ = port.getrf(a)
+    lu, piv, _ = gpu_getrf(a)
+    assert np.array_equal(piv, piv_o)
+    assert np.array_equal(lu, lu_o)
+    monkeypatch.setenv("B200LA_LU_LOOKAHEAD", "0")
+    lu0, piv0, _ = gpu_getrf(a)
+    assert np.array_equal(piv0, piv) and np.array_equal(lu0, lu)
+
+
+def test_lu_lookahead_neutral_large():
+    """n = 7000 (grid panels while more than ~6200 rows remain, cluster
+    panels after): look-ahead on and off give identical bits."""
+    import os
+    a = random_matrix(7000, seed=7000)
+    lu, piv, _ = gpu_getrf(a)
+    os.environ["B200LA_LU_LOOKAHEAD"] = "0"
+    try:
+        lu0, piv0, _ = gpu_getrf(a)
+    finally:
+        del os.environ["B200LA_LU_LOOKAHEAD"]
+    assert np.array_equal(piv0, piv) and np.array_equal(lu0, lu)
+
+
 def wide_exponent_matrix(n, seed, kind):
     """N(0,1) entries scaled by 2^e with e spread over most of the FP64
     range: 'wide' (|e| <= 900, products over- and underflow), 'subnormal'
