@@ -339,11 +339,16 @@ __global__ void __launch_bounds__(kDmThreads, 1) k_dmma_update(int M, int N, int
 }
 
 // The LU trailing update A22 -= L21 U12 (panel depth K <= kBandK) as a
-// band kernel, bit-identical to k_dmma_update<true>: the CTA keeps its
-// kDmTile x K slice of L21 resident in shared memory and walks `tiles`
-// consecutive kDmTile-column tiles of U12 / A22, computing tile j while
-// tile j+1's U12 slice lands in the other buffer and its A22 rows are pulled
-// into L2.  Per tile: delta from zero over k in order, then A22 - delta.
+// band kernel, bit-identical to k_dmma_update<true>.  The kDmTile x kDmTile
+// output tiles (units) are numbered row band by row band; CTA b of G takes
+// units [b*T/G, (b+1)*T/G), and G is a whole number of waves of SMs, so every
+// CTA gets the same count within one and no wave runs nearly empty, while
+// CTAs stay short (a few units) and an SM frees up for a concurrent
+// higher-priority kernel every few tens of microseconds.  It keeps its band's kDmTile x K
+// slice of L21 resident in shared memory, computes tile u while tile u+1's
+// U12 slice lands in the other buffer and its A22 rows are pulled into L2,
+// and reloads the L21 slice only when its run of units enters the next band.
+// Per tile: delta from zero over k in order, then A22 - delta.
 constexpr int    kBandK      = 64;
 constexpr int    kBandLDA    = kBandK + 4;
 constexpr int    kBandAElems = kDmTile * kBandLDA;
@@ -381,18 +386,36 @@ __device__ __forceinline__ void band_prefetch_c(const double* C, int64_t ldc, in
     }
 }
 
+__device__ __forceinline__ void band_load_a(double* sa, const double* A, int64_t lda, int M, int K, int m0,
+    bool vec16)
+{
+    constexpr int APR = kBandK / 2;
+#pragma unroll
+    for (int e = threadIdx.x; e < kDmTile * APR; e += kDmThreads)
+    {
+        const int r = e / APR, q = e - (e / APR) * APR;
+        const int row = m0 + r, col = 2 * q;
+        const int valid = row < M ? min(2, K - col) : 0;
+        dm_piece(sa + r * kBandLDA + col, valid > 0 ? A + (int64_t)row * lda + col : A, A, valid, vec16);
+    }
+}
+
 template <int Unused = 0>
 __global__ void __launch_bounds__(kDmThreads, 1) k_dmma_band(int M, int N, int K, const double* __restrict__ A,
-    int64_t lda, const double* __restrict__ B, int64_t ldb, double* __restrict__ C, int64_t ldc, int tiles,
-    int vec16)
+    int64_t lda, const double* __restrict__ B, int64_t ldb, double* __restrict__ C, int64_t ldc, int vec16,
+    const DeviceStatus* gate)
 {
     extern __shared__ __align__(16) unsigned char dm_smem[];
+    if (gated(gate))
+    {
+        return;
+    }
     double*    sa    = reinterpret_cast<double*>(dm_smem);
     double*    sbuf  = sa + kBandAElems;
-    const int  m0    = blockIdx.y * kDmTile;
-    const int  nt0   = blockIdx.x * tiles;  // first column tile
-    const int  ntile = (N + kDmTile - 1) / kDmTile;
-    const int  nend  = min(ntile, nt0 + tiles);
+    const int  ct    = (N + kDmTile - 1) / kDmTile;
+    const int  total = ct * ((M + kDmTile - 1) / kDmTile);
+    const int  u0    = (int)(((int64_t)blockIdx.x * total) / gridDim.x);
+    const int  u1    = (int)(((int64_t)(blockIdx.x + 1) * total) / gridDim.x);
     const int  warp  = threadIdx.x >> 5;
     const int  lane  = threadIdx.x & 31;
     const int  g     = lane >> 2;
@@ -400,37 +423,30 @@ __global__ void __launch_bounds__(kDmThreads, 1) k_dmma_band(int M, int N, int K
     const int  wm    = (warp >> 2) * 32;
     const int  wn    = (warp & 3) * 32;
     const bool v16   = vec16 != 0;
-    if (nt0 >= nend)
+    if (u0 >= u1)
     {
         return;
     }
 
-    // L21 slice (kDmTile x K, zero-filled past M and K) and the first U12 tile
-    {
-        constexpr int APR = kBandK / 2;
-#pragma unroll
-        for (int e = threadIdx.x; e < kDmTile * APR; e += kDmThreads)
-        {
-            const int r = e / APR, q = e - (e / APR) * APR;
-            const int row = m0 + r, col = 2 * q;
-            const int valid = row < M ? min(2, K - col) : 0;
-            dm_piece(sa + r * kBandLDA + col, valid > 0 ? A + (int64_t)row * lda + col : A, A, valid, v16);
-        }
-    }
-    band_load_b(sbuf, B, ldb, N, K, nt0 * kDmTile, v16);
+    // the first unit's L21 slice (zero-filled past M and K) and U12 tile
+    band_load_a(sa, A, lda, M, K, (u0 / ct) * kDmTile, v16);
+    band_load_b(sbuf, B, ldb, N, K, (u0 % ct) * kDmTile, v16);
     cp_async_commit();
-    band_prefetch_c(C, ldc, M, N, m0, nt0 * kDmTile);
+    band_prefetch_c(C, ldc, M, N, (u0 / ct) * kDmTile, (u0 % ct) * kDmTile);
 
-    for (int nt = nt0; nt < nend; ++nt)
+    for (int u = u0; u < u1; ++u)
     {
-        const int n0  = nt * kDmTile;
-        const int cur = (nt - nt0) & 1;
+        const int  m0   = (u / ct) * kDmTile;
+        const int  n0   = (u % ct) * kDmTile;
+        const int  cur  = (u - u0) & 1;
+        const bool next = u + 1 < u1;
+        const bool same = next && (u + 1) / ct == u / ct;
         cp_async_wait<0>();
-        __syncthreads();  // this tile's U12 landed; the other buffer is free
-        if (nt + 1 < nend)
+        __syncthreads();  // this unit's operands landed; the other buffer is free
+        if (same)
         {
-            band_load_b(sbuf + (cur ^ 1) * kBandBElems, B, ldb, N, K, n0 + kDmTile, v16);
-            band_prefetch_c(C, ldc, M, N, m0, n0 + kDmTile);
+            band_load_b(sbuf + (cur ^ 1) * kBandBElems, B, ldb, N, K, ((u + 1) % ct) * kDmTile, v16);
+            band_prefetch_c(C, ldc, M, N, m0, ((u + 1) % ct) * kDmTile);
         }
         cp_async_commit();
 
@@ -472,64 +488,92 @@ __global__ void __launch_bounds__(kDmThreads, 1) k_dmma_band(int M, int N, int K
             }
         }
 
+        // this thread's A22 values two fragment rows at a time: the loads of
+        // a half are independent (mostly L2 hits after the prefetch) and
+        // issue together, then the subtractions and stores
 #pragma unroll
-        for (int i = 0; i < 4; ++i)
+        for (int h = 0; h < 2; ++h)
         {
-            const int row = m0 + wm + 8 * i + g;
-            if (row >= M)
-            {
-                continue;
-            }
-            double* crow = C + (int64_t)row * ldc;
-            double2 cv[4];
+            double2 cv[2][4];
 #pragma unroll
-            for (int j = 0; j < 4; ++j)
+            for (int ii = 0; ii < 2; ++ii)
             {
-                const int col = n0 + wn + 8 * j + 2 * t;
-                if (v16 && col + 1 < N)
-                {
-                    cv[j] = *reinterpret_cast<const double2*>(crow + col);
-                }
-                else
-                {
-                    cv[j].x = col < N ? crow[col] : 0.0;
-                    cv[j].y = col + 1 < N ? crow[col + 1] : 0.0;
-                }
-            }
+                const int     row  = m0 + wm + 8 * (2 * h + ii) + g;
+                const double* crow = C + (int64_t)row * ldc;
 #pragma unroll
-            for (int j = 0; j < 4; ++j)
-            {
-                const int col = n0 + wn + 8 * j + 2 * t;
-                cv[j].x       = cv[j].x - acc[i][j][0];
-                cv[j].y       = cv[j].y - acc[i][j][1];
-                if (v16 && col + 1 < N)
+                for (int j = 0; j < 4; ++j)
                 {
-                    *reinterpret_cast<double2*>(crow + col) = cv[j];
-                }
-                else
-                {
-                    if (col < N)
+                    const int col = n0 + wn + 8 * j + 2 * t;
+                    if (row < M && v16 && col + 1 < N)
                     {
-                        crow[col] = cv[j].x;
+                        cv[ii][j] = *reinterpret_cast<const double2*>(crow + col);
                     }
-                    if (col + 1 < N)
+                    else
                     {
-                        crow[col + 1] = cv[j].y;
+                        cv[ii][j].x = row < M && col < N ? crow[col] : 0.0;
+                        cv[ii][j].y = row < M && col + 1 < N ? crow[col + 1] : 0.0;
                     }
                 }
             }
+#pragma unroll
+            for (int ii = 0; ii < 2; ++ii)
+            {
+                const int i   = 2 * h + ii;
+                const int row = m0 + wm + 8 * i + g;
+                if (row >= M)
+                {
+                    continue;
+                }
+                double* crow = C + (int64_t)row * ldc;
+#pragma unroll
+                for (int j = 0; j < 4; ++j)
+                {
+                    const int col = n0 + wn + 8 * j + 2 * t;
+                    cv[ii][j].x   = cv[ii][j].x - acc[i][j][0];
+                    cv[ii][j].y   = cv[ii][j].y - acc[i][j][1];
+                    if (v16 && col + 1 < N)
+                    {
+                        *reinterpret_cast<double2*>(crow + col) = cv[ii][j];
+                    }
+                    else
+                    {
+                        if (col < N)
+                        {
+                            crow[col] = cv[ii][j].x;
+                        }
+                        if (col + 1 < N)
+                        {
+                            crow[col + 1] = cv[ii][j].y;
+                        }
+                    }
+                }
+            }
+        }
+
+        if (next && !same)
+        {
+            // the run enters the next band: every warp is done with this
+            // band's L21 slice before it is replaced
+            __syncthreads();
+            band_load_a(sa, A, lda, M, K, ((u + 1) / ct) * kDmTile, v16);
+            band_load_b(sbuf + (cur ^ 1) * kBandBElems, B, ldb, N, K, ((u + 1) % ct) * kDmTile, v16);
+            cp_async_commit();
+            band_prefetch_c(C, ldc, M, N, ((u + 1) / ct) * kDmTile, ((u + 1) % ct) * kDmTile);
         }
     }
     cp_async_wait<0>();
 }
 
-// Column tiles per CTA for k_dmma_band: as many as keep at least two waves
-// of CTAs over the SMs, at most 8.
-inline int band_tiles_per_cta(int rows, int cols, int sms)
+// Grid size for k_dmma_band: whole waves of one CTA per SM, about
+// kBandUnits units per CTA (fewer CTAs only when there are fewer units).
+constexpr int kBandUnits = 4;
+inline int band_grid(int rows, int cols, int sms)
 {
-    const int rt = (rows + kDmTile - 1) / kDmTile, ct = (cols + kDmTile - 1) / kDmTile;
-    const int per = (rt * ct) / (2 * (sms > 0 ? sms : 148));
-    return per < 1 ? 1 : (per > 8 ? 8 : per);
+    const int total = ((rows + kDmTile - 1) / kDmTile) * ((cols + kDmTile - 1) / kDmTile);
+    const int sm    = sms > 0 ? sms : 148;
+    const int waves = (total + sm * kBandUnits - 1) / (sm * kBandUnits);
+    const int g     = waves * sm;
+    return total < g ? total : g;
 }
 
 inline bool dm_aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; }

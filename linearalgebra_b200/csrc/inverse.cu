@@ -553,8 +553,18 @@ int launch_gemm(int M, int N, int K, const T* a, const T* b, T* c, int64_t ld, c
     prof_begin(KC_INV_GEMM, s);
     if constexpr (sizeof(T) == 8)
     {
-        const dim3 dgrid((unsigned)((N + kDmTile - 1) / kDmTile), (unsigned)((M + kDmTile - 1) / kDmTile));
-        k_dmma_update<false><<<dgrid, kDmThreads, kDmSmem, s>>>(M, N, K, a, ld, b, ld, c, ld, vec16, gate);
+        if (K <= kBandK)
+        {
+            // the 64-deep block-row updates: the band kernel (even work per
+            // SM; C - A B from zero, rounding-equivalent)
+            k_dmma_band<0><<<band_grid(M, N, device_sm_count()), kDmThreads, kBandSmem, s>>>(
+                M, N, K, a, ld, b, ld, c, ld, vec16, gate);
+        }
+        else
+        {
+            const dim3 dgrid((unsigned)((N + kDmTile - 1) / kDmTile), (unsigned)((M + kDmTile - 1) / kDmTile));
+            k_dmma_update<false><<<dgrid, kDmThreads, kDmSmem, s>>>(M, N, K, a, ld, b, ld, c, ld, vec16, gate);
+        }
     }
     else
     {

@@ -329,11 +329,8 @@ int launch_trailing(T* m, int n, int k, int w, int c0, int c1, cudaStream_t s)
         const double* u12 = m + (int64_t)k * n + k + w + c0;
         double*       a22 = m + (int64_t)(k + w) * n + k + w + c0;
         const int     nc  = c1 - c0;
-        const int     tpc = band_tiles_per_cta(rest, nc, device_sm_count());
-        const int     ct  = (nc + kDmTile - 1) / kDmTile;
-        const dim3    grid((ct + tpc - 1) / tpc, (rest + kDmTile - 1) / kDmTile);
-        k_dmma_band<0><<<grid, kDmThreads, kBandSmem, s>>>(
-            rest, nc, w, l21, n, u12, n, a22, n, tpc, dm_vec16(l21, n, u12, n, a22, n));
+        k_dmma_band<0><<<band_grid(rest, nc, device_sm_count()), kDmThreads, kBandSmem, s>>>(
+            rest, nc, w, l21, n, u12, n, a22, n, dm_vec16(l21, n, u12, n, a22, n), nullptr);
     }
     else
     {
