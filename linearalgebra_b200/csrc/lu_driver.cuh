@@ -13,6 +13,7 @@
 #include "dmma.cuh"
 #include "lu_kernels.cuh"
 #include "solve_kernels.cuh"
+#include "trsv.cuh"
 
 namespace b200la
 {
@@ -153,15 +154,24 @@ template <typename T> GetrfPlan<T> plan_getrf(Arena& a)
 
 template <typename T> struct SolvePlan
 {
-    int32_t* perm;
-    T*       y;
+    int32_t*  perm;
+    T*        y;
+    // one-launch triangular solves (FP64, one right-hand side)
+    uint64_t* xll;    // flagged copies of solved blocks (16 bytes per row)
+    int32_t*  ticket; // block ticket of k_trsv_blocks
 };
 
 template <typename T> SolvePlan<T> plan_solve(Arena& a, int64_t n, int64_t nrhs)
 {
-    SolvePlan<T> p;
+    SolvePlan<T> p{};
     p.perm = a.next<int32_t>((size_t)n);
     p.y    = a.next<T>((size_t)n * (size_t)nrhs);
+    if (sizeof(T) == 8 && nrhs == 1)
+    {
+        const size_t nb = (size_t)((n + kTvRows - 1) / kTvRows);
+        p.ticket        = a.next<int32_t>(32);
+        p.xll           = a.next<uint64_t>(nb * kTvRows * 2);
+    }
     return p;
 }
 
@@ -616,6 +626,33 @@ int enqueue_getrs(const T* lu, const int64_t* pivot, int n, int nrhs, T* x, int6
     k_gather_rows<T><<<grid_1d(total, 256), 256, 0, s>>>(x, ldx, sp.perm, sp.y, nrhs, n, nrhs, gate);
     prof_end(KC_SOLVE, s);
     B200LA_LAUNCH_CHECK();
+    if constexpr (sizeof(T) == 8)
+    {
+        if (nrhs == 1 && sp.xll != nullptr)
+        {
+            // L then U, each in one launch: 64-row blocks claimed in solve
+            // order, solved blocks published as flagged words (bounded
+            // waits), each diagonal block solved by substitution.  On an
+            // exactly singular factorization (gate set) this works on
+            // scratch only and the final copy below is skipped.
+            const int nb = (n + kTvRows - 1) / kTvRows;
+            for (int pass = 0; pass < 2; ++pass)
+            {
+                B200LA_CUDA(cudaMemsetAsync(sp.ticket, 0, sizeof(int32_t), s));
+                const uint32_t epoch = tv_next_epoch();
+                prof_begin(KC_SOLVE, s);
+                k_trsv_blocks<double, true><<<nb, kTvThreads, 0, s>>>(lu, n, sp.y, n, pass, nullptr, sp.xll, epoch,
+                    sp.ticket, st);
+                prof_end(KC_SOLVE, s);
+                B200LA_LAUNCH_CHECK();
+            }
+            prof_begin(KC_SOLVE, s);
+            k_copy2d<T><<<grid_1d(total, 256), 256, 0, s>>>(sp.y, nrhs, x, ldx, n, nrhs, gate);
+            prof_end(KC_SOLVE, s);
+            B200LA_LAUNCH_CHECK();
+            return B200LA_SUCCESS;
+        }
+    }
     int rc = enqueue_trsm_inplace<T>(false, false, true, n, nrhs, lu, n, sp.y, nrhs, gate, s);
     if (rc != B200LA_SUCCESS)
     {

@@ -524,18 +524,6 @@ struct MixedPlan
 
 constexpr int kMaxNrhsMixed = 64;
 
-// Epochs of the flagged words of k_trsv_blocks: distinct for every launch in
-// this process (never 0, the value of cleared memory).
-uint32_t next_epoch()
-{
-    static std::atomic<uint32_t> e{0};
-    uint32_t v = e.fetch_add(1) + 1;
-    if (v == 0)
-    {
-        v = e.fetch_add(1) + 1;
-    }
-    return v;
-}
 constexpr int kGmresMaxRestart = 50;
 
 MixedPlan plan_mixed(Arena& a, int64_t n, int64_t nrhs, int restart, bool fp64_fallback)
@@ -1034,7 +1022,7 @@ int enqueue_lu_apply(const TA* lu, const int32_t* perm, int n, int nrhs, double*
         for (int pass = 0; pass < 2; ++pass)
         {
             B200LA_CUDA(cudaMemsetAsync(p.tsync, 0, sizeof(int32_t), s));
-            const uint32_t epoch = next_epoch();
+            const uint32_t epoch = tv_next_epoch();
             prof_begin(KC_SOLVE, s);
             k_trsv_blocks<TA><<<nb, kTvThreads, 0, s>>>(lu, n, p.y, n, pass, p.dinv, p.xll, epoch,
                 reinterpret_cast<int32_t*>(p.tsync), st);

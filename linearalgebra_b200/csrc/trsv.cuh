@@ -16,6 +16,10 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <atomic>
+#include <chrono>
+#include <random>
+
 #include "common.cuh"
 
 namespace b200la
@@ -23,6 +27,24 @@ namespace b200la
 
 constexpr int kTvRows    = 64;
 constexpr int kTvThreads = 256;
+
+// Epoch of one k_trsv_blocks launch: the value its flagged words carry.  One
+// counter for every caller in the process, never 0 (the value of cleared
+// memory), started at a random point so that words left in reused device
+// memory by an earlier process do not carry the epochs this one issues.
+inline uint32_t tv_next_epoch()
+{
+    static std::atomic<uint32_t> e{[] {
+        std::random_device rd;
+        return (uint32_t)rd() ^ (uint32_t)std::chrono::steady_clock::now().time_since_epoch().count();
+    }()};
+    uint32_t v = e.fetch_add(1) + 1;
+    if (v == 0)
+    {
+        v = e.fetch_add(1) + 1;
+    }
+    return v;
+}
 
 struct TrsvSync
 {
@@ -113,10 +135,14 @@ __device__ __forceinline__ bool tv_read(const uint64_t* xll, int blk, int i, uin
 }
 
 // x <- T^-1 x for T the unit-lower (upper = 0) or upper (upper = 1) triangle
-// of the factor `a`, using dinv (k_invert_diag_blocks).  CTA = one 64-row
-// block, claimed by ticket in solve order; xll receives the flagged copies of
-// the solved blocks (epoch: a value this call's flags carry, never reused).
-template <typename TA>
+// of the factor `a`.  CTA = one 64-row block, claimed by ticket in solve
+// order; xll receives the flagged copies of the solved blocks (epoch: a value
+// this call's flags carry, never reused).  The diagonal block is applied as
+// its inverse from dinv (k_invert_diag_blocks; SUBST = false, the refinement
+// solves, whose rounding the refinement corrects) or solved by substitution
+// from the block's own triangle (SUBST = true, dinv unused: backward stable,
+// for the plain FP64 solve).
+template <typename TA, bool SUBST = false>
 __global__ void __launch_bounds__(kTvThreads) k_trsv_blocks(const TA* __restrict__ a, int64_t lda,
     double* __restrict__ x, int n, int upper, const double* __restrict__ dinv, uint64_t* __restrict__ xll,
     uint32_t epoch, int32_t* __restrict__ ticket, DeviceStatus* st)
@@ -143,6 +169,17 @@ __global__ void __launch_bounds__(kTvThreads) k_trsv_blocks(const TA* __restrict
     const int blk = upper ? nb - 1 - t : t;
     const int r0  = blk * kTvRows;
     const int br  = min(kTvRows, n - r0);
+    if (SUBST)
+    {
+        // the diagonal block's triangle (unit diagonal not stored for L)
+        for (int e = tid; e < kTvRows * kTvRows; e += kTvThreads)
+        {
+            const int  i = e / kTvRows, c = e % kTvRows;
+            const bool in = i < br && c < br && (upper ? c >= i : c < i);
+            inv[i][c]     = in ? (double)a[(int64_t)(r0 + i) * lda + r0 + c] : 0.0;
+        }
+    }
+    else
     {
         const double* src = dinv + ((size_t)blk * 2 + (upper ? 1 : 0)) * kTvRows * kTvRows;
         for (int e = tid; e < kTvRows * kTvRows; e += kTvThreads)
@@ -216,11 +253,15 @@ __global__ void __launch_bounds__(kTvThreads) k_trsv_blocks(const TA* __restrict
                 xn_ok = tv_read(xll, upper ? nb - 2 - s : s + 1, tid, epoch, xn);
             }
         }
+        // this block's products summed on their own, then added: blocked
+        // summation keeps each row's dependent chain at one add per block
+        double bp = 0.0;
 #pragma unroll
         for (int j = 0; j < Q; ++j)
         {
-            acc = fma((double)ac[j], xs[s & 1][q * Q + j], acc);
+            bp = fma((double)ac[j], xs[s & 1][q * Q + j], bp);
         }
+        acc += bp;
     }
     part[r][q] = acc;
     __syncthreads();
@@ -235,6 +276,57 @@ __global__ void __launch_bounds__(kTvThreads) k_trsv_blocks(const TA* __restrict
         vb[tid] = tid < br ? x[r0 + tid] - sum : 0.0;
     }
     __syncthreads();
+    if (SUBST)
+    {
+        // warp 0: lane l holds rows l and l + 32; at step p the owner of row
+        // p finishes it (divides by the diagonal when upper) and broadcasts
+        // it, and every lane updates its rows still to be solved
+        if (tid < 32)
+        {
+            double v0 = vb[tid], v1 = vb[tid + 32];
+            for (int qq = 0; qq < kTvRows; ++qq)
+            {
+                const int p = upper ? kTvRows - 1 - qq : qq;
+                if (p >= br)
+                {
+                    continue;  // uniform across the warp
+                }
+                double vp = p < 32 ? v0 : v1;
+                if (upper)
+                {
+                    vp = vp / inv[p][p];
+                }
+                vp = __shfl_sync(0xffffffffu, vp, p & 31);
+                if (tid == (p & 31))
+                {
+                    if (p < 32)
+                        v0 = vp;
+                    else
+                        v1 = vp;
+                }
+                const int i0 = tid, i1 = tid + 32;
+                if (upper ? i0 < p : (i0 > p && i0 < br))
+                {
+                    v0 = fma(-inv[i0][p], vp, v0);
+                }
+                if (upper ? i1 < p : (i1 > p && i1 < br))
+                {
+                    v1 = fma(-inv[i1][p], vp, v1);
+                }
+            }
+            if (tid < br)
+            {
+                x[r0 + tid] = v0;
+                tv_publish(xll, blk, tid, v0, epoch);
+            }
+            if (tid + 32 < br)
+            {
+                x[r0 + tid + 32] = v1;
+                tv_publish(xll, blk, tid + 32, v1, epoch);
+            }
+        }
+        return;
+    }
     if (tid < br)
     {
         double v = 0.0;
