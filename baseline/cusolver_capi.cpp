@@ -4,8 +4,9 @@
  * CUDA_BLAS inversion and determinant in LU mode, so bench.py can time the
  * reference's GPU backend beside this library.  Compiled together with the
  * reference's sources (src/matrix_operation/gpu/cublas/{linear_solver,
- * lu_decomposition,transpose,cholesky_decomposition}_cublas.cpp and
- * inversion_cublas.cu) by baseline/Makefile into
+ * lu_decomposition,transpose,cholesky_decomposition}_cublas.cpp,
+ * inversion_cublas.cu and multiplication_batched_cublas.cu) by
+ * baseline/Makefile into
  * baseline/_ref/libref_cublas.so.
  *
  * Timing-comparison code only.  Nothing in the B200 library links or calls
@@ -23,6 +24,7 @@
 #include "include/matrix_operation/determinant.h"
 #include "include/matrix_operation/inversion.h"
 #include "include/matrix_operation/linear_solver.h"
+#include "include/matrix_operation/multiplication_batched.h"
 
 using linalg::linalg_backend;
 using linalg::linear_solver_type;
@@ -114,6 +116,34 @@ int ref_cublas_ddeterminant(double* m, int64_t n, double* out, void* ws, size_t 
     {
         *out = linalg::determinant<double, linalg_backend::CUDA_BLAS>::apply(
             m, nullptr, n, linear_solver_type::LU_LINEAR_SOLVER, ws, ws_bytes, stream);
+        return 0;
+    }
+    catch (const std::exception& e)
+    {
+        g_err = e.what();
+        return -1;
+    }
+}
+
+int ref_cublas_dgemm_batched(int64_t dim, int64_t count, const double* a, const double* b, double* c, void* stream)
+{
+    try
+    {
+        linalg::batched_matrix_multiplication(dim, count, a, b, c, stream);
+        return 0;
+    }
+    catch (const std::exception& e)
+    {
+        g_err = e.what();
+        return -1;
+    }
+}
+
+int ref_cublas_sgemm_batched(int64_t dim, int64_t count, const float* a, const float* b, float* c, void* stream)
+{
+    try
+    {
+        linalg::batched_matrix_multiplication(dim, count, a, b, c, stream);
         return 0;
     }
     catch (const std::exception& e)

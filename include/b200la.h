@@ -199,7 +199,9 @@ B200LA_API int    b200la_sdeterminant(float* m, int64_t* pivot, int64_t n, int m
  * Replaces multiplication<T, Backend>::apply (16-argument form) /
  * ::workspace_size (include/matrix_operation/multiplication.h:47-62,107-114):
  * c = alpha op(a) op(b) + beta c, row-major, BLAS contract (beta == 0: c is
- * write-only; alpha == 0: a and b are not read).  Asynchronous. */
+ * write-only; alpha == 0: a and b are not read).  FP64 with op(b) = b runs
+ * on the FP64 tensor cores and gives the reference NATIVE loop's bits
+ * (beta c, then fma(alpha a_ik, b_kj, c) in k order).  Asynchronous. */
 B200LA_API size_t b200la_dgemm_workspace_size(int64_t rows, int64_t cols, int64_t depth);
 B200LA_API size_t b200la_sgemm_workspace_size(int64_t rows, int64_t cols, int64_t depth);
 B200LA_API int    b200la_dgemm(int transpose_a, int transpose_b, int64_t rows, int64_t cols,
@@ -209,6 +211,19 @@ B200LA_API int    b200la_dgemm(int transpose_a, int transpose_b, int64_t rows, i
 B200LA_API int    b200la_sgemm(int transpose_a, int transpose_b, int64_t rows, int64_t cols,
        int64_t depth, float alpha, const float* a, int64_t lda, const float* b, int64_t ldb,
        float beta, float* c, int64_t ldc, void* workspace, size_t workspace_bytes, void* stream);
+
+/* ---- batched multiplication ------------------------------------------------
+ * Replaces batched_matrix_multiplication (include/matrix_operation/
+ * multiplication_batched.h; CUDA_BLAS kernel src/matrix_operation/gpu/cublas/
+ * multiplication_batched_cublas.cu:15-40): c_i = a_i b_i for i < count,
+ * each a dim x dim row-major matrix, packed back to back (element offset
+ * i*dim*dim).  Each entry is the sum of the products from zero in k order
+ * with fused multiply-adds, like the reference's kernel (FP64 on the FP64
+ * tensor cores, FP32 on the SIMT FMA pipe).  Asynchronous. */
+B200LA_API int b200la_dgemm_batched(int64_t dim, int64_t count, const double* a, const double* b, double* c,
+    void* stream);
+B200LA_API int b200la_sgemm_batched(int64_t dim, int64_t count, const float* a, const float* b, float* c,
+    void* stream);
 
 /* ---- mixed-precision LU solve with FP64 iterative refinement --------------
  * Solves A X = B (A n x n FP64, row stride n, left unchanged; B, X n x nrhs,

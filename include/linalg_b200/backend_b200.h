@@ -20,7 +20,10 @@
  *  - determinant returns det(A) with the pivot sign applied, as CUDA_BLAS
  *    does; the NATIVE reduction omits that sign (include/matrix_operation/
  *    determinant.h), its magnitude is the same bits (b200la_ddeterminant
- *    returns both parts).
+ *    returns both parts);
+ *  - batched_matrix_multiplication (a free function in the reference, one
+ *    definition per build) is defined by this library unless the build
+ *    also compiles the CUDA_BLAS one (LINALG_HAS_CUBLAS), which it replaces.
  */
 #pragma once
 

@@ -9,6 +9,7 @@
  *   include/matrix_operation/multiplication.h:15-114
  *   include/matrix_operation/inversion.h:15-53
  *   include/matrix_operation/determinant.h
+ *   include/matrix_operation/multiplication_batched.h
  * Names, argument order, default arguments and meaning are the reference's;
  * that is what makes the backend a drop-in.  Inside the reference tree define
  * LINALG_B200_USE_REFERENCE_HEADERS and add B200 as the last enumerator of
@@ -27,6 +28,7 @@
 #include "include/matrix_operation/linear_solver.h"
 #include "include/matrix_operation/lu_decomposition.h"
 #include "include/matrix_operation/multiplication.h"
+#include "include/matrix_operation/multiplication_batched.h"
 #include "include/matrix_operation/triangular_solver.h"
 #else
 
@@ -110,6 +112,11 @@ template <typename T, linalg_backend Backend> struct inversion
         void* workspace, size_t workspace_size, void* stream = nullptr);
     LINALG_API static size_t workspace_size(linalg_int lda, linear_solver_type type);
 };
+
+LINALG_API void batched_matrix_multiplication(linalg_int dim, linalg_int count, const float* a, const float* b,
+    float* c, void* stream = nullptr);
+LINALG_API void batched_matrix_multiplication(linalg_int dim, linalg_int count, const double* a,
+    const double* b, double* c, void* stream = nullptr);
 
 template <typename T, linalg_backend Backend> struct determinant
 {

@@ -10,9 +10,11 @@ from .api import (  # noqa: F401
     LU_LINEAR_SOLVER,
     LU_UPFRONT_LINEAR_SOLVER,
     MixedSolver,
+    batched_matrix_multiplication,
     det,
     determinant,
     gemm,
+    gemm_batched,
     gesv,
     getrf,
     getrs,

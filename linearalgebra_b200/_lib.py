@@ -70,6 +70,8 @@ SIGNATURES: dict[str, tuple] = {
     "b200la_sgemm_workspace_size": (_sz, [_i64, _i64, _i64]),
     "b200la_dgemm": (_i32, [_i32, _i32, _i64, _i64, _i64, _d, _p, _i64, _p, _i64, _d, _p, _i64, _p, _sz, _p]),
     "b200la_sgemm": (_i32, [_i32, _i32, _i64, _i64, _i64, _f, _p, _i64, _p, _i64, _f, _p, _i64, _p, _sz, _p]),
+    "b200la_dgemm_batched": (_i32, [_i64, _i64, _p, _p, _p, _p]),
+    "b200la_sgemm_batched": (_i32, [_i64, _i64, _p, _p, _p, _p]),
     "b200la_refine_default_options": (None, [_p]),
     "b200la_dsolve_mixed_workspace_size": (_sz, [_i64, _i64, _p]),
     "b200la_dsolve_mixed": (_i32, [_p, _i64, _i64, _p, _i64, _p, _i64, _p, _p, _p, _sz, _p]),

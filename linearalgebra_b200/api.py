@@ -124,6 +124,13 @@ class multiplication:
                      workspace_size, _stream(stream)))
 
 
+def batched_matrix_multiplication(dim: int, count: int, a, b, c, stream=None):
+    """c_i = a_i b_i for `count` packed dim x dim matrices
+    (include/matrix_operation/multiplication_batched.h).  Asynchronous."""
+    f = getattr(_lib.load(), f"b200la_{_prefix(c.dtype)}gemm_batched")
+    _lib.check(f(dim, count, _ptr(a), _ptr(b), _ptr(c), _stream(stream)))
+
+
 class inversion:
     """inversion<T, B200>, LU modes (include/matrix_operation/inversion.h:15-53)."""
 
@@ -234,6 +241,13 @@ def det(m: torch.Tensor, pivot: torch.Tensor | None = None, type: int = LU_LINEA
     value = 0.0 if product == 0 else (-product if sign < 0 else product)
     return {"det": value, "product": product, "sign": sign, "log_abs": log_abs, "singular": singular,
             "pivot": pivot}
+
+
+def gemm_batched(a: torch.Tensor, b: torch.Tensor, stream=None) -> torch.Tensor:
+    """(count, dim, dim) tensors -> their products, one per matrix."""
+    c = torch.empty_like(a)
+    batched_matrix_multiplication(a.shape[1], a.shape[0], a, b, c, stream)
+    return c
 
 
 def trsm(upper, transpose, unit, a, b, x=None, stream=None):

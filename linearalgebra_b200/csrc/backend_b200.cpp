@@ -204,4 +204,18 @@ size_t determinant<float, linalg_backend::B200>::workspace_size(linalg_int lda, 
 {
     return b200la_sdeterminant_workspace_size(lda, static_cast<int>(type));
 }
+
+// ---- batched multiplication ---------------------------------------------------
+#if !defined(LINALG_HAS_CUBLAS) || !LINALG_HAS_CUBLAS
+void batched_matrix_multiplication(linalg_int dim, linalg_int count, const float* a, const float* b, float* c,
+    void* stream)
+{
+    check_status(b200la_sgemm_batched(dim, count, a, b, c, stream));
+}
+void batched_matrix_multiplication(linalg_int dim, linalg_int count, const double* a, const double* b, double* c,
+    void* stream)
+{
+    check_status(b200la_dgemm_batched(dim, count, a, b, c, stream));
+}
+#endif
 }  // namespace linalg

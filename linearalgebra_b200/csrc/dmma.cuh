@@ -576,6 +576,194 @@ inline int band_grid(int rows, int cols, int sms)
     return total < g ? total : g;
 }
 
+// General FP64 multiplication on the tensor cores, bit-identical to the
+// reference's loops where they are fma chains:
+//   c = beta c (beta == 0: c = 0, c not read), then for k in order
+//   c = fma(alpha a_ik, b_kj, c)  with alpha a_ik rounded first
+// (multiplication_native.cpp, op(b) = b; alpha == 1 leaves a exact), which
+// is also the reference's batched kernel (sum += a b from zero,
+// multiplication_batched_cublas.cu:15-40) with alpha = 1, beta = 0.  A
+// chain of m8n8k4 DMMAs along k is that fma chain.  TRANS_A: op(a) = a^T
+// (a stored depth x rows).  Tiles, warps and the cp.async ring as
+// k_dmma_update; blockIdx.z selects the matrix of a batch (element strides
+// sa, sb, sc).
+template <bool TRANS_A>
+__global__ void __launch_bounds__(kDmThreads, 1) k_dmma_gemm(int M, int N, int K, double alpha,
+    const double* __restrict__ A, int64_t lda, int64_t sa, const double* __restrict__ B, int64_t ldb, int64_t sb,
+    double beta, double* __restrict__ C, int64_t ldc, int64_t sc, int vec16)
+{
+    extern __shared__ __align__(16) unsigned char dm_smem[];
+    double*    smem    = reinterpret_cast<double*>(dm_smem);
+    A += (int64_t)blockIdx.z * sa;
+    B += (int64_t)blockIdx.z * sb;
+    C += (int64_t)blockIdx.z * sc;
+    const int  m0      = blockIdx.y * kDmTile;
+    const int  n0      = blockIdx.x * kDmTile;
+    const int  warp    = threadIdx.x >> 5;
+    const int  lane    = threadIdx.x & 31;
+    const int  g       = lane >> 2;
+    const int  t       = lane & 3;
+    const int  wm      = (warp >> 2) * 32;
+    const int  wn      = (warp & 3) * 32;
+    const int  nchunks = (K + kDmKC - 1) / kDmKC;
+    const bool v16     = vec16 != 0;
+
+    // stage loader: A as [m][k] (row stride kDmLDA) or, transposed, [k][m]
+    // (row stride kDmLDB); B as [k][n] (kDmLDB)
+    auto load_stage = [&](double* st, int k0) {
+        if (!TRANS_A)
+        {
+            constexpr int APR = kDmKC / 2;
+            for (int e = threadIdx.x; e < kDmTile * APR; e += kDmThreads)
+            {
+                const int r = e / APR, q = e - (e / APR) * APR;
+                const int row = m0 + r, col = k0 + 2 * q;
+                const int valid = row < M ? min(2, K - col) : 0;
+                dm_piece(st + r * kDmLDA + 2 * q, valid > 0 ? A + (int64_t)row * lda + col : A, A, valid, v16);
+            }
+        }
+        else
+        {
+            constexpr int APR = kDmTile / 2;
+            for (int e = threadIdx.x; e < kDmKC * APR; e += kDmThreads)
+            {
+                const int p = e / APR, q = e - (e / APR) * APR;
+                const int kk = k0 + p, col = m0 + 2 * q;
+                const int valid = kk < K ? min(2, M - col) : 0;
+                dm_piece(st + p * kDmLDB + 2 * q, valid > 0 ? A + (int64_t)kk * lda + col : A, A, valid, v16);
+            }
+        }
+        constexpr int BPR = kDmTile / 2;
+        for (int e = threadIdx.x; e < kDmKC * BPR; e += kDmThreads)
+        {
+            const int p = e / BPR, q = e - (e / BPR) * BPR;
+            const int kk = k0 + p, col = n0 + 2 * q;
+            const int valid = kk < K ? min(2, N - col) : 0;
+            dm_piece(st + kDmAElems + p * kDmLDB + 2 * q, valid > 0 ? B + (int64_t)kk * ldb + col : B, B, valid,
+                v16);
+        }
+    };
+
+    // accumulators: beta c (c not read when beta == 0)
+    double acc[4][4][2];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+    {
+        const int     row  = m0 + wm + 8 * i + g;
+        const double* crow = C + (int64_t)row * ldc;
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+        {
+            const int col = n0 + wn + 8 * j + 2 * t;
+            double2   v   = make_double2(0.0, 0.0);
+            if (beta != 0.0 && row < M)
+            {
+                if (v16 && col + 1 < N)
+                {
+                    v = *reinterpret_cast<const double2*>(crow + col);
+                }
+                else
+                {
+                    v.x = col < N ? crow[col] : 0.0;
+                    v.y = col + 1 < N ? crow[col + 1] : 0.0;
+                }
+                if (beta != 1.0)
+                {
+                    v.x = v.x * beta;
+                    v.y = v.y * beta;
+                }
+            }
+            acc[i][j][0] = v.x;
+            acc[i][j][1] = v.y;
+        }
+    }
+
+#pragma unroll
+    for (int s = 0; s < kDmStages - 1; ++s)
+    {
+        if (s < nchunks)
+        {
+            load_stage(smem + s * kDmStage, s * kDmKC);
+        }
+        cp_async_commit();
+    }
+    const bool scale = alpha != 1.0;
+    for (int c = 0; c < nchunks; ++c)
+    {
+        cp_async_wait<kDmStages - 2>();
+        __syncthreads();  // stage c landed for every thread; stage c-1 is free
+        const int pf = c + kDmStages - 1;
+        if (pf < nchunks)
+        {
+            load_stage(smem + (pf % kDmStages) * kDmStage, pf * kDmKC);
+        }
+        cp_async_commit();
+        const double* st = smem + (c % kDmStages) * kDmStage;
+        const double* sb_ = st + kDmAElems + t * kDmLDB + wn + g;
+#pragma unroll
+        for (int ks = 0; ks < kDmKC / 4; ++ks)
+        {
+            double af[4], bf[4];
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+            {
+                af[i] = TRANS_A ? st[(4 * ks + t) * kDmLDB + wm + g + 8 * i]
+                                : st[(wm + g + 8 * i) * kDmLDA + 4 * ks + t];
+                if (scale)
+                {
+                    af[i] = alpha * af[i];
+                }
+            }
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+            {
+                bf[j] = sb_[4 * ks * kDmLDB + 8 * j];
+            }
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+            {
+#pragma unroll
+                for (int j = 0; j < 4; ++j)
+                {
+                    dmma_884(acc[i][j][0], acc[i][j][1], af[i], bf[j]);
+                }
+            }
+        }
+    }
+    cp_async_wait<0>();
+
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+    {
+        const int row = m0 + wm + 8 * i + g;
+        if (row >= M)
+        {
+            continue;
+        }
+        double* crow = C + (int64_t)row * ldc;
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+        {
+            const int col = n0 + wn + 8 * j + 2 * t;
+            if (v16 && col + 1 < N)
+            {
+                *reinterpret_cast<double2*>(crow + col) = make_double2(acc[i][j][0], acc[i][j][1]);
+            }
+            else
+            {
+                if (col < N)
+                {
+                    crow[col] = acc[i][j][0];
+                }
+                if (col + 1 < N)
+                {
+                    crow[col + 1] = acc[i][j][1];
+                }
+            }
+        }
+    }
+}
+
 inline bool dm_aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; }
 
 // 1 when every operand's rows start 16-byte aligned (the 16-byte copy path).

@@ -62,6 +62,16 @@ B200LA_API int b200la_sgesv(float* m, int64_t* pivot, int64_t n, float* x, int m
     return gesv<float>(m, pivot, n, x, mode, ws, bytes, stream);
 }
 
+B200LA_API int b200la_dgemm_batched(int64_t dim, int64_t count, const double* a, const double* b, double* c,
+    void* stream)
+{
+    return gemm_batched<double>(dim, count, a, b, c, stream);
+}
+B200LA_API int b200la_sgemm_batched(int64_t dim, int64_t count, const float* a, const float* b, float* c,
+    void* stream)
+{
+    return gemm_batched<float>(dim, count, a, b, c, stream);
+}
 B200LA_API size_t b200la_dgetrs_workspace_size(int64_t n, int64_t nrhs) { return getrs_ws_size<double>(n, nrhs); }
 B200LA_API int b200la_dgetrs(const double* lu, const int64_t* pivot, int64_t n, int64_t nrhs, double* x,
     int64_t ldx, void* ws, size_t bytes, void* stream)

@@ -90,6 +90,8 @@ template <typename T> int ensure_kernel_attributes()
     B200LA_CUDA(cudaFuncSetAttribute(
         k_dmma_update<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDmSmem));
     B200LA_CUDA(cudaFuncSetAttribute(k_dmma_band<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBandSmem));
+    B200LA_CUDA(cudaFuncSetAttribute(k_dmma_gemm<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDmSmem));
+    B200LA_CUDA(cudaFuncSetAttribute(k_dmma_gemm<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDmSmem));
     B200LA_CUDA(cudaFuncSetAttribute(k_gemm<T, false, false>,
         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gemm_smem_bytes<T>()));
     B200LA_CUDA(cudaFuncSetAttribute(k_gemm<T, true, false>,
@@ -885,9 +887,29 @@ int gemm(int ta, int tb, int64_t rows, int64_t cols, int64_t depth, T alpha, con
         }
         return B200LA_SUCCESS;
     }
+    const int r = (int)rows, co = (int)cols, d = (int)depth;
+    if constexpr (sizeof(T) == 8)
+    {
+        if (!tb)
+        {
+            // op(b) = b: the reference's loop is an fma chain per element in
+            // k order from beta c, which the FP64 tensor cores reproduce
+            const int  v16 = dm_vec16(a, lda, b, ldb, c, ldc);
+            const dim3 dgrid((unsigned)((cols + kDmTile - 1) / kDmTile), (unsigned)((rows + kDmTile - 1) / kDmTile));
+            prof_begin(KC_GEMM, s);
+            if (ta)
+                k_dmma_gemm<true><<<dgrid, kDmThreads, kDmSmem, s>>>(r, co, d, alpha, a, lda, 0, b, ldb, 0, beta, c,
+                    ldc, 0, v16);
+            else
+                k_dmma_gemm<false><<<dgrid, kDmThreads, kDmSmem, s>>>(r, co, d, alpha, a, lda, 0, b, ldb, 0, beta, c,
+                    ldc, 0, v16);
+            prof_end(KC_GEMM, s);
+            B200LA_LAUNCH_CHECK();
+            return B200LA_SUCCESS;
+        }
+    }
     dim3         grid((unsigned)((cols + 63) / 64), (unsigned)((rows + 127) / 128));
     const size_t smem = gemm_smem_bytes<T>();
-    const int    r = (int)rows, co = (int)cols, d = (int)depth;
     prof_begin(KC_GEMM, s);
     if (!ta && !tb)
         k_gemm<T, false, false><<<grid, 128, smem, s>>>(r, co, d, alpha, a, lda, b, ldb, beta, c, ldc);
@@ -899,6 +921,62 @@ int gemm(int ta, int tb, int64_t rows, int64_t cols, int64_t depth, T alpha, con
         k_gemm<T, true, true><<<grid, 128, smem, s>>>(r, co, d, alpha, a, lda, b, ldb, beta, c, ldc);
     prof_end(KC_GEMM, s);
     B200LA_LAUNCH_CHECK();
+    return B200LA_SUCCESS;
+}
+
+// ---------------------------------------------------------------------------
+// batched multiplication: c_i = a_i b_i for `count` packed dim x dim matrices
+// (batched_matrix_multiplication, include/matrix_operation/
+// multiplication_batched.h; the CUDA_BLAS kernel sums a b from zero in k
+// order, multiplication_batched_cublas.cu:15-40).  FP64 on the tensor cores
+// (the same fma chain), FP32 on the SIMT kernel (likewise).
+// ---------------------------------------------------------------------------
+template <typename T> int gemm_batched(int64_t dim, int64_t count, const T* a, const T* b, T* c, void* stream)
+{
+    if (a == nullptr || b == nullptr || c == nullptr)
+    {
+        return set_error(B200LA_INVALID_ARGUMENT, "batched_matrix_multiplication: a, b, and c must not be null");
+    }
+    if (dim <= 0 || count <= 0)
+    {
+        return set_error(B200LA_INVALID_ARGUMENT, "batched_matrix_multiplication: dim and count must be positive");
+    }
+    if (dim > INT_MAX / 2)
+    {
+        return set_error(B200LA_NOT_SUPPORTED, "batched_matrix_multiplication: dim too large");
+    }
+    int st = prepare<T>();
+    if (st != B200LA_SUCCESS)
+    {
+        return st;
+    }
+    cudaStream_t  s      = as_stream(stream);
+    const int     d      = (int)dim;
+    const int64_t stride = dim * dim;
+    constexpr int64_t kMaxZ = 65535;
+    for (int64_t c0 = 0; c0 < count; c0 += kMaxZ)
+    {
+        const unsigned nz = (unsigned)(count - c0 < kMaxZ ? count - c0 : kMaxZ);
+        const T*       ab = a + c0 * stride;
+        const T*       bb = b + c0 * stride;
+        T*             cb = c + c0 * stride;
+        prof_begin(KC_GEMM, s);
+        if constexpr (sizeof(T) == 8)
+        {
+            const int  v16 = dm_vec16(ab, dim, bb, dim, cb, dim) && (stride % 2) == 0;
+            const dim3 grid((unsigned)((d + kDmTile - 1) / kDmTile), (unsigned)((d + kDmTile - 1) / kDmTile), nz);
+            k_dmma_gemm<false><<<grid, kDmThreads, kDmSmem, s>>>(d, d, d, 1.0, ab, dim, stride, bb, dim, stride, 0.0,
+                cb, dim, stride, v16);
+        }
+        else
+        {
+            const dim3 grid((unsigned)((d + 63) / 64), (unsigned)((d + 127) / 128), nz);
+            k_gemm<T, false, false><<<grid, 128, gemm_smem_bytes<T>(), s>>>(d, d, d, T(1), ab, dim, bb, dim, T(0),
+                cb, dim, stride, stride, stride);
+        }
+        prof_end(KC_GEMM, s);
+        B200LA_LAUNCH_CHECK();
+    }
     return B200LA_SUCCESS;
 }
 

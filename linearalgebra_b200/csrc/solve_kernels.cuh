@@ -296,7 +296,8 @@ __global__ void __launch_bounds__(256) k_trsm_update(const TA* __restrict__ a, i
     }
 }
 
-// c = alpha op(a) op(b) + beta c.  CTA tile 128 x 64, K in chunks of 32,
+// c = alpha op(a) op(b) + beta c (one matrix of a batch per blockIdx.z).
+// CTA tile 128 x 64, K in chunks of 32,
 // thread mapping as k_trailing.  For op(b) = b (the two cases whose
 // reference loop nest updates c one depth index at a time) the update is
 // c <- beta c, then c = fma(alpha a_ik, b_kj, c) for k in order; with op(b)
@@ -310,8 +311,12 @@ template <typename T> constexpr size_t gemm_smem_bytes()
 template <typename T, bool TA, bool TB>
 __global__ void __launch_bounds__(128, 2) k_gemm(int rows, int cols, int depth, T alpha,
     const T* __restrict__ a, int64_t lda, const T* __restrict__ b, int64_t ldb, T beta,
-    T* __restrict__ c, int64_t ldc)
+    T* __restrict__ c, int64_t ldc, int64_t sa = 0, int64_t sb = 0, int64_t sc = 0)
 {
+    // blockIdx.z: the matrix of a batch (element strides sa, sb, sc)
+    a += (int64_t)blockIdx.z * sa;
+    b += (int64_t)blockIdx.z * sb;
+    c += (int64_t)blockIdx.z * sc;
     extern __shared__ __align__(16) unsigned char gemm_smem[];
     T(*As)[kGemmKC + 1] = reinterpret_cast<T(*)[kGemmKC + 1]>(gemm_smem);  // [128]
     T(*Bs)[64] = reinterpret_cast<T(*)[64]>(gemm_smem + sizeof(T) * 128 * (kGemmKC + 1));

@@ -78,6 +78,10 @@ class Oracle:
             ct = ctypes.c_double if t == "d" else ctypes.c_float
             f.argtypes = [_int, _int, _i64, _i64, _i64, ct, _p, _i64, _p, _i64, ct, _p, _i64]
             f.restype = _int
+            if kind == "port":
+                f = getattr(self.lib, f"or_{t}gemm_batched")
+                f.argtypes = [_i64, _i64, _p, _p, _p]
+                f.restype = _int
             f = getattr(self.lib, f"{pre}{t}getri")
             f.argtypes = [_p, _p, _i64, _int]
             f.restype = _int
@@ -138,6 +142,20 @@ class Oracle:
             int(ta), int(tb), rows, cols, depth, alpha, _ptr(a), lda, _ptr(b), ldb, beta, _ptr(c), ldc)
         if st < 0:
             raise ValueError(f"gemm rejected its arguments (status {st})")
+        return c
+
+    def gemm_batched(self, a: np.ndarray, b: np.ndarray) -> np.ndarray:
+        """c_i = a_i b_i for (count, dim, dim) arrays, the reference CUDA
+        kernel's arithmetic (port build only: the reference has no CPU
+        version)."""
+        if self.kind != "port":
+            raise NotImplementedError("the reference has no CPU batched multiplication")
+        a = np.ascontiguousarray(a)
+        b = np.ascontiguousarray(b)
+        c = np.empty_like(a)
+        st = getattr(self.lib, f"or_{self._t(a)}gemm_batched")(a.shape[1], a.shape[0], _ptr(a), _ptr(b), _ptr(c))
+        if st < 0:
+            raise ValueError(f"gemm_batched rejected its arguments (status {st})")
         return c
 
     def getri(self, a: np.ndarray, mode: int = LU_LINEAR_SOLVER, pivot=None):

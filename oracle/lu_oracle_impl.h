@@ -394,6 +394,38 @@ T OR_FN(det)(T* m, int64_t* pivot, int64_t n, int mode, int* status)
     return det;
 }
 
+/* Batched product c_i = a_i b_i of `count` packed dim x dim matrices:
+ * multiplication_batched_cublas.cu:15-40 (batched_matmul_kernel: each entry
+ * sum += a b from zero in k order, which nvcc contracts into fused
+ * multiply-adds).  The reference has no CPU version. */
+int OR_FN(gemm_batched)(int64_t dim, int64_t count, const T* a, const T* b, T* c)
+{
+    if (!a || !b || !c || dim <= 0 || count <= 0)
+    {
+        return -1;
+    }
+    const int64_t ms = dim * dim;
+    for (int64_t q = 0; q < count; ++q)
+    {
+        const T* A  = a + q * ms;
+        const T* B  = b + q * ms;
+        T*       Cq = c + q * ms;
+        for (int64_t r = 0; r < dim; ++r)
+        {
+            for (int64_t j = 0; j < dim; ++j)
+            {
+                T sum = (T)0;
+                for (int64_t k = 0; k < dim; ++k)
+                {
+                    sum = OR_FMA(A[r * dim + k], B[k * dim + j], sum);
+                }
+                Cq[r * dim + j] = sum;
+            }
+        }
+    }
+    return 0;
+}
+
 /* c = alpha op(a) op(b) + beta c, row-major, BLAS contract:
  * multiplication_native.cpp:1542-1567 (beta applied up front; beta == 0
  * overwrites c), :1807-1814 (alpha == 0 quick return), and the scalar loop

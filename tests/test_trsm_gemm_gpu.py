@@ -109,3 +109,71 @@ def test_gemm_float32():
     torch.cuda.synchronize()
     ref = a.double() @ b.double()
     assert (c.double() - ref).abs().max().item() < 1e-4
+
+
+@pytest.mark.parametrize("ta", [False, True])
+@pytest.mark.parametrize("alpha,beta", [(1.0, 0.0), (1.0, 1.0), (-0.75, 0.5), (3.0, -2.0)])
+def test_gemm_fp64_tensor_core_path_bitwise(port, ta, alpha, beta):
+    """FP64 multiplication with op(b) = b runs on the FP64 tensor cores; it
+    must keep the reference's bits (beta c, then fma(alpha a_ik, b_kj, c) in
+    k order) on sizes that cross the 128 tile and 32-deep stage edges, with
+    odd strides (the element-wise copy path) and wide exponents."""
+    rng = np.random.default_rng(7)
+    for (m, n, k) in ((300, 257, 513), (128, 128, 32), (129, 65, 33), (1, 1, 1)):
+        a = rng.standard_normal((k, m) if ta else (m, k)) * np.exp2(rng.integers(-40, 40, size=(k, m) if ta else (m, k)))
+        b = rng.standard_normal((k, n))
+        c0 = rng.standard_normal((m, n))
+        ref = c0.copy()
+        port.gemm(int(ta), 0, m, n, k, alpha, a, a.shape[1], b, n, beta, ref, n)
+        dc = dev(c0)
+        la.gemm(ta, False, alpha, dev(a), dev(b), beta, dc)
+        torch.cuda.synchronize()
+        assert np.array_equal(dc.cpu().numpy(), ref), (m, n, k, ta, alpha, beta)
+
+
+@pytest.mark.parametrize("dim,count", [(1, 3), (5, 7), (64, 2), (65, 3), (130, 2), (257, 1)])
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+def test_batched_multiplication_bitwise(port, dim, count, dtype):
+    """batched_matrix_multiplication: each entry a sum of products from zero
+    in k order (the reference kernel's fma chain), bit for bit against the
+    oracle's restatement."""
+    rng = np.random.default_rng(dim * 10 + count)
+    a = rng.standard_normal((count, dim, dim)).astype(dtype)
+    b = rng.standard_normal((count, dim, dim)).astype(dtype)
+    ref = port.gemm_batched(a, b)
+    got = la.gemm_batched(dev(a), dev(b))
+    torch.cuda.synchronize()
+    assert np.array_equal(got.cpu().numpy(), ref)
+
+
+def test_batched_multiplication_matches_reference_kernel():
+    """Against the reference's own CUDA kernel (multiplication_batched_cublas.cu,
+    built into baseline/_ref by baseline/Makefile) on the same inputs."""
+    import ctypes
+    import os
+    path = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "baseline", "_ref",
+                        "libref_cublas.so")
+    if not os.path.exists(path):
+        pytest.skip("baseline/_ref/libref_cublas.so is not built")
+    lib = ctypes.CDLL(path)
+    for name in ("ref_cublas_dgemm_batched", "ref_cublas_sgemm_batched"):
+        getattr(lib, name).argtypes = [ctypes.c_int64, ctypes.c_int64] + [ctypes.c_void_p] * 4
+    for dtype, name in ((torch.float64, "ref_cublas_dgemm_batched"), (torch.float32, "ref_cublas_sgemm_batched")):
+        for dim, count in ((48, 5), (200, 3)):
+            a = torch.randn(count, dim, dim, dtype=dtype, device="cuda")
+            b = torch.randn(count, dim, dim, dtype=dtype, device="cuda")
+            ref = torch.empty_like(a)
+            assert getattr(lib, name)(dim, count, a.data_ptr(), b.data_ptr(), ref.data_ptr(), None) == 0
+            got = la.gemm_batched(a, b)
+            torch.cuda.synchronize()
+            assert torch.equal(got, ref), (dtype, dim, count)
+
+
+def test_batched_multiplication_invalid_arguments():
+    a = torch.zeros(2, 4, 4, dtype=torch.float64, device="cuda")
+    with pytest.raises(la.B200InvalidArgument):
+        la.batched_matrix_multiplication(0, 2, a, a, a)
+    with pytest.raises(la.B200InvalidArgument):
+        la.batched_matrix_multiplication(4, 0, a, a, a)
+    lib = la._lib.load()
+    assert lib.b200la_dgemm_batched(4, 2, None, a.data_ptr(), a.data_ptr(), None) == -1
