@@ -58,6 +58,7 @@ def parse():
     p.add_argument("--no-batched", action="store_true")
     p.add_argument("--inv-n", type=int, default=16384, help="order of the inversion / determinant measurement")
     p.add_argument("--no-inversion", action="store_true")
+    p.add_argument("--no-multiplication", action="store_true")
     return p.parse_args()
 
 
@@ -350,6 +351,71 @@ def run_inversion(args, world, rank, local):
                                          f"(n/{ns})^3 to n={n}; 1 thread"}
     del A
     torch.cuda.empty_cache()
+    return out
+
+
+# ---------------------------------------------------------------------------
+# multiplication: FP64 general product on the tensor cores vs measured cuBLAS
+# DGEMM, and batched_matrix_multiplication vs the reference's CUDA kernel
+# ---------------------------------------------------------------------------
+def run_multiplication(args, world, rank, local):
+    import torch
+
+    import linearalgebra_b200 as la
+
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.current_stream(dev)
+    out = {}
+
+    def timed(fn, steps):
+        fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / steps / 1e3
+
+    n = 8192
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(SEED + 2 + rank)
+    a = torch.randn(n, n, dtype=torch.float64, device=dev, generator=gen)
+    b = torch.randn(n, n, dtype=torch.float64, device=dev, generator=gen)
+    c = torch.empty_like(a)
+    t = timed(lambda: la.gemm(False, False, 1.0, a, b, 0.0, c, stream), 3)
+    peak = measured_fp64_peak_tflops()
+    out["general_fp64"] = {"shape": f"{n}x{n}x{n} NN, alpha 1, beta 0", "s": t,
+                           "tflops": 2 * n ** 3 / t / 1e12, "measured_dgemm_tflops": peak,
+                           "frac_of_dgemm": 2 * n ** 3 / t / 1e12 / peak,
+                           "note": "bit-identical to the reference NATIVE loop (fma chain in k order)"}
+    del a, b, c
+    torch.cuda.empty_cache()
+
+    path = os.path.join(ROOT, "baseline", "_ref", "libref_cublas.so")
+    ref = None
+    if rank == 0 and world == 1 and os.path.exists(path):
+        ref = ctypes.CDLL(path)
+        for nm in ("ref_cublas_dgemm_batched", "ref_cublas_sgemm_batched"):
+            getattr(ref, nm).argtypes = [ctypes.c_int64, ctypes.c_int64] + [ctypes.c_void_p] * 4
+    for dtype, tag in ((torch.float64, "d"), (torch.float32, "s")):
+        dim, count = 256, 1000
+        a = torch.randn(count, dim, dim, dtype=dtype, device=dev, generator=gen)
+        b = torch.randn(count, dim, dim, dtype=dtype, device=dev, generator=gen)
+        c = torch.empty_like(a)
+        t = timed(lambda: la.batched_matrix_multiplication(dim, count, a, b, c, stream), 3)
+        entry = {"dim": dim, "count": count, "s": t, "tflops": 2 * dim ** 3 * count / t / 1e12}
+        if ref is not None:
+            rc = torch.empty_like(a)
+            fn = getattr(ref, f"ref_cublas_{tag}gemm_batched")
+            tr = timed(lambda: fn(dim, count, a.data_ptr(), b.data_ptr(), rc.data_ptr(), stream.cuda_stream), 3)
+            entry["reference_kernel_s"] = tr
+            entry["speedup_vs_reference_kernel"] = tr / t
+            entry["bit_identical_to_reference_kernel"] = bool(torch.equal(c, rc))
+        out[f"batched_{'fp64' if tag == 'd' else 'fp32'}"] = entry
+        del a, b, c
+        torch.cuda.empty_cache()
     return out
 
 
@@ -739,6 +805,10 @@ def run_b200(args, world, rank, local):
             torch.cuda.empty_cache()
         inversion = run_inversion(args, world, rank, local)
 
+    multiplication = None
+    if not args.no_multiplication:
+        multiplication = run_multiplication(args, world, rank, local)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         kind, t, ceta = cpu_reference_solve_seconds(CPU_SAMPLE_N)
@@ -787,6 +857,7 @@ def run_b200(args, world, rank, local):
             "breakdown_one_step": breakdown,
             "batched": batched,
             "inversion": inversion,
+            "multiplication": multiplication,
             "clocks": clk,
             "peaks": peaks,
         }

@@ -290,6 +290,35 @@ static void test_inversion_determinant()
     CHECK(threw == 4, "inversion / determinant argument checks throw");
 }
 
+// batched_matrix_multiplication: each entry the fma chain over k from zero
+static void test_batched_multiplication()
+{
+    const int dim = 37, count = 4;
+    auto      a = random_matrix(count * dim, dim, 21);
+    auto      b = random_matrix(count * dim, dim, 22);
+    dbuf<double> da(a.size()), db(b.size()), dc(a.size());
+    da.up(a);
+    db.up(b);
+    linalg::batched_matrix_multiplication(dim, count, da.p, db.p, dc.p);
+    cudaDeviceSynchronize();
+    auto c  = dc.down();
+    bool ok = true;
+    for (int q = 0; q < count; ++q)
+        for (int i = 0; i < dim; ++i)
+            for (int j = 0; j < dim; ++j)
+            {
+                double s = 0;
+                for (int k = 0; k < dim; ++k)
+                    s = std::fma(a[(size_t)q * dim * dim + i * dim + k], b[(size_t)q * dim * dim + k * dim + j], s);
+                ok = ok && s == c[(size_t)q * dim * dim + i * dim + j];
+            }
+    CHECK(ok, "batched_matrix_multiplication bit-identical to the fma chain");
+    int threw = 0;
+    try { linalg::batched_matrix_multiplication(0, count, da.p, db.p, dc.p); } catch (const std::invalid_argument&) { ++threw; }
+    try { linalg::batched_matrix_multiplication(dim, count, static_cast<const double*>(nullptr), db.p, dc.p); } catch (const std::invalid_argument&) { ++threw; }
+    CHECK(threw == 2, "batched_matrix_multiplication argument checks throw");
+}
+
 int main()
 {
     test_lu();
@@ -299,6 +328,7 @@ int main()
     test_validation();
     test_singular_status();
     test_inversion_determinant();
+    test_batched_multiplication();
     std::printf("%s (%d failures)\n", g_fail ? "FAILED" : "ALL PASSED", g_fail);
     return g_fail ? 1 : 0;
 }
