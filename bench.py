@@ -187,7 +187,7 @@ def measured_peaks() -> dict:
 # inversion / determinant (LU modes): this library vs the reference's
 # CUDA_BLAS path (baseline/_ref) at the same order
 # ---------------------------------------------------------------------------
-def inversion_gemm_flops(n: int, nb: int = 256, sub: int = 64) -> int:
+def inversion_gemm_flops(n: int, nb: int = 512, sub: int = 64) -> int:
     """Flops of the inversion's GEMM updates (k_dmma_update launches) for
     order n: the block-row sub-updates and the big forward / backward ones."""
     fl = 0

@@ -10,7 +10,8 @@
 //
 // Inversion, A^-1 = U^-1 L^-1 P:
 //   1. W = I (the n x n workspace);
-//   2. W = L^-1 W, forward substitution in row blocks of kNB: the block row
+//   2. W = L^-1 W, forward substitution in row blocks of kNB (512: deeper
+//      GEMM updates run closer to the tensor pipe's rate): the block row
 //      is solved against L's unit diagonal block (block_solve),
 //      then every row below it is updated by one GEMM, C -= A B with
 //      A = L[below, block], B = W[block, :], restricted to the columns left
@@ -49,7 +50,7 @@ namespace b200la
 namespace inv
 {
 
-constexpr int kNB      = 256;  // rows per substitution block (GEMM depth)
+constexpr int kNB      = 512;  // rows per substitution block (GEMM depth)
 constexpr int kTile    = 128;  // GEMM tile, rows and columns
 constexpr int kThreads = 256;  // 8 warps: 2 (rows) x 4 (columns), warp tile 64 x 32
 constexpr int kStages  = 3;    // cp.async pipeline depth
