@@ -1,6 +1,6 @@
 /*
  * extern "C" wrappers over the reference's own CUDA_BLAS (cuSOLVER) LU solve,
- * linear_solver<double, linalg_backend::CUDA_BLAS> in LU mode, and its
+ * linear_solver<double, linalg_backend::CUDA_BLAS> in LU and Cholesky modes, and its
  * CUDA_BLAS inversion and determinant in LU mode, so bench.py can time the
  * reference's GPU backend beside this library.  Compiled together with the
  * reference's sources (src/matrix_operation/gpu/cublas/{linear_solver,
@@ -58,6 +58,37 @@ int ref_cublas_dgesv(double* m, int64_t* pivot, int64_t n, double* x, void* ws, 
     {
         linalg::linear_solver<double, linalg_backend::CUDA_BLAS>::apply(m, reinterpret_cast<linalg_int*>(pivot), n,
             x, linear_solver_type::LU_LINEAR_SOLVER, ws, ws_bytes, stream);
+        return 0;
+    }
+    catch (const std::exception& e)
+    {
+        g_err = e.what();
+        return -1;
+    }
+}
+
+/* linear_solver<double, CUDA_BLAS> in CHOLESKY_LINEAR_SOLVER mode (cuSOLVER
+ * potrf + potrs); pivot is unused by that mode. */
+size_t ref_cublas_dcholesky_solve_workspace_size(int64_t n)
+{
+    try
+    {
+        return linalg::linear_solver<double, linalg_backend::CUDA_BLAS>::workspace_size(
+            n, linear_solver_type::CHOLESKY_LINEAR_SOLVER);
+    }
+    catch (const std::exception& e)
+    {
+        g_err = e.what();
+        return 0;
+    }
+}
+
+int ref_cublas_dcholesky_solve(double* m, int64_t n, double* x, void* ws, size_t ws_bytes, void* stream)
+{
+    try
+    {
+        linalg::linear_solver<double, linalg_backend::CUDA_BLAS>::apply(m, nullptr, n, x,
+            linear_solver_type::CHOLESKY_LINEAR_SOLVER, ws, ws_bytes, stream);
         return 0;
     }
     catch (const std::exception& e)

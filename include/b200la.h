@@ -48,6 +48,8 @@ typedef enum b200la_status
  * (include/matrix_operation/linear_solver.h:15-21). */
 #define B200LA_LU_LINEAR_SOLVER 1
 #define B200LA_LU_UPFRONT_LINEAR_SOLVER 2
+#define B200LA_CHOLESKY_LINEAR_SOLVER 3
+#define B200LA_CHOLESKY_UPFRONT_LINEAR_SOLVER 4
 
 B200LA_API const char* b200la_last_error(void);
 B200LA_API const char* b200la_status_string(int status);
@@ -100,15 +102,34 @@ B200LA_API int b200la_sgetrf_async(float* m, int64_t n, int64_t* pivot, void* wo
  * returns B200LA_SUCCESS / B200LA_SINGULAR / B200LA_DEVICE_TIMEOUT. */
 B200LA_API int b200la_workspace_status(const void* workspace, int* info, void* stream);
 
-/* ---- linear_solver (LU modes) --------------------------------------------
+/* ---- cholesky_decomposition ------------------------------------------------
+ * Replaces cholesky_decomposition<T, Backend>::apply / ::workspace_size
+ * (include/matrix_operation/cholesky_decomposition.h; NATIVE
+ * src/matrix_operation/cpu/native/cholesky_decomposition_native.cpp): m
+ * (n x n row-major, symmetric positive definite; the lower triangle is read)
+ * becomes L (upper == 0, zeros above) or U = L^T (upper != 0, zeros below),
+ * bit-identical to the reference.  info: HOST int, may be NULL; 0 or the
+ * 1-based index of the first non-positive pivot (the matrix is then left as
+ * the reference leaves it).  Workspace: b200la_dgetrf_workspace_size(n).
+ * Synchronizes `stream`.  Returns B200LA_SUCCESS, B200LA_SINGULAR (not
+ * positive definite) or an error. */
+B200LA_API int b200la_dpotrf(double* m, int64_t n, int upper, void* workspace, size_t workspace_bytes,
+    int* info, void* stream);
+B200LA_API int b200la_spotrf(float* m, int64_t n, int upper, void* workspace, size_t workspace_bytes,
+    int* info, void* stream);
+
+/* ---- linear_solver ---------------------------------------------------------
  * Replaces linear_solver<T, Backend>::apply / ::workspace_size
  * (include/matrix_operation/linear_solver.h:46-64; NATIVE semantics of
  * src/matrix_operation/cpu/native/linear_solver_native.cpp:149-191).
  * mode B200LA_LU_LINEAR_SOLVER factors m in place (pivot written) and then
  * solves, unless the factorization found an exact zero pivot, in which case x
  * is left unchanged; B200LA_LU_UPFRONT_LINEAR_SOLVER reuses m and pivot as
- * given.  x: n device values, overwritten with the solution.  Asynchronous
- * on `stream`. */
+ * given.  B200LA_CHOLESKY_LINEAR_SOLVER factors m in place (lower, as
+ * b200la_dpotrf) and solves unless it is not positive definite;
+ * B200LA_CHOLESKY_UPFRONT_LINEAR_SOLVER solves with the lower factor in m
+ * (pivot unused).  x: n device values, overwritten with the solution.
+ * Asynchronous on `stream`. */
 B200LA_API size_t b200la_dgesv_workspace_size(int64_t n, int mode);
 B200LA_API size_t b200la_sgesv_workspace_size(int64_t n, int mode);
 B200LA_API int    b200la_dgesv(double* m, int64_t* pivot, int64_t n, double* x, int mode,

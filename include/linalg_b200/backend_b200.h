@@ -11,8 +11,13 @@
  *  - lu_decomposition synchronizes `stream` and writes the host `info`;
  *  - linear_solver honours the caller's pivots in LU_UPFRONT mode and, in
  *    LU mode, leaves x unchanged when U is exactly singular;
- *  - the Cholesky modes of linear_solver, inversion and determinant are not
- *    provided by this backend (std::invalid_argument);
+ *  - cholesky_decomposition (lower and upper) and the Cholesky modes of
+ *    linear_solver are provided (factors bit-identical to NATIVE);
+ *    cholesky_decomposition::apply synchronizes its stream and writes info
+ *    to host memory before it returns (the host backends' contract), and
+ *    returns false when the matrix is not positive definite; the Cholesky
+ *    modes of inversion and determinant and apply_aad are not provided
+ *    (std::invalid_argument);
  *  - inversion and determinant honour LU_UPFRONT (m and pivot are the
  *    caller's factors) and, in LU mode, accept a null pivot (CUDA_BLAS's
  *    contract) by keeping the pivots in the workspace; inversion is
@@ -31,6 +36,19 @@
 
 namespace linalg
 {
+template <> bool cholesky_decomposition<double, linalg_backend::B200>::apply(double*, linalg_int,
+    cholesky_decomposition_enum, void*, size_t, int*, void*);
+template <> bool cholesky_decomposition<float, linalg_backend::B200>::apply(float*, linalg_int,
+    cholesky_decomposition_enum, void*, size_t, int*, void*);
+template <> bool cholesky_decomposition<double, linalg_backend::B200>::apply_aad(double*, const double*,
+    linalg_int, cholesky_decomposition_enum, double*);
+template <> bool cholesky_decomposition<float, linalg_backend::B200>::apply_aad(float*, const float*,
+    linalg_int, cholesky_decomposition_enum, float*);
+template <> size_t cholesky_decomposition<double, linalg_backend::B200>::workspace_size(linalg_int,
+    cholesky_decomposition_enum);
+template <> size_t cholesky_decomposition<float, linalg_backend::B200>::workspace_size(linalg_int,
+    cholesky_decomposition_enum);
+
 template <> bool lu_decomposition<double, linalg_backend::B200>::apply(double*, linalg_int,
     linalg_int*, void*, size_t, int*, void*);
 template <> bool lu_decomposition<float, linalg_backend::B200>::apply(float*, linalg_int,

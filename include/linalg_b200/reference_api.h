@@ -10,6 +10,7 @@
  *   include/matrix_operation/inversion.h:15-53
  *   include/matrix_operation/determinant.h
  *   include/matrix_operation/multiplication_batched.h
+ *   include/matrix_operation/cholesky_decomposition.h:15-94
  * Names, argument order, default arguments and meaning are the reference's;
  * that is what makes the backend a drop-in.  Inside the reference tree define
  * LINALG_B200_USE_REFERENCE_HEADERS and add B200 as the last enumerator of
@@ -23,6 +24,7 @@
 #if defined(LINALG_B200_USE_REFERENCE_HEADERS)
 #include "include/common/backend.h"
 #include "include/common/types.h"
+#include "include/matrix_operation/cholesky_decomposition.h"
 #include "include/matrix_operation/determinant.h"
 #include "include/matrix_operation/inversion.h"
 #include "include/matrix_operation/linear_solver.h"
@@ -64,6 +66,21 @@ enum class linear_solver_type : std::uint8_t
     LU_UPFRONT_LINEAR_SOLVER       = 2,
     CHOLESKY_LINEAR_SOLVER         = 3,
     CHOLESKY_UPFRONT_LINEAR_SOLVER = 4,
+};
+
+enum class cholesky_decomposition_enum : char
+{
+    LOWER_TRIANGULAR = 'L',
+    UPPER_TRIANGULAR = 'U'
+};
+
+template <typename T, linalg_backend Backend> struct cholesky_decomposition
+{
+    LINALG_API static bool apply(T* C, linalg_int lda, cholesky_decomposition_enum type, void* workspace,
+        size_t workspace_size, int* info = nullptr, void* stream = nullptr);
+    LINALG_API static bool apply_aad(T* L_aad, const T* L, linalg_int lda, cholesky_decomposition_enum type,
+        T* A_aad);
+    LINALG_API static size_t workspace_size(linalg_int lda, cholesky_decomposition_enum type);
 };
 
 template <typename T, linalg_backend Backend> struct lu_decomposition

@@ -7,10 +7,15 @@ path; importing works without it, the first call raises if it is missing.
 from . import workloads  # noqa: F401
 from ._lib import B200Error, B200InvalidArgument  # noqa: F401
 from .api import (  # noqa: F401
+    CHOLESKY_LINEAR_SOLVER,
+    CHOLESKY_UPFRONT_LINEAR_SOLVER,
+    LOWER_TRIANGULAR,
     LU_LINEAR_SOLVER,
     LU_UPFRONT_LINEAR_SOLVER,
+    UPPER_TRIANGULAR,
     MixedSolver,
     batched_matrix_multiplication,
+    cholesky_decomposition,
     det,
     determinant,
     gemm,
@@ -23,6 +28,7 @@ from .api import (  # noqa: F401
     linear_solver,
     lu_decomposition,
     multiplication,
+    potrf,
     solve_mixed,
     triangular_solver,
     trsm,

@@ -24,6 +24,8 @@ NOT_SUPPORTED = -5
 
 LU_LINEAR_SOLVER = 1
 LU_UPFRONT_LINEAR_SOLVER = 2
+CHOLESKY_LINEAR_SOLVER = 3
+CHOLESKY_UPFRONT_LINEAR_SOLVER = 4
 
 _i64 = ctypes.c_int64
 _i32 = ctypes.c_int
@@ -70,6 +72,8 @@ SIGNATURES: dict[str, tuple] = {
     "b200la_sgemm_workspace_size": (_sz, [_i64, _i64, _i64]),
     "b200la_dgemm": (_i32, [_i32, _i32, _i64, _i64, _i64, _d, _p, _i64, _p, _i64, _d, _p, _i64, _p, _sz, _p]),
     "b200la_sgemm": (_i32, [_i32, _i32, _i64, _i64, _i64, _f, _p, _i64, _p, _i64, _f, _p, _i64, _p, _sz, _p]),
+    "b200la_dpotrf": (_i32, [_p, _i64, _i32, _p, _sz, _p, _p]),
+    "b200la_spotrf": (_i32, [_p, _i64, _i32, _p, _sz, _p, _p]),
     "b200la_dgemm_batched": (_i32, [_i64, _i64, _p, _p, _p, _p]),
     "b200la_sgemm_batched": (_i32, [_i64, _i64, _p, _p, _p, _p]),
     "b200la_refine_default_options": (None, [_p]),

@@ -26,6 +26,10 @@ from . import _lib
 
 LU_LINEAR_SOLVER = _lib.LU_LINEAR_SOLVER
 LU_UPFRONT_LINEAR_SOLVER = _lib.LU_UPFRONT_LINEAR_SOLVER
+CHOLESKY_LINEAR_SOLVER = _lib.CHOLESKY_LINEAR_SOLVER
+CHOLESKY_UPFRONT_LINEAR_SOLVER = _lib.CHOLESKY_UPFRONT_LINEAR_SOLVER
+LOWER_TRIANGULAR = "L"
+UPPER_TRIANGULAR = "U"
 
 
 def _prefix(dtype: torch.dtype) -> str:
@@ -78,8 +82,30 @@ class lu_decomposition:
         return st == _lib.SUCCESS, int(info.value)
 
 
+class cholesky_decomposition:
+    """cholesky_decomposition<T, B200> (include/matrix_operation/cholesky_decomposition.h)."""
+
+    @staticmethod
+    def workspace_size(lda: int, type: str = LOWER_TRIANGULAR, dtype=torch.float64) -> int:
+        return int(getattr(_lib.load(), f"b200la_{_prefix(dtype)}getrf_workspace_size")(lda))
+
+    @staticmethod
+    def apply(C: torch.Tensor, lda: int, type: str, workspace: torch.Tensor, workspace_size: int,
+              stream=None):
+        """Factor C in place (type "L" or "U"); returns (ok, info) like the
+        reference's bool and info.  Synchronizes the stream."""
+        if type not in (LOWER_TRIANGULAR, UPPER_TRIANGULAR):
+            raise _lib.B200InvalidArgument(_lib.INVALID_ARGUMENT, "Unsupported enum type!")
+        info = ctypes.c_int(-1)
+        f = getattr(_lib.load(), f"b200la_{_prefix(C.dtype)}potrf")
+        st = f(_ptr(C), lda, 1 if type == UPPER_TRIANGULAR else 0, _ptr(workspace), workspace_size,
+               ctypes.addressof(info), _stream(stream))
+        _lib.check(st, allow=(_lib.SUCCESS, _lib.SINGULAR))
+        return st == _lib.SUCCESS, int(info.value)
+
+
 class linear_solver:
-    """linear_solver<T, B200>, LU modes (include/matrix_operation/linear_solver.h:26-65)."""
+    """linear_solver<T, B200>, LU and Cholesky modes (include/matrix_operation/linear_solver.h:26-65)."""
 
     @staticmethod
     def workspace_size(lda: int, type: int = LU_LINEAR_SOLVER, dtype=torch.float64) -> int:
@@ -189,7 +215,10 @@ def getrf(m: torch.Tensor, stream=None):
 
 def gesv(m: torch.Tensor, x: torch.Tensor, pivot: torch.Tensor | None = None,
          type: int = LU_LINEAR_SOLVER, stream=None):
-    """linear_solver LU modes in place on (m, x).  Returns the pivot tensor."""
+    """linear_solver in place on (m, x): LU modes (pivot filled or, in
+    LU_UPFRONT mode, read) and Cholesky modes (m's lower triangle factored
+    or, in CHOLESKY_UPFRONT mode, read; pivot unused).  Returns the pivot
+    tensor."""
     n = m.shape[0]
     if pivot is None:
         pivot = torch.empty(n, dtype=torch.int64, device=m.device)
@@ -197,6 +226,16 @@ def gesv(m: torch.Tensor, x: torch.Tensor, pivot: torch.Tensor | None = None,
     ws = workspace(nbytes, m.device)
     linear_solver.apply(m, pivot, n, x, type, ws, ws.numel(), stream)
     return pivot
+
+
+def potrf(m: torch.Tensor, upper: bool = False, stream=None):
+    """cholesky_decomposition in place on m; returns info (0 or the 1-based
+    index of the first non-positive pivot)."""
+    n = m.shape[0]
+    ws = workspace(cholesky_decomposition.workspace_size(n, dtype=m.dtype), m.device)
+    _, info = cholesky_decomposition.apply(m, n, UPPER_TRIANGULAR if upper else LOWER_TRIANGULAR, ws,
+                                           ws.numel(), stream)
+    return info
 
 
 def getrs(lu: torch.Tensor, pivot: torch.Tensor, x: torch.Tensor, stream=None):

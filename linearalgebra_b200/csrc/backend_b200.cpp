@@ -29,7 +29,56 @@ int check_status(int st)
 }
 
 int64_t* pv(linalg_int* p) { return reinterpret_cast<int64_t*>(p); }
+
+// 0 lower, 1 upper; any other enum value reaches the C ABI as 2, which
+// rejects it ("Unsupported enum type!", as cholesky_decomposition_native.cpp)
+int triangle(cholesky_decomposition_enum type)
+{
+    return type == cholesky_decomposition_enum::LOWER_TRIANGULAR   ? 0
+           : type == cholesky_decomposition_enum::UPPER_TRIANGULAR ? 1
+                                                                   : 2;
+}
 }  // namespace
+
+// ---- cholesky_decomposition -------------------------------------------------
+template <>
+bool cholesky_decomposition<double, linalg_backend::B200>::apply(double* C, linalg_int lda,
+    cholesky_decomposition_enum type, void* workspace, size_t workspace_size, int* info, void* stream)
+{
+    return check_status(b200la_dpotrf(C, lda, triangle(type), workspace, workspace_size, info, stream)) ==
+           B200LA_SUCCESS;
+}
+template <>
+bool cholesky_decomposition<float, linalg_backend::B200>::apply(float* C, linalg_int lda,
+    cholesky_decomposition_enum type, void* workspace, size_t workspace_size, int* info, void* stream)
+{
+    return check_status(b200la_spotrf(C, lda, triangle(type), workspace, workspace_size, info, stream)) ==
+           B200LA_SUCCESS;
+}
+template <>
+bool cholesky_decomposition<double, linalg_backend::B200>::apply_aad(double*, const double*, linalg_int,
+    cholesky_decomposition_enum, double*)
+{
+    throw std::invalid_argument("cholesky_decomposition<double, B200>::apply_aad: not provided by this backend");
+}
+template <>
+bool cholesky_decomposition<float, linalg_backend::B200>::apply_aad(float*, const float*, linalg_int,
+    cholesky_decomposition_enum, float*)
+{
+    throw std::invalid_argument("cholesky_decomposition<float, B200>::apply_aad: not provided by this backend");
+}
+template <>
+size_t cholesky_decomposition<double, linalg_backend::B200>::workspace_size(linalg_int lda,
+    cholesky_decomposition_enum)
+{
+    return b200la_dgetrf_workspace_size(lda);
+}
+template <>
+size_t cholesky_decomposition<float, linalg_backend::B200>::workspace_size(linalg_int lda,
+    cholesky_decomposition_enum)
+{
+    return b200la_sgetrf_workspace_size(lda);
+}
 
 // ---- lu_decomposition -------------------------------------------------------
 template <>

@@ -62,6 +62,14 @@ B200LA_API int b200la_sgesv(float* m, int64_t* pivot, int64_t n, float* x, int m
     return gesv<float>(m, pivot, n, x, mode, ws, bytes, stream);
 }
 
+B200LA_API int b200la_dpotrf(double* m, int64_t n, int upper, void* ws, size_t bytes, int* info, void* stream)
+{
+    return potrf<double>(m, n, upper, ws, bytes, info, stream);
+}
+B200LA_API int b200la_spotrf(float* m, int64_t n, int upper, void* ws, size_t bytes, int* info, void* stream)
+{
+    return potrf<float>(m, n, upper, ws, bytes, info, stream);
+}
 B200LA_API int b200la_dgemm_batched(int64_t dim, int64_t count, const double* a, const double* b, double* c,
     void* stream)
 {

@@ -10,6 +10,7 @@
 #include <cstdlib>
 #include <mutex>
 
+#include "cholesky.cuh"
 #include "dmma.cuh"
 #include "lu_kernels.cuh"
 #include "solve_kernels.cuh"
@@ -91,6 +92,9 @@ template <typename T> int ensure_kernel_attributes()
         k_dmma_update<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDmSmem));
     B200LA_CUDA(cudaFuncSetAttribute(k_dmma_band<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBandSmem));
     B200LA_CUDA(cudaFuncSetAttribute(k_dmma_gemm<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDmSmem));
+    B200LA_CUDA(cudaFuncSetAttribute(k_chol_diag<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)chol_smem_bytes<T>()));
+    B200LA_CUDA(cudaFuncSetAttribute(k_chol_trsm<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)chol_smem_bytes<T>()));
+    B200LA_CUDA(cudaFuncSetAttribute(k_chol_syrk<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)chol_smem_bytes<T>()));
     B200LA_CUDA(cudaFuncSetAttribute(k_dmma_gemm<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDmSmem));
     B200LA_CUDA(cudaFuncSetAttribute(k_gemm<T, false, false>,
         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gemm_smem_bytes<T>()));
@@ -672,9 +676,72 @@ int enqueue_getrs(const T* lu, const int64_t* pivot, int n, int nrhs, T* x, int6
     return B200LA_SUCCESS;
 }
 
+// Blocked lower Cholesky of m (n x n, row-major) in the reference's order
+// (cholesky.cuh); upper: then transposed into the upper triangle.  The status
+// block gets the first non-positive pivot; later kernels are gated on it.
+template <typename T> int enqueue_potrf(T* m, int n, bool upper, DeviceStatus* st, cudaStream_t s)
+{
+    prof_begin(KC_PANEL, s);
+    k_status_init<<<1, 32, 0, s>>>(st, nullptr);
+    prof_end(KC_PANEL, s);
+    B200LA_LAUNCH_CHECK();
+    const size_t smem = chol_smem_bytes<T>();
+    for (int k = 0; k < n; k += kCholNB)
+    {
+        const int bs    = n - k < kCholNB ? n - k : kCholNB;
+        const int below = n - k - bs;
+        prof_begin(KC_PANEL, s);
+        k_chol_diag<T><<<1, kCholNB, smem, s>>>(m, n, k, bs, st);
+        prof_end(KC_PANEL, s);
+        B200LA_LAUNCH_CHECK();
+        if (below == 0)
+        {
+            break;
+        }
+        prof_begin(KC_SWAP, s);
+        k_chol_zero<T><<<grid_1d((int64_t)bs * below, 256), 256, 0, s>>>(m, n, k, bs, st);
+        prof_end(KC_SWAP, s);
+        B200LA_LAUNCH_CHECK();
+        prof_begin(KC_SWAP, s);
+        k_chol_trsm<T><<<(below + kCholNB - 1) / kCholNB, kCholNB, smem, s>>>(m, n, k, bs, st);
+        prof_end(KC_SWAP, s);
+        B200LA_LAUNCH_CHECK();
+        const unsigned tiles = (unsigned)((below + kSyrkTile - 1) / kSyrkTile);
+        prof_begin(KC_TRAILING, s);
+        k_chol_syrk<T><<<dim3(tiles, tiles), 256, smem, s>>>(m, n, k, bs, st);
+        prof_end(KC_TRAILING, s);
+        B200LA_LAUNCH_CHECK();
+    }
+    if (upper)
+    {
+        prof_begin(KC_SWAP, s);
+        k_chol_to_upper<T><<<grid_1d((int64_t)n * n, 256), 256, 0, s>>>(m, n, st);
+        prof_end(KC_SWAP, s);
+        B200LA_LAUNCH_CHECK();
+    }
+    prof_begin(KC_PANEL, s);
+    k_status_finish<<<1, 32, 0, s>>>(st);
+    prof_end(KC_PANEL, s);
+    B200LA_LAUNCH_CHECK();
+    return B200LA_SUCCESS;
+}
+
+// Solve with a lower Cholesky factor in place on x (n x nrhs, row stride
+// ldx): L y = x, then L^T x = y.  Gated on the factorization's status.
+template <typename T>
+int enqueue_potrs(const T* l, int n, int nrhs, T* x, int64_t ldx, const DeviceStatus* gate, cudaStream_t s)
+{
+    int rc = enqueue_trsm_inplace<T>(false, false, false, n, nrhs, l, n, x, ldx, gate, s);
+    if (rc != B200LA_SUCCESS)
+    {
+        return rc;
+    }
+    return enqueue_trsm_inplace<T>(false, true, false, n, nrhs, l, n, x, ldx, gate, s);
+}
+
 template <typename T> size_t gesv_ws_size(int64_t n, int mode)
 {
-    if (n <= 0 || (mode != B200LA_LU_LINEAR_SOLVER && mode != B200LA_LU_UPFRONT_LINEAR_SOLVER))
+    if (n <= 0 || mode < B200LA_LU_LINEAR_SOLVER || mode > B200LA_CHOLESKY_UPFRONT_LINEAR_SOLVER)
     {
         return 0;
     }
@@ -695,12 +762,12 @@ int gesv(T* m, int64_t* pivot, int64_t n, T* x, int mode, void* ws, size_t bytes
     {
         return set_error(B200LA_INVALID_ARGUMENT, "linear_solver::apply: lda must be positive");
     }
-    if (mode != B200LA_LU_LINEAR_SOLVER && mode != B200LA_LU_UPFRONT_LINEAR_SOLVER)
+    if (mode < B200LA_LU_LINEAR_SOLVER || mode > B200LA_CHOLESKY_UPFRONT_LINEAR_SOLVER)
     {
-        return set_error(B200LA_NOT_SUPPORTED,
-            "linear_solver: only the LU modes are provided by this backend (mode %d)", mode);
+        return set_error(B200LA_INVALID_ARGUMENT, "unsupported linear_solver_type (%d)", mode);
     }
-    if (pivot == nullptr)
+    const bool chol = mode == B200LA_CHOLESKY_LINEAR_SOLVER || mode == B200LA_CHOLESKY_UPFRONT_LINEAR_SOLVER;
+    if (!chol && pivot == nullptr)
     {
         return set_error(B200LA_INVALID_ARGUMENT, "linear_solver: LU modes need a pivot array");
     }
@@ -723,6 +790,29 @@ int gesv(T* m, int64_t* pivot, int64_t n, T* x, int mode, void* ws, size_t bytes
     GetrfPlan<T>  gp = plan_getrf<T>(a);
     SolvePlan<T>  sp = plan_solve<T>(a, n, 1);
     cudaStream_t  s  = as_stream(stream);
+    if (chol)
+    {
+        // linear_solver_native.cpp: CHOLESKY factors (lower) and solves only
+        // if the matrix is positive definite; CHOLESKY_UPFRONT solves with
+        // the given lower factor
+        if (mode == B200LA_CHOLESKY_LINEAR_SOLVER)
+        {
+            st = enqueue_potrf<T>(m, (int)n, false, gp.st, s);
+        }
+        else
+        {
+            prof_begin(KC_SOLVE, s);
+            k_status_init<<<1, 32, 0, s>>>(gp.st, nullptr);
+            prof_end(KC_SOLVE, s);
+            B200LA_LAUNCH_CHECK();
+            st = B200LA_SUCCESS;
+        }
+        if (st != B200LA_SUCCESS)
+        {
+            return st;
+        }
+        return enqueue_potrs<T>(m, (int)n, 1, x, 1, gp.st, s);
+    }
     if (mode == B200LA_LU_LINEAR_SOLVER)
     {
         st = enqueue_getrf<T>(m, (int)n, pivot, gp, s);
@@ -740,6 +830,47 @@ int gesv(T* m, int64_t* pivot, int64_t n, T* x, int mode, void* ws, size_t bytes
         return st;
     }
     return enqueue_getrs<T>(m, pivot, (int)n, 1, x, 1, sp, gp.st, gp.st, s);
+}
+
+template <typename T>
+int potrf(T* m, int64_t n, int upper, void* ws, size_t bytes, int* info, void* stream)
+{
+    if (m == nullptr)
+    {
+        return set_error(B200LA_INVALID_ARGUMENT, "cholesky_decomposition::apply: C must not be null");
+    }
+    if (n <= 0)
+    {
+        return set_error(B200LA_INVALID_ARGUMENT, "cholesky_decomposition::apply: lda must be positive");
+    }
+    if (upper != 0 && upper != 1)
+    {
+        return set_error(B200LA_INVALID_ARGUMENT, "Unsupported enum type!");
+    }
+    if (n > INT_MAX / 2)
+    {
+        return set_error(B200LA_NOT_SUPPORTED, "cholesky_decomposition: order too large");
+    }
+    const size_t need = getrf_ws_size<T>(n);
+    if (ws == nullptr || bytes < need)
+    {
+        return set_error(B200LA_WORKSPACE_TOO_SMALL,
+            "cholesky_decomposition: workspace is null or too small (%zu < %zu bytes)", bytes, need);
+    }
+    int st = prepare<T>();
+    if (st != B200LA_SUCCESS)
+    {
+        return st;
+    }
+    Arena        a(ws, bytes);
+    GetrfPlan<T> p = plan_getrf<T>(a);
+    cudaStream_t s = as_stream(stream);
+    st             = enqueue_potrf<T>(m, (int)n, upper != 0, p.st, s);
+    if (st != B200LA_SUCCESS)
+    {
+        return st;
+    }
+    return read_status(p.st, info, s);
 }
 
 template <typename T> size_t getrs_ws_size(int64_t n, int64_t nrhs)

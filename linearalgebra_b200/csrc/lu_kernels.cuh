@@ -1283,7 +1283,10 @@ static __global__ void k_status_init(DeviceStatus* st, PermList* perm)
         st->error_site = 0;
         st->first_zero = -1;
         st->info       = 0;
-        perm->count    = 0;
+        if (perm != nullptr)
+        {
+            perm->count = 0;
+        }
     }
 }
 

@@ -118,6 +118,19 @@ def spd_product(n: int, seed: int, dtype=np.float64) -> np.ndarray:
     return (r.astype(np.float64) @ r.T.astype(np.float64)).astype(dtype)
 
 
+def spd_matrix(n: int, seed: int, dtype=np.float64, fail_row: int = -1) -> np.ndarray:
+    """A = R R^T + n I with R iid N(0,1) (symmetric positive definite; the
+    product summed in float64, then cast).  fail_row >= 0: that diagonal
+    entry set to -1, so the leading block of that order is positive
+    definite and the Cholesky pivot of that row is not."""
+    rng = np.random.default_rng(seed)
+    r = rng.standard_normal((n, n))
+    a = r @ r.T + n * np.eye(n)
+    if fail_row >= 0:
+        a[fail_row, fail_row] = -1.0
+    return a.astype(dtype)
+
+
 def determinant_known_answers() -> dict[str, tuple[list[float], float]]:
     """Diagonal matrices and their determinants, the LU-mode cases of the
     reference's determinant test (Testing/Cxx/TestDeterminant.cxx:84-127):

@@ -82,6 +82,9 @@ class Oracle:
                 f = getattr(self.lib, f"or_{t}gemm_batched")
                 f.argtypes = [_i64, _i64, _p, _p, _p]
                 f.restype = _int
+            f = getattr(self.lib, f"{pre}{t}potrf")
+            f.argtypes = [_p, _i64, _int, _p]
+            f.restype = _int
             f = getattr(self.lib, f"{pre}{t}getri")
             f.argtypes = [_p, _p, _i64, _int]
             f.restype = _int
@@ -143,6 +146,18 @@ class Oracle:
         if st < 0:
             raise ValueError(f"gemm rejected its arguments (status {st})")
         return c
+
+    def potrf(self, a: np.ndarray, upper: bool = False):
+        """cholesky_decomposition (lower, or upper) of a copy; returns
+        (factor, info): info 0, or the 1-based index of the first
+        non-positive pivot."""
+        m = np.ascontiguousarray(a).copy()
+        info = ctypes.c_int(-1)
+        st = getattr(self.lib, f"{self._pre}{self._t(m)}potrf")(_ptr(m), m.shape[0], int(upper),
+                                                              ctypes.addressof(info))
+        if st < 0:
+            raise ValueError(f"potrf rejected its arguments (status {st})")
+        return m, int(info.value)
 
     def gemm_batched(self, a: np.ndarray, b: np.ndarray) -> np.ndarray:
         """c_i = a_i b_i for (count, dim, dim) arrays, the reference CUDA

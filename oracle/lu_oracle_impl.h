@@ -264,9 +264,14 @@ void OR_FN(getrs)(const T* m, const int64_t* pivot, int64_t n, T* x)
     }
 }
 
-/* linear_solver LU modes, linear_solver_native.cpp:149-191: mode 1 factors
+int  OR_FN(potrf)(T* m, int64_t n, int upper, int* info);
+void OR_FN(potrs)(const T* m, int64_t n, T* x);
+
+/* linear_solver modes, linear_solver_native.cpp:149-191: mode 1 factors
  * then solves only if the factorization succeeded; mode 2 reuses the factors
- * and pivots.  Returns the getrf status for mode 1, 0 for mode 2. */
+ * and pivots; modes 3 and 4 are the Cholesky ones (factor lower, then
+ * solve if positive definite; solve with the given factor).  Returns the
+ * factorization status for modes 1 and 3, 0 for modes 2 and 4. */
 int OR_FN(gesv)(T* m, int64_t* pivot, int64_t n, T* x, int mode)
 {
     if (m == NULL || x == NULL || n <= 0)
@@ -285,6 +290,21 @@ int OR_FN(gesv)(T* m, int64_t* pivot, int64_t n, T* x, int mode)
     if (mode == 2)
     {
         OR_FN(getrs)(m, pivot, n, x);
+        return 0;
+    }
+    if (mode == 3)
+    {
+        /* linear_solver_native.cpp: factor (lower), solve only if it succeeded */
+        const int st = OR_FN(potrf)(m, n, 0, NULL);
+        if (st == 0)
+        {
+            OR_FN(potrs)(m, n, x);
+        }
+        return st;
+    }
+    if (mode == 4)
+    {
+        OR_FN(potrs)(m, n, x);
         return 0;
     }
     return -1;
@@ -392,6 +412,158 @@ T OR_FN(det)(T* m, int64_t* pivot, int64_t n, int mode, int* status)
         det *= m[i * n + i];
     }
     return det;
+}
+
+/* Reduction `sum -= a[j] * b[j]` over j in order, as the reference build
+ * compiles it (see dots_: full vectors of products rounded, then one half
+ * vector, subtracted one by one in order; the rest fused). */
+static T OR_CAT(dots_sub_, SUF)(T sum, const T* a, int64_t sa, const T* b, int64_t sb, int64_t count)
+{
+    const int64_t vec  = (int64_t)(32 / sizeof(T));
+    const int64_t half = vec / 2;
+    const int64_t main = count >= vec ? (count / vec) * vec : 0;
+    int64_t       j    = 0;
+    for (; j < main; ++j)
+    {
+        const T p = a[j * sa] * b[j * sb];
+        sum       = sum - p;
+    }
+    if (count - j >= half)
+    {
+        for (int64_t q = 0; q < half; ++q, ++j)
+        {
+            const T p = a[j * sa] * b[j * sb];
+            sum       = sum - p;
+        }
+    }
+    for (; j < count; ++j)
+    {
+        sum = OR_FMA(-a[j * sa], b[j * sb], sum);
+    }
+    return sum;
+}
+
+/* Unblocked Cholesky of the n x n diagonal block at A (row stride lda):
+ * cholesky_decomposition_native.cpp (cholesky_decomposition_scalar_impl),
+ * row by row: a_ij = (a_ij - dot(a_i, a_j, j)) / a_jj for j < i (a_ji = 0),
+ * then a_ii = sqrt(a_ii - dot(a_i, a_i, i)); returns i + 1 at the first
+ * non-positive pivot, else 0. */
+static int64_t OR_CAT(potf2_, SUF)(int64_t n, T* A, int64_t lda)
+{
+    for (int64_t i = 0; i < n; ++i)
+    {
+        T* ai = A + i * lda;
+        for (int64_t j = 0; j < i; ++j)
+        {
+            T*      aj  = A + j * lda;
+            const T sum = ai[j] - OR_CAT(dot_, SUF)(ai, aj, j);
+            ai[j]       = sum / aj[j];
+            aj[i]       = (T)0;
+        }
+        const T sum = ai[i] - OR_CAT(dot_, SUF)(ai, ai, i);
+        if (sum <= (T)0)
+        {
+            return i + 1;
+        }
+        ai[i] = (T)sqrt((double)sum);
+    }
+    return 0;
+}
+
+/* Blocked lower Cholesky of the row-major n x n matrix m (lda = n):
+ * cholesky_decomposition_native.cpp (cholesky_decomposition_blocked_lower,
+ * block 64, the non-vectorized trailing update): per block, the diagonal
+ * block by potf2, zeros right of it in its rows, A21 = A21 L11^-T row by row
+ * (row[j] = (row[j] - dot(row, l_j, j)) / l_jj), then for the trailing
+ * lower triangle t_ij -= dot(a21_i, a21_j, bs).  upper != 0: the factor is
+ * transposed into the upper triangle and the lower one cleared
+ * (cholesky_decomposition_apply_impl).  Returns 0, or the 1-based index of
+ * the first non-positive pivot (*info too). */
+int OR_FN(potrf)(T* m, int64_t n, int upper, int* info)
+{
+    if (m == NULL || n <= 0)
+    {
+        return -1;
+    }
+    int64_t rc = 0;
+    for (int64_t k = 0; k < n && rc == 0; k += 64)
+    {
+        const int64_t bs  = (n - k) < 64 ? (n - k) : 64;
+        T*            l11 = m + k * n + k;
+        const int64_t r   = OR_CAT(potf2_, SUF)(bs, l11, n);
+        if (r != 0)
+        {
+            rc = k + r;
+            break;
+        }
+        for (int64_t i = k; i < k + bs; ++i)
+        {
+            for (int64_t j = k + bs; j < n; ++j)
+            {
+                m[i * n + j] = (T)0;
+            }
+        }
+        const int64_t below = n - k - bs;
+        if (below == 0)
+        {
+            continue;
+        }
+        T* a21 = m + (k + bs) * n + k;
+        T* a22 = m + (k + bs) * n + k + bs;
+        for (int64_t r2 = 0; r2 < below; ++r2)
+        {
+            T* row = a21 + r2 * n;
+            for (int64_t j = 0; j < bs; ++j)
+            {
+                const T* lj  = l11 + j * n;
+                const T  sum = row[j] - OR_CAT(dot_, SUF)(row, lj, j);
+                row[j]       = sum / lj[j];
+            }
+        }
+        for (int64_t i = 0; i < below; ++i)
+        {
+            for (int64_t j = 0; j <= i; ++j)
+            {
+                a22[i * n + j] -= OR_CAT(dot_, SUF)(a21 + i * n, a21 + j * n, bs);
+            }
+        }
+    }
+    if (rc == 0 && upper)
+    {
+        for (int64_t i = 0; i < n; ++i)
+        {
+            for (int64_t j = 0; j < i; ++j)
+            {
+                m[j * n + i] = m[i * n + j];
+                m[i * n + j] = (T)0;
+            }
+        }
+    }
+    if (info)
+    {
+        *info = (int)rc;
+    }
+    return (int)rc;
+}
+
+/* Solve with a lower Cholesky factor: linear_solver_native.cpp
+ * (cholesky_solve): forward x_i = (x_i - sum_{j<i} l_ij x_j) / l_ii, then
+ * backward x_i = (x_i - sum_{j>i} l_ji x_j) / l_ii reading the factor's
+ * column i; both reductions round as the reference build compiles them
+ * (dots_sub_; the backward one's loads are strided, the rounding the same). */
+void OR_FN(potrs)(const T* m, int64_t n, T* x)
+{
+    for (int64_t i = 0; i < n; ++i)
+    {
+        const T* ri  = m + i * n;
+        const T  sum = OR_CAT(dots_sub_, SUF)(x[i], ri, 1, x, 1, i);
+        x[i]         = sum / ri[i];
+    }
+    for (int64_t i = n - 1; i >= 0; --i)
+    {
+        const T sum = OR_CAT(dots_sub_, SUF)(x[i], m + (i + 1) * n + i, n, x + i + 1, 1, n - i - 1);
+        x[i]        = sum / m[i * n + i];
+    }
 }
 
 /* Batched product c_i = a_i b_i of `count` packed dim x dim matrices:

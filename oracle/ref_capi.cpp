@@ -21,6 +21,7 @@
 #include <new>
 #include <vector>
 
+#include "include/matrix_operation/cholesky_decomposition.h"
 #include "include/matrix_operation/determinant.h"
 #include "include/matrix_operation/inversion.h"
 #include "include/matrix_operation/linear_solver.h"
@@ -131,6 +132,27 @@ int ref_gemm(int ta, int tb, int64_t rows, int64_t cols, int64_t depth, T alpha,
         return -1;
     }
 }
+template <typename T> int ref_potrf(T* m, int64_t n, int upper, int* info)
+{
+    try
+    {
+        int        local = -1;
+        const auto type  = upper ? linalg::cholesky_decomposition_enum::UPPER_TRIANGULAR
+                                 : linalg::cholesky_decomposition_enum::LOWER_TRIANGULAR;
+        const bool ok    = linalg::cholesky_decomposition<T, linalg_backend::NATIVE>::apply(m, n, type, nullptr, 0,
+            &local);
+        if (info)
+        {
+            *info = local;
+        }
+        return ok ? 0 : 1;
+    }
+    catch (...)
+    {
+        return -1;
+    }
+}
+
 template <typename T> int ref_getri(T* m, int64_t* pivot, int64_t n, int type)
 {
     try
@@ -211,6 +233,14 @@ int ref_sgemm(int ta, int tb, int64_t rows, int64_t cols, int64_t depth, float a
     const float* a, int64_t lda, const float* b, int64_t ldb, float beta, float* c, int64_t ldc)
 {
     return ref_gemm(ta, tb, rows, cols, depth, alpha, a, lda, b, ldb, beta, c, ldc);
+}
+int ref_dpotrf(double* m, int64_t n, int upper, int* info)
+{
+    return ref_potrf(m, n, upper, info);
+}
+int ref_spotrf(float* m, int64_t n, int upper, int* info)
+{
+    return ref_potrf(m, n, upper, info);
 }
 int ref_dgetri(double* m, int64_t* pivot, int64_t n, int type)
 {

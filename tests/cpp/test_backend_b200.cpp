@@ -111,8 +111,10 @@ static void test_linear_solver()
     for (auto& v : x_true) v = u(g);
     for (int i = 0; i < n; ++i)
         for (int j = 0; j < n; ++j) b[i] += a[i * n + j] * x_true[j];
-    for (auto mode : {linalg::linear_solver_type::LU_LINEAR_SOLVER})
+    for (auto mode : {linalg::linear_solver_type::LU_LINEAR_SOLVER,
+             linalg::linear_solver_type::CHOLESKY_LINEAR_SOLVER})
     {
+        const bool chol = mode == linalg::linear_solver_type::CHOLESKY_LINEAR_SOLVER;
         dbuf<double>     m(n * n), x(n);
         dbuf<linalg_int> piv(n);
         m.up(a);
@@ -126,16 +128,19 @@ static void test_linear_solver()
         auto xs = x.down();
         double e = 0;
         for (int i = 0; i < n; ++i) e = std::max(e, std::fabs(xs[i] - x_true[i]));
-        CHECK(e <= 1e-9 * n, "linear_solver LU on a stream");
-        // LU_UPFRONT reuses factors and pivots
+        CHECK(e <= 1e-9 * n, chol ? "linear_solver CHOLESKY on a stream" : "linear_solver LU on a stream");
+        // the UPFRONT modes reuse the factors (and, for LU, the pivots)
         x.up(b);
-        linalg::linear_solver<double, B>::apply(m.p, piv.p, n, x.p,
-            linalg::linear_solver_type::LU_UPFRONT_LINEAR_SOLVER, ws.p, bytes, s);
+        linalg::linear_solver<double, B>::apply(m.p, chol ? nullptr : piv.p, n, x.p,
+            chol ? linalg::linear_solver_type::CHOLESKY_UPFRONT_LINEAR_SOLVER
+                 : linalg::linear_solver_type::LU_UPFRONT_LINEAR_SOLVER,
+            ws.p, bytes, s);
         cudaStreamSynchronize(s);
         xs = x.down();
         e  = 0;
         for (int i = 0; i < n; ++i) e = std::max(e, std::fabs(xs[i] - x_true[i]));
-        CHECK(e <= 1e-9 * n, "linear_solver LU_UPFRONT reuses pivots");
+        CHECK(e <= 1e-9 * n, chol ? "linear_solver CHOLESKY_UPFRONT reuses the factor"
+                                  : "linear_solver LU_UPFRONT reuses pivots");
         cudaStreamDestroy(s);
     }
 }
@@ -291,6 +296,68 @@ static void test_inversion_determinant()
 }
 
 // batched_matrix_multiplication: each entry the fma chain over k from zero
+static void test_cholesky()
+{
+    const int n = 150;
+    auto      r = random_matrix(n, n, 17, -1, 1);
+    std::vector<double> a((size_t)n * n, 0.0);
+    for (int i = 0; i < n; ++i)
+        for (int j = 0; j < n; ++j)
+        {
+            double s = 0;
+            for (int k = 0; k < n; ++k) s += r[i * n + k] * r[j * n + k];
+            a[i * n + j] = s + (i == j ? n : 0.0);
+        }
+    using CD          = linalg::cholesky_decomposition<double, B>;
+    const auto   low  = linalg::cholesky_decomposition_enum::LOWER_TRIANGULAR;
+    const auto   up   = linalg::cholesky_decomposition_enum::UPPER_TRIANGULAR;
+    const size_t bytes = CD::workspace_size(n, low);
+    dbuf<unsigned char> ws(bytes);
+    dbuf<double>        dm(a.size());
+    for (auto type : {low, up})
+    {
+        dm.up(a);
+        int        info = -1;
+        const bool ok   = CD::apply(dm.p, n, type, ws.p, bytes, &info);
+        auto       f    = dm.down();
+        double     err = 0, other = 0;
+        for (int i = 0; i < n; ++i)
+            for (int j = 0; j < n; ++j)
+            {
+                double s = 0;  // (L L^T)_ij, or (U^T U)_ij
+                for (int k = 0; k < n; ++k)
+                    s += type == low ? f[i * n + k] * f[j * n + k] : f[k * n + i] * f[k * n + j];
+                err = std::fmax(err, std::fabs(s - a[i * n + j]));
+                if (type == low ? j > i : j < i) other = std::fmax(other, std::fabs(f[i * n + j]));
+            }
+        CHECK(ok && info == 0 && err <= 1e-11 * n && other == 0.0,
+            type == low ? "cholesky_decomposition LOWER: L L^T == A" : "cholesky_decomposition UPPER: U^T U == A");
+    }
+    std::vector<double> bad = a;
+    bad[40 * n + 40]        = -1.0;
+    dm.up(bad);
+    int info = 0;
+    CHECK(!CD::apply(dm.p, n, low, ws.p, bytes, &info) && info == 41,
+        "cholesky_decomposition: non-positive pivot -> false, info = row + 1");
+    bool threw = false;
+    try
+    {
+        CD::apply(dm.p, n, static_cast<linalg::cholesky_decomposition_enum>('X'), ws.p, bytes, &info);
+    }
+    catch (const std::invalid_argument&)
+    {
+        threw = true;
+    }
+    CHECK(threw, "cholesky_decomposition: unknown enum throws std::invalid_argument");
+    dbuf<float> f2(4);
+    f2.up(std::vector<float>{4.0f, 2.0f, 2.0f, 5.0f});
+    dbuf<unsigned char> fws(linalg::cholesky_decomposition<float, B>::workspace_size(2, low));
+    linalg::cholesky_decomposition<float, B>::apply(f2.p, 2, low, fws.p, fws.n, &info);
+    const auto l = f2.down();
+    CHECK(info == 0 && l[0] == 2.0f && l[1] == 0.0f && l[2] == 1.0f && l[3] == 2.0f,
+        "cholesky_decomposition<float>: [[4,2],[2,5]] -> [[2,0],[1,2]]");
+}
+
 static void test_batched_multiplication()
 {
     const int dim = 37, count = 4;
@@ -328,6 +395,7 @@ int main()
     test_validation();
     test_singular_status();
     test_inversion_determinant();
+    test_cholesky();
     test_batched_multiplication();
     std::printf("%s (%d failures)\n", g_fail ? "FAILED" : "ALL PASSED", g_fail);
     return g_fail ? 1 : 0;

@@ -6,9 +6,10 @@ Run from the repository root, where the reference build exists:
 
     make -f oracle/Makefile && python tests/golden/make_golden.py
 
-Writes tests/golden/lu_golden.npz (LU, solve, triangular solver, GEMM) and
+Writes tests/golden/lu_golden.npz (LU, solve, triangular solver, GEMM),
 tests/golden/inverse_golden.npz (inversion and determinant; `--inverse` writes
-only that one).  Every input is seeded (numpy PCG64) or a closed-form
+only that one) and tests/golden/cholesky_golden.npz (Cholesky factor and the
+Cholesky modes of linear_solver; `--cholesky` writes only that one).  Every input is seeded (numpy PCG64) or a closed-form
 known-answer matrix; each array's name says what it is.
 """
 from __future__ import annotations
@@ -28,6 +29,7 @@ from linearalgebra_b200.workloads import (  # noqa: E402
     determinant_known_answers,
     known_answer_matrices,
     random_matrix,
+    spd_matrix,
     spd_product,
     system,
     triangular_cases,
@@ -37,6 +39,8 @@ LU_SIZES = (1, 2, 3, 17, 63, 64, 65, 130, 200)
 
 OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "lu_golden.npz")
 OUT_INV = os.path.join(os.path.dirname(os.path.abspath(__file__)), "inverse_golden.npz")
+OUT_CHOL = os.path.join(os.path.dirname(os.path.abspath(__file__)), "cholesky_golden.npz")
+CHOL_SIZES = (1, 2, 3, 17, 63, 64, 65, 130, 200)
 INV_SIZES = (1, 2, 3, 17, 64, 65, 130, 257)
 
 
@@ -152,7 +156,44 @@ def inverse_main() -> None:
     print(f"wrote {OUT_INV}: {len(out)} arrays, {os.path.getsize(OUT_INV)} bytes")
 
 
+def cholesky_main() -> None:
+    """Cholesky fixtures: factors (SHA-256 of the bytes, full up to n=17),
+    info, the Cholesky solve, and the state left by a non-positive pivot."""
+    ref = Oracle("reference")
+    out: dict[str, np.ndarray] = {}
+    for dt, npdt in (("f64", np.float64), ("f32", np.float32)):
+        for n in CHOL_SIZES:
+            a = spd_matrix(n, seed=7000 + n, dtype=npdt)
+            key = f"chol_{dt}_{n}"
+            out[key + "_a_sha"] = np.array(sha(a))
+            for up, tag in ((0, "lower"), (1, "upper")):
+                f, info = ref.potrf(a, upper=bool(up))
+                assert info == 0
+                out[f"{key}_{tag}_sha"] = np.array(sha(f))
+                if n <= 17:
+                    out[f"{key}_{tag}"] = f
+            b = np.random.default_rng(8000 + n).standard_normal(n).astype(npdt)
+            m, _, x = ref.gesv(a, b, 3)
+            out[key + "_b"] = b
+            out[key + "_x"] = x
+            _, _, x4 = ref.gesv(m, b, 4)
+            out[key + "_x_upfront"] = x4
+        for n, fr in ((100, 70), (100, 5)):
+            a = spd_matrix(n, seed=7100 + fr, dtype=npdt, fail_row=fr)
+            f, info = ref.potrf(a)
+            out[f"cholfail_{dt}_{n}_{fr}_a_sha"] = np.array(sha(a))
+            out[f"cholfail_{dt}_{n}_{fr}_m"] = f
+            out[f"cholfail_{dt}_{n}_{fr}_info"] = np.array(info)
+    np.savez_compressed(OUT_CHOL, **out)
+    print(f"wrote {OUT_CHOL}: {len(out)} arrays, {os.path.getsize(OUT_CHOL)} bytes")
+
+
 if __name__ == "__main__":
-    if "--inverse" not in sys.argv[1:]:
-        main()
-    inverse_main()
+    args = sys.argv[1:]
+    if "--cholesky" in args:
+        cholesky_main()
+    else:
+        if "--inverse" not in args:
+            main()
+        inverse_main()
+        cholesky_main()

@@ -27,7 +27,15 @@ def test_workspace_sizes_are_host_side_and_consistent():
         assert lib.b200la_dgesv_workspace_size(n, 1) >= d + 8 * n
         assert lib.b200la_dgesv_workspace_size(n, 2) == lib.b200la_dgesv_workspace_size(n, 1)
         assert lib.b200la_dgetrs_workspace_size(n, 64) >= 8 * n * 64
-    assert lib.b200la_dgesv_workspace_size(16, 3) == 0  # Cholesky modes: not provided
+    for mode in (3, 4):  # Cholesky modes share the LU plan's status and solve buffers
+        assert lib.b200la_dgesv_workspace_size(16, mode) == lib.b200la_dgesv_workspace_size(16, 1)
+    assert lib.b200la_dgesv_workspace_size(16, 5) == 0
+    for f in (lib.b200la_dpotrf, lib.b200la_spotrf):
+        info = ctypes.c_int(7)
+        assert f(None, 4, 0, None, 0, ctypes.addressof(info), None) == _lib.INVALID_ARGUMENT
+        assert f(1 << 20, 0, 0, 1 << 20, 1 << 20, None, None) == _lib.INVALID_ARGUMENT
+        assert f(1 << 20, 8, 2, 1 << 20, 1 << 20, None, None) == _lib.INVALID_ARGUMENT
+        assert f(1 << 20, 8, 0, 1 << 20, 16, None, None) == _lib.WORKSPACE_TOO_SMALL
     assert lib.b200la_dgesv_workspace_size(0, 1) == 0
 
 
@@ -58,8 +66,11 @@ def test_invalid_arguments_rejected_without_device():
     # multiplication argument checks
     assert lib.b200la_dgemm(0, 0, 0, 1, 1, 1.0, p, 1, p, 1, 0.0, p, 1, None, 0, None) == _lib.INVALID_ARGUMENT
     assert lib.b200la_dgemm(0, 0, 1, 1, 1, 1.0, None, 1, p, 1, 0.0, p, 1, None, 0, None) == _lib.INVALID_ARGUMENT
-    # linear_solver: Cholesky modes are not part of this backend
-    assert lib.b200la_dgesv(p, p, 4, p, 3, p, 1 << 20, None) == _lib.NOT_SUPPORTED
+    # linear_solver: an unknown mode is rejected; the Cholesky modes need no pivot array
+    assert lib.b200la_dgesv(p, p, 4, p, 5, p, 1 << 20, None) == _lib.INVALID_ARGUMENT
+    assert "unsupported linear_solver_type" in _lib.last_error()
+    assert lib.b200la_dgesv(p, None, 4, p, 1, p, 1 << 20, None) == _lib.INVALID_ARGUMENT
+    assert lib.b200la_dgesv(p, None, 4, p, 3, p, 16, None) == _lib.WORKSPACE_TOO_SMALL
 
 
 def test_python_errors_map_to_exceptions():
