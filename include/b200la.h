@@ -64,7 +64,9 @@ B200LA_API int64_t b200la_launch_count(void);
  * factorization GEMM, 6 FP64 residual, 7 batched solver, 8 mixed-precision
  * operand preparation and outer U12 solve, 9 precision selector: network
  * and matrix statistics, 10 inversion GEMM updates, 11 inversion and
- * determinant helpers: identity, column gather, diagonal product) is
+ * determinant helpers: identity, column gather, diagonal product,
+ * 12 Cholesky trailing updates, 13 Cholesky diagonal blocks, panel solves,
+ * zeroing and transposition) is
  * bracketed by a
  * pair of CUDA events on its stream.  b200la_profile_stop synchronizes those
  * events and returns the summed device time (ms) and launch count of one

@@ -12,13 +12,13 @@
 // (__dmul_rn / __dadd_rn cannot be contracted), so these updates run on the
 // FP64 (or FP32) pipe, not the tensor cores, whose fused products would give
 // other bits.  Per block k (bs = 64 rows, the last one shorter):
-//   k_chol_diag   the diagonal block, row by row in the reference's order; a
-//                 one-CTA wavefront computes entry (i, j) at step i + j (it
-//                 needs row i's entries left of j and the finished row j);
-//                 a non-positive pivot leaves the block exactly as the
+//   k_chol_diag   the diagonal block, one CTA, column by column: every dot
+//                 product of the reference is accumulated term by term in
+//                 its order as the columns it needs are finished; a
+//                 non-positive pivot leaves the block exactly as the
 //                 reference leaves it when it returns there;
-//   k_chol_zero   zeros right of the diagonal block in its rows;
-//   k_chol_trsm   A21 = A21 L11^-T, row by row (a thread per row);
+//   k_chol_trsm   A21 = A21 L11^-T, a thread per row, term by term likewise,
+//                 and zeros right of the diagonal block in its rows;
 //   k_chol_syrk   the trailing lower triangle, t_ij -= dot(a21_i, a21_j, 64).
 // The first non-positive pivot goes to the status block (first_zero, then
 // info = first_zero + 1) and gates every later kernel, as the reference
@@ -78,10 +78,40 @@ template <typename T> __device__ __forceinline__ T chol_sqrt(T v);
 template <> __device__ __forceinline__ double chol_sqrt(double v) { return sqrt(v); }
 template <> __device__ __forceinline__ float chol_sqrt(float v) { return sqrtf(v); }
 
-// Dynamic shared memory of the kernels below: two padded 64 x 64 tiles.
-template <typename T> constexpr size_t chol_smem_bytes() { return sizeof(T) * 2 * kCholNB * (kCholNB + 1); }
+// The number of leading terms chol_dot rounds separately for a dot of len
+// terms (the rest are fused): whole vectors, then one half vector if the
+// remainder holds one.
+template <typename T> __host__ __device__ constexpr int chol_rend(int len)
+{
+    constexpr int vec  = 32 / (int)sizeof(T);
+    constexpr int half = vec / 2;
+    const int     main = len >= vec ? (len / vec) * vec : 0;
+    return main + (len - main >= half ? half : 0);
+}
 
-// The diagonal block [k, k+bs)^2, one CTA of kCholNB threads (thread i: row i).
+// s += x y in the reference's rounding for term `term` of a dot of `len`
+// terms (both compile-time after unrolling).
+template <typename T> __device__ __forceinline__ T chol_term(T s, T x, T y, int term, int len)
+{
+    return term < chol_rend<T>(len) ? rn_add(s, rn_mul(x, y)) : fma(x, y, s);
+}
+
+// Dynamic shared memory of the kernels below (padded rows of kCholNB + 1).
+constexpr int kCholTrsmRows = 128;  // rows of A21 per k_chol_trsm CTA
+template <typename T> constexpr size_t chol_smem_bytes() { return sizeof(T) * 2 * kCholNB * (kCholNB + 1); }
+template <typename T> constexpr size_t chol_trsm_smem_bytes()
+{
+    return sizeof(T) * (kCholNB + kCholTrsmRows) * (kCholNB + 1);
+}
+
+// The diagonal block [k, k+bs)^2, one CTA of kCholNB threads (thread i: row
+// i).  Column-by-column (right-looking): at column c the pivot is
+// sqrt(a_cc - s_cc), rows below get l_ic = (a_ic - s_ic) / l_cc, then every
+// row adds its term c to s_ij (j > c).  Each s_ij therefore receives the
+// terms l_i0 l_j0, l_i1 l_j1, ... in the reference's order and rounding (its
+// row-by-row loop computes the same dot product from zero), so the factor
+// is the same bits, with a critical path of bs steps instead of one dot
+// product per entry.  The partial sums live in registers (s[j], row tid).
 template <typename T>
 __global__ void __launch_bounds__(kCholNB) k_chol_diag(T* __restrict__ A, int n, int k, int bs, DeviceStatus* st)
 {
@@ -105,34 +135,54 @@ __global__ void __launch_bounds__(kCholNB) k_chol_diag(T* __restrict__ A, int n,
     {
         fail = -1;
     }
-    __syncthreads();
-    for (int t = 0; t <= 2 * (bs - 1); ++t)
+    T s[kCholNB];
+#pragma unroll
+    for (int j = 0; j < kCholNB; ++j)
     {
-        const int i = tid, j = t - tid;
-        if (i < bs && j >= 0 && j <= i)
+        s[j] = T(0);
+    }
+    __syncthreads();
+#pragma unroll
+    for (int c = 0; c < kCholNB; ++c)
+    {
+        if (c >= bs)
         {
-            if (j < i)
+            break;
+        }
+        if (tid == c)
+        {
+            const T d = rn_sub(blk[c][c], s[c]);
+            if (d <= T(0))
             {
-                const T s = rn_sub(blk[i][j], chol_dot(&blk[i][0], &blk[j][0], j));
-                blk[i][j] = s / blk[j][j];
+                fail = c;
             }
             else
             {
-                const T s = rn_sub(blk[i][i], chol_dot(&blk[i][0], &blk[i][0], i));
-                if (s <= T(0))
-                {
-                    fail = i;  // one diagonal per step
-                }
-                else
-                {
-                    blk[i][i] = chol_sqrt(s);
-                }
+                blk[c][c] = chol_sqrt(d);
             }
         }
         __syncthreads();
         if (fail >= 0)
         {
             break;
+        }
+        const bool below = tid > c && tid < bs;
+        if (below)
+        {
+            blk[tid][c] = rn_sub(blk[tid][c], s[c]) / blk[c][c];
+        }
+        __syncthreads();
+        if (below)
+        {
+            const T v = blk[tid][c];
+#pragma unroll
+            for (int j = c + 1; j < kCholNB; ++j)
+            {
+                if (j <= tid)
+                {
+                    s[j] = chol_term(s[j], v, blk[j][c], c, j);
+                }
+            }
         }
     }
     const int f = fail;
@@ -163,93 +213,186 @@ __global__ void __launch_bounds__(kCholNB) k_chol_diag(T* __restrict__ A, int n,
     }
 }
 
-// Zeros right of the diagonal block in its rows: A[k..k+bs)[k+bs..n).
-template <typename T> __global__ void k_chol_zero(T* __restrict__ A, int n, int k, int bs, const DeviceStatus* gate)
+// Failure gate of the block that ends at row `limit`: a device error, or a
+// non-positive pivot found before `limit`.  A later block's diagonal kernel
+// may run concurrently (look-ahead) and set a later pivot; that one does not
+// stop this block's work, as in the reference, which finished this block
+// before it reached the failing one.
+__device__ __forceinline__ bool chol_gated(const DeviceStatus* st, int64_t limit)
 {
-    if (gated(gate))
+    if (ld_volatile_i32(&st->error) != 0)
     {
-        return;
+        return true;
     }
-    const int     w     = n - k - bs;
-    const int64_t total = (int64_t)bs * w;
-    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x)
-    {
-        const int r = (int)(e / w), c = (int)(e - (e / w) * w);
-        A[(int64_t)(k + r) * n + k + bs + c] = T(0);
-    }
+    const int64_t f = *reinterpret_cast<const volatile int64_t*>(&st->first_zero);
+    return f >= 0 && f < limit;
 }
 
-// A21 = A21 L11^-T: rows [k+bs, n), thread per row; L11 and the CTA's rows
-// staged in shared memory (padded rows).
+// A21 = A21 L11^-T for a full block (bs = kCholNB): rows [k+64, n), a
+// thread per row, kCholTrsmRows rows per CTA staged in shared memory with
+// L11.  Row r, column c: l_rc = (a_rc - s_rc) / l_cc, then the row's later
+// partial sums s_rj (j > c, registers) get the term l_rc l_jc: the
+// reference's dot products term by term, in its order and rounding.  The
+// CTAs also clear the block's rows right of it (A[k..k+64)[k+64..n)),
+// kCholTrsmRows columns each, as the reference does once the block is
+// factored.
 template <typename T>
-__global__ void __launch_bounds__(kCholNB) k_chol_trsm(T* __restrict__ A, int n, int k, int bs,
-    const DeviceStatus* gate)
+__global__ void __launch_bounds__(kCholTrsmRows) k_chol_trsm(T* __restrict__ A, int n, int k, const DeviceStatus* st)
 {
     extern __shared__ __align__(16) unsigned char chol_smem[];
     T(*l11)[kCholNB + 1]  = reinterpret_cast<T(*)[kCholNB + 1]>(chol_smem);
     T(*rows)[kCholNB + 1] = l11 + kCholNB;
-    if (gated(gate))
+    if (chol_gated(st, (int64_t)k + kCholNB))
     {
         return;
     }
     const int tid = threadIdx.x;
-    const int r0  = k + bs + blockIdx.x * kCholNB;
-    const int nr  = min(kCholNB, n - r0);
-    for (int e = tid; e < bs * bs; e += kCholNB)
+    const int r0  = k + kCholNB + blockIdx.x * kCholTrsmRows;
+    const int nr  = min(kCholTrsmRows, n - r0);
+    for (int e = tid; e < kCholNB * kCholNB; e += kCholTrsmRows)
     {
-        const int r = e / bs, c = e - (e / bs) * bs;
+        const int r = e / kCholNB, c = e % kCholNB;
         l11[r][c]   = A[(int64_t)(k + r) * n + k + c];
     }
-    for (int e = tid; e < nr * bs; e += kCholNB)
+    for (int e = tid; e < nr * kCholNB; e += kCholTrsmRows)
     {
-        const int r = e / bs, c = e - (e / bs) * bs;
+        const int r = e / kCholNB, c = e % kCholNB;
         rows[r][c]  = A[(int64_t)(r0 + r) * n + k + c];
+    }
+    for (int e = tid; e < kCholNB * nr; e += kCholTrsmRows)
+    {
+        const int r = e / nr, c = e - (e / nr) * nr;
+        A[(int64_t)(k + r) * n + r0 + c] = T(0);
     }
     __syncthreads();
     if (tid < nr)
     {
         T* row = &rows[tid][0];
-        for (int j = 0; j < bs; ++j)
+        T  s[kCholNB];
+#pragma unroll
+        for (int j = 0; j < kCholNB; ++j)
         {
-            const T s = rn_sub(row[j], chol_dot(row, &l11[j][0], j));
-            row[j]    = s / l11[j][j];
+            s[j] = T(0);
+        }
+#pragma unroll
+        for (int c = 0; c < kCholNB; ++c)
+        {
+            const T v = rn_sub(row[c], s[c]) / l11[c][c];
+            row[c]    = v;
+#pragma unroll
+            for (int j = c + 1; j < kCholNB; ++j)
+            {
+                s[j] = chol_term(s[j], v, l11[j][c], c, j);
+            }
         }
     }
     __syncthreads();
-    for (int e = tid; e < nr * bs; e += kCholNB)
+    for (int e = tid; e < nr * kCholNB; e += kCholTrsmRows)
     {
-        const int r = e / bs, c = e - (e / bs) * bs;
+        const int r = e / kCholNB, c = e % kCholNB;
         A[(int64_t)(r0 + r) * n + k + c] = rows[r][c];
     }
 }
 
-// Trailing lower triangle t_ij -= dot(a21_i, a21_j, bs), i >= j, over
-// [k+bs, n)^2.  CTA tile 64 x 64 (tile (I, J), J <= I; tiles above the
-// diagonal exit), 256 threads with 4 x 4 entries each; the two A21 slices in
-// shared memory.  With bs = 64 every product is rounded and added in order
-// (chol_dot's full-vector part covers all 64 terms).
+// Trailing lower triangle t_ij -= dot(a21_i, a21_j, 64), i >= j, over
+// [k+64, n)^2 for a full block.  With 64 terms every product is rounded and
+// added in order (chol_dot's whole-vector part covers them all).  CTA tile
+// 64 x 64 of 256 threads with 4 x 4 entries each.  The tiles on or below the
+// diagonal are launched in one of three sets: all of them (blockIdx.x
+// enumerates the triangle row by row), the first tile column only (the
+// columns the next block factors), or the rest.  The two A21 slices arrive
+// in shared memory by cp.async in two halves of 32 columns, the second
+// landing while the first is multiplied; the C tile is prefetched into L2.
 constexpr int kSyrkTile = 64;
+enum Chol_syrk_set
+{
+    kSyrkAll   = 0,
+    kSyrkFirst = 1,
+    kSyrkRest  = 2
+};
+static_assert(chol_rend<double>(kCholNB) == kCholNB && chol_rend<float>(kCholNB) == kCholNB,
+    "a full block's trailing dot products round every product");
+
+__device__ __forceinline__ void chol_tri_tile(int b, int& I, int& J)
+{
+    int i = (int)((sqrt(8.0 * (double)b + 1.0) - 1.0) * 0.5);
+    while ((int64_t)i * (i + 1) / 2 > b)
+    {
+        --i;
+    }
+    while ((int64_t)(i + 1) * (i + 2) / 2 <= b)
+    {
+        ++i;
+    }
+    I = i;
+    J = b - i * (i + 1) / 2;
+}
+
+template <int BYTES> __device__ __forceinline__ void chol_cp_async(void* dst, const void* src, bool valid)
+{
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;\n" ::"r"(d), "l"(src), "n"(BYTES),
+        "r"(valid ? BYTES : 0)
+        : "memory");
+}
+__device__ __forceinline__ void chol_cp_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N> __device__ __forceinline__ void chol_cp_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
 template <typename T>
-__global__ void __launch_bounds__(256) k_chol_syrk(T* __restrict__ A, int n, int k, int bs, const DeviceStatus* gate)
+__global__ void __launch_bounds__(256) k_chol_syrk(T* __restrict__ A, int n, int k, int set, const DeviceStatus* st)
 {
     extern __shared__ __align__(16) unsigned char chol_smem[];
     T(*ai)[kCholNB + 1] = reinterpret_cast<T(*)[kCholNB + 1]>(chol_smem);
     T(*aj)[kCholNB + 1] = ai + kSyrkTile;
-    const int I = blockIdx.y, J = blockIdx.x;
-    if (J > I || gated(gate))
+    if (chol_gated(st, (int64_t)k + kCholNB))
     {
         return;
     }
-    const int base = k + bs;
+    int I, J;
+    if (set == kSyrkFirst)
+    {
+        I = blockIdx.x;
+        J = 0;
+    }
+    else
+    {
+        chol_tri_tile(blockIdx.x, I, J);
+        if (set == kSyrkRest)
+        {
+            ++I;
+            ++J;
+        }
+    }
+    const int base = k + kCholNB;
     const int i0 = base + I * kSyrkTile, j0 = base + J * kSyrkTile;
     const int tid = threadIdx.x;
-    for (int e = tid; e < kSyrkTile * bs; e += 256)
+    // C tile into L2: 64 rows of 64 entries, 128-byte lines
+    constexpr int lines = kSyrkTile * (int)sizeof(T) / 128;
+    if (tid < kSyrkTile * lines)
     {
-        const int r = e / bs, c = e - (e / bs) * bs;
-        ai[r][c]    = i0 + r < n ? A[(int64_t)(i0 + r) * n + k + c] : T(0);
-        aj[r][c]    = j0 + r < n ? A[(int64_t)(j0 + r) * n + k + c] : T(0);
+        const int r = tid / lines, l = tid - (tid / lines) * lines;
+        if (i0 + r < n)
+        {
+            const T* p = A + (int64_t)(i0 + r) * n + j0 + l * (128 / (int)sizeof(T));
+            asm volatile("prefetch.global.L2 [%0];\n" ::"l"(p));
+        }
     }
-    __syncthreads();
+    // the A21 slices, two halves of 32 columns (8 elements per thread per
+    // slice and half); rows past n read as zeros
+#pragma unroll
+    for (int h = 0; h < 2; ++h)
+    {
+#pragma unroll
+        for (int q = 0; q < 8; ++q)
+        {
+            const int  e  = tid + 256 * q;
+            const int  r  = e >> 5, c = (e & 31) + 32 * h;
+            const bool vi = i0 + r < n, vj = j0 + r < n;
+            chol_cp_async<sizeof(T)>(&ai[r][c], A + (int64_t)(vi ? i0 + r : base) * n + k + c, vi);
+            chol_cp_async<sizeof(T)>(&aj[r][c], A + (int64_t)(vj ? j0 + r : base) * n + k + c, vj);
+        }
+        chol_cp_commit();
+    }
     const int tr = tid >> 4, tc = tid & 15;  // rows tr + 16a, columns tc + 16b
     T         acc[4][4];
 #pragma unroll
@@ -261,26 +404,36 @@ __global__ void __launch_bounds__(256) k_chol_syrk(T* __restrict__ A, int n, int
             acc[a][b] = T(0);
         }
     }
-    constexpr int vec  = 32 / (int)sizeof(T);
-    constexpr int half = vec / 2;
-    const int     main = bs >= vec ? (bs / vec) * vec : 0;
-    const int     rend = main + (bs - main >= half ? half : 0);  // products rounded before [0, rend)
-    for (int p = 0; p < bs; ++p)
+#pragma unroll
+    for (int h = 0; h < 2; ++h)
     {
-        T x[4], y[4];
-#pragma unroll
-        for (int a = 0; a < 4; ++a)
+        if (h == 0)
         {
-            x[a] = ai[tr + 16 * a][p];
-            y[a] = aj[tc + 16 * a][p];
+            chol_cp_wait<1>();
         }
-#pragma unroll
-        for (int a = 0; a < 4; ++a)
+        else
         {
+            chol_cp_wait<0>();
+        }
+        __syncthreads();
+#pragma unroll 8
+        for (int p = 32 * h; p < 32 * h + 32; ++p)
+        {
+            T x[4], y[4];
 #pragma unroll
-            for (int b = 0; b < 4; ++b)
+            for (int a = 0; a < 4; ++a)
             {
-                acc[a][b] = p < rend ? rn_add(acc[a][b], rn_mul(x[a], y[b])) : fma(x[a], y[b], acc[a][b]);
+                x[a] = ai[tr + 16 * a][p];
+                y[a] = aj[tc + 16 * a][p];
+            }
+#pragma unroll
+            for (int a = 0; a < 4; ++a)
+            {
+#pragma unroll
+                for (int b = 0; b < 4; ++b)
+                {
+                    acc[a][b] = rn_add(acc[a][b], rn_mul(x[a], y[b]));
+                }
             }
         }
     }
@@ -296,10 +449,10 @@ __global__ void __launch_bounds__(256) k_chol_syrk(T* __restrict__ A, int n, int
         for (int b = 0; b < 4; ++b)
         {
             const int j = j0 + tc + 16 * b;
-            if (j <= i && j < n)
+            if (j <= i)
             {
-                T* p  = A + (int64_t)i * n + j;
-                *p    = rn_sub(*p, acc[a][b]);
+                T* p = A + (int64_t)i * n + j;
+                *p   = rn_sub(*p, acc[a][b]);
             }
         }
     }

@@ -132,7 +132,9 @@ enum KernelClass : int
     KC_SELECT   = 9,
     KC_INV_GEMM = 10,  // inversion: the blocked substitutions' GEMM updates
     KC_INV_AUX  = 11,  // inversion / determinant: identity, column gather, diagonal product
-    KC_COUNT    = 12
+    KC_CHOL_UPD = 12,  // Cholesky: the trailing lower-triangle updates
+    KC_CHOL_AUX = 13,  // Cholesky: diagonal blocks, panel solves, zeroing, transposition
+    KC_COUNT    = 14
 };
 
 // Host helpers shared by the entry points (defined in runtime.cu).

@@ -93,7 +93,7 @@ template <typename T> int ensure_kernel_attributes()
     B200LA_CUDA(cudaFuncSetAttribute(k_dmma_band<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBandSmem));
     B200LA_CUDA(cudaFuncSetAttribute(k_dmma_gemm<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDmSmem));
     B200LA_CUDA(cudaFuncSetAttribute(k_chol_diag<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)chol_smem_bytes<T>()));
-    B200LA_CUDA(cudaFuncSetAttribute(k_chol_trsm<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)chol_smem_bytes<T>()));
+    B200LA_CUDA(cudaFuncSetAttribute(k_chol_trsm<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)chol_trsm_smem_bytes<T>()));
     B200LA_CUDA(cudaFuncSetAttribute(k_chol_syrk<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)chol_smem_bytes<T>()));
     B200LA_CUDA(cudaFuncSetAttribute(k_dmma_gemm<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDmSmem));
     B200LA_CUDA(cudaFuncSetAttribute(k_gemm<T, false, false>,
@@ -679,49 +679,118 @@ int enqueue_getrs(const T* lu, const int64_t* pivot, int n, int nrhs, T* x, int6
 // Blocked lower Cholesky of m (n x n, row-major) in the reference's order
 // (cholesky.cuh); upper: then transposed into the upper triangle.  The status
 // block gets the first non-positive pivot; later kernels are gated on it.
+// Look-ahead: the trailing update of block k is split into its first tile
+// column (the next block's columns) and the rest; the next block's diagonal
+// and panel kernels run on a side stream beside the rest.
+template <typename T> int launch_chol_block(T* m, int n, int k, DeviceStatus* st, cudaStream_t s)
+{
+    const int bs    = n - k < kCholNB ? n - k : kCholNB;
+    const int below = n - k - bs;
+    prof_begin(KC_CHOL_AUX, s);
+    k_chol_diag<T><<<1, kCholNB, chol_smem_bytes<T>(), s>>>(m, n, k, bs, st);
+    prof_end(KC_CHOL_AUX, s);
+    B200LA_LAUNCH_CHECK();
+    if (below > 0)
+    {
+        prof_begin(KC_CHOL_AUX, s);
+        k_chol_trsm<T><<<(below + kCholTrsmRows - 1) / kCholTrsmRows, kCholTrsmRows, chol_trsm_smem_bytes<T>(),
+            s>>>(m, n, k, st);
+        prof_end(KC_CHOL_AUX, s);
+        B200LA_LAUNCH_CHECK();
+    }
+    return B200LA_SUCCESS;
+}
+
+template <typename T> int launch_chol_syrk(T* m, int n, int k, int set, DeviceStatus* st, cudaStream_t s)
+{
+    const int64_t tiles = (n - k - kCholNB + kSyrkTile - 1) / kSyrkTile;
+    const int64_t grid  = set == kSyrkFirst ? tiles : set == kSyrkRest ? tiles * (tiles - 1) / 2 : tiles * (tiles + 1) / 2;
+    if (grid <= 0)
+    {
+        return B200LA_SUCCESS;
+    }
+    prof_begin(KC_CHOL_UPD, s);
+    k_chol_syrk<T><<<(unsigned)grid, 256, chol_smem_bytes<T>(), s>>>(m, n, k, set, st);
+    prof_end(KC_CHOL_UPD, s);
+    B200LA_LAUNCH_CHECK();
+    return B200LA_SUCCESS;
+}
+
 template <typename T> int enqueue_potrf(T* m, int n, bool upper, DeviceStatus* st, cudaStream_t s)
 {
-    prof_begin(KC_PANEL, s);
+    prof_begin(KC_CHOL_AUX, s);
     k_status_init<<<1, 32, 0, s>>>(st, nullptr);
-    prof_end(KC_PANEL, s);
+    prof_end(KC_CHOL_AUX, s);
     B200LA_LAUNCH_CHECK();
-    const size_t smem = chol_smem_bytes<T>();
-    for (int k = 0; k < n; k += kCholNB)
+    const bool   ahead = lu_lookahead_enabled() && n > 2 * kCholNB;
+    cudaStream_t side  = nullptr;
+    cudaEvent_t  ev_cols = nullptr, ev_block = nullptr;
+    if (ahead)
     {
-        const int bs    = n - k < kCholNB ? n - k : kCholNB;
-        const int below = n - k - bs;
-        prof_begin(KC_PANEL, s);
-        k_chol_diag<T><<<1, kCholNB, smem, s>>>(m, n, k, bs, st);
-        prof_end(KC_PANEL, s);
-        B200LA_LAUNCH_CHECK();
-        if (below == 0)
+        int rc = B200LA_SUCCESS;
+        side   = panel_side_stream(&rc);
+        if (rc != B200LA_SUCCESS)
         {
-            break;
+            return rc;
         }
-        prof_begin(KC_SWAP, s);
-        k_chol_zero<T><<<grid_1d((int64_t)bs * below, 256), 256, 0, s>>>(m, n, k, bs, st);
-        prof_end(KC_SWAP, s);
-        B200LA_LAUNCH_CHECK();
-        prof_begin(KC_SWAP, s);
-        k_chol_trsm<T><<<(below + kCholNB - 1) / kCholNB, kCholNB, smem, s>>>(m, n, k, bs, st);
-        prof_end(KC_SWAP, s);
-        B200LA_LAUNCH_CHECK();
-        const unsigned tiles = (unsigned)((below + kSyrkTile - 1) / kSyrkTile);
-        prof_begin(KC_TRAILING, s);
-        k_chol_syrk<T><<<dim3(tiles, tiles), 256, smem, s>>>(m, n, k, bs, st);
-        prof_end(KC_TRAILING, s);
-        B200LA_LAUNCH_CHECK();
+        B200LA_CUDA(cudaEventCreateWithFlags(&ev_cols, cudaEventDisableTiming));
+        B200LA_CUDA(cudaEventCreateWithFlags(&ev_block, cudaEventDisableTiming));
+    }
+    struct EventGuard
+    {
+        cudaEvent_t a, b;
+        ~EventGuard()
+        {
+            if (a)
+                cudaEventDestroy(a);
+            if (b)
+                cudaEventDestroy(b);
+        }
+    } guard{ev_cols, ev_block};
+    int rc = launch_chol_block<T>(m, n, 0, st, s);
+    for (int k = 0; rc == B200LA_SUCCESS && n - k > kCholNB; k += kCholNB)
+    {
+        if (ahead)
+        {
+            rc = launch_chol_syrk<T>(m, n, k, kSyrkFirst, st, s);
+            if (rc != B200LA_SUCCESS)
+            {
+                break;
+            }
+            B200LA_CUDA(cudaEventRecord(ev_cols, s));
+            B200LA_CUDA(cudaStreamWaitEvent(side, ev_cols, 0));
+            rc = launch_chol_block<T>(m, n, k + kCholNB, st, side);
+            if (rc != B200LA_SUCCESS)
+            {
+                break;
+            }
+            B200LA_CUDA(cudaEventRecord(ev_block, side));
+            rc = launch_chol_syrk<T>(m, n, k, kSyrkRest, st, s);
+            B200LA_CUDA(cudaStreamWaitEvent(s, ev_block, 0));
+        }
+        else
+        {
+            rc = launch_chol_syrk<T>(m, n, k, kSyrkAll, st, s);
+            if (rc == B200LA_SUCCESS)
+            {
+                rc = launch_chol_block<T>(m, n, k + kCholNB, st, s);
+            }
+        }
+    }
+    if (rc != B200LA_SUCCESS)
+    {
+        return rc;
     }
     if (upper)
     {
-        prof_begin(KC_SWAP, s);
+        prof_begin(KC_CHOL_AUX, s);
         k_chol_to_upper<T><<<grid_1d((int64_t)n * n, 256), 256, 0, s>>>(m, n, st);
-        prof_end(KC_SWAP, s);
+        prof_end(KC_CHOL_AUX, s);
         B200LA_LAUNCH_CHECK();
     }
-    prof_begin(KC_PANEL, s);
+    prof_begin(KC_CHOL_AUX, s);
     k_status_finish<<<1, 32, 0, s>>>(st);
-    prof_end(KC_PANEL, s);
+    prof_end(KC_CHOL_AUX, s);
     B200LA_LAUNCH_CHECK();
     return B200LA_SUCCESS;
 }
@@ -729,8 +798,38 @@ template <typename T> int enqueue_potrf(T* m, int n, bool upper, DeviceStatus* s
 // Solve with a lower Cholesky factor in place on x (n x nrhs, row stride
 // ldx): L y = x, then L^T x = y.  Gated on the factorization's status.
 template <typename T>
-int enqueue_potrs(const T* l, int n, int nrhs, T* x, int64_t ldx, const DeviceStatus* gate, cudaStream_t s)
+int enqueue_potrs(const T* l, int n, int nrhs, T* x, int64_t ldx, const SolvePlan<T>& sp, DeviceStatus* st,
+    const DeviceStatus* gate, cudaStream_t s)
 {
+    if constexpr (sizeof(T) == 8)
+    {
+        if (nrhs == 1 && sp.xll != nullptr)
+        {
+            // L y = x, then L^T x = y, each in one launch (k_trsv_blocks, the
+            // Cholesky variant) on scratch; the result is copied back only if
+            // the factorization succeeded
+            const int nb = (n + kTvRows - 1) / kTvRows;
+            prof_begin(KC_SOLVE, s);
+            k_copy2d<T><<<grid_1d(n, 256), 256, 0, s>>>(x, ldx, sp.y, 1, n, 1, nullptr);
+            prof_end(KC_SOLVE, s);
+            B200LA_LAUNCH_CHECK();
+            for (int pass = 0; pass < 2; ++pass)
+            {
+                B200LA_CUDA(cudaMemsetAsync(sp.ticket, 0, sizeof(int32_t), s));
+                const uint32_t epoch = tv_next_epoch();
+                prof_begin(KC_SOLVE, s);
+                k_trsv_blocks<double, true, true><<<nb, kTvThreads, 0, s>>>(l, n, sp.y, n, pass, nullptr, sp.xll,
+                    epoch, sp.ticket, st);
+                prof_end(KC_SOLVE, s);
+                B200LA_LAUNCH_CHECK();
+            }
+            prof_begin(KC_SOLVE, s);
+            k_copy2d<T><<<grid_1d(n, 256), 256, 0, s>>>(sp.y, 1, x, ldx, n, 1, gate);
+            prof_end(KC_SOLVE, s);
+            B200LA_LAUNCH_CHECK();
+            return B200LA_SUCCESS;
+        }
+    }
     int rc = enqueue_trsm_inplace<T>(false, false, false, n, nrhs, l, n, x, ldx, gate, s);
     if (rc != B200LA_SUCCESS)
     {
@@ -811,7 +910,7 @@ int gesv(T* m, int64_t* pivot, int64_t n, T* x, int mode, void* ws, size_t bytes
         {
             return st;
         }
-        return enqueue_potrs<T>(m, (int)n, 1, x, 1, gp.st, s);
+        return enqueue_potrs<T>(m, (int)n, 1, x, 1, sp, gp.st, gp.st, s);
     }
     if (mode == B200LA_LU_LINEAR_SOLVER)
     {

@@ -135,14 +135,17 @@ __device__ __forceinline__ bool tv_read(const uint64_t* xll, int blk, int i, uin
 }
 
 // x <- T^-1 x for T the unit-lower (upper = 0) or upper (upper = 1) triangle
-// of the factor `a`.  CTA = one 64-row block, claimed by ticket in solve
+// of the factor `a`; with CHOL, of a Cholesky factor L (lower triangle of
+// `a`): T = L (upper = 0, non-unit) or T = L^T (upper = 1, read from L's
+// rows: a block's off-diagonal tile is the transpose of a 64-column slice of
+// the solved rows, loaded row by row, coalesced).  CTA = one 64-row block, claimed by ticket in solve
 // order; xll receives the flagged copies of the solved blocks (epoch: a value
 // this call's flags carry, never reused).  The diagonal block is applied as
 // its inverse from dinv (k_invert_diag_blocks; SUBST = false, the refinement
 // solves, whose rounding the refinement corrects) or solved by substitution
 // from the block's own triangle (SUBST = true, dinv unused: backward stable,
 // for the plain FP64 solve).
-template <typename TA, bool SUBST = false>
+template <typename TA, bool SUBST = false, bool CHOL = false>
 __global__ void __launch_bounds__(kTvThreads) k_trsv_blocks(const TA* __restrict__ a, int64_t lda,
     double* __restrict__ x, int n, int upper, const double* __restrict__ dinv, uint64_t* __restrict__ xll,
     uint32_t epoch, int32_t* __restrict__ ticket, DeviceStatus* st)
@@ -175,8 +178,9 @@ __global__ void __launch_bounds__(kTvThreads) k_trsv_blocks(const TA* __restrict
         for (int e = tid; e < kTvRows * kTvRows; e += kTvThreads)
         {
             const int  i = e / kTvRows, c = e % kTvRows;
-            const bool in = i < br && c < br && (upper ? c >= i : c < i);
-            inv[i][c]     = in ? (double)a[(int64_t)(r0 + i) * lda + r0 + c] : 0.0;
+            const bool in = i < br && c < br && (upper ? c >= i : (CHOL ? c <= i : c < i));
+            const int  ri = CHOL && upper ? c : i, ci = CHOL && upper ? i : c;
+            inv[i][c]     = in ? (double)a[(int64_t)(r0 + ri) * lda + r0 + ci] : 0.0;
         }
     }
     else
@@ -201,7 +205,8 @@ __global__ void __launch_bounds__(kTvThreads) k_trsv_blocks(const TA* __restrict
 #pragma unroll
         for (int j = 0; j < Q; ++j)
         {
-            dst[j] = (r < br && c0 + j < n) ? a[(int64_t)(r0 + r) * lda + c0 + j] : TA(0);
+            const int64_t at = CHOL && upper ? (int64_t)(c0 + j) * lda + r0 + r : (int64_t)(r0 + r) * lda + c0 + j;
+            dst[j]           = (r < br && c0 + j < n) ? a[at] : TA(0);
         }
     };
     if (t > 0)
@@ -292,7 +297,7 @@ __global__ void __launch_bounds__(kTvThreads) k_trsv_blocks(const TA* __restrict
                     continue;  // uniform across the warp
                 }
                 double vp = p < 32 ? v0 : v1;
-                if (upper)
+                if (upper || CHOL)
                 {
                     vp = vp / inv[p][p];
                 }

@@ -82,6 +82,23 @@ def test_cholesky_not_positive_definite_state(port, cg, dt, npdt, n, fail_row):
     assert info_u == info and np.array_equal(fu, port.potrf(a, True)[0])
 
 
+def test_cholesky_lookahead_neutral(port, monkeypatch):
+    """The look-ahead schedule (next block's kernels beside the trailing
+    update) gives the same bits as the plain sequence, also when a late
+    block is not positive definite."""
+    for fail_row in (-1, 1400):
+        a = spd_matrix(1500, seed=15, fail_row=fail_row)
+        monkeypatch.delenv("B200LA_LU_LOOKAHEAD", raising=False)
+        f1, i1 = gpu_potrf(a)
+        monkeypatch.setenv("B200LA_LU_LOOKAHEAD", "0")
+        f0, i0 = gpu_potrf(a)
+        monkeypatch.delenv("B200LA_LU_LOOKAHEAD")
+        assert i0 == i1 == fail_row + 1
+        assert np.array_equal(f0, f1)
+        if fail_row >= 0:
+            assert np.array_equal(f1, port.potrf(a)[0])
+
+
 def test_cholesky_large_bitwise(port):
     n = 2500
     a = spd_matrix(n, seed=2500)
