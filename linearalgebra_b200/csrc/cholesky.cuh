@@ -104,6 +104,18 @@ template <typename T> constexpr size_t chol_trsm_smem_bytes()
     return sizeof(T) * (kCholNB + kCholTrsmRows) * (kCholNB + 1);
 }
 
+// Element-wise asynchronous copies global -> shared (zero-filled when not
+// valid), so a CTA issues all of its staging loads before it waits.
+template <int BYTES> __device__ __forceinline__ void chol_cp_async(void* dst, const void* src, bool valid)
+{
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;\n" ::"r"(d), "l"(src), "n"(BYTES),
+        "r"(valid ? BYTES : 0)
+        : "memory");
+}
+__device__ __forceinline__ void chol_cp_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N> __device__ __forceinline__ void chol_cp_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
 // The diagonal block [k, k+bs)^2, one CTA of kCholNB threads (thread i: row
 // i).  Column-by-column (right-looking): at column c the pivot is
 // sqrt(a_cc - s_cc), rows below get l_ic = (a_ic - s_ic) / l_cc, then every
@@ -124,16 +136,25 @@ __global__ void __launch_bounds__(kCholNB) k_chol_diag(T* __restrict__ A, int n,
         return;
     }
     const int tid = threadIdx.x;
-    for (int e = tid; e < bs * bs; e += kCholNB)
+    for (int e = tid; e < kCholNB * kCholNB; e += kCholNB)
     {
-        const int r = e / bs, c = e - (e / bs) * bs;
-        const T   v = A[(int64_t)(k + r) * n + k + c];
-        blk[r][c]   = v;
-        orig[r][c]  = v;
+        const int r = e / kCholNB, c = e % kCholNB;
+        if (r < bs && c < bs)
+        {
+            chol_cp_async<sizeof(T)>(&blk[r][c], A + (int64_t)(k + r) * n + k + c, true);
+        }
     }
+    chol_cp_commit();
     if (tid == 0)
     {
         fail = -1;
+    }
+    chol_cp_wait<0>();
+    __syncthreads();
+    for (int e = tid; e < bs * bs; e += kCholNB)
+    {
+        const int r = e / bs, c = e - (e / bs) * bs;
+        orig[r][c]  = blk[r][c];
     }
     T s[kCholNB];
 #pragma unroll
@@ -252,18 +273,20 @@ __global__ void __launch_bounds__(kCholTrsmRows) k_chol_trsm(T* __restrict__ A, 
     for (int e = tid; e < kCholNB * kCholNB; e += kCholTrsmRows)
     {
         const int r = e / kCholNB, c = e % kCholNB;
-        l11[r][c]   = A[(int64_t)(k + r) * n + k + c];
+        chol_cp_async<sizeof(T)>(&l11[r][c], A + (int64_t)(k + r) * n + k + c, true);
     }
     for (int e = tid; e < nr * kCholNB; e += kCholTrsmRows)
     {
         const int r = e / kCholNB, c = e % kCholNB;
-        rows[r][c]  = A[(int64_t)(r0 + r) * n + k + c];
+        chol_cp_async<sizeof(T)>(&rows[r][c], A + (int64_t)(r0 + r) * n + k + c, true);
     }
+    chol_cp_commit();
     for (int e = tid; e < kCholNB * nr; e += kCholTrsmRows)
     {
         const int r = e / nr, c = e - (e / nr) * nr;
         A[(int64_t)(k + r) * n + r0 + c] = T(0);
     }
+    chol_cp_wait<0>();
     __syncthreads();
     if (tid < nr)
     {
@@ -327,16 +350,6 @@ __device__ __forceinline__ void chol_tri_tile(int b, int& I, int& J)
     I = i;
     J = b - i * (i + 1) / 2;
 }
-
-template <int BYTES> __device__ __forceinline__ void chol_cp_async(void* dst, const void* src, bool valid)
-{
-    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
-    asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;\n" ::"r"(d), "l"(src), "n"(BYTES),
-        "r"(valid ? BYTES : 0)
-        : "memory");
-}
-__device__ __forceinline__ void chol_cp_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-template <int N> __device__ __forceinline__ void chol_cp_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
 template <typename T>
 __global__ void __launch_bounds__(256) k_chol_syrk(T* __restrict__ A, int n, int k, int set, const DeviceStatus* st)
