@@ -59,6 +59,8 @@ def parse():
     p.add_argument("--inv-n", type=int, default=16384, help="order of the inversion / determinant measurement")
     p.add_argument("--no-inversion", action="store_true")
     p.add_argument("--no-multiplication", action="store_true")
+    p.add_argument("--chol-n", type=int, default=16384, help="order of the Cholesky-mode solve measurement")
+    p.add_argument("--no-cholesky", action="store_true")
     return p.parse_args()
 
 
@@ -355,6 +357,155 @@ def run_inversion(args, world, rank, local):
 
 
 # ---------------------------------------------------------------------------
+# Cholesky modes of linear_solver: this library vs the reference's CUDA_BLAS
+# path (cuSOLVER potrf + potrs, baseline/_ref) at the same order
+# ---------------------------------------------------------------------------
+def cholesky_update_flops(n: int, nb: int = 64) -> int:
+    """Algorithmic flops of the trailing updates (k_chol_syrk): for each full
+    block, 2 * 64 per entry of the trailing lower triangle."""
+    fl = 0
+    for k in range(0, n, nb):
+        below = n - k - nb
+        if below > 0:
+            fl += 2 * nb * below * (below + 1) // 2
+    return fl
+
+
+def cuda_blas_cholesky(lib_path, A, b, stream, steps):
+    import torch
+    lib = ctypes.CDLL(lib_path)
+    lib.ref_cublas_dcholesky_solve_workspace_size.restype = ctypes.c_size_t
+    lib.ref_cublas_dcholesky_solve_workspace_size.argtypes = [ctypes.c_int64]
+    lib.ref_cublas_dcholesky_solve.argtypes = [ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p,
+                                               ctypes.c_size_t, ctypes.c_void_p]
+    lib.ref_cublas_last_error.restype = ctypes.c_char_p
+    n = A.shape[0]
+    nb = int(lib.ref_cublas_dcholesky_solve_workspace_size(n))
+    ws = torch.empty(max(nb, 256), dtype=torch.uint8, device=A.device)
+    m, x = torch.empty_like(A), torch.empty_like(b)
+
+    def step():
+        m.copy_(A)
+        x.copy_(b)
+        if lib.ref_cublas_dcholesky_solve(m.data_ptr(), n, x.data_ptr(), ws.data_ptr(), nb, stream.cuda_stream) != 0:
+            raise RuntimeError(lib.ref_cublas_last_error().decode())
+
+    step()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    t = e0.elapsed_time(e1) / steps / 1e3
+    r = (torch.mv(A, x) - b).abs().max().item()
+    eta = r / (torch.linalg.matrix_norm(A, ord=float("inf")).item() * x.abs().max().item() + b.abs().max().item())
+    del m, x, ws
+    torch.cuda.empty_cache()
+    return {"s": t, "backward_error": eta, "steps": steps,
+            "what": "the reference's linear_solver<double,CUDA_BLAS> CHOLESKY mode (cuSOLVER potrf + potrs)"}
+
+
+def run_cholesky(args, world, rank, local):
+    """linear_solver<double, B200> CHOLESKY mode at order args.chol_n: each
+    step restores m and x (device copies), factors (bit-identical to the
+    reference's NATIVE factor) and solves in place."""
+    import torch
+
+    import linearalgebra_b200 as la
+    from linearalgebra_b200 import _lib
+
+    lib = _lib.load()
+    n = args.chol_n
+    dev = torch.device("cuda", local)
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(SEED + 2 + rank)
+    R = torch.randn(n, n, dtype=torch.float64, device=dev, generator=gen)
+    A = torch.mm(R, R.t())
+    A.diagonal().add_(float(n))
+    del R
+    b = torch.randn(n, dtype=torch.float64, device=dev, generator=gen)
+    m, x = torch.empty_like(A), torch.empty_like(b)
+    piv = torch.empty(n, dtype=torch.int64, device=dev)
+    nbytes = la.linear_solver.workspace_size(n, la.CHOLESKY_LINEAR_SOLVER)
+    ws = torch.empty(max(nbytes, 256), dtype=torch.uint8, device=dev)
+    stream = torch.cuda.current_stream(dev)
+
+    def step():
+        m.copy_(A)
+        x.copy_(b)
+        la.linear_solver.apply(m, piv, n, x, la.CHOLESKY_LINEAR_SOLVER, ws, nbytes, stream)
+
+    steps = 3
+    step()
+    torch.cuda.synchronize()
+    lib.b200la_profile_start(sum(1 << c for c in CLASS_NAMES))
+    step()
+    torch.cuda.synchronize()
+    breakdown = {}
+    for c, name in CLASS_NAMES.items():
+        t_ms, cnt = ctypes.c_double(0), ctypes.c_int64(0)
+        lib.b200la_profile_stop(c, ctypes.addressof(t_ms), ctypes.addressof(cnt))
+        if cnt.value:
+            breakdown[name] = {"ms": round(t_ms.value, 3), "launches": int(cnt.value)}
+    lib.b200la_profile_start(1 << 12)
+    barrier(world)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier(world)
+    k_ms, k_n = ctypes.c_double(0), ctypes.c_int64(0)
+    lib.b200la_profile_stop(12, ctypes.addressof(k_ms), ctypes.addressof(k_n))
+    t = max_over_ranks(world, e0.elapsed_time(e1) / steps) / 1e3
+    r = (torch.mv(A, x) - b).abs().max().item()
+    eta = r / (torch.linalg.matrix_norm(A, ord=float("inf")).item() * x.abs().max().item() + b.abs().max().item())
+    fl = cholesky_update_flops(n)
+    # every product of the update is rounded on its own (the reference's
+    # compiled loop), so it runs as a DMUL and a DADD on the FP64 pipe, not
+    # as fused or tensor-core work: its bound is half the FP64 peak
+    peak = measured_fp64_peak_tflops() / 2
+    achieved = fl * steps / (k_ms.value * 1e-3) / 1e12 if k_ms.value else None
+    out = {"n": n, "s": t, "steps": steps, "backward_error": eta,
+           "roofline": {"kernel": "k_chol_syrk (trailing lower-triangle update, FP64 pipe)", "bound": "fp64_unfused",
+                        "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                        "frac": achieved / peak if achieved else None,
+                        "peak_source": "half of cuBLAS DGEMM 8192^3 (torch.matmul, best of 5, measured in this run): "
+                                       "one separately rounded multiply and one add per term",
+                        "flops_per_step": fl, "launches": int(k_n.value),
+                        "share_of_step": (k_ms.value / steps / 1e3) / t if t else None},
+           "breakdown_one_step": breakdown}
+    del m, x, ws
+    torch.cuda.empty_cache()
+    path = os.path.join(ROOT, "baseline", "_ref", "libref_cublas.so")
+    if rank == 0 and world == 1 and os.path.exists(path):
+        out["cuda_blas"] = cuda_blas_cholesky(path, A, b, stream, steps)
+        out["speedup_vs_cuda_blas"] = out["cuda_blas"]["s"] / t
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        import numpy as np
+        from oracle import Oracle, available
+        from linearalgebra_b200.workloads import spd_matrix
+        kind = "reference" if available("reference") else "port"
+        o = Oracle(kind)
+        ns = 3072
+        a = spd_matrix(ns, seed=ns)
+        bb = np.ones(ns)
+        t0 = time.perf_counter()
+        o.gesv(a, bb, 3)
+        tc = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": tc * (n / ns) ** 3, "unit": "s", "cores": 1, "kind": kind,
+                               "sample": f"linear_solver<double,NATIVE> CHOLESKY mode at n={ns} ({tc:.2f} s) "
+                                         f"scaled by (n/{ns})^3 to n={n}; 1 thread"}
+    del A, b
+    torch.cuda.empty_cache()
+    return out
+
+
+# ---------------------------------------------------------------------------
 # multiplication: FP64 general product on the tensor cores vs measured cuBLAS
 # DGEMM, and batched_matrix_multiplication vs the reference's CUDA kernel
 # ---------------------------------------------------------------------------
@@ -515,7 +666,7 @@ TRAFFIC_PER_ALGORITHMIC_BYTE = {5: 0.913, 2: 0.766}
 
 CLASS_NAMES = {0: "panel", 1: "laswp_u12", 2: "trailing", 3: "solve", 4: "gemm", 5: "tc_update",
                6: "residual", 7: "batched", 8: "operand_prep", 9: "selector", 10: "inversion_gemm",
-               11: "inversion_aux"}
+               11: "inversion_aux", 12: "cholesky_update", 13: "cholesky_aux"}
 
 
 def algorithmic_work(n: int, method: str, nb_out: int = 256):
@@ -809,6 +960,10 @@ def run_b200(args, world, rank, local):
     if not args.no_multiplication:
         multiplication = run_multiplication(args, world, rank, local)
 
+    cholesky = None
+    if not args.no_cholesky:
+        cholesky = run_cholesky(args, world, rank, local)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         kind, t, ceta = cpu_reference_solve_seconds(CPU_SAMPLE_N)
@@ -858,6 +1013,7 @@ def run_b200(args, world, rank, local):
             "batched": batched,
             "inversion": inversion,
             "multiplication": multiplication,
+            "cholesky": cholesky,
             "clocks": clk,
             "peaks": peaks,
         }
