@@ -25,6 +25,7 @@
 #include "include/matrix_operation/inversion.h"
 #include "include/matrix_operation/linear_solver.h"
 #include "include/matrix_operation/multiplication_batched.h"
+#include "include/matrix_operation/transpose.h"
 
 using linalg::linalg_backend;
 using linalg::linear_solver_type;
@@ -89,6 +90,35 @@ int ref_cublas_dcholesky_solve(double* m, int64_t n, double* x, void* ws, size_t
     {
         linalg::linear_solver<double, linalg_backend::CUDA_BLAS>::apply(m, nullptr, n, x,
             linear_solver_type::CHOLESKY_LINEAR_SOLVER, ws, ws_bytes, stream);
+        return 0;
+    }
+    catch (const std::exception& e)
+    {
+        g_err = e.what();
+        return -1;
+    }
+}
+
+/* transpose<double, CUDA_BLAS> in place (cuBLAS geam into scratch, then a
+ * device-to-device copy back). */
+size_t ref_cublas_dtranspose_workspace_size(int64_t rows, int64_t cols)
+{
+    try
+    {
+        return linalg::transpose<double, linalg_backend::CUDA_BLAS>::workspace_size(rows, cols);
+    }
+    catch (const std::exception& e)
+    {
+        g_err = e.what();
+        return 0;
+    }
+}
+
+int ref_cublas_dtranspose(int64_t rows, int64_t cols, double* m, void* ws, size_t ws_bytes, void* stream)
+{
+    try
+    {
+        linalg::transpose<double, linalg_backend::CUDA_BLAS>::apply(rows, cols, m, ws, ws_bytes, stream);
         return 0;
     }
     catch (const std::exception& e)

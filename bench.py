@@ -61,6 +61,7 @@ def parse():
     p.add_argument("--no-multiplication", action="store_true")
     p.add_argument("--chol-n", type=int, default=16384, help="order of the Cholesky-mode solve measurement")
     p.add_argument("--no-cholesky", action="store_true")
+    p.add_argument("--no-transpose", action="store_true")
     return p.parse_args()
 
 
@@ -506,6 +507,85 @@ def run_cholesky(args, world, rank, local):
 
 
 # ---------------------------------------------------------------------------
+# transpose: in place (square: one read and one write per element) and out of
+# place, vs the reference's CUDA_BLAS transpose (geam into scratch + copy)
+# ---------------------------------------------------------------------------
+def run_transpose(args, world, rank, local):
+    import torch
+
+    import linearalgebra_b200 as la
+    from linearalgebra_b200 import api
+
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.current_stream(dev)
+    pk = measured_peaks()
+    peak, peak_src = pk["hbm_gbs"], pk["source"]
+    n = 16384
+    m = torch.randn(n, n, dtype=torch.float64, device=dev)
+    dst = torch.empty_like(m)
+
+    def timed(fn, steps=5):
+        fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / steps / 1e3
+
+    # an even number of in-place transposes leaves m as it was
+    t_sq = timed(lambda: api.transpose.apply(n, n, m, None, 0, stream), steps=6)
+    t_out = timed(lambda: la.transpose_out(m, dst, stream))
+    rows, cols = 8192, 32768
+    r = torch.randn(rows, cols, dtype=torch.float64, device=dev)
+    nb = api.transpose.workspace_size(rows, cols)
+    ws = torch.empty(nb, dtype=torch.uint8, device=dev)
+    state = {"shape": (rows, cols)}
+
+    def rect():
+        rr, cc = state["shape"]
+        api.transpose.apply(rr, cc, r, ws, nb, stream)
+        state["shape"] = (cc, rr)
+
+    t_rect = timed(rect, steps=4)
+    sq_bytes = 16 * n * n
+    out = {"square": {"n": n, "s": t_sq, "bytes": sq_bytes, "gbs": sq_bytes / t_sq / 1e9},
+           "out_of_place": {"n": n, "s": t_out, "bytes": sq_bytes, "gbs": sq_bytes / t_out / 1e9},
+           "rectangular_in_place": {"rows": rows, "columns": cols, "s": t_rect, "bytes": 32 * rows * cols,
+                                    "gbs": 32 * rows * cols / t_rect / 1e9,
+                                    "note": "transpose into the workspace, then one device copy back"},
+           "roofline": {"kernel": "k_transpose_square (in place, n=16384 FP64)", "bound": "hbm",
+                        "achieved": sq_bytes / t_sq / 1e9, "peak": peak, "unit": "GB/s",
+                        "frac": sq_bytes / t_sq / 1e9 / peak, "peak_source": peak_src},
+           "dtype": "f64"}
+    del r, ws
+    path = os.path.join(ROOT, "baseline", "_ref", "libref_cublas.so")
+    if rank == 0 and world == 1 and os.path.exists(path):
+        lib = ctypes.CDLL(path)
+        lib.ref_cublas_dtranspose_workspace_size.restype = ctypes.c_size_t
+        lib.ref_cublas_dtranspose_workspace_size.argtypes = [ctypes.c_int64, ctypes.c_int64]
+        lib.ref_cublas_dtranspose.argtypes = [ctypes.c_int64, ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p,
+                                              ctypes.c_size_t, ctypes.c_void_p]
+        rb = int(lib.ref_cublas_dtranspose_workspace_size(n, n))
+        rws = torch.empty(max(rb, 256), dtype=torch.uint8, device=dev)
+
+        def ref_step():
+            if lib.ref_cublas_dtranspose(n, n, m.data_ptr(), rws.data_ptr(), rb, stream.cuda_stream) != 0:
+                raise RuntimeError("reference transpose failed")
+
+        t_ref = timed(ref_step, steps=6)
+        out["cuda_blas"] = {"s": t_ref, "what": "the reference's transpose<double,CUDA_BLAS> (cuBLAS geam into "
+                                                "scratch, device copy back), n=16384 in place"}
+        out["speedup_vs_cuda_blas"] = t_ref / t_sq
+        del rws
+    del m, dst
+    torch.cuda.empty_cache()
+    return out
+
+
+# ---------------------------------------------------------------------------
 # multiplication: FP64 general product on the tensor cores vs measured cuBLAS
 # DGEMM, and batched_matrix_multiplication vs the reference's CUDA kernel
 # ---------------------------------------------------------------------------
@@ -666,7 +746,7 @@ TRAFFIC_PER_ALGORITHMIC_BYTE = {5: 0.913, 2: 0.766}
 
 CLASS_NAMES = {0: "panel", 1: "laswp_u12", 2: "trailing", 3: "solve", 4: "gemm", 5: "tc_update",
                6: "residual", 7: "batched", 8: "operand_prep", 9: "selector", 10: "inversion_gemm",
-               11: "inversion_aux", 12: "cholesky_update", 13: "cholesky_aux"}
+               11: "inversion_aux", 12: "cholesky_update", 13: "cholesky_aux", 14: "transpose"}
 
 
 def algorithmic_work(n: int, method: str, nb_out: int = 256):
@@ -964,6 +1044,10 @@ def run_b200(args, world, rank, local):
     if not args.no_cholesky:
         cholesky = run_cholesky(args, world, rank, local)
 
+    transpose = None
+    if not args.no_transpose:
+        transpose = run_transpose(args, world, rank, local)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         kind, t, ceta = cpu_reference_solve_seconds(CPU_SAMPLE_N)
@@ -1014,6 +1098,7 @@ def run_b200(args, world, rank, local):
             "inversion": inversion,
             "multiplication": multiplication,
             "cholesky": cholesky,
+            "transpose": transpose,
             "clocks": clk,
             "peaks": peaks,
         }

@@ -66,7 +66,7 @@ B200LA_API int64_t b200la_launch_count(void);
  * and matrix statistics, 10 inversion GEMM updates, 11 inversion and
  * determinant helpers: identity, column gather, diagonal product,
  * 12 Cholesky trailing updates, 13 Cholesky diagonal blocks, panel solves,
- * zeroing and transposition) is
+ * zeroing and transposition, 14 transpose) is
  * bracketed by a
  * pair of CUDA events on its stream.  b200la_profile_stop synchronizes those
  * events and returns the summed device time (ms) and launch count of one
@@ -247,6 +247,27 @@ B200LA_API int b200la_dgemm_batched(int64_t dim, int64_t count, const double* a,
     void* stream);
 B200LA_API int b200la_sgemm_batched(int64_t dim, int64_t count, const float* a, const float* b, float* c,
     void* stream);
+
+/* ---- transpose and row-major <-> column-major interop -----------------------
+ * Replaces transpose<T, Backend>::apply / ::workspace_size
+ * (include/matrix_operation/transpose.h; CUDA_BLAS src/matrix_operation/gpu/
+ * cublas/transpose_cublas.cpp:25-57, NATIVE src/matrix_operation/cpu/native/
+ * transpose_native.cpp): the row-major rows x columns matrix m becomes its
+ * row-major columns x rows transpose, in place.  A square matrix needs no
+ * workspace (workspace_size returns 0); otherwise the workspace holds
+ * rows*columns elements.  rows and columns must be positive.  Asynchronous.
+ * b200la_?transpose_out writes the transpose of src into dst (no overlap),
+ * which is also the column-major copy of a row-major matrix and back:
+ * the interop between this backend's row-major buffers and column-major
+ * BLAS buffers.  Extension, no reference counterpart. */
+B200LA_API size_t b200la_dtranspose_workspace_size(int64_t rows, int64_t columns);
+B200LA_API size_t b200la_stranspose_workspace_size(int64_t rows, int64_t columns);
+B200LA_API int b200la_dtranspose(int64_t rows, int64_t columns, double* m, void* workspace, size_t workspace_bytes,
+    void* stream);
+B200LA_API int b200la_stranspose(int64_t rows, int64_t columns, float* m, void* workspace, size_t workspace_bytes,
+    void* stream);
+B200LA_API int b200la_dtranspose_out(int64_t rows, int64_t columns, const double* src, double* dst, void* stream);
+B200LA_API int b200la_stranspose_out(int64_t rows, int64_t columns, const float* src, float* dst, void* stream);
 
 /* ---- mixed-precision LU solve with FP64 iterative refinement --------------
  * Solves A X = B (A n x n FP64, row stride n, left unchanged; B, X n x nrhs,

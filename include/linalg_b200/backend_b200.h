@@ -104,4 +104,11 @@ template <> size_t determinant<double, linalg_backend::B200>::workspace_size(lin
     linear_solver_type);
 template <> size_t determinant<float, linalg_backend::B200>::workspace_size(linalg_int,
     linear_solver_type);
+
+template <> void transpose<double, linalg_backend::B200>::apply(linalg_long, linalg_long, double*, void*,
+    size_t, void*);
+template <> void transpose<float, linalg_backend::B200>::apply(linalg_long, linalg_long, float*, void*,
+    size_t, void*);
+template <> size_t transpose<double, linalg_backend::B200>::workspace_size(linalg_long, linalg_long);
+template <> size_t transpose<float, linalg_backend::B200>::workspace_size(linalg_long, linalg_long);
 }  // namespace linalg

@@ -11,6 +11,7 @@
  *   include/matrix_operation/determinant.h
  *   include/matrix_operation/multiplication_batched.h
  *   include/matrix_operation/cholesky_decomposition.h:15-94
+ *   include/matrix_operation/transpose.h
  * Names, argument order, default arguments and meaning are the reference's;
  * that is what makes the backend a drop-in.  Inside the reference tree define
  * LINALG_B200_USE_REFERENCE_HEADERS and add B200 as the last enumerator of
@@ -31,6 +32,7 @@
 #include "include/matrix_operation/lu_decomposition.h"
 #include "include/matrix_operation/multiplication.h"
 #include "include/matrix_operation/multiplication_batched.h"
+#include "include/matrix_operation/transpose.h"
 #include "include/matrix_operation/triangular_solver.h"
 #else
 
@@ -140,6 +142,13 @@ template <typename T, linalg_backend Backend> struct determinant
     LINALG_API static T apply(T* m, linalg_int* pivot, linalg_int lda, linear_solver_type type,
         void* workspace, size_t workspace_size, void* stream = nullptr);
     LINALG_API static size_t workspace_size(linalg_int lda, linear_solver_type type);
+};
+
+template <typename T, linalg_backend Backend> struct transpose
+{
+    LINALG_API static void apply(linalg_long rows, linalg_long columns, T* m, void* workspace,
+        size_t workspace_size, void* stream = nullptr);
+    LINALG_API static size_t workspace_size(linalg_long rows, linalg_long columns);
 };
 }  // namespace linalg
 #endif

@@ -30,6 +30,9 @@ from .api import (  # noqa: F401
     multiplication,
     potrf,
     solve_mixed,
+    transpose,
+    transpose_in_place,
+    transpose_out,
     triangular_solver,
     trsm,
 )

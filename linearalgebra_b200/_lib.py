@@ -76,6 +76,12 @@ SIGNATURES: dict[str, tuple] = {
     "b200la_spotrf": (_i32, [_p, _i64, _i32, _p, _sz, _p, _p]),
     "b200la_dgemm_batched": (_i32, [_i64, _i64, _p, _p, _p, _p]),
     "b200la_sgemm_batched": (_i32, [_i64, _i64, _p, _p, _p, _p]),
+    "b200la_dtranspose_workspace_size": (_sz, [_i64, _i64]),
+    "b200la_stranspose_workspace_size": (_sz, [_i64, _i64]),
+    "b200la_dtranspose": (_i32, [_i64, _i64, _p, _p, _sz, _p]),
+    "b200la_stranspose": (_i32, [_i64, _i64, _p, _p, _sz, _p]),
+    "b200la_dtranspose_out": (_i32, [_i64, _i64, _p, _p, _p]),
+    "b200la_stranspose_out": (_i32, [_i64, _i64, _p, _p, _p]),
     "b200la_refine_default_options": (None, [_p]),
     "b200la_dsolve_mixed_workspace_size": (_sz, [_i64, _i64, _p]),
     "b200la_dsolve_mixed": (_i32, [_p, _i64, _i64, _p, _i64, _p, _i64, _p, _p, _p, _sz, _p]),

@@ -157,6 +157,41 @@ def batched_matrix_multiplication(dim: int, count: int, a, b, c, stream=None):
     _lib.check(f(dim, count, _ptr(a), _ptr(b), _ptr(c), _stream(stream)))
 
 
+class transpose:
+    """transpose<T, B200> (include/matrix_operation/transpose.h): the row-major
+    rows x columns matrix m becomes its columns x rows transpose in place."""
+
+    @staticmethod
+    def workspace_size(rows: int, columns: int, dtype=torch.float64) -> int:
+        return int(getattr(_lib.load(), f"b200la_{_prefix(dtype)}transpose_workspace_size")(rows, columns))
+
+    @staticmethod
+    def apply(rows: int, columns: int, m, workspace=None, workspace_size: int = 0, stream=None):
+        f = getattr(_lib.load(), f"b200la_{_prefix(m.dtype)}transpose")
+        _lib.check(f(rows, columns, _ptr(m), _ptr(workspace), workspace_size, _stream(stream)))
+
+
+def transpose_in_place(m: torch.Tensor, stream=None) -> torch.Tensor:
+    """Transpose the contiguous 2-D tensor m in its own storage; returns the
+    (columns, rows) view of that storage."""
+    rows, cols = m.shape
+    nbytes = transpose.workspace_size(rows, cols, m.dtype)
+    ws = workspace(nbytes, m.device) if nbytes else None
+    transpose.apply(rows, cols, m, ws, nbytes, stream)
+    return m.view(cols, rows)
+
+
+def transpose_out(src: torch.Tensor, dst: torch.Tensor | None = None, stream=None) -> torch.Tensor:
+    """dst = src^T for a contiguous 2-D src (the column-major copy of a
+    row-major matrix, and back)."""
+    rows, cols = src.shape
+    if dst is None:
+        dst = torch.empty(cols, rows, dtype=src.dtype, device=src.device)
+    f = getattr(_lib.load(), f"b200la_{_prefix(src.dtype)}transpose_out")
+    _lib.check(f(rows, cols, _ptr(src), _ptr(dst), _stream(stream)))
+    return dst
+
+
 class inversion:
     """inversion<T, B200>, LU modes (include/matrix_operation/inversion.h:15-53)."""
 

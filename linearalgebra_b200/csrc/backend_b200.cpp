@@ -195,6 +195,34 @@ size_t multiplication<float, linalg_backend::B200>::workspace_size(
     return b200la_sgemm_workspace_size(rows, columns, depth);
 }
 
+// ---- transpose --------------------------------------------------------------
+namespace
+{
+// rows / columns above INT64_MAX cannot describe a device matrix; they reach
+// the C ABI as negative values, which it rejects like zero
+int64_t extent(linalg_long v) { return static_cast<int64_t>(v); }
+}  // namespace
+template <>
+void transpose<double, linalg_backend::B200>::apply(linalg_long rows, linalg_long columns, double* m,
+    void* workspace, size_t workspace_size, void* stream)
+{
+    check_status(b200la_dtranspose(extent(rows), extent(columns), m, workspace, workspace_size, stream));
+}
+template <>
+void transpose<float, linalg_backend::B200>::apply(linalg_long rows, linalg_long columns, float* m,
+    void* workspace, size_t workspace_size, void* stream)
+{
+    check_status(b200la_stranspose(extent(rows), extent(columns), m, workspace, workspace_size, stream));
+}
+template <> size_t transpose<double, linalg_backend::B200>::workspace_size(linalg_long rows, linalg_long columns)
+{
+    return b200la_dtranspose_workspace_size(extent(rows), extent(columns));
+}
+template <> size_t transpose<float, linalg_backend::B200>::workspace_size(linalg_long rows, linalg_long columns)
+{
+    return b200la_stranspose_workspace_size(extent(rows), extent(columns));
+}
+
 // ---- inversion --------------------------------------------------------------
 template <>
 void inversion<double, linalg_backend::B200>::apply(double* m, linalg_int* pivot, linalg_int lda,

@@ -134,7 +134,8 @@ enum KernelClass : int
     KC_INV_AUX  = 11,  // inversion / determinant: identity, column gather, diagonal product
     KC_CHOL_UPD = 12,  // Cholesky: the trailing lower-triangle updates
     KC_CHOL_AUX = 13,  // Cholesky: diagonal blocks, panel solves, zeroing, transposition
-    KC_COUNT    = 14
+    KC_TRANSPOSE = 14, // transpose and the out-of-place interop copy
+    KC_COUNT    = 15
 };
 
 // Host helpers shared by the entry points (defined in runtime.cu).

@@ -85,6 +85,9 @@ class Oracle:
             f = getattr(self.lib, f"{pre}{t}potrf")
             f.argtypes = [_p, _i64, _int, _p]
             f.restype = _int
+            f = getattr(self.lib, f"{pre}{t}transpose")
+            f.argtypes = [_i64, _i64, _p] + ([_p] if kind == "port" else [])
+            f.restype = _int
             f = getattr(self.lib, f"{pre}{t}getri")
             f.argtypes = [_p, _p, _i64, _int]
             f.restype = _int
@@ -158,6 +161,21 @@ class Oracle:
         if st < 0:
             raise ValueError(f"potrf rejected its arguments (status {st})")
         return m, int(info.value)
+
+    def transpose(self, a: np.ndarray) -> np.ndarray:
+        """transpose::apply on a copy of the row-major 2-D array a; returns
+        the (columns, rows) result."""
+        m = np.ascontiguousarray(a).copy()
+        rows, cols = m.shape
+        f = getattr(self.lib, f"{self._pre}{self._t(m)}transpose")
+        if self.kind == "port":
+            scratch = np.empty(rows * cols, dtype=m.dtype)
+            st = f(rows, cols, _ptr(m), _ptr(scratch))
+        else:
+            st = f(rows, cols, _ptr(m))
+        if st < 0:
+            raise ValueError(f"transpose rejected its arguments (status {st})")
+        return m.reshape(cols, rows)
 
     def gemm_batched(self, a: np.ndarray, b: np.ndarray) -> np.ndarray:
         """c_i = a_i b_i for (count, dim, dim) arrays, the reference CUDA

@@ -566,6 +566,46 @@ void OR_FN(potrs)(const T* m, int64_t n, T* x)
     }
 }
 
+/* transpose::apply, transpose_native.cpp: the row-major rows x cols matrix
+ * m becomes its row-major cols x rows transpose in place.  Square: the
+ * reference swaps m[i][j] and m[j][i] (j > i) tile by tile; otherwise it
+ * follows the permutation cycles of the in-place transposition.  Both are
+ * data movement, so this restatement swaps the square case and transposes
+ * the other through scratch (rows*cols elements) and copies back: the same
+ * result.  Returns -1 for invalid arguments. */
+int OR_FN(transpose)(int64_t rows, int64_t cols, T* m, T* scratch)
+{
+    if (!m || rows <= 0 || cols <= 0 || (rows != cols && !scratch))
+    {
+        return -1;
+    }
+    if (rows == cols)
+    {
+        for (int64_t i = 0; i < rows; ++i)
+        {
+            for (int64_t j = i + 1; j < rows; ++j)
+            {
+                const T t        = m[i * rows + j];
+                m[i * rows + j]  = m[j * rows + i];
+                m[j * rows + i]  = t;
+            }
+        }
+        return 0;
+    }
+    for (int64_t i = 0; i < rows; ++i)
+    {
+        for (int64_t j = 0; j < cols; ++j)
+        {
+            scratch[j * rows + i] = m[i * cols + j];
+        }
+    }
+    for (int64_t e = 0; e < rows * cols; ++e)
+    {
+        m[e] = scratch[e];
+    }
+    return 0;
+}
+
 /* Batched product c_i = a_i b_i of `count` packed dim x dim matrices:
  * multiplication_batched_cublas.cu:15-40 (batched_matmul_kernel: each entry
  * sum += a b from zero in k order, which nvcc contracts into fused

@@ -27,6 +27,7 @@
 #include "include/matrix_operation/linear_solver.h"
 #include "include/matrix_operation/lu_decomposition.h"
 #include "include/matrix_operation/multiplication.h"
+#include "include/matrix_operation/transpose.h"
 #include "include/matrix_operation/triangular_solver.h"
 
 using linalg::linalg_backend;
@@ -194,6 +195,24 @@ template <typename T> int ref_det(T* m, int64_t* pivot, int64_t n, int type, T* 
         return -1;
     }
 }
+template <typename T> int ref_transpose(int64_t rows, int64_t cols, T* m)
+{
+    try
+    {
+        const size_t bytes = linalg::transpose<T, linalg_backend::NATIVE>::workspace_size(rows, cols);
+        std::vector<unsigned char> ws(bytes ? bytes : 1);
+        linalg::transpose<T, linalg_backend::NATIVE>::apply(rows, cols, m, ws.data(), bytes);
+        return 0;
+    }
+    catch (const std::bad_alloc&)
+    {
+        return -2;
+    }
+    catch (...)
+    {
+        return -1;
+    }
+}
 }  // namespace
 
 extern "C" {
@@ -257,6 +276,14 @@ int ref_ddet(double* m, int64_t* pivot, int64_t n, int type, double* out)
 int ref_sdet(float* m, int64_t* pivot, int64_t n, int type, float* out)
 {
     return ref_det(m, pivot, n, type, out);
+}
+int ref_dtranspose(int64_t rows, int64_t cols, double* m)
+{
+    return ref_transpose(rows, cols, m);
+}
+int ref_stranspose(int64_t rows, int64_t cols, float* m)
+{
+    return ref_transpose(rows, cols, m);
 }
 size_t ref_dgetrf_workspace_size(int64_t n)
 {

@@ -11,6 +11,7 @@
 #include <cstdlib>
 #include <random>
 #include <stdexcept>
+#include <utility>
 #include <vector>
 
 #include "linalg_b200/backend_b200.h"
@@ -358,6 +359,38 @@ static void test_cholesky()
         "cholesky_decomposition<float>: [[4,2],[2,5]] -> [[2,0],[1,2]]");
 }
 
+static void test_transpose()
+{
+    using TD = linalg::transpose<double, B>;
+    for (auto shape : {std::pair<int, int>{130, 130}, std::pair<int, int>{70, 200}})
+    {
+        const int           rows = shape.first, cols = shape.second;
+        std::vector<double> a((size_t)rows * cols);
+        for (size_t e = 0; e < a.size(); ++e) a[e] = (double)e;
+        dbuf<double>        dm(a.size());
+        dm.up(a);
+        const size_t        bytes = TD::workspace_size(rows, cols);
+        dbuf<unsigned char> ws(bytes ? bytes : 1);
+        TD::apply(rows, cols, dm.p, ws.p, bytes);
+        cudaDeviceSynchronize();
+        const auto t  = dm.down();
+        bool       ok = (rows == cols) == (bytes == 0);
+        for (int i = 0; i < rows; ++i)
+            for (int j = 0; j < cols; ++j) ok = ok && t[(size_t)j * rows + i] == a[(size_t)i * cols + j];
+        CHECK(ok, rows == cols ? "transpose square, in place, no workspace" : "transpose 70 x 200 through the workspace");
+    }
+    bool threw = false;
+    try
+    {
+        TD::apply(0, 4, nullptr, nullptr, 0);
+    }
+    catch (const std::invalid_argument&)
+    {
+        threw = true;
+    }
+    CHECK(threw, "transpose: null matrix throws std::invalid_argument");
+}
+
 static void test_batched_multiplication()
 {
     const int dim = 37, count = 4;
@@ -396,6 +429,7 @@ int main()
     test_singular_status();
     test_inversion_determinant();
     test_cholesky();
+    test_transpose();
     test_batched_multiplication();
     std::printf("%s (%d failures)\n", g_fail ? "FAILED" : "ALL PASSED", g_fail);
     return g_fail ? 1 : 0;
