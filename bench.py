@@ -62,6 +62,7 @@ def parse():
     p.add_argument("--chol-n", type=int, default=16384, help="order of the Cholesky-mode solve measurement")
     p.add_argument("--no-cholesky", action="store_true")
     p.add_argument("--no-transpose", action="store_true")
+    p.add_argument("--tp-n", type=int, default=16384, help="order of the square transpose measurement")
     return p.parse_args()
 
 
@@ -520,7 +521,7 @@ def run_transpose(args, world, rank, local):
     stream = torch.cuda.current_stream(dev)
     pk = measured_peaks()
     peak, peak_src = pk["hbm_gbs"], pk["source"]
-    n = 16384
+    n = args.tp_n
     m = torch.randn(n, n, dtype=torch.float64, device=dev)
     dst = torch.empty_like(m)
 
@@ -538,7 +539,7 @@ def run_transpose(args, world, rank, local):
     # an even number of in-place transposes leaves m as it was
     t_sq = timed(lambda: api.transpose.apply(n, n, m, None, 0, stream), steps=6)
     t_out = timed(lambda: la.transpose_out(m, dst, stream))
-    rows, cols = 8192, 32768
+    rows, cols = n // 2, n * 2
     r = torch.randn(rows, cols, dtype=torch.float64, device=dev)
     nb = api.transpose.workspace_size(rows, cols)
     ws = torch.empty(nb, dtype=torch.uint8, device=dev)
@@ -556,7 +557,7 @@ def run_transpose(args, world, rank, local):
            "rectangular_in_place": {"rows": rows, "columns": cols, "s": t_rect, "bytes": 32 * rows * cols,
                                     "gbs": 32 * rows * cols / t_rect / 1e9,
                                     "note": "transpose into the workspace, then one device copy back"},
-           "roofline": {"kernel": "k_transpose_square (in place, n=16384 FP64)", "bound": "hbm",
+           "roofline": {"kernel": f"k_transpose_square (in place, n={n} FP64)", "bound": "hbm",
                         "achieved": sq_bytes / t_sq / 1e9, "peak": peak, "unit": "GB/s",
                         "frac": sq_bytes / t_sq / 1e9 / peak, "peak_source": peak_src},
            "dtype": "f64"}
@@ -577,7 +578,7 @@ def run_transpose(args, world, rank, local):
 
         t_ref = timed(ref_step, steps=6)
         out["cuda_blas"] = {"s": t_ref, "what": "the reference's transpose<double,CUDA_BLAS> (cuBLAS geam into "
-                                                "scratch, device copy back), n=16384 in place"}
+                                                f"scratch, device copy back), n={n} in place"}
         out["speedup_vs_cuda_blas"] = t_ref / t_sq
         del rws
     del m, dst
