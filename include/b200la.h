@@ -198,7 +198,7 @@ B200LA_API int    b200la_dinverse(double* m, int64_t* pivot, int64_t n, int mode
 B200LA_API int    b200la_sinverse(float* m, int64_t* pivot, int64_t n, int mode, void* workspace,
        size_t workspace_bytes, void* stream);
 
-/* ---- determinant (LU modes) -------------------------------------------------
+/* ---- determinant (LU and Cholesky modes) -------------------------------------
  * Replaces determinant<T, Backend>::apply / ::workspace_size
  * (include/matrix_operation/determinant.h; src/matrix_operation/cpu/
  * determinant.cpp:18-27,56-80).  Mode B200LA_LU_LINEAR_SOLVER factors m in
@@ -210,7 +210,13 @@ B200LA_API int    b200la_sinverse(float* m, int64_t* pivot, int64_t n, int mode,
  * pivot[i] != i+1), may be NULL, so that det(A) = sign * product (the
  * reference's NATIVE reduction omits this sign, its CUDA_BLAS one applies
  * it); *log_abs = sum of log|u_ii|, may be NULL, finite where the product
- * over- or underflows.  Synchronous (the reference returns the value). */
+ * over- or underflows.  Cholesky modes (determinant.cpp:28-37,80-90):
+ * B200LA_CHOLESKY_LINEAR_SOLVER factors m (lower, bit-identical to NATIVE)
+ * and B200LA_CHOLESKY_UPFRONT_LINEAR_SOLVER reads the given lower factor;
+ * *product = the product of the factor's diagonal in index order (NATIVE's
+ * value, which is sqrt(det A); 0 and B200LA_SINGULAR when m is not positive
+ * definite), *sign = 1, *log_abs = log det(A) = 2 sum log l_ii; pivot is
+ * unused.  Synchronous (the reference returns the value). */
 B200LA_API size_t b200la_ddeterminant_workspace_size(int64_t n, int mode);
 B200LA_API size_t b200la_sdeterminant_workspace_size(int64_t n, int mode);
 B200LA_API int    b200la_ddeterminant(double* m, int64_t* pivot, int64_t n, int mode, double* product,

@@ -215,9 +215,11 @@ class determinant:
 
     @staticmethod
     def parts(m, pivot, lda: int, type: int, workspace, workspace_size: int, stream=None):
-        """(product, sign, log_abs, singular): U's diagonal product in index
-        order (the reference's NATIVE value), the pivot sign, sum log|u_ii|,
-        and whether LU mode met an exact zero pivot (product 0)."""
+        """(product, sign, log_abs, singular): the factor's diagonal product
+        in index order (the reference's NATIVE value: U's in the LU modes,
+        the Cholesky factor's, i.e. sqrt(det A), in the Cholesky modes), the
+        pivot sign (1 in the Cholesky modes), log|det A|, and whether the
+        factorization failed (product 0)."""
         ct = ctypes.c_double if m.dtype == torch.float64 else ctypes.c_float
         product, sign, log_abs = ct(0), ctypes.c_int(1), ctypes.c_double(0)
         f = getattr(_lib.load(), f"b200la_{_prefix(m.dtype)}determinant")
@@ -228,8 +230,11 @@ class determinant:
 
     @staticmethod
     def apply(m, pivot, lda: int, type: int, workspace, workspace_size: int, stream=None) -> float:
-        """det(A) = sign * product (0 when LU mode met an exact zero pivot)."""
+        """det(A): sign * product in the LU modes, product squared in the
+        Cholesky modes (0 when the factorization failed)."""
         product, sign, _, _ = determinant.parts(m, pivot, lda, type, workspace, workspace_size, stream)
+        if type in (CHOLESKY_LINEAR_SOLVER, CHOLESKY_UPFRONT_LINEAR_SOLVER):
+            return product * product
         return 0.0 if product == 0 else (-product if sign < 0 else product)
 
 

@@ -259,6 +259,11 @@ double determinant<double, linalg_backend::B200>::apply(double* m, linalg_int* p
     int    sign    = 1;
     check_status(b200la_ddeterminant(m, pv(pivot), lda, static_cast<int>(type), &product, &sign,
         nullptr, workspace, workspace_size, stream));
+    if (type == linear_solver_type::CHOLESKY_LINEAR_SOLVER ||
+        type == linear_solver_type::CHOLESKY_UPFRONT_LINEAR_SOLVER)
+    {
+        return product * product;  // det(A) = (prod l_ii)^2, as CUDA_BLAS returns it
+    }
     return product == 0.0 ? 0.0 : (sign < 0 ? -product : product);
 }
 template <>
@@ -269,6 +274,11 @@ float determinant<float, linalg_backend::B200>::apply(float* m, linalg_int* pivo
     int   sign    = 1;
     check_status(b200la_sdeterminant(m, pv(pivot), lda, static_cast<int>(type), &product, &sign,
         nullptr, workspace, workspace_size, stream));
+    if (type == linear_solver_type::CHOLESKY_LINEAR_SOLVER ||
+        type == linear_solver_type::CHOLESKY_UPFRONT_LINEAR_SOLVER)
+    {
+        return product * product;  // det(A) = (prod l_ii)^2, as CUDA_BLAS returns it
+    }
     return product == 0.0f ? 0.0f : (sign < 0 ? -product : product);
 }
 template <>

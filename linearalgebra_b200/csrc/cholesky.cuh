@@ -7,7 +7,9 @@
 // Rounding.  Every dot product of the reference (cholesky_dot, `sum += x*y`
 // from zero) is compiled by g++ -O3 with AVX2+FMA into full vectors of
 // products, each product rounded, added to the sum one by one in order, then
-// one half vector the same way, and the last products fused into the sum.
+// one half vector the same way, and the last products fused into the sum;
+// the pivot's dot(a_i, a_i, i) in double has no half vector
+// (chol_rend_pivot).
 // chol_dot reproduces that with separately rounded multiplies and adds
 // (__dmul_rn / __dadd_rn cannot be contracted), so these updates run on the
 // FP64 (or FP32) pipe, not the tensor cores, whose fused products would give
@@ -94,6 +96,30 @@ template <typename T> __host__ __device__ constexpr int chol_rend(int len)
 template <typename T> __device__ __forceinline__ T chol_term(T s, T x, T y, int term, int len)
 {
     return term < chol_rend<T>(len) ? rn_add(s, rn_mul(x, y)) : fma(x, y, s);
+}
+
+// The pivot's reduction dot(a_i, a_i, i) is compiled differently in the
+// reference build (the same row as both operands): for double, whole vectors
+// of 4 products rounded and the rest (up to 3) fused, no half vector; for
+// float as chol_rend.  Established by probing the reference build one call
+// site and length at a time.
+template <typename T> __host__ __device__ constexpr int chol_rend_pivot(int len)
+{
+    return sizeof(T) == 8 ? (len / 4) * 4 : chol_rend<T>(len);
+}
+
+// Term `term` of row i's sum s_ij (dot of length j) in the diagonal block:
+// the pivot's pattern when j == i (is_pivot, known at run time), the common
+// one otherwise.  The two differ only for a few (term, j) pairs, which are
+// known at compile time after unrolling; only those carry a select.
+template <typename T>
+__device__ __forceinline__ T chol_term_blk(T s, T x, T y, int term, int len, bool is_pivot)
+{
+    if (term >= chol_rend_pivot<T>(len) && term < chol_rend<T>(len))
+    {
+        return is_pivot ? fma(x, y, s) : rn_add(s, rn_mul(x, y));
+    }
+    return chol_term(s, x, y, term, len);
 }
 
 // Dynamic shared memory of the kernels below (padded rows of kCholNB + 1).
@@ -201,7 +227,7 @@ __global__ void __launch_bounds__(kCholNB) k_chol_diag(T* __restrict__ A, int n,
             {
                 if (j <= tid)
                 {
-                    s[j] = chol_term(s[j], v, blk[j][c], c, j);
+                    s[j] = chol_term_blk(s[j], v, blk[j][c], c, j, j == tid);
                 }
             }
         }

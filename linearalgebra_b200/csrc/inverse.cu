@@ -35,7 +35,12 @@
 // reference for the same factors), the pivot parity (the number of i with
 // pivot[i] != i+1) and, beyond the reference, log|det| for orders whose
 // product over- or underflows.  LU mode returns 0 when the factorization met
-// an exact zero pivot (determinant.cpp:66-75).
+// an exact zero pivot (determinant.cpp:66-75).  The Cholesky modes
+// (determinant.cpp:28-37,80-90) take the product of the lower Cholesky
+// factor's diagonal the same way (CHOLESKY factors m first with the
+// bit-exact blocked Cholesky and returns 0 if m is not positive definite;
+// CHOLESKY_UPFRONT reads the given factor); that product is sqrt(det A),
+// so log|det| is twice the sum of log l_ii.
 #include <cuda_runtime.h>
 
 #include <climits>
@@ -405,7 +410,7 @@ __global__ void __launch_bounds__(kDetThreads) k_det(const T* __restrict__ m, in
     double     lg    = 0.0;
     for (int i = threadIdx.x; i < n; i += kDetThreads)
     {
-        swaps += pivot[i] - 1 != i ? 1 : 0;
+        swaps += pivot != nullptr && pivot[i] - 1 != i ? 1 : 0;
         lg += log(fabs((double)m[(int64_t)i * (n + 1)]));
     }
 #pragma unroll
@@ -480,11 +485,17 @@ template <typename T> Plan<T> plan(Arena& a, int64_t n, bool with_w)
     return p;
 }
 
-bool valid_mode(int mode) { return mode == B200LA_LU_LINEAR_SOLVER || mode == B200LA_LU_UPFRONT_LINEAR_SOLVER; }
+bool lu_mode(int mode) { return mode == B200LA_LU_LINEAR_SOLVER || mode == B200LA_LU_UPFRONT_LINEAR_SOLVER; }
+bool chol_mode(int mode)
+{
+    return mode == B200LA_CHOLESKY_LINEAR_SOLVER || mode == B200LA_CHOLESKY_UPFRONT_LINEAR_SOLVER;
+}
+// inversion: the LU modes; determinant: the LU and Cholesky modes
+bool valid_mode(int mode, bool inversion) { return lu_mode(mode) || (!inversion && chol_mode(mode)); }
 
 template <typename T> size_t ws_size(int64_t n, int mode, bool with_w)
 {
-    if (n <= 0 || n > INT_MAX / 2 || !valid_mode(mode))
+    if (n <= 0 || n > INT_MAX / 2 || !valid_mode(mode, with_w))
     {
         return 0;
     }
@@ -504,12 +515,13 @@ int check_args(const void* m, const int64_t* pivot, int64_t n, int mode, const c
     {
         return set_error(B200LA_INVALID_ARGUMENT, "%s::apply: lda must be positive", op);
     }
-    if (mode == 3 || mode == 4)
+    const bool inversion = op[0] == 'i';
+    if (inversion && chol_mode(mode))
     {
         return set_error(B200LA_NOT_SUPPORTED,
             "%s: only the LU modes are provided by this backend (mode %d)", op, mode);
     }
-    if (!valid_mode(mode))
+    if (!valid_mode(mode, inversion))
     {
         return set_error(B200LA_INVALID_ARGUMENT, "unsupported linear_solver_type (%d)", mode);
     }
@@ -635,6 +647,18 @@ template <typename T> int enqueue_factor(T* m, int n, int64_t* piv, int mode, co
     if (mode == B200LA_LU_LINEAR_SOLVER)
     {
         return enqueue_getrf<T>(m, n, piv, p.gp, s);
+    }
+    if (mode == B200LA_CHOLESKY_LINEAR_SOLVER)
+    {
+        return enqueue_potrf<T>(m, n, false, p.gp.st, s);  // lower, as determinant.cpp factors
+    }
+    if (mode == B200LA_CHOLESKY_UPFRONT_LINEAR_SOLVER)
+    {
+        prof_begin(KC_INV_AUX, s);
+        k_status_init<<<1, 32, 0, s>>>(p.gp.st, nullptr);
+        prof_end(KC_INV_AUX, s);
+        B200LA_LAUNCH_CHECK();
+        return B200LA_SUCCESS;
     }
     prof_begin(KC_INV_AUX, s);
     k_status_init<<<1, 32, 0, s>>>(p.gp.st, p.gp.perm);
@@ -769,10 +793,11 @@ int determinant(T* m, int64_t* pivot, int64_t n, int mode, T* product, int* sign
         return st;
     }
     Arena        a(ws, bytes);
-    Plan<T>      p   = plan<T>(a, n, false);
-    cudaStream_t s   = as_stream(stream);
-    int64_t*     piv = pivot != nullptr ? pivot : p.piv;
-    st               = enqueue_factor<T>(m, (int)n, piv, mode, p, s);
+    Plan<T>      p    = plan<T>(a, n, false);
+    cudaStream_t s    = as_stream(stream);
+    const bool   chol = chol_mode(mode);
+    int64_t*     piv  = chol ? nullptr : pivot != nullptr ? pivot : p.piv;
+    st                = enqueue_factor<T>(m, (int)n, piv, mode, p, s);
     if (st != B200LA_SUCCESS)
     {
         return st;
@@ -796,7 +821,7 @@ int determinant(T* m, int64_t* pivot, int64_t n, int mode, T* product, int* sign
     }
     if (log_abs != nullptr)
     {
-        *log_abs = h.log_abs;
+        *log_abs = chol ? 2.0 * h.log_abs : h.log_abs;  // det(A) = (prod l_ii)^2
     }
     return h.skipped ? B200LA_SINGULAR : B200LA_SUCCESS;
 }

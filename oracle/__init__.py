@@ -203,9 +203,10 @@ class Oracle:
         return m, piv, int(st)
 
     def det(self, a: np.ndarray, mode: int = LU_LINEAR_SOLVER, pivot=None):
-        """determinant LU modes on a copy; returns (value, m, pivot): the
-        reference's value (U's diagonal product, no pivot sign; 0 when mode 1
-        met an exact zero pivot) and the factored matrix."""
+        """determinant on a copy; returns (value, m, pivot): the reference's
+        value (the factor's diagonal product: U's without the pivot sign in
+        the LU modes, L's in the Cholesky modes; 0 when mode 1 met an exact
+        zero pivot or mode 3 a non-positive one) and the factored matrix."""
         m = np.ascontiguousarray(a).copy()
         n = m.shape[0]
         piv = np.full(n, -1, dtype=np.int64) if pivot is None else np.ascontiguousarray(pivot, dtype=np.int64).copy()

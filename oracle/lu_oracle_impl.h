@@ -75,6 +75,34 @@ static T OR_CAT(dot_, SUF)(const T* a, const T* b, int64_t count)
     return OR_CAT(dots_, SUF)(a, 1, b, 1, count);
 }
 
+/* The Cholesky pivot's reduction, dot(a_i, a_i, i) in
+ * cholesky_decomposition_scalar_impl (both operands the same row): the
+ * reference build compiles this inlined call of cholesky_dot differently from
+ * its other call sites.  For double: whole vectors of 4 products rounded and
+ * added in order, then the remaining (up to 3) products fused, with no half
+ * vector; for float: as dots_.  Established by probing the reference build
+ * with inputs that isolate one dot product of each call site and length. */
+static T OR_CAT(dot_pivot_, SUF)(const T* a, int64_t count)
+{
+    if (sizeof(T) != 8)
+    {
+        return OR_CAT(dots_, SUF)(a, 1, a, 1, count);
+    }
+    const int64_t main = (count / 4) * 4;
+    T             s    = 0;
+    int64_t       j    = 0;
+    for (; j < main; ++j)
+    {
+        const T p = a[j] * a[j];
+        s         = s + p;
+    }
+    for (; j < count; ++j)
+    {
+        s = OR_FMA(a[j], a[j], s);
+    }
+    return s;
+}
+
 /* Unblocked panel factorization over columns [start, start+width), all rows
  * below: lu_decomposition_native.cpp:158-232 (lu_panel_factor).
  *  - pivot search: initial candidate |a[i][i]|, then rows i+1..n-1 with a
@@ -385,22 +413,25 @@ int OR_FN(getri)(T* m, int64_t* pivot, int64_t n, int mode)
     return st;
 }
 
-/* Determinant, determinant.cpp:18-27 (lu_determinant: the product of U's
- * diagonal in index order, no pivot sign) and :56-80 (LU modes): mode 1
- * factors m in place and returns the product if the factorization found no
- * exact zero pivot, else 0; mode 2 multiplies the diagonal of m as given.
- * *status: the getrf status (mode 1), 0 (mode 2) or -1 (invalid). */
+/* Determinant, determinant.cpp:18-37 (lu_determinant / cholesky_determinant:
+ * the product of the factor's diagonal in index order, no pivot sign, not
+ * squared for Cholesky) and :56-90 (modes): mode 1 factors m in place (LU)
+ * and returns the product if the factorization found no exact zero pivot,
+ * else 0; mode 3 likewise with the lower Cholesky factor (0 if m is not
+ * positive definite); modes 2 and 4 multiply the diagonal of m as given.
+ * *status: the factorization's status (modes 1, 3), 0 (modes 2, 4) or -1
+ * (invalid). */
 T OR_FN(det)(T* m, int64_t* pivot, int64_t n, int mode, int* status)
 {
     *status = -1;
-    if (m == NULL || n <= 0 || (mode != 1 && mode != 2) || (mode == 1 && pivot == NULL))
+    if (m == NULL || n <= 0 || mode < 1 || mode > 4 || (mode == 1 && pivot == NULL))
     {
         return (T)0;
     }
     *status = 0;
-    if (mode == 1)
+    if (mode == 1 || mode == 3)
     {
-        *status = OR_FN(getrf)(m, n, pivot, NULL);
+        *status = mode == 1 ? OR_FN(getrf)(m, n, pivot, NULL) : OR_FN(potrf)(m, n, 0, NULL);
         if (*status != 0)
         {
             return (T)0;
@@ -446,8 +477,8 @@ static T OR_CAT(dots_sub_, SUF)(T sum, const T* a, int64_t sa, const T* b, int64
 /* Unblocked Cholesky of the n x n diagonal block at A (row stride lda):
  * cholesky_decomposition_native.cpp (cholesky_decomposition_scalar_impl),
  * row by row: a_ij = (a_ij - dot(a_i, a_j, j)) / a_jj for j < i (a_ji = 0),
- * then a_ii = sqrt(a_ii - dot(a_i, a_i, i)); returns i + 1 at the first
- * non-positive pivot, else 0. */
+ * then a_ii = sqrt(a_ii - dot(a_i, a_i, i)) (dot_pivot_'s rounding);
+ * returns i + 1 at the first non-positive pivot, else 0. */
 static int64_t OR_CAT(potf2_, SUF)(int64_t n, T* A, int64_t lda)
 {
     for (int64_t i = 0; i < n; ++i)
@@ -460,7 +491,7 @@ static int64_t OR_CAT(potf2_, SUF)(int64_t n, T* A, int64_t lda)
             ai[j]       = sum / aj[j];
             aj[i]       = (T)0;
         }
-        const T sum = ai[i] - OR_CAT(dot_, SUF)(ai, ai, i);
+        const T sum = ai[i] - OR_CAT(dot_pivot_, SUF)(ai, i);
         if (sum <= (T)0)
         {
             return i + 1;

@@ -273,6 +273,13 @@ static void test_inversion_determinant()
     const double        det = linalg::determinant<double, B>::apply(dm.p, nullptr, n, type, dws.p, dbytes);
     CHECK(det > 0.0, "determinant of an SPD matrix is positive");
 
+    dm.up(a);
+    const auto   ctype  = linalg::linear_solver_type::CHOLESKY_LINEAR_SOLVER;
+    const size_t cbytes = linalg::determinant<double, B>::workspace_size(n, ctype);
+    dbuf<unsigned char> cws(cbytes);
+    const double cdet = linalg::determinant<double, B>::apply(dm.p, nullptr, n, ctype, cws.p, cbytes);
+    CHECK(std::fabs(cdet - det) <= 1e-10 * std::fabs(det), "determinant CHOLESKY mode == LU mode on an SPD matrix");
+
     dbuf<double> d2(4);
     d2.up({4.0, 0.0, 0.0, 2.0});
     cudaStream_t s = nullptr;

@@ -41,6 +41,7 @@ OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "lu_golden.npz")
 OUT_INV = os.path.join(os.path.dirname(os.path.abspath(__file__)), "inverse_golden.npz")
 OUT_CHOL = os.path.join(os.path.dirname(os.path.abspath(__file__)), "cholesky_golden.npz")
 CHOL_SIZES = (1, 2, 3, 17, 63, 64, 65, 130, 200)
+PIVOT_CASES = ((10, 100), (12, 312), (21, 111), (45, 345), (70, 370), (95, 7095))
 INV_SIZES = (1, 2, 3, 17, 64, 65, 130, 257)
 
 
@@ -184,6 +185,13 @@ def cholesky_main() -> None:
             out[f"cholfail_{dt}_{n}_{fr}_a_sha"] = np.array(sha(a))
             out[f"cholfail_{dt}_{n}_{fr}_m"] = f
             out[f"cholfail_{dt}_{n}_{fr}_info"] = np.array(info)
+    # inputs whose pivot dot products round differently in the pivot call
+    # site of the reference build than in its other call sites
+    for n, seed in PIVOT_CASES:
+        a = spd_matrix(n, seed=seed)
+        f, info = ref.potrf(a)
+        assert info == 0
+        out[f"pivot_{n}_{seed}_sha"] = np.array(sha(f))
     np.savez_compressed(OUT_CHOL, **out)
     print(f"wrote {OUT_CHOL}: {len(out)} arrays, {os.path.getsize(OUT_CHOL)} bytes")
 

@@ -82,6 +82,25 @@ def test_cholesky_not_positive_definite_state(port, cg, dt, npdt, n, fail_row):
     assert info_u == info and np.array_equal(fu, port.potrf(a, True)[0])
 
 
+@pytest.mark.parametrize("n,seed", [(10, 100), (12, 312), (21, 111), (45, 345), (70, 370), (95, 7095)])
+def test_cholesky_pivot_rounding(port, cg, n, seed):
+    """Inputs on which the reference build's pivot dot products round
+    differently from its other dot products (for double: no half vector)."""
+    a = spd_matrix(n, seed=seed)
+    f, info = gpu_potrf(a)
+    assert info == 0
+    assert sha(f) == str(cg[f"pivot_{n}_{seed}_sha"])
+    assert np.array_equal(f, port.potrf(a)[0])
+
+
+@pytest.mark.parametrize("dt,npdt", TYPES)
+def test_cholesky_sweep_bitwise(port, dt, npdt):
+    for n in range(1, 97, 5):
+        for seed in (300 + n, 90 + n):
+            a = spd_matrix(n, seed=seed, dtype=npdt)
+            assert np.array_equal(gpu_potrf(a)[0], port.potrf(a)[0]), (n, seed)
+
+
 def test_cholesky_lookahead_neutral(port, monkeypatch):
     """The look-ahead schedule (next block's kernels beside the trailing
     update) gives the same bits as the plain sequence, also when a late

@@ -74,6 +74,28 @@ def test_port_cholesky_not_positive_definite(port, cg, dt, npdt, fail_row):
     assert np.array_equal(m, f)
 
 
+PIVOT_CASES = ((10, 100), (12, 312), (21, 111), (45, 345), (70, 370), (95, 7095))
+
+
+def test_port_cholesky_pivot_rounding_golden(port, cg):
+    """Inputs on which the reference build's pivot dot products (its
+    dot(a_i, a_i, i) call site: for double, no half vector) round
+    differently from its other call sites."""
+    for n, seed in PIVOT_CASES:
+        f, info = port.potrf(spd_matrix(n, seed=seed))
+        assert info == 0 and sha(f) == str(cg[f"pivot_{n}_{seed}_sha"]), (n, seed)
+
+
+@pytest.mark.skipif(not os.path.exists(REF_LIB), reason="reference build not present")
+@pytest.mark.parametrize("dt", [np.float64, np.float32])
+def test_port_cholesky_sweep_equals_reference_build(port, dt):
+    ref = Oracle("reference")
+    for n in range(1, 97):
+        for seed in (300 + n, 90 + n):
+            a = spd_matrix(n, seed=seed, dtype=dt)
+            assert np.array_equal(port.potrf(a)[0], ref.potrf(a)[0]), (n, seed)
+
+
 @pytest.mark.skipif(not os.path.exists(REF_LIB), reason="reference build not present")
 @pytest.mark.parametrize("n", [4, 65, 129, 257])
 def test_port_cholesky_equals_reference_build(port, n):
@@ -88,3 +110,35 @@ def test_port_cholesky_equals_reference_build(port, n):
             mr, _, xr = ref.gesv(a, b, mode)
             assert np.array_equal(mp, mr) and np.array_equal(xp, xr)
             assert np.array_equal(port.gesv(mp, b, 4)[2], ref.gesv(mr, b, 4)[2])
+
+
+@pytest.mark.parametrize("dt,npdt", TYPES)
+def test_port_cholesky_determinant(port, cg, dt, npdt):
+    """determinant CHOLESKY modes: the product of the lower factor's diagonal
+    in index order (determinant.cpp cholesky_determinant, not squared)."""
+    for n in (1, 17, 65, 200):
+        a = spd_matrix(n, seed=7000 + n, dtype=npdt)
+        d, f, _ = port.det(a, mode=CHOLESKY_LINEAR_SOLVER)
+        assert sha(f) == str(cg[f"chol_{dt}_{n}_lower_sha"])
+        expect = f[0, 0]
+        for i in range(1, n):
+            expect = npdt(expect * f[i, i])
+        assert d == expect
+        d4, _, _ = port.det(f, mode=CHOLESKY_UPFRONT_LINEAR_SOLVER)
+        assert np.array_equal(np.array(d4), np.array(d))
+    bad = spd_matrix(100, seed=7170, dtype=npdt, fail_row=70)
+    assert port.det(bad, mode=CHOLESKY_LINEAR_SOLVER)[0] == 0
+
+
+@pytest.mark.skipif(not os.path.exists(REF_LIB), reason="reference build not present")
+def test_port_cholesky_determinant_equals_reference_build(port):
+    ref = Oracle("reference")
+    for npdt in (np.float64, np.float32):
+        for n in (3, 70, 129):
+            a = spd_matrix(n, seed=300 + n, dtype=npdt)
+            for mode in (CHOLESKY_LINEAR_SOLVER,):
+                dp, fp, _ = port.det(a, mode=mode)
+                dr, fr, _ = ref.det(a, mode=mode)
+                assert np.array_equal(np.array(dp), np.array(dr)) and np.array_equal(fp, fr)
+                assert np.array_equal(np.array(port.det(fp, mode=4)[0]), np.array(ref.det(fr, mode=4)[0]))
+

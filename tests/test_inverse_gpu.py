@@ -185,9 +185,10 @@ def test_invalid_arguments_raise():
     m = dev(np.eye(4))
     piv = torch.zeros(4, dtype=torch.int64, device="cuda")
     ws = api.workspace(la.inversion.workspace_size(4, la.LU_LINEAR_SOLVER))
-    for mode in (3, 4, 5, 0):  # Cholesky modes: not provided; others: invalid
+    for mode in (3, 4, 5, 0):  # inversion's Cholesky modes: not provided; others: invalid
         with pytest.raises(la.B200Error):
             la.inversion.apply(m, piv, 4, mode, ws, ws.numel())
+    for mode in (5, 0):
         with pytest.raises(la.B200Error):
             la.determinant.apply(m, piv, 4, mode, ws, ws.numel())
     lib = la._lib.load()
@@ -202,3 +203,31 @@ def test_invalid_arguments_raise():
         la.inversion.apply(m, piv, 4, la.LU_LINEAR_SOLVER, ws, 16)
     with pytest.raises(la.B200InvalidArgument):
         la.determinant.apply(m, None, 4, la.LU_UPFRONT_LINEAR_SOLVER, ws, ws.numel())
+
+
+@pytest.mark.parametrize("dt,npdt", TYPES)
+def test_determinant_cholesky_modes(port, dt, npdt):
+    """CHOLESKY: the lower factor's diagonal product in index order, bit for
+    bit (NATIVE's value, sqrt(det A)); CHOLESKY_UPFRONT on the given factor;
+    0 when the matrix is not positive definite."""
+    from linearalgebra_b200.workloads import spd_matrix
+    for n in (1, 17, 70, 130, 300):
+        a = spd_matrix(n, seed=300 + n, dtype=npdt)
+        m = dev(a)
+        nbytes = la.determinant.workspace_size(n, la.CHOLESKY_LINEAR_SOLVER, m.dtype)
+        ws = api.workspace(nbytes)
+        prod, sign, log_abs, singular = la.determinant.parts(m, None, n, la.CHOLESKY_LINEAR_SOLVER, ws, ws.numel())
+        d_ref, f_ref, _ = port.det(a, mode=3)
+        assert np.array_equal(np.array(prod, dtype=npdt), np.array(d_ref)) and sign == 1 and not singular
+        assert np.array_equal(m.cpu().numpy(), f_ref)
+        l64 = np.log(np.diag(f_ref).astype(np.float64))
+        assert abs(log_abs - 2 * l64.sum()) <= 1e-9 * max(1.0, abs(log_abs))
+        prod4, _, _, _ = la.determinant.parts(m, None, n, la.CHOLESKY_UPFRONT_LINEAR_SOLVER, ws, ws.numel())
+        assert np.array_equal(np.array(prod4, dtype=npdt), np.array(d_ref))
+        assert la.determinant.apply(dev(a), None, n, la.CHOLESKY_LINEAR_SOLVER, ws, ws.numel()) == \
+            pytest.approx(float(d_ref) ** 2, rel=1e-12)
+    bad = dev(spd_matrix(100, seed=5, dtype=npdt, fail_row=60))
+    ws = api.workspace(la.determinant.workspace_size(100, la.CHOLESKY_LINEAR_SOLVER, bad.dtype))
+    prod, _, _, singular = la.determinant.parts(bad, None, 100, la.CHOLESKY_LINEAR_SOLVER, ws, ws.numel())
+    assert prod == 0 and singular
+

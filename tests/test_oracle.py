@@ -213,7 +213,7 @@ def test_port_inverse_rejects_bad_mode(port):
     with pytest.raises(ValueError):
         port.getri(np.eye(3), mode=5)
     with pytest.raises(ValueError):
-        port.det(np.eye(3), mode=3)
+        port.det(np.eye(3), mode=5)
 
 
 @pytest.mark.skipif(not os.path.exists(REF_LIB), reason="reference build not present")
