@@ -15,8 +15,10 @@
  *    linear_solver are provided (factors bit-identical to NATIVE);
  *    cholesky_decomposition::apply synchronizes its stream and writes info
  *    to host memory before it returns (the host backends' contract), and
- *    returns false when the matrix is not positive definite; the Cholesky
- *    modes of inversion and determinant and apply_aad are not provided
+ *    returns false when the matrix is not positive definite; determinant's
+ *    Cholesky modes return det(A) = (prod l_ii)^2 (CUDA_BLAS's value; NATIVE
+ *    returns prod l_ii, which b200la_ddeterminant reports as `product`);
+ *    the Cholesky modes of inversion and apply_aad are not provided
  *    (std::invalid_argument);
  *  - inversion and determinant honour LU_UPFRONT (m and pivot are the
  *    caller's factors) and, in LU mode, accept a null pivot (CUDA_BLAS's
