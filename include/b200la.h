@@ -150,7 +150,8 @@ B200LA_API int    b200la_dgetrs(const double* lu, const int64_t* pivot, int64_t 
  * device memory (for example a host-language binding or a plugin host that is
  * handed only the matrix, pivot and right-hand-side pointers, or a service
  * that forbids allocation after start-up).  No counterpart in the reference.
- * Same arguments and semantics as b200la_dgesv minus the workspace: the
+ * Same arguments and semantics as b200la_dgesv minus the workspace (all four
+ * modes; pivot may be NULL in the Cholesky modes): the
  * scratch is one fixed 1 MiB device array inside this library, which every
  * GPU that loads the library holds until the process exits.  Limit: n <= 16384
  * (larger orders return B200LA_INVALID_ARGUMENT).  The first call on a device

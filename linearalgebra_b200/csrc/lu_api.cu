@@ -195,8 +195,9 @@ extern "C" B200LA_API int b200la_dgesv_noalloc(double* m, int64_t* pivot, int64_
         return set_error(B200LA_NOT_SUPPORTED, "dgesv_noalloc: needs %zu bytes of scratch, has %zu",
             need, kNoAllocScratchBytes);
     }
-    if (m == nullptr || x == nullptr || pivot == nullptr || n <= 0 ||
-        (mode != B200LA_LU_LINEAR_SOLVER && mode != B200LA_LU_UPFRONT_LINEAR_SOLVER))
+    const bool chol = mode == B200LA_CHOLESKY_LINEAR_SOLVER || mode == B200LA_CHOLESKY_UPFRONT_LINEAR_SOLVER;
+    if (m == nullptr || x == nullptr || (pivot == nullptr && !chol) || n <= 0 ||
+        (mode != B200LA_LU_LINEAR_SOLVER && mode != B200LA_LU_UPFRONT_LINEAR_SOLVER && !chol))
     {
         // argument errors are reported by the shared checks, before any
         // device work

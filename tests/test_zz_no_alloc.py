@@ -83,6 +83,30 @@ def test_no_alloc_singular_then_regular_and_upfront():
     np.testing.assert_allclose(x4, x3, rtol=0, atol=1e-12 * np.abs(x3).max())
 
 
+def test_no_alloc_cholesky_modes_twice(port):
+    """The Cholesky modes (no pivot array): same factor and solution as the
+    workspace entry point, on two calls in a row."""
+    from linearalgebra_b200.workloads import spd_matrix
+    lib = _lib.load()
+    for call, n in enumerate((300, 700)):
+        a = spd_matrix(n, seed=40 + n)
+        b = np.random.default_rng(n).standard_normal(n)
+        m1, _, x1 = _with_workspace(a, b, mode=3)
+        m, x = _dev(a), _dev(b)
+        _lib.check(lib.b200la_dgesv_noalloc(m.data_ptr(), None, n, x.data_ptr(), 3,
+                                            torch.cuda.current_stream().cuda_stream))
+        torch.cuda.synchronize()
+        m2, x2 = m.cpu().numpy(), x.cpu().numpy()
+        assert np.array_equal(m2, m1), f"call {call}: factors differ"
+        np.testing.assert_allclose(x2, x1, rtol=0, atol=1e-12 * np.abs(x1).max())
+        assert port.backward_error(a, x2, b) <= 10 * n * EPS64
+        x = _dev(b)
+        _lib.check(lib.b200la_dgesv_noalloc(m.data_ptr(), None, n, x.data_ptr(), 4,
+                                            torch.cuda.current_stream().cuda_stream))
+        torch.cuda.synchronize()
+        np.testing.assert_allclose(x.cpu().numpy(), x1, rtol=0, atol=1e-12 * np.abs(x1).max())
+
+
 def test_no_alloc_rejects_orders_beyond_its_scratch():
     lib = _lib.load()
     p = torch.empty(8, dtype=torch.float64, device="cuda").data_ptr()
