@@ -104,6 +104,19 @@ B200LA_API int b200la_sgetrf_async(float* m, int64_t n, int64_t* pivot, void* wo
  * returns B200LA_SUCCESS / B200LA_SINGULAR / B200LA_DEVICE_TIMEOUT. */
 B200LA_API int b200la_workspace_status(const void* workspace, int* info, void* stream);
 
+/* Failure-detection check of the bounded device-side waits.  No counterpart
+ * in the reference (its CPU path has no inter-thread waits; its numerical
+ * status is lu_decomposition_native.cpp:147-157,424-428).  Runs the forward
+ * triangular solve of b200la_dgesv's solve step on the factors `lu` (n x n,
+ * n >= 128) with its first 64-row block never claimed, so every other block
+ * waits, at most wait_ns (100 us .. 2 s), for a publication that never
+ * comes, records DEV_WAIT_TIMEOUT in the workspace's status block and
+ * returns.  x is left unchanged.  Synchronizes `stream`; returns
+ * B200LA_DEVICE_TIMEOUT when the waits ran out.  Workspace: the size
+ * b200la_dgesv_workspace_size(n, B200LA_LU_LINEAR_SOLVER) reports. */
+B200LA_API int b200la_test_wait_expiry(const double* lu, int64_t n, double* x, uint64_t wait_ns,
+    void* workspace, size_t workspace_bytes, void* stream);
+
 /* ---- cholesky_decomposition ------------------------------------------------
  * Replaces cholesky_decomposition<T, Backend>::apply / ::workspace_size
  * (include/matrix_operation/cholesky_decomposition.h; NATIVE
@@ -151,14 +164,21 @@ B200LA_API int    b200la_dgetrs(const double* lu, const int64_t* pivot, int64_t 
  * handed only the matrix, pivot and right-hand-side pointers, or a service
  * that forbids allocation after start-up).  No counterpart in the reference.
  * Same arguments and semantics as b200la_dgesv minus the workspace (all four
- * modes; pivot may be NULL in the Cholesky modes): the
- * scratch is one fixed 1 MiB device array inside this library, which every
- * GPU that loads the library holds until the process exits.  Limit: n <= 16384
- * (larger orders return B200LA_INVALID_ARGUMENT).  The first call on a device
- * looks up that array's device address (cudaGetSymbolAddress) with the device
- * current; make that first call before any stream capture.  Every call shares
- * the one array, so calls whose GPU work overlaps (other streams, other host
- * threads) race and must be serialized by the caller.  Allocates nothing. */
+ * modes; pivot may be NULL in the Cholesky modes): the scratch is one fixed
+ * 1 MiB device array inside this library, which every GPU that loads the
+ * library holds until the process exits.  Limit: n <= 16384 (larger orders
+ * return B200LA_INVALID_ARGUMENT).  It allocates no device memory; it does
+ * use other driver resources:
+ *   - the first call in a CUDA context looks up the array's device address
+ *     (cudaGetSymbolAddress, with the device current) and caches it under
+ *     that context's id;
+ *   - the first LU-mode call with n > 128 on a device creates the library's
+ *     process-wide side stream for the factorization's look-ahead;
+ *   - every LU-mode call with n > 128 creates and destroys two CUDA events.
+ * Make the first call on each device (with n > 128) before any stream
+ * capture.  Every call shares the one array, so calls whose GPU work overlaps
+ * (other streams, other host threads) race and must be serialized by the
+ * caller. */
 B200LA_API int b200la_dgesv_noalloc(double* m, int64_t* pivot, int64_t n, double* x, int mode,
     void* stream);
 

@@ -49,6 +49,7 @@ SIGNATURES: dict[str, tuple] = {
     "b200la_dgetrf_async": (_i32, [_p, _i64, _p, _p, _sz, _p]),
     "b200la_sgetrf_async": (_i32, [_p, _i64, _p, _p, _sz, _p]),
     "b200la_workspace_status": (_i32, [_p, _p, _p]),
+    "b200la_test_wait_expiry": (_i32, [_p, _i64, _p, ctypes.c_uint64, _p, _sz, _p]),
     "b200la_dgesv_workspace_size": (_sz, [_i64, _i32]),
     "b200la_sgesv_workspace_size": (_sz, [_i64, _i32]),
     "b200la_dgesv": (_i32, [_p, _p, _i64, _p, _i32, _p, _sz, _p]),

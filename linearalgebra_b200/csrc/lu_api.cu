@@ -49,6 +49,51 @@ B200LA_API int b200la_workspace_status(const void* ws, int* info, void* stream)
     return read_status(static_cast<const DeviceStatus*>(ws), info, as_stream(stream));
 }
 
+// Failure-detection check of the bounded device waits: the forward
+// triangular solve of b200la_dgesv's solve step with block 0 never claimed
+// (its ticket is started at 1), so every other block waits for a block that
+// nothing publishes until wait_ns runs out.  The factors are not read past
+// the first wait.  Returns what the workspace's status block reports
+// (B200LA_DEVICE_TIMEOUT when the waits ran out).
+B200LA_API int b200la_test_wait_expiry(const double* lu, int64_t n, double* x, uint64_t wait_ns, void* ws,
+    size_t bytes, void* stream)
+{
+    if (lu == nullptr || x == nullptr || n < 2 * kTvRows || n > INT_MAX)
+    {
+        return set_error(B200LA_INVALID_ARGUMENT, "test_wait_expiry: needs factors, x and n >= %d", 2 * kTvRows);
+    }
+    if (wait_ns < 100000ull || wait_ns > kWaitLimitNs)
+    {
+        return set_error(B200LA_INVALID_ARGUMENT, "test_wait_expiry: wait limit outside [100 us, 2 s]");
+    }
+    const size_t need = gesv_ws_size<double>(n, B200LA_LU_LINEAR_SOLVER);
+    if (ws == nullptr || bytes < need)
+    {
+        return set_error(B200LA_WORKSPACE_TOO_SMALL, "test_wait_expiry: workspace too small (%zu < %zu)", bytes,
+            need);
+    }
+    int st = prepare<double>();
+    if (st != B200LA_SUCCESS)
+    {
+        return st;
+    }
+    Arena             a(ws, bytes);
+    GetrfPlan<double> gp = plan_getrf<double>(a);
+    SolvePlan<double> sp = plan_solve<double>(a, n, 1);
+    cudaStream_t      s  = as_stream(stream);
+    k_status_init<<<1, 32, 0, s>>>(gp.st, gp.perm);
+    B200LA_LAUNCH_CHECK();
+    const int32_t withheld = 1;
+    B200LA_CUDA(cudaMemcpyAsync(sp.ticket, &withheld, sizeof(withheld), cudaMemcpyHostToDevice, s));
+    const int nb = (int)((n + kTvRows - 1) / kTvRows);
+    k_trsv_blocks<double, true><<<nb, kTvThreads, 0, s>>>(lu, n, x, (int)n, 0, nullptr, sp.xll, tv_next_epoch(),
+        sp.ticket, gp.st, wait_ns);
+    B200LA_LAUNCH_CHECK();
+    k_status_finish<<<1, 32, 0, s>>>(gp.st);
+    B200LA_LAUNCH_CHECK();
+    return read_status(gp.st, nullptr, s);
+}
+
 B200LA_API size_t b200la_dgesv_workspace_size(int64_t n, int mode) { return gesv_ws_size<double>(n, mode); }
 B200LA_API size_t b200la_sgesv_workspace_size(int64_t n, int mode) { return gesv_ws_size<float>(n, mode); }
 B200LA_API int b200la_dgesv(double* m, int64_t* pivot, int64_t n, double* x, int mode, void* ws,
@@ -147,12 +192,56 @@ namespace b200la
 {
 namespace
 {
-std::mutex g_noalloc_mutex;
-void*      g_noalloc_address[64] = {};
+// Driver entry points for identifying the current context (resolved through
+// the runtime, so the library does not link libcuda).
+using CtxGetCurrentFn = int (*)(void**);
+using CtxGetIdFn      = int (*)(void*, unsigned long long*);
 
-// Device address of g_noalloc_scratch on the current device.  The host-side
-// name of the array is only a stand-in, so the address is looked up once per
-// device (with that device current) and cached.
+struct NoAllocCache
+{
+    unsigned long long ctx_id;  // 0: free slot
+    void*              address;
+};
+
+std::mutex   g_noalloc_mutex;
+NoAllocCache g_noalloc_cache[64] = {};
+
+// Unique id of the current context (cuCtxGetId), 0 if it cannot be had.
+unsigned long long current_context_id()
+{
+    static CtxGetCurrentFn get_current = [] {
+        void*                           p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        return (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) == cudaSuccess &&
+                   q == cudaDriverEntryPointSuccess)
+                   ? reinterpret_cast<CtxGetCurrentFn>(p)
+                   : nullptr;
+    }();
+    static CtxGetIdFn get_id = [] {
+        void*                           p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        return (cudaGetDriverEntryPoint("cuCtxGetId", &p, cudaEnableDefault, &q) == cudaSuccess &&
+                   q == cudaDriverEntryPointSuccess)
+                   ? reinterpret_cast<CtxGetIdFn>(p)
+                   : nullptr;
+    }();
+    void*              ctx = nullptr;
+    unsigned long long id  = 0;
+    if (get_current == nullptr || get_id == nullptr || get_current(&ctx) != 0 || ctx == nullptr ||
+        get_id(ctx, &id) != 0)
+    {
+        return 0;
+    }
+    return id;
+}
+
+// Device address of g_noalloc_scratch in the current context.  The host-side
+// name of the array is only a stand-in, so the address is looked up with the
+// device current (cudaGetSymbolAddress) the first time a context calls, and
+// cached under that context's unique id: a context created later (after a
+// cudaDeviceReset, say, which unloads the module and may place the array
+// elsewhere) has a new id and gets its own lookup.  Without a context id
+// the address is looked up on every call.
 int noalloc_scratch(void** out)
 {
     int dev = 0;
@@ -162,17 +251,23 @@ int noalloc_scratch(void** out)
         return set_error(B200LA_NOT_SUPPORTED, "dgesv_noalloc: device index %d out of range", dev);
     }
     std::lock_guard<std::mutex> lock(g_noalloc_mutex);
-    if (g_noalloc_address[dev] == nullptr)
+    const unsigned long long    id = current_context_id();
+    if (id != 0 && g_noalloc_cache[dev].ctx_id == id)
     {
-        void*             p = nullptr;
-        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-        if (e != cudaSuccess)
-        {
-            return cuda_check(e, "cudaGetSymbolAddress(g_noalloc_scratch)");
-        }
-        g_noalloc_address[dev] = p;
+        *out = g_noalloc_cache[dev].address;
+        return B200LA_SUCCESS;
     }
-    *out = g_noalloc_address[dev];
+    void*             p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess)
+    {
+        return cuda_check(e, "cudaGetSymbolAddress(g_noalloc_scratch)");
+    }
+    // cudaGetSymbolAddress makes the primary context current if none was:
+    // key the entry on the context it answered for
+    const unsigned long long id_now = id != 0 ? id : current_context_id();
+    g_noalloc_cache[dev]            = NoAllocCache{id_now, p};
+    *out                            = p;
     return B200LA_SUCCESS;
 }
 }  // namespace

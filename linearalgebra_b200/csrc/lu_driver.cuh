@@ -648,7 +648,7 @@ int enqueue_getrs(const T* lu, const int64_t* pivot, int n, int nrhs, T* x, int6
                 const uint32_t epoch = tv_next_epoch();
                 prof_begin(KC_SOLVE, s);
                 k_trsv_blocks<double, true><<<nb, kTvThreads, 0, s>>>(lu, n, sp.y, n, pass, nullptr, sp.xll, epoch,
-                    sp.ticket, st);
+                    sp.ticket, st, kWaitLimitNs);
                 prof_end(KC_SOLVE, s);
                 B200LA_LAUNCH_CHECK();
             }
@@ -819,7 +819,7 @@ int enqueue_potrs(const T* l, int n, int nrhs, T* x, int64_t ldx, const SolvePla
                 const uint32_t epoch = tv_next_epoch();
                 prof_begin(KC_SOLVE, s);
                 k_trsv_blocks<double, true, true><<<nb, kTvThreads, 0, s>>>(l, n, sp.y, n, pass, nullptr, sp.xll,
-                    epoch, sp.ticket, st);
+                    epoch, sp.ticket, st, kWaitLimitNs);
                 prof_end(KC_SOLVE, s);
                 B200LA_LAUNCH_CHECK();
             }

@@ -1025,7 +1025,7 @@ int enqueue_lu_apply(const TA* lu, const int32_t* perm, int n, int nrhs, double*
             const uint32_t epoch = tv_next_epoch();
             prof_begin(KC_SOLVE, s);
             k_trsv_blocks<TA><<<nb, kTvThreads, 0, s>>>(lu, n, p.y, n, pass, p.dinv, p.xll, epoch,
-                reinterpret_cast<int32_t*>(p.tsync), st);
+                reinterpret_cast<int32_t*>(p.tsync), st, kWaitLimitNs);
             prof_end(KC_SOLVE, s);
             B200LA_LAUNCH_CHECK();
         }

@@ -144,11 +144,12 @@ __device__ __forceinline__ bool tv_read(const uint64_t* xll, int blk, int i, uin
 // its inverse from dinv (k_invert_diag_blocks; SUBST = false, the refinement
 // solves, whose rounding the refinement corrects) or solved by substitution
 // from the block's own triangle (SUBST = true, dinv unused: backward stable,
-// for the plain FP64 solve).
+// for the plain FP64 solve).  wait_ns bounds each wait for another block
+// (kWaitLimitNs in the library's own launches).
 template <typename TA, bool SUBST = false, bool CHOL = false>
 __global__ void __launch_bounds__(kTvThreads) k_trsv_blocks(const TA* __restrict__ a, int64_t lda,
     double* __restrict__ x, int n, int upper, const double* __restrict__ dinv, uint64_t* __restrict__ xll,
-    uint32_t epoch, int32_t* __restrict__ ticket, DeviceStatus* st)
+    uint32_t epoch, int32_t* __restrict__ ticket, DeviceStatus* st, uint64_t wait_ns)
 {
     constexpr int Q = kTvRows / (kTvThreads / kTvRows);  // columns per thread per tile (16)
     __shared__ double inv[kTvRows][kTvRows + 1];
@@ -235,7 +236,7 @@ __global__ void __launch_bounds__(kTvThreads) k_trsv_blocks(const TA* __restrict
                 uint32_t       polls = 0;
                 while (!tv_read(xll, jb, tid, epoch, xn))
                 {
-                    if ((++polls & 255u) == 0 && global_ns() - t0 > kWaitLimitNs)
+                    if ((++polls & 255u) == 0 && global_ns() - t0 > wait_ns)
                     {
                         raise_error(st, DEV_WAIT_TIMEOUT, 20);
                         s_abort = 1;

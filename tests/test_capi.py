@@ -85,5 +85,7 @@ def test_no_alloc_scratch_covers_its_largest_order():
     lib = _lib.load()
     # the allocation-free solve carves the same plan as b200la_dgesv from a
     # fixed 1 MiB device array, for orders up to 16384
-    assert lib.b200la_dgesv_workspace_size(16384, 1) <= 1 << 20
-    assert lib.b200la_dgesv_workspace_size(16384, 2) <= 1 << 20
+    for mode in (1, 2, 3, 4):
+        for n in (1, 129, 4096, 16384):
+            size = lib.b200la_dgesv_workspace_size(n, mode)
+            assert 0 < size <= 1 << 20, (mode, n, size)

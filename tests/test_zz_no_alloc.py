@@ -107,6 +107,31 @@ def test_no_alloc_cholesky_modes_twice(port):
         np.testing.assert_allclose(x.cpu().numpy(), x1, rtol=0, atol=1e-12 * np.abs(x1).max())
 
 
+def test_no_alloc_failed_cholesky_leaves_x_and_next_call_unaffected():
+    """A non-positive-definite matrix in mode 3 leaves x unchanged; the next
+    call, which finds the failed call's status and factor state in the
+    shared scratch, still matches b200la_dgesv."""
+    from linearalgebra_b200.workloads import spd_matrix
+    lib = _lib.load()
+    s = torch.cuda.current_stream().cuda_stream
+    n = 400
+    bad = spd_matrix(n, seed=77, fail_row=200)  # the pivot of row 200 is not positive
+    b = np.random.default_rng(3).standard_normal(n)
+    m, x = _dev(bad), _dev(b)
+    _lib.check(lib.b200la_dgesv_noalloc(m.data_ptr(), None, n, x.data_ptr(), 3, s))
+    torch.cuda.synchronize()
+    assert np.array_equal(x.cpu().numpy(), b), "x changed although the factorization failed"
+    for call, nn in enumerate((400, 650)):
+        a = spd_matrix(nn, seed=78 + call)
+        bb = np.random.default_rng(4 + call).standard_normal(nn)
+        m1, _, x1 = _with_workspace(a, bb, mode=3)
+        m2, x2 = _dev(a), _dev(bb)
+        _lib.check(lib.b200la_dgesv_noalloc(m2.data_ptr(), None, nn, x2.data_ptr(), 3, s))
+        torch.cuda.synchronize()
+        assert np.array_equal(m2.cpu().numpy(), m1), f"call {call}: factors differ"
+        np.testing.assert_allclose(x2.cpu().numpy(), x1, rtol=0, atol=1e-12 * np.abs(x1).max())
+
+
 def test_no_alloc_rejects_orders_beyond_its_scratch():
     lib = _lib.load()
     p = torch.empty(8, dtype=torch.float64, device="cuda").data_ptr()
