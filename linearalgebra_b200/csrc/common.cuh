@@ -81,6 +81,56 @@ __device__ __forceinline__ int32_t ld_volatile_i32(const int32_t* p)
 }
 
 // ---------------------------------------------------------------------------
+// Shared-memory mbarriers (TMA and distributed-shared-memory pushes complete
+// on them).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t smem_u32(const void* p)
+{
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+        "r"(bytes)
+        : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity)
+{
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// Bounded wait on an mbarrier phase; false when the 2 s limit ran out.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity)
+{
+    if (mbar_try_wait(bar, parity))
+    {
+        return true;
+    }
+    const uint64_t t0    = global_ns();
+    uint32_t       polls = 0;
+    while (!mbar_try_wait(bar, parity))
+    {
+        if ((++polls & 255u) == 0 && global_ns() - t0 > kWaitLimitNs)
+        {
+            return false;
+        }
+    }
+    return true;
+}
+
+// ---------------------------------------------------------------------------
 // Host-side workspace arena: the same carve order computes the size (base ==
 // nullptr) and the real pointers, so size queries and carving cannot drift
 // apart.  256-byte alignment for every carve (TMA and vector access safe).

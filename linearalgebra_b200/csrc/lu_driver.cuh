@@ -13,6 +13,7 @@
 #include "cholesky.cuh"
 #include "dmma.cuh"
 #include "lu_kernels.cuh"
+#include "panel_push.cuh"
 #include "solve_kernels.cuh"
 #include "trsv.cuh"
 
@@ -58,6 +59,39 @@ template <typename T> int probe_cluster_size()
     return 0;
 }
 
+// Cluster size usable by k_panel_push on each device (0: none).
+template <typename T> int& push_cluster_slot(int dev)
+{
+    static int sizes[64] = {};
+    return sizes[dev];
+}
+
+template <typename T> int probe_push_cluster_size()
+{
+    for (int cl : {16, 8})
+    {
+        cudaLaunchConfig_t  cfg = {};
+        cudaLaunchAttribute attr[1];
+        cfg.gridDim              = dim3(cl);
+        cfg.blockDim             = dim3(kPushThreads);
+        cfg.dynamicSmemBytes     = kPushSmemMax;
+        attr[0].id               = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = cl;
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        cfg.attrs                = attr;
+        cfg.numAttrs             = 1;
+        int clusters             = 0;
+        if (cudaOccupancyMaxActiveClusters(&clusters, (const void*)k_panel_push<T, 64>, &cfg) == cudaSuccess &&
+            clusters > 0)
+        {
+            return cl;
+        }
+        cudaGetLastError();
+    }
+    return 0;
+}
+
 // Raise the dynamic shared-memory limits once per device and type.
 template <typename T> int ensure_kernel_attributes()
 {
@@ -81,6 +115,16 @@ template <typename T> int ensure_kernel_attributes()
     if (dev >= 0 && dev < 64)
     {
         cluster_size_slot<T>(dev) = probe_cluster_size<T>();
+    }
+    B200LA_CUDA(cudaFuncSetAttribute(
+        k_panel_push<T, 64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPushSmemMax));
+    B200LA_CUDA(cudaFuncSetAttribute(k_panel_push<T, 64>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+    B200LA_CUDA(cudaFuncSetAttribute(
+        k_panel_push<T, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPushSmemMax));
+    B200LA_CUDA(cudaFuncSetAttribute(k_panel_push<T, 32>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+    if (dev >= 0 && dev < 64)
+    {
+        push_cluster_slot<T>(dev) = probe_push_cluster_size<T>();
     }
     B200LA_CUDA(cudaFuncSetAttribute(
         k_laswp_trsm<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)laswp_smem_bytes<T>()));
@@ -194,6 +238,60 @@ inline int grid_1d(int64_t total, int threads)
 // ---------------------------------------------------------------------------
 // Factor panel [k, k+w) of rows [k, n): inside one thread-block cluster when
 // its rows fit there (cl > 0), else with the grid-wide kernel.
+// B200LA_PANEL_EXCHANGE=barrier selects the cluster-barrier panel kernel
+// instead of the push-exchange one (both give the same bits; the tests
+// compare them).
+inline bool panel_push_enabled()
+{
+    const char* e = getenv("B200LA_PANEL_EXCHANGE");
+    return !(e != nullptr && e[0] == 'b');
+}
+
+// Cluster size of the push-exchange panel on the current device (0: none).
+template <typename T> int push_cluster_size()
+{
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64)
+    {
+        return 0;
+    }
+    return push_cluster_slot<T>(dev);
+}
+
+template <typename T, int W>
+int launch_panel_push(T* m, int n, int k, int w, int rpc, int cl, int64_t* pivot, const GetrfPlan<T>& p,
+    cudaStream_t s)
+{
+    cudaLaunchConfig_t  cfg = {};
+    cudaLaunchAttribute attr[1];
+    cfg.gridDim              = dim3(cl);
+    cfg.blockDim             = dim3(kPushThreads);
+    cfg.dynamicSmemBytes     = push_smem_bytes<T, W>(rpc);
+    cfg.stream               = s;
+    attr[0].id               = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = cl;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs                = attr;
+    cfg.numAttrs             = 1;
+    prof_begin(KC_PANEL, s);
+    B200LA_CUDA(cudaLaunchKernelEx(&cfg, k_panel_push<T, W>, m, n, k, w, rpc, pivot, p.perm, p.st));
+    prof_end(KC_PANEL, s);
+    return B200LA_SUCCESS;
+}
+
+// Whether a panel of `rows` rows and width w fits the push-exchange kernel
+// of a cluster of `cl` CTAs.
+template <typename T> bool push_panel_fits(int rows, int w, int cl)
+{
+    if (cl <= 0)
+    {
+        return false;
+    }
+    const int rpc = (rows + cl - 1) / cl;
+    return w <= 32 ? push_smem_bytes<T, 32>(rpc) <= kPushSmemMax : push_smem_bytes<T, 64>(rpc) <= kPushSmemMax;
+}
+
 template <typename T>
 int launch_panel(T* m, int n, int k, int w, int64_t* pivot, const GetrfPlan<T>& p, int cl, int gmax,
     cudaStream_t s, bool lean = false)
@@ -201,6 +299,16 @@ int launch_panel(T* m, int n, int k, int w, int64_t* pivot, const GetrfPlan<T>& 
     const int R = n - k;
     PanelWs<T> ws{p.hdr, p.payload, p.diag, p.perm};
     DeviceStatus* st = p.st;
+    if (cl > 0 && panel_push_enabled())
+    {
+        const int pcl = push_cluster_size<T>();
+        if (push_panel_fits<T>(R, w, pcl))
+        {
+            const int rpc = (R + pcl - 1) / pcl;
+            return w <= 32 ? launch_panel_push<T, 32>(m, n, k, w, rpc, pcl, pivot, p, s)
+                           : launch_panel_push<T, 64>(m, n, k, w, rpc, pcl, pivot, p, s);
+        }
+    }
         // the panel inside one thread-block cluster when its rows fit there
         if (cl > 0)
         {

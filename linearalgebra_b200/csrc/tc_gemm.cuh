@@ -88,52 +88,6 @@ template <bool SPLIT3> constexpr size_t tc_smem_bytes()
     return (size_t)tc_stages<SPLIT3>() * tc_stage_bytes<SPLIT3>() + 1024 + 256;
 }
 
-__device__ __forceinline__ uint32_t smem_u32(const void* p)
-{
-    return (uint32_t)__cvta_generic_to_shared(p);
-}
-
-__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count)
-{
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
-}
-__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes)
-{
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
-        "r"(bytes)
-        : "memory");
-}
-__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity)
-{
-    uint32_t ok;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}\n"
-        : "=r"(ok)
-        : "r"(smem_u32(bar)), "r"(parity)
-        : "memory");
-    return ok != 0;
-}
-// Bounded wait on an mbarrier phase; false when the 2 s limit ran out.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity)
-{
-    if (mbar_try_wait(bar, parity))
-    {
-        return true;
-    }
-    const uint64_t t0    = global_ns();
-    uint32_t       polls = 0;
-    while (!mbar_try_wait(bar, parity))
-    {
-        if ((++polls & 255u) == 0 && global_ns() - t0 > kWaitLimitNs)
-        {
-            return false;
-        }
-    }
-    return true;
-}
-
 __device__ __forceinline__ void tma_load_2d(void* smem, const CUtensorMap* map, int x, int y, uint64_t* bar)
 {
     asm volatile(
