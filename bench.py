@@ -63,6 +63,9 @@ def parse():
     p.add_argument("--no-cholesky", action="store_true")
     p.add_argument("--no-transpose", action="store_true")
     p.add_argument("--tp-n", type=int, default=16384, help="order of the square transpose measurement")
+    p.add_argument("--no-configs", action="store_true",
+                   help="skip config 1 (n=512), the rest of config 2 (BF16/FP16, nrhs=64) and config 3 (sweep)")
+    p.add_argument("--selector-systems", type=int, default=5000, help="held-out systems of config 5 (0: skip)")
     return p.parse_args()
 
 
@@ -855,6 +858,263 @@ def run_batched(args, world, rank, local):
     return out
 
 
+# ---------------------------------------------------------------------------
+# config 1: plain FP64 LU + solve at n = 512 (latency-bound), beside the
+# mixed solve and the reference's NATIVE CPU solve of the same system
+# ---------------------------------------------------------------------------
+def run_config1(args, local, fp64_peak):
+    import numpy as np
+    import torch
+
+    import linearalgebra_b200 as la
+    from linearalgebra_b200 import _lib
+    from linearalgebra_b200.workloads import system
+    from oracle import Oracle
+
+    lib = _lib.load()
+    n = 512
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.current_stream(dev)
+    sp = stream.cuda_stream
+    a, x_true, b = system(n, seed=512)
+    A = torch.from_numpy(a).to(dev)
+    B = torch.from_numpy(b).to(dev)
+    m, x = torch.empty_like(A), torch.empty_like(B)
+    piv = torch.empty(n, dtype=torch.int64, device=dev)
+    nbytes = lib.b200la_dgesv_workspace_size(n, la.LU_LINEAR_SOLVER)
+    ws = torch.empty(nbytes, dtype=torch.uint8, device=dev)
+
+    def step():
+        m.copy_(A)
+        x.copy_(B)
+        _lib.check(lib.b200la_dgesv(m.data_ptr(), piv.data_ptr(), n, x.data_ptr(), la.LU_LINEAR_SOLVER,
+                                    ws.data_ptr(), nbytes, sp))
+
+    def timed(fn, reps=50):
+        for _ in range(5):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps / 1e3
+
+    t64 = timed(step)
+    port = Oracle("port")
+    eta64 = port.backward_error(a, x.cpu().numpy(), b)
+    flops = 2 * n ** 3 / 3 + 2 * n * n
+    solver = la.MixedSolver(n, 1, dev, precision="fp32", tolerance=1e-14)
+    xm = torch.empty_like(B)
+    res = {}
+
+    def mstep():
+        _, r, _ = solver(A, B, xm, stream)
+        res.update(r)
+
+    tm = timed(mstep, reps=20)
+    etam = port.backward_error(a, xm.cpu().numpy(), b)
+    kind, tcpu, etacpu = cpu_reference_solve_seconds(n, repeats=5)
+    return {"n": n, "workload": "A iid N(0,1), x_true iid U[-1,1], b = A x_true (numpy seed 512), nrhs=1",
+            "fp64_lu_solve_s": t64, "fp64_backward_error": eta64,
+            "fp64_tflops": flops / t64 / 1e12, "fp64_frac_of_measured_dgemm": flops / t64 / 1e12 / fp64_peak,
+            "mixed_fp32_ir_s": tm, "mixed_backward_error": etam, "mixed_iterations": res.get("iterations"),
+            "reference_native_cpu_s": tcpu, "reference_native_backward_error": etacpu,
+            "reference_kind": kind, "bound_10_n_eps": 10 * n * EPS64,
+            "note": "device time per solve incl. the 2 MiB device copies restoring A and b; latency-bound "
+                    "(the FP64 fraction is of measured cuBLAS DGEMM 8192^3)"}
+
+
+# ---------------------------------------------------------------------------
+# config 2, the rest: BF16 and FP16 factorizations and nrhs = 64 at n = 16384
+# ---------------------------------------------------------------------------
+def run_config2_more(args, A, b, stream, local):
+    import torch
+
+    import linearalgebra_b200 as la
+    from linearalgebra_b200 import _lib
+
+    lib = _lib.load()
+    n = A.shape[0]
+    dev = A.device
+    sp = stream.cuda_stream
+    anorm = A.abs().sum(1).max()
+
+    def eta_of(xx, bb):
+        r = bb - A @ xx
+        if r.dim() == 1:
+            return (r.abs().max() / (anorm * xx.abs().max() + bb.abs().max())).item()
+        return ((r.abs().amax(0)) / (anorm * xx.abs().amax(0) + bb.abs().amax(0))).max().item()
+
+    def timed(fn, reps=2):
+        fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps / 1e3
+
+    out = {}
+    x = torch.empty_like(b)
+    for prec in ("bf16", "fp16"):
+        solver = la.MixedSolver(n, 1, dev, precision=prec, tolerance=1e-14)
+        res = {}
+
+        def st(solver=solver, res=res):
+            _, r, _ = solver(A, b, x, stream)
+            res.update(r)
+
+        t = timed(st)
+        out[prec] = {"s": t, "backward_error": eta_of(x, b),
+                     **{k: res[k] for k in ("precision_used", "iterations", "gmres_iterations", "escalations",
+                                            "converged", "factor_ms", "refine_ms")}}
+        del solver
+        torch.cuda.empty_cache()
+    # nrhs = 64: mixed FP32 LU-IR and the plain FP64 LU + multi-RHS solve
+    nrhs = 64
+    g = torch.Generator(device=dev)
+    g.manual_seed(SEED + 64)
+    xt = torch.rand(n, nrhs, dtype=torch.float64, device=dev, generator=g) * 2 - 1
+    B = A @ xt
+    X = torch.empty_like(B)
+    solver = la.MixedSolver(n, nrhs, dev, precision="fp32", tolerance=1e-14)
+    res = {}
+
+    def st64():
+        _, r, _ = solver(A, B, X, stream)
+        res.update(r)
+
+    t = timed(st64)
+    out["nrhs64_mixed_fp32"] = {"s": t, "backward_error_max_over_columns": eta_of(X, B),
+                                "forward_error": ((X - xt).abs().max() / xt.abs().max()).item(),
+                                **{k: res[k] for k in ("precision_used", "iterations", "gmres_iterations",
+                                                       "escalations", "converged", "factor_ms", "refine_ms")}}
+    del solver
+    torch.cuda.empty_cache()
+    m = torch.empty_like(A)
+    piv = torch.empty(n, dtype=torch.int64, device=dev)
+    fb = lib.b200la_dgetrf_workspace_size(n)
+    sb = lib.b200la_dgetrs_workspace_size(n, nrhs)
+    ws = torch.empty(max(fb, sb), dtype=torch.uint8, device=dev)
+
+    def st_fp64():
+        m.copy_(A)
+        X.copy_(B)
+        _lib.check(lib.b200la_dgetrf_async(m.data_ptr(), n, piv.data_ptr(), ws.data_ptr(), fb, sp))
+        _lib.check(lib.b200la_dgetrs(m.data_ptr(), piv.data_ptr(), n, nrhs, X.data_ptr(), nrhs, ws.data_ptr(),
+                                     sb, sp))
+
+    t64 = timed(st_fp64)
+    out["nrhs64_fp64"] = {"s": t64, "backward_error_max_over_columns": eta_of(X, B),
+                          "what": "plain FP64 LU (bit-identical factors) + 64-column triangular solves"}
+    out["nrhs64_speedup_mixed_vs_fp64"] = t64 / out["nrhs64_mixed_fp32"]["s"]
+    del m, ws, B, X, xt
+    torch.cuda.empty_cache()
+    return out
+
+
+# ---------------------------------------------------------------------------
+# config 3: conditioning sweep, n in {4096, 8192}, kappa 1e2 .. 1e10,
+# FP8-E4M3 / BF16 / FP32 factorizations against the FP64 oracle solution
+# ---------------------------------------------------------------------------
+KAPPAS = (1e2, 1e4, 1e6, 1e8, 1e10)
+SWEEP_PRECISIONS = ("fp8", "bf16", "fp32")
+
+
+def run_config3(args, local):
+    import torch
+
+    import linearalgebra_b200 as la
+    from linearalgebra_b200 import _lib
+    from linearalgebra_b200.selector import conditioned_device
+
+    lib = _lib.load()
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.current_stream(dev)
+    sp = stream.cuda_stream
+    rows = []
+    for n in (4096, 8192):
+        solvers = {p: la.MixedSolver(n, 1, dev, precision=p, tolerance=1e-14) for p in SWEEP_PRECISIONS}
+        m = torch.empty(n, n, dtype=torch.float64, device=dev)
+        piv = torch.empty(n, dtype=torch.int64, device=dev)
+        nbytes = lib.b200la_dgesv_workspace_size(n, la.LU_LINEAR_SOLVER)
+        ws = torch.empty(nbytes, dtype=torch.uint8, device=dev)
+        for ki, kappa in enumerate(KAPPAS):
+            seed = 3000 + 10 * ki + n
+            A = conditioned_device(n, kappa, seed, device=dev)
+            g = torch.Generator(device=dev)
+            g.manual_seed(seed)
+            xt = torch.rand(n, dtype=torch.float64, device=dev, generator=g) * 2 - 1
+            b = A @ xt
+            anorm = A.abs().sum(1).max()
+            # the FP64 oracle solution: plain FP64 LU, factors bit-identical to the reference's
+            m.copy_(A)
+            x64 = b.clone()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            _lib.check(lib.b200la_dgesv(m.data_ptr(), piv.data_ptr(), n, x64.data_ptr(), la.LU_LINEAR_SOLVER,
+                                        ws.data_ptr(), nbytes, sp))
+            e1.record(stream)
+            torch.cuda.synchronize()
+
+            def errs(xx):
+                r = b - A @ xx
+                return ((r.abs().max() / (anorm * xx.abs().max() + b.abs().max())).item(),
+                        ((xx - xt).abs().max() / xt.abs().max()).item(),
+                        ((xx - x64).abs().max() / x64.abs().max()).item())
+
+            eta64, fwd64, _ = errs(x64)
+            row = {"n": n, "kappa": kappa, "seed": seed,
+                   "fp64_oracle": {"ms": e0.elapsed_time(e1), "backward_error": eta64, "forward_error": fwd64}}
+            for prec in SWEEP_PRECISIONS:
+                x = torch.empty_like(b)
+                if ki == 0:
+                    solvers[prec](A, b, x, stream)  # warm-up of this order and precision
+                torch.cuda.synchronize()
+                s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                s0.record(stream)
+                _, r, status = solvers[prec](A, b, x, stream)
+                s1.record(stream)
+                torch.cuda.synchronize()
+                eta, fwd, fwd_o = errs(x)
+                row[prec] = {"ms": s0.elapsed_time(s1), "status": int(status),
+                             "precision_used": _lib.PREC_NAMES.get(r["precision_used"], r["precision_used"]),
+                             "iterations": r["iterations"], "gmres_iterations": r["gmres_iterations"],
+                             "escalations": r["escalations"], "converged": r["converged"],
+                             "backward_error": eta, "forward_error": fwd, "forward_error_vs_fp64_oracle": fwd_o}
+            rows.append(row)
+            del A, b, xt, x64
+        del solvers, m, ws
+        torch.cuda.empty_cache()
+    return {"construction": "A = U diag(sigma) V^T, U and V products of 8 seeded Householder reflectors, sigma "
+                            "geometric from 1 to 1/kappa; x_true iid U[-1,1]; tolerance eta <= 1e-14; "
+                            "escalation on (FP8 -> BF16 -> FP32 -> FP64)",
+            "fp8_scaling": "power-of-two scale per row of L21 and per column of U12 (finer than per 128x128 block)",
+            "rows": rows}
+
+
+# ---------------------------------------------------------------------------
+# config 5: the learned precision selector on the held-out stream
+# ---------------------------------------------------------------------------
+def run_selector(args):
+    from linearalgebra_b200 import selector
+
+    net = selector.Network.load()
+    summary, recs = selector.evaluate(net, args.selector_systems, seed=2)
+    best_fixed = max(("fixed_fp32", "fp64"), key=lambda k: summary[k]["solves_per_s"])
+    return {"systems": args.selector_systems, "stream_seed": 2,
+            "stream": "n log-uniform in [64, 4096], kappa log-uniform in [1e1, 1e12] (Householder construction)",
+            "summary": summary, "best_fixed_policy": best_fixed,
+            "selected_vs_best_fixed": summary["selected"]["solves_per_s"] / summary[best_fixed]["solves_per_s"],
+            "timing": "host wall clock per solve, synchronized, matrices built on the device beforehand",
+            "weights_meta": net.meta}
+
+
 def run_b200(args, world, rank, local):
     import numpy as np
     import torch
@@ -967,6 +1227,33 @@ def run_b200(args, world, rank, local):
         "tensor_tflops": (w["flops"] * args.steps / secs / 1e12) if (secs and w["bound"] == "hbm") else None,
     }
 
+    # ---- the panel chain's latency roofline: per-column time of the panel
+    # kernels in this step against the measured floor of their per-column
+    # exchange (cluster barrier, keys and pivot row through distributed
+    # shared memory, two block barriers), 64- and 32-column forms
+    panel_roofline = None
+    if "panel" in breakdown:
+        fws = torch.empty(256, dtype=torch.uint8, device=dev)
+        floors = {}
+        for width in (64, 32):
+            v = ctypes.c_double(0)
+            elem = 8 if args.method == "fp64" else 4
+            if lib.b200la_panel_exchange_floor(elem, width, 2048, ctypes.addressof(v), fws.data_ptr(), 256,
+                                               sp) == 0:
+                floors[width] = v.value / 1e3
+        us_col = breakdown["panel"]["ms"] * 1e3 / n
+        floor = min(floors.values()) if floors else None
+        panel_roofline = {
+            "kernel": "k_panel_cluster (per-column pivot exchange inside one 16-CTA cluster) and k_panel (grid)",
+            "bound": "latency", "unit": "us per column",
+            "achieved": us_col, "floor": floor, "floors_by_width": floors,
+            "frac": floor / us_col if floor else None,
+            "launches": breakdown["panel"]["launches"],
+            "note": "achieved = the step's panel-class time (CUDA events around each panel launch, so it includes "
+                    "waiting for SMs held by the concurrent trailing update) / n columns; floor = "
+                    "b200la_panel_exchange_floor, device-timed, exchange only"}
+        del fws
+
     # ---- the other arm, timed the same way (fewer steps)
     other = {}
     if not args.no_compare:
@@ -1049,6 +1336,15 @@ def run_b200(args, world, rank, local):
     if not args.no_transpose:
         transpose = run_transpose(args, world, rank, local)
 
+    configs = {}
+    if rank == 0 and world == 1 and not args.no_configs:
+        fp64_peak = measured_fp64_peak_tflops()
+        configs["config1_n512"] = run_config1(args, local, fp64_peak)
+        configs["config2_more"] = run_config2_more(args, A, b, stream, local)
+        configs["config3_sweep"] = run_config3(args, local)
+    if rank == 0 and world == 1 and args.selector_systems > 0:
+        configs["config5_selector"] = run_selector(args)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         kind, t, ceta = cpu_reference_solve_seconds(CPU_SAMPLE_N)
@@ -1060,9 +1356,6 @@ def run_b200(args, world, rank, local):
                          "has no threading"}
 
     if rank == 0:
-        method_desc = (f"mixed-precision LU-IR ({args.precision} factorization on tcgen05, FP64 "
-                       "refinement to backward error <= 1e-14)" if args.method == "mixed"
-                       else "plain FP64 blocked LU + solve")
         line = {
             "metric": METRIC,
             "value": ms_per_step / 1e3,
@@ -1076,13 +1369,7 @@ def run_b200(args, world, rank, local):
             "vs_baseline": None,
             "dtype": "f64" if args.method == "fp64" else f"{args.precision}+f64",
             "data": f"synthetic: A iid N(0,1) (torch generator seed {SEED}+rank), x_true iid U[-1,1], b = A x_true",
-            "config": {"workload": f"dense LU solve n={n} nrhs=1, {method_desc}",
-                       "n": n, "nrhs": 1, "method": args.method,
-                       "precision": args.precision if args.method == "mixed" else "fp64",
-                       "step": ("solve from A, b resident in HBM (A left unchanged)" if args.method == "mixed"
-                                else "restore A and b (device copies, 2 GiB), factor, solve"),
-                       "l2": "inputs (2 GiB) larger than L2; no flush",
-                       "parallelism": "replicas" if world > 1 else "single GPU"},
+            "config": arm_config(n, args.method, args.precision, world),
             "accuracy": {"backward_error": eta, "forward_error": fwd, "target": 1e-14,
                          "refinement": {k: last[k] for k in ("precision_used", "iterations", "gmres_iterations",
                                                              "escalations", "converged", "factor_ms", "refine_ms")}
@@ -1090,6 +1377,7 @@ def run_b200(args, world, rank, local):
             "compare": other,
             "speedup_vs_fp64_lu": (other["s"] / (ms_per_step / 1e3)) if other and args.method == "mixed" else None,
             "roofline": roofline,
+            "panel_roofline": panel_roofline,
             "cpu_baseline": cpu,
             "cusolver_baseline": cusolver,
             "e2e": e2e,
@@ -1100,6 +1388,7 @@ def run_b200(args, world, rank, local):
             "multiplication": multiplication,
             "cholesky": cholesky,
             "transpose": transpose,
+            **configs,
             "clocks": clk,
             "peaks": peaks,
         }
@@ -1109,36 +1398,105 @@ def run_b200(args, world, rank, local):
 # ---------------------------------------------------------------------------
 # reference arm: the reference's NATIVE CPU LU solve (oracle/_ref)
 # ---------------------------------------------------------------------------
+def arm_config(n: int, method: str, precision: str, world: int) -> dict:
+    """The `config` of the JSON line, shared by both arms."""
+    method_desc = (f"mixed-precision LU-IR ({precision} factorization on tcgen05, FP64 "
+                   "refinement to backward error <= 1e-14)" if method == "mixed"
+                   else "plain FP64 blocked LU + solve")
+    return {"workload": f"dense LU solve n={n} nrhs=1, {method_desc}",
+            "n": n, "nrhs": 1, "method": method,
+            "precision": precision if method == "mixed" else "fp64",
+            "step": ("solve from A, b resident in HBM (A left unchanged)" if method == "mixed"
+                     else "restore A and b (device copies, 2 GiB), factor, solve"),
+            "l2": "inputs (2 GiB) larger than L2; no flush",
+            "parallelism": "replicas" if world > 1 else "single GPU"}
+
+
 def run_reference(args, world, rank):
+    """Every timed step is one full linear_solver<double, NATIVE> LU solve of
+    order n (A iid N(0,1), x_true iid U[-1,1], b = A x_true) by the
+    reference's own build (oracle/_ref).  The reference is single-threaded,
+    so it uses the host's threads the only way it can: the K steps run as K
+    independent solves in concurrent threads (each on its own copy of A and
+    b, made before the clock starts; at most as many at once as host memory
+    holds).  value = wall time of all K solves / K: seconds of host time per
+    n=16384 solve with every host thread busy."""
     if rank != 0:
         return
-    from oracle import available
+    import numpy as np
+    from concurrent.futures import ThreadPoolExecutor
+
+    from linearalgebra_b200.workloads import system
+    from oracle import Oracle, available
 
     if not (available("reference") or available("port")):
         print(json.dumps({"impl": "reference", "unavailable": "CPU reference build missing"}))
         return
+    kind = "reference" if available("reference") else "port"
+    orc = Oracle(kind)
+    fn = getattr(orc.lib, f"{orc._pre}dgesv")
     n = args.n
     for _ in range(args.warmup):
         cpu_reference_solve_seconds(1024)
-    times = []
-    kind = "reference"
-    eta = None
-    for _ in range(args.steps):
-        kind, t, eta = cpu_reference_solve_seconds(CPU_SAMPLE_N)
-        times.append(t)
-    scale = (n / CPU_SAMPLE_N) ** 3
-    value = statistics.median(times) * scale
+    a, x_true, b = system(n, seed=SEED)
+    try:
+        avail = os.sysconf("SC_PAGE_SIZE") * os.sysconf("SC_AVPHYS_PAGES")
+    except (ValueError, OSError):
+        avail = 64 << 30
+    ws_fn = getattr(orc.lib, "ref_dgetrf_workspace_size", None)
+    if ws_fn is not None:
+        ws_fn.restype = ctypes.c_size_t
+        ws_fn.argtypes = [ctypes.c_int64]
+        ws_bytes = int(ws_fn(n))
+    else:
+        ws_bytes = 8 * n * n + (64 << 20)
+    per_solve = 8 * n * n + ws_bytes + 16 * n  # the copy of A, the reference's workspace, x and pivots
+    threads = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
+    concurrent = max(1, min(args.steps, int(0.8 * avail // per_solve)))
+    ms = [np.empty_like(a) for _ in range(concurrent)]
+    xs = [np.empty_like(b) for _ in range(concurrent)]
+    pivs = [np.empty(n, dtype=np.int64) for _ in range(concurrent)]
+    times = [0.0] * args.steps
+    etas = [None] * args.steps
+
+    def one(i):
+        slot = i % concurrent
+        m, x, piv = ms[slot], xs[slot], pivs[slot]
+        np.copyto(m, a)
+        np.copyto(x, b)
+        t0 = time.perf_counter()
+        st = fn(m.ctypes.data, piv.ctypes.data, n, x.ctypes.data, 1)
+        times[i] = time.perf_counter() - t0
+        if st < 0:
+            raise RuntimeError(f"reference gesv failed ({st})")
+        if i < concurrent:
+            etas[i] = float(np.abs(b - a @ x).max() / (np.abs(a).sum(1).max() * np.abs(x).max() + np.abs(b).max()))
+
+    t0 = time.perf_counter()
+    with ThreadPoolExecutor(max_workers=concurrent) as ex:
+        list(ex.map(one, range(args.steps)))
+    wall = time.perf_counter() - t0
+    value = wall / args.steps
+    eta = max(e for e in etas if e is not None)
+    sample = (f"{args.steps} full linear_solver<double,NATIVE> LU solves at n={n} (A iid N(0,1), numpy seed {SEED}), "
+              f"{concurrent} at a time in threads on {threads} host threads ({cpu_model()}); "
+              f"value = wall {wall:.1f} s / {args.steps}; each solve alone-in-thread took "
+              f"{min(times):.1f}..{max(times):.1f} s (median {statistics.median(times):.1f} s, "
+              f"input copies excluded); max eta {eta:.2e}; warm-up: {args.warmup} solves at n=1024")
     line = {
         "metric": METRIC, "impl": "reference", "value": value, "unit": "s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": value * 1e3, "higher_is_better": False, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic: A iid N(0,1), x_true iid U[-1,1]",
-        "config": {"workload": f"dense LU solve n={n} nrhs=1 (plain FP64 blocked LU + solve)",
-                   "n": n, "nrhs": 1, "method": "reference NATIVE linear_solver LU mode"},
-        "cpu_baseline": {"value": value, "unit": "s", "cores": 1, "kind": kind,
-                         "sample": f"each step one n={CPU_SAMPLE_N} solve, median scaled by "
-                                   f"(n/{CPU_SAMPLE_N})^3={scale:.0f}; warm-up steps at n=1024; "
-                                   f"1 thread (the reference has no threading); eta={eta}"},
+        "vs_baseline": None, "dtype": "f64",
+        "data": f"synthetic: A iid N(0,1), x_true iid U[-1,1], b = A x_true (numpy seed {SEED})",
+        "config": arm_config(n, args.method, args.precision, world),
+        "reference_solve": {"what": "linear_solver<double,NATIVE> LU mode, the reference's own sources "
+                                    "(oracle/_ref, LINALG_HAS_LU_PIVOTING=1)",
+                            "per_solve_s": times, "median_per_solve_s": statistics.median(times),
+                            "concurrent_solves": concurrent, "host_threads": threads, "wall_s": wall,
+                            "backward_error": eta},
+        "cpu_baseline": {"value": value, "unit": "s", "cores": min(concurrent, threads), "kind": kind,
+                         "sample": sample},
         "e2e": {"value": value, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)

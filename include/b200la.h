@@ -114,6 +114,18 @@ B200LA_API int b200la_workspace_status(const void* workspace, int* info, void* s
  * returns.  x is left unchanged.  Synchronizes `stream`; returns
  * B200LA_DEVICE_TIMEOUT when the waits ran out.  Workspace: the size
  * b200la_dgesv_workspace_size(n, B200LA_LU_LINEAR_SOLVER) reports. */
+/* Latency floor of the cluster panel's per-column pivot exchange, for the
+ * panel's latency roofline.  No counterpart in the reference (its panel,
+ * lu_decomposition_native.cpp:158-232, is sequential).  Runs only the
+ * exchange of the cluster panel kernel (a key posted by every CTA, cluster
+ * barrier, the keys and one pivot row read through distributed shared
+ * memory by one warp, two block barriers) for `columns` columns of FP64
+ * (elem_bytes 8) or FP32 (4) rows of a width-32 or -64 panel, and writes the
+ * device-timed nanoseconds per column.  Synchronizes `stream`.
+ * Workspace: 256 bytes. */
+B200LA_API int b200la_panel_exchange_floor(int elem_bytes, int width, int columns, double* ns_per_column,
+    void* workspace, size_t workspace_bytes, void* stream);
+
 B200LA_API int b200la_test_wait_expiry(const double* lu, int64_t n, double* x, uint64_t wait_ns,
     void* workspace, size_t workspace_bytes, void* stream);
 
@@ -422,10 +434,16 @@ B200LA_API int b200la_dsolve_selected(const double* a, int64_t n, const double* 
  * U; -1000000 if not converged), backward_error[count].  total_a / total_v: element sizes of a and b.  precision
  * B200LA_PREC_FP32 (FP32 factors, FP64 refinement to `tolerance`; systems
  * whose refinement stalls are refactored in FP64 by a second persistent
- * launch that skips all others) or B200LA_PREC_FP64 (FP64 LU + refinement).  nb_table[8]: panel width per order
- * bucket of 64 (the autotuner's choice; 16 or 32 for FP32, 16 for FP64).
+ * launch that skips all others) or B200LA_PREC_FP64 (FP64 LU + refinement).
+ * nb_table[8]: per order bucket of 64 (the autotuner's choice), bits 0-7 the
+ * panel width (1..32 for FP32 factors, 1..16 for FP64) and bits 8-15 the
+ * threads that solve one system / 32 (2 or 4; 0 = a whole CTA of 256): a CTA
+ * solves 256 / that many systems at once.  b200la_batched_table_valid says
+ * whether every bucket's largest order fits its group's shared memory.
  * Asynchronous.  Extension: the reference has no batched solver. */
 B200LA_API size_t b200la_dgesv_batched_workspace_size(int64_t total_a, int64_t total_v, int precision);
+/* 1 if the host array table[8] is a valid nb_table for `precision`, else 0. */
+B200LA_API int    b200la_batched_table_valid(int precision, const int32_t* table);
 B200LA_API int    b200la_dgesv_batched(int64_t count, const int32_t* sizes, const int64_t* offsets_a,
        const int64_t* offsets_v, const int32_t* order, const double* a, const double* b, double* x,
        int64_t total_a, int64_t total_v, int precision, const int32_t* nb_table, int max_iterations,

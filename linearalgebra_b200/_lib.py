@@ -50,6 +50,7 @@ SIGNATURES: dict[str, tuple] = {
     "b200la_sgetrf_async": (_i32, [_p, _i64, _p, _p, _sz, _p]),
     "b200la_workspace_status": (_i32, [_p, _p, _p]),
     "b200la_test_wait_expiry": (_i32, [_p, _i64, _p, ctypes.c_uint64, _p, _sz, _p]),
+    "b200la_panel_exchange_floor": (_i32, [_i32, _i32, _i32, _p, _p, _sz, _p]),
     "b200la_dgesv_workspace_size": (_sz, [_i64, _i32]),
     "b200la_sgesv_workspace_size": (_sz, [_i64, _i32]),
     "b200la_dgesv": (_i32, [_p, _p, _i64, _p, _i32, _p, _sz, _p]),
@@ -87,6 +88,7 @@ SIGNATURES: dict[str, tuple] = {
     "b200la_dsolve_mixed_workspace_size": (_sz, [_i64, _i64, _p]),
     "b200la_dsolve_mixed": (_i32, [_p, _i64, _i64, _p, _i64, _p, _i64, _p, _p, _p, _sz, _p]),
     "b200la_dgesv_batched_workspace_size": (_sz, [_i64, _i64, _i32]),
+    "b200la_batched_table_valid": (_i32, [_i32, _p]),
     "b200la_dgesv_batched": (_i32, [_i64, _p, _p, _p, _p, _p, _p, _p, _i64, _i64, _i32, _p, _i32, _d, _p, _p,
                                     _p, _sz, _p]),
     "b200la_tc_update_workspace_size": (_sz, []),

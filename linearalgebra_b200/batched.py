@@ -5,9 +5,11 @@ optionally replayed as a CUDA graph.
 * ``BatchedSolver(sizes)`` packs the batch layout (row-major matrices back to
   back, offsets per system), orders the systems largest first so the last
   CTAs get the smallest work, and owns the workspace.
-* ``autotune(...)`` picks the panel width per order bucket of 64 by timing the
-  candidates on a sample of the batch's own systems, and caches the choice on
-  disk per device (``B200LA_TUNE_CACHE`` or ~/.cache/b200la/batched_tune.json).
+* ``autotune(...)`` picks the panel width and the threads per system (a CTA
+  of 256 threads solves 1, 2 or 4 systems at once) per order bucket of 64 by
+  timing the candidates on a sample of the batch's own systems, and caches
+  the choice on disk per device (``B200LA_TUNE_CACHE`` or
+  ~/.cache/b200la/batched_tune.json).
 * ``shard(sizes, world, rank)`` splits a batch across ranks with balanced
   sum(n^3) (greedy, largest first); ranks share nothing in the data path.
 """
@@ -24,12 +26,47 @@ from . import _lib
 from .api import _ptr, _stream, workspace
 
 NB_BUCKETS = 8
-NB_CHOICES = {_lib.PREC_FP32: (16, 32), _lib.PREC_FP64: (16,)}
-DEFAULT_NB = {_lib.PREC_FP32: 32, _lib.PREC_FP64: 16}
+NB_CHOICES = {_lib.PREC_FP32: (16, 32), _lib.PREC_FP64: (8, 16)}
+GROUP_CHOICES = (64, 128, 256)  # threads that solve one system
 
 
 def bucket_of(n: int) -> int:
     return min((int(n) - 1) // 64, NB_BUCKETS - 1)
+
+
+def entry(nb: int, threads: int) -> int:
+    """A bucket's table entry: panel width in bits 0-7, threads per system / 32
+    in bits 8-15 (0 for a whole CTA of 256)."""
+    return int(nb) | ((0 if threads >= 256 else threads // 32) << 8)
+
+
+def entry_parts(e: int) -> tuple[int, int]:
+    g = ((int(e) >> 8) & 0xFF) * 32
+    return int(e) & 0xFF, (g if g in (64, 128) else 256)
+
+
+def table_valid(prec: int, table) -> bool:
+    arr = (ctypes.c_int32 * NB_BUCKETS)(*[int(v) for v in table])
+    return bool(_lib.load().b200la_batched_table_valid(prec, arr))
+
+
+def default_table(prec: int) -> list[int]:
+    """Per bucket: the widest panel and the fewest threads per system whose
+    shared-memory slice holds the bucket's largest order."""
+    out = []
+    for bk in range(NB_BUCKETS):
+        chosen = None
+        for g in GROUP_CHOICES:
+            for nb in sorted(NB_CHOICES[prec], reverse=True):
+                trial = [entry(NB_CHOICES[prec][-1], 256)] * NB_BUCKETS
+                trial[bk] = entry(nb, g)
+                if table_valid(prec, trial):
+                    chosen = entry(nb, g)
+                    break
+            if chosen is not None:
+                break
+        out.append(chosen if chosen is not None else entry(NB_CHOICES[prec][0], 256))
+    return out
 
 
 def shard(sizes, world: int, rank: int) -> np.ndarray:
@@ -76,7 +113,7 @@ class BatchedSolver:
         self.tolerance = tolerance
         self.max_iterations = max_iterations
         if nb_table is None:
-            nb_table = [DEFAULT_NB[self.prec]] * NB_BUCKETS
+            nb_table = default_table(self.prec)
         self.set_nb_table(nb_table)
         lib = _lib.load()
         self.ws_bytes = int(lib.b200la_dgesv_batched_workspace_size(self.total_a, self.total_v, self.prec))
@@ -119,9 +156,12 @@ class BatchedSolver:
     def replay(self):
         self.graph.replay()
 
-    # --- autotuning of the panel width per order bucket -------------------
+    # --- autotuning of the panel width and threads per system, per bucket --
     def autotune(self, a, b, x, sample_per_bucket: int = 48, use_cache: bool = True):
-        key = f"{torch.cuda.get_device_name(self.device)}|prec{self.prec}"
+        """Per order bucket, time every valid (panel width, threads per
+        system) pair on up to `sample_per_bucket` of the batch's own systems
+        of that bucket and keep the fastest; cached per device and precision."""
+        key = f"{torch.cuda.get_device_name(self.device)}|prec{self.prec}|v2"
         path = _cache_path()
         cache = {}
         if use_cache and os.path.exists(path):
@@ -132,13 +172,12 @@ class BatchedSolver:
         if use_cache and key in cache:
             self.set_nb_table(cache[key]["nb_table"])
             return cache[key]
-        choices = NB_CHOICES[self.prec]
-        table = [DEFAULT_NB[self.prec]] * NB_BUCKETS
+        table = default_table(self.prec)
         timings = {}
         buckets = np.array([bucket_of(n) for n in self.sizes_h])
         for bk in range(NB_BUCKETS):
             idx = np.nonzero(buckets == bk)[0][:sample_per_bucket]
-            if len(idx) == 0 or len(choices) == 1:
+            if len(idx) == 0:
                 continue
             sub = BatchedSolver(self.sizes_h[idx], "fp32" if self.prec == _lib.PREC_FP32 else "fp64",
                                 self.device, self.tolerance, self.max_iterations)
@@ -146,31 +185,39 @@ class BatchedSolver:
             sb = torch.cat([self.views(b, int(i), False) for i in idx])
             sx = torch.empty_like(sb)
             best = None
-            for nb in choices:
-                sub.set_nb_table([nb] * NB_BUCKETS)
-                sub.launch(sa, sb, sx)
-                torch.cuda.synchronize(self.device)
-                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-                e0.record()
-                for _ in range(3):
+            for g in GROUP_CHOICES:
+                for nb in NB_CHOICES[self.prec]:
+                    trial = list(table)
+                    trial[bk] = entry(nb, g)
+                    if not table_valid(self.prec, trial):
+                        continue
+                    sub.set_nb_table(trial)
                     sub.launch(sa, sb, sx)
-                e1.record()
-                torch.cuda.synchronize(self.device)
-                t = e0.elapsed_time(e1) / 3
-                timings[f"{bk}:{nb}"] = t
-                if best is None or t < best[0]:
-                    best = (t, nb)
-            table[bk] = best[1]
+                    torch.cuda.synchronize(self.device)
+                    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                    e0.record()
+                    for _ in range(3):
+                        sub.launch(sa, sb, sx)
+                    e1.record()
+                    torch.cuda.synchronize(self.device)
+                    t = e0.elapsed_time(e1) / 3
+                    timings[f"{bk}:nb{nb}:t{g}"] = t
+                    if best is None or t < best[0]:
+                        best = (t, entry(nb, g))
+            if best is not None:
+                table[bk] = best[1]
         self.set_nb_table(table)
-        entry = {"nb_table": table, "timings_ms": timings}
+        out = {"nb_table": table, "timings_ms": timings,
+               "per_bucket": [{"panel_width": entry_parts(e)[0], "threads_per_system": entry_parts(e)[1]}
+                              for e in table]}
         if use_cache:
             try:
                 os.makedirs(os.path.dirname(path), exist_ok=True)
-                cache[key] = entry
+                cache[key] = out
                 json.dump(cache, open(path, "w"), indent=1)
             except OSError:
                 pass
-        return entry
+        return out
 
 
 def make_batch(count: int, seed: int, device="cuda", lo: int = 16, hi: int = 512):

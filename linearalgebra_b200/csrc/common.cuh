@@ -81,8 +81,8 @@ __device__ __forceinline__ int32_t ld_volatile_i32(const int32_t* p)
 }
 
 // ---------------------------------------------------------------------------
-// Shared-memory mbarriers (TMA and distributed-shared-memory pushes complete
-// on them).
+// Shared-memory mbarriers (TMA copies and tensor-core commits complete on
+// them).
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ uint32_t smem_u32(const void* p)
 {

@@ -94,6 +94,70 @@ B200LA_API int b200la_test_wait_expiry(const double* lu, int64_t n, double* x, u
     return read_status(gp.st, nullptr, s);
 }
 
+// Latency floor of the cluster panel's per-column exchange (measurement
+// hook): k_panel_exchange_floor for `columns` columns, FP64 (elem_bytes 8)
+// or FP32 (4) records of a 64- or 32-column panel, in the cluster size the
+// panel kernel uses.  Synchronizes `stream`; *ns_per_column receives the
+// device-timed nanoseconds per column.  Workspace: 256 bytes.
+B200LA_API int b200la_panel_exchange_floor(int elem_bytes, int width, int columns, double* ns_per_column, void* ws,
+    size_t bytes, void* stream)
+{
+    if (ns_per_column == nullptr || ws == nullptr || bytes < 256 || columns < 1 || columns > 1 << 20 ||
+        (elem_bytes != 4 && elem_bytes != 8) || (width != 32 && width != 64))
+    {
+        return set_error(B200LA_INVALID_ARGUMENT, "panel_exchange_floor: bad arguments");
+    }
+    int st = elem_bytes == 8 ? prepare<double>() : prepare<float>();
+    if (st != B200LA_SUCCESS)
+    {
+        return st;
+    }
+    int cl = 0, gmax = 0;
+    st = elem_bytes == 8 ? panel_config<double>(cl, gmax) : panel_config<float>(cl, gmax);
+    if (st != B200LA_SUCCESS)
+    {
+        return st;
+    }
+    if (cl <= 0)
+    {
+        return set_error(B200LA_NOT_SUPPORTED, "panel_exchange_floor: no usable cluster size");
+    }
+    cudaStream_t        s  = as_stream(stream);
+    unsigned long long* ns = static_cast<unsigned long long*>(ws);
+    cudaLaunchConfig_t  cfg = {};
+    cudaLaunchAttribute attr[1];
+    cfg.gridDim              = dim3(cl);
+    cfg.blockDim             = dim3(kPanelThreads);
+    cfg.stream               = s;
+    attr[0].id               = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = cl;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs                = attr;
+    cfg.numAttrs             = 1;
+    if (elem_bytes == 8 && width == 64)
+    {
+        B200LA_CUDA(cudaLaunchKernelEx(&cfg, k_panel_exchange_floor<double, 64>, columns, ns));
+    }
+    else if (elem_bytes == 8)
+    {
+        B200LA_CUDA(cudaLaunchKernelEx(&cfg, k_panel_exchange_floor<double, 32>, columns, ns));
+    }
+    else if (width == 64)
+    {
+        B200LA_CUDA(cudaLaunchKernelEx(&cfg, k_panel_exchange_floor<float, 64>, columns, ns));
+    }
+    else
+    {
+        B200LA_CUDA(cudaLaunchKernelEx(&cfg, k_panel_exchange_floor<float, 32>, columns, ns));
+    }
+    unsigned long long h = 0;
+    B200LA_CUDA(cudaMemcpyAsync(&h, ns, sizeof(h), cudaMemcpyDeviceToHost, s));
+    B200LA_CUDA(cudaStreamSynchronize(s));
+    *ns_per_column = (double)h / columns;
+    return B200LA_SUCCESS;
+}
+
 B200LA_API size_t b200la_dgesv_workspace_size(int64_t n, int mode) { return gesv_ws_size<double>(n, mode); }
 B200LA_API size_t b200la_sgesv_workspace_size(int64_t n, int mode) { return gesv_ws_size<float>(n, mode); }
 B200LA_API int b200la_dgesv(double* m, int64_t* pivot, int64_t n, double* x, int mode, void* ws,

@@ -13,7 +13,6 @@
 #include "cholesky.cuh"
 #include "dmma.cuh"
 #include "lu_kernels.cuh"
-#include "panel_push.cuh"
 #include "solve_kernels.cuh"
 #include "trsv.cuh"
 
@@ -22,6 +21,9 @@ namespace b200la
 int require_sm100();
 
 constexpr size_t kPanelSmemMax = 200 * 1024;
+// dynamic shared memory of the cluster panel: sm_100's 227 KB per CTA less
+// 6 KB for its static arrays
+constexpr size_t kClusterSmemMax = 227 * 1024 - 6 * 1024;
 constexpr int    kLeanPanelCtas = 48;  // grid panel CTAs beside a concurrent trailing update
 
 
@@ -40,7 +42,7 @@ template <typename T> int probe_cluster_size()
         cudaLaunchAttribute attr[1];
         cfg.gridDim                    = dim3(cl);
         cfg.blockDim                   = dim3(kPanelThreads);
-        cfg.dynamicSmemBytes           = kPanelSmemMax;
+        cfg.dynamicSmemBytes           = kClusterSmemMax;
         attr[0].id                     = cudaLaunchAttributeClusterDimension;
         attr[0].val.clusterDim.x       = cl;
         attr[0].val.clusterDim.y       = 1;
@@ -48,41 +50,8 @@ template <typename T> int probe_cluster_size()
         cfg.attrs                      = attr;
         cfg.numAttrs                   = 1;
         int clusters                   = 0;
-        if (cudaOccupancyMaxActiveClusters(&clusters, (const void*)k_panel_cluster<T>, &cfg) ==
+        if (cudaOccupancyMaxActiveClusters(&clusters, (const void*)k_panel_cluster<T, 64>, &cfg) ==
                 cudaSuccess &&
-            clusters > 0)
-        {
-            return cl;
-        }
-        cudaGetLastError();
-    }
-    return 0;
-}
-
-// Cluster size usable by k_panel_push on each device (0: none).
-template <typename T> int& push_cluster_slot(int dev)
-{
-    static int sizes[64] = {};
-    return sizes[dev];
-}
-
-template <typename T> int probe_push_cluster_size()
-{
-    for (int cl : {16, 8})
-    {
-        cudaLaunchConfig_t  cfg = {};
-        cudaLaunchAttribute attr[1];
-        cfg.gridDim              = dim3(cl);
-        cfg.blockDim             = dim3(kPushThreads);
-        cfg.dynamicSmemBytes     = kPushSmemMax;
-        attr[0].id               = cudaLaunchAttributeClusterDimension;
-        attr[0].val.clusterDim.x = cl;
-        attr[0].val.clusterDim.y = 1;
-        attr[0].val.clusterDim.z = 1;
-        cfg.attrs                = attr;
-        cfg.numAttrs             = 1;
-        int clusters             = 0;
-        if (cudaOccupancyMaxActiveClusters(&clusters, (const void*)k_panel_push<T, 64>, &cfg) == cudaSuccess &&
             clusters > 0)
         {
             return cl;
@@ -109,22 +78,18 @@ template <typename T> int ensure_kernel_attributes()
     B200LA_CUDA(cudaFuncSetAttribute(
         k_perm_from_pivots<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
     B200LA_CUDA(cudaFuncSetAttribute(
-        k_panel_cluster<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPanelSmemMax));
+        k_panel_cluster<T, 64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kClusterSmemMax));
+    B200LA_CUDA(cudaFuncSetAttribute(k_panel_cluster<T, 64>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
     B200LA_CUDA(cudaFuncSetAttribute(
-        k_panel_cluster<T>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+        k_panel_cluster<T, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kClusterSmemMax));
+    B200LA_CUDA(cudaFuncSetAttribute(k_panel_cluster<T, 32>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+    B200LA_CUDA(cudaFuncSetAttribute(
+        k_panel_exchange_floor<T, 64>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+    B200LA_CUDA(cudaFuncSetAttribute(
+        k_panel_exchange_floor<T, 32>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
     if (dev >= 0 && dev < 64)
     {
         cluster_size_slot<T>(dev) = probe_cluster_size<T>();
-    }
-    B200LA_CUDA(cudaFuncSetAttribute(
-        k_panel_push<T, 64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPushSmemMax));
-    B200LA_CUDA(cudaFuncSetAttribute(k_panel_push<T, 64>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
-    B200LA_CUDA(cudaFuncSetAttribute(
-        k_panel_push<T, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPushSmemMax));
-    B200LA_CUDA(cudaFuncSetAttribute(k_panel_push<T, 32>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
-    if (dev >= 0 && dev < 64)
-    {
-        push_cluster_slot<T>(dev) = probe_push_cluster_size<T>();
     }
     B200LA_CUDA(cudaFuncSetAttribute(
         k_laswp_trsm<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)laswp_smem_bytes<T>()));
@@ -238,58 +203,16 @@ inline int grid_1d(int64_t total, int threads)
 // ---------------------------------------------------------------------------
 // Factor panel [k, k+w) of rows [k, n): inside one thread-block cluster when
 // its rows fit there (cl > 0), else with the grid-wide kernel.
-// B200LA_PANEL_EXCHANGE=barrier selects the cluster-barrier panel kernel
-// instead of the push-exchange one (both give the same bits; the tests
-// compare them).
-inline bool panel_push_enabled()
-{
-    const char* e = getenv("B200LA_PANEL_EXCHANGE");
-    return !(e != nullptr && e[0] == 'b');
-}
-
-// Cluster size of the push-exchange panel on the current device (0: none).
-template <typename T> int push_cluster_size()
-{
-    int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64)
-    {
-        return 0;
-    }
-    return push_cluster_slot<T>(dev);
-}
-
-template <typename T, int W>
-int launch_panel_push(T* m, int n, int k, int w, int rpc, int cl, int64_t* pivot, const GetrfPlan<T>& p,
-    cudaStream_t s)
-{
-    cudaLaunchConfig_t  cfg = {};
-    cudaLaunchAttribute attr[1];
-    cfg.gridDim              = dim3(cl);
-    cfg.blockDim             = dim3(kPushThreads);
-    cfg.dynamicSmemBytes     = push_smem_bytes<T, W>(rpc);
-    cfg.stream               = s;
-    attr[0].id               = cudaLaunchAttributeClusterDimension;
-    attr[0].val.clusterDim.x = cl;
-    attr[0].val.clusterDim.y = 1;
-    attr[0].val.clusterDim.z = 1;
-    cfg.attrs                = attr;
-    cfg.numAttrs             = 1;
-    prof_begin(KC_PANEL, s);
-    B200LA_CUDA(cudaLaunchKernelEx(&cfg, k_panel_push<T, W>, m, n, k, w, rpc, pivot, p.perm, p.st));
-    prof_end(KC_PANEL, s);
-    return B200LA_SUCCESS;
-}
-
-// Whether a panel of `rows` rows and width w fits the push-exchange kernel
-// of a cluster of `cl` CTAs.
-template <typename T> bool push_panel_fits(int rows, int w, int cl)
+// Whether a panel of `rows` rows and width w fits the cluster panel kernel
+// on a cluster of `cl` CTAs.
+template <typename T> bool cluster_panel_fits(int rows, int w, int cl)
 {
     if (cl <= 0)
     {
         return false;
     }
-    const int rpc = (rows + cl - 1) / cl;
-    return w <= 32 ? push_smem_bytes<T, 32>(rpc) <= kPushSmemMax : push_smem_bytes<T, 64>(rpc) <= kPushSmemMax;
+    const size_t rpc = (size_t)((rows + cl - 1) / cl);
+    return rpc * (w <= 32 ? cluster_row_bytes<T, 32>() : cluster_row_bytes<T, 64>()) <= kClusterSmemMax;
 }
 
 template <typename T>
@@ -299,43 +222,35 @@ int launch_panel(T* m, int n, int k, int w, int64_t* pivot, const GetrfPlan<T>& 
     const int R = n - k;
     PanelWs<T> ws{p.hdr, p.payload, p.diag, p.perm};
     DeviceStatus* st = p.st;
-    if (cl > 0 && panel_push_enabled())
+    // the panel inside one thread-block cluster when its rows fit there
+    if (cluster_panel_fits<T>(R, w, cl))
     {
-        const int pcl = push_cluster_size<T>();
-        if (push_panel_fits<T>(R, w, pcl))
+        const int           rpc = (R + cl - 1) / cl;
+        cudaLaunchConfig_t  cfg = {};
+        cudaLaunchAttribute attr[1];
+        cfg.gridDim              = dim3(cl);
+        cfg.blockDim             = dim3(kPanelThreads);
+        cfg.dynamicSmemBytes     = (size_t)rpc * (w <= 32 ? cluster_row_bytes<T, 32>() : cluster_row_bytes<T, 64>());
+        cfg.stream               = s;
+        attr[0].id               = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = cl;
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        cfg.attrs                = attr;
+        cfg.numAttrs             = 1;
+        prof_begin(KC_PANEL, s);
+        if (w <= 32)
         {
-            const int rpc = (R + pcl - 1) / pcl;
-            return w <= 32 ? launch_panel_push<T, 32>(m, n, k, w, rpc, pcl, pivot, p, s)
-                           : launch_panel_push<T, 64>(m, n, k, w, rpc, pcl, pivot, p, s);
+            B200LA_CUDA(cudaLaunchKernelEx(&cfg, k_panel_cluster<T, 32>, m, n, k, w, rpc, pivot, p.perm, p.st));
         }
+        else
+        {
+            B200LA_CUDA(cudaLaunchKernelEx(&cfg, k_panel_cluster<T, 64>, m, n, k, w, rpc, pivot, p.perm, p.st));
+        }
+        prof_end(KC_PANEL, s);
+        return B200LA_SUCCESS;
     }
-        // the panel inside one thread-block cluster when its rows fit there
-        if (cl > 0)
-        {
-            const int    cl_use = cl;  // the widest cluster: the most update bandwidth per column
-            const int    rpc_c  = (R + cl_use - 1) / cl_use;
-            const size_t smem_c = (size_t)rpc_c * panel_ldl<T>() * sizeof(T);
-            if (smem_c <= kPanelSmemMax)
-            {
-                cudaLaunchConfig_t  cfg = {};
-                cudaLaunchAttribute attr[1];
-                cfg.gridDim              = dim3(cl_use);
-                cfg.blockDim             = dim3(kPanelThreads);
-                cfg.dynamicSmemBytes     = smem_c;
-                cfg.stream               = s;
-                attr[0].id               = cudaLaunchAttributeClusterDimension;
-                attr[0].val.clusterDim.x = cl_use;
-                attr[0].val.clusterDim.y = 1;
-                attr[0].val.clusterDim.z = 1;
-                cfg.attrs                = attr;
-                cfg.numAttrs             = 1;
-                prof_begin(KC_PANEL, s);
-                B200LA_CUDA(cudaLaunchKernelEx(&cfg, k_panel_cluster<T>, m, n, k, w, rpc_c, pivot, p.perm, p.st));
-                prof_end(KC_PANEL, s);
-                return B200LA_SUCCESS;
-            }
-        }
-        {
+    {
         int       G   = (R + 15) / 16;
         if (lean)
         {

@@ -396,13 +396,13 @@ __device__ __forceinline__ void panel_slice_copy(T* loc, int ldl, T* A, int n, i
     using VT         = typename Vec16<T>::type;
     constexpr int V  = 16 / (int)sizeof(T);
     constexpr int B  = 8;
-    const bool    vec = w == kNB && (n % V) == 0 && (k % V) == 0 &&
+    const bool    vec = (w % V) == 0 && (n % V) == 0 && (k % V) == 0 &&
                      (reinterpret_cast<uintptr_t>(A) & 15) == 0 && ((ldl * sizeof(T)) % 16) == 0 &&
                      (reinterpret_cast<uintptr_t>(loc) & 15) == 0;
     if (vec)
     {
-        constexpr int CPR   = kNB / V;  // chunks per row
-        const int     total = nloc * CPR;
+        const int CPR   = w / V;  // chunks per row
+        const int total = nloc * CPR;
         for (int e0 = threadIdx.x; e0 < total; e0 += kPanelThreads * B)
         {
             VT v[B];
@@ -747,174 +747,398 @@ __global__ void __launch_bounds__(kPanelThreads) k_panel(T* __restrict__ A, int 
 // ---------------------------------------------------------------------------
 // Panel factorization inside one thread-block cluster.
 //
-// Used when the panel's rows fit in the shared memory of one cluster of `CL`
-// CTAs (16 where the device allows that cluster size, else 8).  Same
-// arithmetic as k_panel.  Per column, one cluster barrier:
-//   * before it, every CTA posts in its own shared memory (double-buffered
-//     by column parity) its candidate's key, row index and the candidate
-//     row's w values, and the owner of the diagonal row c posts row c;
-//   * after it, warp 0 reads the CL keys and picks the pivot, then the pivot
-//     row is read from its owner's posted copy (and, by the owner of row p,
-//     row c from its posted copy) through distributed shared memory.
-// A slot of parity q is rewritten two columns later, after the next barrier,
-// which no CTA passes before every CTA has finished reading it, so no second
-// barrier is needed.  Cluster barriers are hardware barriers over
-// co-scheduled CTAs: there is no spin-wait in this kernel.
+// Used when the panel's rows fit in the shared memory of one cluster of CL
+// CTAs (16 where the device allows that cluster size, else 8); W is the
+// panel width the slice is laid out for (64, or 32 for the mixed-precision
+// factorization's tallest panels, whose 64-column slices would not fit).
+// Same arithmetic as k_panel.  Per column, one cluster barrier and two
+// block barriers:
+//   * warp 0 posts this CTA's candidate (the warps' best, reduced with
+//     redux.sync over integer keys that order like the reference's
+//     comparisons) with the candidate row's values, and warp 1 of the CTA
+//     that holds the diagonal row c posts row c, in shared memory
+//     double-buffered by column parity;
+//   * after the cluster barrier, warp 0 reads the CL posted keys through
+//     distributed shared memory, reduces them, reads the pivot row (and, in
+//     the CTA that holds row p, row c) and hands them over through shared
+//     memory; block barrier;
+//   * row c takes the pivot row, every row below is updated (the thread of
+//     row p takes row c's values as it updates it) and the warps reduce
+//     their next-column candidates; block barrier.
+// A post of parity q is rewritten two columns later, after the next cluster
+// barrier, which no CTA passes before every CTA has finished reading it.
+// Cluster and block barriers are hardware barriers over co-scheduled CTAs:
+// there is no spin-wait in this kernel.
 // ---------------------------------------------------------------------------
 
-template <typename T>
-__global__ void __launch_bounds__(kPanelThreads, 1) k_panel_cluster(T* __restrict__ A, int n, int k,
-    int w, int rows_per_cta, int64_t* __restrict__ pivot, PermList* __restrict__ perm,
-    DeviceStatus* __restrict__ st)
+template <typename T> struct PivKey;
+template <> struct PivKey<float>
 {
-    namespace cg = cooperative_groups;
-    cg::cluster_group cluster = cg::this_cluster();
+    using type = uint32_t;
+};
+template <> struct PivKey<double>
+{
+    using type = unsigned long long;
+};
+
+// Integer pivot-search key of value v (larger wins, ties go to the lower
+// row): |v|'s bits + 2, 1 for a NaN below the diagonal (never wins over a
+// number), the maximum for a NaN on the diagonal (never displaced), and 0
+// for "no candidate".  Orders exactly like pivot_key.
+template <typename T> __device__ __forceinline__ typename PivKey<T>::type piv_key_bits(T v, bool diag)
+{
+    using K = typename PivKey<T>::type;
+    if (v != v)
+    {
+        return diag ? ~K(0) : K(1);
+    }
+    if constexpr (sizeof(T) == 4)
+    {
+        return (K)__float_as_uint(fabsf(v)) + K(2);
+    }
+    else
+    {
+        return (K)__double_as_longlong(fabs(v)) + K(2);
+    }
+}
+
+// Warp-wide best (key, row) with redux.sync: largest key, then lowest row.
+template <typename K> __device__ __forceinline__ void warp_best_bits(K& key, int& row)
+{
+    if constexpr (sizeof(K) == 4)
+    {
+        const uint32_t m = __reduce_max_sync(0xffffffffu, key);
+        row              = __reduce_min_sync(0xffffffffu, key == m ? row : INT_MAX);
+        key              = m;
+    }
+    else
+    {
+        const uint32_t hi = __reduce_max_sync(0xffffffffu, (uint32_t)(key >> 32));
+        const uint32_t lo = __reduce_max_sync(0xffffffffu, (uint32_t)(key >> 32) == hi ? (uint32_t)key : 0u);
+        const K        m  = ((K)hi << 32) | lo;
+        row               = __reduce_min_sync(0xffffffffu, key == m ? row : INT_MAX);
+        key               = m;
+    }
+}
+
+__device__ __forceinline__ uint32_t cluster_rank()
+{
+    uint32_t r;
+    asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+    return r;
+}
+__device__ __forceinline__ uint32_t cluster_size()
+{
+    uint32_t r;
+    asm volatile("mov.u32 %0, %%cluster_nctarank;" : "=r"(r));
+    return r;
+}
+__device__ __forceinline__ void cluster_barrier()
+{
+    asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+__device__ __forceinline__ uint32_t map_to_rank(uint32_t local_addr, uint32_t rank)
+{
+    uint32_t r;
+    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(local_addr), "r"(rank));
+    return r;
+}
+__device__ __forceinline__ float ld_dsmem(const float* local_equiv, uint32_t rank)
+{
+    float v;
+    asm volatile("ld.shared::cluster.f32 %0, [%1];" : "=f"(v) : "r"(map_to_rank(smem_u32(local_equiv), rank)) : "memory");
+    return v;
+}
+__device__ __forceinline__ double ld_dsmem(const double* local_equiv, uint32_t rank)
+{
+    double v;
+    asm volatile("ld.shared::cluster.f64 %0, [%1];" : "=d"(v) : "r"(map_to_rank(smem_u32(local_equiv), rank)) : "memory");
+    return v;
+}
+__device__ __forceinline__ void ld_dsmem_u64x2(const void* local_equiv, uint32_t rank, unsigned long long& a,
+    unsigned long long& b)
+{
+    asm volatile("ld.shared::cluster.v2.u64 {%0, %1}, [%2];"
+                 : "=l"(a), "=l"(b)
+                 : "r"(map_to_rank(smem_u32(local_equiv), rank))
+                 : "memory");
+}
+
+// What one CTA posts for a column: its candidate and the candidate row.
+template <typename T, int W> struct alignas(16) ClusterPost
+{
+    unsigned long long key;  // PivKey<T>::type, widened
+    int32_t            row;  // global row, INT_MAX if none
+    int32_t            pad;
+    T                  data[W];
+};
+
+template <typename T, int W> constexpr int cluster_ldl() { return W + 16 / (int)sizeof(T); }
+template <typename T, int W> constexpr size_t cluster_row_bytes() { return (size_t)cluster_ldl<T, W>() * sizeof(T); }
+
+template <typename T, int W>
+__global__ void __launch_bounds__(kPanelThreads, 1) k_panel_cluster(T* __restrict__ A, int n, int k, int w,
+    int rows_per_cta, int64_t* __restrict__ pivot, PermList* __restrict__ perm, DeviceStatus* __restrict__ st)
+{
+    using K             = typename PivKey<T>::type;
+    using VT            = typename Vec16<T>::type;
+    constexpr int V     = 16 / (int)sizeof(T);
+    constexpr int LDL   = cluster_ldl<T, W>();
+    constexpr int WARPS = kPanelThreads / 32;
+    static_assert(W % 32 == 0 && W <= kNB, "panel width");
 
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    __shared__ __align__(16) T urow[kNB];               // the pivot row
-    __shared__ __align__(16) T drow[kNB];               // row c
-    __shared__ __align__(16) T post_data[2][kNB];       // read by the cluster
-    __shared__ __align__(16) T post_crow[2][kNB];
-    __shared__ double post_key[2];
-    __shared__ int    post_row[2];
-    __shared__ int    piv_loc[kNB];
-    __shared__ double red_key[kPanelThreads / 32 + 1];
-    __shared__ int    red_row[kPanelThreads / 32 + 1];
-    __shared__ int    s_p, s_rank_p;
+    __shared__ ClusterPost<T, W> post[2];
+    __shared__ __align__(16) T   post_crow[2][W];  // row c, posted by its owner
+    __shared__ __align__(16) T   urow[W];          // the pivot row
+    __shared__ __align__(16) T   drow[W];          // row c, in the CTA that holds row p
+    __shared__ K                 red_key[WARPS];
+    __shared__ int               red_row[WARPS];
+    __shared__ int               piv_loc[W];
+    __shared__ int               s_p;
 
-    const int tid  = threadIdx.x;
-    const int lane = tid & 31;
-    const int warp = tid >> 5;
-    const int CL   = (int)cluster.num_blocks();
-    const int b    = (int)cluster.block_rank();
-    const int r0   = k + b * rows_per_cta;
-    const int nloc = max(0, min(n, r0 + rows_per_cta) - r0);
-    constexpr int ldl = panel_ldl<T>();
+    const int      tid  = threadIdx.x;
+    const int      lane = tid & 31;
+    const int      warp = tid >> 5;
+    const uint32_t CL   = cluster_size();
+    const uint32_t b    = cluster_rank();
+    const int      r0   = k + (int)b * rows_per_cta;
+    const int      nloc = max(0, min(n, r0 + rows_per_cta) - r0);
+
+    // threads per row (a power of two, 1..W/CW_MIN) so that the CTA's rows
+    // keep every thread busy; each thread of a row owns CW contiguous columns
+    constexpr int CW_MIN = 16 / (int)sizeof(T) > 4 ? 16 / (int)sizeof(T) : 4;  // 4 columns (a vector or two)
+    int           TPR    = 1;
+    while (TPR * 2 <= W / CW_MIN && rows_per_cta * TPR * 2 <= kPanelThreads)
+    {
+        TPR *= 2;
+    }
+    const int CW    = W / TPR;
+    const int slots = kPanelThreads / TPR;  // rows updated at once
+    const int slot  = tid / TPR;
+    const int chunk = tid % TPR;
 
     T* loc = reinterpret_cast<T*>(smem_raw);
-    panel_slice_copy<T, true>(loc, ldl, A, n, r0, k, nloc, w);
+    panel_slice_copy<T, true>(loc, LDL, A, n, r0, k, nloc, w);
     __syncthreads();
 
-    double cand_key = -2.0;
-    int    cand_row = INT_MAX;
-    for (int r = max(0, k - r0) + tid; r < nloc; r += kPanelThreads)
     {
-        const double key = pivot_key(loc[r * ldl], r0 + r, k);
-        if (better(key, r0 + r, cand_key, cand_row))
+        K   ck = 0;
+        int cr = INT_MAX;
+        for (int r = max(0, k - r0) + tid; r < nloc; r += kPanelThreads)
         {
-            cand_key = key;
-            cand_row = r0 + r;
+            const K key = piv_key_bits(loc[(size_t)r * LDL], r0 + r == k);
+            if (key > ck)
+            {
+                ck = key;
+                cr = r0 + r;
+            }
+        }
+        warp_best_bits(ck, cr);
+        if (lane == 0)
+        {
+            red_key[warp] = ck;
+            red_row[warp] = cr;
         }
     }
-    block_best(cand_key, cand_row, red_key, red_row);
+    __syncthreads();
 
     int64_t first_zero = -1;
     for (int jj = 0; jj < w; ++jj)
     {
-        const int  c      = k + jj;
-        const int  par    = jj & 1;
-        const int  rank_c = (c - k) / rows_per_cta;
-        const bool own_c  = b == rank_c;
-        // ---- post
-        if (tid == 0)
-        {
-            post_key[par] = cand_key;
-            post_row[par] = cand_row;
-        }
-        if (tid < w && cand_row != INT_MAX)
-        {
-            post_data[par][tid] = loc[(size_t)(cand_row - r0) * ldl + tid];
-        }
-        else if (own_c && tid >= 64 && tid < 64 + w)
-        {
-            post_crow[par][tid - 64] = loc[(size_t)(c - r0) * ldl + (tid - 64)];
-        }
-        cluster.sync();  // every CTA's posts are readable
-        // ---- the pivot: keys (warp 0), then the pivot row and row c
+        const int      c      = k + jj;
+        const int      par    = jj & 1;
+        const uint32_t rank_c = (uint32_t)((c - k) / rows_per_cta);
+        // ---- post: warp 0 the CTA's candidate, warp 1 of row c's CTA row c
         if (warp == 0)
         {
-            double wk = -2.0;
-            int    wr = INT_MAX, wrank = -1;
-            if (lane < CL)
+            K   key = lane < WARPS ? red_key[lane] : K(0);
+            int row = lane < WARPS ? red_row[lane] : INT_MAX;
+            warp_best_bits(key, row);
+            if (lane == 0)
             {
-                wk    = cluster.map_shared_rank(post_key, lane)[par];
-                wr    = cluster.map_shared_rank(post_row, lane)[par];
-                wrank = lane;
+                post[par].key = (unsigned long long)key;
+                post[par].row = row;
             }
-#pragma unroll
-            for (int off = 16; off > 0; off >>= 1)
+            if (row != INT_MAX)
             {
-                const double ok    = __shfl_down_sync(0xffffffffu, wk, off);
-                const int    orow  = __shfl_down_sync(0xffffffffu, wr, off);
-                const int    orank = __shfl_down_sync(0xffffffffu, wrank, off);
-                if (better(ok, orow, wk, wr))
+                const T* src = loc + (size_t)(row - r0) * LDL;
+                for (int j = lane; j < w; j += 32)
                 {
-                    wk    = ok;
-                    wr    = orow;
-                    wrank = orank;
+                    post[par].data[j] = src[j];
+                }
+            }
+        }
+        else if (warp == 1 && b == rank_c)
+        {
+            const T* src = loc + (size_t)(c - r0) * LDL;
+            for (int j = lane; j < w; j += 32)
+            {
+                post_crow[par][j] = src[j];
+            }
+        }
+        cluster_barrier();
+        // ---- the pivot (warp 0): keys, then the pivot row (and row c)
+        if (warp == 0)
+        {
+            unsigned long long hk = 0, hr = INT_MAX;
+            if (lane < (int)CL)
+            {
+                ld_dsmem_u64x2(&post[par], (uint32_t)lane, hk, hr);
+            }
+            K   pk = (K)hk;
+            int p  = (int)(uint32_t)hr;
+            warp_best_bits(pk, p);
+            const uint32_t rank_p = (uint32_t)((p - k) / rows_per_cta);
+            for (int j = lane; j < w; j += 32)
+            {
+                urow[j] = ld_dsmem(&post[par].data[j], rank_p);
+            }
+            if (p != c && rank_p == b)
+            {
+                for (int j = lane; j < w; j += 32)
+                {
+                    drow[j] = ld_dsmem(&post_crow[par][j], rank_c);
                 }
             }
             if (lane == 0)
             {
-                s_p      = wr;
-                s_rank_p = wrank;
+                s_p         = p;
+                piv_loc[jj] = p;
+                if (b == 0)
+                {
+                    pivot[c] = (int64_t)p + 1;
+                }
             }
         }
         __syncthreads();
-        const int  p      = s_p;
-        const int  rank_p = s_rank_p;
-        const bool own_p  = p != c && b == rank_p;
-        if (tid < w)
-        {
-            urow[tid] = cluster.map_shared_rank(&post_data[0][0], rank_p)[par * kNB + tid];
-        }
-        else if (own_p && tid >= 64 && tid < 64 + w)
-        {
-            drow[tid - 64] = cluster.map_shared_rank(&post_crow[0][0], rank_c)[par * kNB + tid - 64];
-        }
-        __syncthreads();
-        if (tid == 0)
-        {
-            piv_loc[jj] = p;
-            if (b == 0)
-            {
-                pivot[c] = (int64_t)p + 1;
-            }
-        }
-        if (p != c)
-        {
-            if (own_c)
-            {
-                for (int cc = tid; cc < w; cc += kPanelThreads)
-                {
-                    loc[(size_t)(c - r0) * ldl + cc] = urow[cc];
-                }
-            }
-            if (own_p)
-            {
-                for (int cc = tid; cc < w; cc += kPanelThreads)
-                {
-                    loc[(size_t)(p - r0) * ldl + cc] = drow[cc];
-                }
-            }
-            __syncthreads();
-        }
-
-        const T d = urow[jj];
+        const int  p     = s_p;
+        const bool own_p = p != c && p >= r0 && p < r0 + nloc;
+        const T    d     = urow[jj];
         if (d == T(0) && first_zero < 0)
         {
             first_zero = c;
         }
-        double nk = -2.0;
-        int    nr = INT_MAX;
-        panel_update_rows(loc, ldl, max(0, c + 1 - r0), nloc, r0, jj, w, c, urow, d, nk, nr);
-        cand_key = nk;
-        cand_row = nr;
-        block_best(cand_key, cand_row, red_key, red_row);
+        // row c takes the pivot row (no other thread reads row c this column)
+        if (p != c && b == rank_c)
+        {
+            for (int j = tid; j < w; j += kPanelThreads)
+            {
+                loc[(size_t)(c - r0) * LDL + j] = urow[j];
+            }
+        }
+        // multipliers, rank-1 update and the next column's candidates: TPR
+        // threads per row, each on a chunk of CW columns (the multiplier is
+        // computed by each of them, identically)
+        const bool zero      = d == T(0);
+        const bool use_recip = fabs(d) >= Limits<T>::min_normal();
+        const T    recip     = use_recip ? (T)(T(1) / d) : T(1);
+        const bool has_next  = jj + 1 < w;
+        const int  cc0       = chunk * CW;  // this thread's columns [cc0, cc0 + CW)
+        K          ck        = 0;
+        int        cr        = INT_MAX;
+        const int rb = max(0, c + 1 - r0);
+        // the same trip count in every thread, so that the warp-wide sync
+        // below is reached by all lanes
+        const int trips = nloc > rb ? (nloc - rb + slots - 1) / slots : 0;
+        for (int t = 0; t < trips; ++t)
+        {
+            const int r = rb + slot + t * slots;
+            if (r >= nloc)
+            {
+                if (TPR > 1 && !zero)
+                {
+                    __syncwarp();
+                }
+                continue;
+            }
+            T*         row     = loc + (size_t)r * LDL;
+            const bool swapped = own_p && r0 + r == p;
+            const T*   src     = swapped ? drow : row;
+            if (swapped)
+            {
+                // row c's multipliers move with it (vectors, cc0 is aligned)
+                const int je = min(cc0 + CW, jj);
+                int       j  = cc0;
+                for (; j + V <= je; j += V)
+                {
+                    *reinterpret_cast<VT*>(row + j) = *reinterpret_cast<const VT*>(drow + j);
+                }
+                for (; j < je; ++j)
+                {
+                    row[j] = drow[j];
+                }
+            }
+            if (!zero)
+            {
+                const T x = src[jj];
+                const T l = use_recip ? x * recip : x / d;
+                if (TPR > 1)
+                {
+                    __syncwarp();  // every thread of the row has read a_rj before it is overwritten
+                }
+                if (jj >= cc0 && jj < cc0 + CW)
+                {
+                    row[jj] = l;
+                }
+                const int ce = min(cc0 + CW, w);
+                int       cc = max(cc0, jj + 1);
+                for (; cc < ce && (cc % V) != 0; ++cc)
+                {
+                    row[cc] = fma(-l, urow[cc], src[cc]);
+                }
+                for (; cc + V <= ce; cc += V)
+                {
+                    const VT sv = *reinterpret_cast<const VT*>(src + cc);
+                    const VT uv = *reinterpret_cast<const VT*>(urow + cc);
+                    VT       rv;
+                    if constexpr (V == 2)
+                    {
+                        rv.x = fma(-l, uv.x, sv.x);
+                        rv.y = fma(-l, uv.y, sv.y);
+                    }
+                    else
+                    {
+                        rv.x = fma(-l, uv.x, sv.x);
+                        rv.y = fma(-l, uv.y, sv.y);
+                        rv.z = fma(-l, uv.z, sv.z);
+                        rv.w = fma(-l, uv.w, sv.w);
+                    }
+                    *reinterpret_cast<VT*>(row + cc) = rv;
+                }
+                for (; cc < ce; ++cc)
+                {
+                    row[cc] = fma(-l, urow[cc], src[cc]);
+                }
+            }
+            else if (swapped)
+            {
+                for (int j = max(cc0, jj); j < cc0 + CW && j < w; ++j)
+                {
+                    row[j] = drow[j];
+                }
+            }
+            if (has_next && jj + 1 >= cc0 && jj + 1 < cc0 + CW)
+            {
+                const K key = piv_key_bits(row[jj + 1], r0 + r == c + 1);
+                if (key > ck)
+                {
+                    ck = key;
+                    cr = r0 + r;
+                }
+            }
+        }
+        warp_best_bits(ck, cr);
+        if (lane == 0)
+        {
+            red_key[warp] = ck;
+            red_row[warp] = cr;
+        }
+        __syncthreads();
     }
-    cluster.sync();  // no CTA exits while its shared memory may still be read
+    cluster_barrier();  // no CTA exits while its shared memory may still be read
 
-    panel_slice_copy<T, false>(loc, ldl, A, n, r0, k, nloc, w);
+    panel_slice_copy<T, false>(loc, LDL, A, n, r0, k, nloc, w);
     if (b == 0)
     {
         if (tid == 0 && first_zero >= 0 && st->first_zero < 0)
@@ -925,6 +1149,93 @@ __global__ void __launch_bounds__(kPanelThreads, 1) k_panel_cluster(T* __restric
         {
             build_perm_list(piv_loc, k, w, perm, lane);
         }
+    }
+}
+
+// The floor of k_panel_cluster's per-column exchange: the same cluster and
+// threads, warp 0's post of a key, the cluster barrier, warp 0's reads of
+// the CL keys and of W pivot-row values through distributed shared memory,
+// and the two block barriers; no slice, no update, no candidate search.
+// Thread 0 of rank 0 writes the elapsed %globaltimer nanoseconds of
+// `columns` columns to *ns.
+template <typename T, int W>
+__global__ void __launch_bounds__(kPanelThreads, 1) k_panel_exchange_floor(int columns,
+    unsigned long long* __restrict__ ns)
+{
+    using K             = typename PivKey<T>::type;
+    constexpr int WARPS = kPanelThreads / 32;
+    __shared__ ClusterPost<T, W> post[2];
+    __shared__ __align__(16) T   urow[W];
+    __shared__ K                 red_key[WARPS];
+    __shared__ int               red_row[WARPS];
+    __shared__ int               s_p;
+    const int      tid  = threadIdx.x;
+    const int      lane = tid & 31;
+    const int      warp = tid >> 5;
+    const uint32_t CL   = cluster_size();
+    const uint32_t b    = cluster_rank();
+    for (int j = tid; j < W; j += kPanelThreads)
+    {
+        post[0].data[j] = T(j);
+        post[1].data[j] = T(j);
+    }
+    if (lane == 0)
+    {
+        red_key[warp] = (K)(warp * 7 % 5 + 2);
+        red_row[warp] = warp + (int)b * 100;
+    }
+    cluster_barrier();
+    const uint64_t t0  = global_ns();
+    T              acc = T(0);
+    for (int jj = 0; jj < columns; ++jj)
+    {
+        const int par = jj & 1;
+        if (warp == 0)
+        {
+            K   key = lane < WARPS ? red_key[lane] : K(0);
+            int row = lane < WARPS ? red_row[lane] : INT_MAX;
+            warp_best_bits(key, row);
+            if (lane == 0)
+            {
+                post[par].key = (unsigned long long)key;
+                post[par].row = row;
+            }
+        }
+        cluster_barrier();
+        if (warp == 0)
+        {
+            unsigned long long hk = 0, hr = INT_MAX;
+            if (lane < (int)CL)
+            {
+                ld_dsmem_u64x2(&post[par], (uint32_t)lane, hk, hr);
+            }
+            K   pk = (K)hk;
+            int p  = (int)(uint32_t)hr;
+            warp_best_bits(pk, p);
+            const uint32_t rank_p = (uint32_t)(p % 100) % CL;
+            for (int j = lane; j < W; j += 32)
+            {
+                urow[j] = ld_dsmem(&post[par].data[j], rank_p);
+            }
+            if (lane == 0)
+            {
+                s_p = p;
+            }
+        }
+        __syncthreads();
+        acc += urow[jj % W];
+        if (lane == 0)
+        {
+            red_key[warp] = (K)(s_p & 1023) + K(2);
+            red_row[warp] = s_p + warp;
+        }
+        __syncthreads();
+    }
+    const uint64_t t1 = global_ns();
+    cluster_barrier();
+    if (b == 0 && tid == 0)
+    {
+        *ns = (t1 - t0) + (acc == T(-1) ? 1ull : 0ull);
     }
 }
 

@@ -39,6 +39,7 @@ namespace b200la
 namespace
 {
 constexpr int kOuterNB = 256;
+constexpr int kMaxBlockPanels = kOuterNB / 32;  // panels of an outer block (32 or 64 columns wide)
 
 // ---------------------------------------------------------------------------
 // kernels
@@ -537,7 +538,7 @@ MixedPlan plan_mixed(Arena& a, int64_t n, int64_t nrhs, int restart, bool fp64_f
     p.u12op    = a.next<float>((size_t)n * kOuterNB);
     p.u12small = a.next<float>((size_t)n * kOuterNB);
     p.perm     = a.next<int32_t>((size_t)n);
-    p.perms    = a.next<PermList>(2 * (kOuterNB / kNB));
+    p.perms    = a.next<PermList>(2 * kMaxBlockPanels);
     p.sel      = a.next<float>(64);
     p.l21inv   = a.next<float>((size_t)n);
     p.u12inv   = a.next<float>((size_t)n);
@@ -639,7 +640,32 @@ __global__ void __launch_bounds__(kBlockSwapThreads) k_laswp_block(float* __rest
 
 // The interchange lists of outer block K's panels (two sets, by the block's
 // parity, so a block's lists stay valid while the next block's panels run).
-inline PermList* block_perms(MixedPlan& p, int K) { return p.perms + ((K / kOuterNB) & 1) * (kOuterNB / kNB); }
+inline PermList* block_perms(MixedPlan& p, int K) { return p.perms + ((K / kOuterNB) & 1) * kMaxBlockPanels; }
+
+// Panel width of the outer blocks: 32 columns whenever a 32-column panel of
+// the block fits one cluster's shared memory (every order up to about
+// 25,000), else 64 on the grid-wide kernel.  32-column panels hold twice the
+// rows of 64-column ones in a cluster, cost a little less per column, and
+// one width for the whole factorization keeps its rounding the same from
+// block to block (measured at n = 16384: 5 refinement corrections, against 7
+// when the blocks whose 64-column panels fit used those).
+// B200LA_MIXED_PANEL_WIDTH=64 keeps 64-column panels where they fit.
+int block_panel_width(int n, int K)
+{
+    int cl = 0, gmax = 0;
+    if (panel_config<float>(cl, gmax) != B200LA_SUCCESS || cl == 0)
+        return 64;
+    const char* e = getenv("B200LA_MIXED_PANEL_WIDTH");
+    if (e != nullptr && e[0] == '6' && cluster_panel_fits<float>(n - K, 64, cl))
+        return 64;
+    return cluster_panel_fits<float>(n - K, 32, cl) ? 32 : 64;
+}
+
+inline int block_panel_count(int n, int K, int Kend)
+{
+    const int pw = block_panel_width(n, K);
+    return (Kend - K + pw - 1) / pw;
+}
 
 // Inner panels of the outer block [K, Kend): 64-column panels, their row
 // interchanges on columns [0, Kend) (right of the block they are applied
@@ -647,11 +673,12 @@ inline PermList* block_perms(MixedPlan& p, int K) { return p.perms + ((K / kOute
 // inside the block.  Panel j's interchange list goes to block_perms(p, K)[j].
 int enqueue_block_panels(MixedPlan& p, int n, int K, int Kend, int cl, int gmax, cudaStream_t s)
 {
-    float* a32 = p.a32;
-    int    rc  = B200LA_SUCCESS;
-    for (int k = K, j = 0; k < Kend; k += kNB, ++j)
+    float*    a32 = p.a32;
+    int       rc  = B200LA_SUCCESS;
+    const int pw  = block_panel_width(n, K);
+    for (int k = K, j = 0; k < Kend; k += pw, ++j)
     {
-        const int        w  = n - k < kNB ? n - k : kNB;
+        const int        w  = Kend - k < pw ? Kend - k : pw;
         GetrfPlan<float> gp = p.gp;
         gp.perm             = block_perms(p, K) + j;
         if ((rc = launch_panel<float>(a32, n, k, w, p.piv, gp, cl, gmax, s)) != B200LA_SUCCESS)
@@ -692,7 +719,7 @@ int enqueue_block_swaps(MixedPlan& p, int n, int K, int Kend, int c_begin, int c
         return B200LA_SUCCESS;
     prof_begin(KC_SWAP, s);
     k_laswp_block<<<(cols + kSwapCols - 1) / kSwapCols, kBlockSwapThreads, 0, s>>>(p.a32, n, block_perms(p, K),
-        (Kend - K + kNB - 1) / kNB, c_begin, c_end);
+        block_panel_count(n, K, Kend), c_begin, c_end);
     prof_end(KC_SWAP, s);
     B200LA_LAUNCH_CHECK();
     return B200LA_SUCCESS;
@@ -705,9 +732,9 @@ int enqueue_block_left_swaps(MixedPlan& p, int n, int K, int Kend, cudaStream_t 
 }
 
 // The outer block's interchanges applied to the row permutation.
-int enqueue_block_rowid(MixedPlan& p, int K, int Kend, cudaStream_t s)
+int enqueue_block_rowid(MixedPlan& p, int n, int K, int Kend, cudaStream_t s)
 {
-    k_rowid_apply<<<1, 2 * kNB, 0, s>>>(p.perm, block_perms(p, K), (Kend - K + kNB - 1) / kNB);
+    k_rowid_apply<<<1, 2 * kNB, 0, s>>>(p.perm, block_perms(p, K), block_panel_count(n, K, Kend));
     B200LA_LAUNCH_CHECK();
     return B200LA_SUCCESS;
 }
@@ -801,11 +828,24 @@ void enqueue_block_operands(MixedPlan& p, int n, int K, int Kend, int rest, int 
 // The tensor-core trailing update of the outer block (columns [c0, n) of
 // A22 = rows and columns from Kend), operands from the block's copies.
 int enqueue_block_update(MixedPlan& p, int n, int Kend, int c0, int kind, bool split, const CUtensorMap& ma,
-    const CUtensorMap& mb, const CUtensorMap& mas, const CUtensorMap& mbs, int ncols, cudaStream_t s)
+    const CUtensorMap& mb, const CUtensorMap& mas, const CUtensorMap& mbs, int ncols, cudaStream_t s,
+    int max_ctas = 0)
 {
     const int rest = n - Kend;
     return enqueue_tc_update(kind, split, ma, mb, mas, mbs, p.a32 + (int64_t)Kend * n + c0, n, rest, ncols, kOuterNB,
-        p.gp.st, s, p.l21inv, p.u12inv + (c0 - Kend));
+        p.gp.st, s, p.l21inv, p.u12inv + (c0 - Kend), max_ctas);
+}
+
+// CTAs of the persistent tensor-core update that runs beside the next
+// block's panels: the SMs less those the panel cluster and the panels'
+// in-block kernels use (B200LA_MIXED_UPDATE_CTAS overrides).
+int beside_panel_ctas()
+{
+    const char* e = getenv("B200LA_MIXED_UPDATE_CTAS");
+    if (e != nullptr && atoi(e) > 0)
+        return atoi(e);
+    const int sms = device_sm_count();
+    return sms > 40 ? sms - 24 : sms;
 }
 
 // Mixed-precision factorization of p.a32 in place; pivots in p.piv.
@@ -907,7 +947,7 @@ int enqueue_getrf_mixed(MixedPlan& p, int n, int kind, bool split, cudaStream_t 
             B200LA_CUDA(cudaStreamWaitEvent(s, ev_panels, 0));
             panels_on_side = false;
         }
-        if ((rc = enqueue_block_rowid(p, K, Kend, s)) != B200LA_SUCCESS)
+        if ((rc = enqueue_block_rowid(p, n, K, Kend, s)) != B200LA_SUCCESS)
             return rc;
         const int rest = n - Kend;
         if (rest <= 0)
@@ -953,7 +993,8 @@ int enqueue_getrf_mixed(MixedPlan& p, int n, int kind, bool split, cudaStream_t 
             enqueue_block_operands(p, n, K, Kend, rest, kind, split, first, nstrips - first, false, s);
             prof_end(KC_PREP, s);
             B200LA_LAUNCH_CHECK();
-            if ((rc = enqueue_block_update(p, n, Kend, Kend2, kind, split, ma, mb2, mas, mbs2, n - Kend2, s)) !=
+            if ((rc = enqueue_block_update(p, n, Kend, Kend2, kind, split, ma, mb2, mas, mbs2, n - Kend2, s,
+                     beside_panel_ctas())) !=
                 B200LA_SUCCESS)
                 return rc;
         }

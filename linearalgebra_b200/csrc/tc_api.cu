@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 
 #include <climits>
+#include <cstdlib>
 #include <mutex>
 
 #include "tc_api.cuh"
@@ -50,6 +51,8 @@ template <int KIND, bool SPLIT3> int set_attr_once()
     }
     B200LA_CUDA(cudaFuncSetAttribute(k_tc_update<KIND, SPLIT3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
         (int)tc_smem_bytes<SPLIT3>()));
+    B200LA_CUDA(cudaFuncSetAttribute(k_tc_update_persistent<KIND, SPLIT3>,
+        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tcp_smem_bytes<SPLIT3>()));
     if (dev >= 0 && dev < 64)
     {
         done[dev] = true;
@@ -89,15 +92,43 @@ int make_kmajor_map(CUtensorMap* map, const void* base, int kind, int64_t rows, 
     return B200LA_SUCCESS;
 }
 
+// B200LA_TC_PERSISTENT=0 launches one CTA per tile (k_tc_update) instead of
+// the persistent kernel (same per-element arithmetic).
+static bool tc_persistent_enabled()
+{
+    const char* e = getenv("B200LA_TC_PERSISTENT");
+    return !(e != nullptr && e[0] == '0');
+}
+
 template <int KIND, bool SPLIT3>
 static int launch_tc(const CUtensorMap& a, const CUtensorMap& b, const CUtensorMap& as, const CUtensorMap& bs,
     float* c, int64_t ldc, int m, int n, int k, DeviceStatus* st, const float* inv_sa, const float* inv_sb,
-    cudaStream_t s)
+    cudaStream_t s, int max_ctas)
 {
     int rc = set_attr_once<KIND, SPLIT3>();
     if (rc != B200LA_SUCCESS)
     {
         return rc;
+    }
+    const int tiles = ((n + kTcBN - 1) / kTcBN) * ((m + kTcBM - 1) / kTcBM);
+    if (tc_persistent_enabled())
+    {
+        const int sms = device_sm_count();
+        // B200LA_TC_CTAS caps the persistent grid (the tests use it to make
+        // every CTA walk many tiles)
+        const char* cap = getenv("B200LA_TC_CTAS");
+        if (cap != nullptr && atoi(cap) > 0)
+        {
+            max_ctas = max_ctas > 0 && max_ctas < atoi(cap) ? max_ctas : atoi(cap);
+        }
+        int g = max_ctas > 0 && max_ctas < sms ? max_ctas : sms;
+        g             = g < tiles ? g : tiles;
+        prof_begin(KC_MIXED, s);
+        k_tc_update_persistent<KIND, SPLIT3><<<g, kTcpThreads, tcp_smem_bytes<SPLIT3>(), s>>>(a, b, as, bs, c, ldc,
+            m, n, k, st, inv_sa, inv_sb);
+        prof_end(KC_MIXED, s);
+        B200LA_LAUNCH_CHECK();
+        return B200LA_SUCCESS;
     }
     dim3 grid((n + kTcBN - 1) / kTcBN, (m + kTcBM - 1) / kTcBM);
     prof_begin(KC_MIXED, s);
@@ -110,7 +141,7 @@ static int launch_tc(const CUtensorMap& a, const CUtensorMap& b, const CUtensorM
 
 int enqueue_tc_update(int kind, bool split3, const CUtensorMap& a, const CUtensorMap& b, const CUtensorMap& as,
     const CUtensorMap& bs, float* c, int64_t ldc, int m, int n, int k, DeviceStatus* st, cudaStream_t s,
-    const float* inv_sa, const float* inv_sb)
+    const float* inv_sa, const float* inv_sb, int max_ctas)
 {
     if (m <= 0 || n <= 0)
     {
@@ -123,8 +154,8 @@ int enqueue_tc_update(int kind, bool split3, const CUtensorMap& a, const CUtenso
     }
     if (kind == TC_TF32)
     {
-        return split3 ? launch_tc<TC_TF32, true>(a, b, as, bs, c, ldc, m, n, k, st, nullptr, nullptr, s)
-                      : launch_tc<TC_TF32, false>(a, b, as, bs, c, ldc, m, n, k, st, nullptr, nullptr, s);
+        return split3 ? launch_tc<TC_TF32, true>(a, b, as, bs, c, ldc, m, n, k, st, nullptr, nullptr, s, max_ctas)
+                      : launch_tc<TC_TF32, false>(a, b, as, bs, c, ldc, m, n, k, st, nullptr, nullptr, s, max_ctas);
     }
     if (split3)
     {
@@ -132,7 +163,7 @@ int enqueue_tc_update(int kind, bool split3, const CUtensorMap& a, const CUtenso
     }
     if (kind == TC_BF16)
     {
-        return launch_tc<TC_BF16, false>(a, b, as, bs, c, ldc, m, n, k, st, nullptr, nullptr, s);
+        return launch_tc<TC_BF16, false>(a, b, as, bs, c, ldc, m, n, k, st, nullptr, nullptr, s, max_ctas);
     }
     if (kind == TC_FP8)
     {
@@ -140,9 +171,9 @@ int enqueue_tc_update(int kind, bool split3, const CUtensorMap& a, const CUtenso
         {
             return set_error(B200LA_INVALID_ARGUMENT, "tensor-core update: FP8 operands need their scales");
         }
-        return launch_tc<TC_FP8, false>(a, b, as, bs, c, ldc, m, n, k, st, inv_sa, inv_sb, s);
+        return launch_tc<TC_FP8, false>(a, b, as, bs, c, ldc, m, n, k, st, inv_sa, inv_sb, s, max_ctas);
     }
-    return launch_tc<TC_FP16, false>(a, b, as, bs, c, ldc, m, n, k, st, nullptr, nullptr, s);
+    return launch_tc<TC_FP16, false>(a, b, as, bs, c, ldc, m, n, k, st, nullptr, nullptr, s, max_ctas);
 }
 
 }  // namespace b200la

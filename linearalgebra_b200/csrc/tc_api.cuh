@@ -13,9 +13,11 @@ namespace b200la
 int make_kmajor_map(CUtensorMap* map, const void* base, int kind, int64_t rows, int64_t k, int64_t ld,
     int box_rows);
 
-// C[m x n] -= A B^T on the tensor cores (see k_tc_update).  FP8 operands
-// need the inverse power-of-two scales of their rows (inv_sa[m], inv_sb[n]).
+// C[m x n] -= A B^T on the tensor cores (k_tc_update_persistent, or
+// k_tc_update with B200LA_TC_PERSISTENT=0).  FP8 operands need the inverse
+// power-of-two scales of their rows (inv_sa[m], inv_sb[n]).  max_ctas > 0
+// caps the persistent grid (leaving SMs to kernels on other streams).
 int enqueue_tc_update(int kind, bool split3, const CUtensorMap& a, const CUtensorMap& b, const CUtensorMap& as,
     const CUtensorMap& bs, float* c, int64_t ldc, int m, int n, int k, DeviceStatus* st, cudaStream_t s,
-    const float* inv_sa = nullptr, const float* inv_sb = nullptr);
+    const float* inv_sa = nullptr, const float* inv_sb = nullptr, int max_ctas = 0);
 }  // namespace b200la

@@ -420,4 +420,330 @@ __global__ void __launch_bounds__(128, 1) k_tc_update(const __grid_constant__ CU
     }
 }
 
+// ---------------------------------------------------------------------------
+// Persistent form of the same update: one CTA per SM walks the 128 x 256
+// tiles t = blockIdx.x, blockIdx.x + gridDim.x, ... (tile t covers rows
+// (t % Mt) * 128 and columns (t / Mt) * 256), with two accumulators of 256
+// TMEM columns so the epilogue of tile i runs while the MMAs of tile i + 1
+// do:
+//   * warp 0 / lane 0: TMA loads into the stage ring, across tiles;
+//   * warp 1: allocates 512 TMEM columns; lane 0 issues the MMAs of tile i
+//     into accumulator i % 2 once the epilogue has released it, and commits
+//     the accumulator to acc_full[i % 2];
+//   * warps 2..5: epilogue, one row of the tile per thread (warp w reads
+//     TMEM lanes 32 (w % 4) ...), C -= acc in 32-column chunks with the
+//     next chunk's C loads in flight, then release the accumulator
+//     (acc_empty, 128 arrivals); the C rows of the CTA's next tile are
+//     prefetched into L2 when a tile's epilogue starts.
+// The per-element arithmetic is that of k_tc_update.  Every wait is bounded;
+// on a timeout the CTA records the error, stops issuing, drains its loads
+// and MMAs in flight (bounded) and frees its tensor memory.
+// ---------------------------------------------------------------------------
+constexpr int kTcpThreads = 192;
+
+template <bool SPLIT3> constexpr size_t tcp_smem_bytes()
+{
+    return (size_t)tc_stages<SPLIT3>() * tc_stage_bytes<SPLIT3>() + 1024 + 256;
+}
+
+template <int KIND, bool SPLIT3>
+__global__ void __launch_bounds__(kTcpThreads, 1) k_tc_update_persistent(const __grid_constant__ CUtensorMap tmA,
+    const __grid_constant__ CUtensorMap tmB, const __grid_constant__ CUtensorMap tmAs,
+    const __grid_constant__ CUtensorMap tmBs, float* __restrict__ C, int64_t ldc, int M, int N, int K,
+    DeviceStatus* __restrict__ st, const float* __restrict__ inv_sa, const float* __restrict__ inv_sb)
+{
+    constexpr int      S     = tc_stages<SPLIT3>();
+    constexpr int      SB    = tc_stage_bytes<SPLIT3>();
+    constexpr int      EA    = kTcAtomBytes / TcTraits<KIND>::elem;
+    constexpr uint32_t IDESC = tc_idesc<KIND>();
+
+    extern __shared__ __align__(1024) unsigned char tcp_smem_raw[];
+    unsigned char* base = reinterpret_cast<unsigned char*>(
+        (reinterpret_cast<uintptr_t>(tcp_smem_raw) + 1023) & ~uintptr_t(1023));
+    unsigned char* tiles     = base;
+    uint64_t*      full      = reinterpret_cast<uint64_t*>(base + (size_t)S * SB);
+    uint64_t*      empty     = full + S;
+    uint64_t*      acc_full  = empty + S;     // [2]
+    uint64_t*      acc_empty = acc_full + 2;  // [2]
+    uint64_t*      mma_done  = acc_empty + 2;
+    uint32_t*      tmem_ptr  = reinterpret_cast<uint32_t*>(mma_done + 1);
+    int*           s_fail    = reinterpret_cast<int*>(tmem_ptr + 1);
+    int*           s_issued  = s_fail + 1;  // stage-ring loads issued
+
+    const int warp   = threadIdx.x >> 5;
+    const int lane   = threadIdx.x & 31;
+    const int Mt     = (M + kTcBM - 1) / kTcBM;
+    const int Nt     = (N + kTcBN - 1) / kTcBN;
+    const int tiles_ = Mt * Nt;
+    const int natoms = K / EA;
+
+    if (threadIdx.x == 0)
+    {
+        for (int s = 0; s < S; ++s)
+        {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], 1);
+        }
+        mbar_init(&acc_full[0], 1);
+        mbar_init(&acc_full[1], 1);
+        mbar_init(&acc_empty[0], 128);
+        mbar_init(&acc_empty[1], 128);
+        mbar_init(mma_done, 1);
+        *s_fail   = 0;
+        *s_issued = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 1)
+    {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                         smem_u32(tmem_ptr)),
+            "r"(2 * kTcBN)
+            : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tmem_ptr;
+    auto failed = [&]() { return *reinterpret_cast<volatile int*>(s_fail) != 0; };
+    auto fail   = [&](int site) {
+        raise_error(st, DEV_WAIT_TIMEOUT, site);
+        atomicExch(s_fail, 1);
+    };
+
+    if (warp == 0)
+    {
+        if (lane == 0)
+        {
+            int it = 0;
+            for (int t = blockIdx.x; t < tiles_ && !failed(); t += gridDim.x)
+            {
+                const int m0 = (t % Mt) * kTcBM;
+                const int n0 = (t / Mt) * kTcBN;
+                for (int a = 0; a < natoms; ++a, ++it)
+                {
+                    const int s = it % S;
+                    if (it >= S && !mbar_wait(&empty[s], ((it / S) - 1) & 1))
+                    {
+                        fail(13);
+                        break;
+                    }
+                    if (failed())
+                    {
+                        break;
+                    }
+                    unsigned char* stage = tiles + (size_t)s * SB;
+                    mbar_expect_tx(&full[s], SB);
+                    tma_load_2d(stage, &tmA, a * EA, m0, &full[s]);
+                    tma_load_2d(stage + kTcTileA, &tmB, a * EA, n0, &full[s]);
+                    if constexpr (SPLIT3)
+                    {
+                        tma_load_2d(stage + kTcPair, &tmAs, a * EA, m0, &full[s]);
+                        tma_load_2d(stage + kTcPair + kTcTileA, &tmBs, a * EA, n0, &full[s]);
+                    }
+                    *reinterpret_cast<volatile int*>(s_issued) = it + 1;
+                }
+            }
+        }
+    }
+    else if (warp == 1)
+    {
+        if (lane == 0)
+        {
+            int it = 0, ti = 0;
+            for (int t = blockIdx.x; t < tiles_ && !failed(); t += gridDim.x, ++ti)
+            {
+                const int acc = ti & 1;
+                if (ti >= 2 && !mbar_wait(&acc_empty[acc], ((ti >> 1) - 1) & 1))
+                {
+                    fail(14);
+                    break;
+                }
+                tc_fence_after();
+                const uint32_t d  = tmem + (uint32_t)(acc * kTcBN);
+                bool           ok = true;
+                for (int a = 0; a < natoms; ++a, ++it)
+                {
+                    const int s = it % S;
+                    if (!mbar_wait(&full[s], (it / S) & 1))
+                    {
+                        fail(15);
+                        ok = false;
+                        break;
+                    }
+                    tc_fence_after();
+                    const uint32_t sa = smem_u32(tiles + (size_t)s * SB);
+                    const uint32_t sb = sa + kTcTileA;
+#pragma unroll
+                    for (int kk = 0; kk < kTcAtomBytes / 32; ++kk)
+                    {
+                        const uint64_t da = tc_desc(sa + kk * 32);
+                        const uint64_t db = tc_desc(sb + kk * 32);
+                        tc_mma<KIND>(d, da, db, IDESC, (a > 0 || kk > 0) ? 1u : 0u);
+                        if constexpr (SPLIT3)
+                        {
+                            const uint64_t das = tc_desc(sa + kTcPair + kk * 32);
+                            const uint64_t dbs = tc_desc(sa + kTcPair + kTcTileA + kk * 32);
+                            tc_mma<KIND>(d, da, dbs, IDESC, 1u);
+                            tc_mma<KIND>(d, das, db, IDESC, 1u);
+                        }
+                    }
+                    tc_commit(&empty[s]);
+                }
+                if (!ok)
+                {
+                    break;
+                }
+                tc_commit(&acc_full[acc]);
+            }
+            tc_commit(mma_done);  // every MMA this thread issued has completed when this arrives
+        }
+    }
+    else
+    {
+        // epilogue warps: TMEM lane quarter q = warp % 4
+        const int  q   = warp & 3;
+        const int  row = q * 32 + lane;
+        const bool vec = ((ldc & 3) == 0) && ((reinterpret_cast<uintptr_t>(C) & 15) == 0);
+        auto prefetch_rows = [&](int t) {
+            if (t >= tiles_)
+            {
+                return;
+            }
+            const int r  = (t % Mt) * kTcBM + row;
+            const int n0 = (t / Mt) * kTcBN;
+            if (r < M && n0 + kTcBN <= N && vec)
+            {
+                asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(C + (size_t)r * ldc + n0),
+                    "r"(kTcBN * 4)
+                    : "memory");
+            }
+        };
+        prefetch_rows(blockIdx.x);
+        int ti = 0;
+        for (int t = blockIdx.x; t < tiles_; t += gridDim.x, ++ti)
+        {
+            const int  acc = ti & 1;
+            const bool got = __all_sync(0xffffffffu, mbar_wait(&acc_full[acc], (ti >> 1) & 1));
+            if (!got)
+            {
+                if (lane == 0)
+                {
+                    fail(16);
+                }
+                break;
+            }
+            if (__any_sync(0xffffffffu, failed()))
+            {
+                break;
+            }
+            tc_fence_after();
+            prefetch_rows(t + gridDim.x);
+            const int  m0     = (t % Mt) * kTcBM;
+            const int  n0     = (t / Mt) * kTcBN;
+            const int  r      = m0 + row;
+            const bool row_ok = r < M;
+            float*     crow   = C + (size_t)(row_ok ? r : 0) * ldc;
+            float4     cv[8], cn[8];
+            auto       fast_at = [&](int j) { return row_ok && vec && n0 + j * 32 + 32 <= N; };
+            auto       load_c  = [&](int j, float4(&dst)[8]) {
+                const float4* p = reinterpret_cast<const float4*>(crow + n0 + j * 32);
+#pragma unroll
+                for (int qq = 0; qq < 8; ++qq)
+                {
+                    dst[qq] = p[qq];
+                }
+            };
+            if (fast_at(0))
+            {
+                load_c(0, cv);
+            }
+#pragma unroll 1
+            for (int j = 0; j < kTcBN / 32; ++j)
+            {
+                const int  c0   = n0 + j * 32;
+                const bool fast = fast_at(j);
+                if (j + 1 < kTcBN / 32 && fast_at(j + 1))
+                {
+                    load_c(j + 1, cn);
+                }
+                float v[32];
+                tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(acc * kTcBN + j * 32), v);
+                if (row_ok)
+                {
+                    if constexpr (KIND == TC_FP8)
+                    {
+                        const float ra = inv_sa[r];
+#pragma unroll
+                        for (int qq = 0; qq < 32; ++qq)
+                        {
+                            v[qq] *= ra * (c0 + qq < N ? inv_sb[c0 + qq] : 0.f);
+                        }
+                    }
+                    if (fast)
+                    {
+                        float4* p = reinterpret_cast<float4*>(crow + c0);
+#pragma unroll
+                        for (int qq = 0; qq < 8; ++qq)
+                        {
+                            float4 x = cv[qq];
+                            x.x -= v[4 * qq];
+                            x.y -= v[4 * qq + 1];
+                            x.z -= v[4 * qq + 2];
+                            x.w -= v[4 * qq + 3];
+                            p[qq] = x;
+                        }
+                    }
+                    else
+                    {
+#pragma unroll
+                        for (int qq = 0; qq < 32; ++qq)
+                        {
+                            if (c0 + qq < N)
+                            {
+                                crow[c0 + qq] -= v[qq];
+                            }
+                        }
+                    }
+                }
+#pragma unroll
+                for (int qq = 0; qq < 8; ++qq)
+                {
+                    cv[qq] = cn[qq];
+                }
+            }
+            tc_fence_before();
+            asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&acc_empty[acc])) : "memory");
+        }
+    }
+    __syncwarp();
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 1 && lane == 0)
+    {
+        // every MMA issued has completed (bounded wait)
+        mbar_wait(mma_done, 0);
+    }
+    if (warp == 0 && lane == 0 && failed())
+    {
+        // drain: the loads this CTA issued and nobody consumed
+        const int issued = *reinterpret_cast<volatile int*>(s_issued);
+        for (int s = 0; s < S; ++s)
+        {
+            if (s < issued)
+            {
+                const int last = ((issued - 1 - s) / S) * S + s;
+                mbar_wait(&full[s], (last / S) & 1);
+            }
+        }
+    }
+    __syncthreads();
+    if (warp == 1)
+    {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2 * kTcBN)
+                     : "memory");
+    }
+}
+
 }  // namespace b200la

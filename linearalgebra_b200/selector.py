@@ -226,6 +226,7 @@ class Network:
                                np.asarray(inv_std, np.float32)])
         self.buf = torch.from_numpy(host).to(device)
         self.device = device
+        self.meta: dict = {}
 
     @property
     def params(self) -> torch.Tensor:
@@ -275,7 +276,9 @@ class Network:
         p = np.asarray(d["params"], np.float32)
         if p.size != N_PARAMS or hashlib.sha256(p.tobytes()).hexdigest() != d["sha256"]:
             raise ValueError(f"{path}: parameter checksum mismatch")
-        return cls(p, np.asarray(d["mean"]), np.asarray(d["inv_std"]), device)
+        net = cls(p, np.asarray(d["mean"]), np.asarray(d["inv_std"]), device)
+        net.meta = d.get("meta", {})
+        return net
 
 
 def train(feats: np.ndarray, labels: np.ndarray, epochs: int = 300, batch: int = 512, lr: float = 3e-3,

@@ -49,6 +49,49 @@ def test_batched_matches_oracle(port, precision):
         assert np.abs(X - xr).max() / np.abs(xr).max() < 1e-8
 
 
+@pytest.mark.parametrize("threads", [64, 128, 256])
+def test_batched_group_sizes_match_oracle(port, threads):
+    """Every threads-per-system choice (a CTA solving 4, 2 or 1 systems at
+    once) and both panel widths give solutions at eta <= 1e-14."""
+    from linearalgebra_b200.batched import entry, table_valid
+    rng = np.random.default_rng(threads)
+    sizes = np.concatenate([rng.integers(1, 129, size=40), [1, 2, 3, 31, 32, 33, 64, 65, 127, 128]])
+    for nb in (16, 32, 7):
+        table = [entry(nb, threads)] * 2 + [entry(16, 256)] * 6
+        if not table_valid(_lib.PREC_FP32, table):
+            continue
+        solver = BatchedSolver(sizes, "fp32", nb_table=table)
+        a = torch.randn(solver.total_a, dtype=torch.float64, device="cuda")
+        b = torch.randn(solver.total_v, dtype=torch.float64, device="cuda")
+        x = torch.empty_like(b)
+        solver.launch(a, b, x)
+        torch.cuda.synchronize()
+        st = solver.status.cpu().numpy()
+        assert np.all(st >= 0), (nb, st)
+        assert solver.berr.max().item() <= 1e-14
+        for i in range(0, solver.count, 7):
+            A, B, X = host_views(solver, a, b, x, i)
+            assert port.backward_error(A, X, B) <= 1e-14
+
+
+def test_batched_unsorted_order_is_safe(port):
+    """An order that is not largest first (a larger system after a smaller
+    one in a chunk) is solved with the whole CTA instead of overflowing a
+    group's shared memory."""
+    sizes = np.array([20, 500, 30, 480, 100, 512, 17, 256])
+    solver = BatchedSolver(sizes, "fp32")
+    solver.order = torch.arange(len(sizes), dtype=torch.int32, device="cuda")
+    a = torch.randn(solver.total_a, dtype=torch.float64, device="cuda")
+    b = torch.randn(solver.total_v, dtype=torch.float64, device="cuda")
+    x = torch.empty_like(b)
+    solver.launch(a, b, x)
+    torch.cuda.synchronize()
+    assert np.all(solver.status.cpu().numpy() >= 0)
+    for i in range(len(sizes)):
+        A, B, X = host_views(solver, a, b, x, i)
+        assert port.backward_error(A, X, B) <= 1e-14
+
+
 def test_batched_singular_and_graph(tmp_path, monkeypatch):
     monkeypatch.setenv("B200LA_TUNE_CACHE", str(tmp_path / "tune.json"))
     sizes = np.array([40, 300, 33, 129])
@@ -71,7 +114,9 @@ def test_batched_singular_and_graph(tmp_path, monkeypatch):
     torch.cuda.synchronize()
     assert torch.equal(x1, x)
     entry = solver.autotune(a, b, x, sample_per_bucket=2)
-    assert len(entry["nb_table"]) == 8 and all(v in (16, 32) for v in entry["nb_table"])
+    assert len(entry["nb_table"]) == 8
+    assert all(p["panel_width"] in (16, 32) and p["threads_per_system"] in (64, 128, 256)
+               for p in entry["per_bucket"])
     assert (tmp_path / "tune.json").exists()
     again = solver.autotune(a, b, x)  # from the cache
     assert again["nb_table"] == entry["nb_table"]

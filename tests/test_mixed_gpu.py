@@ -36,6 +36,55 @@ def test_mixed_reaches_fp64_accuracy(port, precision, n):
     assert np.abs(xs - x_ref).max() / np.abs(x_ref).max() < 1e-9
 
 
+def test_mixed_64_column_panels(port, monkeypatch):
+    """64-column cluster panels (B200LA_MIXED_PANEL_WIDTH=64) instead of the
+    default 32-column ones: same accuracy."""
+    monkeypatch.setenv("B200LA_MIXED_PANEL_WIDTH", "64")
+    n = 1100
+    a, _, b = system(n, seed=1132)
+    x, res, st = la.solve_mixed(dev(a), dev(b), precision="fp32", tolerance=1e-14)
+    torch.cuda.synchronize()
+    assert st == 0 and res["converged"] == 1 and res["escalations"] == 0, res
+    assert port.backward_error(a, x.cpu().numpy(), b) <= 1e-14
+
+
+def test_mixed_at_headline_order_agrees_with_fp64_lu():
+    """n = 16384, A iid N(0,1) (the benchmark's system): the mixed solve
+    (FP32 factors, FP64 refinement) reaches eta <= 1e-14 and agrees with the
+    plain FP64 LU solve (the reference's algorithm, bit-identical factors)
+    to well within what the conditioning allows."""
+    from linearalgebra_b200 import _lib
+    n = 16384
+    g = torch.Generator(device="cuda").manual_seed(16384)
+    A = torch.randn(n, n, dtype=torch.float64, device="cuda", generator=g)
+    x_true = torch.rand(n, dtype=torch.float64, device="cuda", generator=g) * 2 - 1
+    b = A @ x_true
+    x, res, st = la.solve_mixed(A, b, precision="fp32", tolerance=1e-14)
+    assert st == 0 and res["converged"] == 1, res
+    lib = _lib.load()
+    m = A.clone()
+    x64 = b.clone()
+    piv = torch.empty(n, dtype=torch.int64, device="cuda")
+    nbytes = lib.b200la_dgesv_workspace_size(n, 1)
+    ws = torch.empty(nbytes, dtype=torch.uint8, device="cuda")
+    _lib.check(lib.b200la_dgesv(m.data_ptr(), piv.data_ptr(), n, x64.data_ptr(), 1, ws.data_ptr(), nbytes,
+                                torch.cuda.current_stream().cuda_stream))
+    del m, ws
+    anorm = A.abs().sum(1).max()
+
+    def eta(xx):
+        return ((b - A @ xx).abs().max() / (anorm * xx.abs().max() + b.abs().max())).item()
+
+    assert eta(x) <= 1e-14
+    assert eta(x64) <= 10 * n * EPS64
+    # both solutions are backward stable; their difference is bounded by
+    # cond(A) times their backward errors (cond_inf of this class is ~1e5-1e6)
+    diff = ((x - x64).abs().max() / x64.abs().max()).item()
+    assert diff < 1e-7, diff
+    fwd = ((x - x_true).abs().max() / x_true.abs().max()).item()
+    assert fwd < 1e-7, fwd
+
+
 def test_mixed_fp32_takes_few_iterations():
     a, _, b = system(2048, seed=5)
     _, res, st = la.solve_mixed(dev(a), dev(b), precision="fp32")

@@ -113,3 +113,20 @@ def test_tc_update_fp8_rejects_missing_scales():
     st = lib.b200la_sgemm_tc_update_fp8(p.data_ptr(), 8, 8, 8, 128, p.data_ptr(), p.data_ptr(), None,
                                         p.data_ptr(), ws.data_ptr(), 256, None)
     assert st == _lib.INVALID_ARGUMENT
+
+
+@pytest.mark.parametrize("kind,split3", [(TF32, True), (BF16, False)])
+@pytest.mark.parametrize("ctas", ["3", "148"])
+def test_tc_update_persistent_walks_many_tiles(monkeypatch, kind, split3, ctas):
+    """The persistent kernel with 3 CTAs (each walks ~30 tiles through both
+    accumulators and the stage ring) and with a full grid over 4 x 12 tile
+    rows: same result as the reference."""
+    monkeypatch.setenv("B200LA_TC_CTAS", ctas)
+    err, tol = run(kind, split3, 1500, 1800, 256, seed=5)
+    assert err <= tol, (err, tol)
+
+
+def test_tc_update_per_tile_kernel_still_matches(monkeypatch):
+    monkeypatch.setenv("B200LA_TC_PERSISTENT", "0")
+    err, tol = run(TF32, True, 1000, 520, 128)
+    assert err <= tol, (err, tol)
