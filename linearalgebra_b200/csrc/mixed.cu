@@ -510,7 +510,7 @@ struct MixedPlan
     double*            y;       // n x nrhs scratch for the solves
     unsigned long long* norms;  // [0] ||A||, [1..] per-column maxima (3 x 64)
     TrsvSync*          tsync;
-    double*            dinv;    // inverses of the 64 x 64 diagonal blocks of L and U
+    double*            dinv;    // inverses of the 128 x 128 diagonal blocks of L and U
     uint64_t*          xll;     // flagged copies of solved blocks (k_trsv_blocks)
     double*            V;       // GMRES basis (m+1) x n
     double*            h;       // GMRES dot products (m+1)
@@ -546,7 +546,7 @@ MixedPlan plan_mixed(Arena& a, int64_t n, int64_t nrhs, int restart, bool fp64_f
     p.y        = a.next<double>((size_t)n * nrhs);
     p.norms    = a.next<unsigned long long>(4 + 3 * kMaxNrhsMixed + 16);
     p.tsync    = reinterpret_cast<TrsvSync*>(a.next<int32_t>(32 + (size_t)(n + kTvRows - 1) / kTvRows + 32));
-    p.dinv     = a.next<double>((size_t)((n + kTvRows - 1) / kTvRows) * 2 * kTvRows * kTvRows);
+    p.dinv     = a.next<double>((size_t)((n + kTrRows - 1) / kTrRows) * 2 * kTrRows * kTrRows);
     p.xll      = a.next<uint64_t>((size_t)((n + kTvRows - 1) / kTvRows) * kTvRows * 2);
     const int m = restart > 0 ? restart : 0;
     p.V        = a.next<double>((size_t)(m + 1) * n);
@@ -1041,6 +1041,10 @@ int set_mixed_attributes()
     B200LA_CUDA(cudaFuncSetAttribute(k_outer_u12<TC_BF16, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)outer_u12_smem()));
     B200LA_CUDA(cudaFuncSetAttribute(k_outer_u12<TC_FP16, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)outer_u12_smem()));
     B200LA_CUDA(cudaFuncSetAttribute(k_outer_u12<TC_FP8, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)outer_u12_smem()));
+    B200LA_CUDA(cudaFuncSetAttribute(k_trsv_refine<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTrInvSmem));
+    B200LA_CUDA(cudaFuncSetAttribute(k_trsv_refine<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTrInvSmem));
+    B200LA_CUDA(cudaFuncSetAttribute(k_invert_diag_blocks128<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTrInvSmem));
+    B200LA_CUDA(cudaFuncSetAttribute(k_invert_diag_blocks128<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTrInvSmem));
     if (dev >= 0 && dev < 64)
         done[dev] = true;
     return B200LA_SUCCESS;
@@ -1059,13 +1063,13 @@ int enqueue_lu_apply(const TA* lu, const int32_t* perm, int n, int nrhs, double*
     B200LA_LAUNCH_CHECK();
     if (nrhs == 1)
     {
-        const int nb = (n + kTvRows - 1) / kTvRows;
+        const int nb = (n + kTrRows - 1) / kTrRows;
         for (int pass = 0; pass < 2; ++pass)
         {
             B200LA_CUDA(cudaMemsetAsync(p.tsync, 0, sizeof(int32_t), s));
             const uint32_t epoch = tv_next_epoch();
             prof_begin(KC_SOLVE, s);
-            k_trsv_blocks<TA><<<nb, kTvThreads, 0, s>>>(lu, n, p.y, n, pass, p.dinv, p.xll, epoch,
+            k_trsv_refine<TA><<<nb, kTrThreads, kTrInvSmem, s>>>(lu, n, p.y, n, pass, p.dinv, p.xll, epoch,
                 reinterpret_cast<int32_t*>(p.tsync), st, kWaitLimitNs);
             prof_end(KC_SOLVE, s);
             B200LA_LAUNCH_CHECK();
@@ -1289,12 +1293,12 @@ int mixed_factor(const double* a, int nn, int nr, int precision, MixedPlan& p, S
     }
     B200LA_LAUNCH_CHECK();
     {
-        const int nbk = (nn + kTvRows - 1) / kTvRows;
+        const int nbk = (nn + kTrRows - 1) / kTrRows;
         prof_begin(KC_SOLVE, s);
         if (use64)
-            k_invert_diag_blocks<double><<<dim3(nbk, 2), kTvRows, 0, s>>>(p.a64, n, nn, p.dinv);
+            k_invert_diag_blocks128<double><<<dim3(nbk, 2), kTrRows, kTrInvSmem, s>>>(p.a64, n, nn, p.dinv);
         else
-            k_invert_diag_blocks<float><<<dim3(nbk, 2), kTvRows, 0, s>>>(p.a32, n, nn, p.dinv);
+            k_invert_diag_blocks128<float><<<dim3(nbk, 2), kTrRows, kTrInvSmem, s>>>(p.a32, n, nn, p.dinv);
         prof_end(KC_SOLVE, s);
         B200LA_LAUNCH_CHECK();
     }

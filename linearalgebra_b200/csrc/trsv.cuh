@@ -346,4 +346,210 @@ __global__ void __launch_bounds__(kTvThreads) k_trsv_blocks(const TA* __restrict
     }
 }
 
+// ---------------------------------------------------------------------------
+// Refinement solves: the same one-launch scheme with 128-row blocks and the
+// diagonal block applied as its inverse by every thread.
+// ---------------------------------------------------------------------------
+constexpr int    kTrRows    = 128;
+constexpr int    kTrThreads = 512;  // 128 rows x 4 quarters of 32 columns
+constexpr int    kTrQ       = kTrRows / (kTrThreads / kTrRows);
+constexpr size_t kTrInvSmem = sizeof(double) * kTrRows * (kTrRows + 1);
+
+// Inverses of the 128 x 128 diagonal blocks of the unit-lower (blockIdx.y 0)
+// and upper (1) triangles of an LU factor, FP64, row-major per block:
+// dinv[2 b + 0] = L_bb^-1, dinv[2 b + 1] = U_bb^-1.  One thread per column of
+// the inverse (substitution on e_j), the triangle in shared memory; a partial
+// last block is padded with the identity.
+template <typename TA>
+__global__ void __launch_bounds__(kTrRows) k_invert_diag_blocks128(const TA* __restrict__ a, int64_t lda, int n,
+    double* __restrict__ dinv)
+{
+    extern __shared__ double tri[];  // [kTrRows][kTrRows + 1]
+    constexpr int LD    = kTrRows + 1;
+    const int     blk   = blockIdx.x;
+    const bool    upper = blockIdx.y == 1;
+    const int     r0    = blk * kTrRows;
+    const int     br    = min(kTrRows, n - r0);
+    const int     j     = threadIdx.x;
+    for (int e = j; e < kTrRows * kTrRows; e += kTrRows)
+    {
+        const int i = e / kTrRows, c = e % kTrRows;
+        double    v = (i == c) ? 1.0 : 0.0;
+        if (i < br && c < br && (upper ? c >= i : c < i))
+        {
+            v = (double)a[(int64_t)(r0 + i) * lda + r0 + c];
+        }
+        tri[i * LD + c] = v;
+    }
+    __syncthreads();
+    double* out = dinv + ((size_t)blk * 2 + (upper ? 1 : 0)) * kTrRows * kTrRows;
+    if (!upper)
+    {
+        for (int i = 0; i < kTrRows; ++i)
+        {
+            double s = (i == j) ? 1.0 : 0.0;
+            for (int p = j; p < i; ++p)
+            {
+                s = fma(-tri[i * LD + p], out[p * kTrRows + j], s);
+            }
+            out[i * kTrRows + j] = i < j ? 0.0 : s;
+        }
+    }
+    else
+    {
+        for (int i = kTrRows - 1; i >= 0; --i)
+        {
+            double s = (i == j) ? 1.0 : 0.0;
+            for (int p = i + 1; p <= j; ++p)
+            {
+                s = fma(-tri[i * LD + p], out[p * kTrRows + j], s);
+            }
+            out[i * kTrRows + j] = i > j ? 0.0 : s / tri[i * LD + i];
+        }
+    }
+}
+
+// x <- T^-1 x for the unit-lower (upper = 0) or upper triangle of the factor
+// `a` (FP32 or FP64 values, FP64 arithmetic), one right-hand side, for the
+// refinement's corrections.  CTA = one 128-row block, claimed by ticket in
+// solve order; thread (r, q) multiplies row r of each solved block's 128 x
+// 128 tile by quarter q of that block's values (the next tile already in
+// registers while it waits for the block's publication, bounded by wait_ns),
+// the quarters are summed, and the block's values are the inverse diagonal
+// block (k_invert_diag_blocks128, staged in shared memory at the start)
+// applied by every thread.  Solved values are published as flagged words
+// (tv_publish layout, indexed by row) with the call's epoch.
+template <typename TA>
+__global__ void __launch_bounds__(kTrThreads, 1) k_trsv_refine(const TA* __restrict__ a, int64_t lda,
+    double* __restrict__ x, int n, int upper, const double* __restrict__ dinv, uint64_t* __restrict__ xll,
+    uint32_t epoch, int32_t* __restrict__ ticket, DeviceStatus* st, uint64_t wait_ns)
+{
+    extern __shared__ double inv[];  // [kTrRows][kTrRows + 1]
+    constexpr int LD = kTrRows + 1;
+    constexpr int NQ = kTrThreads / kTrRows;
+    __shared__ double xs[2][kTrRows];
+    __shared__ double part[kTrRows][NQ + 1];
+    __shared__ double vb[kTrRows];
+    __shared__ int    s_t, s_abort;
+    const int nb  = (n + kTrRows - 1) / kTrRows;
+    const int tid = threadIdx.x;
+    if (tid == 0)
+    {
+        s_t     = atomicAdd(ticket, 1);
+        s_abort = 0;
+    }
+    __syncthreads();
+    const int t = s_t;
+    if (t >= nb)
+    {
+        return;
+    }
+    const int blk = upper ? nb - 1 - t : t;
+    const int r0  = blk * kTrRows;
+    const int br  = min(kTrRows, n - r0);
+    {
+        const double* src = dinv + ((size_t)blk * 2 + (upper ? 1 : 0)) * kTrRows * kTrRows;
+        for (int e = tid; e < kTrRows * kTrRows; e += kTrThreads)
+        {
+            inv[(e / kTrRows) * LD + (e % kTrRows)] = src[e];
+        }
+    }
+    const int r   = tid % kTrRows;
+    const int q   = tid / kTrRows;
+    double    acc = 0.0;
+    TA        an[kTrQ];
+    auto      load_a = [&](int s, TA (&dst)[kTrQ]) {
+        const int jb  = upper ? nb - 1 - s : s;
+        const int c0  = jb * kTrRows + q * kTrQ;
+        const TA* src = a + (int64_t)(r0 + (r < br ? r : 0)) * lda + c0;
+#pragma unroll
+        for (int j = 0; j < kTrQ; ++j)
+        {
+            dst[j] = (r < br && c0 + j < n) ? src[j] : TA(0);
+        }
+    };
+    if (t > 0)
+    {
+        load_a(0, an);
+    }
+    for (int s = 0; s < t; ++s)
+    {
+        const int jb = upper ? nb - 1 - s : s;
+        TA        ac[kTrQ];
+#pragma unroll
+        for (int j = 0; j < kTrQ; ++j)
+        {
+            ac[j] = an[j];
+        }
+        if (tid < kTrRows)
+        {
+            const int cw = min(kTrRows, n - jb * kTrRows);
+            double    xv = 0.0;
+            if (tid < cw)
+            {
+                const uint64_t t0    = global_ns();
+                uint32_t       polls = 0;
+                while (!tv_read(xll, 0, jb * kTrRows + tid, epoch, xv))
+                {
+                    if ((++polls & 255u) == 0 && global_ns() - t0 > wait_ns)
+                    {
+                        raise_error(st, DEV_WAIT_TIMEOUT, 21);
+                        s_abort = 1;
+                        break;
+                    }
+                }
+            }
+            xs[s & 1][tid] = tid < cw ? xv : 0.0;  // double-buffered: read below until the next barrier
+        }
+        __syncthreads();
+        if (s_abort)
+        {
+            return;
+        }
+        if (s + 1 < t)
+        {
+            load_a(s + 1, an);
+        }
+        double bp = 0.0;
+#pragma unroll
+        for (int j = 0; j < kTrQ; ++j)
+        {
+            bp = fma((double)ac[j], xs[s & 1][q * kTrQ + j], bp);
+        }
+        acc += bp;
+    }
+    part[r][q] = acc;
+    __syncthreads();
+    if (tid < kTrRows)
+    {
+        double sum = 0.0;
+#pragma unroll
+        for (int g = 0; g < NQ; ++g)
+        {
+            sum += part[tid][g];
+        }
+        vb[tid] = tid < br ? x[r0 + tid] - sum : 0.0;
+    }
+    __syncthreads();
+    double v = 0.0;
+#pragma unroll 8
+    for (int c = 0; c < kTrQ; ++c)
+    {
+        v = fma(inv[r * LD + q * kTrQ + c], vb[q * kTrQ + c], v);
+    }
+    part[r][q] = v;
+    __syncthreads();
+    if (tid < br)
+    {
+        double sum = 0.0;
+#pragma unroll
+        for (int g = 0; g < NQ; ++g)
+        {
+            sum += part[tid][g];
+        }
+        x[r0 + tid] = sum;
+        tv_publish(xll, 0, r0 + tid, sum, epoch);
+    }
+}
+
 }  // namespace b200la
