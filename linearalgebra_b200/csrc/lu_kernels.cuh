@@ -1004,11 +1004,8 @@ __global__ void __launch_bounds__(kPanelThreads, 1) k_panel_cluster(T* __restric
             if (lane == 0)
             {
                 s_p         = p;
-                piv_loc[jj] = p;
-                if (b == 0)
-                {
-                    pivot[c] = (int64_t)p + 1;
-                }
+                piv_loc[jj] = p;  // pivot[] is written after the last column: a global store
+                                  // here would hold up the next release barrier
             }
         }
         __syncthreads();
@@ -1148,6 +1145,13 @@ __global__ void __launch_bounds__(kPanelThreads, 1) k_panel_cluster(T* __restric
         if (warp == 0)
         {
             build_perm_list(piv_loc, k, w, perm, lane);
+        }
+        else if (warp == 1)
+        {
+            for (int j = lane; j < w; j += 32)
+            {
+                pivot[k + j] = (int64_t)piv_loc[j] + 1;
+            }
         }
     }
 }

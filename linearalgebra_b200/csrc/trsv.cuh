@@ -351,8 +351,7 @@ __global__ void __launch_bounds__(kTvThreads) k_trsv_blocks(const TA* __restrict
 // diagonal block applied as its inverse by every thread.
 // ---------------------------------------------------------------------------
 constexpr int    kTrRows    = 128;
-constexpr int    kTrThreads = 512;  // 128 rows x 4 quarters of 32 columns
-constexpr int    kTrQ       = kTrRows / (kTrThreads / kTrRows);
+constexpr int    kTrThreads = 512;  // 16 warps x 8 rows
 constexpr size_t kTrInvSmem = sizeof(double) * kTrRows * (kTrRows + 1);
 
 // Inverses of the 128 x 128 diagonal blocks of the unit-lower (blockIdx.y 0)
@@ -409,30 +408,75 @@ __global__ void __launch_bounds__(kTrRows) k_invert_diag_blocks128(const TA* __r
     }
 }
 
+// Sums, over the 32 lanes, eight per-lane values v[0..7] (one per row of a
+// warp's 8 rows) in 9 shuffles: the halves exchanged at distance 16, 8, 4
+// carry a row index bit each (4, 2, 1), the last two steps are plain sums.
+// Lane l with (l & 3) == 0 ends with the sum for row
+// 4 ((l >> 4) & 1) + 2 ((l >> 3) & 1) + ((l >> 2) & 1); tr_row gives it.
+__device__ __forceinline__ double tr_reduce8(double (&v)[8], int lane)
+{
+    double h[4];
+    const bool b4 = lane & 16;
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+    {
+        const double send = b4 ? v[j] : v[j + 4];
+        const double keep = b4 ? v[j + 4] : v[j];
+        h[j]              = keep + __shfl_xor_sync(0xffffffffu, send, 16);
+    }
+    double    g[2];
+    const bool b3 = lane & 8;
+#pragma unroll
+    for (int j = 0; j < 2; ++j)
+    {
+        const double send = b3 ? h[j] : h[j + 2];
+        const double keep = b3 ? h[j + 2] : h[j];
+        g[j]              = keep + __shfl_xor_sync(0xffffffffu, send, 8);
+    }
+    const bool   b2   = lane & 4;
+    const double send = b2 ? g[0] : g[1];
+    double       r    = (b2 ? g[1] : g[0]) + __shfl_xor_sync(0xffffffffu, send, 4);
+    r += __shfl_xor_sync(0xffffffffu, r, 2);
+    r += __shfl_xor_sync(0xffffffffu, r, 1);
+    return r;
+}
+
+__device__ __forceinline__ int tr_row(int lane)
+{
+    return 4 * ((lane >> 4) & 1) + 2 * ((lane >> 3) & 1) + ((lane >> 2) & 1);
+}
+
 // x <- T^-1 x for the unit-lower (upper = 0) or upper triangle of the factor
 // `a` (FP32 or FP64 values, FP64 arithmetic), one right-hand side, for the
 // refinement's corrections.  CTA = one 128-row block, claimed by ticket in
-// solve order; thread (r, q) multiplies row r of each solved block's 128 x
-// 128 tile by quarter q of that block's values (the next tile already in
-// registers while it waits for the block's publication, bounded by wait_ns),
-// the quarters are summed, and the block's values are the inverse diagonal
-// block (k_invert_diag_blocks128, staged in shared memory at the start)
-// applied by every thread.  Solved values are published as flagged words
+// solve order.  Warp w owns rows 8 w .. 8 w + 7 of the block and reads them
+// row by row, coalesced: lane l multiplies columns 4 l .. 4 l + 3 of each
+// solved block's tile by that block's values and keeps one partial sum per
+// row; the partial sums are reduced across the warp once, after the last
+// tile.  The tile of the block being waited for is already loaded (FP32: the
+// next one too) when the block's publication is polled (bounded by wait_ns).
+// The block's own values are the inverse diagonal block
+// (k_invert_diag_blocks128, staged in shared memory at the start) applied in
+// the same warp-per-row layout.  Solved values are published as flagged words
 // (tv_publish layout, indexed by row) with the call's epoch.
 template <typename TA>
 __global__ void __launch_bounds__(kTrThreads, 1) k_trsv_refine(const TA* __restrict__ a, int64_t lda,
     double* __restrict__ x, int n, int upper, const double* __restrict__ dinv, uint64_t* __restrict__ xll,
     uint32_t epoch, int32_t* __restrict__ ticket, DeviceStatus* st, uint64_t wait_ns)
 {
-    extern __shared__ double inv[];  // [kTrRows][kTrRows + 1]
-    constexpr int LD = kTrRows + 1;
-    constexpr int NQ = kTrThreads / kTrRows;
-    __shared__ double xs[2][kTrRows];
-    __shared__ double part[kTrRows][NQ + 1];
-    __shared__ double vb[kTrRows];
-    __shared__ int    s_t, s_abort;
-    const int nb  = (n + kTrRows - 1) / kTrRows;
-    const int tid = threadIdx.x;
+    extern __shared__ __align__(16) double inv[];  // [kTrRows][kTrRows]
+    constexpr int  NW   = kTrThreads / 32;
+    constexpr int  RPW  = kTrRows / NW;  // 8 rows per warp
+    constexpr int  CPL  = kTrRows / 32;  // 4 columns per lane
+    constexpr bool PREF = sizeof(TA) == 4;
+    static_assert(RPW == 8 && CPL == 4, "warp-per-row layout");
+    __shared__ __align__(16) double xs[2][kTrRows];
+    __shared__ __align__(16) double vb[kTrRows];
+    __shared__ int                  s_t, s_abort;
+    const int nb   = (n + kTrRows - 1) / kTrRows;
+    const int tid  = threadIdx.x;
+    const int lane = tid & 31;
+    const int w    = tid >> 5;
     if (tid == 0)
     {
         s_t     = atomicAdd(ticket, 1);
@@ -448,38 +492,82 @@ __global__ void __launch_bounds__(kTrThreads, 1) k_trsv_refine(const TA* __restr
     const int r0  = blk * kTrRows;
     const int br  = min(kTrRows, n - r0);
     {
-        const double* src = dinv + ((size_t)blk * 2 + (upper ? 1 : 0)) * kTrRows * kTrRows;
-        for (int e = tid; e < kTrRows * kTrRows; e += kTrThreads)
+        const double2* src =
+            reinterpret_cast<const double2*>(dinv + ((size_t)blk * 2 + (upper ? 1 : 0)) * kTrRows * kTrRows);
+        double2* dst = reinterpret_cast<double2*>(inv);
+        for (int e = tid; e < kTrRows * kTrRows / 2; e += kTrThreads)
         {
-            inv[(e / kTrRows) * LD + (e % kTrRows)] = src[e];
+            dst[e] = src[e];
         }
     }
-    const int r   = tid % kTrRows;
-    const int q   = tid / kTrRows;
-    double    acc = 0.0;
-    TA        an[kTrQ];
-    auto      load_a = [&](int s, TA (&dst)[kTrQ]) {
-        const int jb  = upper ? nb - 1 - s : s;
-        const int c0  = jb * kTrRows + q * kTrQ;
-        const TA* src = a + (int64_t)(r0 + (r < br ? r : 0)) * lda + c0;
+    // vector loads need every row start aligned to CPL elements
+    const bool vec = (lda % CPL) == 0 && (reinterpret_cast<uintptr_t>(a) % (CPL * sizeof(TA))) == 0;
+    auto load_tile = [&](int s, TA (&dst)[RPW][CPL]) {
+        const int jb = upper ? nb - 1 - s : s;
+        const int c  = jb * kTrRows + lane * CPL;
 #pragma unroll
-        for (int j = 0; j < kTrQ; ++j)
+        for (int i = 0; i < RPW; ++i)
         {
-            dst[j] = (r < br && c0 + j < n) ? src[j] : TA(0);
+            const int row = w * RPW + i;
+            const TA* src = a + (int64_t)(r0 + (row < br ? row : 0)) * lda + c;
+            if (row < br && vec && c + CPL <= n)
+            {
+                if constexpr (sizeof(TA) == 4)
+                {
+                    const float4 q = __ldg(reinterpret_cast<const float4*>(src));
+                    dst[i][0] = q.x, dst[i][1] = q.y, dst[i][2] = q.z, dst[i][3] = q.w;
+                }
+                else
+                {
+                    const double2 q0 = __ldg(reinterpret_cast<const double2*>(src));
+                    const double2 q1 = __ldg(reinterpret_cast<const double2*>(src) + 1);
+                    dst[i][0] = q0.x, dst[i][1] = q0.y, dst[i][2] = q1.x, dst[i][3] = q1.y;
+                }
+            }
+            else
+            {
+#pragma unroll
+                for (int j = 0; j < CPL; ++j)
+                {
+                    dst[i][j] = (row < br && c + j < n) ? src[j] : TA(0);
+                }
+            }
         }
     };
-    if (t > 0)
+    double acc[RPW];
+#pragma unroll
+    for (int i = 0; i < RPW; ++i)
     {
-        load_a(0, an);
+        acc[i] = 0.0;
+    }
+    TA cur[RPW][CPL];
+    TA nxt[RPW][CPL];
+    if (PREF && t > 0)
+    {
+        load_tile(0, nxt);
     }
     for (int s = 0; s < t; ++s)
     {
         const int jb = upper ? nb - 1 - s : s;
-        TA        ac[kTrQ];
-#pragma unroll
-        for (int j = 0; j < kTrQ; ++j)
+        if constexpr (PREF)
         {
-            ac[j] = an[j];
+#pragma unroll
+            for (int i = 0; i < RPW; ++i)
+            {
+#pragma unroll
+                for (int j = 0; j < CPL; ++j)
+                {
+                    cur[i][j] = nxt[i][j];
+                }
+            }
+            if (s + 1 < t)
+            {
+                load_tile(s + 1, nxt);
+            }
+        }
+        else
+        {
+            load_tile(s, cur);
         }
         if (tid < kTrRows)
         {
@@ -506,49 +594,43 @@ __global__ void __launch_bounds__(kTrThreads, 1) k_trsv_refine(const TA* __restr
         {
             return;
         }
-        if (s + 1 < t)
-        {
-            load_a(s + 1, an);
-        }
-        double bp = 0.0;
+        const double2 x01 = reinterpret_cast<const double2*>(xs[s & 1])[lane * 2];
+        const double2 x23 = reinterpret_cast<const double2*>(xs[s & 1])[lane * 2 + 1];
 #pragma unroll
-        for (int j = 0; j < kTrQ; ++j)
+        for (int i = 0; i < RPW; ++i)
         {
-            bp = fma((double)ac[j], xs[s & 1][q * kTrQ + j], bp);
+            acc[i] = fma((double)cur[i][0], x01.x, acc[i]);
+            acc[i] = fma((double)cur[i][1], x01.y, acc[i]);
+            acc[i] = fma((double)cur[i][2], x23.x, acc[i]);
+            acc[i] = fma((double)cur[i][3], x23.y, acc[i]);
         }
-        acc += bp;
     }
-    part[r][q] = acc;
-    __syncthreads();
-    if (tid < kTrRows)
+    const int my = w * RPW + tr_row(lane);  // the row whose sums this lane ends with (lane % 4 == 0)
     {
-        double sum = 0.0;
-#pragma unroll
-        for (int g = 0; g < NQ; ++g)
+        const double sum = tr_reduce8(acc, lane);
+        if ((lane & 3) == 0)
         {
-            sum += part[tid][g];
+            vb[my] = my < br ? x[r0 + my] - sum : 0.0;
         }
-        vb[tid] = tid < br ? x[r0 + tid] - sum : 0.0;
     }
     __syncthreads();
-    double v = 0.0;
-#pragma unroll 8
-    for (int c = 0; c < kTrQ; ++c)
-    {
-        v = fma(inv[r * LD + q * kTrQ + c], vb[q * kTrQ + c], v);
-    }
-    part[r][q] = v;
-    __syncthreads();
-    if (tid < br)
-    {
-        double sum = 0.0;
+    const double2 v01 = reinterpret_cast<const double2*>(vb)[lane * 2];
+    const double2 v23 = reinterpret_cast<const double2*>(vb)[lane * 2 + 1];
 #pragma unroll
-        for (int g = 0; g < NQ; ++g)
-        {
-            sum += part[tid][g];
-        }
-        x[r0 + tid] = sum;
-        tv_publish(xll, 0, r0 + tid, sum, epoch);
+    for (int i = 0; i < RPW; ++i)
+    {
+        const double2 m01 = reinterpret_cast<const double2*>(inv + (w * RPW + i) * kTrRows)[lane * 2];
+        const double2 m23 = reinterpret_cast<const double2*>(inv + (w * RPW + i) * kTrRows)[lane * 2 + 1];
+        double        v   = m01.x * v01.x;
+        v                 = fma(m01.y, v01.y, v);
+        v                 = fma(m23.x, v23.x, v);
+        acc[i]            = fma(m23.y, v23.y, v);
+    }
+    const double sum = tr_reduce8(acc, lane);
+    if ((lane & 3) == 0 && my < br)
+    {
+        x[r0 + my] = sum;
+        tv_publish(xll, 0, r0 + my, sum, epoch);
     }
 }
 
