@@ -8,27 +8,35 @@
 // bucket, and every other group takes one more system; each group then solves
 // its system with its own named barrier, and the CTA meets again.  Per
 // system:
-//   * A (FP64, global) is copied into the factor buffer in the
+//   * A (FP64, global) is copied into the group's factor scratch in the
 //     factorization type T (float: FP32 factors + FP64 refinement; double:
-//     plain FP64 LU), with ||A||_inf on the way;
-//   * blocked right-looking LU with partial pivoting, panel width NB:
-//       - the panel (all remaining rows x NB columns) is factored in shared
-//         memory: per column a pivot search (integer keys, redux.sync), the
-//         row swap inside the panel and the rank-1 update with the next
-//         column's pivot search fused into it;
-//       - the panel's interchanges are composed into one permutation of the
-//         rows they touch and applied to the other columns as one gather
-//         (staged in shared memory) and one scatter;
-//       - U12 = L11^-1 A12, one thread per column, in shared memory;
+//     plain FP64 LU), row stride padded to 16 bytes, with ||A||_inf on the
+//     way;
+//   * blocked right-looking LU with partial pivoting, panel width NB.  Rows
+//     never move in the scratch: a logical-to-physical row map takes every
+//     interchange, so a panel's interchanges cost one map update instead of a
+//     gather and scatter of whole rows, and the map is the solve's row
+//     permutation at the end;
+//       - the panel (all remaining rows x NB columns) is factored in
+//         registers (RPT rows per thread, rows staying in their thread with
+//         their current position in a register, when the rows fit) or in
+//         shared memory: per column a pivot search (integer keys,
+//         redux.sync), the pivot row posted through shared memory, and the
+//         rank-1 update;
+//       - U12 = L11^-1 A12, one thread per column;
 //       - A22 -= L21 U12 with 8 x 8 (FP32) or 4 x 8 (FP64) register tiles per
-//         thread, L21 (transposed) and U12 from shared memory;
-//   * the solve applies the factors in FP64: 32-row blocks, the diagonal
-//     block in one warp's registers (rows by lane, substitution with
-//     shuffles), the other rows updated by every thread; then FP64 refinement
-//     r = b - A x, d = U^-1 L^-1 P r, x += d until the normwise backward
-//     error ||r|| / (||A|| ||x|| + ||b||) <= tol, the refinement stalls (less
-//     than a factor 2 gained per correction after the first) or max_iter
-//     corrections.
+//         thread: the tile of A22 is loaded (16-byte vectors) before the
+//         product, L21 (transposed) and U12 come from shared memory in
+//         16-byte vectors without bank conflicts;
+//   * the solve applies the factors in FP64: 32-row blocks in solve order;
+//     for each block the products with the solved values are dot products
+//     over whole factor rows read by G / 32 threads per row (16-byte
+//     vectors), the diagonal block is staged in shared memory and solved in
+//     one warp's registers (rows by lane, substitution with shuffles); then
+//     FP64 refinement r = b - A x, d = U^-1 L^-1 P r, x += d until the
+//     normwise backward error ||r|| / (||A|| ||x|| + ||b||) <= tol, the
+//     refinement stalls (less than a factor 2 gained per correction after
+//     the first) or max_iter corrections.
 // With FP32 factors a second launch with FP64 factors takes only the
 // systems whose refinement did not converge (ill-conditioned ones); it
 // skips every other system at the cost of one queue step.
@@ -42,6 +50,16 @@
 
 #include "common.cuh"
 
+// Phase hook: B200LA_BPHASE(i) marks the end of phase i of a system's solve
+// (nothing by default; a timing harness may define it before including this
+// file).
+#ifndef B200LA_BPHASE
+#define B200LA_BPHASE(i) \
+    do                   \
+    {                    \
+    } while (0)
+#endif
+
 namespace b200la
 {
 namespace
@@ -50,6 +68,11 @@ constexpr int kBT       = 256;  // threads per CTA
 constexpr int kBMaxN    = 512;
 constexpr int kBBuckets = 8;    // order buckets of 64
 constexpr int kBSolveNB = 32;   // rows per block of the triangular solves
+constexpr int kBDgLd    = kBSolveNB + 1;
+// factor scratch: one slot of kBScratch bytes per CTA (split between the
+// CTA's groups), at most kBMaxCTAs slots
+constexpr size_t kBScratch = (size_t)kBMaxN * kBMaxN * sizeof(double);
+constexpr int    kBMaxCTAs = 192;
 // status of a system whose refinement stalled or ran out of corrections; the
 // FP64 pass picks these up.  Systems finished by that pass get 1000 + k.
 constexpr int32_t kNotConverged = -1000000;
@@ -59,14 +82,14 @@ template <typename T> struct BatchTraits;
 template <> struct BatchTraits<float>
 {
     static constexpr int kMaxNB = 32;
-    static constexpr int TM     = 8;  // rows of a thread's update tile
-    static constexpr int TN     = 8;  // columns
+    static constexpr int kMinNB = 16;
+    static constexpr int TM     = 8;  // rows of a thread's update tile (8 x 8)
 };
 template <> struct BatchTraits<double>
 {
     static constexpr int kMaxNB = 16;
-    static constexpr int TM     = 4;
-    static constexpr int TN     = 8;
+    static constexpr int kMinNB = 8;
+    static constexpr int TM     = 4;  // 4 x 8
 };
 
 // A bucket's table entry: bits 0-7 the panel width NB, bits 8-15 the
@@ -77,37 +100,73 @@ __host__ __device__ inline int entry_g(int e)
     const int g = ((e >> 8) & 0xff) * 32;
     return g == 64 || g == 128 ? g : kBT;
 }
+// The panel widths the kernel is built for: kMaxNB or kMinNB.
+template <typename T> __host__ __device__ inline bool nb_supported(int nb)
+{
+    return nb == BatchTraits<T>::kMaxNB || nb == BatchTraits<T>::kMinNB;
+}
 
 __host__ __device__ inline int group_np(int n) { return (n + 7) / 8 * 8 + 8; }
+// Row stride of the factor scratch: n rounded up to 16 bytes.
+template <typename T> __host__ __device__ inline int bat_ld(int n)
+{
+    constexpr int v = 16 / (int)sizeof(T);
+    return (n + v - 1) / v * v;
+}
 
-// Shared-memory slice of one group solving a system of order n with panel
-// width nb (the same function sizes and carves).
+// Rows per thread of the register panel for order n and G threads: 2 or 4
+// (4 only while RPT x NB stays within 64 FP32 / 32 FP64 values), 0 if the
+// panel is factored in shared memory.
+template <typename T> __host__ __device__ inline int panel_rpt(int n, int nb, int G)
+{
+    if (n <= 2 * G)
+        return 2;
+    if (n <= 4 * G && 4 * nb * (int)sizeof(T) <= 256)
+        return 4;
+    return 0;
+}
+
+// Shared-memory slice of one group of G threads solving a system of order n
+// with panel width nb (the same function sizes and carves).
 struct GroupSmem
 {
-    size_t P, LT, U, y, r, x, sigma, list, piv, perm, red, end;
+    size_t P, LT, U, y, r, x, dg, dpart, sigma, list, rowp, red, end;
 };
-template <typename T> __host__ __device__ inline GroupSmem group_layout(int n, int nb)
+template <typename T> __host__ __device__ inline GroupSmem group_layout(int n, int nb, int G)
 {
     auto up = [](size_t v) { return (v + 15) / 16 * 16; };
-    const int np = group_np(n);              // padded rows of LT and U (the update tiles read past n)
-    const int nv = n > 16 ? n : 16;          // FP64 vectors (also the group's reductions: 2 per warp)
+    const int np = group_np(n);      // padded rows of LT and U (the update tiles read past n)
+    const int nv = n > 16 ? n : 16;  // FP64 vectors (also the group's reductions: 2 per warp)
+    // the register panel keeps only L11 in P, the shared-memory panel all rows
+    const int prow = panel_rpt<T>(n, nb, G) != 0 ? nb : n;
     GroupSmem g;
-    g.P     = 0;                                                   // T[n][nb + 1]: the panel
-    g.LT    = up(g.P + sizeof(T) * (size_t)n * (nb + 1));          // T[nb][np]: L21 transposed / staging
-    g.U     = up(g.LT + sizeof(T) * (size_t)nb * np);              // T[nb][np]: U12
-    g.y     = up(g.U + sizeof(T) * (size_t)nb * np);               // double[nv]
-    g.r     = up(g.y + sizeof(double) * nv);                       // double[nv]
-    g.x     = up(g.r + sizeof(double) * nv);                       // double[nv]
-    g.sigma = up(g.x + sizeof(double) * nv);                       // int[n]: composed panel permutation
-    g.list  = up(g.sigma + sizeof(int) * n);                       // int[2][2 nb]: rows it moves
-    g.piv   = up(g.list + sizeof(int) * 4 * nb);                   // int[n]: pivot row of each step
-    g.perm  = up(g.piv + sizeof(int) * n);                         // int[n]: final row permutation
-    g.red   = up(g.perm + sizeof(int) * n);                        // 8 x (u64 key, int row) + flags
+    g.P     = 0;                                              // T[prow][nb + 1]: the panel
+    g.LT    = up(g.P + sizeof(T) * (size_t)prow * (nb + 1));  // T[nb][np]: L21 transposed
+    g.U     = up(g.LT + sizeof(T) * (size_t)nb * np);      // T[nb][np]: U12
+    g.y     = up(g.U + sizeof(T) * (size_t)nb * np);       // double[nv]
+    g.r     = up(g.y + sizeof(double) * nv);               // double[nv]
+    g.x     = up(g.r + sizeof(double) * nv);               // double[nv]
+    g.dg    = up(g.x + sizeof(double) * nv);               // T[32][33]: diagonal block / posted rows
+    g.dpart = up(g.dg + sizeof(T) * kBSolveNB * kBDgLd);   // double[32]: the block's products
+    g.sigma = up(g.dpart + sizeof(double) * kBSolveNB);    // int[n]: the panel's row order
+    g.list  = up(g.sigma + sizeof(int) * n);               // int[4 nb]: moved rows, their old map
+    g.rowp  = up(g.list + sizeof(int) * 4 * nb);           // int[n]: logical -> physical row
+    g.red   = up(g.rowp + sizeof(int) * n);                // 8 x (u64 key, int row) + flags
     g.end   = up(g.red + 8 * 8 + 8 * 4 + 64);
     return g;
 }
 
 constexpr size_t kBatchedSmem = 227 * 1024 - 1024;  // dynamic shared memory per CTA
+
+__host__ __device__ inline size_t group_smem_bytes(int G) { return kBatchedSmem / (kBT / G) / 16 * 16; }
+__host__ __device__ inline size_t group_scratch_bytes(int G) { return kBScratch / (kBT / G); }
+
+// Whether a system of order n fits a group of G threads with panel width nb.
+template <typename T> __host__ __device__ inline bool group_fits(int n, int nb, int G)
+{
+    return group_layout<T>(n, nb, G).end <= group_smem_bytes(G) &&
+           (size_t)n * bat_ld<T>(n) * sizeof(T) <= group_scratch_bytes(G);
+}
 
 __device__ __forceinline__ void group_sync(int id, int threads)
 {
@@ -153,49 +212,156 @@ template <typename K> __device__ __forceinline__ void bwarp_best(K& key, int& ro
     }
 }
 
+// 16-byte vector <-> elements
+template <typename T> __device__ __forceinline__ void vload(const T* p, T* e)
+{
+    if constexpr (sizeof(T) == 4)
+    {
+        const float4 v = *reinterpret_cast<const float4*>(p);
+        e[0] = v.x, e[1] = v.y, e[2] = v.z, e[3] = v.w;
+    }
+    else
+    {
+        const double2 v = *reinterpret_cast<const double2*>(p);
+        e[0] = v.x, e[1] = v.y;
+    }
+}
+template <typename T> __device__ __forceinline__ void vstore(T* p, const T* e)
+{
+    if constexpr (sizeof(T) == 4)
+    {
+        *reinterpret_cast<float4*>(p) = make_float4(e[0], e[1], e[2], e[3]);
+    }
+    else
+    {
+        *reinterpret_cast<double2*>(p) = make_double2(e[0], e[1]);
+    }
+}
+
 // One group's state for one system.
 template <typename T> struct Sys
 {
     int      n, nb, G, gt, bar;  // order, panel width, threads, this thread's index, barrier id
-    T*       f;                  // factor buffer (global), n x n row-major
+    int      ld;                 // row stride of f
+    T*       f;                  // factor scratch (global), n rows of stride ld, rows in physical order
     T*       P;                  // [n][nb + 1]
     T*       LT;                 // [nb][np]
     T*       U;                  // [nb][np]
     int      np;
     double * y, *r, *x;
-    int *    sigma, *list, *piv, *perm;
+    T*       dg;     // [32][33]
+    double*  dpart;  // [32]
+    int *    sigma, *list, *rowp;
     unsigned long long* red_key;
     int*                red_row;
-    int*                flags;  // [0] first zero pivot (-1 none), [1] list count, [2] pivot of the column
+    int*                flags;  // [0] first zero pivot (-1 none), [1] list count
 
     __device__ void sync() const { group_sync(bar, G); }
+    __device__ T*   row(int logical) const { return f + (size_t)rowp[logical] * ld; }
 };
 
 // y <- T^-1 y for the unit-lower (upper = false) or upper triangle of the
-// factor (FP64 arithmetic).  32-row blocks in solve order: warp 0 of the group
-// holds the diagonal block in registers (row b0 + lane) and substitutes with
-// shuffles; then every thread updates its rows not yet solved.
+// factor (FP64 arithmetic).  32-row blocks in solve order.  Per block: the
+// block's rows times the values already solved, G / 32 threads per row, each
+// on 16-byte vectors of the row (the row's diagonal block staged in shared
+// memory on the way), summed with shuffles; then warp 0 holds the diagonal
+// block in registers (row b0 + lane) and substitutes with shuffles.
 template <typename T> __device__ void bat_trsv(const Sys<T>& s, bool upper)
 {
-    const int lane = s.gt & 31, warp = s.gt >> 5;
-    const int n    = s.n;
-    const int nblk = (n + kBSolveNB - 1) / kBSolveNB;
-    double*   y    = s.y;
+    constexpr int VN   = 16 / (int)sizeof(T);
+    const int     lane = s.gt & 31, warp = s.gt >> 5;
+    const int     n    = s.n;
+    const int     nblk = (n + kBSolveNB - 1) / kBSolveNB;
+    const int     tpr  = s.G >> 5;  // threads per block row: 8, 4 or 2 (consecutive lanes)
+    const int     ri   = s.gt / tpr;
+    const int     ch   = s.gt - ri * tpr;
+    double*       y    = s.y;
     for (int bi = 0; bi < nblk; ++bi)
     {
-        const int b  = upper ? nblk - 1 - bi : bi;
-        const int b0 = b * kBSolveNB;
-        const int bw = min(kBSolveNB, n - b0);
+        const int b   = upper ? nblk - 1 - bi : bi;
+        const int b0  = b * kBSolveNB;
+        const int bw  = min(kBSolveNB, n - b0);
+        const int jlo = upper ? b0 + bw : 0;  // the solved columns [jlo, jhi)
+        const int jhi = upper ? n : b0;
+        double    acc = 0.0;
+        if (ri < bw)
+        {
+            const T* row = s.row(b0 + ri);
+            for (int v = ch; v < kBSolveNB / VN; v += tpr)
+            {
+                const int c = b0 + v * VN;
+                T         e[VN];
+                if (c + VN <= n)
+                {
+                    vload(row + c, e);
+                }
+                else
+                {
+#pragma unroll
+                    for (int j = 0; j < VN; ++j)
+                        e[j] = c + j < n ? row[c + j] : T(0);
+                }
+#pragma unroll
+                for (int j = 0; j < VN; ++j)
+                    s.dg[ri * kBDgLd + v * VN + j] = e[j];
+            }
+            // whole vectors in batches of 8 per thread, every load of a batch
+            // issued before the first product; then the ragged tail
+            const int nvec = (jhi - jlo) / VN;
+            for (int m0 = ch; m0 < nvec; m0 += 8 * tpr)
+            {
+                T e[8][VN];
+#pragma unroll
+                for (int u = 0; u < 8; ++u)
+                {
+                    const int m = m0 + u * tpr;
+                    if (m < nvec)
+                    {
+                        vload(row + jlo + m * VN, e[u]);
+                    }
+                    else
+                    {
+#pragma unroll
+                        for (int j = 0; j < VN; ++j)
+                            e[u][j] = T(0);
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < 8; ++u)
+                {
+                    const int m = m0 + u * tpr;
+                    if (m < nvec)
+                    {
+#pragma unroll
+                        for (int j = 0; j < VN; ++j)
+                            acc = fma((double)e[u][j], y[jlo + m * VN + j], acc);
+                    }
+                }
+            }
+            if (ch == 0)
+            {
+                for (int c = jlo + nvec * VN; c < jhi; ++c)
+                    acc = fma((double)row[c], y[c], acc);
+            }
+        }
+        for (int off = tpr >> 1; off > 0; off >>= 1)
+        {
+            acc += __shfl_xor_sync(0xffffffffu, acc, off);
+        }
+        if (ch == 0 && ri < bw)
+        {
+            s.dpart[ri] = acc;
+        }
+        s.sync();
         if (warp == 0)
         {
             double a[kBSolveNB];
-            const T* row = s.f + (size_t)(b0 + (lane < bw ? lane : 0)) * n + b0;
 #pragma unroll
             for (int j = 0; j < kBSolveNB; ++j)
             {
-                a[j] = (lane < bw && j < bw) ? (double)row[j] : 0.0;
+                a[j] = (lane < bw && j < bw) ? (double)s.dg[lane * kBDgLd + j] : 0.0;
             }
-            double v = lane < bw ? y[b0 + lane] : 0.0;
+            double v = lane < bw ? y[b0 + lane] - s.dpart[lane] : 0.0;
             if (!upper)
             {
 #pragma unroll
@@ -231,100 +397,117 @@ template <typename T> __device__ void bat_trsv(const Sys<T>& s, bool upper)
             }
         }
         s.sync();
-        for (int i = s.gt; i < n; i += s.G)
+    }
+}
+
+// The rows the panel moved (sigma[r] != r: new local row r is old local row
+// sigma[r]) take their new physical rows in the map: rowp[k + r] <-
+// rowp[k + sigma[r]].  At most 2 nb rows move.  Ends with a group barrier.
+template <typename T> __device__ void remap_rows(const Sys<T>& s, int k, int R)
+{
+    const int lane = s.gt & 31, warp = s.gt >> 5;
+    int*      dst  = s.list;
+    int*      old  = s.list + 2 * s.nb;
+    if (warp == 0)
+    {
+        int cnt = 0;
+        for (int r0 = 0; r0 < R; r0 += 32)
         {
-            if (upper ? i < b0 : i >= b0 + bw)
+            const int      r    = r0 + lane;
+            const bool     mv   = r < R && s.sigma[r] != r;
+            const unsigned bits = __ballot_sync(0xffffffffu, mv);
+            if (mv)
             {
-                const T* row = s.f + (size_t)i * n + b0;
-                double   acc = 0.0;
-#pragma unroll 8
-                for (int j = 0; j < bw; ++j)
+                const int q = cnt + __popc(bits & ((1u << lane) - 1u));
+                dst[q]      = r;
+                old[q]      = s.rowp[k + s.sigma[r]];
+            }
+            cnt += __popc(bits);
+        }
+        __syncwarp();
+        for (int q = lane; q < cnt; q += 32)
+        {
+            s.rowp[k + dst[q]] = old[q];
+        }
+    }
+    s.sync();
+}
+
+// Panel [k, k + w) x rows [k, n) in registers.  Rows never leave their
+// thread: thread gt owns the panel's local rows gt + q G (q < RPT) and keeps
+// each row's current position (the row order that partial pivoting's
+// interchanges give, ties going to the lower position) in a register.  Per
+// column: the pivot search over the rows at positions >= jj (redux.sync per
+// warp, then over the warps), the pivot row posted to shared memory, and the
+// update of every row not yet a pivot.  The column loop is not unrolled (the
+// code of 32 unrolled columns outgrows the instruction cache): every row's
+// registers rotate left by one per column, so the active column is always
+// register 0 and the column just finished (a multiplier, or the pivot row's
+// own value) moves to the end; after NB rotations each row is back in
+// column order: multipliers, then (for a pivot row) its row of U.
+// On return: the map is updated, the factor rows are written back, P holds
+// L11 (positions < w) and LT holds L21^T.
+template <typename T, int NB, int RPT> __device__ void panel_regs(const Sys<T>& s, int k, int w)
+{
+    using K            = typename BKey<T>::type;
+    constexpr int VN   = 16 / (int)sizeof(T);
+    const int     n    = s.n;
+    const int     R    = n - k;
+    const int     lane = s.gt & 31, warp = s.gt >> 5, warps = s.G >> 5;
+    const int     ldp  = s.nb + 1;
+    T*            urow = s.dg;  // the pivot row, active column first
+    T             v[RPT][NB];
+    int           pos[RPT];
+    bool          live[RPT];    // a row of the panel that is not yet a pivot
+#pragma unroll
+    for (int q = 0; q < RPT; ++q)
+    {
+        const int r = s.gt + q * s.G;
+        pos[q]      = r;
+        live[q]     = r < R;
+        if (r < R)
+        {
+            const T* src = s.row(k + r) + k;
+            if (w == NB)
+            {
+#pragma unroll
+                for (int c = 0; c < NB; c += VN)
+                    vload(src + c, &v[q][c]);
+            }
+            else
+            {
+#pragma unroll
+                for (int c = 0; c < NB; ++c)
+                    v[q][c] = c < w ? src[c] : T(0);
+            }
+        }
+        else
+        {
+#pragma unroll
+            for (int c = 0; c < NB; ++c)
+                v[q][c] = T(0);
+        }
+    }
+#pragma unroll 1
+    for (int jj = 0; jj < NB; ++jj)
+    {
+        if (jj < w)
+        {
+            K   ck = 0;
+            int cr = INT_MAX;
+#pragma unroll
+            for (int q = 0; q < RPT; ++q)
+            {
+                if (live[q])
                 {
-                    acc = fma((double)row[j], y[b0 + j], acc);
+                    const K key = bkey(v[q][0], pos[q] == jj);
+                    if (key > ck || (key == ck && pos[q] < cr))
+                    {
+                        ck = key;
+                        cr = pos[q];
+                    }
                 }
-                y[i] -= acc;
             }
-        }
-        s.sync();
-    }
-}
-
-// The panel's interchanges (sigma: new row r of the block [k, n) is old row
-// sigma[r]) on columns [c0, c1) of the factor, for the `cnt` rows in the
-// list: values gathered into the LT buffer (cnt x 32 columns at a time),
-// then scattered.
-template <typename T> __device__ void apply_interchanges(const Sys<T>& s, int k, int cnt, int c0, int c1)
-{
-    const int* dst = s.list;
-    const int* src = s.list + 2 * s.nb;
-    // staging in the LT and U buffers (2 nb x np elements; cnt <= np rows of
-    // 2 nb columns per round)
-    T*        stg = s.LT;
-    const int cwp = 2 * s.nb;
-    for (int cb = c0; cb < c1; cb += cwp)
-    {
-        const int cw = min(cwp, c1 - cb);
-        for (int e = s.gt; e < cnt * cwp; e += s.G)
-        {
-            const int q = e / cwp, c = e - q * cwp;
-            if (c < cw)
-            {
-                stg[e] = s.f[(size_t)(k + src[q]) * s.n + cb + c];
-            }
-        }
-        s.sync();
-        for (int e = s.gt; e < cnt * cwp; e += s.G)
-        {
-            const int q = e / cwp, c = e - q * cwp;
-            if (c < cw)
-            {
-                s.f[(size_t)(k + dst[q]) * s.n + cb + c] = stg[e];
-            }
-        }
-        s.sync();
-    }
-}
-
-template <typename T> __device__ void lu_factor(const Sys<T>& s)
-{
-    using K             = typename BKey<T>::type;
-    constexpr int TM    = BatchTraits<T>::TM;
-    constexpr int TN    = BatchTraits<T>::TN;
-    const int     n     = s.n;
-    const int     lane  = s.gt & 31;
-    const int     warp  = s.gt >> 5;
-    const int     warps = s.G >> 5;
-    const int     ldp   = s.nb + 1;
-    for (int k = 0; k < n; k += s.nb)
-    {
-        const int w    = min(s.nb, n - k);
-        const int R    = n - k;
-        const int rest = R - w;
-        // ---- the panel into shared memory
-        for (int e = s.gt; e < R * w; e += s.G)
-        {
-            const int r = e / w, c = e - r * w;
-            s.P[r * ldp + c] = s.f[(size_t)(k + r) * n + k + c];
-        }
-        for (int r = s.gt; r < R; r += s.G)
-        {
-            s.sigma[r] = r;
-        }
-        s.sync();
-        // ---- factor it: per column a pivot search, the swap, the update
-        K   ck = 0;
-        int cr = INT_MAX;
-        for (int r = s.gt; r < R; r += s.G)
-        {
-            const K key = bkey(s.P[r * ldp], r == 0);
-            if (key > ck)
-            {
-                ck = key;
-                cr = r;
-            }
-        }
-        for (int jj = 0; jj < w; ++jj)
-        {
             bwarp_best(ck, cr);
             if (lane == 0)
             {
@@ -332,196 +515,457 @@ template <typename T> __device__ void lu_factor(const Sys<T>& s)
                 s.red_row[warp] = cr;
             }
             s.sync();
-            K   pk = 0;
-            int p  = INT_MAX;
-            for (int q = 0; q < warps; ++q)
+            K   pk = lane < warps ? (K)s.red_key[lane] : K(0);
+            int p  = lane < warps ? s.red_row[lane] : INT_MAX;
+            bwarp_best(pk, p);
+            // position jj holds a live row, so p is a position of the panel
+#pragma unroll
+            for (int q = 0; q < RPT; ++q)
             {
-                const K   kq = (K)s.red_key[q];
-                const int rq = s.red_row[q];
-                if (kq > pk || (kq == pk && rq < p))
+                if (live[q] && pos[q] == p)
                 {
-                    pk = kq;
-                    p  = rq;
+#pragma unroll
+                    for (int c = 0; c < NB; ++c)
+                        urow[c] = v[q][c];
                 }
-            }
-            if (p != jj)
-            {
-                for (int c = s.gt; c < w; c += s.G)
-                {
-                    const T t         = s.P[jj * ldp + c];
-                    s.P[jj * ldp + c] = s.P[p * ldp + c];
-                    s.P[p * ldp + c]  = t;
-                }
-            }
-            if (s.gt == 0)
-            {
-                s.piv[k + jj] = k + p;
-                const int t   = s.sigma[jj];
-                s.sigma[jj]   = s.sigma[p];
-                s.sigma[p]    = t;
             }
             s.sync();
-            const T d = s.P[jj * ldp + jj];
-            if (d == T(0))
+            const T d = urow[0];
+            if (d == T(0) && s.gt == 0 && s.flags[0] < 0)
             {
-                if (s.gt == 0 && s.flags[0] < 0)
+                s.flags[0] = k + jj;
+            }
+            // the interchange of positions jj and p
+#pragma unroll
+            for (int q = 0; q < RPT; ++q)
+            {
+                if (live[q] && pos[q] == p)
                 {
-                    s.flags[0] = k + jj;
+                    live[q] = false;
+                    pos[q]  = jj;
+                }
+                else if (live[q] && pos[q] == jj)
+                {
+                    pos[q] = p;
                 }
             }
-            ck = 0;
-            cr = INT_MAX;
-            for (int r = jj + 1 + s.gt; r < R; r += s.G)
+            T u[NB];
+#pragma unroll
+            for (int c = 1; c < NB; ++c)
+                u[c] = urow[c];
+            const int lim = NB - jj;  // registers [1, lim) hold the columns still to update
+#pragma unroll
+            for (int q = 0; q < RPT; ++q)
             {
-                T* row = s.P + r * ldp;
-                if (d != T(0))
+                if (live[q] && d != T(0))
                 {
-                    const T l = row[jj] / d;
-                    row[jj]   = l;
-                    for (int c = jj + 1; c < w; ++c)
+                    const T l = v[q][0] / d;
+                    v[q][0]   = l;
+#pragma unroll
+                    for (int c = 1; c < NB; ++c)
                     {
-                        row[c] = fma(-l, s.P[jj * ldp + c], row[c]);
+                        if (c < lim)
+                            v[q][c] = fma(-l, u[c], v[q][c]);
                     }
                 }
-                if (jj + 1 < w)
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < RPT; ++q)
+        {
+            const T t = v[q][0];
+#pragma unroll
+            for (int c = 0; c < NB - 1; ++c)
+                v[q][c] = v[q][c + 1];
+            v[q][NB - 1] = t;
+        }
+    }
+    // write back (the rows' physical places do not change), L11 into P,
+    // L21^T into LT, and the final order into sigma for the map
+#pragma unroll
+    for (int q = 0; q < RPT; ++q)
+    {
+        const int r = s.gt + q * s.G;
+        if (r < R)
+        {
+            T* dst = s.row(k + r) + k;
+            if (w == NB)
+            {
+#pragma unroll
+                for (int c = 0; c < NB; c += VN)
+                    vstore(dst + c, &v[q][c]);
+            }
+            else
+            {
+#pragma unroll
+                for (int c = 0; c < NB; ++c)
+                    if (c < w)
+                        dst[c] = v[q][c];
+            }
+            const int ps = pos[q];
+            if (ps < w)
+            {
+#pragma unroll
+                for (int c = 0; c < NB; ++c)
+                    if (c < w)
+                        s.P[ps * ldp + c] = v[q][c];
+            }
+            else
+            {
+#pragma unroll
+                for (int c = 0; c < NB; ++c)
+                    if (c < w)
+                        s.LT[c * s.np + (ps - w)] = v[q][c];
+            }
+            s.sigma[ps] = r;
+        }
+    }
+    s.sync();
+    remap_rows(s, k, R);
+}
+
+// The same panel in shared memory (P), for orders whose rows do not fit the
+// register panel's rows per thread.
+template <typename T> __device__ void panel_smem(const Sys<T>& s, int k, int w)
+{
+    using K        = typename BKey<T>::type;
+    const int n    = s.n;
+    const int R    = n - k;
+    const int lane = s.gt & 31, warp = s.gt >> 5, warps = s.G >> 5;
+    const int ldp  = s.nb + 1;
+    // load: 4 elements in flight per thread
+    for (int e0 = s.gt; e0 < R * w; e0 += 4 * s.G)
+    {
+        T   t[4];
+        int rr[4], cc[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+        {
+            const int e = e0 + u * s.G;
+            rr[u]       = e / w;
+            cc[u]       = e - rr[u] * w;
+            t[u]        = e < R * w ? s.row(k + rr[u])[k + cc[u]] : T(0);
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+        {
+            if (e0 + u * s.G < R * w)
+                s.P[rr[u] * ldp + cc[u]] = t[u];
+        }
+    }
+    for (int r = s.gt; r < R; r += s.G)
+    {
+        s.sigma[r] = r;
+    }
+    s.sync();
+    K   ck = 0;
+    int cr = INT_MAX;
+    for (int r = s.gt; r < R; r += s.G)
+    {
+        const K key = bkey(s.P[r * ldp], r == 0);
+        if (key > ck)
+        {
+            ck = key;
+            cr = r;
+        }
+    }
+    for (int jj = 0; jj < w; ++jj)
+    {
+        bwarp_best(ck, cr);
+        if (lane == 0)
+        {
+            s.red_key[warp] = (unsigned long long)ck;
+            s.red_row[warp] = cr;
+        }
+        s.sync();
+        K   pk = lane < warps ? (K)s.red_key[lane] : K(0);
+        int p  = lane < warps ? s.red_row[lane] : INT_MAX;
+        bwarp_best(pk, p);
+        if (p != jj)
+        {
+            for (int c = s.gt; c < w; c += s.G)
+            {
+                const T t         = s.P[jj * ldp + c];
+                s.P[jj * ldp + c] = s.P[p * ldp + c];
+                s.P[p * ldp + c]  = t;
+            }
+        }
+        if (s.gt == 0 && p != jj)
+        {
+            const int t = s.sigma[jj];
+            s.sigma[jj] = s.sigma[p];
+            s.sigma[p]  = t;
+        }
+        s.sync();
+        const T d = s.P[jj * ldp + jj];
+        if (d == T(0) && s.gt == 0 && s.flags[0] < 0)
+        {
+            s.flags[0] = k + jj;
+        }
+        ck = 0;
+        cr = INT_MAX;
+        for (int r = jj + 1 + s.gt; r < R; r += s.G)
+        {
+            T* row = s.P + r * ldp;
+            if (d != T(0))
+            {
+                const T l = row[jj] / d;
+                row[jj]   = l;
+                for (int c = jj + 1; c < w; ++c)
                 {
-                    const K key = bkey(row[jj + 1], r == jj + 1);
-                    if (key > ck)
+                    row[c] = fma(-l, s.P[jj * ldp + c], row[c]);
+                }
+            }
+            if (jj + 1 < w)
+            {
+                const K key = bkey(row[jj + 1], r == jj + 1);
+                if (key > ck)
+                {
+                    ck = key;
+                    cr = r;
+                }
+            }
+        }
+    }
+    s.sync();
+    remap_rows(s, k, R);
+    for (int e = s.gt; e < R * w; e += s.G)
+    {
+        const int r         = e / w, c = e - r * w;
+        const T   t         = s.P[r * ldp + c];
+        s.row(k + r)[k + c] = t;
+        if (r >= w)
+        {
+            s.LT[c * s.np + (r - w)] = t;
+        }
+    }
+    s.sync();
+}
+
+// A22 -= L21 U12 for the rows and columns [k + w, n): TM x 8 tiles per
+// thread, (G / 16) TM rows x 128 columns per pass; a thread's 8 columns are
+// two 4-column halves 64 apart, so that the 16 threads of a row read U12 in
+// one contiguous 256-byte run.  The tile of A22 is loaded before the product
+// so that its latency hides behind the w rank-1 steps.
+template <typename T> __device__ void trailing_update(const Sys<T>& s, int k, int w, int rest)
+{
+    constexpr int TM = BatchTraits<T>::TM;
+    constexpr int VN = 16 / (int)sizeof(T);
+    constexpr int HN = 4;  // columns per half
+    const int     tx = s.gt & 15, ty = s.gt >> 4;
+    const int     th = (s.G >> 4) * TM;
+    const int     c0 = k + w;
+    for (int i0 = 0; i0 < rest; i0 += th)
+    {
+        for (int j0 = 0; j0 < rest; j0 += 128)
+        {
+            const int ri  = i0 + ty * TM;
+            const int cl  = j0 + tx * HN;
+            const int chi = cl + 64;
+            if (ri >= rest || cl >= rest)
+            {
+                continue;
+            }
+            const bool hi = chi < rest;
+            T          c[TM][2 * HN];
+#pragma unroll
+            for (int a = 0; a < TM; ++a)
+            {
+#pragma unroll
+                for (int h = 0; h < 2; ++h)
+                {
+                    const int col = h ? chi : cl;
+                    if (ri + a < rest && (h == 0 || hi))
                     {
-                        ck = key;
-                        cr = r;
+                        const T* src = s.row(c0 + ri + a) + c0 + col;
+                        if (col + HN <= rest)
+                        {
+#pragma unroll
+                            for (int j = 0; j < HN; j += VN)
+                                vload(src + j, &c[a][h * HN + j]);
+                        }
+                        else
+                        {
+#pragma unroll
+                            for (int j = 0; j < HN; ++j)
+                                c[a][h * HN + j] = col + j < rest ? src[j] : T(0);
+                        }
+                    }
+                    else
+                    {
+#pragma unroll
+                        for (int j = 0; j < HN; ++j)
+                            c[a][h * HN + j] = T(0);
+                    }
+                }
+            }
+            T acc[TM][2 * HN];
+#pragma unroll
+            for (int a = 0; a < TM; ++a)
+#pragma unroll
+                for (int b = 0; b < 2 * HN; ++b)
+                    acc[a][b] = T(0);
+            for (int kk = 0; kk < w; ++kk)
+            {
+                T        lv[TM], uv[2 * HN];
+                const T* lt = s.LT + kk * s.np + ri;
+                const T* ut = s.U + kk * s.np;
+#pragma unroll
+                for (int a = 0; a < TM; a += VN)
+                    vload(lt + a, &lv[a]);
+#pragma unroll
+                for (int j = 0; j < HN; j += VN)
+                    vload(ut + cl + j, &uv[j]);
+                if (hi)
+                {
+#pragma unroll
+                    for (int j = 0; j < HN; j += VN)
+                        vload(ut + chi + j, &uv[HN + j]);
+                }
+                else
+                {
+#pragma unroll
+                    for (int j = 0; j < HN; ++j)
+                        uv[HN + j] = T(0);
+                }
+#pragma unroll
+                for (int a = 0; a < TM; ++a)
+#pragma unroll
+                    for (int b = 0; b < 2 * HN; ++b)
+                        acc[a][b] = fma(lv[a], uv[b], acc[a][b]);
+            }
+#pragma unroll
+            for (int a = 0; a < TM; ++a)
+            {
+                if (ri + a >= rest)
+                {
+                    continue;
+                }
+#pragma unroll
+                for (int h = 0; h < 2; ++h)
+                {
+                    const int col = h ? chi : cl;
+                    if (h == 1 && !hi)
+                    {
+                        continue;
+                    }
+                    T out[HN];
+#pragma unroll
+                    for (int j = 0; j < HN; ++j)
+                        out[j] = c[a][h * HN + j] - acc[a][h * HN + j];
+                    T* dst = s.row(c0 + ri + a) + c0 + col;
+                    if (col + HN <= rest)
+                    {
+#pragma unroll
+                        for (int j = 0; j < HN; j += VN)
+                            vstore(dst + j, &out[j]);
+                    }
+                    else
+                    {
+#pragma unroll
+                        for (int j = 0; j < HN; ++j)
+                            if (col + j < rest)
+                                dst[j] = out[j];
                     }
                 }
             }
         }
-        s.sync();
-        // ---- the panel back; its interchanges as one permutation list
-        for (int e = s.gt; e < R * w; e += s.G)
+    }
+}
+
+template <typename T, int NB> __device__ void lu_factor_nb(const Sys<T>& s)
+{
+    const int n   = s.n;
+    const int ldp = NB + 1;
+    const int rpt = panel_rpt<T>(n, NB, s.G);
+    for (int k = 0; k < n; k += NB)
+    {
+        const int w    = min(NB, n - k);
+        const int rest = n - k - w;
+        // ---- the panel: factored, rows remapped, written back; L11 in P,
+        // L21^T in LT
+        if (rpt == 2)
         {
-            const int r = e / w, c = e - r * w;
-            s.f[(size_t)(k + r) * n + k + c] = s.P[r * ldp + c];
+            panel_regs<T, NB, 2>(s, k, w);
         }
-        if (warp == 0)
+        else
         {
-            int cnt = 0;
-            for (int r0 = 0; r0 < R; r0 += 32)
+            if constexpr (4 * NB * sizeof(T) <= 256)
             {
-                const int      r    = r0 + lane;
-                const bool     mv   = r < R && s.sigma[r] != r;
-                const unsigned bits = __ballot_sync(0xffffffffu, mv);
-                if (mv)
-                {
-                    const int q            = cnt + __popc(bits & ((1u << lane) - 1u));
-                    s.list[q]              = r;           // destination
-                    s.list[2 * s.nb + q]   = s.sigma[r];  // source
-                }
-                cnt += __popc(bits);
+                if (rpt == 4)
+                    panel_regs<T, NB, 4>(s, k, w);
+                else
+                    panel_smem(s, k, w);
             }
-            if (lane == 0)
+            else
             {
-                s.flags[1] = cnt;
+                panel_smem(s, k, w);
             }
         }
-        s.sync();
-        const int cnt = s.flags[1];
-        if (cnt > 0)
-        {
-            apply_interchanges(s, k, cnt, 0, k);
-            apply_interchanges(s, k, cnt, k + w, n);
-        }
+        B200LA_BPHASE(1);
         if (rest <= 0)
         {
             break;
         }
-        // ---- U12 = L11^-1 A12 (thread per column) and L21 transposed
+        // ---- U12 = L11^-1 A12 (thread per column)
         for (int c = s.gt; c < rest; c += s.G)
         {
-            T u[BatchTraits<T>::kMaxNB];
+            T u[NB];
 #pragma unroll
-            for (int i = 0; i < BatchTraits<T>::kMaxNB; ++i)
+            for (int i = 0; i < NB; ++i)
             {
-                u[i] = i < w ? s.f[(size_t)(k + i) * n + k + w + c] : T(0);
+                u[i] = i < w ? s.row(k + i)[k + w + c] : T(0);
             }
 #pragma unroll
-            for (int i = 1; i < BatchTraits<T>::kMaxNB; ++i)
+            for (int i = 1; i < NB; ++i)
             {
-                if (i < w)
-                {
 #pragma unroll
-                    for (int j = 0; j < i; ++j)
-                    {
-                        u[i] = fma(-s.P[i * ldp + j], u[j], u[i]);
-                    }
+                for (int j = 0; j < i; ++j)
+                {
+                    u[i] = fma(-s.P[i * ldp + j], u[j], u[i]);
                 }
             }
 #pragma unroll
-            for (int i = 0; i < BatchTraits<T>::kMaxNB; ++i)
+            for (int i = 0; i < NB; ++i)
             {
                 if (i < w)
                 {
-                    s.f[(size_t)(k + i) * n + k + w + c] = u[i];
-                    s.U[i * s.np + c]                    = u[i];
-                }
-            }
-        }
-        for (int e = s.gt; e < rest * w; e += s.G)
-        {
-            const int r = e / w, c = e - r * w;
-            s.LT[c * s.np + r] = s.P[(w + r) * ldp + c];
-        }
-        s.sync();
-        // ---- A22 -= L21 U12: TM x TN tiles per thread, (G/16 TM) x (16 TN) per pass
-        const int tx = s.gt & 15, ty = s.gt >> 4;
-        const int th = (s.G >> 4) * TM, tw = 16 * TN;
-        T*        c22 = s.f + (size_t)(k + w) * n + k + w;
-        for (int i0 = 0; i0 < rest; i0 += th)
-        {
-            for (int j0 = 0; j0 < rest; j0 += tw)
-            {
-                const int ri = i0 + ty * TM, cj = j0 + tx * TN;
-                if (ri < rest && cj < rest)
-                {
-                    T acc[TM][TN];
-#pragma unroll
-                    for (int a = 0; a < TM; ++a)
-#pragma unroll
-                        for (int b = 0; b < TN; ++b)
-                            acc[a][b] = T(0);
-                    for (int kk = 0; kk < w; ++kk)
-                    {
-                        T lv[TM], uv[TN];
-#pragma unroll
-                        for (int a = 0; a < TM; ++a)
-                            lv[a] = s.LT[kk * s.np + ri + a];
-#pragma unroll
-                        for (int b = 0; b < TN; ++b)
-                            uv[b] = s.U[kk * s.np + cj + b];
-#pragma unroll
-                        for (int a = 0; a < TM; ++a)
-#pragma unroll
-                            for (int b = 0; b < TN; ++b)
-                                acc[a][b] = fma(lv[a], uv[b], acc[a][b]);
-                    }
-#pragma unroll
-                    for (int a = 0; a < TM; ++a)
-                    {
-                        if (ri + a < rest)
-                        {
-                            T* crow = c22 + (size_t)(ri + a) * n + cj;
-#pragma unroll
-                            for (int b = 0; b < TN; ++b)
-                            {
-                                if (cj + b < rest)
-                                {
-                                    crow[b] -= acc[a][b];
-                                }
-                            }
-                        }
-                    }
+                    s.row(k + i)[k + w + c] = u[i];
+                    s.U[i * s.np + c]       = u[i];
                 }
             }
         }
         s.sync();
+        B200LA_BPHASE(2);
+        trailing_update(s, k, w, rest);
+        s.sync();
+        B200LA_BPHASE(3);
+    }
+}
+
+template <typename T> __device__ void lu_factor(const Sys<T>& s)
+{
+    if (s.nb == BatchTraits<T>::kMaxNB)
+        lu_factor_nb<T, BatchTraits<T>::kMaxNB>(s);
+    else
+        lu_factor_nb<T, BatchTraits<T>::kMinNB>(s);
+}
+
+// Rows [i0, i0 + 2) of A (FP64, row-major n x n), a warp's lanes over the
+// columns: both rows' loads are issued before any is used.
+constexpr int kBPerLane = kBMaxN / 32;
+__device__ __forceinline__ void load_two_rows(const double* __restrict__ a, int n, int i0, int lane,
+    double (&e)[2][kBPerLane])
+{
+#pragma unroll
+    for (int h = 0; h < 2; ++h)
+    {
+#pragma unroll
+        for (int m = 0; m < kBPerLane; ++m)
+        {
+            const int j = lane + 32 * m;
+            e[h][m]     = (i0 + h < n && j < n) ? a[(size_t)(i0 + h) * n + j] : 0.0;
+        }
     }
 }
 
@@ -529,30 +973,50 @@ template <typename T>
 __device__ void solve_system(Sys<T>& s, const double* __restrict__ a, const double* __restrict__ b,
     double* __restrict__ x, int max_iter, double tol, bool fallback, int32_t* status, double* berr, int sys)
 {
-    const int n    = s.n;
-    const int lane = s.gt & 31, warp = s.gt >> 5;
+    const int n     = s.n;
+    const int lane  = s.gt & 31, warp = s.gt >> 5;
     const int warps = s.G >> 5;
     if (s.gt == 0)
     {
         s.flags[0] = -1;
     }
-    // ---- A -> F in T, ||A||_inf (a warp per row); the norm lands in r[0..)
-    double anorm = 0.0;
-    for (int i = warp; i < n; i += warps)
+    for (int i = s.gt; i < n; i += s.G)
     {
-        double acc = 0.0;
-        for (int j = lane; j < n; j += 32)
-        {
-            const double v         = a[(size_t)i * n + j];
-            s.f[(size_t)i * n + j] = (T)v;
-            acc += fabs(v);
-        }
+        s.rowp[i] = i;
+    }
+    // ---- A -> F in T, ||A||_inf: a warp per row, two rows in flight; the
+    // norm lands in y[0..warps)
+    double anorm = 0.0;
+    for (int i0 = 2 * warp; i0 < n; i0 += 2 * warps)
+    {
+        double e[2][kBPerLane];
+        load_two_rows(a, n, i0, lane, e);
 #pragma unroll
-        for (int off = 16; off > 0; off >>= 1)
+        for (int h = 0; h < 2; ++h)
         {
-            acc += __shfl_down_sync(0xffffffffu, acc, off);
+            if (i0 + h >= n)
+            {
+                continue;
+            }
+            T*     dst = s.f + (size_t)(i0 + h) * s.ld;
+            double acc = 0.0;
+#pragma unroll
+            for (int m = 0; m < kBPerLane; ++m)
+            {
+                const int j = lane + 32 * m;
+                if (j < n)
+                {
+                    dst[j] = (T)e[h][m];
+                    acc += fabs(e[h][m]);
+                }
+            }
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1)
+            {
+                acc += __shfl_xor_sync(0xffffffffu, acc, off);
+            }
+            anorm = fmax(anorm, acc);
         }
-        anorm = fmax(anorm, acc);
     }
     if (lane == 0)
     {
@@ -565,6 +1029,7 @@ __device__ void solve_system(Sys<T>& s, const double* __restrict__ a, const doub
         anorm = fmax(anorm, s.y[q]);
     }
     s.sync();
+    B200LA_BPHASE(0);
     lu_factor(s);
     if (s.flags[0] >= 0)
     {
@@ -575,21 +1040,6 @@ __device__ void solve_system(Sys<T>& s, const double* __restrict__ a, const doub
         }
         s.sync();
         return;
-    }
-    // row permutation of the pivot sequence (n <= 512 swaps, one thread)
-    if (s.gt == 0)
-    {
-        for (int i = 0; i < n; ++i)
-        {
-            s.perm[i] = i;
-        }
-        for (int i = 0; i < n; ++i)
-        {
-            const int t = s.piv[i];
-            const int v = s.perm[i];
-            s.perm[i]   = s.perm[t];
-            s.perm[t]   = v;
-        }
     }
     double bnorm = 0.0;
     for (int i = s.gt; i < n; i += s.G)
@@ -608,9 +1058,10 @@ __device__ void solve_system(Sys<T>& s, const double* __restrict__ a, const doub
     bool   done     = false;
     for (;;)
     {
+        // the factor's logical row i is A's row rowp[i]
         for (int i = s.gt; i < n; i += s.G)
         {
-            s.y[i] = s.r[s.perm[i]];
+            s.y[i] = s.r[s.rowp[i]];
         }
         s.sync();
         bat_trsv(s, false);
@@ -620,26 +1071,39 @@ __device__ void solve_system(Sys<T>& s, const double* __restrict__ a, const doub
             s.x[i] += s.y[i];
         }
         s.sync();
-        // r = b - A x (a warp per row), max|r|, max|x|
+        B200LA_BPHASE(4);
+        // r = b - A x (a warp per row, two rows in flight), max|r|, max|x|
         double rmax = 0.0, xmax = 0.0;
-        for (int i = warp; i < n; i += warps)
+        for (int i0 = 2 * warp; i0 < n; i0 += 2 * warps)
         {
-            double acc = 0.0;
-            for (int j = lane; j < n; j += 32)
-            {
-                acc = fma(a[(size_t)i * n + j], s.x[j], acc);
-            }
+            double e[2][kBPerLane];
+            load_two_rows(a, n, i0, lane, e);
 #pragma unroll
-            for (int off = 16; off > 0; off >>= 1)
+            for (int h = 0; h < 2; ++h)
             {
-                acc += __shfl_down_sync(0xffffffffu, acc, off);
-            }
-            if (lane == 0)
-            {
-                const double ri = b[i] - acc;  // lane 0 holds the row's full sum
-                s.r[i]          = ri;
-                rmax            = fmax(rmax, fabs(ri));
-                xmax            = fmax(xmax, fabs(s.x[i]));
+                double acc = 0.0;
+#pragma unroll
+                for (int m = 0; m < kBPerLane; ++m)
+                {
+                    const int j = lane + 32 * m;
+                    if (j < n)
+                    {
+                        acc = fma(e[h][m], s.x[j], acc);
+                    }
+                }
+#pragma unroll
+                for (int off = 16; off > 0; off >>= 1)
+                {
+                    acc += __shfl_xor_sync(0xffffffffu, acc, off);
+                }
+                const int i = i0 + h;
+                if (lane == 0 && i < n)
+                {
+                    const double ri = b[i] - acc;
+                    s.r[i]          = ri;
+                    rmax            = fmax(rmax, fabs(ri));
+                    xmax            = fmax(xmax, fabs(s.x[i]));
+                }
             }
         }
         if (lane == 0)
@@ -655,6 +1119,7 @@ __device__ void solve_system(Sys<T>& s, const double* __restrict__ a, const doub
             xmax = fmax(xmax, s.y[2 * q + 1]);
         }
         s.sync();
+        B200LA_BPHASE(5);
         const double den = anorm * xmax + bnorm;
         eta              = den > 0 ? rmax / den : 0.0;
         ++it;
@@ -697,6 +1162,7 @@ __global__ void __launch_bounds__(kBT, 1) k_batched_gesv(int count, const int32_
     auto entry_of = [&](int n) {
         return table != nullptr ? table[min((n - 1) / 64, kBBuckets - 1)] : BatchTraits<T>::kMaxNB;
     };
+    T* slot = F + (size_t)blockIdx.x * (kBScratch / sizeof(T));
     for (;;)
     {
         // the CTA's next chunk: the first system sets the group size and
@@ -712,15 +1178,14 @@ __global__ void __launch_bounds__(kBT, 1) k_batched_gesv(int count, const int32_
                 const int e    = entry_of(sizes[sys0]);
                 int       G    = entry_g(e);
                 int       nb   = entry_nb(e);
-                nb             = nb < 1 ? 1 : (nb > BatchTraits<T>::kMaxNB ? BatchTraits<T>::kMaxNB : nb);
+                nb             = nb_supported<T>(nb) ? nb : BatchTraits<T>::kMaxNB;
                 s_sys[0]       = sys0;
-                bool fits      = true;
+                bool fits      = group_fits<T>(sizes[sys0], nb, G);
                 for (int g = 1; g < kBT / G; ++g)
                 {
                     const int q = atomicAdd(queue, 1);
                     s_sys[g]    = q < count ? (order != nullptr ? order[q] : q) : -1;
-                    if (s_sys[g] >= 0 &&
-                        group_layout<T>(sizes[s_sys[g]], nb).end > kBatchedSmem / (kBT / G) / 16 * 16)
+                    if (s_sys[g] >= 0 && !group_fits<T>(sizes[s_sys[g]], nb, G))
                     {
                         fits = false;  // a larger system than the first (an unsorted order)
                     }
@@ -753,20 +1218,22 @@ __global__ void __launch_bounds__(kBT, 1) k_batched_gesv(int count, const int32_
                 s.G                  = G;
                 s.gt                 = tid - group * G;
                 s.bar                = 1 + group;
-                s.f                  = F + offa[sys];
+                s.ld                 = bat_ld<T>(s.n);
+                s.f                  = slot + (size_t)group * (group_scratch_bytes(G) / sizeof(T));
                 s.np                 = group_np(s.n);
-                const GroupSmem L    = group_layout<T>(s.n, s.nb);
-                unsigned char*  base = smem_raw + (size_t)group * (kBatchedSmem / (kBT / G) / 16 * 16);
+                const GroupSmem L    = group_layout<T>(s.n, s.nb, G);
+                unsigned char*  base = smem_raw + (size_t)group * group_smem_bytes(G);
                 s.P                  = reinterpret_cast<T*>(base + L.P);
                 s.LT                 = reinterpret_cast<T*>(base + L.LT);
                 s.U                  = reinterpret_cast<T*>(base + L.U);
                 s.y                  = reinterpret_cast<double*>(base + L.y);
                 s.r                  = reinterpret_cast<double*>(base + L.r);
                 s.x                  = reinterpret_cast<double*>(base + L.x);
+                s.dg                 = reinterpret_cast<T*>(base + L.dg);
+                s.dpart              = reinterpret_cast<double*>(base + L.dpart);
                 s.sigma              = reinterpret_cast<int*>(base + L.sigma);
                 s.list               = reinterpret_cast<int*>(base + L.list);
-                s.piv                = reinterpret_cast<int*>(base + L.piv);
-                s.perm               = reinterpret_cast<int*>(base + L.perm);
+                s.rowp               = reinterpret_cast<int*>(base + L.rowp);
                 s.red_key            = reinterpret_cast<unsigned long long*>(base + L.red);
                 s.red_row            = reinterpret_cast<int*>(base + L.red + 64);
                 s.flags              = reinterpret_cast<int*>(base + L.red + 64 + 32);
@@ -792,9 +1259,10 @@ template <typename T> int set_batched_attr()
     return B200LA_SUCCESS;
 }
 
-// Whether the largest order of every bucket fits its group's shared-memory
-// slice with the bucket's panel width (the systems are taken largest first,
-// so a group never gets a larger one than its chunk's first).
+// Whether the largest order of every bucket fits its group (shared-memory
+// slice and factor scratch) with the bucket's panel width, and every panel
+// width is one the kernel is built for (the systems are taken largest
+// first, so a group never gets a larger one than its chunk's first).
 template <typename T> bool table_fits(const int32_t* table_host)
 {
     for (int bk = 0; bk < kBBuckets; ++bk)
@@ -802,14 +1270,17 @@ template <typename T> bool table_fits(const int32_t* table_host)
         const int e  = table_host[bk];
         const int G  = entry_g(e);
         const int nb = entry_nb(e);
-        if (nb < 1 || nb > BatchTraits<T>::kMaxNB)
+        if (!nb_supported<T>(nb))
             return false;
         const int nmax = bk == kBBuckets - 1 ? kBMaxN : 64 * (bk + 1);
-        if (group_layout<T>(nmax, nb).end > kBatchedSmem / (kBT / G) / 16 * 16)
+        if (!group_fits<T>(nmax, nb, G))
             return false;
     }
     return true;
 }
+
+// Factor-scratch slots for a batch of at most `systems` systems.
+inline int64_t scratch_slots(int64_t systems) { return systems < kBMaxCTAs ? systems : kBMaxCTAs; }
 }  // namespace
 int require_sm100();
 }  // namespace b200la
@@ -820,15 +1291,14 @@ extern "C" {
 
 B200LA_API size_t b200la_dgesv_batched_workspace_size(int64_t total_a, int64_t total_v, int precision)
 {
-    (void)total_v;
     (void)precision;
     if (total_a <= 0 || total_v <= 0)
         return 0;
     Arena a;
     a.next<int32_t>(64);  // queue counters of the two passes
-    // factors: FP32 in the first pass; the FP64 pass for systems whose FP32
-    // refinement stalled reuses the same buffer as FP64
-    a.next<double>((size_t)total_a);
+    // factor scratch: one slot per CTA (a batch has at most total_v
+    // systems); the FP32 and the FP64 pass use the same slots
+    a.next<unsigned char>((size_t)scratch_slots(total_v) * kBScratch);
     return a.size();
 }
 
@@ -853,6 +1323,8 @@ B200LA_API int b200la_dgesv_batched(int64_t count, const int32_t* sizes, const i
         return set_error(B200LA_NOT_SUPPORTED, "dgesv_batched: precision must be FP32 (refined) or FP64");
     if (max_iterations < 0 || !(tolerance > 0))
         return set_error(B200LA_INVALID_ARGUMENT, "dgesv_batched: invalid refinement options");
+    if (count > total_v)
+        return set_error(B200LA_INVALID_ARGUMENT, "dgesv_batched: more systems than right-hand-side values");
     const size_t need = b200la_dgesv_batched_workspace_size(total_a, total_v, precision);
     if (workspace == nullptr || workspace_bytes < need)
         return set_error(B200LA_WORKSPACE_TOO_SMALL, "dgesv_batched: workspace too small (%zu < %zu)",
@@ -860,12 +1332,14 @@ B200LA_API int b200la_dgesv_batched(int64_t count, const int32_t* sizes, const i
     int rc = require_sm100();
     if (rc != B200LA_SUCCESS)
         return rc;
-    cudaStream_t s = static_cast<cudaStream_t>(stream);
-    Arena        ar(workspace, workspace_bytes);
-    int32_t*     queue = ar.next<int32_t>(64);
-    const int grid = device_sm_count();
+    cudaStream_t  s     = static_cast<cudaStream_t>(stream);
+    Arena         ar(workspace, workspace_bytes);
+    int32_t*      queue = ar.next<int32_t>(64);
+    const int64_t slots = scratch_slots(total_v);
+    const int64_t sms   = device_sm_count();
+    const int     grid  = (int)(sms < slots ? sms : slots);
     B200LA_CUDA(cudaMemsetAsync(queue, 0, sizeof(int32_t) * 2, s));
-    void* fbuf = ar.next<double>((size_t)total_a);
+    void* fbuf = ar.next<unsigned char>((size_t)slots * kBScratch);
     if ((rc = set_batched_attr<double>()) != B200LA_SUCCESS)
         return rc;
     if (precision == B200LA_PREC_FP64)
