@@ -263,12 +263,17 @@ template <typename T> struct Sys
 // y <- T^-1 y for the unit-lower (upper = false) or upper triangle of the
 // factor (FP64 arithmetic).  32-row blocks in solve order.  Per block: the
 // block's rows times the values already solved, G / 32 threads per row, each
-// on 16-byte vectors of the row (the row's diagonal block staged in shared
-// memory on the way), summed with shuffles; then warp 0 holds the diagonal
-// block in registers (row b0 + lane) and substitutes with shuffles.
+// on 16-byte vectors of the row, summed with shuffles; then warp 0 holds the
+// diagonal block (staged in shared memory) in registers, row b0 + lane, and
+// substitutes with shuffles (the upper triangle's divisions as products with
+// reciprocals each lane takes beforehand).  A block's first kTrPre vectors
+// per thread and its diagonal block are loaded while the block before it is
+// substituted: the loads do not depend on the values being solved.
+constexpr int kTrPre = 16;
 template <typename T> __device__ void bat_trsv(const Sys<T>& s, bool upper)
 {
     constexpr int VN   = 16 / (int)sizeof(T);
+    constexpr int DV   = kBSolveNB / VN / 2;  // diagonal-block vectors per thread, at most (2+ threads per row)
     const int     lane = s.gt & 31, warp = s.gt >> 5;
     const int     n    = s.n;
     const int     nblk = (n + kBSolveNB - 1) / kBSolveNB;
@@ -276,54 +281,103 @@ template <typename T> __device__ void bat_trsv(const Sys<T>& s, bool upper)
     const int     ri   = s.gt / tpr;
     const int     ch   = s.gt - ri * tpr;
     double*       y    = s.y;
+    T             e[kTrPre][VN];
+    T             dv[DV][VN];
+    // block bi's bounds: rows [b0, b0 + bw), solved columns [jlo, jhi)
+    auto bounds = [&](int bi, int& b0, int& bw, int& jlo, int& jhi) {
+        const int b = upper ? nblk - 1 - bi : bi;
+        b0          = b * kBSolveNB;
+        bw          = min(kBSolveNB, n - b0);
+        jlo         = upper ? b0 + bw : 0;
+        jhi         = upper ? n : b0;
+    };
+    auto prefetch = [&](int bi) {
+        int b0, bw, jlo, jhi;
+        bounds(bi, b0, bw, jlo, jhi);
+        const int nvec = (jhi - jlo) / VN;
+        const T*  row  = s.row(b0 + (ri < bw ? ri : 0));
+#pragma unroll
+        for (int u = 0; u < kTrPre; ++u)
+        {
+            const int m = ch + u * tpr;
+            if (ri < bw && m < nvec)
+            {
+                vload(row + jlo + m * VN, e[u]);
+            }
+            else
+            {
+#pragma unroll
+                for (int j = 0; j < VN; ++j)
+                    e[u][j] = T(0);
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < DV; ++u)
+        {
+            const int vv = ch + u * tpr;
+            const int c  = b0 + vv * VN;
+            if (ri < bw && vv < kBSolveNB / VN && c + VN <= n)
+            {
+                vload(row + c, dv[u]);
+            }
+            else
+            {
+#pragma unroll
+                for (int j = 0; j < VN; ++j)
+                    dv[u][j] = (ri < bw && vv < kBSolveNB / VN && c + j < n) ? row[c + j] : T(0);
+            }
+        }
+    };
+    prefetch(0);
     for (int bi = 0; bi < nblk; ++bi)
     {
-        const int b   = upper ? nblk - 1 - bi : bi;
-        const int b0  = b * kBSolveNB;
-        const int bw  = min(kBSolveNB, n - b0);
-        const int jlo = upper ? b0 + bw : 0;  // the solved columns [jlo, jhi)
-        const int jhi = upper ? n : b0;
-        double    acc = 0.0;
+        int b0, bw, jlo, jhi;
+        bounds(bi, b0, bw, jlo, jhi);
+        const int nvec = (jhi - jlo) / VN;
+        double    acc  = 0.0;
         if (ri < bw)
         {
-            const T* row = s.row(b0 + ri);
-            for (int v = ch; v < kBSolveNB / VN; v += tpr)
+#pragma unroll
+            for (int u = 0; u < DV; ++u)
             {
-                const int c = b0 + v * VN;
-                T         e[VN];
-                if (c + VN <= n)
-                {
-                    vload(row + c, e);
-                }
-                else
+                const int vv = ch + u * tpr;
+                if (vv < kBSolveNB / VN)
                 {
 #pragma unroll
                     for (int j = 0; j < VN; ++j)
-                        e[j] = c + j < n ? row[c + j] : T(0);
+                        s.dg[ri * kBDgLd + vv * VN + j] = dv[u][j];
                 }
-#pragma unroll
-                for (int j = 0; j < VN; ++j)
-                    s.dg[ri * kBDgLd + v * VN + j] = e[j];
             }
-            // whole vectors in batches of 8 per thread, every load of a batch
-            // issued before the first product; then the ragged tail
-            const int nvec = (jhi - jlo) / VN;
-            for (int m0 = ch; m0 < nvec; m0 += 8 * tpr)
+#pragma unroll
+            for (int u = 0; u < kTrPre; ++u)
             {
-                T e[8][VN];
+                const int m = ch + u * tpr;
+                if (m < nvec)
+                {
+#pragma unroll
+                    for (int j = 0; j < VN; ++j)
+                        acc = fma((double)e[u][j], y[jlo + m * VN + j], acc);
+                }
+            }
+            // vectors past the prefetched ones, in batches of 8; then the
+            // ragged tail
+            const T* row = s.row(b0 + ri);
+            for (int m0 = ch + kTrPre * tpr; m0 < nvec; m0 += 8 * tpr)
+            {
+                T f[8][VN];
 #pragma unroll
                 for (int u = 0; u < 8; ++u)
                 {
                     const int m = m0 + u * tpr;
                     if (m < nvec)
                     {
-                        vload(row + jlo + m * VN, e[u]);
+                        vload(row + jlo + m * VN, f[u]);
                     }
                     else
                     {
 #pragma unroll
                         for (int j = 0; j < VN; ++j)
-                            e[u][j] = T(0);
+                            f[u][j] = T(0);
                     }
                 }
 #pragma unroll
@@ -334,7 +388,7 @@ template <typename T> __device__ void bat_trsv(const Sys<T>& s, bool upper)
                     {
 #pragma unroll
                         for (int j = 0; j < VN; ++j)
-                            acc = fma((double)e[u][j], y[jlo + m * VN + j], acc);
+                            acc = fma((double)f[u][j], y[jlo + m * VN + j], acc);
                     }
                 }
             }
@@ -351,6 +405,10 @@ template <typename T> __device__ void bat_trsv(const Sys<T>& s, bool upper)
         if (ch == 0 && ri < bw)
         {
             s.dpart[ri] = acc;
+        }
+        if (bi + 1 < nblk)
+        {
+            prefetch(bi + 1);
         }
         s.sync();
         if (warp == 0)
@@ -376,13 +434,14 @@ template <typename T> __device__ void bat_trsv(const Sys<T>& s, bool upper)
             }
             else
             {
+                const double rinv = lane < bw ? 1.0 / (double)s.dg[lane * kBDgLd + lane] : 0.0;
 #pragma unroll
                 for (int jj = 0; jj < kBSolveNB; ++jj)
                 {
                     const int j = kBSolveNB - 1 - jj;
                     if (lane == j && j < bw)
                     {
-                        v = v / a[j];
+                        v *= rinv;
                     }
                     const double yj = __shfl_sync(0xffffffffu, v, j);
                     if (lane < j && j < bw)
@@ -455,7 +514,7 @@ template <typename T, int NB, int RPT> __device__ void panel_regs(const Sys<T>& 
     const int     R    = n - k;
     const int     lane = s.gt & 31, warp = s.gt >> 5, warps = s.G >> 5;
     const int     ldp  = s.nb + 1;
-    T*            urow = s.dg;  // the pivot row, active column first
+    T*            urow = s.dg;  // the pivot row, active column first (16-byte aligned)
     T             v[RPT][NB];
     int           pos[RPT];
     bool          live[RPT];    // a row of the panel that is not yet a pivot
@@ -525,8 +584,8 @@ template <typename T, int NB, int RPT> __device__ void panel_regs(const Sys<T>& 
                 if (live[q] && pos[q] == p)
                 {
 #pragma unroll
-                    for (int c = 0; c < NB; ++c)
-                        urow[c] = v[q][c];
+                    for (int c = 0; c < NB; c += VN)
+                        vstore(urow + c, &v[q][c]);
                 }
             }
             s.sync();
@@ -551,8 +610,8 @@ template <typename T, int NB, int RPT> __device__ void panel_regs(const Sys<T>& 
             }
             T u[NB];
 #pragma unroll
-            for (int c = 1; c < NB; ++c)
-                u[c] = urow[c];
+            for (int c = 0; c < NB; c += VN)
+                vload(urow + c, &u[c]);
             const int lim = NB - jj;  // registers [1, lim) hold the columns still to update
 #pragma unroll
             for (int q = 0; q < RPT; ++q)

@@ -829,16 +829,27 @@ void enqueue_block_operands(MixedPlan& p, int n, int K, int Kend, int rest, int 
 // A22 = rows and columns from Kend), operands from the block's copies.
 int enqueue_block_update(MixedPlan& p, int n, int Kend, int c0, int kind, bool split, const CUtensorMap& ma,
     const CUtensorMap& mb, const CUtensorMap& mas, const CUtensorMap& mbs, int ncols, cudaStream_t s,
-    int max_ctas = 0)
+    int max_ctas = 0, int place_cluster = 0)
 {
     const int rest = n - Kend;
     return enqueue_tc_update(kind, split, ma, mb, mas, mbs, p.a32 + (int64_t)Kend * n + c0, n, rest, ncols, kOuterNB,
-        p.gp.st, s, p.l21inv, p.u12inv + (c0 - Kend), max_ctas);
+        p.gp.st, s, p.l21inv, p.u12inv + (c0 - Kend), max_ctas, place_cluster);
 }
 
 // CTAs of the persistent tensor-core update that runs beside the next
 // block's panels: the SMs less those the panel cluster and the panels'
 // in-block kernels use (B200LA_MIXED_UPDATE_CTAS overrides).
+// The update beside the panels is launched as clusters of this many CTAs
+// (whole GPCs, one left free for the panel's cluster); 0 (variable
+// B200LA_MIXED_UPDATE_CLUSTER=0) launches it without placement.
+int beside_panel_cluster()
+{
+    const char* e = getenv("B200LA_MIXED_UPDATE_CLUSTER");
+    if (e != nullptr)
+        return atoi(e) > 1 && atoi(e) <= 16 ? atoi(e) : 0;
+    return 16;
+}
+
 int beside_panel_ctas()
 {
     const char* e = getenv("B200LA_MIXED_UPDATE_CTAS");
@@ -994,7 +1005,7 @@ int enqueue_getrf_mixed(MixedPlan& p, int n, int kind, bool split, cudaStream_t 
             prof_end(KC_PREP, s);
             B200LA_LAUNCH_CHECK();
             if ((rc = enqueue_block_update(p, n, Kend, Kend2, kind, split, ma, mb2, mas, mbs2, n - Kend2, s,
-                     beside_panel_ctas())) !=
+                     beside_panel_ctas(), beside_panel_cluster())) !=
                 B200LA_SUCCESS)
                 return rc;
         }

@@ -53,6 +53,8 @@ template <int KIND, bool SPLIT3> int set_attr_once()
         (int)tc_smem_bytes<SPLIT3>()));
     B200LA_CUDA(cudaFuncSetAttribute(k_tc_update_persistent<KIND, SPLIT3>,
         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tcp_smem_bytes<SPLIT3>()));
+    B200LA_CUDA(cudaFuncSetAttribute(k_tc_update_persistent<KIND, SPLIT3>,
+        cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
     if (dev >= 0 && dev < 64)
     {
         done[dev] = true;
@@ -100,10 +102,47 @@ static bool tc_persistent_enabled()
     return !(e != nullptr && e[0] == '0');
 }
 
+// Clusters of `cl` persistent-update CTAs that fit the device at once (0 if
+// the query fails), per device.
+template <int KIND, bool SPLIT3> int tc_active_clusters(int cl)
+{
+    static std::mutex m;
+    static int        known[64][17] = {};
+    int               dev           = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64 || cl < 2 || cl > 16)
+    {
+        return 0;
+    }
+    std::lock_guard<std::mutex> lock(m);
+    if (known[dev][cl] == 0)
+    {
+        cudaLaunchConfig_t  cfg = {};
+        cudaLaunchAttribute attr[1];
+        cfg.gridDim              = dim3(cl);
+        cfg.blockDim             = dim3(kTcpThreads);
+        cfg.dynamicSmemBytes     = tcp_smem_bytes<SPLIT3>();
+        attr[0].id               = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = cl;
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        cfg.attrs                = attr;
+        cfg.numAttrs             = 1;
+        int count                = 0;
+        if (cudaOccupancyMaxActiveClusters(&count, (const void*)k_tc_update_persistent<KIND, SPLIT3>, &cfg) !=
+            cudaSuccess)
+        {
+            cudaGetLastError();
+            count = -1;
+        }
+        known[dev][cl] = count;
+    }
+    return known[dev][cl] > 0 ? known[dev][cl] : 0;
+}
+
 template <int KIND, bool SPLIT3>
 static int launch_tc(const CUtensorMap& a, const CUtensorMap& b, const CUtensorMap& as, const CUtensorMap& bs,
     float* c, int64_t ldc, int m, int n, int k, DeviceStatus* st, const float* inv_sa, const float* inv_sb,
-    cudaStream_t s, int max_ctas)
+    cudaStream_t s, int max_ctas, int place_cluster)
 {
     int rc = set_attr_once<KIND, SPLIT3>();
     if (rc != B200LA_SUCCESS)
@@ -123,6 +162,33 @@ static int launch_tc(const CUtensorMap& a, const CUtensorMap& b, const CUtensorM
         }
         int g = max_ctas > 0 && max_ctas < sms ? max_ctas : sms;
         g             = g < tiles ? g : tiles;
+        int ncl = 0;  // clusters of the placed launch
+        if (place_cluster > 1)
+        {
+            const int cap = g / place_cluster;
+            ncl           = tc_active_clusters<KIND, SPLIT3>(place_cluster) - 1;  // leave one GPC free
+            ncl           = ncl < cap ? ncl : cap;
+        }
+        if (ncl >= 1)
+        {
+            cudaLaunchConfig_t  cfg = {};
+            cudaLaunchAttribute attr[1];
+            cfg.gridDim              = dim3(ncl * place_cluster);
+            cfg.blockDim             = dim3(kTcpThreads);
+            cfg.dynamicSmemBytes     = tcp_smem_bytes<SPLIT3>();
+            cfg.stream               = s;
+            attr[0].id               = cudaLaunchAttributeClusterDimension;
+            attr[0].val.clusterDim.x = place_cluster;
+            attr[0].val.clusterDim.y = 1;
+            attr[0].val.clusterDim.z = 1;
+            cfg.attrs                = attr;
+            cfg.numAttrs             = 1;
+            prof_begin(KC_MIXED, s);
+            B200LA_CUDA(cudaLaunchKernelEx(&cfg, k_tc_update_persistent<KIND, SPLIT3>, a, b, as, bs, c, ldc, m, n,
+                k, st, inv_sa, inv_sb));
+            prof_end(KC_MIXED, s);
+            return B200LA_SUCCESS;
+        }
         prof_begin(KC_MIXED, s);
         k_tc_update_persistent<KIND, SPLIT3><<<g, kTcpThreads, tcp_smem_bytes<SPLIT3>(), s>>>(a, b, as, bs, c, ldc,
             m, n, k, st, inv_sa, inv_sb);
@@ -141,7 +207,7 @@ static int launch_tc(const CUtensorMap& a, const CUtensorMap& b, const CUtensorM
 
 int enqueue_tc_update(int kind, bool split3, const CUtensorMap& a, const CUtensorMap& b, const CUtensorMap& as,
     const CUtensorMap& bs, float* c, int64_t ldc, int m, int n, int k, DeviceStatus* st, cudaStream_t s,
-    const float* inv_sa, const float* inv_sb, int max_ctas)
+    const float* inv_sa, const float* inv_sb, int max_ctas, int place_cluster)
 {
     if (m <= 0 || n <= 0)
     {
@@ -154,8 +220,8 @@ int enqueue_tc_update(int kind, bool split3, const CUtensorMap& a, const CUtenso
     }
     if (kind == TC_TF32)
     {
-        return split3 ? launch_tc<TC_TF32, true>(a, b, as, bs, c, ldc, m, n, k, st, nullptr, nullptr, s, max_ctas)
-                      : launch_tc<TC_TF32, false>(a, b, as, bs, c, ldc, m, n, k, st, nullptr, nullptr, s, max_ctas);
+        return split3 ? launch_tc<TC_TF32, true>(a, b, as, bs, c, ldc, m, n, k, st, nullptr, nullptr, s, max_ctas, place_cluster)
+                      : launch_tc<TC_TF32, false>(a, b, as, bs, c, ldc, m, n, k, st, nullptr, nullptr, s, max_ctas, place_cluster);
     }
     if (split3)
     {
@@ -163,7 +229,7 @@ int enqueue_tc_update(int kind, bool split3, const CUtensorMap& a, const CUtenso
     }
     if (kind == TC_BF16)
     {
-        return launch_tc<TC_BF16, false>(a, b, as, bs, c, ldc, m, n, k, st, nullptr, nullptr, s, max_ctas);
+        return launch_tc<TC_BF16, false>(a, b, as, bs, c, ldc, m, n, k, st, nullptr, nullptr, s, max_ctas, place_cluster);
     }
     if (kind == TC_FP8)
     {
@@ -171,9 +237,9 @@ int enqueue_tc_update(int kind, bool split3, const CUtensorMap& a, const CUtenso
         {
             return set_error(B200LA_INVALID_ARGUMENT, "tensor-core update: FP8 operands need their scales");
         }
-        return launch_tc<TC_FP8, false>(a, b, as, bs, c, ldc, m, n, k, st, inv_sa, inv_sb, s, max_ctas);
+        return launch_tc<TC_FP8, false>(a, b, as, bs, c, ldc, m, n, k, st, inv_sa, inv_sb, s, max_ctas, place_cluster);
     }
-    return launch_tc<TC_FP16, false>(a, b, as, bs, c, ldc, m, n, k, st, nullptr, nullptr, s, max_ctas);
+    return launch_tc<TC_FP16, false>(a, b, as, bs, c, ldc, m, n, k, st, nullptr, nullptr, s, max_ctas, place_cluster);
 }
 
 }  // namespace b200la
