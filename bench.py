@@ -772,6 +772,35 @@ def algorithmic_work(n: int, method: str, nb_out: int = 256):
     return work
 
 
+def batched_roofline(sizes, status, seconds, prec, dev) -> dict:
+    """Both ceilings of the batched solve.  Compute: 2 n^3 / 3 per system
+    against the CUDA cores' nominal FP32 (FP64: half) rate at the maximum SM
+    clock.  Memory: the algorithmic bytes per system, (c + 2) (8 + e) n^2 for
+    c corrections and factor elements of e bytes (A read once for the copy
+    and once per solve for the residual, the factor written once and read
+    once per solve), against the measured HBM copy bandwidth."""
+    import numpy as np
+    import torch
+
+    es = 4 if prec == "fp32" else 8
+    st = np.asarray(status)
+    corr = np.maximum(np.where(st >= 1000, st - 1000, st), 0).astype(np.float64)
+    n = np.asarray(sizes, dtype=np.float64)
+    flops = float((2.0 * n ** 3 / 3).sum())
+    nbytes = float(((corr + 2) * (8 + es) * n * n).sum())
+    sms = torch.cuda.get_device_properties(dev).multi_processor_count
+    simt_peak = sms * (128 if prec == "fp32" else 64) * 2 * 1965e6 / 1e12
+    pk = measured_peaks()
+    tflops = flops / seconds / 1e12
+    gbs = nbytes / seconds / 1e9
+    return {"bound": "latency (both fractions low)" if max(tflops / simt_peak, gbs / pk["hbm_gbs"]) < 0.5
+            else ("simt" if tflops / simt_peak >= gbs / pk["hbm_gbs"] else "hbm"),
+            "tflops": tflops, "simt_peak_tflops": simt_peak, "simt_frac": tflops / simt_peak,
+            "simt_peak_source": f"nominal: {sms} SMs x {128 if prec == 'fp32' else 64} FMA/clk x 1965 MHz",
+            "gbs": gbs, "hbm_peak_gbs": pk["hbm_gbs"], "hbm_frac": gbs / pk["hbm_gbs"],
+            "hbm_peak_source": pk["source"], "algorithmic_bytes_per_batch": nbytes, "flops_per_batch": flops}
+
+
 def run_batched(args, world, rank, local):
     """Config 4: 20,000 uneven systems (n uniform in [16, 512], half
     diagonally dominant), FP32 factors + FP64 refinement to eta <= 1e-14 in one
@@ -818,6 +847,7 @@ def run_batched(args, world, rank, local):
                      "escalated_to_fp64": int((st >= 1000).sum()), "not_converged": int((st == -1000000).sum()),
                      "max_corrections": int(np.where(st >= 1000, st - 1000, st).max()),
                      "singular": int(((st < 0) & (st != -1000000)).sum()), "nb_table": tune["nb_table"]}
+        out[prec]["roofline"] = batched_roofline(sizes, st, t, prec, dev)
         del solver
     # a loop of single-system solves through the one-system mixed solver (sampled)
     if rank == 0:
