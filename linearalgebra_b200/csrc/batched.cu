@@ -348,6 +348,9 @@ template <typename T> __device__ void bat_trsv(const Sys<T>& s, bool upper)
                         s.dg[ri * kBDgLd + vv * VN + j] = dv[u][j];
                 }
             }
+            // four independent sums (a single chain of 64 dependent FP64
+            // FMAs would set the pace)
+            double a4[4] = {0.0, 0.0, 0.0, 0.0};
 #pragma unroll
             for (int u = 0; u < kTrPre; ++u)
             {
@@ -356,9 +359,10 @@ template <typename T> __device__ void bat_trsv(const Sys<T>& s, bool upper)
                 {
 #pragma unroll
                     for (int j = 0; j < VN; ++j)
-                        acc = fma((double)e[u][j], y[jlo + m * VN + j], acc);
+                        a4[u & 3] = fma((double)e[u][j], y[jlo + m * VN + j], a4[u & 3]);
                 }
             }
+            acc = (a4[0] + a4[1]) + (a4[2] + a4[3]);
             // vectors past the prefetched ones, in batches of 8; then the
             // ragged tail
             const T* row = s.row(b0 + ri);
@@ -864,6 +868,7 @@ template <typename T> __device__ void trailing_update(const Sys<T>& s, int k, in
 #pragma unroll
                 for (int b = 0; b < 2 * HN; ++b)
                     acc[a][b] = T(0);
+#pragma unroll 4
             for (int kk = 0; kk < w; ++kk)
             {
                 T        lv[TM], uv[2 * HN];
