@@ -375,7 +375,7 @@ int launch_trailing(T* m, int n, int k, int w, int c0, int c1, cudaStream_t s)
     {
         // k_trailing covers columns [0, ncols) of A22; only whole updates here
         dim3 grid((c1 + kChunkN - 1) / kChunkN, (rest + kBandM - 1) / kBandM);
-        k_trailing<T><<<grid, 128, trailing_smem_bytes<T>(), s>>>(m, n, k, w, c1);
+        k_trailing<T><<<grid, 128, trailing_smem_bytes<T>(), s>>>(m, n, k, w, c1, 0);
     }
     prof_end(KC_TRAILING, s);
     B200LA_LAUNCH_CHECK();
@@ -451,7 +451,8 @@ int enqueue_getrf(T* m, int n, int64_t* pivot, const GetrfPlan<T>& p, cudaStream
         if (nl + nr > 0)
         {
             prof_begin(KC_SWAP, s);
-            k_laswp_trsm<T><<<nl + nr, kSwapThreads, laswp_smem_bytes<T>(), s>>>(m, n, k, w, p.perm, nl, n, 0, k, n);
+            k_laswp_trsm<T><<<nl + nr, kSwapThreads, laswp_smem_bytes<T>(), s>>>(m, n, k, w, p.perm, nl, n, 0, k, n,
+                k + w);
             prof_end(KC_SWAP, s);
             B200LA_LAUNCH_CHECK();
         }

@@ -1246,10 +1246,11 @@ __global__ void __launch_bounds__(kPanelThreads, 1) k_panel_exchange_floor(int c
 // Row interchanges outside the panel and, right of it, U12 = L11^-1 A12.
 // CTA b < n_left: columns [left_begin + b*kSwapCols, ...) of
 // [left_begin, left_end), interchanges only; otherwise columns of
-// [k+w, right_end), with U12 solved for those below u12_end.  (The plain LU
-// passes left [0, k) and right [k+w, n); the mixed LU's look-ahead applies an
-// outer block's interchanges right of the block in a later launch with only
-// a left range.)  256 threads: 4 row groups x 64 columns for the gather/scatter
+// [right_begin, right_end) (right_begin >= k+w), with U12 solved for those
+// below u12_end.  (The plain LU passes left [0, k) and right [k+w, n); the
+// mixed LU's look-ahead applies an outer block's interchanges right of the
+// block in a later launch with only a left range, and inside a block first
+// the next panel's columns, then the rest of the block.)  256 threads: 4 row groups x 64 columns for the gather/scatter
 // (each thread loads its up to 32 rows before storing, so the loads overlap),
 // then one thread per column for the substitution.
 constexpr int kSwapThreads = 256;
@@ -1263,7 +1264,8 @@ template <typename T> constexpr size_t laswp_smem_bytes()
 
 template <typename T>
 __global__ void __launch_bounds__(kSwapThreads) k_laswp_trsm(T* __restrict__ A, int n, int k, int w,
-    const PermList* __restrict__ perm, int n_left, int u12_end, int left_begin, int left_end, int right_end)
+    const PermList* __restrict__ perm, int n_left, int u12_end, int left_begin, int left_end, int right_end,
+    int right_begin)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T(*staged)[kSwapCols] = reinterpret_cast<T(*)[kSwapCols]>(smem_raw);  // [2*kNB]
@@ -1273,7 +1275,7 @@ __global__ void __launch_bounds__(kSwapThreads) k_laswp_trsm(T* __restrict__ A, 
     const int  cl    = tid % kSwapCols;
     const int  rg    = tid / kSwapCols;
     const int  c0    = (int)blockIdx.x < n_left ? left_begin + (int)blockIdx.x * kSwapCols
-                                                : k + w + ((int)blockIdx.x - n_left) * kSwapCols;
+                                                : right_begin + ((int)blockIdx.x - n_left) * kSwapCols;
     // `left`: only the interchanges (the left range, or right of the panel
     // at or beyond u12_end, whose U12 rows are solved later)
     const bool left  = (int)blockIdx.x < n_left || c0 >= u12_end;
@@ -1464,7 +1466,8 @@ __device__ __forceinline__ void trailing_issue_tile(T* Bs, T* Cs, const T* U12, 
 }
 
 template <typename T>
-__global__ void __launch_bounds__(128, 1) k_trailing(T* __restrict__ A, int n, int k, int w, int ncols)
+__global__ void __launch_bounds__(128, 1) k_trailing(T* __restrict__ A, int n, int k, int w, int ncols,
+    int c_off)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     constexpr int CE = chunk_elems<T>();
@@ -1472,7 +1475,7 @@ __global__ void __launch_bounds__(128, 1) k_trailing(T* __restrict__ A, int n, i
     T*            Bs = As + kBandM * kNB;                          // [2][kNB][kTileNc]
     T*            Cs = Bs + 2 * kNB * kTileNc;                     // [2][kBandM][kTileNc]
 
-    const int rest = n - k - w;  // rows of A22; its columns are [0, ncols)
+    const int rest = n - k - w;  // rows of A22; its columns are [c_off, c_off + ncols) from k + w
     const int m0   = blockIdx.y * kBandM;
     const int n0   = blockIdx.x * kChunkN;
     const int tid  = threadIdx.x;
@@ -1483,8 +1486,8 @@ __global__ void __launch_bounds__(128, 1) k_trailing(T* __restrict__ A, int n, i
     const bool vec16 = (((size_t)n * sizeof(T)) % 16 == 0) && ((reinterpret_cast<uintptr_t>(A) & 15) == 0);
 
     const T* L21 = A + (size_t)(k + w) * n + k;
-    const T* U12 = A + (size_t)k * n + k + w;
-    T*       C   = A + (size_t)(k + w) * n + k + w;
+    const T* U12 = A + (size_t)k * n + k + w + c_off;
+    T*       C   = A + (size_t)(k + w) * n + k + w + c_off;
 
     // stage the band's L21 rows (chunk index XOR (row % 4))
     {

@@ -667,15 +667,55 @@ inline int block_panel_count(int n, int K, int Kend)
     return (Kend - K + pw - 1) / pw;
 }
 
-// Inner panels of the outer block [K, Kend): 64-column panels, their row
-// interchanges on columns [0, Kend) (right of the block they are applied
-// later by enqueue_block_swaps), U12 inside the block and the SIMT updates
-// inside the block.  Panel j's interchange list goes to block_perms(p, K)[j].
-int enqueue_block_panels(MixedPlan& p, int n, int K, int Kend, int cl, int gmax, cudaStream_t s)
+// Nested look-ahead inside a block (B200LA_MIXED_NESTED=0: off).
+bool nested_enabled()
 {
-    float*    a32 = p.a32;
-    int       rc  = B200LA_SUCCESS;
-    const int pw  = block_panel_width(n, K);
+    const char* e = getenv("B200LA_MIXED_NESTED");
+    return !(e != nullptr && e[0] == '0');
+}
+
+// Inner panels of the outer block [K, Kend): panels of block_panel_width
+// columns, their row interchanges on columns [K, Kend) (left of the block
+// they are applied later by enqueue_block_left_swaps, right of it after the
+// block by enqueue_block_swaps), U12 inside the block and the SIMT updates
+// inside the block.  Panel j's interchange list goes to block_perms(p, K)[j].
+//
+// With a second stream `rs` (and two events), the work after panel j is
+// split: the next panel's columns (interchanges, U12, update) stay on `s`
+// right behind the panel, and the block's other columns (the interchanges
+// left of the panel and the columns after the next panel) go to `rs`, so
+// panel j + 1 starts as soon as its own columns are ready.  The two streams
+// touch disjoint columns; the next panel's columns were last written by the
+// rest of panel j - 1, which `s` waits for first.  `s` waits for the block's
+// last rest before it returns.
+int enqueue_block_panels(MixedPlan& p, int n, int K, int Kend, int cl, int gmax, cudaStream_t s,
+    cudaStream_t rs = nullptr, cudaEvent_t ev_p = nullptr, cudaEvent_t ev_r = nullptr)
+{
+    float*     a32  = p.a32;
+    int        rc   = B200LA_SUCCESS;
+    const int  pw   = block_panel_width(n, K);
+    const bool nest = rs != nullptr && rs != s && ev_p != nullptr && ev_r != nullptr && nested_enabled();
+    auto swaps = [&](const PermList* perm, int k, int w, int left_cols, int rb, int re, cudaStream_t st) {
+        const int nl = (left_cols + kSwapCols - 1) / kSwapCols;
+        const int nr = re > rb ? (re - rb + kSwapCols - 1) / kSwapCols : 0;
+        if (nl + nr > 0)
+        {
+            prof_begin(KC_SWAP, st);
+            k_laswp_trsm<float><<<nl + nr, kSwapThreads, laswp_smem_bytes<float>(), st>>>(a32, n, k, w, perm, nl,
+                Kend, K, K + left_cols, re, rb);
+            prof_end(KC_SWAP, st);
+        }
+    };
+    auto update = [&](int k, int w, int c_off, int ncols, cudaStream_t st) {
+        const int rest = n - k - w;
+        if (rest > 0 && ncols > 0)
+        {
+            dim3 grid((ncols + kChunkN - 1) / kChunkN, (rest + kBandM - 1) / kBandM);
+            prof_begin(KC_TRAILING, st);
+            k_trailing<float><<<grid, 128, trailing_smem_bytes<float>(), st>>>(a32, n, k, w, ncols, c_off);
+            prof_end(KC_TRAILING, st);
+        }
+    };
     for (int k = K, j = 0; k < Kend; k += pw, ++j)
     {
         const int        w  = Kend - k < pw ? Kend - k : pw;
@@ -683,29 +723,35 @@ int enqueue_block_panels(MixedPlan& p, int n, int K, int Kend, int cl, int gmax,
         gp.perm             = block_perms(p, K) + j;
         if ((rc = launch_panel<float>(a32, n, k, w, p.piv, gp, cl, gmax, s)) != B200LA_SUCCESS)
             return rc;
-        // interchanges inside the block here; left of the block they are
-        // applied later (enqueue_block_left_swaps), right of it after the
-        // block (enqueue_block_swaps)
-        const int nl = (k - K + kSwapCols - 1) / kSwapCols;
-        const int nr = (Kend - (k + w) + kSwapCols - 1) / kSwapCols;
-        if (nl + nr > 0)
+        const int kn  = k + w;                              // the next panel's columns [kn, kn2)
+        const int kn2 = kn + pw < Kend ? kn + pw : Kend;
+        if (!nest)
         {
-            prof_begin(KC_SWAP, s);
-            k_laswp_trsm<float><<<nl + nr, kSwapThreads, laswp_smem_bytes<float>(), s>>>(a32, n, k, w, gp.perm, nl,
-                Kend, K, k, Kend);
-            prof_end(KC_SWAP, s);
+            swaps(gp.perm, k, w, k - K, kn, Kend, s);
             B200LA_LAUNCH_CHECK();
+            update(k, w, 0, Kend - kn, s);
+            B200LA_LAUNCH_CHECK();
+            continue;
         }
-        const int rest  = n - k - w;
-        const int ncols = Kend - (k + w);
-        if (rest > 0 && ncols > 0)
+        B200LA_CUDA(cudaEventRecord(ev_p, s));
+        if (j > 0)
         {
-            dim3 grid((ncols + kChunkN - 1) / kChunkN, (rest + kBandM - 1) / kBandM);
-            prof_begin(KC_TRAILING, s);
-            k_trailing<float><<<grid, 128, trailing_smem_bytes<float>(), s>>>(a32, n, k, w, ncols);
-            prof_end(KC_TRAILING, s);
-            B200LA_LAUNCH_CHECK();
+            B200LA_CUDA(cudaStreamWaitEvent(s, ev_r, 0));  // the rest of panel j - 1
         }
+        swaps(gp.perm, k, w, 0, kn, kn2, s);
+        B200LA_LAUNCH_CHECK();
+        update(k, w, 0, kn2 - kn, s);
+        B200LA_LAUNCH_CHECK();
+        B200LA_CUDA(cudaStreamWaitEvent(rs, ev_p, 0));
+        swaps(gp.perm, k, w, k - K, kn2, Kend, rs);
+        B200LA_LAUNCH_CHECK();
+        update(k, w, kn2 - kn, Kend - kn2, rs);
+        B200LA_LAUNCH_CHECK();
+        B200LA_CUDA(cudaEventRecord(ev_r, rs));
+    }
+    if (nest)
+    {
+        B200LA_CUDA(cudaStreamWaitEvent(s, ev_r, 0));
     }
     return B200LA_SUCCESS;
 }
@@ -739,13 +785,14 @@ int enqueue_block_rowid(MixedPlan& p, int n, int K, int Kend, cudaStream_t s)
     return B200LA_SUCCESS;
 }
 
-// A stream per device (high priority for the look-ahead panels, low for the
-// interchanges left of a block, which nothing reads before the solve).
-cudaStream_t lookahead_stream(int* rc, bool high = true)
+// A stream per device and slot (high priority for the look-ahead panels and,
+// slot 1, the rest of each panel's block work; low for the interchanges left
+// of a block, which nothing reads before the solve).
+cudaStream_t lookahead_stream(int* rc, bool high = true, int slot = 0)
 {
     static std::mutex   m;
-    static cudaStream_t all_streams[2][64] = {};
-    cudaStream_t*       streams            = all_streams[high ? 0 : 1];
+    static cudaStream_t all_streams[3][64] = {};
+    cudaStream_t*       streams            = all_streams[high ? (slot != 0 ? 2 : 0) : 1];
     int                 dev         = 0;
     *rc                             = B200LA_SUCCESS;
     cudaError_t e                   = cudaGetDevice(&dev);
@@ -904,8 +951,9 @@ int enqueue_getrf_mixed(MixedPlan& p, int n, int kind, bool split, cudaStream_t 
                           kTcBN)) != B200LA_SUCCESS)
             return rc;
     }
-    cudaStream_t side = s, left = s;
+    cudaStream_t side = s, left = s, rest_s = nullptr;
     cudaEvent_t  ev_update = nullptr, ev_panels = nullptr, ev_left[2] = {nullptr, nullptr};
+    cudaEvent_t  ev_np = nullptr, ev_nr = nullptr;  // nested look-ahead inside a block
     if (la)
     {
         side = lookahead_stream(&rc);
@@ -914,21 +962,26 @@ int enqueue_getrf_mixed(MixedPlan& p, int n, int kind, bool split, cudaStream_t 
         left = lookahead_stream(&rc, false);
         if (rc != B200LA_SUCCESS)
             return rc;
+        rest_s = lookahead_stream(&rc, true, 1);
+        if (rc != B200LA_SUCCESS)
+            return rc;
         B200LA_CUDA(cudaEventCreateWithFlags(&ev_update, cudaEventDisableTiming));
         B200LA_CUDA(cudaEventCreateWithFlags(&ev_panels, cudaEventDisableTiming));
         B200LA_CUDA(cudaEventCreateWithFlags(&ev_left[0], cudaEventDisableTiming));
         B200LA_CUDA(cudaEventCreateWithFlags(&ev_left[1], cudaEventDisableTiming));
+        B200LA_CUDA(cudaEventCreateWithFlags(&ev_np, cudaEventDisableTiming));
+        B200LA_CUDA(cudaEventCreateWithFlags(&ev_nr, cudaEventDisableTiming));
     }
     struct EventGuard
     {
-        cudaEvent_t e[4];
+        cudaEvent_t e[6];
         ~EventGuard()
         {
             for (cudaEvent_t x : e)
                 if (x)
                     cudaEventDestroy(x);
         }
-    } guard{{ev_update, ev_panels, ev_left[0], ev_left[1]}};
+    } guard{{ev_update, ev_panels, ev_left[0], ev_left[1], ev_np, ev_nr}};
     // interchanges left of block K once its panels are done (`done_on`:
     // where they ran); the event guards the interchange lists' slot
     auto left_swaps = [&](int K, int Kend, cudaStream_t done_on) -> int {
@@ -947,7 +1000,8 @@ int enqueue_getrf_mixed(MixedPlan& p, int n, int kind, bool split, cudaStream_t 
     };
 
     float* a32 = p.a32;
-    if ((rc = enqueue_block_panels(p, n, 0, n < kOuterNB ? n : kOuterNB, cl, gmax, s)) != B200LA_SUCCESS)
+    if ((rc = enqueue_block_panels(p, n, 0, n < kOuterNB ? n : kOuterNB, cl, gmax, s, rest_s, ev_np, ev_nr)) !=
+        B200LA_SUCCESS)
         return rc;
     bool panels_on_side = false;
     for (int K = 0; K < n; K += kOuterNB)
@@ -991,7 +1045,7 @@ int enqueue_getrf_mixed(MixedPlan& p, int n, int kind, bool split, cudaStream_t 
             {
                 B200LA_CUDA(cudaStreamWaitEvent(side, ev_left[((K / kOuterNB) + 1) & 1], 0));
             }
-            if ((rc = enqueue_block_panels(p, n, Kend, Kend2, cl, gmax, side)) != B200LA_SUCCESS)
+            if ((rc = enqueue_block_panels(p, n, Kend, Kend2, cl, gmax, side, rest_s, ev_np, ev_nr)) != B200LA_SUCCESS)
                 return rc;
             B200LA_CUDA(cudaEventRecord(ev_panels, side));
             panels_on_side = true;
@@ -1017,7 +1071,7 @@ int enqueue_getrf_mixed(MixedPlan& p, int n, int kind, bool split, cudaStream_t 
             {
                 B200LA_CUDA(cudaStreamWaitEvent(s, ev_left[((K / kOuterNB) + 1) & 1], 0));
             }
-            if ((rc = enqueue_block_panels(p, n, Kend, Kend2, cl, gmax, s)) != B200LA_SUCCESS)
+            if ((rc = enqueue_block_panels(p, n, Kend, Kend2, cl, gmax, s, rest_s, ev_np, ev_nr)) != B200LA_SUCCESS)
                 return rc;
             if (la)
             {
@@ -1054,6 +1108,8 @@ int set_mixed_attributes()
     B200LA_CUDA(cudaFuncSetAttribute(k_outer_u12<TC_FP8, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)outer_u12_smem()));
     B200LA_CUDA(cudaFuncSetAttribute(k_trsv_refine<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTrInvSmem));
     B200LA_CUDA(cudaFuncSetAttribute(k_trsv_refine<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTrInvSmem));
+    B200LA_CUDA(cudaFuncSetAttribute(k_trsm_refine<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tm_smem_bytes<float>()));
+    B200LA_CUDA(cudaFuncSetAttribute(k_trsm_refine<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tm_smem_bytes<double>()));
     B200LA_CUDA(cudaFuncSetAttribute(k_invert_diag_blocks128<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTrInvSmem));
     B200LA_CUDA(cudaFuncSetAttribute(k_invert_diag_blocks128<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTrInvSmem));
     if (dev >= 0 && dev < 64)
@@ -1082,6 +1138,22 @@ int enqueue_lu_apply(const TA* lu, const int32_t* perm, int n, int nrhs, double*
             prof_begin(KC_SOLVE, s);
             k_trsv_refine<TA><<<nb, kTrThreads, kTrInvSmem, s>>>(lu, n, p.y, n, pass, p.dinv, p.xll, epoch,
                 reinterpret_cast<int32_t*>(p.tsync), st, kWaitLimitNs);
+            prof_end(KC_SOLVE, s);
+            B200LA_LAUNCH_CHECK();
+        }
+    }
+    else if (nrhs <= kTmRhs)
+    {
+        // one launch per triangle, all right-hand sides per 128-row block;
+        // flags[] (one word per block) live in the flagged-word buffer
+        const int nb = (n + kTrRows - 1) / kTrRows;
+        for (int pass = 0; pass < 2; ++pass)
+        {
+            B200LA_CUDA(cudaMemsetAsync(p.tsync, 0, sizeof(int32_t), s));
+            const uint32_t epoch = tv_next_epoch();
+            prof_begin(KC_SOLVE, s);
+            k_trsm_refine<TA><<<nb, kTmThreads, tm_smem_bytes<TA>(), s>>>(lu, n, p.y, n, nrhs, pass, p.dinv,
+                reinterpret_cast<uint32_t*>(p.xll), epoch, reinterpret_cast<int32_t*>(p.tsync), st, kWaitLimitNs);
             prof_end(KC_SOLVE, s);
             B200LA_LAUNCH_CHECK();
         }

@@ -634,4 +634,208 @@ __global__ void __launch_bounds__(kTrThreads, 1) k_trsv_refine(const TA* __restr
     }
 }
 
+// X <- T^-1 X for the unit-lower (upper = 0) or upper triangle of the factor
+// `a` (FP32 or FP64 values, FP64 arithmetic), nrhs <= 64 right-hand sides
+// stored row-major (n x nrhs, row stride nrhs), for the refinement's
+// corrections of several right-hand sides.  One launch per triangle: CTA =
+// one 128-row block, claimed by ticket in solve order; thread (i, j) keeps
+// the 4 x 4 products of rows 4i..4i+3 and right-hand sides 4j..4j+3.  For
+// each solved block the CTA stages its 128 x 128 tile of the factor in
+// shared memory, then waits (thread 0, bounded by wait_ns) for that block's
+// flag, reads the block's solved rows (L2, not L1: other SMs wrote them) and
+// multiplies; the block's own rows are the inverse diagonal block
+// (k_invert_diag_blocks128) times (B - products), applied in two 64-column
+// halves.  A solved block is stored to x, fenced, and published by a release
+// store of the call's epoch into flags[block].
+constexpr int    kTmRhs     = 64;
+constexpr int    kTmThreads = 512;
+constexpr int    kTmLd      = kTrRows + 4;  // factor tile row stride (16-byte rows)
+constexpr int    kTmDLd     = 68;           // inverse half-tile row stride (doubles)
+template <typename TA> constexpr size_t tm_tile_bytes()
+{
+    return sizeof(TA) * kTrRows * kTmLd > sizeof(double) * kTrRows * kTmDLd ? sizeof(TA) * kTrRows * kTmLd
+                                                                           : sizeof(double) * kTrRows * kTmDLd;
+}
+template <typename TA> constexpr size_t tm_smem_bytes()
+{
+    return sizeof(double) * kTrRows * kTmRhs + tm_tile_bytes<TA>();
+}
+
+template <typename TA>
+__global__ void __launch_bounds__(kTmThreads, 1) k_trsm_refine(const TA* __restrict__ a, int64_t lda,
+    double* __restrict__ x, int n, int nrhs, int upper, const double* __restrict__ dinv,
+    uint32_t* __restrict__ flags, uint32_t epoch, int32_t* __restrict__ ticket, DeviceStatus* st, uint64_t wait_ns)
+{
+    extern __shared__ __align__(16) unsigned char tm_smem[];
+    double*     Xs = reinterpret_cast<double*>(tm_smem);                                   // [128][64]
+    TA*         Ls = reinterpret_cast<TA*>(tm_smem + sizeof(double) * kTrRows * kTmRhs);  // [128][kTmLd]
+    double*     Ds = reinterpret_cast<double*>(Ls);                                      // [128][kTmDLd]
+    __shared__ int s_t, s_abort;
+    const int      nb  = (n + kTrRows - 1) / kTrRows;
+    const int      tid = threadIdx.x;
+    const int      ti  = tid >> 4;  // rows 4 ti .. 4 ti + 3
+    const int      tj  = tid & 15;  // right-hand sides 4 tj .. 4 tj + 3
+    if (tid == 0)
+    {
+        s_t     = atomicAdd(ticket, 1);
+        s_abort = 0;
+    }
+    __syncthreads();
+    const int t = s_t;
+    if (t >= nb)
+    {
+        return;
+    }
+    const int  blk = upper ? nb - 1 - t : t;
+    const int  r0  = blk * kTrRows;
+    const int  br  = min(kTrRows, n - r0);
+    constexpr int V   = 16 / (int)sizeof(TA);
+    const bool vec = (lda % V) == 0 && (reinterpret_cast<uintptr_t>(a) % 16) == 0;
+    double     acc[4][4];
+#pragma unroll
+    for (int m = 0; m < 4; ++m)
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+            acc[m][q] = 0.0;
+    auto product = [&](const auto* S, int lds, int kcount, int xrow0) {
+#pragma unroll 4
+        for (int kk = 0; kk < kcount; ++kk)
+        {
+            double av[4];
+#pragma unroll
+            for (int m = 0; m < 4; ++m)
+                av[m] = (double)S[(4 * ti + m) * lds + kk];
+            const double2 x01 = *reinterpret_cast<const double2*>(Xs + (xrow0 + kk) * kTmRhs + 4 * tj);
+            const double2 x23 = *reinterpret_cast<const double2*>(Xs + (xrow0 + kk) * kTmRhs + 4 * tj + 2);
+#pragma unroll
+            for (int m = 0; m < 4; ++m)
+            {
+                acc[m][0] = fma(av[m], x01.x, acc[m][0]);
+                acc[m][1] = fma(av[m], x01.y, acc[m][1]);
+                acc[m][2] = fma(av[m], x23.x, acc[m][2]);
+                acc[m][3] = fma(av[m], x23.y, acc[m][3]);
+            }
+        }
+    };
+    for (int s = 0; s < t; ++s)
+    {
+        const int jb = upper ? nb - 1 - s : s;
+        const int c0 = jb * kTrRows;
+        const int cw = min(kTrRows, n - c0);
+        __syncthreads();  // the previous tile's reads are done
+        // the factor tile: rows r0.., columns c0.. (zeros outside)
+        for (int e = tid; e < kTrRows * (kTrRows / V); e += kTmThreads)
+        {
+            const int row = e / (kTrRows / V);
+            const int col = (e - row * (kTrRows / V)) * V;
+            TA        v[V];
+            const TA* src = a + (int64_t)(r0 + (row < br ? row : 0)) * lda + c0 + col;
+            if (row < br && vec && col + V <= cw)
+            {
+                if constexpr (sizeof(TA) == 4)
+                {
+                    const float4 q = __ldg(reinterpret_cast<const float4*>(src));
+                    v[0] = q.x, v[1] = q.y, v[2] = q.z, v[3] = q.w;
+                }
+                else
+                {
+                    const double2 q = __ldg(reinterpret_cast<const double2*>(src));
+                    v[0] = q.x, v[1] = q.y;
+                }
+            }
+            else
+            {
+#pragma unroll
+                for (int u = 0; u < V; ++u)
+                    v[u] = (row < br && col + u < cw) ? src[u] : TA(0);
+            }
+#pragma unroll
+            for (int u = 0; u < V; ++u)
+                Ls[row * kTmLd + col + u] = v[u];
+        }
+        if (tid == 0)
+        {
+            const uint64_t t0    = global_ns();
+            uint32_t       polls = 0;
+            for (;;)
+            {
+                uint32_t f;
+                asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(f) : "l"(flags + jb) : "memory");
+                if (f == epoch)
+                {
+                    break;
+                }
+                if ((++polls & 255u) == 0 && global_ns() - t0 > wait_ns)
+                {
+                    raise_error(st, DEV_WAIT_TIMEOUT, 22);
+                    s_abort = 1;
+                    break;
+                }
+            }
+        }
+        __syncthreads();
+        if (s_abort)
+        {
+            return;
+        }
+        for (int e = tid; e < kTrRows * kTmRhs; e += kTmThreads)
+        {
+            const int row = e / kTmRhs, q = e - row * kTmRhs;
+            Xs[e]         = (row < cw && q < nrhs) ? __ldcg(x + (size_t)(c0 + row) * nrhs + q) : 0.0;
+        }
+        __syncthreads();
+        product(Ls, kTmLd, kTrRows, 0);
+    }
+    __syncthreads();
+    // V = B - products, in Xs
+#pragma unroll
+    for (int m = 0; m < 4; ++m)
+    {
+        const int row = 4 * ti + m;
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+        {
+            const int c = 4 * tj + q;
+            Xs[row * kTmRhs + c] =
+                (row < br && c < nrhs) ? __ldcg(x + (size_t)(r0 + row) * nrhs + c) - acc[m][q] : 0.0;
+            acc[m][q] = 0.0;
+        }
+    }
+    // X = Dinv V, the inverse in two 64-column halves
+    const double* D = dinv + ((size_t)blk * 2 + (upper ? 1 : 0)) * kTrRows * kTrRows;
+    for (int h = 0; h < 2; ++h)
+    {
+        __syncthreads();
+        for (int e = tid; e < kTrRows * 32; e += kTmThreads)
+        {
+            const int     row = e >> 5, c2 = (e & 31) * 2;
+            const double2 v   = __ldg(reinterpret_cast<const double2*>(D + (size_t)row * kTrRows + h * 64 + c2));
+            Ds[row * kTmDLd + c2]     = v.x;
+            Ds[row * kTmDLd + c2 + 1] = v.y;
+        }
+        __syncthreads();
+        product(Ds, kTmDLd, 64, h * 64);
+    }
+#pragma unroll
+    for (int m = 0; m < 4; ++m)
+    {
+        const int row = 4 * ti + m;
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+        {
+            const int c = 4 * tj + q;
+            if (row < br && c < nrhs)
+            {
+                x[(size_t)(r0 + row) * nrhs + c] = acc[m][q];
+            }
+        }
+    }
+    __threadfence();
+    __syncthreads();
+    if (tid == 0)
+    {
+        asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(flags + blk), "r"(epoch) : "memory");
+    }
+}
+
 }  // namespace b200la
