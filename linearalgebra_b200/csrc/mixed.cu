@@ -1108,8 +1108,8 @@ int set_mixed_attributes()
     B200LA_CUDA(cudaFuncSetAttribute(k_outer_u12<TC_FP8, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)outer_u12_smem()));
     B200LA_CUDA(cudaFuncSetAttribute(k_trsv_refine<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTrInvSmem));
     B200LA_CUDA(cudaFuncSetAttribute(k_trsv_refine<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTrInvSmem));
-    B200LA_CUDA(cudaFuncSetAttribute(k_trsm_refine<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tm_smem_bytes<float>()));
-    B200LA_CUDA(cudaFuncSetAttribute(k_trsm_refine<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tm_smem_bytes<double>()));
+    B200LA_CUDA(cudaFuncSetAttribute(k_trsm_refine<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTmSmem));
+    B200LA_CUDA(cudaFuncSetAttribute(k_trsm_refine<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTmSmem));
     B200LA_CUDA(cudaFuncSetAttribute(k_invert_diag_blocks128<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTrInvSmem));
     B200LA_CUDA(cudaFuncSetAttribute(k_invert_diag_blocks128<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTrInvSmem));
     if (dev >= 0 && dev < 64)
@@ -1152,7 +1152,7 @@ int enqueue_lu_apply(const TA* lu, const int32_t* perm, int n, int nrhs, double*
             B200LA_CUDA(cudaMemsetAsync(p.tsync, 0, sizeof(int32_t), s));
             const uint32_t epoch = tv_next_epoch();
             prof_begin(KC_SOLVE, s);
-            k_trsm_refine<TA><<<nb, kTmThreads, tm_smem_bytes<TA>(), s>>>(lu, n, p.y, n, nrhs, pass, p.dinv,
+            k_trsm_refine<TA><<<nb, kTmThreads, kTmSmem, s>>>(lu, n, p.y, n, nrhs, pass, p.dinv,
                 reinterpret_cast<uint32_t*>(p.xll), epoch, reinterpret_cast<int32_t*>(p.tsync), st, kWaitLimitNs);
             prof_end(KC_SOLVE, s);
             B200LA_LAUNCH_CHECK();
@@ -1195,11 +1195,11 @@ int residual_eta(const double* a, int64_t lda, int n, int nrhs, const double* b,
         prof_begin(KC_RESIDUAL, s);
         k_copy2d<double><<<grid_for((int64_t)n * nrhs), 256, 0, s>>>(b, ldb, p.r, nrhs, n, nrhs, nullptr);
         prof_end(KC_RESIDUAL, s);
-        dim3 grid((unsigned)((nrhs + 63) / 64), (unsigned)((n + 127) / 128));
-        prof_begin(KC_RESIDUAL, s);
-        k_gemm<double, false, false><<<grid, 128, gemm_smem_bytes<double>(), s>>>(n, nrhs, n, -1.0, a, lda, x, ldx, 1.0, p.r, nrhs);
-        prof_end(KC_RESIDUAL, s);
-        B200LA_LAUNCH_CHECK();
+        // the FP64 tensor-core GEMM of the multiplication row (its launches
+        // count in the gemm class)
+        const int grc = gemm<double>(0, 0, n, nrhs, n, -1.0, a, lda, x, ldx, 1.0, p.r, nrhs, s);
+        if (grc != B200LA_SUCCESS)
+            return grc;
         prof_begin(KC_RESIDUAL, s);
         k_colmax<<<grid_for((int64_t)n * nrhs), 256, 0, s>>>(p.r, nrhs, n, nrhs, p.norms + 4);
         k_colmax<<<grid_for((int64_t)n * nrhs), 256, 0, s>>>(x, ldx, n, nrhs, p.norms + 4 + kMaxNrhsMixed);

@@ -639,42 +639,36 @@ __global__ void __launch_bounds__(kTrThreads, 1) k_trsv_refine(const TA* __restr
 // stored row-major (n x nrhs, row stride nrhs), for the refinement's
 // corrections of several right-hand sides.  One launch per triangle: CTA =
 // one 128-row block, claimed by ticket in solve order; thread (i, j) keeps
-// the 4 x 4 products of rows 4i..4i+3 and right-hand sides 4j..4j+3.  For
+// the 8 x 4 products of rows 8i..8i+7 and right-hand sides j, j+16, j+32,
+// j+48 (so a warp's reads of a solved row are one broadcast wavefront).  For
 // each solved block the CTA stages its 128 x 128 tile of the factor in
-// shared memory, then waits (thread 0, bounded by wait_ns) for that block's
-// flag, reads the block's solved rows (L2, not L1: other SMs wrote them) and
-// multiplies; the block's own rows are the inverse diagonal block
-// (k_invert_diag_blocks128) times (B - products), applied in two 64-column
-// halves.  A solved block is stored to x, fenced, and published by a release
-// store of the call's epoch into flags[block].
+// shared memory as FP64 (converted once, not per product), then waits
+// (thread 0, bounded by wait_ns) for that block's flag, reads the block's
+// solved rows (L2, not L1: other SMs wrote them) and multiplies; the block's
+// own rows are the inverse diagonal block (k_invert_diag_blocks128) times
+// (B - products), applied in two 64-column halves.  A solved block is stored
+// to x, fenced, and published by a release store of the call's epoch into
+// flags[block].  Row strides of the staged tiles are odd (129, 65 doubles)
+// so the two rows a warp reads fall in different banks.
 constexpr int    kTmRhs     = 64;
-constexpr int    kTmThreads = 512;
-constexpr int    kTmLd      = kTrRows + 4;  // factor tile row stride (16-byte rows)
-constexpr int    kTmDLd     = 68;           // inverse half-tile row stride (doubles)
-template <typename TA> constexpr size_t tm_tile_bytes()
-{
-    return sizeof(TA) * kTrRows * kTmLd > sizeof(double) * kTrRows * kTmDLd ? sizeof(TA) * kTrRows * kTmLd
-                                                                           : sizeof(double) * kTrRows * kTmDLd;
-}
-template <typename TA> constexpr size_t tm_smem_bytes()
-{
-    return sizeof(double) * kTrRows * kTmRhs + tm_tile_bytes<TA>();
-}
+constexpr int    kTmThreads = 256;
+constexpr int    kTmLd      = kTrRows + 1;  // staged factor tile row stride (doubles)
+constexpr int    kTmDLd     = 65;           // staged inverse half-tile row stride (doubles)
+constexpr size_t kTmSmem    = sizeof(double) * kTrRows * kTmRhs + sizeof(double) * kTrRows * kTmLd;
 
 template <typename TA>
 __global__ void __launch_bounds__(kTmThreads, 1) k_trsm_refine(const TA* __restrict__ a, int64_t lda,
     double* __restrict__ x, int n, int nrhs, int upper, const double* __restrict__ dinv,
     uint32_t* __restrict__ flags, uint32_t epoch, int32_t* __restrict__ ticket, DeviceStatus* st, uint64_t wait_ns)
 {
-    extern __shared__ __align__(16) unsigned char tm_smem[];
-    double*     Xs = reinterpret_cast<double*>(tm_smem);                                   // [128][64]
-    TA*         Ls = reinterpret_cast<TA*>(tm_smem + sizeof(double) * kTrRows * kTmRhs);  // [128][kTmLd]
-    double*     Ds = reinterpret_cast<double*>(Ls);                                      // [128][kTmDLd]
+    extern __shared__ __align__(16) double tm_smem[];
+    double*        Xs = tm_smem;                      // [128][64]
+    double*        Ls = tm_smem + kTrRows * kTmRhs;   // [128][kTmLd]; also the inverse halves [128][kTmDLd]
     __shared__ int s_t, s_abort;
     const int      nb  = (n + kTrRows - 1) / kTrRows;
     const int      tid = threadIdx.x;
-    const int      ti  = tid >> 4;  // rows 4 ti .. 4 ti + 3
-    const int      tj  = tid & 15;  // right-hand sides 4 tj .. 4 tj + 3
+    const int      ti  = tid >> 4;  // rows 8 ti .. 8 ti + 7
+    const int      tj  = tid & 15;  // right-hand sides tj + 16 q
     if (tid == 0)
     {
         s_t     = atomicAdd(ticket, 1);
@@ -686,35 +680,33 @@ __global__ void __launch_bounds__(kTmThreads, 1) k_trsm_refine(const TA* __restr
     {
         return;
     }
-    const int  blk = upper ? nb - 1 - t : t;
-    const int  r0  = blk * kTrRows;
-    const int  br  = min(kTrRows, n - r0);
+    const int     blk = upper ? nb - 1 - t : t;
+    const int     r0  = blk * kTrRows;
+    const int     br  = min(kTrRows, n - r0);
     constexpr int V   = 16 / (int)sizeof(TA);
-    const bool vec = (lda % V) == 0 && (reinterpret_cast<uintptr_t>(a) % 16) == 0;
-    double     acc[4][4];
+    const bool    vec = (lda % V) == 0 && (reinterpret_cast<uintptr_t>(a) % 16) == 0;
+    double        acc[8][4];
 #pragma unroll
-    for (int m = 0; m < 4; ++m)
+    for (int m = 0; m < 8; ++m)
 #pragma unroll
         for (int q = 0; q < 4; ++q)
             acc[m][q] = 0.0;
-    auto product = [&](const auto* S, int lds, int kcount, int xrow0) {
-#pragma unroll 4
+    auto product = [&](const double* S, int lds, int kcount, int xrow0) {
+#pragma unroll 2
         for (int kk = 0; kk < kcount; ++kk)
         {
-            double av[4];
+            double av[8], xv[4];
 #pragma unroll
-            for (int m = 0; m < 4; ++m)
-                av[m] = (double)S[(4 * ti + m) * lds + kk];
-            const double2 x01 = *reinterpret_cast<const double2*>(Xs + (xrow0 + kk) * kTmRhs + 4 * tj);
-            const double2 x23 = *reinterpret_cast<const double2*>(Xs + (xrow0 + kk) * kTmRhs + 4 * tj + 2);
+            for (int m = 0; m < 8; ++m)
+                av[m] = S[(8 * ti + m) * lds + kk];
 #pragma unroll
-            for (int m = 0; m < 4; ++m)
-            {
-                acc[m][0] = fma(av[m], x01.x, acc[m][0]);
-                acc[m][1] = fma(av[m], x01.y, acc[m][1]);
-                acc[m][2] = fma(av[m], x23.x, acc[m][2]);
-                acc[m][3] = fma(av[m], x23.y, acc[m][3]);
-            }
+            for (int q = 0; q < 4; ++q)
+                xv[q] = Xs[(xrow0 + kk) * kTmRhs + tj + 16 * q];
+#pragma unroll
+            for (int m = 0; m < 8; ++m)
+#pragma unroll
+                for (int q = 0; q < 4; ++q)
+                    acc[m][q] = fma(av[m], xv[q], acc[m][q]);
         }
     };
     for (int s = 0; s < t; ++s)
@@ -723,7 +715,7 @@ __global__ void __launch_bounds__(kTmThreads, 1) k_trsm_refine(const TA* __restr
         const int c0 = jb * kTrRows;
         const int cw = min(kTrRows, n - c0);
         __syncthreads();  // the previous tile's reads are done
-        // the factor tile: rows r0.., columns c0.. (zeros outside)
+        // the factor tile: rows r0.., columns c0.. (zeros outside), as FP64
         for (int e = tid; e < kTrRows * (kTrRows / V); e += kTmThreads)
         {
             const int row = e / (kTrRows / V);
@@ -751,7 +743,7 @@ __global__ void __launch_bounds__(kTmThreads, 1) k_trsm_refine(const TA* __restr
             }
 #pragma unroll
             for (int u = 0; u < V; ++u)
-                Ls[row * kTmLd + col + u] = v[u];
+                Ls[row * kTmLd + col + u] = (double)v[u];
         }
         if (tid == 0)
         {
@@ -789,13 +781,13 @@ __global__ void __launch_bounds__(kTmThreads, 1) k_trsm_refine(const TA* __restr
     __syncthreads();
     // V = B - products, in Xs
 #pragma unroll
-    for (int m = 0; m < 4; ++m)
+    for (int m = 0; m < 8; ++m)
     {
-        const int row = 4 * ti + m;
+        const int row = 8 * ti + m;
 #pragma unroll
         for (int q = 0; q < 4; ++q)
         {
-            const int c = 4 * tj + q;
+            const int c = tj + 16 * q;
             Xs[row * kTmRhs + c] =
                 (row < br && c < nrhs) ? __ldcg(x + (size_t)(r0 + row) * nrhs + c) - acc[m][q] : 0.0;
             acc[m][q] = 0.0;
@@ -810,20 +802,20 @@ __global__ void __launch_bounds__(kTmThreads, 1) k_trsm_refine(const TA* __restr
         {
             const int     row = e >> 5, c2 = (e & 31) * 2;
             const double2 v   = __ldg(reinterpret_cast<const double2*>(D + (size_t)row * kTrRows + h * 64 + c2));
-            Ds[row * kTmDLd + c2]     = v.x;
-            Ds[row * kTmDLd + c2 + 1] = v.y;
+            Ls[row * kTmDLd + c2]     = v.x;
+            Ls[row * kTmDLd + c2 + 1] = v.y;
         }
         __syncthreads();
-        product(Ds, kTmDLd, 64, h * 64);
+        product(Ls, kTmDLd, 64, h * 64);
     }
 #pragma unroll
-    for (int m = 0; m < 4; ++m)
+    for (int m = 0; m < 8; ++m)
     {
-        const int row = 4 * ti + m;
+        const int row = 8 * ti + m;
 #pragma unroll
         for (int q = 0; q < 4; ++q)
         {
-            const int c = 4 * tj + q;
+            const int c = tj + 16 * q;
             if (row < br && c < nrhs)
             {
                 x[(size_t)(r0 + row) * nrhs + c] = acc[m][q];
