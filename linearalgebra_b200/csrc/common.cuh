@@ -24,6 +24,7 @@ enum DeviceError : int32_t
     DEV_OK           = 0,
     DEV_WAIT_TIMEOUT = 1,  // a bounded inter-CTA wait gave up
     DEV_BAD_PIVOT    = 2,  // a pivot entry outside [i+1, n] was supplied
+    DEV_BAD_INPUT    = 3,  // a launch broke a kernel's precondition (the kernel skipped the work)
 };
 
 struct alignas(64) DeviceStatus

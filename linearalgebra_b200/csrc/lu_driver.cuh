@@ -21,9 +21,9 @@ namespace b200la
 int require_sm100();
 
 constexpr size_t kPanelSmemMax = 200 * 1024;
-// dynamic shared memory of the cluster panel: sm_100's 227 KB per CTA less
-// 6 KB for its static arrays
-constexpr size_t kClusterSmemMax = 227 * 1024 - 6 * 1024;
+// dynamic shared memory of the 64-column cluster panel (the probe's kernel):
+// sm_100's 227 KB per CTA less 6 KB for its static arrays
+constexpr size_t kClusterSmemMax = cluster_dyn_max<double, 64>();
 constexpr int    kLeanPanelCtas = 48;  // grid panel CTAs beside a concurrent trailing update
 
 
@@ -78,10 +78,10 @@ template <typename T> int ensure_kernel_attributes()
     B200LA_CUDA(cudaFuncSetAttribute(
         k_perm_from_pivots<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
     B200LA_CUDA(cudaFuncSetAttribute(
-        k_panel_cluster<T, 64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kClusterSmemMax));
+        k_panel_cluster<T, 64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cluster_dyn_max<T, 64>()));
     B200LA_CUDA(cudaFuncSetAttribute(k_panel_cluster<T, 64>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
     B200LA_CUDA(cudaFuncSetAttribute(
-        k_panel_cluster<T, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kClusterSmemMax));
+        k_panel_cluster<T, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cluster_dyn_max<T, 32>()));
     B200LA_CUDA(cudaFuncSetAttribute(k_panel_cluster<T, 32>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
     B200LA_CUDA(cudaFuncSetAttribute(
         k_panel_exchange_floor<T, 64>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
@@ -212,13 +212,28 @@ template <typename T> bool cluster_panel_fits(int rows, int w, int cl)
         return false;
     }
     const size_t rpc = (size_t)((rows + cl - 1) / cl);
-    return rpc * (w <= 32 ? cluster_row_bytes<T, 32>() : cluster_row_bytes<T, 64>()) <= kClusterSmemMax;
+    return w <= 32 ? rpc * cluster_row_bytes<T, 32>() <= cluster_dyn_max<T, 32>()
+                   : rpc * cluster_row_bytes<T, 64>() <= cluster_dyn_max<T, 64>();
 }
 
+// Whether launch_panel takes the fusing cluster kernel for this panel and
+// can apply a previous panel of width prev_w first (both at most 32 wide).
+template <typename T> bool panel_can_fuse(int rows, int w, int prev_w, int cl)
+{
+    return cluster_fuses<T, 32>() && w <= 32 && prev_w >= 1 && prev_w <= 32 && cluster_panel_fits<T>(rows, w, cl);
+}
+
+// pperm / pk: the previous panel's interchange list and first column, whose
+// interchanges, U12 and update on this panel's columns the panel kernel then
+// applies first (only where panel_can_fuse; an error otherwise).
 template <typename T>
 int launch_panel(T* m, int n, int k, int w, int64_t* pivot, const GetrfPlan<T>& p, int cl, int gmax,
-    cudaStream_t s, bool lean = false)
+    cudaStream_t s, bool lean = false, const PermList* pperm = nullptr, int pk = -1)
 {
+    if (pperm != nullptr && !panel_can_fuse<T>(n - k, w, k - pk, cl))
+    {
+        return set_error(B200LA_NOT_SUPPORTED, "panel: the fused update needs the FP32 32-column cluster kernel");
+    }
     const int R = n - k;
     PanelWs<T> ws{p.hdr, p.payload, p.diag, p.perm};
     DeviceStatus* st = p.st;
@@ -241,11 +256,13 @@ int launch_panel(T* m, int n, int k, int w, int64_t* pivot, const GetrfPlan<T>& 
         prof_begin(KC_PANEL, s);
         if (w <= 32)
         {
-            B200LA_CUDA(cudaLaunchKernelEx(&cfg, k_panel_cluster<T, 32>, m, n, k, w, rpc, pivot, p.perm, p.st));
+            B200LA_CUDA(cudaLaunchKernelEx(&cfg, k_panel_cluster<T, 32>, m, n, k, w, rpc, pivot, p.perm, p.st,
+                pperm, pk));
         }
         else
         {
-            B200LA_CUDA(cudaLaunchKernelEx(&cfg, k_panel_cluster<T, 64>, m, n, k, w, rpc, pivot, p.perm, p.st));
+            B200LA_CUDA(cudaLaunchKernelEx(&cfg, k_panel_cluster<T, 64>, m, n, k, w, rpc, pivot, p.perm, p.st,
+                (const PermList*)nullptr, -1));
         }
         prof_end(KC_PANEL, s);
         return B200LA_SUCCESS;

@@ -875,10 +875,21 @@ template <typename T, int W> struct alignas(16) ClusterPost
 
 template <typename T, int W> constexpr int cluster_ldl() { return W + 16 / (int)sizeof(T); }
 template <typename T, int W> constexpr size_t cluster_row_bytes() { return (size_t)cluster_ldl<T, W>() * sizeof(T); }
+// The FP32 32-column kernel (the mixed factorization's) can start with the
+// previous panel's interchanges, U12 and update of its own columns; it holds
+// that panel's L11 and U12 in 8.3 KB more static shared memory.
+template <typename T, int W> constexpr bool cluster_fuses() { return W == 32 && sizeof(T) == 4; }
+// Dynamic shared memory of k_panel_cluster<T, W>: 227 KB less its static
+// arrays (6 KB; 14 KB for the fusing kernel).
+template <typename T, int W> constexpr size_t cluster_dyn_max()
+{
+    return cluster_fuses<T, W>() ? 227 * 1024 - 14 * 1024 : 227 * 1024 - 6 * 1024;
+}
 
 template <typename T, int W>
 __global__ void __launch_bounds__(kPanelThreads, 1) k_panel_cluster(T* __restrict__ A, int n, int k, int w,
-    int rows_per_cta, int64_t* __restrict__ pivot, PermList* __restrict__ perm, DeviceStatus* __restrict__ st)
+    int rows_per_cta, int64_t* __restrict__ pivot, PermList* __restrict__ perm, DeviceStatus* __restrict__ st,
+    const PermList* __restrict__ pperm, int pk)
 {
     using K             = typename PivKey<T>::type;
     using VT            = typename Vec16<T>::type;
@@ -896,6 +907,9 @@ __global__ void __launch_bounds__(kPanelThreads, 1) k_panel_cluster(T* __restric
     __shared__ int               red_row[WARPS];
     __shared__ int               piv_loc[W];
     __shared__ int               s_p;
+    constexpr int                FZ = cluster_fuses<T, W>() ? 32 : 1;
+    __shared__ __align__(16) T   fz_l[FZ][FZ + 1];  // the previous panel's L11
+    __shared__ __align__(16) T   fz_u[FZ][FZ];      // its U12 for this panel's columns
 
     const int      tid  = threadIdx.x;
     const int      lane = tid & 31;
@@ -921,6 +935,145 @@ __global__ void __launch_bounds__(kPanelThreads, 1) k_panel_cluster(T* __restric
     T* loc = reinterpret_cast<T*>(smem_raw);
     panel_slice_copy<T, true>(loc, LDL, A, n, r0, k, nloc, w);
     __syncthreads();
+
+    // With pperm: this panel's columns have not yet received the previous
+    // panel's (columns [pk, k)) interchanges, U12 and update; apply them here
+    // with the arithmetic of k_laswp_trsm and k_trailing (U12 row i takes rows
+    // 0..i-1 in order; each element's products summed from zero in order,
+    // then subtracted), so the factors are bit-identical to the unfused path.
+    if constexpr (FZ == 32)
+    {
+        if (pperm != nullptr && (k - pk < 1 || k - pk > 32))
+        {
+            if (tid == 0)
+            {
+                raise_error(st, DEV_BAD_INPUT, 30);  // the host only fuses panels up to 32 wide
+            }
+        }
+        else if (pperm != nullptr)
+        {
+            const int pw  = k - pk;
+            const int cnt = pperm->count;
+            // rows of this CTA that the interchanges replace: their sources'
+            // values, from global memory (not yet interchanged there)
+            for (int q = pw + warp; q < cnt; q += WARPS)
+            {
+                const int dst = pperm->dst[q], src = pperm->src[q];
+                if (dst != src && dst >= r0 && dst < r0 + nloc)
+                {
+                    for (int j = lane; j < w; j += 32)
+                    {
+                        loc[(size_t)(dst - r0) * LDL + j] = A[(size_t)src * n + k + j];
+                    }
+                }
+            }
+            // L11 of the previous panel, and its rows' new contents here
+            for (int e = tid; e < pw * pw; e += kPanelThreads)
+            {
+                const int i = e / pw, m = e - i * pw;
+                fz_l[i][m]  = A[(size_t)(pk + i) * n + pk + m];
+            }
+            for (int e = tid; e < 32 * 32; e += kPanelThreads)
+            {
+                const int i = e >> 5, c = e & 31;
+                fz_u[i][c]  = (i < pw && c < w) ? A[(size_t)pperm->src[i] * n + k + c] : T(0);
+            }
+            __syncthreads();
+            // U12 = L11^-1 (those rows), one thread per column
+            if (tid < 32)
+            {
+                T u[32];
+#pragma unroll
+                for (int i = 0; i < 32; ++i)
+                {
+                    u[i] = fz_u[i][tid];
+                }
+#pragma unroll
+                for (int pp = 0; pp < 31; ++pp)
+                {
+#pragma unroll
+                    for (int i = pp + 1; i < 32; ++i)
+                    {
+                        if (i < pw)
+                        {
+                            u[i] = fma(-fz_l[i][pp], u[pp], u[i]);
+                        }
+                    }
+                }
+#pragma unroll
+                for (int i = 0; i < 32; ++i)
+                {
+                    fz_u[i][tid] = u[i];
+                }
+            }
+            __syncthreads();
+            if (b == 0)
+            {
+                for (int e = tid; e < pw * w; e += kPanelThreads)
+                {
+                    const int i = e / w, c = e - i * w;
+                    A[(size_t)(pk + i) * n + k + c] = fz_u[i][c];
+                }
+            }
+            // this CTA's rows -= L21 U12 (L21: the previous panel's final
+            // rows, in global memory); a thread per row, all 32 columns
+            const bool lvec = (n % 4) == 0 && (pk % 4) == 0 && (reinterpret_cast<uintptr_t>(A) & 15) == 0;
+            for (int r = tid; r < nloc; r += kPanelThreads)
+            {
+                const T* lr = A + (size_t)(r0 + r) * n + pk;
+                T        lv[32];
+                if (lvec && pw == 32)
+                {
+#pragma unroll
+                    for (int m = 0; m < 32; m += 4)
+                    {
+                        const float4 q = *reinterpret_cast<const float4*>(lr + m);
+                        lv[m] = q.x, lv[m + 1] = q.y, lv[m + 2] = q.z, lv[m + 3] = q.w;
+                    }
+                }
+                else
+                {
+#pragma unroll
+                    for (int m = 0; m < 32; ++m)
+                    {
+                        lv[m] = m < pw ? lr[m] : T(0);
+                    }
+                }
+                T acc[32];
+#pragma unroll
+                for (int c = 0; c < 32; ++c)
+                {
+                    acc[c] = T(0);
+                }
+#pragma unroll
+                for (int m = 0; m < 32; ++m)
+                {
+                    if (m < pw)
+                    {
+#pragma unroll
+                        for (int c = 0; c < 32; c += 4)
+                        {
+                            const float4 uq = *reinterpret_cast<const float4*>(&fz_u[m][c]);
+                            acc[c]          = fma(lv[m], uq.x, acc[c]);
+                            acc[c + 1]      = fma(lv[m], uq.y, acc[c + 1]);
+                            acc[c + 2]      = fma(lv[m], uq.z, acc[c + 2]);
+                            acc[c + 3]      = fma(lv[m], uq.w, acc[c + 3]);
+                        }
+                    }
+                }
+                T* row = loc + (size_t)r * LDL;
+#pragma unroll
+                for (int c = 0; c < 32; ++c)
+                {
+                    if (c < w)
+                    {
+                        row[c] = row[c] - acc[c];
+                    }
+                }
+            }
+            __syncthreads();
+        }
+    }
 
     {
         K   ck = 0;

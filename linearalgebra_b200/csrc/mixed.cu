@@ -680,16 +680,17 @@ bool nested_enabled()
 // block by enqueue_block_swaps), U12 inside the block and the SIMT updates
 // inside the block.  Panel j's interchange list goes to block_perms(p, K)[j].
 //
-// With a second stream `rs` (and two events), the work after panel j is
-// split: the next panel's columns (interchanges, U12, update) stay on `s`
-// right behind the panel, and the block's other columns (the interchanges
-// left of the panel and the columns after the next panel) go to `rs`, so
-// panel j + 1 starts as soon as its own columns are ready.  The two streams
-// touch disjoint columns; the next panel's columns were last written by the
-// rest of panel j - 1, which `s` waits for first.  `s` waits for the block's
-// last rest before it returns.
+// With a second stream `rs` and the events ev_p, ev_r[2] (nested
+// look-ahead), the work after panel j is split: the next panel's columns
+// (interchanges, U12, update) are applied by the next panel kernel itself
+// when it is the FP32 32-column cluster kernel (else by the two kernels
+// right before it on `s`), and the block's other columns (the interchanges
+// left of the panel, the columns after the next panel) go to `rs`, so panel
+// j + 1 starts as soon as panel j is done and the rest of panel j - 1 has
+// reached its columns.  The streams touch disjoint columns; `s` waits for
+// the block's last rest before it returns.
 int enqueue_block_panels(MixedPlan& p, int n, int K, int Kend, int cl, int gmax, cudaStream_t s,
-    cudaStream_t rs = nullptr, cudaEvent_t ev_p = nullptr, cudaEvent_t ev_r = nullptr)
+    cudaStream_t rs = nullptr, cudaEvent_t ev_p = nullptr, cudaEvent_t* ev_r = nullptr)
 {
     float*     a32  = p.a32;
     int        rc   = B200LA_SUCCESS;
@@ -716,42 +717,53 @@ int enqueue_block_panels(MixedPlan& p, int n, int K, int Kend, int cl, int gmax,
             prof_end(KC_TRAILING, st);
         }
     };
+    int last = -1;
     for (int k = K, j = 0; k < Kend; k += pw, ++j)
     {
         const int        w  = Kend - k < pw ? Kend - k : pw;
         GetrfPlan<float> gp = p.gp;
         gp.perm             = block_perms(p, K) + j;
-        if ((rc = launch_panel<float>(a32, n, k, w, p.piv, gp, cl, gmax, s)) != B200LA_SUCCESS)
-            return rc;
-        const int kn  = k + w;                              // the next panel's columns [kn, kn2)
-        const int kn2 = kn + pw < Kend ? kn + pw : Kend;
+        const int kn        = k + w;  // the next panel's columns [kn, kn2)
+        const int kn2       = kn + pw < Kend ? kn + pw : Kend;
         if (!nest)
         {
+            if ((rc = launch_panel<float>(a32, n, k, w, p.piv, gp, cl, gmax, s)) != B200LA_SUCCESS)
+                return rc;
             swaps(gp.perm, k, w, k - K, kn, Kend, s);
             B200LA_LAUNCH_CHECK();
             update(k, w, 0, Kend - kn, s);
             B200LA_LAUNCH_CHECK();
             continue;
         }
-        B200LA_CUDA(cudaEventRecord(ev_p, s));
-        if (j > 0)
+        if (j >= 2)
         {
-            B200LA_CUDA(cudaStreamWaitEvent(s, ev_r, 0));  // the rest of panel j - 1
+            B200LA_CUDA(cudaStreamWaitEvent(s, ev_r[j & 1], 0));  // the rest of panel j - 2
         }
-        swaps(gp.perm, k, w, 0, kn, kn2, s);
-        B200LA_LAUNCH_CHECK();
-        update(k, w, 0, kn2 - kn, s);
-        B200LA_LAUNCH_CHECK();
+        const PermList* prev = j >= 1 ? block_perms(p, K) + (j - 1) : nullptr;
+        const bool      fuse = prev != nullptr && panel_can_fuse<float>(n - k, w, pw, cl);
+        if (prev != nullptr && !fuse)
+        {
+            // panel j - 1's work on this panel's columns, before it
+            swaps(prev, k - pw, pw, 0, k, kn, s);
+            B200LA_LAUNCH_CHECK();
+            update(k - pw, pw, 0, w, s);
+            B200LA_LAUNCH_CHECK();
+        }
+        if ((rc = launch_panel<float>(a32, n, k, w, p.piv, gp, cl, gmax, s, false, fuse ? prev : nullptr,
+                 fuse ? k - pw : -1)) != B200LA_SUCCESS)
+            return rc;
+        B200LA_CUDA(cudaEventRecord(ev_p, s));
         B200LA_CUDA(cudaStreamWaitEvent(rs, ev_p, 0));
         swaps(gp.perm, k, w, k - K, kn2, Kend, rs);
         B200LA_LAUNCH_CHECK();
         update(k, w, kn2 - kn, Kend - kn2, rs);
         B200LA_LAUNCH_CHECK();
-        B200LA_CUDA(cudaEventRecord(ev_r, rs));
+        B200LA_CUDA(cudaEventRecord(ev_r[j & 1], rs));
+        last = j;
     }
-    if (nest)
+    if (nest && last >= 0)
     {
-        B200LA_CUDA(cudaStreamWaitEvent(s, ev_r, 0));
+        B200LA_CUDA(cudaStreamWaitEvent(s, ev_r[last & 1], 0));
     }
     return B200LA_SUCCESS;
 }
@@ -953,7 +965,7 @@ int enqueue_getrf_mixed(MixedPlan& p, int n, int kind, bool split, cudaStream_t 
     }
     cudaStream_t side = s, left = s, rest_s = nullptr;
     cudaEvent_t  ev_update = nullptr, ev_panels = nullptr, ev_left[2] = {nullptr, nullptr};
-    cudaEvent_t  ev_np = nullptr, ev_nr = nullptr;  // nested look-ahead inside a block
+    cudaEvent_t  ev_np = nullptr, ev_nr[2] = {nullptr, nullptr};  // nested look-ahead inside a block
     if (la)
     {
         side = lookahead_stream(&rc);
@@ -970,18 +982,19 @@ int enqueue_getrf_mixed(MixedPlan& p, int n, int kind, bool split, cudaStream_t 
         B200LA_CUDA(cudaEventCreateWithFlags(&ev_left[0], cudaEventDisableTiming));
         B200LA_CUDA(cudaEventCreateWithFlags(&ev_left[1], cudaEventDisableTiming));
         B200LA_CUDA(cudaEventCreateWithFlags(&ev_np, cudaEventDisableTiming));
-        B200LA_CUDA(cudaEventCreateWithFlags(&ev_nr, cudaEventDisableTiming));
+        B200LA_CUDA(cudaEventCreateWithFlags(&ev_nr[0], cudaEventDisableTiming));
+        B200LA_CUDA(cudaEventCreateWithFlags(&ev_nr[1], cudaEventDisableTiming));
     }
     struct EventGuard
     {
-        cudaEvent_t e[6];
+        cudaEvent_t e[7];
         ~EventGuard()
         {
             for (cudaEvent_t x : e)
                 if (x)
                     cudaEventDestroy(x);
         }
-    } guard{{ev_update, ev_panels, ev_left[0], ev_left[1], ev_np, ev_nr}};
+    } guard{{ev_update, ev_panels, ev_left[0], ev_left[1], ev_np, ev_nr[0], ev_nr[1]}};
     // interchanges left of block K once its panels are done (`done_on`:
     // where they ran); the event guards the interchange lists' slot
     auto left_swaps = [&](int K, int Kend, cudaStream_t done_on) -> int {

@@ -159,6 +159,29 @@ def test_mixed_fp8_escalation_chain_reaches_fp64():
     assert eta_of(a, x.cpu().numpy(), b) <= 1e-14
 
 
+@pytest.mark.parametrize("width", ["32", "64"])
+def test_mixed_nested_lookahead_is_neutral(monkeypatch, width):
+    """Inside a block, the next panel's interchanges, U12 and update applied
+    by the next panel kernel itself (the FP32 32-column cluster kernel) or by
+    two kernels before it, and the rest of the block on a second stream: the
+    same arithmetic, so the refined solution is bit-identical with the nesting
+    switched off.  Width 64 mixes 64-column panels (not fused) with a narrow
+    last panel after a 64-column one (not fused either)."""
+    monkeypatch.setenv("B200LA_MIXED_PANEL_WIDTH", width)
+    n = 1100
+    a, _, b = system(n, seed=1100)
+    da, db = dev(a), dev(b)
+    out = {}
+    for flag in ("1", "0"):
+        monkeypatch.setenv("B200LA_MIXED_NESTED", flag)
+        x, res, st = la.solve_mixed(da, db, precision="fp32")
+        torch.cuda.synchronize()
+        assert st == 0 and res["converged"] == 1 and res["gmres_iterations"] == 0, res
+        out[flag] = (x.cpu().numpy(), res)
+    assert out["1"][1]["iterations"] == out["0"][1]["iterations"]
+    assert np.array_equal(out["1"][0], out["0"][0])
+
+
 @pytest.mark.parametrize("precision", ["fp32", "tf32", "fp8"])
 @pytest.mark.parametrize("n", [777, 1300, 2048])
 def test_mixed_lookahead_is_neutral(monkeypatch, precision, n):
