@@ -441,9 +441,15 @@ __global__ void __launch_bounds__(128, 1) k_tc_update(const __grid_constant__ CU
 // ---------------------------------------------------------------------------
 constexpr int kTcpThreads = 192;
 
+// Epilogue staging: each of the 4 epilogue warps turns its 32 rows x 32
+// columns of the accumulator (thread = row, as tcgen05.ld delivers them)
+// into row-contiguous pieces for coalesced C traffic.
+constexpr int kTcpEpiLd = 33;
+constexpr size_t kTcpEpiBytes = (size_t)4 * 32 * kTcpEpiLd * sizeof(float);
+
 template <bool SPLIT3> constexpr size_t tcp_smem_bytes()
 {
-    return (size_t)tc_stages<SPLIT3>() * tc_stage_bytes<SPLIT3>() + 1024 + 256;
+    return (size_t)tc_stages<SPLIT3>() * tc_stage_bytes<SPLIT3>() + 1024 + 256 + kTcpEpiBytes;
 }
 
 template <int KIND, bool SPLIT3>
@@ -469,6 +475,7 @@ __global__ void __launch_bounds__(kTcpThreads, 1) k_tc_update_persistent(const _
     uint32_t*      tmem_ptr  = reinterpret_cast<uint32_t*>(mma_done + 1);
     int*           s_fail    = reinterpret_cast<int*>(tmem_ptr + 1);
     int*           s_issued  = s_fail + 1;  // stage-ring loads issued
+    float*         epi       = reinterpret_cast<float*>(base + (size_t)S * SB + 256);  // [4][32][kTcpEpiLd]
 
     const int warp   = threadIdx.x >> 5;
     const int lane   = threadIdx.x & 31;
@@ -643,73 +650,94 @@ __global__ void __launch_bounds__(kTcpThreads, 1) k_tc_update_persistent(const _
             const int  n0     = (t / Mt) * kTcBN;
             const int  r      = m0 + row;
             const bool row_ok = r < M;
-            float*     crow   = C + (size_t)(row_ok ? r : 0) * ldc;
-            float4     cv[8], cn[8];
-            auto       fast_at = [&](int j) { return row_ok && vec && n0 + j * 32 + 32 <= N; };
-            auto       load_c  = [&](int j, float4(&dst)[8]) {
-                const float4* p = reinterpret_cast<const float4*>(crow + n0 + j * 32);
+            // C traffic in row-contiguous pieces: lane (rr, c4) reads and writes
+            // columns c4..c4+3 of the warp's rows rr, rr + 4, ..., rr + 28
+            float*    S   = epi + q * 32 * kTcpEpiLd;
+            const int rr  = lane >> 3;
+            const int c4  = (lane & 7) * 4;
+            const int wr0 = m0 + q * 32;  // the warp's first row
+            float4    cv[8], cn[8], cn2[8];  // chunks j, j + 1, j + 2 of C in flight
+            auto      load_c = [&](int j, float4(&dst)[8]) {
+                const int c = n0 + j * 32 + c4;
 #pragma unroll
-                for (int qq = 0; qq < 8; ++qq)
+                for (int i = 0; i < 8; ++i)
                 {
-                    dst[qq] = p[qq];
-                }
-            };
-            if (fast_at(0))
-            {
-                load_c(0, cv);
-            }
-#pragma unroll 1
-            for (int j = 0; j < kTcBN / 32; ++j)
-            {
-                const int  c0   = n0 + j * 32;
-                const bool fast = fast_at(j);
-                if (j + 1 < kTcBN / 32 && fast_at(j + 1))
-                {
-                    load_c(j + 1, cn);
-                }
-                float v[32];
-                tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(acc * kTcBN + j * 32), v);
-                if (row_ok)
-                {
-                    if constexpr (KIND == TC_FP8)
+                    const int rw = wr0 + rr + 4 * i;
+                    if (rw < M && vec && c + 4 <= N)
                     {
-                        const float ra = inv_sa[r];
-#pragma unroll
-                        for (int qq = 0; qq < 32; ++qq)
-                        {
-                            v[qq] *= ra * (c0 + qq < N ? inv_sb[c0 + qq] : 0.f);
-                        }
-                    }
-                    if (fast)
-                    {
-                        float4* p = reinterpret_cast<float4*>(crow + c0);
-#pragma unroll
-                        for (int qq = 0; qq < 8; ++qq)
-                        {
-                            float4 x = cv[qq];
-                            x.x -= v[4 * qq];
-                            x.y -= v[4 * qq + 1];
-                            x.z -= v[4 * qq + 2];
-                            x.w -= v[4 * qq + 3];
-                            p[qq] = x;
-                        }
+                        dst[i] = *reinterpret_cast<const float4*>(C + (size_t)rw * ldc + c);
                     }
                     else
                     {
-#pragma unroll
-                        for (int qq = 0; qq < 32; ++qq)
-                        {
-                            if (c0 + qq < N)
-                            {
-                                crow[c0 + qq] -= v[qq];
-                            }
-                        }
+                        const float* pc = C + (size_t)(rw < M ? rw : 0) * ldc;
+                        dst[i].x        = (rw < M && c < N) ? pc[c] : 0.f;
+                        dst[i].y        = (rw < M && c + 1 < N) ? pc[c + 1] : 0.f;
+                        dst[i].z        = (rw < M && c + 2 < N) ? pc[c + 2] : 0.f;
+                        dst[i].w        = (rw < M && c + 3 < N) ? pc[c + 3] : 0.f;
                     }
                 }
+            };
+            load_c(0, cv);
+            load_c(1, cn);
+#pragma unroll 1
+            for (int j = 0; j < kTcBN / 32; ++j)
+            {
+                const int c0 = n0 + j * 32;
+                if (j + 2 < kTcBN / 32)
+                {
+                    load_c(j + 2, cn2);
+                }
+                float v[32];
+                tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(acc * kTcBN + j * 32), v);
+                if constexpr (KIND == TC_FP8)
+                {
+                    const float ra = row_ok ? inv_sa[r] : 0.f;
+#pragma unroll
+                    for (int qq = 0; qq < 32; ++qq)
+                    {
+                        v[qq] *= ra * (c0 + qq < N ? inv_sb[c0 + qq] : 0.f);
+                    }
+                }
+#pragma unroll
+                for (int qq = 0; qq < 32; ++qq)
+                {
+                    S[lane * kTcpEpiLd + qq] = v[qq];
+                }
+                __syncwarp();
+#pragma unroll
+                for (int i = 0; i < 8; ++i)
+                {
+                    const int rl = rr + 4 * i;
+                    const int rw = wr0 + rl;
+                    const int c  = c0 + c4;
+                    float4    x  = cv[i];
+                    x.x -= S[rl * kTcpEpiLd + c4];
+                    x.y -= S[rl * kTcpEpiLd + c4 + 1];
+                    x.z -= S[rl * kTcpEpiLd + c4 + 2];
+                    x.w -= S[rl * kTcpEpiLd + c4 + 3];
+                    if (rw < M && vec && c + 4 <= N)
+                    {
+                        *reinterpret_cast<float4*>(C + (size_t)rw * ldc + c) = x;
+                    }
+                    else if (rw < M)
+                    {
+                        float* pc = C + (size_t)rw * ldc;
+                        if (c < N)
+                            pc[c] = x.x;
+                        if (c + 1 < N)
+                            pc[c + 1] = x.y;
+                        if (c + 2 < N)
+                            pc[c + 2] = x.z;
+                        if (c + 3 < N)
+                            pc[c + 3] = x.w;
+                    }
+                }
+                __syncwarp();
 #pragma unroll
                 for (int qq = 0; qq < 8; ++qq)
                 {
                     cv[qq] = cn[qq];
+                    cn[qq] = cn2[qq];
                 }
             }
             tc_fence_before();
