@@ -430,22 +430,24 @@ __global__ void __launch_bounds__(128, 1) k_tc_update(const __grid_constant__ CU
 //   * warp 1: allocates 512 TMEM columns; lane 0 issues the MMAs of tile i
 //     into accumulator i % 2 once the epilogue has released it, and commits
 //     the accumulator to acc_full[i % 2];
-//   * warps 2..5: epilogue, one row of the tile per thread (warp w reads
-//     TMEM lanes 32 (w % 4) ...), C -= acc in 32-column chunks with the
-//     next chunk's C loads in flight, then release the accumulator
-//     (acc_empty, 128 arrivals); the C rows of the CTA's next tile are
+//   * warps 2..9: epilogue, two warps per TMEM lane quarter (warp w reads
+//     TMEM lanes 32 (w % 4) ...; warps 2..5 take the tile's first 128
+//     columns, 6..9 the last 128), C -= acc in 32-column chunks with the
+//     next chunks' C loads in flight, then release the accumulator
+//     (acc_empty, 256 arrivals); the C rows of the CTA's next tile are
 //     prefetched into L2 when a tile's epilogue starts.
 // The per-element arithmetic is that of k_tc_update.  Every wait is bounded;
 // on a timeout the CTA records the error, stops issuing, drains its loads
 // and MMAs in flight (bounded) and frees its tensor memory.
 // ---------------------------------------------------------------------------
-constexpr int kTcpThreads = 192;
+constexpr int kTcpThreads = 320;  // 2 producer/MMA warps + 8 epilogue warps
+constexpr int kTcpEpiWarps = 8;
 
-// Epilogue staging: each of the 4 epilogue warps turns its 32 rows x 32
+// Epilogue staging: each of the 8 epilogue warps turns its 32 rows x 32
 // columns of the accumulator (thread = row, as tcgen05.ld delivers them)
 // into row-contiguous pieces for coalesced C traffic.
 constexpr int kTcpEpiLd = 33;
-constexpr size_t kTcpEpiBytes = (size_t)4 * 32 * kTcpEpiLd * sizeof(float);
+constexpr size_t kTcpEpiBytes = (size_t)8 * 32 * kTcpEpiLd * sizeof(float);
 
 template <bool SPLIT3> constexpr size_t tcp_smem_bytes()
 {
@@ -475,7 +477,7 @@ __global__ void __launch_bounds__(kTcpThreads, 1) k_tc_update_persistent(const _
     uint32_t*      tmem_ptr  = reinterpret_cast<uint32_t*>(mma_done + 1);
     int*           s_fail    = reinterpret_cast<int*>(tmem_ptr + 1);
     int*           s_issued  = s_fail + 1;  // stage-ring loads issued
-    float*         epi       = reinterpret_cast<float*>(base + (size_t)S * SB + 256);  // [4][32][kTcpEpiLd]
+    float*         epi       = reinterpret_cast<float*>(base + (size_t)S * SB + 256);  // [8][32][kTcpEpiLd]
 
     const int warp   = threadIdx.x >> 5;
     const int lane   = threadIdx.x & 31;
@@ -493,8 +495,8 @@ __global__ void __launch_bounds__(kTcpThreads, 1) k_tc_update_persistent(const _
         }
         mbar_init(&acc_full[0], 1);
         mbar_init(&acc_full[1], 1);
-        mbar_init(&acc_empty[0], 128);
-        mbar_init(&acc_empty[1], 128);
+        mbar_init(&acc_empty[0], 32 * kTcpEpiWarps);
+        mbar_init(&acc_empty[1], 32 * kTcpEpiWarps);
         mbar_init(mma_done, 1);
         *s_fail   = 0;
         *s_issued = 0;
@@ -608,21 +610,23 @@ __global__ void __launch_bounds__(kTcpThreads, 1) k_tc_update_persistent(const _
     }
     else
     {
-        // epilogue warps: TMEM lane quarter q = warp % 4
+        // epilogue warps: TMEM lane quarter q = warp % 4, column half h
         const int  q   = warp & 3;
+        const int  h   = (warp - 2) >> 2;
         const int  row = q * 32 + lane;
         const bool vec = ((ldc & 3) == 0) && ((reinterpret_cast<uintptr_t>(C) & 15) == 0);
+        constexpr int HC = kTcBN / 2;  // columns of a half
         auto prefetch_rows = [&](int t) {
             if (t >= tiles_)
             {
                 return;
             }
             const int r  = (t % Mt) * kTcBM + row;
-            const int n0 = (t / Mt) * kTcBN;
-            if (r < M && n0 + kTcBN <= N && vec)
+            const int n0 = (t / Mt) * kTcBN + h * HC;
+            if (r < M && n0 + HC <= N && vec)
             {
                 asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(C + (size_t)r * ldc + n0),
-                    "r"(kTcBN * 4)
+                    "r"(HC * 4)
                     : "memory");
             }
         };
@@ -652,7 +656,7 @@ __global__ void __launch_bounds__(kTcpThreads, 1) k_tc_update_persistent(const _
             const bool row_ok = r < M;
             // C traffic in row-contiguous pieces: lane (rr, c4) reads and writes
             // columns c4..c4+3 of the warp's rows rr, rr + 4, ..., rr + 28
-            float*    S   = epi + q * 32 * kTcpEpiLd;
+            float*    S   = epi + (warp - 2) * 32 * kTcpEpiLd;
             const int rr  = lane >> 3;
             const int c4  = (lane & 7) * 4;
             const int wr0 = m0 + q * 32;  // the warp's first row
@@ -677,15 +681,33 @@ __global__ void __launch_bounds__(kTcpThreads, 1) k_tc_update_persistent(const _
                     }
                 }
             };
-            load_c(0, cv);
-            load_c(1, cn);
+            // this warp's chunks [j0, j0 + NJ); FP8 keeps one chunk ahead
+            // (its scale loads need the registers), the others two
+            constexpr int NJ    = HC / 32;
+            constexpr int AHEAD = KIND == TC_FP8 ? 1 : 2;
+            const int     j0    = h * NJ;
+            load_c(j0, cv);
+            if constexpr (AHEAD == 2)
+            {
+                load_c(j0 + 1, cn);
+            }
 #pragma unroll 1
-            for (int j = 0; j < kTcBN / 32; ++j)
+            for (int j = j0; j < j0 + NJ; ++j)
             {
                 const int c0 = n0 + j * 32;
-                if (j + 2 < kTcBN / 32)
+                if constexpr (AHEAD == 2)
                 {
-                    load_c(j + 2, cn2);
+                    if (j + 2 < j0 + NJ)
+                    {
+                        load_c(j + 2, cn2);
+                    }
+                }
+                else
+                {
+                    if (j + 1 < j0 + NJ)
+                    {
+                        load_c(j + 1, cn);
+                    }
                 }
                 float v[32];
                 tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(acc * kTcBN + j * 32), v);
@@ -737,7 +759,10 @@ __global__ void __launch_bounds__(kTcpThreads, 1) k_tc_update_persistent(const _
                 for (int qq = 0; qq < 8; ++qq)
                 {
                     cv[qq] = cn[qq];
-                    cn[qq] = cn2[qq];
+                    if constexpr (AHEAD == 2)
+                    {
+                        cn[qq] = cn2[qq];
+                    }
                 }
             }
             tc_fence_before();

@@ -36,6 +36,28 @@ def test_mixed_reaches_fp64_accuracy(port, precision, n):
     assert np.abs(xs - x_ref).max() / np.abs(x_ref).max() < 1e-9
 
 
+@pytest.mark.parametrize("precision", ["bf16", "fp16", "fp8"])
+def test_mixed_low_precision_at_4096(precision):
+    """The low-precision factorizations at n = 4096 (the conditioning
+    sweep's order; kappa = 1e2 by the sweep's Householder construction): the
+    refined solution reaches eta <= 1e-14 and agrees with the plain FP64 LU
+    solve (bit-identical to the reference's) to the conditioning."""
+    from linearalgebra_b200 import selector
+    n = 4096
+    a, b, _ = selector.make_system(n, 1e2, 4096)
+    x, res, st = la.solve_mixed(a, b, precision=precision, tolerance=1e-14)
+    torch.cuda.synchronize()
+    assert st == 0 and res["converged"] == 1, res
+    x64, res64, st64 = la.solve_mixed(a, b, precision="fp64", tolerance=1e-14)
+    torch.cuda.synchronize()
+    assert st64 == 0, res64
+    anorm = a.abs().sum(1).max()
+    eta = ((b - a @ x).abs().max() / (anorm * x.abs().max() + b.abs().max())).item()
+    assert eta <= 1e-14, eta
+    diff = ((x - x64).abs().max() / x64.abs().max()).item()
+    assert diff < 1e-10, diff  # measured 1e-13..7e-13 for this system class
+
+
 def test_mixed_64_column_panels(port, monkeypatch):
     """64-column cluster panels (B200LA_MIXED_PANEL_WIDTH=64) instead of the
     default 32-column ones: same accuracy."""
