@@ -89,3 +89,29 @@ def test_no_alloc_scratch_covers_its_largest_order():
         for n in (1, 129, 4096, 16384):
             size = lib.b200la_dgesv_workspace_size(n, mode)
             assert 0 < size <= 1 << 20, (mode, n, size)
+
+
+def test_batched_table_rules_and_workspace_host_side():
+    """b200la_batched_table_valid (host only): panel widths the kernel is
+    built for (FP32 16/32, FP64 8/16), every bucket's largest order fitting
+    its group's shared memory and factor scratch; the workspace holds one
+    2 MiB factor slot per CTA: min(total_v, 192) slots."""
+    from linearalgebra_b200 import _lib
+    from linearalgebra_b200.batched import default_table, entry, table_valid
+
+    lib = _lib.load()
+    for prec in (_lib.PREC_FP32, _lib.PREC_FP64):
+        assert table_valid(prec, default_table(prec))
+    whole_cta = [entry(32, 256)] * 8
+    assert table_valid(_lib.PREC_FP32, whole_cta)
+    assert not table_valid(_lib.PREC_FP32, [entry(24, 256)] * 8)   # no kernel for width 24
+    assert not table_valid(_lib.PREC_FP64, whole_cta)              # FP64 goes up to width 16
+    assert table_valid(_lib.PREC_FP64, [entry(16, 256)] * 8)
+    # a 512-order system does not fit a 64-thread group's quarter of the CTA
+    assert not table_valid(_lib.PREC_FP32, [entry(32, 64)] * 8)
+    slot = 512 * 512 * 8
+    small = lib.b200la_dgesv_batched_workspace_size(10 * 16 * 16, 10 * 16, _lib.PREC_FP32)
+    large = lib.b200la_dgesv_batched_workspace_size(20000 * 300 * 300, 20000 * 300, _lib.PREC_FP32)
+    # the count is bounded by total_v (every system has at least one row)
+    assert 160 * slot <= small < 161 * slot
+    assert 192 * slot <= large < 193 * slot
