@@ -741,12 +741,12 @@ def cusolver_reference_seconds(A, b, stream, steps: int = 2):
 # ---------------------------------------------------------------------------
 # DRAM bytes (ncu dram__bytes_read.sum + dram__bytes_write.sum) per algorithmic
 # byte of the dominant kernels, from one capture each on a smaller case
-# (profiles/): the tensor-core update at n=8192 (M=6400, N=6144 launch:
-# 287.2 of 314.6 MB) and the FP64 trailing update (DMMA band kernel) at
-# n=4096 (rest=3712: 168.8 of 220.5 MB; the rest of the writes were still
-# in L2 when the launch ended).  Traffic grows with the C tile bytes, so it
-# scales to a full launch by the algorithmic bytes.
-TRAFFIC_PER_ALGORITHMIC_BYTE = {5: 0.913, 2: 0.766}
+# (profiles/): the persistent tensor-core update at n=4096 (the M=3328,
+# N=3072 launch beside the panels: 55.0 of 81.8 MB; its last tiles' C writes
+# were still in L2 when the launch ended) and the FP64 trailing update (DMMA
+# band kernel) at n=4096 (rest=3712: 168.8 of 220.5 MB).  Traffic grows with
+# the C tile bytes, so it scales to a full launch by the algorithmic bytes.
+TRAFFIC_PER_ALGORITHMIC_BYTE = {5: 0.673, 2: 0.766}
 
 CLASS_NAMES = {0: "panel", 1: "laswp_u12", 2: "trailing", 3: "solve", 4: "gemm", 5: "tc_update",
                6: "residual", 7: "batched", 8: "operand_prep", 9: "selector", 10: "inversion_gemm",
