@@ -436,10 +436,14 @@ B200LA_API int b200la_dsolve_selected(const double* a, int64_t n, const double* 
  * whose refinement stalls are refactored in FP64 by a second persistent
  * launch that skips all others) or B200LA_PREC_FP64 (FP64 LU + refinement).
  * nb_table[8]: per order bucket of 64 (the autotuner's choice), bits 0-7 the
- * panel width (1..32 for FP32 factors, 1..16 for FP64) and bits 8-15 the
- * threads that solve one system / 32 (2 or 4; 0 = a whole CTA of 256): a CTA
- * solves 256 / that many systems at once.  b200la_batched_table_valid says
- * whether every bucket's largest order fits its group's shared memory.
+ * panel width (16 or 32 for FP32 factors, 8 or 16 for FP64; another width
+ * falls back to the largest) and bits 8-15 the threads that solve one
+ * system / 32 (2 or 4; 0 = a whole CTA of 256): a CTA solves 256 / that many
+ * systems at once.  b200la_batched_table_valid says whether every width is
+ * one of those and every bucket's largest order fits its group's shared
+ * memory and factor scratch.  The workspace holds one 2 MiB factor scratch
+ * slot per CTA, min(total_v, 192) slots (a batch has at most total_v
+ * systems); the systems are factored there, A is only read.
  * Asynchronous.  Extension: the reference has no batched solver. */
 B200LA_API size_t b200la_dgesv_batched_workspace_size(int64_t total_a, int64_t total_v, int precision);
 /* 1 if the host array table[8] is a valid nb_table for `precision`, else 0. */
