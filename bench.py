@@ -63,9 +63,11 @@ def parse():
     p.add_argument("--no-cholesky", action="store_true")
     p.add_argument("--no-transpose", action="store_true")
     p.add_argument("--tp-n", type=int, default=16384, help="order of the square transpose measurement")
-    p.add_argument("--no-configs", action="store_true",
-                   help="skip config 1 (n=512), the rest of config 2 (BF16/FP16, nrhs=64) and config 3 (sweep)")
-    p.add_argument("--selector-systems", type=int, default=5000, help="held-out systems of config 5 (0: skip)")
+    p.add_argument("--no-side-workloads", "--no-configs", dest="no_side_workloads", action="store_true",
+                   help="skip the n=512 solve, the BF16/FP16 and nrhs=64 solves at n=16384 and the "
+                        "conditioning sweep at n=4096/8192")
+    p.add_argument("--selector-systems", type=int, default=5000,
+                   help="held-out systems of the precision selector's stream (0: skip)")
     return p.parse_args()
 
 
@@ -889,10 +891,10 @@ def run_batched(args, world, rank, local):
 
 
 # ---------------------------------------------------------------------------
-# config 1: plain FP64 LU + solve at n = 512 (latency-bound), beside the
+# n = 512: plain FP64 LU + solve (latency-bound), beside the
 # mixed solve and the reference's NATIVE CPU solve of the same system
 # ---------------------------------------------------------------------------
-def run_config1(args, local, fp64_peak):
+def run_n512(args, local, fp64_peak):
     import numpy as np
     import torch
 
@@ -958,9 +960,9 @@ def run_config1(args, local, fp64_peak):
 
 
 # ---------------------------------------------------------------------------
-# config 2, the rest: BF16 and FP16 factorizations and nrhs = 64 at n = 16384
+# n = 16384, the rest: BF16 and FP16 factorizations and nrhs = 64
 # ---------------------------------------------------------------------------
-def run_config2_more(args, A, b, stream, local):
+def run_n16384_more(args, A, b, stream, local):
     import torch
 
     import linearalgebra_b200 as la
@@ -1049,14 +1051,14 @@ def run_config2_more(args, A, b, stream, local):
 
 
 # ---------------------------------------------------------------------------
-# config 3: conditioning sweep, n in {4096, 8192}, kappa 1e2 .. 1e10,
+# conditioning sweep, n in {4096, 8192}, kappa 1e2 .. 1e10,
 # FP8-E4M3 / BF16 / FP32 factorizations against the FP64 oracle solution
 # ---------------------------------------------------------------------------
 KAPPAS = (1e2, 1e4, 1e6, 1e8, 1e10)
 SWEEP_PRECISIONS = ("fp8", "bf16", "fp32")
 
 
-def run_config3(args, local):
+def run_conditioning_sweep(args, local):
     import torch
 
     import linearalgebra_b200 as la
@@ -1129,7 +1131,7 @@ def run_config3(args, local):
 
 
 # ---------------------------------------------------------------------------
-# config 5: the learned precision selector on the held-out stream
+# the learned precision selector on the held-out stream of systems
 # ---------------------------------------------------------------------------
 def run_selector(args):
     from linearalgebra_b200 import selector
@@ -1366,14 +1368,14 @@ def run_b200(args, world, rank, local):
     if not args.no_transpose:
         transpose = run_transpose(args, world, rank, local)
 
-    configs = {}
-    if rank == 0 and world == 1 and not args.no_configs:
+    side = {}
+    if rank == 0 and world == 1 and not args.no_side_workloads:
         fp64_peak = measured_fp64_peak_tflops()
-        configs["config1_n512"] = run_config1(args, local, fp64_peak)
-        configs["config2_more"] = run_config2_more(args, A, b, stream, local)
-        configs["config3_sweep"] = run_config3(args, local)
+        side["solve_n512"] = run_n512(args, local, fp64_peak)
+        side["mixed_n16384_bf16_fp16_nrhs64"] = run_n16384_more(args, A, b, stream, local)
+        side["conditioning_sweep_n4096_n8192"] = run_conditioning_sweep(args, local)
     if rank == 0 and world == 1 and args.selector_systems > 0:
-        configs["config5_selector"] = run_selector(args)
+        side["precision_selector"] = run_selector(args)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -1418,7 +1420,7 @@ def run_b200(args, world, rank, local):
             "multiplication": multiplication,
             "cholesky": cholesky,
             "transpose": transpose,
-            **configs,
+            **side,
             "clocks": clk,
             "peaks": peaks,
         }

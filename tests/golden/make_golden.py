@@ -77,12 +77,12 @@ def main() -> None:
     # 3. the n=512 plain FP64 LU + solve workload: A ~ N(0,1), x_true ~ U[-1,1]
     a, x_true, b = system(512, seed=512)
     m, piv, x = ref.gesv(a, b)
-    out["cfg1_a_sha"] = np.array(sha(a))
-    out["cfg1_b_sha"] = np.array(sha(b))
-    out["cfg1_lu_sha"] = np.array(sha(m))
-    out["cfg1_piv"] = piv
-    out["cfg1_x"] = x
-    out["cfg1_lu_diag"] = np.diag(m).copy()
+    out["n512_a_sha"] = np.array(sha(a))
+    out["n512_b_sha"] = np.array(sha(b))
+    out["n512_lu_sha"] = np.array(sha(m))
+    out["n512_piv"] = piv
+    out["n512_x"] = x
+    out["n512_lu_diag"] = np.diag(m).copy()
 
     # 4. triangular solver known-answer cases (reference outputs)
     for key, case in triangular_cases(np.float64).items():

@@ -176,19 +176,19 @@ def test_lu_float32_bitwise_vs_oracle(port):
     assert np.array_equal(lu, lu_o)
 
 
-def test_config1_solve_parity(port, golden):
+def test_n512_solve_parity(port, golden):
     """n=512 plain FP64 LU + solve: same pivots, same factors, eta <= 10 n eps."""
     n = 512
     a, x_true, b = system(n, seed=512)
     m, x = dev(a), dev(b)
     piv = la.gesv(m, x)
     torch.cuda.synchronize()
-    assert np.array_equal(piv.cpu().numpy(), golden["cfg1_piv"])
-    assert sha(m.cpu().numpy()) == str(golden["cfg1_lu_sha"])
+    assert np.array_equal(piv.cpu().numpy(), golden["n512_piv"])
+    assert sha(m.cpu().numpy()) == str(golden["n512_lu_sha"])
     xs = x.cpu().numpy()
     eta = port.backward_error(a, xs, b)
     assert eta <= 10 * n * EPS64, eta
-    x_ref = golden["cfg1_x"]
+    x_ref = golden["n512_x"]
     assert port.backward_error(a, x_ref, b) <= 10 * n * EPS64
     assert np.max(np.abs(xs - x_ref)) / np.max(np.abs(x_ref)) < 1e-11
 

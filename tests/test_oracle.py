@@ -61,14 +61,14 @@ def test_port_known_answers(port, golden, name, dt, npdt):
     assert np.max(np.abs(r - a)) <= tol
 
 
-def test_port_config1_solve_matches_golden(port, golden):
+def test_port_n512_solve_matches_golden(port, golden):
     a, x_true, b = system(512, seed=512)
-    assert sha(a) == str(golden["cfg1_a_sha"])
-    assert sha(b) == str(golden["cfg1_b_sha"])
+    assert sha(a) == str(golden["n512_a_sha"])
+    assert sha(b) == str(golden["n512_b_sha"])
     m, piv, x = port.gesv(a, b)
-    assert np.array_equal(piv, golden["cfg1_piv"])
-    assert sha(m) == str(golden["cfg1_lu_sha"])
-    assert np.array_equal(x, golden["cfg1_x"])
+    assert np.array_equal(piv, golden["n512_piv"])
+    assert sha(m) == str(golden["n512_lu_sha"])
+    assert np.array_equal(x, golden["n512_x"])
     eta = port.backward_error(a, x, b)
     assert eta <= 10 * 512 * EPS64
     assert port.min_pivot_gap(a) > 1e-9
