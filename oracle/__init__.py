@@ -192,8 +192,10 @@ class Oracle:
         return c
 
     def getri(self, a: np.ndarray, mode: int = LU_LINEAR_SOLVER, pivot=None):
-        """inversion LU modes on copies; returns (m, pivot, status): m holds
-        the inverse, or the factors when mode 1 met an exact zero pivot."""
+        """inversion on copies, all four modes (1, 2: LU; 3, 4: Cholesky);
+        returns (m, pivot, status): m holds the inverse, or the factors when
+        mode 1 met an exact zero pivot (the partial Cholesky factor when mode
+        3 met a non-positive one; status is then that 1-based index)."""
         m = np.ascontiguousarray(a).copy()
         n = m.shape[0]
         piv = np.full(n, -1, dtype=np.int64) if pivot is None else np.ascontiguousarray(pivot, dtype=np.int64).copy()

@@ -338,6 +338,66 @@ int OR_FN(gesv)(T* m, int64_t* pivot, int64_t n, T* x, int mode)
     return -1;
 }
 
+/* Inverse from a lower Cholesky factor, inversion_native.cpp:306-410
+ * (cholesky_invert), three passes over the lower triangle of m:
+ *  A. X = L^-1 in place, column j = 0..n-1 in order: x_jj = 1 / l_jj, then
+ *     rows i = j+1..n-1 in order x_ij = -dot(m_i[j..i), x[j..i) of column j)
+ *     / l_ii (row i right of column j and its diagonal still hold L);
+ *  B. xt = X^T (only q >= p of xt_p written and read);
+ *  C. a_ij for i <= j = dot(xt_i[j..n), xt_j[j..n)), then the lower
+ *     triangle copied from the upper.
+ * invert_dot (:147-204) is compiled without its vector branch in the
+ * reference build; its loop rounds like dots_.  Returns -2 if the scratch
+ * cannot be had. */
+static int OR_CAT(chol_invert_, SUF)(T* m, int64_t n)
+{
+    T* col = (T*)malloc((size_t)n * sizeof(T));
+    T* xt  = (T*)malloc((size_t)(n * n) * sizeof(T));
+    if (col == NULL || xt == NULL)
+    {
+        free(col);
+        free(xt);
+        return -2;
+    }
+    for (int64_t j = 0; j < n; ++j)
+    {
+        const T d        = (T)1 / m[j * n + j];
+        m[j * n + j] = d;
+        col[j]           = d;
+        for (int64_t i = j + 1; i < n; ++i)
+        {
+            T*      mi = m + i * n;
+            const T v  = -OR_CAT(dot_, SUF)(mi + j, col + j, i - j) / mi[i];
+            mi[j]      = v;
+            col[i]     = v;
+        }
+    }
+    for (int64_t p = 0; p < n; ++p)
+    {
+        for (int64_t q = p; q < n; ++q)
+        {
+            xt[p * n + q] = m[q * n + p];
+        }
+    }
+    for (int64_t j = 0; j < n; ++j)
+    {
+        for (int64_t i = 0; i <= j; ++i)
+        {
+            m[i * n + j] = OR_CAT(dot_, SUF)(xt + i * n + j, xt + j * n + j, n - j);
+        }
+    }
+    for (int64_t i = 1; i < n; ++i)
+    {
+        for (int64_t j = 0; j < i; ++j)
+        {
+            m[i * n + j] = m[j * n + i];
+        }
+    }
+    free(col);
+    free(xt);
+    return 0;
+}
+
 /* Inverse from LU factors, inversion_native.cpp:228-304 (lu_invert):
  *  - inv = I, then rows (i, pivot[i]-1) swapped for i = 0..n-1 in order;
  *  - forward, rows i = 0..n-1: row_i -= m[i][k] row_k for k = 0..i-1 in
@@ -345,15 +405,27 @@ int OR_FN(gesv)(T* m, int64_t* pivot, int64_t n, T* x, int mode)
  *  - backward, rows i = n-1..0: row_i -= m[i][k] row_k for k = i+1..n-1 in
  *    order, then row_i *= 1 / m[i][i] (a reciprocal, then products);
  *  - m = inv.
- * Mode dispatch, inversion_native.cpp:412-440: mode 1 factors m first and
+ * Mode dispatch, inversion_native.cpp:412-452: mode 1 factors m first and
  * inverts only if the factorization found no exact zero pivot (m then keeps
- * the factors); mode 2 inverts the factors and pivots as given.  Returns the
- * getrf status for mode 1, 0 for mode 2, -1 for invalid arguments. */
+ * the factors); mode 2 inverts the factors and pivots as given; mode 3
+ * factors m (lower Cholesky) and inverts only if every pivot was positive
+ * (m then keeps the partial factor); mode 4 inverts the lower factor given
+ * in m (its upper triangle is not read).  Returns the getrf (potrf) status
+ * for mode 1 (3), 0 for modes 2 and 4, -1 for invalid arguments. */
 int OR_FN(getri)(T* m, int64_t* pivot, int64_t n, int mode)
 {
-    if (m == NULL || pivot == NULL || n <= 0 || (mode != 1 && mode != 2))
+    if (m == NULL || n <= 0 || mode < 1 || mode > 4 || (mode <= 2 && pivot == NULL))
     {
         return -1;
+    }
+    if (mode >= 3)
+    {
+        const int pst = mode == 3 ? OR_FN(potrf)(m, n, 0, NULL) : 0;
+        if (pst != 0)
+        {
+            return pst;
+        }
+        return OR_CAT(chol_invert_, SUF)(m, n);
     }
     int st = 0;
     if (mode == 1)

@@ -7,9 +7,10 @@ Run from the repository root, where the reference build exists:
     make -f oracle/Makefile && python tests/golden/make_golden.py
 
 Writes tests/golden/lu_golden.npz (LU, solve, triangular solver, GEMM),
-tests/golden/inverse_golden.npz (inversion and determinant; `--inverse` writes
-only that one) and tests/golden/cholesky_golden.npz (Cholesky factor and the
-Cholesky modes of linear_solver; `--cholesky` writes only that one).  Every input is seeded (numpy PCG64) or a closed-form
+tests/golden/inverse_golden.npz (inversion in its LU and Cholesky modes, and
+the determinant; `--inverse` writes that one and the next) and
+tests/golden/cholesky_golden.npz (Cholesky factor and the Cholesky modes of
+linear_solver; `--cholesky` writes only that one).  Every input is seeded (numpy PCG64) or a closed-form
 known-answer matrix; each array's name says what it is.
 """
 from __future__ import annotations
@@ -43,6 +44,7 @@ OUT_CHOL = os.path.join(os.path.dirname(os.path.abspath(__file__)), "cholesky_go
 CHOL_SIZES = (1, 2, 3, 17, 63, 64, 65, 130, 200)
 PIVOT_CASES = ((10, 100), (12, 312), (21, 111), (45, 345), (70, 370), (95, 7095))
 INV_SIZES = (1, 2, 3, 17, 64, 65, 130, 257)
+CHOLINV_SIZES = (1, 2, 3, 17, 63, 64, 65, 130, 257)
 
 
 def sha(a: np.ndarray) -> str:
@@ -153,6 +155,30 @@ def inverse_main() -> None:
         m, piv, _ = ref.getri(a, mode=1)
         out[f"sing_{dt}_m"] = m
         out[f"sing_{dt}_piv"] = piv
+        # 5. Cholesky modes: mode 3 factors and inverts, mode 4 inverts the
+        # reference's own lower factor (same bits); a non-positive pivot
+        # leaves the partial factor
+        for n in CHOLINV_SIZES:
+            a = spd_matrix(n, seed=9000 + n, dtype=npdt)
+            inv, _, _ = ref.getri(a, mode=3)
+            f, info = ref.potrf(a)
+            assert info == 0
+            inv4, _, _ = ref.getri(f, mode=4)
+            assert sha(inv4) == sha(inv)
+            key = f"cholinv_{dt}_{n}"
+            out[key + "_a_sha"] = np.array(sha(a))
+            out[key + "_inv_sha"] = np.array(sha(inv))
+            out[key + "_absmax"] = np.array(np.abs(inv).max())
+            if n <= 17:
+                out[key + "_inv"] = inv
+        for n, fr in ((100, 70), (130, 3)):
+            a = spd_matrix(n, seed=9100 + fr, dtype=npdt, fail_row=fr)
+            m, _, _ = ref.getri(a, mode=3)
+            f, info = ref.potrf(a)
+            assert info == fr + 1 and np.array_equal(m, f)
+            out[f"cholinvfail_{dt}_{n}_{fr}_a_sha"] = np.array(sha(a))
+            out[f"cholinvfail_{dt}_{n}_{fr}_m_sha"] = np.array(sha(m))
+            out[f"cholinvfail_{dt}_{n}_{fr}_info"] = np.array(info)
     np.savez_compressed(OUT_INV, **out)
     print(f"wrote {OUT_INV}: {len(out)} arrays, {os.path.getsize(OUT_INV)} bytes")
 

@@ -11,6 +11,7 @@ from linearalgebra_b200.workloads import (
     KNOWN_ANSWER_INFO,
     known_answer_matrices,
     random_matrix,
+    spd_matrix,
     system,
     triangular_cases,
 )
@@ -209,6 +210,47 @@ def test_port_singular_inverse_leaves_factors(port, inverse_golden, dt, npdt):
     assert np.array_equal(m, lu) and np.array_equal(piv, lpiv)
 
 
+CHOLINV_SIZES = (1, 2, 3, 17, 63, 64, 65, 130, 257)
+
+
+@pytest.mark.parametrize("n", CHOLINV_SIZES)
+@pytest.mark.parametrize("dt,npdt", INV_TYPES)
+def test_port_cholesky_inverse_matches_golden_bitwise(port, inverse_golden, n, dt, npdt):
+    """inversion's CHOLESKY modes (inversion_native.cpp:306-410): mode 3
+    factors and inverts, mode 4 inverts the given lower factor; both give
+    the reference build's bits, and the result is symmetric."""
+    g = inverse_golden
+    key = f"cholinv_{dt}_{n}"
+    a = spd_matrix(n, seed=9000 + n, dtype=npdt)
+    assert sha(a) == str(g[key + "_a_sha"])
+    inv, _, st = port.getri(a, mode=3)
+    assert st == 0
+    assert sha(inv) == str(g[key + "_inv_sha"])
+    if key + "_inv" in g:
+        assert np.array_equal(inv, g[key + "_inv"])
+    assert np.array_equal(inv, inv.T)
+    f, info = port.potrf(a)
+    assert info == 0
+    # the upper triangle of a mode-4 input is not read
+    f_junk = f + np.triu(np.full((n, n), 7.0, dtype=npdt), 1)
+    inv4, _, st4 = port.getri(f_junk, mode=4)
+    assert st4 == 0 and sha(inv4) == sha(inv)
+    err = np.abs(inv.astype(np.float64) @ a.astype(np.float64) - np.eye(n)).max()
+    assert err <= (1e-12 if npdt == np.float64 else 1e-4)
+
+
+@pytest.mark.parametrize("n,fr", [(100, 70), (130, 3)])
+@pytest.mark.parametrize("dt,npdt", INV_TYPES)
+def test_port_cholesky_inverse_failed_pivot_leaves_factor(port, inverse_golden, n, fr, dt, npdt):
+    key = f"cholinvfail_{dt}_{n}_{fr}"
+    a = spd_matrix(n, seed=9100 + fr, dtype=npdt, fail_row=fr)
+    assert sha(a) == str(inverse_golden[key + "_a_sha"])
+    m, _, st = port.getri(a, mode=3)
+    assert st == fr + 1 == int(inverse_golden[key + "_info"])
+    assert sha(m) == str(inverse_golden[key + "_m_sha"])
+    assert np.array_equal(m, port.potrf(a)[0])
+
+
 def test_port_inverse_rejects_bad_mode(port):
     with pytest.raises(ValueError):
         port.getri(np.eye(3), mode=5)
@@ -224,3 +266,7 @@ def test_port_inverse_equals_reference_build(port, n):
         a = random_matrix(n, seed=88 + n, dtype=npdt)
         assert sha(port.getri(a)[0]) == sha(ref.getri(a)[0])
         assert np.array_equal(np.array(port.det(a)[0]), np.array(ref.det(a)[0]))
+        s = spd_matrix(n, seed=77 + n, dtype=npdt)
+        assert sha(port.getri(s, mode=3)[0]) == sha(ref.getri(s, mode=3)[0])
+        f = port.potrf(s)[0]
+        assert sha(port.getri(f, mode=4)[0]) == sha(ref.getri(f, mode=4)[0])
