@@ -210,20 +210,25 @@ B200LA_API int    b200la_strsm(int upper, int transpose, int unit, int64_t n, in
        const float* a, int64_t lda, const float* b, int64_t ldb, float* x, int64_t ldx,
        void* workspace, size_t workspace_bytes, void* stream);
 
-/* ---- inversion (LU modes) ---------------------------------------------------
+/* ---- inversion (LU and Cholesky modes) ----------------------------------------
  * Replaces inversion<T, Backend>::apply / ::workspace_size
  * (include/matrix_operation/inversion.h:15-53; NATIVE semantics of
- * src/matrix_operation/cpu/native/inversion_native.cpp:412-440).  m: n x n
+ * src/matrix_operation/cpu/native/inversion_native.cpp:412-452).  m: n x n
  * row-major (lda == n), overwritten with the inverse.  Mode
  * B200LA_LU_LINEAR_SOLVER factors m first (pivots written to `pivot`, or kept
  * in the workspace when pivot is NULL, as the CUDA_BLAS backend allows) and
  * leaves the factors in m when the factorization met an exact zero pivot;
  * B200LA_LU_UPFRONT_LINEAR_SOLVER inverts the factors and pivots given in m
- * and pivot.  The Cholesky modes are not provided (B200LA_NOT_SUPPORTED).
- * Asynchronous on `stream`; the factorization's status lands in the
- * workspace (b200la_workspace_status).  Workspace: one n x n scratch plus
- * O(n); the inverse agrees with the reference's to rounding, not bit for
- * bit (its entries come from GEMM-blocked substitutions). */
+ * and pivot.  B200LA_CHOLESKY_LINEAR_SOLVER factors m (lower Cholesky) and
+ * leaves the partial factor in m at a non-positive pivot;
+ * B200LA_CHOLESKY_UPFRONT_LINEAR_SOLVER inverts the lower factor given in m
+ * (its upper triangle is not read); both return an exactly symmetric
+ * inverse and ignore `pivot`.  Asynchronous on `stream`; the
+ * factorization's status (info = the 1-based row of the first zero or
+ * non-positive pivot) lands in the workspace (b200la_workspace_status).
+ * Workspace: one n x n scratch plus O(n), the same in every mode; the
+ * inverse agrees with the reference's to rounding, not bit for bit (its
+ * entries come from GEMM-blocked substitutions). */
 B200LA_API size_t b200la_dinverse_workspace_size(int64_t n, int mode);
 B200LA_API size_t b200la_sinverse_workspace_size(int64_t n, int mode);
 B200LA_API int    b200la_dinverse(double* m, int64_t* pivot, int64_t n, int mode, void* workspace,

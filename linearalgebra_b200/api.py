@@ -193,7 +193,7 @@ def transpose_out(src: torch.Tensor, dst: torch.Tensor | None = None, stream=Non
 
 
 class inversion:
-    """inversion<T, B200>, LU modes (include/matrix_operation/inversion.h:15-53)."""
+    """inversion<T, B200>, LU and Cholesky modes (include/matrix_operation/inversion.h:15-53)."""
 
     @staticmethod
     def workspace_size(lda: int, type: int = LU_LINEAR_SOLVER, dtype=torch.float64) -> int:
@@ -201,13 +201,14 @@ class inversion:
 
     @staticmethod
     def apply(m, pivot, lda: int, type: int, workspace, workspace_size: int, stream=None):
-        """Invert m in place (asynchronous).  pivot may be None in LU mode."""
+        """Invert m in place (asynchronous).  pivot may be None in LU mode and
+        is not used by the Cholesky modes."""
         f = getattr(_lib.load(), f"b200la_{_prefix(m.dtype)}inverse")
         _lib.check(f(_ptr(m), _ptr(pivot), lda, type, _ptr(workspace), workspace_size, _stream(stream)))
 
 
 class determinant:
-    """determinant<T, B200>, LU modes (include/matrix_operation/determinant.h)."""
+    """determinant<T, B200>, LU and Cholesky modes (include/matrix_operation/determinant.h)."""
 
     @staticmethod
     def workspace_size(lda: int, type: int = LU_LINEAR_SOLVER, dtype=torch.float64) -> int:
@@ -293,8 +294,9 @@ def getrs(lu: torch.Tensor, pivot: torch.Tensor, x: torch.Tensor, stream=None):
 
 def inverse(m: torch.Tensor, pivot: torch.Tensor | None = None, type: int = LU_LINEAR_SOLVER,
             stream=None):
-    """inversion LU modes in place on m.  Returns (pivot, info): info is the
-    factorization's LAPACK info (nonzero: m holds the factors, not the
+    """inversion in place on m, any of the four modes.  Returns (pivot,
+    info): info is the factorization's LAPACK info (nonzero: m holds the
+    factors -- the partial Cholesky factor in CHOLESKY mode -- not the
     inverse).  Synchronizes the stream to read it."""
     n = m.shape[0]
     if pivot is None:
@@ -309,8 +311,9 @@ def inverse(m: torch.Tensor, pivot: torch.Tensor | None = None, type: int = LU_L
 
 
 def det(m: torch.Tensor, pivot: torch.Tensor | None = None, type: int = LU_LINEAR_SOLVER, stream=None):
-    """determinant LU modes (m factored in place in LU mode).  Returns a dict
-    with det (signed), product, sign, log_abs, singular and the pivot tensor."""
+    """determinant, any of the four modes (m factored in place in the LU and
+    CHOLESKY modes).  Returns a dict with det (signed), product, sign,
+    log_abs, singular and the pivot tensor."""
     n = m.shape[0]
     if pivot is None:
         pivot = torch.empty(n, dtype=torch.int64, device=m.device)

@@ -1,12 +1,11 @@
-// inversion and determinant, LU modes, on the B200.
+// inversion and determinant on the B200.
 //
 // Replaces inversion<T, Backend>::apply / ::workspace_size
 // (include/matrix_operation/inversion.h:15-53) and determinant<T, Backend>::
-// apply / ::workspace_size (include/matrix_operation/determinant.h) for the
-// LU_LINEAR_SOLVER and LU_UPFRONT_LINEAR_SOLVER modes.  Both reuse the LU
-// factors: LU mode factors m in place with the bit-exact blocked LU of
-// lu_driver.cuh (the reference's NATIVE lu_decomposition), LU_UPFRONT takes
-// m and pivot as the caller's factors.
+// apply / ::workspace_size (include/matrix_operation/determinant.h) in all
+// four modes.  The LU modes reuse the LU factors: LU mode factors m in place
+// with the bit-exact blocked LU of lu_driver.cuh (the reference's NATIVE
+// lu_decomposition), LU_UPFRONT takes m and pivot as the caller's factors.
 //
 // Inversion, A^-1 = U^-1 L^-1 P:
 //   1. W = I (the n x n workspace);
@@ -29,6 +28,23 @@
 // order whose backward pass is a dependent chain of about n^2/2 fused
 // multiply-adds per column; no blocked order reproduces it, so the inverse
 // agrees with the reference to rounding (a normwise bound), not bit for bit.
+//
+// Inversion, Cholesky modes, A^-1 = U^-1 L^-1 with U = L^T (A = L L^T):
+//   1. CHOLESKY factors m with the bit-exact blocked Cholesky in its upper
+//      form (U in the upper triangle, the lower cleared); CHOLESKY_UPFRONT
+//      moves the caller's lower factor into the upper triangle (its upper
+//      triangle is not read, as passes A and B of inversion_native.cpp:
+//      341-375 read only the lower one);
+//   2. W = I, then W = U^-1 W by the back substitution of the LU modes;
+//   3. W = W^T = L^-1, in place;
+//   4. W = U^-1 W, the same back substitution: W = A^-1;
+//   5. m = W's upper triangle, mirrored into the lower one, so the inverse
+//      is exactly symmetric as the reference's is (inversion_native.cpp:
+//      393-409).
+// A non-positive pivot stops at step 1 with m holding the partial lower
+// factor (the upper form transposes only a complete factor), as the
+// reference's lower factorization leaves it (:440-448); the status block
+// gates steps 2-5.  Work: 2 n^3 flops, to rounding like the LU modes.
 //
 // Determinant: the product of U's diagonal in index order, one multiply at a
 // time in the input type (determinant.cpp:18-27, so bit-identical to the
@@ -383,6 +399,25 @@ __global__ void k_inv_gather(const T* __restrict__ w, const int32_t* __restrict_
     }
 }
 
+// m[r][c] = w[min(r,c)][max(r,c)]: the upper triangle of w, mirrored.  One
+// CTA per row at a time; the lower part reads w's column r (strided, once).
+template <typename T>
+__global__ void k_inv_sym_copy(const T* __restrict__ w, T* __restrict__ m, int n, const DeviceStatus* gate)
+{
+    if (gated(gate))
+    {
+        return;
+    }
+    for (int r = blockIdx.x; r < n; r += gridDim.x)
+    {
+        T* mr = m + (int64_t)r * n;
+        for (int c = threadIdx.x; c < n; c += blockDim.x)
+        {
+            mr[c] = c >= r ? w[(int64_t)r * n + c] : w[(int64_t)c * n + r];
+        }
+    }
+}
+
 // Determinant result block in the workspace.
 struct DetResult
 {
@@ -490,8 +525,8 @@ bool chol_mode(int mode)
 {
     return mode == B200LA_CHOLESKY_LINEAR_SOLVER || mode == B200LA_CHOLESKY_UPFRONT_LINEAR_SOLVER;
 }
-// inversion: the LU modes; determinant: the LU and Cholesky modes
-bool valid_mode(int mode, bool inversion) { return lu_mode(mode) || (!inversion && chol_mode(mode)); }
+// inversion and determinant: the LU and Cholesky modes
+bool valid_mode(int mode, bool) { return lu_mode(mode) || chol_mode(mode); }
 
 template <typename T> size_t ws_size(int64_t n, int mode, bool with_w)
 {
@@ -516,11 +551,6 @@ int check_args(const void* m, const int64_t* pivot, int64_t n, int mode, const c
         return set_error(B200LA_INVALID_ARGUMENT, "%s::apply: lda must be positive", op);
     }
     const bool inversion = op[0] == 'i';
-    if (inversion && chol_mode(mode))
-    {
-        return set_error(B200LA_NOT_SUPPORTED,
-            "%s: only the LU modes are provided by this backend (mode %d)", op, mode);
-    }
     if (!valid_mode(mode, inversion))
     {
         return set_error(B200LA_INVALID_ARGUMENT, "unsupported linear_solver_type (%d)", mode);
@@ -641,8 +671,12 @@ int block_solve(bool upper, int bw, int ncols, const T* a, T* x, int64_t ld, con
     return B200LA_SUCCESS;
 }
 
-// Factor (LU mode) or reset the status (LU_UPFRONT); gate = the status block.
-template <typename T> int enqueue_factor(T* m, int n, int64_t* piv, int mode, const Plan<T>& p, cudaStream_t s)
+// Factor (LU, CHOLESKY) or reset the status (the UPFRONT modes); gate = the
+// status block.  chol_upper: the Cholesky factor ends in the upper triangle
+// (U = L^T, the inversion's form; the given lower one moved there for
+// CHOLESKY_UPFRONT), else it stays lower (the determinant's form).
+template <typename T>
+int enqueue_factor(T* m, int n, int64_t* piv, int mode, const Plan<T>& p, cudaStream_t s, bool chol_upper = false)
 {
     if (mode == B200LA_LU_LINEAR_SOLVER)
     {
@@ -650,7 +684,7 @@ template <typename T> int enqueue_factor(T* m, int n, int64_t* piv, int mode, co
     }
     if (mode == B200LA_CHOLESKY_LINEAR_SOLVER)
     {
-        return enqueue_potrf<T>(m, n, false, p.gp.st, s);  // lower, as determinant.cpp factors
+        return enqueue_potrf<T>(m, n, chol_upper, p.gp.st, s);
     }
     if (mode == B200LA_CHOLESKY_UPFRONT_LINEAR_SOLVER)
     {
@@ -658,12 +692,46 @@ template <typename T> int enqueue_factor(T* m, int n, int64_t* piv, int mode, co
         k_status_init<<<1, 32, 0, s>>>(p.gp.st, nullptr);
         prof_end(KC_INV_AUX, s);
         B200LA_LAUNCH_CHECK();
+        if (chol_upper)
+        {
+            prof_begin(KC_INV_AUX, s);
+            k_chol_to_upper<T><<<grid_1d((int64_t)n * n, 256), 256, 0, s>>>(m, n, p.gp.st);
+            prof_end(KC_INV_AUX, s);
+            B200LA_LAUNCH_CHECK();
+        }
         return B200LA_SUCCESS;
     }
     prof_begin(KC_INV_AUX, s);
     k_status_init<<<1, 32, 0, s>>>(p.gp.st, p.gp.perm);
     prof_end(KC_INV_AUX, s);
     B200LA_LAUNCH_CHECK();
+    return B200LA_SUCCESS;
+}
+
+// W = U^-1 W with U the upper triangle of m (its diagonal included), all n
+// columns: from the bottom block row, the block row solved against its
+// diagonal block, then the rows above it updated by one GEMM.
+template <typename T> int upper_solve(const T* m, T* w, int n, const DeviceStatus* gate, cudaStream_t s)
+{
+    const int64_t ld      = n;
+    const int     nblocks = (n + kNB - 1) / kNB;
+    for (int b = nblocks - 1; b >= 0; --b)
+    {
+        const int k0 = b * kNB, bw = n - k0 < kNB ? n - k0 : kNB;
+        int rc = block_solve<T>(true, bw, n, m + (int64_t)k0 * ld + k0, w + (int64_t)k0 * ld, ld, gate, s);
+        if (rc != B200LA_SUCCESS)
+        {
+            return rc;
+        }
+        if (k0 > 0)
+        {
+            rc = launch_gemm<T>(k0, n, bw, m + k0, w + (int64_t)k0 * ld, w, ld, gate, s);
+            if (rc != B200LA_SUCCESS)
+            {
+                return rc;
+            }
+        }
+    }
     return B200LA_SUCCESS;
 }
 
@@ -707,26 +775,55 @@ template <typename T> int enqueue_inverse(T* m, int n, const int64_t* piv, const
             }
         }
     }
-    // W = U^-1 W: block row solve, then the rows above, all columns.
-    for (int b = nblocks - 1; b >= 0; --b)
+    const int rc = upper_solve<T>(m, p.w, n, gate, s);
+    if (rc != B200LA_SUCCESS)
     {
-        const int k0 = b * kNB, bw = n - k0 < kNB ? n - k0 : kNB;
-        int rc = block_solve<T>(true, bw, n, m + (int64_t)k0 * ld + k0, p.w + (int64_t)k0 * ld, ld, gate, s);
-        if (rc != B200LA_SUCCESS)
-        {
-            return rc;
-        }
-        if (k0 > 0)
-        {
-            rc = launch_gemm<T>(k0, n, bw, m + k0, p.w + (int64_t)k0 * ld, p.w, ld, gate, s);
-            if (rc != B200LA_SUCCESS)
-            {
-                return rc;
-            }
-        }
+        return rc;
     }
     prof_begin(KC_INV_AUX, s);
     k_inv_gather<T><<<rows, 256, 0, s>>>(p.w, p.iperm, m, n, gate);
+    prof_end(KC_INV_AUX, s);
+    B200LA_LAUNCH_CHECK();
+    return B200LA_SUCCESS;
+}
+
+// The Cholesky modes after the factor is in m's upper triangle: W = I,
+// W = U^-1 W, W = W^T, W = U^-1 W, m = W (upper triangle mirrored).
+template <typename T> int enqueue_chol_inverse(T* m, int n, const Plan<T>& p, cudaStream_t s)
+{
+    const DeviceStatus* gate = p.gp.st;
+    const int           sms  = device_sm_count();
+    const int           rows = n < 4 * sms ? n : 4 * sms;
+    prof_begin(KC_INV_AUX, s);
+    k_inv_identity<T><<<rows, 256, 0, s>>>(p.w, n, gate);
+    prof_end(KC_INV_AUX, s);
+    B200LA_LAUNCH_CHECK();
+    int rc = upper_solve<T>(m, p.w, n, gate, s);
+    if (rc != B200LA_SUCCESS)
+    {
+        return rc;
+    }
+    // in place, square: no workspace (not gated: after a failed
+    // factorization it only moves the unused scratch)
+    if constexpr (sizeof(T) == 8)
+    {
+        rc = b200la_dtranspose(n, n, p.w, nullptr, 0, s);
+    }
+    else
+    {
+        rc = b200la_stranspose(n, n, p.w, nullptr, 0, s);
+    }
+    if (rc != B200LA_SUCCESS)
+    {
+        return rc;
+    }
+    rc = upper_solve<T>(m, p.w, n, gate, s);
+    if (rc != B200LA_SUCCESS)
+    {
+        return rc;
+    }
+    prof_begin(KC_INV_AUX, s);
+    k_inv_sym_copy<T><<<rows, 256, 0, s>>>(p.w, m, n, gate);
     prof_end(KC_INV_AUX, s);
     B200LA_LAUNCH_CHECK();
     return B200LA_SUCCESS;
@@ -759,8 +856,17 @@ int inverse(T* m, int64_t* pivot, int64_t n, int mode, void* ws, size_t bytes, v
     Arena        a(ws, bytes);
     Plan<T>      p   = plan<T>(a, n, true);
     cudaStream_t s   = as_stream(stream);
-    int64_t*     piv = pivot != nullptr ? pivot : p.piv;
-    st               = enqueue_factor<T>(m, (int)n, piv, mode, p, s);
+    if (chol_mode(mode))
+    {
+        st = enqueue_factor<T>(m, (int)n, nullptr, mode, p, s, true);
+        if (st != B200LA_SUCCESS)
+        {
+            return st;
+        }
+        return enqueue_chol_inverse<T>(m, (int)n, p, s);
+    }
+    int64_t* piv = pivot != nullptr ? pivot : p.piv;
+    st           = enqueue_factor<T>(m, (int)n, piv, mode, p, s);
     if (st != B200LA_SUCCESS)
     {
         return st;

@@ -39,6 +39,24 @@ def test_workspace_sizes_are_host_side_and_consistent():
     assert lib.b200la_dgesv_workspace_size(0, 1) == 0
 
 
+def test_inversion_modes_host_side():
+    """inversion takes all four linear_solver_type modes; the Cholesky ones
+    need no pivot array and the same workspace as the LU ones."""
+    lib = _lib.load()
+    for n in (1, 64, 513):
+        for f in (lib.b200la_dinverse_workspace_size, lib.b200la_sinverse_workspace_size):
+            sizes = [f(n, mode) for mode in (1, 2, 3, 4)]
+            assert sizes[0] > 0 and len(set(sizes)) == 1
+            assert f(n, 0) == 0 and f(n, 5) == 0
+    p = 1 << 20
+    for mode in (3, 4):
+        assert lib.b200la_dinverse(p, None, 4, mode, p, 16, None) == _lib.WORKSPACE_TOO_SMALL
+        assert lib.b200la_sinverse(p, None, 4, mode, p, 16, None) == _lib.WORKSPACE_TOO_SMALL
+    assert lib.b200la_dinverse(p, None, 4, 5, p, 1 << 20, None) == _lib.INVALID_ARGUMENT
+    assert "unsupported linear_solver_type" in _lib.last_error()
+    assert lib.b200la_dinverse(p, None, 4, 2, p, 1 << 20, None) == _lib.INVALID_ARGUMENT
+
+
 def test_status_strings():
     lib = _lib.load()
     for st in (0, 1, 2, -1, -2, -3, -4, -5):

@@ -185,7 +185,7 @@ def test_invalid_arguments_raise():
     m = dev(np.eye(4))
     piv = torch.zeros(4, dtype=torch.int64, device="cuda")
     ws = api.workspace(la.inversion.workspace_size(4, la.LU_LINEAR_SOLVER))
-    for mode in (3, 4, 5, 0):  # inversion's Cholesky modes: not provided; others: invalid
+    for mode in (5, 0):  # not a linear_solver_type
         with pytest.raises(la.B200Error):
             la.inversion.apply(m, piv, 4, mode, ws, ws.numel())
     for mode in (5, 0):
