@@ -16,7 +16,6 @@ known-answer matrix; each array's name says what it is.
 from __future__ import annotations
 
 import hashlib
-import math
 import os
 import sys
 

@@ -1,7 +1,6 @@
 """transpose (include/matrix_operation/transpose.h) without a GPU: the oracle
 against numpy and the reference's NATIVE build, the C ABI's workspace sizes
 and argument checks."""
-import ctypes
 import os
 
 import numpy as np

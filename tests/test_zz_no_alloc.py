@@ -10,8 +10,6 @@ scratch keeps the previous call's contents, so the second call checks that
 everything that must start cleared is cleared).  This file is collected last
 so that a failure here does not hide the other tests.
 """
-import ctypes
-
 import numpy as np
 import pytest
 import torch
