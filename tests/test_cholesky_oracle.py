@@ -121,8 +121,9 @@ def test_port_cholesky_determinant(port, cg, dt, npdt):
         d, f, _ = port.det(a, mode=CHOLESKY_LINEAR_SOLVER)
         assert sha(f) == str(cg[f"chol_{dt}_{n}_lower_sha"])
         expect = f[0, 0]
-        for i in range(1, n):
-            expect = npdt(expect * f[i, i])
+        with np.errstate(over="ignore"):  # FP32 at n = 200 overflows to inf, as the reference's product does
+            for i in range(1, n):
+                expect = npdt(expect * f[i, i])
         assert d == expect
         d4, _, _ = port.det(f, mode=CHOLESKY_UPFRONT_LINEAR_SOLVER)
         assert np.array_equal(np.array(d4), np.array(d))
