@@ -362,6 +362,21 @@ B200LA_API int    b200la_dsolve_mixed(const double* a, int64_t n, int64_t nrhs, 
        int64_t ldb, double* x, int64_t ldx, const b200la_refine_options* options,
        b200la_refine_result* result, void* workspace, size_t workspace_bytes, void* stream);
 
+/* Mixed-precision Cholesky-IR for a symmetric positive definite A (both
+ * triangles given; the factorization reads the lower one): the Cholesky
+ * factor of an FP32 copy of A (the blocked Cholesky of the CHOLESKY modes, in
+ * FP32), used in LU form (L D^-1 and D L^T, D = diag(l_ii), identity
+ * permutation) by the same FP64 refinement, GMRES-IR and escalation as
+ * b200la_dsolve_mixed.  A non-positive pivot in FP32 ends that attempt
+ * (info = its row) and escalates to the plain FP64 LU.  options->precision is
+ * B200LA_PREC_FP32 or B200LA_PREC_FP64; same arguments, workspace
+ * (b200la_dsolve_mixed_workspace_size), result and return codes as
+ * b200la_dsolve_mixed.  Synchronous.  Extension: the reference's Cholesky
+ * solve (linear_solver_native.cpp:177-189) has no mixed-precision form. */
+B200LA_API int    b200la_dsolve_mixed_spd(const double* a, int64_t n, int64_t nrhs, const double* b,
+       int64_t ldb, double* x, int64_t ldx, const b200la_refine_options* options,
+       b200la_refine_result* result, void* workspace, size_t workspace_bytes, void* stream);
+
 /* ---- learned precision selector --------------------------------------------
  * Extension: the reference has no precision selection.
  *

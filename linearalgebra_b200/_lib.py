@@ -87,6 +87,7 @@ SIGNATURES: dict[str, tuple] = {
     "b200la_refine_default_options": (None, [_p]),
     "b200la_dsolve_mixed_workspace_size": (_sz, [_i64, _i64, _p]),
     "b200la_dsolve_mixed": (_i32, [_p, _i64, _i64, _p, _i64, _p, _i64, _p, _p, _p, _sz, _p]),
+    "b200la_dsolve_mixed_spd": (_i32, [_p, _i64, _i64, _p, _i64, _p, _i64, _p, _p, _p, _sz, _p]),
     "b200la_dgesv_batched_workspace_size": (_sz, [_i64, _i64, _i32]),
     "b200la_batched_table_valid": (_i32, [_i32, _p]),
     "b200la_dgesv_batched": (_i32, [_i64, _p, _p, _p, _p, _p, _p, _p, _i64, _i64, _i32, _p, _i32, _d, _p, _p,

@@ -369,10 +369,12 @@ def refine_options(precision="fp32", tolerance=1e-14, max_iterations=50, gmres_r
 
 
 class MixedSolver:
-    """Reusable workspace + call of b200la_dsolve_mixed for one (n, nrhs, options)."""
+    """Reusable workspace + call of b200la_dsolve_mixed (spd: the Cholesky-IR,
+    b200la_dsolve_mixed_spd) for one (n, nrhs, options)."""
 
-    def __init__(self, n, nrhs=1, device=None, **opts):
+    def __init__(self, n, nrhs=1, device=None, spd=False, **opts):
         self.n, self.nrhs = n, nrhs
+        self.entry = "b200la_dsolve_mixed_spd" if spd else "b200la_dsolve_mixed"
         self.opts = refine_options(**opts)
         lib = _lib.load()
         self.nbytes = int(lib.b200la_dsolve_mixed_workspace_size(n, nrhs, ctypes.byref(self.opts)))
@@ -385,16 +387,17 @@ class MixedSolver:
         ldb = 1 if b.dim() == 1 else b.stride(0)
         ldx = 1 if x.dim() == 1 else x.stride(0)
         res = _lib.RefineResult()
-        st = _lib.load().b200la_dsolve_mixed(_ptr(a), n, nrhs, _ptr(b), ldb, _ptr(x), ldx,
-                                             ctypes.byref(self.opts), ctypes.byref(res), _ptr(self.ws),
-                                             self.nbytes, _stream(stream))
+        st = getattr(_lib.load(), self.entry)(_ptr(a), n, nrhs, _ptr(b), ldb, _ptr(x), ldx,
+                                              ctypes.byref(self.opts), ctypes.byref(res), _ptr(self.ws),
+                                              self.nbytes, _stream(stream))
         _lib.check(st, allow=(_lib.SUCCESS, _lib.NOT_CONVERGED, _lib.SINGULAR))
         return x, res.as_dict(), st
 
 
-def solve_mixed(a, b, precision="fp32", **opts):
+def solve_mixed(a, b, precision="fp32", spd=False, **opts):
     """Mixed-precision LU-IR solve of a x = b (FP64 CUDA tensors, a row-major
-    n x n, b n or n x nrhs).  Returns (x, result dict, status)."""
+    n x n, b n or n x nrhs); spd: the Cholesky-IR for a symmetric positive
+    definite a (precision fp32 or fp64).  Returns (x, result dict, status)."""
     nrhs = 1 if b.dim() == 1 else b.shape[1]
-    solver = MixedSolver(a.shape[0], nrhs, a.device, precision=precision, **opts)
+    solver = MixedSolver(a.shape[0], nrhs, a.device, spd=spd, precision=precision, **opts)
     return solver(a, b)

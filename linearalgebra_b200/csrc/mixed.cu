@@ -1343,6 +1343,42 @@ int gmres_correction(const double* a, int64_t lda, const TA* lu, int n, int rest
 // ---------------------------------------------------------------------------
 // factor / refine steps shared by the mixed and the selected solves
 // ---------------------------------------------------------------------------
+// The FP32 Cholesky factor in LU form for the Cholesky-IR: with L lower
+// (l_ij, i >= j) and D = diag(l_ii), L_u = L D^-1 (unit lower) and
+// U = D L^T satisfy L_u U = L L^T, so the LU refinement applies it with the
+// identity permutation.  One thread per strictly lower (i, j) writes
+// u_ji = l_jj l_ij and l_ij / l_jj; the diagonal is only read here.
+__global__ void k_chol_lu_pairs(float* __restrict__ a, int n, const DeviceStatus* gate)
+{
+    if (gated(gate))
+        return;
+    const int64_t total = (int64_t)n * n;
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x)
+    {
+        const int i = (int)(e / n), j = (int)(e - (e / n) * n);
+        if (j < i)
+        {
+            const float l         = a[e];
+            const float d         = a[(int64_t)j * n + j];
+            a[(int64_t)j * n + i] = d * l;
+            a[e]                  = l / d;
+        }
+    }
+}
+
+// Then u_ii = l_ii^2, and the identity permutation.
+__global__ void k_chol_lu_diag(float* __restrict__ a, int n, int32_t* __restrict__ perm, const DeviceStatus* gate)
+{
+    if (gated(gate))
+        return;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    {
+        const float d        = a[(int64_t)i * n + i];
+        a[(int64_t)i * n + i] = d * d;
+        perm[i]              = i;
+    }
+}
+
 struct SolveState
 {
     double              anorm      = 0.0;
@@ -1352,9 +1388,11 @@ struct SolveState
 
 // Factor A in `precision` into p.a32 (or p.a64 for FP64), with p.perm and the
 // inverted diagonal blocks; *info = LAPACK info.  Adds the device time to
-// out.factor_ms.  Reads ||A|| and ||b_j|| the first time.
+// out.factor_ms.  Reads ||A|| and ||b_j|| the first time.  spd: the FP32
+// factorization is the Cholesky of A's lower triangle, stored in LU form
+// (info = the first non-positive pivot's row); FP64 stays the plain LU.
 int mixed_factor(const double* a, int nn, int nr, int precision, MixedPlan& p, SolveState& ss, int* info,
-    b200la_refine_result& out, cudaEvent_t e0, cudaEvent_t e1, cudaStream_t s)
+    b200la_refine_result& out, cudaEvent_t e0, cudaEvent_t e1, cudaStream_t s, bool spd = false)
 {
     const int64_t n     = nn;
     const bool    use64 = precision == B200LA_PREC_FP64;
@@ -1370,8 +1408,20 @@ int mixed_factor(const double* a, int nn, int nr, int precision, MixedPlan& p, S
     {
         k_convert_a<<<(nn * 32 + 255) / 256, 256, 0, s>>>(a, n, p.a32, nn, p.norms);
         B200LA_LAUNCH_CHECK();
+        if (spd)
+        {
+            if ((rc = enqueue_potrf<float>(p.a32, nn, false, st, s)) != B200LA_SUCCESS)
+                return rc;
+            prof_begin(KC_CHOL_AUX, s);
+            k_chol_lu_pairs<<<grid_for(n * n), 256, 0, s>>>(p.a32, nn, st);
+            prof_end(KC_CHOL_AUX, s);
+            B200LA_LAUNCH_CHECK();
+            prof_begin(KC_CHOL_AUX, s);
+            k_chol_lu_diag<<<grid_for(n), 256, 0, s>>>(p.a32, nn, p.perm, st);
+            prof_end(KC_CHOL_AUX, s);
+        }
         // the factorization leaves its row permutation in p.perm
-        if ((rc = enqueue_getrf_mixed(p, nn, kind, split, s)) != B200LA_SUCCESS)
+        else if ((rc = enqueue_getrf_mixed(p, nn, kind, split, s)) != B200LA_SUCCESS)
             return rc;
     }
     else
@@ -1504,10 +1554,10 @@ int next_precision(int precision)
 
 // Factor-refine-escalate loop from `precision`.  With `prefactored` the FP32
 // factors (three-term TF32) are already in p (info `pre_info`) and the first
-// attempt reuses them.
+// attempt reuses them.  spd: FP32 is the Cholesky (see mixed_factor).
 int mixed_loop(const double* a, int nn, int nr, const double* b, int64_t ldb, double* x, int64_t ldx,
     int precision, bool prefactored, int pre_info, const b200la_refine_options* o, int restart, MixedPlan& p,
-    SolveState& ss, b200la_refine_result& out, cudaEvent_t e0, cudaEvent_t e1, cudaStream_t s)
+    SolveState& ss, b200la_refine_result& out, cudaEvent_t e0, cudaEvent_t e1, cudaStream_t s, bool spd = false)
 {
     int escalations = 0;
     for (;;)
@@ -1519,7 +1569,7 @@ int mixed_loop(const double* a, int nn, int nr, const double* b, int64_t ldb, do
             out.info = info;
             prefactored = false;
         }
-        else if ((rc = mixed_factor(a, nn, nr, precision, p, ss, &info, out, e0, e1, s)) != B200LA_SUCCESS &&
+        else if ((rc = mixed_factor(a, nn, nr, precision, p, ss, &info, out, e0, e1, s, spd)) != B200LA_SUCCESS &&
                  rc != B200LA_SINGULAR)
         {
             return rc;
@@ -1780,13 +1830,10 @@ static int finish_result(b200la_refine_result& out, b200la_refine_result* res)
     return out.converged ? B200LA_SUCCESS : B200LA_NOT_CONVERGED;
 }
 
-B200LA_API int b200la_dsolve_mixed(const double* a, int64_t n, int64_t nrhs, const double* b, int64_t ldb,
-    double* x, int64_t ldx, const b200la_refine_options* opts, b200la_refine_result* res, void* ws,
-    size_t ws_bytes, void* stream)
+static int solve_mixed(const double* a, int64_t n, int64_t nrhs, const double* b, int64_t ldb, double* x,
+    int64_t ldx, const b200la_refine_options* o, b200la_refine_result* res, void* ws, size_t ws_bytes,
+    void* stream, bool spd)
 {
-    b200la_refine_options d;
-    b200la_refine_default_options(&d);
-    const b200la_refine_options* o = opts ? opts : &d;
     int rc = check_mixed_call(a, n, nrhs, b, ldb, x, ldx, o, ws, ws_bytes);
     if (rc != B200LA_SUCCESS)
         return rc;
@@ -1806,9 +1853,30 @@ B200LA_API int b200la_dsolve_mixed(const double* a, int64_t n, int64_t nrhs, con
     B200LA_LAUNCH_CHECK();
     SolveState ss;
     if ((rc = mixed_loop(a, nn, nr, b, ldb, x, ldx, o->precision, false, 0, o, restart, p, ss, out, ev.e0, ev.e1,
-             s)) != B200LA_SUCCESS)
+             s, spd)) != B200LA_SUCCESS)
         return rc;
     return finish_result(out, res);
+}
+
+B200LA_API int b200la_dsolve_mixed(const double* a, int64_t n, int64_t nrhs, const double* b, int64_t ldb,
+    double* x, int64_t ldx, const b200la_refine_options* opts, b200la_refine_result* res, void* ws,
+    size_t ws_bytes, void* stream)
+{
+    b200la_refine_options d;
+    b200la_refine_default_options(&d);
+    return solve_mixed(a, n, nrhs, b, ldb, x, ldx, opts ? opts : &d, res, ws, ws_bytes, stream, false);
+}
+
+B200LA_API int b200la_dsolve_mixed_spd(const double* a, int64_t n, int64_t nrhs, const double* b, int64_t ldb,
+    double* x, int64_t ldx, const b200la_refine_options* opts, b200la_refine_result* res, void* ws,
+    size_t ws_bytes, void* stream)
+{
+    b200la_refine_options d;
+    b200la_refine_default_options(&d);
+    const b200la_refine_options* o = opts ? opts : &d;
+    if (o->precision != B200LA_PREC_FP32 && o->precision != B200LA_PREC_FP64)
+        return set_error(B200LA_INVALID_ARGUMENT, "Cholesky-IR: the factorization precision is FP32 or FP64");
+    return solve_mixed(a, n, nrhs, b, ldb, x, ldx, o, res, ws, ws_bytes, stream, true);
 }
 
 B200LA_API int b200la_selector_features(const double* a, int64_t n, float* features, void* ws, size_t ws_bytes,

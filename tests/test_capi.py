@@ -57,6 +57,27 @@ def test_inversion_modes_host_side():
     assert lib.b200la_dinverse(p, None, 4, 2, p, 1 << 20, None) == _lib.INVALID_ARGUMENT
 
 
+def test_cholesky_ir_checks_host_side():
+    """b200la_dsolve_mixed_spd factorizes in FP32 or FP64 only, and checks its
+    arguments and workspace like b200la_dsolve_mixed before any device work."""
+    lib = _lib.load()
+    p = 1 << 20
+    o = _lib.RefineOptions()
+    lib.b200la_refine_default_options(ctypes.byref(o))
+    need = lib.b200la_dsolve_mixed_workspace_size(64, 1, ctypes.byref(o))
+    assert need > 0
+    for prec in (_lib.PREC_TF32, _lib.PREC_BF16, _lib.PREC_FP16, _lib.PREC_FP8):
+        o.precision = prec
+        assert lib.b200la_dsolve_mixed_spd(p, 64, 1, p, 1, p, 1, ctypes.byref(o), None, p, need,
+                                           None) == _lib.INVALID_ARGUMENT
+        assert "FP32 or FP64" in _lib.last_error()
+    o.precision = _lib.PREC_FP32
+    assert lib.b200la_dsolve_mixed_spd(None, 64, 1, p, 1, p, 1, ctypes.byref(o), None, p, need,
+                                       None) == _lib.INVALID_ARGUMENT
+    assert lib.b200la_dsolve_mixed_spd(p, 64, 1, p, 1, p, 1, ctypes.byref(o), None, p, 16,
+                                       None) == _lib.WORKSPACE_TOO_SMALL
+
+
 def test_status_strings():
     lib = _lib.load()
     for st in (0, 1, 2, -1, -2, -3, -4, -5):
