@@ -91,6 +91,26 @@ def test_committed_weights_load():
     assert meta["systems"] >= 1000 and np.isfinite(net.params.numpy()).all()
 
 
+def test_committed_label_data_are_the_methods_outcomes():
+    """The committed training shards hold, per system, the measured time and
+    convergence of each attempted precision (FP8 and BF16 only after the one
+    above converged); FP64 always converged, and each label is the fastest
+    attempt that did."""
+    import glob
+    files = sorted(glob.glob(os.path.join(os.path.dirname(sel.__file__), "selector_data", "*.npz")))
+    if not files:
+        pytest.skip("no label data")
+    for f in files:
+        d = np.load(f)
+        ms, conv, lab = d["ms"], d["converged"].astype(bool), d["labels"]
+        assert ms.shape[1] == len(sel.CLASSES) and d["features"].shape[1] == 12
+        assert d["n"].min() >= 64 and d["n"].max() <= 4096
+        assert d["kappa"].min() >= 10 * (1 - 1e-9) and d["kappa"].max() <= 1e12 * (1 + 1e-9)
+        assert conv[:, 3].all() and not np.isnan(ms[:, 2:]).any()
+        ok = conv & ~np.isnan(ms)
+        assert np.array_equal(np.where(ok, ms, np.inf).argmin(1), lab)
+
+
 # ---------------------------------------------------------------------------
 # GPU
 # ---------------------------------------------------------------------------
