@@ -362,21 +362,39 @@ __global__ void k_row_stats(const double* __restrict__ a, int n, unsigned long l
     }
 }
 
-// [5] [10]: one thread per column, coalesced across the warp.
-__global__ void k_col_stats(const double* __restrict__ a, int n, unsigned long long* out)
+// [5] [10]: column sums of |a|, 32 columns per CTA whose kColWarps warps
+// split the rows (warp w takes rows w, w + kColWarps, ...; a warp reads 32
+// consecutive entries of a row, 256 coalesced bytes), then the warps'
+// partial sums are added in warp order in shared memory.  One thread per
+// column walking all n rows left a few CTAs latency-bound on their loads.
+constexpr int kColWarps = 32;
+
+__global__ void __launch_bounds__(32 * kColWarps) k_col_stats(const double* __restrict__ a, int n,
+    unsigned long long* out)
 {
-    const int j = blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= n)
+    __shared__ double part[kColWarps][33];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int j    = blockIdx.x * 32 + lane;
+    double    s    = 0.0;
+    if (j < n)
     {
-        return;
+        for (int i = warp; i < n; i += kColWarps)
+        {
+            s += fabs(a[(int64_t)i * n + j]);
+        }
     }
-    double s = 0.0;
-    for (int i = 0; i < n; ++i)
+    part[warp][lane] = s;
+    __syncthreads();
+    if (warp == 0 && j < n)
     {
-        s += fabs(a[(int64_t)i * n + j]);
+        double t = 0.0;
+        for (int w = 0; w < kColWarps; ++w)
+        {
+            t += part[w][lane];
+        }
+        amax_d(out + 5, t);
+        amin_d(out + 10, t);
     }
-    amax_d(out + 5, s);
-    amin_d(out + 10, s);
 }
 
 }  // namespace
@@ -397,7 +415,7 @@ int enqueue_matrix_stats(const double* a, int n, unsigned long long* out, cudaSt
     prof_begin(KC_SELECT, s);
     k_stats_init<<<1, 32, 0, s>>>(out);
     k_row_stats<<<(int)(((int64_t)n * 32 + 255) / 256), 256, 0, s>>>(a, n, out);
-    k_col_stats<<<(n + 255) / 256, 256, 0, s>>>(a, n, out);
+    k_col_stats<<<(n + 31) / 32, 32 * kColWarps, 0, s>>>(a, n, out);
     prof_end(KC_SELECT, s);
     B200LA_LAUNCH_CHECK();
     return B200LA_SUCCESS;
